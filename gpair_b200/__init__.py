@@ -1,0 +1,11 @@
+"""gpair_b200 -- B200 (sm_100a) implementation of GPAIR's image-reconstruction
+hot path: image -> DFT visibilities -> V2 / bispectrum -> chi2 + Gull-Skilling
+entropy -> analytic gradients -> nonlinear CG with strong-Wolfe line search.
+
+The compute runs in libgpair_b200.so (CUDA kernels + C ABI, include/gpair_b200.h);
+this package holds the ctypes mirror of that ABI (api), OIFITS tables (oifits),
+the seeded synthetic data generator (synth) and the build script (build).
+"""
+from .api import (IMG_CURR, IMG_TEMP, PREC_FP32, PREC_SPLIT16, PREC_TF32, GpairError, Indexed, Problem,  # noqa: F401
+                  Reconstructor, dft_tables, index_oifits, init_data, lib, problem_from_oifits, set_model,
+                  workload_problem)

@@ -1,0 +1,480 @@
+// context.cu -- device contexts, problem upload and the evaluation / CG
+// orchestration behind the extension API of gpair_b200.h.
+//
+// One criterion evaluation (gpair_criterion) = k_prep -> forward DFT ->
+// k_vis_data; one gradient evaluation (gpair_gradient) = k_adj_weights ->
+// adjoint DFT -> k_grad_finalize. gpair_cg_run chains them with the device
+// controller k_cg_ctrl, which holds every CG scalar in FP64 on the GPU; the
+// host only reads back the controller's next action (evaluate criterion,
+// evaluate gradient, or accept the step).
+#include <stdlib.h>
+#include <string.h>
+
+#include <vector>
+
+#include "gpair_internal.cuh"
+
+int gp_default_splits(int N, int nuv);
+
+static const char *k_err_names[] = {"GPAIR_OK",      "GPAIR_ERR_INVALID", "GPAIR_ERR_ALLOC",     "GPAIR_ERR_CUDA",
+                                    "GPAIR_ERR_STATE", "GPAIR_ERR_TIMEOUT", "GPAIR_ERR_NO_DEVICE", "GPAIR_ERR_NUMERIC"};
+
+extern "C" const char *gpair_strerror(int status)
+{
+    int i = -status;
+    if (i < 0 || i >= (int)(sizeof(k_err_names) / sizeof(k_err_names[0]))) return "GPAIR_ERR_UNKNOWN";
+    return k_err_names[i];
+}
+
+extern "C" const char *gpair_last_error(gpair_ctx *ctx) { return ctx ? ctx->last_error : "no context"; }
+
+#define FREE_DEV(p)              \
+    do {                         \
+        if (p) cudaFree(p);      \
+        (p) = nullptr;           \
+    } while (0)
+
+static void free_problem(gpair_ctx *c)
+{
+    FREE_DEV(c->data); FREE_DEV(c->data_err); FREE_DEV(c->mock);
+    FREE_DEV(c->tri); FREE_DEV(c->phasor); FREE_DEV(c->uvc);
+    FREE_DEV(c->fx); FREE_DEV(c->fy); FREE_DEV(c->vpart); FREE_DEV(c->visd); FREE_DEV(c->visi);
+    FREE_DEV(c->trib); FREE_DEV(c->cw); FREE_DEV(c->inc_off); FREE_DEV(c->inc_idx); FREE_DEV(c->gpart);
+    gp_tc_free(c);
+    c->have_problem = 0;
+}
+
+static void free_images(gpair_ctx *c)
+{
+    FREE_DEV(c->image); FREE_DEV(c->image_temp); FREE_DEV(c->model);
+    FREE_DEV(c->data_grad); FREE_DEV(c->entropy_grad); FREE_DEV(c->full_grad_new);
+    FREE_DEV(c->full_grad); FREE_DEV(c->grad_temp); FREE_DEV(c->descent_dir);
+    c->N = 0;
+    c->npix = 0;
+    c->have_image = 0;
+}
+
+static void set_handle(gpair_buf *h, float *p, size_t n, int id)
+{
+    h->ptr = p;
+    h->count = n;
+    h->id = id;
+}
+
+// (Re)allocate the image-sized buffers for width N; contents are zeroed.
+int gp_alloc_images(gpair_ctx *c, int N)
+{
+    if (N <= 0 || (long long)N * N > (1LL << 30)) return GPAIR_ERR_INVALID;
+    if (c->N == N && c->image) return GPAIR_OK;
+    GP_CUDA(c, cudaSetDevice(c->device));
+    free_images(c);
+    size_t n = (size_t)N * N, bytes = n * sizeof(float);
+    float **bufs[] = {&c->image, &c->image_temp, &c->model, &c->data_grad, &c->entropy_grad,
+                      &c->full_grad_new, &c->full_grad, &c->grad_temp, &c->descent_dir};
+    for (float **b : bufs) {
+        GP_CUDA(c, cudaMalloc(b, bytes));
+        GP_CUDA(c, cudaMemsetAsync(*b, 0, bytes, c->stream));
+    }
+    c->N = N;
+    c->npix = (int)n;
+    set_handle(&c->h_image, c->image, n, 0);
+    set_handle(&c->h_image_temp, c->image_temp, n, 1);
+    set_handle(&c->h_fgn, c->full_grad_new, n, 2);
+    set_handle(&c->h_fg, c->full_grad, n, 3);
+    set_handle(&c->h_dd, c->descent_dir, n, 4);
+    set_handle(&c->h_tg, c->grad_temp, n, 5);
+    set_handle(&c->h_eg, c->entropy_grad, n, 6);
+    set_handle(&c->h_dg, c->data_grad, n, 7);
+    set_handle(&c->h_model, c->model, n, 8);
+    return GPAIR_OK;
+}
+
+extern "C" int gpair_create(gpair_ctx **out, int device)
+{
+    if (!out) return GPAIR_ERR_INVALID;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= device || device < 0) return GPAIR_ERR_NO_DEVICE;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return GPAIR_ERR_NO_DEVICE;
+    if (prop.major != 10) return GPAIR_ERR_NO_DEVICE;  // built for sm_100a only
+    gpair_ctx *c = (gpair_ctx *)calloc(1, sizeof(gpair_ctx));
+    if (!c) return GPAIR_ERR_ALLOC;
+    c->device = device;
+    c->precision = GPAIR_PREC_FP32;
+    c->last_image_src = -1;
+    int rc = GPAIR_OK;
+    do {
+        if (cudaSetDevice(device) != cudaSuccess) { rc = GPAIR_ERR_CUDA; break; }
+        if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) { rc = GPAIR_ERR_CUDA; break; }
+        if (cudaMalloc(&c->sc, sizeof(DevScalars)) != cudaSuccess) { rc = GPAIR_ERR_ALLOC; break; }
+        if (cudaMemset(c->sc, 0, sizeof(DevScalars)) != cudaSuccess) { rc = GPAIR_ERR_CUDA; break; }
+        if (cudaMallocHost(&c->sc_host, sizeof(DevScalars)) != cudaSuccess) { rc = GPAIR_ERR_ALLOC; break; }
+        size_t pbytes = sizeof(double) * RED_NSLOTS * GP_MAX_PARTIALS * 4;
+        if (cudaMalloc(&c->partials, pbytes) != cudaSuccess) { rc = GPAIR_ERR_ALLOC; break; }
+    } while (0);
+    if (rc != GPAIR_OK) {
+        gpair_destroy(c);
+        return rc;
+    }
+    *out = c;
+    return GPAIR_OK;
+}
+
+extern "C" int gpair_destroy(gpair_ctx *c)
+{
+    if (!c) return GPAIR_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    free_problem(c);
+    free_images(c);
+    FREE_DEV(c->sc);
+    FREE_DEV(c->partials);
+    if (c->sc_host) cudaFreeHost(c->sc_host);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    free(c->ref_dft_x); free(c->ref_dft_y); free(c->ref_data); free(c->ref_data_err); free(c->ref_model);
+    free(c->ref_phasor); free(c->ref_uvpnt); free(c->ref_sign);
+    free(c);
+    return GPAIR_OK;
+}
+
+// CSR map uv point -> incident (triangle, vertex) slots, ascending (t, vertex)
+int gp_build_incidence(gpair_ctx *c, const int64_t *uvpnt)
+{
+    std::vector<int> off(c->nuv + 1, 0), idx((size_t)3 * c->nbis);
+    for (long long j = 0; j < 3LL * c->nbis; j++) off[uvpnt[j] + 1]++;
+    for (int k = 0; k < c->nuv; k++) off[k + 1] += off[k];
+    std::vector<int> pos(off.begin(), off.end() - 1);
+    for (long long j = 0; j < 3LL * c->nbis; j++) idx[pos[uvpnt[j]]++] = (int)j;
+    GP_CUDA(c, cudaMalloc(&c->inc_off, sizeof(int) * (c->nuv + 1)));
+    GP_CUDA(c, cudaMalloc(&c->inc_idx, sizeof(int) * (idx.empty() ? 1 : idx.size())));
+    GP_CUDA(c, cudaMemcpyAsync(c->inc_off, off.data(), sizeof(int) * (c->nuv + 1), cudaMemcpyHostToDevice, c->stream));
+    if (!idx.empty())
+        GP_CUDA(c, cudaMemcpyAsync(c->inc_idx, idx.data(), sizeof(int) * idx.size(), cudaMemcpyHostToDevice, c->stream));
+    GP_CUDA(c, cudaStreamSynchronize(c->stream));
+    return GPAIR_OK;
+}
+
+// Problem upload. uv may be NULL when the twiddles are supplied as tables
+// afterwards (reference boundary path, gpu_copy_dft).
+int gp_set_problem_core(gpair_ctx *c, int N, float pix, int nuv, const gpair_uv *uv, int npow, int nbis,
+                        const float *data, const float *data_err, const gpair_float2 *phasor, const int64_t *uvpnt,
+                        const int16_t *sign, const float *model)
+{
+    if (!c || N <= 0 || nuv < 0 || npow < 0 || nbis < 0 || npow > nuv) return GPAIR_ERR_INVALID;
+    if ((npow + 2LL * nbis) > (1LL << 31) - 1 || (long long)nuv * N > (1LL << 31)) return GPAIR_ERR_INVALID;
+    if ((npow + nbis) > 0 && (!data || !data_err)) return GPAIR_ERR_INVALID;
+    if (nbis > 0 && (!phasor || !uvpnt || !sign)) return GPAIR_ERR_INVALID;
+    for (long long j = 0; j < 3LL * nbis; j++)
+        if (uvpnt[j] < 0 || uvpnt[j] >= nuv) return GPAIR_ERR_INVALID;
+    GP_CUDA(c, cudaSetDevice(c->device));
+    int rc = gp_alloc_images(c, N);
+    if (rc) return rc;
+    free_problem(c);
+    c->pix = pix;
+    c->nuv = nuv;
+    c->npow = npow;
+    c->nbis = nbis;
+    c->ndata = npow + 2 * nbis;
+    size_t nd = c->ndata ? c->ndata : 1, nt = nbis ? nbis : 1, nk = nuv ? nuv : 1;
+    c->mt = gp_cdiv(N, 64);
+    c->splits = gp_default_splits(N, nuv ? nuv : 1);
+    GP_CUDA(c, cudaMalloc(&c->data, nd * sizeof(float)));
+    GP_CUDA(c, cudaMalloc(&c->data_err, nd * sizeof(float)));
+    GP_CUDA(c, cudaMalloc(&c->mock, nd * sizeof(float)));
+    GP_CUDA(c, cudaMalloc(&c->tri, nt * sizeof(int4)));
+    GP_CUDA(c, cudaMalloc(&c->phasor, nt * sizeof(float2)));
+    GP_CUDA(c, cudaMalloc(&c->uvc, nk * sizeof(float2)));
+    GP_CUDA(c, cudaMalloc(&c->fx, nk * N * sizeof(float2)));
+    GP_CUDA(c, cudaMalloc(&c->fy, nk * N * sizeof(float2)));
+    GP_CUDA(c, cudaMalloc(&c->vpart, (size_t)c->mt * nk * sizeof(float2)));
+    GP_CUDA(c, cudaMalloc(&c->visd, nk * sizeof(double2)));
+    GP_CUDA(c, cudaMalloc(&c->visi, nk * sizeof(float2)));
+    GP_CUDA(c, cudaMalloc(&c->cw, nk * sizeof(float2)));
+    GP_CUDA(c, cudaMalloc(&c->trib, 3 * nt * sizeof(float2)));
+    GP_CUDA(c, cudaMalloc(&c->gpart, (size_t)c->splits * c->npix * sizeof(float)));
+    GP_CUDA(c, cudaMemsetAsync(c->mock, 0, nd * sizeof(float), c->stream));
+    GP_CUDA(c, cudaMemsetAsync(c->visd, 0, nk * sizeof(double2), c->stream));
+    GP_CUDA(c, cudaMemsetAsync(c->visi, 0, nk * sizeof(float2), c->stream));
+    if (c->ndata) {
+        GP_CUDA(c, cudaMemcpyAsync(c->data, data, c->ndata * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+        GP_CUDA(c, cudaMemcpyAsync(c->data_err, data_err, c->ndata * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    }
+    std::vector<int4> tri(nt);
+    for (int t = 0; t < nbis; t++) {
+        int w = (sign[3 * t] < 0 ? 1 : 0) | (sign[3 * t + 1] < 0 ? 2 : 0) | (sign[3 * t + 2] < 0 ? 4 : 0);
+        tri[t] = make_int4((int)uvpnt[3 * t], (int)uvpnt[3 * t + 1], (int)uvpnt[3 * t + 2], w);
+    }
+    if (nbis) {
+        GP_CUDA(c, cudaMemcpyAsync(c->tri, tri.data(), nbis * sizeof(int4), cudaMemcpyHostToDevice, c->stream));
+        GP_CUDA(c, cudaMemcpyAsync(c->phasor, phasor, nbis * sizeof(float2), cudaMemcpyHostToDevice, c->stream));
+    }
+    if (model)
+        GP_CUDA(c, cudaMemcpyAsync(c->model, model, c->npix * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    // the entropy-gradient buffer starts at zero: where image <= 0 or model <= 0
+    // it keeps its previous value (gpair1/trunk/gpu.c:1332-1338, kernel_entropy_gs_grad.cl)
+    GP_CUDA(c, cudaMemsetAsync(c->entropy_grad, 0, c->npix * sizeof(float), c->stream));
+    if (uv && nuv) {
+        std::vector<float2> uvc(nuv);
+        for (int k = 0; k < nuv; k++) uvc[k] = make_float2(uv[k].u, uv[k].v);
+        GP_CUDA(c, cudaMemcpyAsync(c->uvc, uvc.data(), nuv * sizeof(float2), cudaMemcpyHostToDevice, c->stream));
+        rc = gp_gen_twiddles(c);
+        if (rc) return rc;
+    }
+    rc = gp_build_incidence(c, uvpnt);
+    if (rc) return rc;
+    c->have_problem = 1;
+    if (c->precision != GPAIR_PREC_FP32) {
+        rc = gp_tc_prepare(c);
+        if (rc) return rc;
+    }
+    GP_CUDA(c, cudaStreamSynchronize(c->stream));
+    return GPAIR_OK;
+}
+
+extern "C" int gpair_set_problem(gpair_ctx *c, int N, float pix, int nuv, const gpair_uv *uv, int npow, int nbis,
+                                 const float *data, const float *data_err, const gpair_float2 *phasor,
+                                 const int64_t *uvpnt, const int16_t *sign, const float *model)
+{
+    if (!uv && nuv > 0) return GPAIR_ERR_INVALID;
+    return gp_set_problem_core(c, N, pix, nuv, uv, npow, nbis, data, data_err, phasor, uvpnt, sign, model);
+}
+
+extern "C" int gpair_set_precision(gpair_ctx *c, int mode)
+{
+    if (!c || mode < GPAIR_PREC_FP32 || mode > GPAIR_PREC_TF32) return GPAIR_ERR_INVALID;
+    int old = c->precision;
+    c->precision = mode;
+    if (mode != GPAIR_PREC_FP32 && c->have_problem) {
+        int rc = gp_tc_prepare(c);
+        if (rc) {
+            c->precision = old;
+            return rc;
+        }
+    }
+    return GPAIR_OK;
+}
+
+extern "C" int gpair_get_precision(gpair_ctx *c) { return c ? c->precision : -1; }
+
+extern "C" int gpair_set_image(gpair_ctx *c, int which, const float *image)
+{
+    if (!c || !image || !c->image) return GPAIR_ERR_STATE;
+    float *dst = which == GPAIR_IMG_TEMP ? c->image_temp : c->image;
+    GP_CUDA(c, cudaMemcpyAsync(dst, image, c->npix * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    GP_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->have_image = 1;
+    return GPAIR_OK;
+}
+
+static int d2h(gpair_ctx *c, void *dst, const void *src, size_t bytes)
+{
+    GP_CUDA(c, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->stream));
+    GP_CUDA(c, cudaStreamSynchronize(c->stream));
+    return GPAIR_OK;
+}
+
+extern "C" int gpair_get_image(gpair_ctx *c, int which, float *image)
+{
+    if (!c || !image || !c->image) return GPAIR_ERR_STATE;
+    return d2h(c, image, which == GPAIR_IMG_TEMP ? c->image_temp : c->image, c->npix * sizeof(float));
+}
+
+int gp_sync_scalars(gpair_ctx *c)
+{
+    GP_CUDA(c, cudaMemcpyAsync(c->sc_host, c->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, c->stream));
+    GP_CUDA(c, cudaStreamSynchronize(c->stream));
+    return GPAIR_OK;
+}
+
+// ----------------------------------------------------------- evaluations
+
+int gp_eval_criterion(gpair_ctx *c, int which, int trial)
+{
+    int rc;
+    if ((rc = gp_prep_image(c, trial ? GPAIR_IMG_TEMP : which, trial, 0.0, trial))) return rc;
+    if ((rc = gp_forward(c, trial ? GPAIR_IMG_TEMP : which))) return rc;
+    if ((rc = gp_vis_data(c))) return rc;
+    c->last_image_src = trial ? GPAIR_IMG_TEMP : which;
+    return GPAIR_OK;
+}
+
+int gp_eval_gradient(gpair_ctx *c, int which, float alpha)
+{
+    int rc;
+    if ((rc = gp_adjoint(c, which))) return rc;
+    return gp_grad_finalize(c, which, GRAD_FUSED, alpha);
+}
+
+extern "C" int gpair_criterion(gpair_ctx *c, int which, double *chi2, double *entropy)
+{
+    if (!c || !c->have_problem) return GPAIR_ERR_STATE;
+    GP_CUDA(c, cudaSetDevice(c->device));
+    int rc = gp_eval_criterion(c, which, 0);
+    if (rc) return rc;
+    if ((rc = gp_sync_scalars(c))) return rc;
+    if (chi2) *chi2 = c->sc_host->chi2;
+    if (entropy) *entropy = c->sc_host->entropy;
+    return (c->sc_host->nonfinite & 3u) ? GPAIR_ERR_NUMERIC : GPAIR_OK;
+}
+
+extern "C" int gpair_gradient(gpair_ctx *c, int which, float alpha)
+{
+    if (!c || !c->have_problem || c->last_image_src < 0) return GPAIR_ERR_STATE;
+    GP_CUDA(c, cudaSetDevice(c->device));
+    int rc = gp_eval_gradient(c, which, alpha);
+    if (rc) return rc;
+    GP_CUDA(c, cudaStreamSynchronize(c->stream));
+    return GPAIR_OK;
+}
+
+extern "C" int gpair_get_visibilities(gpair_ctx *c, gpair_float2 *visi)
+{
+    if (!c || !c->have_problem) return GPAIR_ERR_STATE;
+    return d2h(c, visi, c->visi, sizeof(float2) * c->nuv);
+}
+extern "C" int gpair_get_mock(gpair_ctx *c, float *mock)
+{
+    if (!c || !c->have_problem) return GPAIR_ERR_STATE;
+    return d2h(c, mock, c->mock, sizeof(float) * c->ndata);
+}
+extern "C" int gpair_get_data_gradient(gpair_ctx *c, float *g)
+{
+    if (!c || !c->image) return GPAIR_ERR_STATE;
+    return d2h(c, g, c->data_grad, sizeof(float) * c->npix);
+}
+extern "C" int gpair_get_entropy_gradient(gpair_ctx *c, float *g)
+{
+    if (!c || !c->image) return GPAIR_ERR_STATE;
+    return d2h(c, g, c->entropy_grad, sizeof(float) * c->npix);
+}
+extern "C" int gpair_get_full_gradient(gpair_ctx *c, int which, float *g)
+{
+    if (!c || !c->image) return GPAIR_ERR_STATE;
+    return d2h(c, g, which == GPAIR_IMG_TEMP ? c->grad_temp : c->full_grad_new, sizeof(float) * c->npix);
+}
+
+// ---------------------------------------------------------------- CG
+
+extern "C" void gpair_cg_default_params(gpair_cg_params *p)
+{
+    p->method = 2;
+    p->iterations = 10;
+    p->alpha = 1e-3f;
+    p->minvalue = 1e-8;
+    p->wolfe1 = 1e-4;
+    p->wolfe2 = 0.1;
+    p->step_max = 100.0;
+    p->max_zoom = 200;
+    p->max_bracket = 100;
+}
+
+static int read_action(gpair_ctx *c, int *action)
+{
+    GP_CUDA(c, cudaMemcpyAsync(&c->sc_host->cg.action, &c->sc->cg.action, sizeof(int), cudaMemcpyDeviceToHost,
+                               c->stream));
+    GP_CUDA(c, cudaStreamSynchronize(c->stream));
+    *action = c->sc_host->cg.action;
+    return GPAIR_OK;
+}
+
+extern "C" int gpair_cg_run(gpair_ctx *c, const gpair_cg_params *p, gpair_cg_result *res, double *tJ, double *tchi2,
+                            double *tS, double *tstep, double *tbeta)
+{
+    if (!c || !p || !c->have_problem) return GPAIR_ERR_STATE;
+    if (p->iterations < 0 || p->method < 0 || p->method > 3) return GPAIR_ERR_INVALID;
+    GP_CUDA(c, cudaSetDevice(c->device));
+    // parameters into the device state
+    CgState h;
+    memset(&h, 0, sizeof(h));
+    h.method = p->method;
+    h.max_zoom = p->max_zoom > 0 ? p->max_zoom : 200;
+    h.max_bracket = p->max_bracket > 0 ? p->max_bracket : 100;
+    h.alpha = p->alpha;
+    h.minvalue = p->minvalue;
+    h.c1 = p->wolfe1;
+    h.c2 = p->wolfe2;
+    h.step_max = p->step_max;
+    GP_CUDA(c, cudaMemcpyAsync(&c->sc->cg, &h, sizeof(CgState), cudaMemcpyHostToDevice, c->stream));
+    int rc = gp_cg_kernel(c, CTRL_INIT);
+    if (rc) return rc;
+    cudaEvent_t e0, e1;
+    GP_CUDA(c, cudaEventCreate(&e0));
+    GP_CUDA(c, cudaEventCreate(&e1));
+    long long launches0 = c->launches;
+    GP_CUDA(c, cudaEventRecord(e0, c->stream));
+    int status = GPAIR_OK, it;
+    for (it = 0; it < p->iterations && status == GPAIR_OK; it++) {
+        if ((rc = gp_eval_criterion(c, GPAIR_IMG_CURR, 0)) || (rc = gp_eval_gradient(c, GPAIR_IMG_CURR, p->alpha))
+            || (rc = gp_cg_kernel(c, CTRL_BEGIN)) || (rc = gp_descent_dir(c, 1, 0.0))
+            || (rc = gp_cg_kernel(c, CTRL_AFTER_DIR))) {
+            status = rc;
+            break;
+        }
+        int action = CG_EVAL_CRIT, trials = 0;
+        while (action != CG_DONE) {
+            if (++trials > 10000) { status = GPAIR_ERR_TIMEOUT; break; }
+            if (action == CG_EVAL_CRIT) {
+                if ((rc = gp_eval_criterion(c, GPAIR_IMG_TEMP, 1)) || (rc = gp_cg_kernel(c, CTRL_AFTER_CRIT))) {
+                    status = rc;
+                    break;
+                }
+            } else {
+                if ((rc = gp_eval_gradient(c, GPAIR_IMG_TEMP, p->alpha)) || (rc = gp_cg_kernel(c, CTRL_AFTER_GRAD))) {
+                    status = rc;
+                    break;
+                }
+            }
+            if ((rc = read_action(c, &action))) { status = rc; break; }
+        }
+        if (status) break;
+        if ((rc = gp_update_image(c, 1, 0.0, p->minvalue, 1))) { status = rc; break; }
+        if (tJ || tchi2 || tS || tstep || tbeta || it == p->iterations - 1) {
+            if ((rc = gp_sync_scalars(c))) { status = rc; break; }
+            const CgState &s = c->sc_host->cg;
+            if (tJ) tJ[it] = s.J;
+            if (tchi2) tchi2[it] = s.chi2;
+            if (tS) tS[it] = s.entropy;
+            if (tstep) tstep[it] = s.sel;
+            if (tbeta) tbeta[it] = s.beta;
+            if (c->sc_host->nonfinite) { status = GPAIR_ERR_NUMERIC; it++; break; }
+        }
+        rc = 0;
+    }
+    GP_CUDA(c, cudaEventRecord(e1, c->stream));
+    GP_CUDA(c, cudaEventSynchronize(e1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    int rc2 = gp_sync_scalars(c);
+    if (rc2 && !status) status = rc2;
+    const CgState &s = c->sc_host->cg;
+    c->last_ms = ms;
+    double per = 4.0 * (double)c->npix * c->nuv + 8.0 * c->N * (double)c->nuv;
+    c->last_flops = per * (s.criterion_evals + s.grad_evals);
+    c->last_launches = c->launches - launches0;
+    if (res) {
+        res->iterations_done = it;
+        res->criterion_evals = s.criterion_evals;
+        res->grad_evals = s.grad_evals;
+        res->J = s.J;
+        res->chi2 = s.chi2;
+        res->entropy = s.entropy;
+        res->last_step = s.sel;
+        res->last_beta = s.beta;
+        res->status = status;
+    }
+    return status;
+}
+
+extern "C" int gpair_last_run_stats(gpair_ctx *c, double *ms, double *flops, int *launches)
+{
+    if (!c) return GPAIR_ERR_INVALID;
+    if (ms) *ms = c->last_ms;
+    if (flops) *flops = c->last_flops;
+    if (launches) *launches = (int)c->last_launches;
+    return GPAIR_OK;
+}
+
+double gp_adjoint_scale(gpair_ctx *c);

@@ -1,0 +1,184 @@
+// gpair_internal.cuh -- device context, HBM layout and shared helpers of the
+// B200 reconstruction path. Not part of the public ABI.
+//
+// HBM layout of one problem (N = image width, K = nuv, T = nbis):
+//   images        image, image_temp, model, grads: float[N*N], x fastest
+//   data          data, data_err, mock: float[npow + 2T]
+//   triangles     tri: int4 {ab, bc, ca, sign bits} (bit j set = vertex j conjugated)
+//                 phasor: float2[T]
+//   uv            uvc: float2[K] (u, v in wavelengths)
+//   twiddles      fx, fy: float2[K][N]  (Fx[k][x] = e^{+2 pi i s u_k x}, Fy[k][y] = e^{-2 pi i s v_k y})
+//                 generated on the device with FP64 phase and argument reduction
+//   forward       vpart: float2[MT][K], per-row-tile partial visibilities (before 1/F)
+//                 visd: double2[K] (1/F included), visi: float2[K] (the reference's visi)
+//   adjoint       trib: float2[T][3] per-vertex adjoint weights, inc_off/inc_idx: CSR map
+//                 uv -> incident (triangle, vertex); cw: float2[K] summed weights c_k
+//                 gpart: float[S][N*N] split-K partial adjoint images
+//   scalars       DevScalars (FP64 sums, CG state) + reduction partials
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include "gpair_b200.h"
+
+#define GP_THREADS 256
+#define GP_MAX_PARTIALS 4096
+
+// Reduction slots (index into DevScalars::counter / partial areas)
+enum {
+    RED_PREP = 0,  // flux, entropy
+    RED_CHI2 = 1,  // chi2
+    RED_ADJ = 2,   // C = Re sum c_k V_k, max |c_k|
+    RED_GRAD = 3,  // gradient finalize dots
+    RED_DIR = 4,   // descent direction dot
+    RED_DOT = 5,   // generic scalar product
+    RED_NSLOTS = 8
+};
+
+// CG line-search actions decided on the device
+enum { CG_EVAL_CRIT = 1, CG_EVAL_GRAD = 2, CG_DONE = 3 };
+enum { CG_PH_BRACKET = 0, CG_PH_ZOOM = 1 };
+
+struct CgState {
+    // parameters
+    int method, max_zoom, max_bracket;
+    double alpha, minvalue, c1, c2, step_max;
+    // per iteration
+    int it;
+    double J, chi2, entropy, beta, wolfe1;
+    double prev_nn;  // g_new.g_new of the previous iteration (= g_old.g_old now)
+    // bracketing
+    int phase, ls_it, action, zoom_counter, zoom_trials, bracket_trials;
+    double s, s_old, J_init, J_old, Jt;
+    // zoom
+    double lo, hi, J_lo, z_s, z_s_old, z_J_old;
+    double sel;
+    // counters
+    int criterion_evals, grad_evals;
+};
+
+struct DevScalars {
+    double flux, invflux, entropy, chi2;
+    double adj_c;      // C = Re sum_k c_k V_k
+    double cmax;       // max |c_k| (scaling of split operands)
+    double grad_dots[2][4];  // [CURR/TEMP]: g.g, g.g_old, g.d, d.g_old
+    double dir_dot;    // d.g_new after the descent update
+    double dot;        // generic scalar product
+    float flux_f, invflux_f, chi2_f, entropy_f, dot_f;
+    unsigned int counter[RED_NSLOTS];
+    unsigned int nonfinite;  // set when a NaN/Inf reaches a reduction
+    CgState cg;
+};
+
+struct gpair_buf {
+    float *ptr;
+    size_t count;  // floats
+    int id;
+};
+
+struct gpair_ctx {
+    int device;
+    cudaStream_t stream;
+    char last_error[256];
+    int precision;
+
+    // problem
+    int N, npix, nuv, npow, nbis, ndata;
+    float pix;
+    int have_problem, have_image;
+    int mt;           // number of row tiles of the forward DFT
+    int splits;       // split-K factor of the adjoint
+
+    // buffers
+    float *image, *image_temp, *model;
+    float *data, *data_err, *mock;
+    int4 *tri;
+    float2 *phasor;
+    float2 *uvc;
+    float2 *fx, *fy;
+    float2 *vpart;
+    double2 *visd;
+    float2 *visi;
+    float2 *trib, *cw;
+    int *inc_off, *inc_idx;
+    float *gpart;
+    float *data_grad, *entropy_grad, *full_grad_new, *full_grad, *grad_temp, *descent_dir;
+    double *partials;  // RED_NSLOTS * GP_MAX_PARTIALS * 4 doubles
+    DevScalars *sc;
+    DevScalars *sc_host;  // pinned mirror for reads
+
+    // tensor-core operand buffers (GPAIR_PREC_SPLIT16 / TF32), see umma path
+    void *tc_state;
+
+    // handles for layer 1
+    gpair_buf h_image, h_image_temp, h_fgn, h_fg, h_dd, h_tg, h_eg, h_dg, h_model;
+
+    // timing / stats of the last gpair_cg_run
+    double last_ms, last_flops;
+    long long launches;       // running count of kernel launches
+    long long last_launches;  // launches of the last gpair_cg_run
+    int last_image_src;  // which image the last criterion used (0/1), -1 none
+
+    // reference-boundary staging (layer 1)
+    gpair_float2 *ref_dft_x, *ref_dft_y;  // host copies of the transposed tables
+    int ref_dft_size;
+    float *ref_data, *ref_data_err, *ref_model;
+    gpair_float2 *ref_phasor;
+    gpair_long4 *ref_uvpnt;
+    gpair_short4 *ref_sign;
+    int ref_data_size, ref_phasor_size, ref_bsref_size, ref_npow;
+    int bound_nuv, bound_npow, bound_nbis;
+};
+
+// ---------------------------------------------------------------- helpers
+#define GP_CUDA(ctx, call)                                                                          \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess) {                                                                    \
+            snprintf((ctx)->last_error, sizeof((ctx)->last_error), "%s: %s (%s:%d)", #call,        \
+                     cudaGetErrorString(e_), __FILE__, __LINE__);                                   \
+            return GPAIR_ERR_CUDA;                                                                  \
+        }                                                                                           \
+    } while (0)
+
+#define GP_LAUNCH_CHECK(ctx)                                                                        \
+    do {                                                                                            \
+        (ctx)->launches++;                                                                          \
+        cudaError_t e_ = cudaGetLastError();                                                        \
+        if (e_ != cudaSuccess) {                                                                    \
+            snprintf((ctx)->last_error, sizeof((ctx)->last_error), "launch: %s (%s:%d)",           \
+                     cudaGetErrorString(e_), __FILE__, __LINE__);                                   \
+            return GPAIR_ERR_CUDA;                                                                  \
+        }                                                                                           \
+    } while (0)
+
+static inline int gp_cdiv(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+// kernel launchers (kernels_core.cu)
+int gp_gen_twiddles(gpair_ctx *c);
+int gp_twiddles_from_ref_tables(gpair_ctx *c, const float2 *dft_x_t, const float2 *dft_y_t);
+int gp_build_incidence(gpair_ctx *c, const int64_t *uvpnt);
+int gp_prep_image(gpair_ctx *c, int which, int trial_mode, double step_host, int step_from_state);
+int gp_forward(gpair_ctx *c, int which);
+int gp_vis_data(gpair_ctx *c);
+int gp_adjoint(gpair_ctx *c, int which);
+int gp_grad_finalize(gpair_ctx *c, int which, int mode, float alpha);
+int gp_entropy_gradient(gpair_ctx *c, int which);
+int gp_criterion_gradient(gpair_ctx *c, float alpha, float *out);
+int gp_dot(gpair_ctx *c, const float *a, const float *b, int n);
+int gp_descent_dir(gpair_ctx *c, int beta_from_state, double beta_host);
+int gp_update_image(gpair_ctx *c, int step_from_state, double step_host, double minval, int backup);
+int gp_update_temp(gpair_ctx *c, double step, double minval, int clamp);
+int gp_cg_kernel(gpair_ctx *c, int which_ctrl);
+int gp_sync_scalars(gpair_ctx *c);
+
+enum { GRAD_FUSED = 0, GRAD_DATA_ONLY = 1 };
+enum { CTRL_BEGIN = 0, CTRL_AFTER_DIR = 1, CTRL_AFTER_CRIT = 2, CTRL_AFTER_GRAD = 3, CTRL_INIT = 4 };
+
+// tensor-core path (umma_dft.cu); return GPAIR_ERR_STATE when unavailable
+int gp_tc_prepare(gpair_ctx *c);
+int gp_tc_forward(gpair_ctx *c, int which);
+int gp_tc_adjoint(gpair_ctx *c, int which);
+void gp_tc_free(gpair_ctx *c);

@@ -1,0 +1,936 @@
+// kernels_core.cu -- device kernels of the reconstruction path (everything
+// except the tcgen05 contractions, which live in umma_dft.cu).
+//
+//   k_gen_twiddles   Fx, Fy tables from (u, v), FP64 phase in turns reduced to
+//                    [-1/2, 1/2] before sincospi (the reference builds them on the
+//                    host in double, gpair1/trunk/gpair.c:231-245)
+//   k_prep           image (or trial image max(I + s d, minval)) -> flux and
+//                    Gull-Skilling entropy, FP64 sums (gpu.c:860-884, cpu.c:385-400,
+//                    kernel_update_tempimage.cl)
+//   k_fwd_simt       forward DFT on CUDA cores: T = I Fx^T per row tile, reduced
+//                    against Fy in the epilogue (kernel_visi.cl / cpu.c:449-475)
+//   k_vis_data       V = sum of row-tile partials / F; V2, T3, chi2 (FP64 sum) and
+//                    the adjoint weights of every V2 point and triangle vertex
+//                    (kernel_pow_spec.cl, kernel_bispec.cl, kernel_chi2.cl,
+//                    cpu.c:758-802, cpu.c:371-383)
+//   k_adj_weights    c_k = a_k + sum of incident triangle-vertex weights (CSR
+//                    gather, fixed order), C = Re sum c_k V_k
+//   k_adj_simt       adjoint image G[y][x] = Re sum_k c_k Fy[k][y] Fx[k][x],
+//                    split over k (kernel_grad_pow.cl + kernel_grad_bis.cl, cpu.c:279-369)
+//   k_grad_finalize  data grad = sum of splits - C; entropy gradient (previous
+//                    value kept where I <= 0 or m <= 0); full gradient and the CG
+//                    dot products in FP64 (kernel_entropy_gs_grad.cl,
+//                    kernel_criterion_grad.cl)
+//   k_descent, k_update_image, k_update_temp, k_dot, k_cg_ctrl
+//                    CG vectors and the line-search state machine of
+//                    gpair1/trunk/gpair.c:682-915 and gpair1/trunk/gpu.c:1947-2065,
+//                    with FP64 scalars that stay on the device.
+#include <math.h>
+#include <string.h>
+
+#include "gpair_internal.cuh"
+
+#define RPMAS_D ((3.14159265358979323 / 180.0) / 3600000.0)
+
+// ------------------------------------------------------------ reductions
+
+template <int NV>
+__device__ __forceinline__ void block_sum(double (&v)[NV], double *smem)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int i = 0; i < NV; i++)
+        for (int off = 16; off > 0; off >>= 1) v[i] += __shfl_down_sync(0xffffffffu, v[i], off);
+    if (lane == 0)
+        for (int i = 0; i < NV; i++) smem[i * 32 + warp] = v[i];
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int i = 0; i < NV; i++) {
+            v[i] = lane < nw ? smem[i * 32 + lane] : 0.0;
+            for (int off = 16; off > 0; off >>= 1) v[i] += __shfl_down_sync(0xffffffffu, v[i], off);
+        }
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ double block_max(double v, double *smem)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int off = 16; off > 0; off >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, off));
+    if (lane == 0) smem[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        v = lane < nw ? smem[lane] : 0.0;
+        for (int off = 16; off > 0; off >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, off));
+    }
+    __syncthreads();
+    return v;
+}
+
+// True in exactly one block: the last to arrive. Partials written before the
+// call are visible to it. The counter is reset by that block.
+__device__ __forceinline__ bool last_block(unsigned int *counter)
+{
+    __shared__ bool am_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned int prev = atomicAdd(counter, 1u);
+        am_last = (prev == gridDim.x - 1);
+    }
+    __syncthreads();
+    return am_last;
+}
+
+// Sum NV partial vectors (layout [block][NV]) in a fixed order.
+template <int NV>
+__device__ void finish_sum(const double *partials, int nblocks, double (&out)[NV], double *smem)
+{
+    double v[NV];
+#pragma unroll
+    for (int i = 0; i < NV; i++) v[i] = 0.0;
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
+#pragma unroll
+        for (int i = 0; i < NV; i++) v[i] += __ldcg(&partials[(size_t)b * NV + i]);
+    block_sum<NV>(v, smem);
+#pragma unroll
+    for (int i = 0; i < NV; i++) out[i] = v[i];
+}
+
+static inline double *slot_partials(gpair_ctx *c, int slot) { return c->partials + (size_t)slot * GP_MAX_PARTIALS * 4; }
+
+// ------------------------------------------------------------- twiddles
+
+__global__ void k_gen_twiddles(const float2 *__restrict__ uvc, int nuv, int N, float pix, float2 *__restrict__ fx,
+                               float2 *__restrict__ fy)
+{
+    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)nuv * N) return;
+    int k = (int)(idx / N), i = (int)(idx % N);
+    float2 uv = uvc[k];
+    // phase / (2 pi) in turns, FP64, then reduced to [-1/2, 1/2]
+    double tu = RPMAS_D * (double)pix * (double)uv.x * (double)i;
+    double tv = RPMAS_D * (double)pix * (double)uv.y * (double)i;
+    tu -= rint(tu);
+    tv -= rint(tv);
+    double su, cu, sv, cv;
+    sincospi(2.0 * tu, &su, &cu);
+    sincospi(2.0 * tv, &sv, &cv);
+    fx[idx] = make_float2((float)cu, (float)su);   // e^{+2 pi i s u x}
+    fy[idx] = make_float2((float)cv, (float)(-sv)); // e^{-2 pi i s v y}
+}
+
+int gp_gen_twiddles(gpair_ctx *c)
+{
+    long long n = (long long)c->nuv * c->N;
+    if (n == 0) return GPAIR_OK;
+    k_gen_twiddles<<<gp_cdiv(n, 256), 256, 0, c->stream>>>(c->uvc, c->nuv, c->N, c->pix, c->fx, c->fy);
+    GP_LAUNCH_CHECK(c);
+    return GPAIR_OK;
+}
+
+// transposed reference tables [x][uv] -> [uv][x]
+__global__ void k_transpose_tables(const float2 *__restrict__ tx, const float2 *__restrict__ ty, int nuv, int N,
+                                   float2 *__restrict__ fx, float2 *__restrict__ fy)
+{
+    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)nuv * N) return;
+    int k = (int)(idx / N), i = (int)(idx % N);
+    fx[idx] = tx[(size_t)nuv * i + k];
+    fy[idx] = ty[(size_t)nuv * i + k];
+}
+
+int gp_twiddles_from_ref_tables(gpair_ctx *c, const float2 *dft_x_t, const float2 *dft_y_t)
+{
+    size_t n = (size_t)c->nuv * c->N;
+    if (n == 0) return GPAIR_OK;
+    float2 *tx = nullptr, *ty = nullptr;
+    GP_CUDA(c, cudaMallocAsync(&tx, n * sizeof(float2), c->stream));
+    GP_CUDA(c, cudaMallocAsync(&ty, n * sizeof(float2), c->stream));
+    GP_CUDA(c, cudaMemcpyAsync(tx, dft_x_t, n * sizeof(float2), cudaMemcpyHostToDevice, c->stream));
+    GP_CUDA(c, cudaMemcpyAsync(ty, dft_y_t, n * sizeof(float2), cudaMemcpyHostToDevice, c->stream));
+    k_transpose_tables<<<gp_cdiv((long long)n, 256), 256, 0, c->stream>>>(tx, ty, c->nuv, c->N, c->fx, c->fy);
+    GP_LAUNCH_CHECK(c);
+    GP_CUDA(c, cudaFreeAsync(tx, c->stream));
+    GP_CUDA(c, cudaFreeAsync(ty, c->stream));
+    return GPAIR_OK;
+}
+
+// ---------------------------------------------------------- image prep
+
+// src: image to evaluate. In trial mode the evaluated image is
+// max(src + s d, minval), written to dst. Sums flux and entropy in FP64.
+__global__ void __launch_bounds__(GP_THREADS) k_prep(const float *__restrict__ src, const float *__restrict__ d,
+                                                     float *__restrict__ dst, const float *__restrict__ model,
+                                                     int npix, int trial, double step, int step_from_state,
+                                                     double minval, double *__restrict__ partials,
+                                                     DevScalars *__restrict__ sc)
+{
+    __shared__ double smem[2 * 32];
+    double s = step_from_state ? sc->cg.s : step;
+    double acc[2] = {0.0, 0.0};
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
+        float I = src[p];
+        if (trial) {
+            double t = (double)I + s * (double)d[p];
+            if (t < minval) t = minval;
+            I = (float)t;
+            dst[p] = I;
+        }
+        double Id = I, m = model[p];
+        acc[0] += Id;
+        acc[1] += (Id > 0.0 && m > 0.0) ? (Id - m - Id * log(Id / m)) : -m;
+    }
+    block_sum<2>(acc, smem);
+    if (threadIdx.x == 0) {
+        partials[2 * blockIdx.x] = acc[0];
+        partials[2 * blockIdx.x + 1] = acc[1];
+    }
+    if (last_block(&sc->counter[RED_PREP])) {
+        double out[2];
+        finish_sum<2>(partials, gridDim.x, out, smem);
+        if (threadIdx.x == 0) {
+            sc->flux = out[0];
+            sc->invflux = 1.0 / out[0];
+            sc->entropy = out[1];
+            sc->flux_f = (float)out[0];
+            sc->invflux_f = (float)(1.0 / out[0]);
+            sc->entropy_f = (float)out[1];
+            if (!isfinite(out[0]) || !isfinite(out[1])) sc->nonfinite |= 1u;
+            sc->counter[RED_PREP] = 0;
+        }
+    }
+}
+
+static int red_grid(long long n) { int g = gp_cdiv(n, GP_THREADS * 4); return g < 1 ? 1 : (g > 1184 ? 1184 : g); }
+
+int gp_prep_image(gpair_ctx *c, int which, int trial_mode, double step_host, int step_from_state)
+{
+    const float *src = (which == GPAIR_IMG_TEMP && !trial_mode) ? c->image_temp : c->image;
+    int g = red_grid(c->npix);
+    k_prep<<<g, GP_THREADS, 0, c->stream>>>(src, c->descent_dir, c->image_temp, c->model, c->npix, trial_mode,
+                                            step_host, step_from_state, (double)1e-8, slot_partials(c, RED_PREP),
+                                            c->sc);
+    GP_LAUNCH_CHECK(c);
+    return GPAIR_OK;
+}
+
+// ----------------------------------------------------- forward, CUDA cores
+
+#define FB_M 64
+#define FB_K 32
+#define FB_X 32
+
+__global__ void __launch_bounds__(256) k_fwd_simt(const float *__restrict__ img, const float2 *__restrict__ fx,
+                                                  const float2 *__restrict__ fy, int N, int nuv,
+                                                  float2 *__restrict__ vpart)
+{
+    __shared__ float As[FB_X][FB_M + 1];
+    __shared__ float2 Bs[FB_X][FB_K + 1];
+    __shared__ float2 red[16][FB_K + 1];
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    const int k0 = blockIdx.x * FB_K, y0 = blockIdx.y * FB_M;
+    float2 acc[4][2];
+#pragma unroll
+    for (int r = 0; r < 4; r++) acc[r][0] = acc[r][1] = make_float2(0.f, 0.f);
+    for (int x0 = 0; x0 < N; x0 += FB_X) {
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            int r = (tid >> 5) + 8 * i, cx = tid & 31, y = y0 + r, x = x0 + cx;
+            As[cx][r] = (y < N && x < N) ? img[(size_t)y * N + x] : 0.f;
+        }
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            int kk = (tid >> 5) + 8 * i, cx = tid & 31, k = k0 + kk, x = x0 + cx;
+            Bs[cx][kk] = (k < nuv && x < N) ? fx[(size_t)k * N + x] : make_float2(0.f, 0.f);
+        }
+        __syncthreads();
+#pragma unroll 8
+        for (int cx = 0; cx < FB_X; cx++) {
+            float2 b0 = Bs[cx][tx * 2], b1 = Bs[cx][tx * 2 + 1];
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                float a = As[cx][ty * 4 + r];
+                acc[r][0].x = fmaf(a, b0.x, acc[r][0].x);
+                acc[r][0].y = fmaf(a, b0.y, acc[r][0].y);
+                acc[r][1].x = fmaf(a, b1.x, acc[r][1].x);
+                acc[r][1].y = fmaf(a, b1.y, acc[r][1].y);
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+        int k = k0 + tx * 2 + j;
+        float2 part = make_float2(0.f, 0.f);
+        if (k < nuv) {
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                int y = y0 + ty * 4 + r;
+                if (y < N) {
+                    float2 f = fy[(size_t)k * N + y];
+                    part.x += acc[r][j].x * f.x - acc[r][j].y * f.y;
+                    part.y += acc[r][j].x * f.y + acc[r][j].y * f.x;
+                }
+            }
+        }
+        red[ty][tx * 2 + j] = part;
+    }
+    __syncthreads();
+    if (tid < FB_K) {
+        float2 s = make_float2(0.f, 0.f);
+        for (int r = 0; r < 16; r++) { s.x += red[r][tid].x; s.y += red[r][tid].y; }
+        int k = k0 + tid;
+        if (k < nuv) vpart[(size_t)blockIdx.y * nuv + k] = s;
+    }
+}
+
+int gp_forward(gpair_ctx *c, int which)
+{
+    if (c->precision != GPAIR_PREC_FP32) {
+        int rc = gp_tc_forward(c, which);
+        if (rc != GPAIR_ERR_STATE) return rc;
+        return GPAIR_ERR_STATE; // tensor path requested but unavailable: fail loudly
+    }
+    const float *img = (which == GPAIR_IMG_TEMP) ? c->image_temp : c->image;
+    c->mt = gp_cdiv(c->N, FB_M);
+    dim3 grid(gp_cdiv(c->nuv, FB_K), c->mt);
+    k_fwd_simt<<<grid, 256, 0, c->stream>>>(img, c->fx, c->fy, c->N, c->nuv, c->vpart);
+    GP_LAUNCH_CHECK(c);
+    return GPAIR_OK;
+}
+
+// ------------------------------------------------- V2, T3, chi2, weights
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b)
+{
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+
+__device__ __forceinline__ double2 sum_vpart(const float2 *__restrict__ vpart, int mt, int nuv, int k, double invF)
+{
+    double re = 0.0, im = 0.0;
+    for (int m = 0; m < mt; m++) {
+        float2 p = vpart[(size_t)m * nuv + k];
+        re += p.x;
+        im += p.y;
+    }
+    return make_double2(re * invF, im * invF);
+}
+
+__global__ void __launch_bounds__(GP_THREADS) k_vis_data(const float2 *__restrict__ vpart, int mt, int nuv,
+                                                         int npow, int nbis, const float *__restrict__ data,
+                                                         const float *__restrict__ data_err,
+                                                         const int4 *__restrict__ tri,
+                                                         const float2 *__restrict__ phasor, int nblk_uv,
+                                                         double2 *__restrict__ visd, float2 *__restrict__ visi,
+                                                         float *__restrict__ mock, float2 *__restrict__ cw,
+                                                         float2 *__restrict__ trib, double *__restrict__ partials,
+                                                         DevScalars *__restrict__ sc)
+{
+    __shared__ double smem[32];
+    const double invF = sc->invflux;
+    double chi[1] = {0.0};
+    if ((int)blockIdx.x < nblk_uv) {
+        for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nuv; k += nblk_uv * blockDim.x) {
+            double2 V = sum_vpart(vpart, mt, nuv, k, invF);
+            visd[k] = V;
+            visi[k] = make_float2((float)V.x, (float)V.y);
+            float2 a = make_float2(0.f, 0.f);
+            if (k < npow) {
+                double m2 = V.x * V.x + V.y * V.y;
+                mock[k] = (float)m2;
+                double w = data_err[k], res = m2 - (double)data[k], r = res * w;
+                chi[0] += r * r;
+                double f = 4.0 * w * w * res * invF; // a_k = f conj(V_k)
+                a = make_float2((float)(f * V.x), (float)(-f * V.y));
+            }
+            cw[k] = a;
+        }
+    } else {
+        const int nblk_tri = gridDim.x - nblk_uv;
+        for (int t = (blockIdx.x - nblk_uv) * blockDim.x + threadIdx.x; t < nbis; t += nblk_tri * blockDim.x) {
+            int4 q = tri[t];
+            double2 va = sum_vpart(vpart, mt, nuv, q.x, invF);
+            double2 vb = sum_vpart(vpart, mt, nuv, q.y, invF);
+            double2 vc = sum_vpart(vpart, mt, nuv, q.z, invF);
+            if (q.w & 1) va = cconj(va);
+            if (q.w & 2) vb = cconj(vb);
+            if (q.w & 4) vc = cconj(vc);
+            float2 phf = phasor[t];
+            double2 ph = make_double2(phf.x, phf.y);
+            double2 t3 = cmul(cmul(cmul(va, vb), vc), ph);
+            int r0 = npow + 2 * t;
+            mock[r0] = (float)t3.x;
+            mock[r0 + 1] = (float)t3.y;
+            double wre = data_err[r0], wim = data_err[r0 + 1];
+            double rre = t3.x - (double)data[r0], rim = t3.y - (double)data[r0 + 1];
+            chi[0] += (rre * wre) * (rre * wre) + (rim * wim) * (rim * wim);
+            // adjoint: Re(conj(g) * t3der) with g = 2 w_re^2 (T3re - d_re) + i 2 w_im^2 T3im
+            // (the reference uses the mock imaginary part alone, gpair1/trunk/cpu.c:364-365)
+            double2 g = make_double2(2.0 * wre * wre * rre, 2.0 * wim * wim * t3.y);
+            double2 base = cmul(cconj(g), ph);
+            base.x *= invF;
+            base.y *= invF;
+            double2 bab = cmul(base, cmul(vb, vc));
+            double2 bbc = cmul(base, cmul(va, vc));
+            double2 bca = cmul(base, cmul(va, vb));
+            if (q.w & 1) bab = cconj(bab);
+            if (q.w & 2) bbc = cconj(bbc);
+            if (q.w & 4) bca = cconj(bca);
+            trib[3 * (size_t)t + 0] = make_float2((float)bab.x, (float)bab.y);
+            trib[3 * (size_t)t + 1] = make_float2((float)bbc.x, (float)bbc.y);
+            trib[3 * (size_t)t + 2] = make_float2((float)bca.x, (float)bca.y);
+        }
+    }
+    block_sum<1>(chi, smem);
+    if (threadIdx.x == 0) partials[blockIdx.x] = chi[0];
+    if (last_block(&sc->counter[RED_CHI2])) {
+        double out[1];
+        finish_sum<1>(partials, gridDim.x, out, smem);
+        if (threadIdx.x == 0) {
+            sc->chi2 = out[0];
+            sc->chi2_f = (float)out[0];
+            if (!isfinite(out[0])) sc->nonfinite |= 2u;
+            sc->counter[RED_CHI2] = 0;
+        }
+    }
+}
+
+int gp_vis_data(gpair_ctx *c)
+{
+    int nbu = gp_cdiv(c->nuv, GP_THREADS);
+    if (nbu > 512) nbu = 512;
+    if (nbu < 1) nbu = 1;
+    int nbt = gp_cdiv(c->nbis, GP_THREADS);
+    if (nbt > 1536) nbt = 1536;
+    k_vis_data<<<nbu + nbt, GP_THREADS, 0, c->stream>>>(c->vpart, c->mt, c->nuv, c->npow, c->nbis, c->data,
+                                                        c->data_err, c->tri, c->phasor, nbu, c->visd, c->visi,
+                                                        c->mock, c->cw, c->trib, slot_partials(c, RED_CHI2), c->sc);
+    GP_LAUNCH_CHECK(c);
+    return GPAIR_OK;
+}
+
+// ----------------------------------------------------- adjoint weights
+
+__global__ void __launch_bounds__(GP_THREADS) k_adj_weights(int nuv, const int *__restrict__ inc_off,
+                                                            const int *__restrict__ inc_idx,
+                                                            const float2 *__restrict__ trib,
+                                                            const double2 *__restrict__ visd, float2 *__restrict__ cw,
+                                                            double *__restrict__ partials, DevScalars *__restrict__ sc)
+{
+    __shared__ double smem[32];
+    double acc[1] = {0.0};
+    double cmax = 0.0;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nuv; k += gridDim.x * blockDim.x) {
+        float2 a = cw[k];
+        double re = a.x, im = a.y;
+        for (int p = inc_off[k]; p < inc_off[k + 1]; p++) {
+            float2 b = trib[inc_idx[p]];
+            re += b.x;
+            im += b.y;
+        }
+        float2 cf = make_float2((float)re, (float)im);
+        cw[k] = cf;
+        double2 V = visd[k];
+        acc[0] += (double)cf.x * V.x - (double)cf.y * V.y;
+        cmax = fmax(cmax, fmax(fabs((double)cf.x), fabs((double)cf.y)));
+    }
+    block_sum<1>(acc, smem);
+    cmax = block_max(cmax, smem);
+    if (threadIdx.x == 0) {
+        partials[2 * blockIdx.x] = acc[0];
+        partials[2 * blockIdx.x + 1] = cmax;
+    }
+    if (last_block(&sc->counter[RED_ADJ])) {
+        double s = 0.0, m = 0.0;
+        for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
+            s += __ldcg(&partials[2 * b]);
+            m = fmax(m, __ldcg(&partials[2 * b + 1]));
+        }
+        double sv[1] = {s};
+        block_sum<1>(sv, smem);
+        m = block_max(m, smem);
+        if (threadIdx.x == 0) {
+            sc->adj_c = sv[0];
+            sc->cmax = m;
+            sc->counter[RED_ADJ] = 0;
+        }
+    }
+}
+
+// ----------------------------------------------------- adjoint, CUDA cores
+
+#define AB_M 64
+#define AB_N 64
+#define AB_K 16  // complex uv per k-step
+
+__global__ void __launch_bounds__(256) k_adj_simt(const float2 *__restrict__ fx, const float2 *__restrict__ fy,
+                                                  const float2 *__restrict__ cw, int N, int nuv, int kchunk,
+                                                  float *__restrict__ gpart)
+{
+    __shared__ float As[2 * AB_K][AB_M + 4];
+    __shared__ float Bs[2 * AB_K][AB_N + 4];
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    const int x0 = blockIdx.x * AB_N, y0 = blockIdx.y * AB_M;
+    const int kb = blockIdx.z * kchunk, ke = min(nuv, kb + kchunk);
+    float acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[i][j] = 0.f;
+    for (int k0 = kb; k0 < ke; k0 += AB_K) {
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            int kk = (tid >> 6) + 4 * i, cc = tid & 63, k = k0 + kk;
+            float2 wa = make_float2(0.f, 0.f), fb = make_float2(0.f, 0.f);
+            if (k < ke) {
+                int y = y0 + cc, x = x0 + cc;
+                float2 cwk = cw[k];
+                if (y < N) {
+                    float2 f = fy[(size_t)k * N + y];
+                    wa = make_float2(cwk.x * f.x - cwk.y * f.y, cwk.x * f.y + cwk.y * f.x);
+                }
+                if (x < N) fb = fx[(size_t)k * N + x];
+            }
+            As[2 * kk][cc] = wa.x;
+            As[2 * kk + 1][cc] = -wa.y;
+            Bs[2 * kk][cc] = fb.x;
+            Bs[2 * kk + 1][cc] = fb.y;
+        }
+        __syncthreads();
+#pragma unroll 8
+        for (int kp = 0; kp < 2 * AB_K; kp++) {
+            float4 a = *reinterpret_cast<const float4 *>(&As[kp][ty * 4]);
+            float4 b = *reinterpret_cast<const float4 *>(&Bs[kp][tx * 4]);
+            float av[4] = {a.x, a.y, a.z, a.w}, bv[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+        }
+        __syncthreads();
+    }
+    float *out = gpart + (size_t)blockIdx.z * N * N;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        int y = y0 + ty * 4 + i;
+        if (y >= N) continue;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            int x = x0 + tx * 4 + j;
+            if (x < N) out[(size_t)y * N + x] = acc[i][j];
+        }
+    }
+}
+
+static int adj_splits(int N, int nuv)
+{
+    int tiles = gp_cdiv(N, AB_M) * gp_cdiv(N, AB_N);
+    int s = gp_cdiv(148 * 3, tiles);
+    int maxs = gp_cdiv(nuv, 64);
+    if (s > maxs) s = maxs;
+    if (s > 64) s = 64;
+    return s < 1 ? 1 : s;
+}
+
+int gp_adjoint(gpair_ctx *c, int which)
+{
+    (void)which;
+    int nb = gp_cdiv(c->nuv, GP_THREADS);
+    if (nb > 592) nb = 592;
+    if (nb < 1) nb = 1;
+    k_adj_weights<<<nb, GP_THREADS, 0, c->stream>>>(c->nuv, c->inc_off, c->inc_idx, c->trib, c->visd, c->cw,
+                                                    slot_partials(c, RED_ADJ), c->sc);
+    GP_LAUNCH_CHECK(c);
+    if (c->precision != GPAIR_PREC_FP32) return gp_tc_adjoint(c, which);
+    int S = c->splits;
+    int kchunk = gp_cdiv(c->nuv, S);
+    kchunk = gp_cdiv(kchunk, AB_K) * AB_K;
+    S = gp_cdiv(c->nuv, kchunk);
+    if (S < 1) S = 1;
+    c->splits = S;
+    dim3 grid(gp_cdiv(c->N, AB_N), gp_cdiv(c->N, AB_M), S);
+    if (c->nuv == 0) {
+        GP_CUDA(c, cudaMemsetAsync(c->gpart, 0, sizeof(float) * c->npix, c->stream));
+        c->splits = 1;
+        return GPAIR_OK;
+    }
+    k_adj_simt<<<grid, 256, 0, c->stream>>>(c->fx, c->fy, c->cw, c->N, c->nuv, kchunk, c->gpart);
+    GP_LAUNCH_CHECK(c);
+    return GPAIR_OK;
+}
+
+int gp_default_splits(int N, int nuv) { return adj_splits(N, nuv); }
+
+// ------------------------------------------------------ gradient finalize
+
+__global__ void __launch_bounds__(GP_THREADS) k_grad_finalize(const float *__restrict__ gpart, int splits,
+                                                              int npix, double gscale, int mode,
+                                                              const float *__restrict__ img,
+                                                              const float *__restrict__ model, float alpha,
+                                                              float *__restrict__ data_grad,
+                                                              float *__restrict__ entropy_grad,
+                                                              float *__restrict__ out,
+                                                              const float *__restrict__ g_old,
+                                                              const float *__restrict__ d, int dot_slot,
+                                                              double *__restrict__ partials,
+                                                              DevScalars *__restrict__ sc)
+{
+    __shared__ double smem[4 * 32];
+    const double C = sc->adj_c;
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
+        double g = 0.0;
+        for (int s = 0; s < splits; s++) g += gpart[(size_t)s * npix + p];
+        float gd = (float)(g * gscale - C);
+        data_grad[p] = gd;
+        if (mode == GRAD_FUSED) {
+            float I = img[p], m = model[p];
+            float eg = entropy_grad[p];
+            if (I > 0.f && m > 0.f) eg = (float)(-log((double)I / (double)m));
+            entropy_grad[p] = eg;
+            float fg = gd - alpha * eg;
+            out[p] = fg;
+            double fgd = fg, go = g_old[p], dd = d[p];
+            acc[0] += fgd * fgd;
+            acc[1] += fgd * go;
+            acc[2] += fgd * dd;
+            acc[3] += dd * go;
+        }
+    }
+    if (mode != GRAD_FUSED) return;
+    block_sum<4>(acc, smem);
+    if (threadIdx.x == 0)
+        for (int i = 0; i < 4; i++) partials[4 * blockIdx.x + i] = acc[i];
+    if (last_block(&sc->counter[RED_GRAD])) {
+        double o[4];
+        finish_sum<4>(partials, gridDim.x, o, smem);
+        if (threadIdx.x == 0) {
+            for (int i = 0; i < 4; i++) sc->grad_dots[dot_slot][i] = o[i];
+            if (!isfinite(o[0])) sc->nonfinite |= 4u;
+            sc->counter[RED_GRAD] = 0;
+        }
+    }
+}
+
+double gp_adjoint_scale(gpair_ctx *c);
+
+int gp_grad_finalize(gpair_ctx *c, int which, int mode, float alpha)
+{
+    const float *img = (which == GPAIR_IMG_TEMP) ? c->image_temp : c->image;
+    float *out = (which == GPAIR_IMG_TEMP) ? c->grad_temp : c->full_grad_new;
+    int g = red_grid(c->npix);
+    k_grad_finalize<<<g, GP_THREADS, 0, c->stream>>>(c->gpart, c->splits, c->npix, gp_adjoint_scale(c), mode, img,
+                                                     c->model, alpha, c->data_grad, c->entropy_grad, out,
+                                                     c->full_grad, c->descent_dir, which == GPAIR_IMG_TEMP ? 1 : 0,
+                                                     slot_partials(c, RED_GRAD), c->sc);
+    GP_LAUNCH_CHECK(c);
+    return GPAIR_OK;
+}
+
+// entropy gradient alone (gpu_compute_entropy_gradient, kernel_entropy_gs_grad.cl)
+__global__ void k_entropy_grad(const float *__restrict__ img, const float *__restrict__ model, int npix,
+                               float *__restrict__ eg)
+{
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npix) return;
+    float I = img[p], m = model[p];
+    if (I > 0.f && m > 0.f) eg[p] = (float)(-log((double)I / (double)m));
+}
+
+int gp_entropy_gradient(gpair_ctx *c, int which)
+{
+    const float *img = (which == GPAIR_IMG_TEMP) ? c->image_temp : c->image;
+    k_entropy_grad<<<gp_cdiv(c->npix, 256), 256, 0, c->stream>>>(img, c->model, c->npix, c->entropy_grad);
+    GP_LAUNCH_CHECK(c);
+    return GPAIR_OK;
+}
+
+// criterion gradient alone (kernel_criterion_grad.cl)
+__global__ void k_crit_grad(const float *__restrict__ dg, const float *__restrict__ eg, float alpha, int npix,
+                            float *__restrict__ out)
+{
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < npix) out[p] = dg[p] - alpha * eg[p];
+}
+
+int gp_criterion_gradient(gpair_ctx *c, float alpha, float *out)
+{
+    k_crit_grad<<<gp_cdiv(c->npix, 256), 256, 0, c->stream>>>(c->data_grad, c->entropy_grad, alpha, c->npix, out);
+    GP_LAUNCH_CHECK(c);
+    return GPAIR_OK;
+}
+
+// -------------------------------------------------------------- CG vectors
+
+__global__ void __launch_bounds__(GP_THREADS) k_dot(const float *__restrict__ a, const float *__restrict__ b, int n,
+                                                    double *__restrict__ partials, DevScalars *__restrict__ sc)
+{
+    __shared__ double smem[32];
+    double acc[1] = {0.0};
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x)
+        acc[0] += (double)a[p] * (double)b[p];
+    block_sum<1>(acc, smem);
+    if (threadIdx.x == 0) partials[blockIdx.x] = acc[0];
+    if (last_block(&sc->counter[RED_DOT])) {
+        double o[1];
+        finish_sum<1>(partials, gridDim.x, o, smem);
+        if (threadIdx.x == 0) {
+            sc->dot = o[0];
+            sc->dot_f = (float)o[0];
+            sc->counter[RED_DOT] = 0;
+        }
+    }
+}
+
+int gp_dot(gpair_ctx *c, const float *a, const float *b, int n)
+{
+    k_dot<<<red_grid(n), GP_THREADS, 0, c->stream>>>(a, b, n, slot_partials(c, RED_DOT), c->sc);
+    GP_LAUNCH_CHECK(c);
+    return GPAIR_OK;
+}
+
+// d = beta d - g_new, and d.g_new (FP64)
+__global__ void __launch_bounds__(GP_THREADS) k_descent(float *__restrict__ d, const float *__restrict__ g, int n,
+                                                        int beta_from_state, double beta_host,
+                                                        double *__restrict__ partials, DevScalars *__restrict__ sc)
+{
+    __shared__ double smem[32];
+    const double beta = beta_from_state ? sc->cg.beta : beta_host;
+    double acc[1] = {0.0};
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        float dn = (float)(beta * (double)d[p] - (double)g[p]);
+        d[p] = dn;
+        acc[0] += (double)dn * (double)g[p];
+    }
+    block_sum<1>(acc, smem);
+    if (threadIdx.x == 0) partials[blockIdx.x] = acc[0];
+    if (last_block(&sc->counter[RED_DIR])) {
+        double o[1];
+        finish_sum<1>(partials, gridDim.x, o, smem);
+        if (threadIdx.x == 0) {
+            sc->dir_dot = o[0];
+            sc->counter[RED_DIR] = 0;
+        }
+    }
+}
+
+int gp_descent_dir(gpair_ctx *c, int beta_from_state, double beta_host)
+{
+    k_descent<<<red_grid(c->npix), GP_THREADS, 0, c->stream>>>(c->descent_dir, c->full_grad_new, c->npix,
+                                                               beta_from_state, beta_host,
+                                                               slot_partials(c, RED_DIR), c->sc);
+    GP_LAUNCH_CHECK(c);
+    return GPAIR_OK;
+}
+
+// image = max(image + s d, minval); optionally full_grad = full_grad_new
+__global__ void k_update_image(float *__restrict__ img, const float *__restrict__ d, int n, int step_from_state,
+                               double step_host, double minval, const float *__restrict__ gnew,
+                               float *__restrict__ gold, const DevScalars *__restrict__ sc)
+{
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    double s = step_from_state ? sc->cg.sel : step_host;
+    double t = (double)img[p] + s * (double)d[p];
+    if (t < minval) t = minval;
+    img[p] = (float)t;
+    if (gold) gold[p] = gnew[p];
+}
+
+int gp_update_image(gpair_ctx *c, int step_from_state, double step_host, double minval, int backup)
+{
+    k_update_image<<<gp_cdiv(c->npix, 256), 256, 0, c->stream>>>(c->image, c->descent_dir, c->npix, step_from_state,
+                                                                 step_host, minval, c->full_grad_new,
+                                                                 backup ? c->full_grad : nullptr, c->sc);
+    GP_LAUNCH_CHECK(c);
+    return GPAIR_OK;
+}
+
+// temp = image + s d (clamped at minval when clamp != 0), float arithmetic of
+// kernel_update_tempimage.cl / kernel_criterion_step.cl
+__global__ void k_update_temp(const float *__restrict__ img, const float *__restrict__ d, int n, float s,
+                              float minval, int clamp, float *__restrict__ temp)
+{
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    float t = img[p] + s * d[p];
+    if (clamp && t < minval) t = minval;
+    temp[p] = t;
+}
+
+int gp_update_temp(gpair_ctx *c, double step, double minval, int clamp)
+{
+    k_update_temp<<<gp_cdiv(c->npix, 256), 256, 0, c->stream>>>(c->image, c->descent_dir, c->npix, (float)step,
+                                                                (float)minval, clamp, c->image_temp);
+    GP_LAUNCH_CHECK(c);
+    return GPAIR_OK;
+}
+
+// ------------------------------------------------------- CG controller
+
+__device__ void cg_zoom_next(CgState &s)
+{
+    // top of the zoom loop, gpair1/trunk/gpu.c:1977-1990
+    if (s.zoom_counter > 0 && (s.z_J_old - s.J_init - s.wolfe1 * s.z_s_old) != 0.0)
+        s.z_s = fabs(s.wolfe1 * s.z_s_old * s.z_s_old / (2.0 * (s.z_J_old - s.J_init - s.wolfe1 * s.z_s_old)));
+    if (s.zoom_counter == 0 || s.z_s < s.lo || s.z_s > s.hi) s.z_s = (s.hi - s.lo) / 2.0 + s.lo;
+    if (fabs(s.hi - s.lo) < 1e-14 || s.zoom_trials >= s.max_zoom) {
+        s.sel = s.lo;
+        s.action = CG_DONE;
+        return;
+    }
+    s.s = s.z_s;
+    s.zoom_trials++;
+    s.action = CG_EVAL_CRIT;
+}
+
+__device__ void cg_zoom_enter(CgState &s, double lo, double hi, double J_lo)
+{
+    s.phase = CG_PH_ZOOM;
+    s.lo = lo;
+    s.hi = hi;
+    s.J_lo = J_lo;
+    s.z_s = 0.0;
+    s.z_s_old = 0.0;
+    s.z_J_old = 0.0;
+    s.zoom_counter = 0;
+    s.zoom_trials = 0;
+    cg_zoom_next(s);
+}
+
+__global__ void k_cg_ctrl(DevScalars *__restrict__ sc, int what)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    CgState &s = sc->cg;
+    switch (what) {
+    case CTRL_INIT:
+        s.it = 0;
+        s.criterion_evals = s.grad_evals = 0;
+        s.beta = 0.0;
+        s.sel = 0.0;
+        s.prev_nn = 0.0;
+        s.action = CG_EVAL_CRIT;
+        sc->nonfinite = 0;
+        break;
+    case CTRL_BEGIN: {
+        // criterion and gradient of the current image are done (gpair.c:688-724);
+        // beta from the FP64 dot products of the gradient finalize (gpair.c:727-758)
+        s.J = sc->chi2 - s.alpha * sc->entropy;
+        s.chi2 = sc->chi2;
+        s.entropy = sc->entropy;
+        s.criterion_evals++;
+        s.grad_evals++;
+        const double nn = sc->grad_dots[0][0], no = sc->grad_dots[0][1];
+        const double dn = sc->grad_dots[0][2], dold = sc->grad_dots[0][3];
+        const double oo = s.prev_nn;
+        double beta = 0.0;
+        if (!(s.it == 0 || s.method == 0)) {
+            if (s.method == 1) beta = nn / oo;
+            if (s.method == 2) {
+                beta = (nn - no) / oo;
+                if (beta < 0.0) beta = 0.0;
+            }
+            if (s.method == 3) {
+                beta = (nn - no) / (dn - dold);
+                if (beta < 0.0) beta = 0.0;
+            }
+            if (fabs(no / nn) > 0.5) beta = 0.0;
+        }
+        s.beta = beta;
+        s.prev_nn = nn;
+        s.it++;
+        break;
+    }
+    case CTRL_AFTER_DIR:
+        // line search initialisation (gpair.c:792-806)
+        s.wolfe1 = sc->dir_dot;
+        s.sel = 0.0;
+        s.s = 1.0;
+        s.s_old = 0.0;
+        s.J_init = s.J;
+        s.J_old = s.J;
+        s.ls_it = 1;
+        s.phase = CG_PH_BRACKET;
+        s.bracket_trials = 0;
+        s.action = CG_EVAL_CRIT;
+        break;
+    case CTRL_AFTER_CRIT: {
+        double Jt = sc->chi2 - s.alpha * sc->entropy;
+        s.Jt = Jt;
+        s.criterion_evals++;
+        if (s.phase == CG_PH_BRACKET) {
+            // gpair.c:832-849
+            if ((Jt > (s.J_init + s.c1 * s.s * s.wolfe1)) || ((Jt >= s.J_old) && (s.ls_it > 1)))
+                cg_zoom_enter(s, s.s_old, s.s, s.J_old);
+            else
+                s.action = CG_EVAL_GRAD;
+        } else {
+            // gpu.c:2019-2023
+            if ((Jt > (s.J_init + s.c1 * s.z_s * s.wolfe1)) || (Jt >= s.J_lo)) {
+                s.hi = s.z_s;
+                s.z_s_old = s.z_s;
+                s.z_J_old = Jt;
+                s.zoom_counter++;
+                cg_zoom_next(s);
+            } else {
+                s.action = CG_EVAL_GRAD;
+            }
+        }
+        if (!isfinite(Jt)) {
+            sc->nonfinite |= 8u;
+            s.sel = 0.0;
+            s.action = CG_DONE;
+        }
+        break;
+    }
+    case CTRL_AFTER_GRAD: {
+        const double w2 = sc->grad_dots[1][2];  // d . g_trial
+        s.grad_evals++;
+        if (s.phase == CG_PH_BRACKET) {
+            // gpair.c:861-903
+            if (fabs(w2) <= -s.c2 * s.wolfe1) {
+                s.sel = s.s;
+                s.action = CG_DONE;
+            } else if (w2 >= 0.0) {
+                cg_zoom_enter(s, s.s, s.s_old, s.Jt);
+            } else {
+                s.s_old = s.s;
+                s.J_old = s.Jt;
+                s.s = 10.0 * s.s;
+                if (s.s > s.step_max) s.s = s.step_max;
+                s.ls_it++;
+                s.bracket_trials++;
+                s.action = (s.bracket_trials >= s.max_bracket) ? CG_DONE : CG_EVAL_CRIT;
+                if (s.action == CG_DONE) s.sel = s.s_old;
+            }
+        } else {
+            // gpu.c:2036-2056
+            if ((w2 >= s.c2 * s.wolfe1) || (s.zoom_counter > 10)) {
+                s.sel = s.z_s;
+                s.action = CG_DONE;
+            } else {
+                if (w2 * (s.hi - s.lo) >= 0.0) s.hi = s.lo;
+                s.lo = s.z_s;
+                s.z_s_old = s.z_s;
+                s.z_J_old = s.Jt;
+                s.zoom_counter++;
+                cg_zoom_next(s);
+            }
+        }
+        break;
+    }
+    default:
+        break;
+    }
+}
+
+int gp_cg_kernel(gpair_ctx *c, int which_ctrl)
+{
+    k_cg_ctrl<<<1, 32, 0, c->stream>>>(c->sc, which_ctrl);
+    GP_LAUNCH_CHECK(c);
+    return GPAIR_OK;
+}

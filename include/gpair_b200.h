@@ -1,0 +1,293 @@
+/*
+ * gpair_b200.h -- C ABI of the B200 (sm_100a) implementation of GPAIR's
+ * image-reconstruction hot path.
+ *
+ * Two layers, both plain C (pointers and sizes only):
+ *
+ * 1. The reference's own GPU boundary, gpair1/trunk/gpu.h:5-120, with the same
+ *    function names, argument order and meaning. OpenCL types are replaced by
+ *    layout-identical structs (cl_float2 -> gpair_float2, cl_long4 ->
+ *    gpair_long4, cl_short4 -> gpair_short4) and cl_mem* by the opaque
+ *    gpair_buf*. As in the reference these functions use one global context,
+ *    block until the device work is done, copy caller arrays in, and on error
+ *    print a message and exit (print_opencl_error, gpair1/trunk/gpu.c:186-202)
+ *    unless gpair_set_exit_on_error(0) was called.
+ *
+ * 2. Extensions: per-context handles, status codes instead of exit, device
+ *    twiddle generation from (u, v), precision modes, a device-resident CG
+ *    whose scalars never leave the GPU, and the host-side OIFITS indexer and
+ *    setup routines the reference keeps in getoifits.c / gpair.c.
+ *
+ * Image layout everywhere: float[N*N], x fastest (index x + y*N), as in
+ * gpair1/trunk/cpu.c:469. Data layout: data/data_err/mock are
+ * [npow V2 values][nbis x (T3 real, T3 imaginary)] (gpair1/trunk/gpair.c:1003-1062).
+ */
+#ifndef GPAIR_B200_H
+#define GPAIR_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ status codes */
+#define GPAIR_OK 0
+#define GPAIR_ERR_INVALID (-1)   /* bad argument / size / state */
+#define GPAIR_ERR_ALLOC (-2)     /* host or device allocation failed */
+#define GPAIR_ERR_CUDA (-3)      /* a CUDA runtime call failed */
+#define GPAIR_ERR_STATE (-4)     /* call out of order (e.g. no problem loaded) */
+#define GPAIR_ERR_TIMEOUT (-5)   /* a bounded device wait gave up */
+#define GPAIR_ERR_NO_DEVICE (-6) /* no CUDA device / not an sm_100 device */
+#define GPAIR_ERR_NUMERIC (-7)   /* NaN or Inf reached a reduction */
+
+/* ------------------------------------------------------------------ types */
+typedef struct { float s0, s1; } gpair_float2;                /* cl_float2 */
+typedef struct { int64_t s0, s1, s2, s3; } gpair_long4;       /* cl_long4 */
+typedef struct { int16_t s0, s1, s2, s3; } gpair_short4;      /* cl_short4 */
+typedef struct gpair_buf gpair_buf;                           /* cl_mem */
+typedef struct gpair_ctx gpair_ctx;
+
+/* oi_uv, gpair1/trunk/getoifits.h:53-59 */
+typedef struct { float u, v, bandwidth, wavelength; } gpair_uv;
+
+/* =========================================================================
+ * Layer 1: the reference boundary (gpair1/trunk/gpu.h)
+ * ========================================================================= */
+
+/* gpu.h:5   -- print the message and code, release the GPU, exit(0) */
+void print_opencl_error(char *error_message, int error_code);
+/* gpu.h:7   -- human-readable name of a status code */
+char *print_cl_errstring(int err);
+/* gpu.h:9   -- copy data_size floats from buffer input to buffer output */
+void gpu_backup_gradient(int data_size, gpair_buf *input, gpair_buf *output);
+/* gpu.h:11  -- prepares device-side tables (twiddle operands, triangle map) */
+void gpu_build_kernels(int data_size, int image_width, int image_size);
+/* gpu.h:17  -- debug comparison of CPU results against the device's
+ *             (prints like gpair1/trunk/gpu.c:501-612); NULL pointers are skipped */
+void gpu_check_data(float *cpu_chi2, int nuv, float *visi /* complex64[nuv] */, int data_size,
+                    float *mock_data, int image_size, float *data_grad);
+/* gpu.h:22  */
+void gpu_compare_data(int size, float *cpu_data, gpair_buf *pGpu_data);
+/* gpu.h:24  */
+void gpu_compare_complex_data(int size, float *cpu_data /* complex64 */, gpair_buf *pGpu_data);
+/* gpu.h:26-28 -- gradient_buffer = data_gradient - alpha * entropy_gradient */
+void gpu_compute_criterion_gradient(int image_width, float hyperparameter_entropy, gpair_buf *gradient_buffer);
+void gpu_compute_criterion_gradient_curr(int image_width, float hyperparameter_entropy);
+void gpu_compute_criterion_gradient_temp(int image_width, float hyperparameter_entropy);
+/* gpu.h:30  -- temp_image = current_image + steplength * descent_direction (no clamp) */
+void gpu_compute_criterion_step(int image_width, float steplength, float minvalue);
+/* gpu.h:32-35 */
+void gpu_compute_entropy(int image_width, gpair_buf *gpu_image, gpair_buf *entropy_storage);
+void gpu_compute_entropy_gradient(int image_width, gpair_buf *gpu_image);
+void gpu_compute_entropy_gradient_curr(int image_width);
+void gpu_compute_entropy_gradient_temp(int image_width);
+/* gpu.h:37  -- flux_storage = sum(image); flux_inverse_storage = 1/flux (on the device) */
+void gpu_compute_flux(gpair_buf *gpu_image, gpair_buf *flux_storage, gpair_buf *flux_inverse_storage);
+/* gpu.h:44-46 -- d chi2 / d image, from the visibilities and mock data of the
+ *                immediately preceding gpu_get_chi2 on the same image */
+void gpu_compute_data_gradient(gpair_buf *gpu_image, int nuv, int npow, int nbis, int image_width);
+void gpu_compute_data_gradient_curr(int nuv, int npow, int nbis, int image_width);
+void gpu_compute_data_gradient_temp(int nuv, int npow, int nbis, int image_width);
+/* gpu.h:48  -- descent_direction = beta * descent_direction - full_gradient_new */
+void gpu_compute_descent_dir(int image_width, float beta);
+/* gpu.h:50  -- upload data (padded to data_size), biphasors, triangle references, prior */
+void gpu_copy_data(float *data, float *data_err, int data_size, int data_size_uv, gpair_float2 *data_phasor,
+                   int phasor_size, int pow_size, gpair_long4 *gpu_bsref_uvpnt, gpair_short4 *gpu_bsref_sign,
+                   int bsref_size, float *default_model, int image_size, int image_width);
+/* gpu.h:56  -- DFT tables in the transposed layout [x][uv] (i = nuv*x + uv), dft_size entries each */
+void gpu_copy_dft(gpair_float2 *dft_x, gpair_float2 *dft_y, int dft_size);
+/* gpu.h:58  -- upload the current image (x_size * y_size floats) */
+void gpu_copy_image(float *image, int x_size, int y_size);
+/* gpu.h:60  */
+void gpu_cleanup(void);
+/* gpu.h:62  -- chi2 of the current mock data (device-resident result) */
+void gpu_data2chi2(int data_size);
+/* gpu.h:64  */
+int gpu_error_callback(char *error);
+/* gpu.h:66-68 -- chi2 of the current / temporary / given image */
+float gpu_get_chi2_curr(int nuv, int npow, int nbis, int data_alloc, int data_alloc_uv);
+float gpu_get_chi2_temp(int nuv, int npow, int nbis, int data_alloc, int data_alloc_uv);
+float gpu_get_chi2(int nuv, int npow, int nbis, int data_alloc, int data_alloc_uv, gpair_buf *gpu_image);
+/* gpu.h:70-72 -- Gull-Skilling entropy of the image */
+float gpu_get_entropy(int image_width, gpair_buf *gpu_image);
+float gpu_get_entropy_curr(int image_width);
+float gpu_get_entropy_temp(int image_width);
+/* gpu.h:74  -- blocking read of `size` floats of a device buffer into cpu_buffer */
+float *gpu_get_image(int size, float *cpu_buffer, gpair_buf *gpu_image);
+/* gpu.h:76  -- sum(array1 * array2) over data_width*data_height elements */
+float gpu_get_scalprod(int data_width, int data_height, gpair_buf *array1, gpair_buf *array2);
+/* gpu.h:78-84 -- borrowed handles of the device buffers */
+gpair_buf *gpu_getp_ci(void);  /* current image */
+gpair_buf *gpu_getp_ti(void);  /* temporary (trial) image */
+gpair_buf *gpu_getp_fgn(void); /* full gradient, new */
+gpair_buf *gpu_getp_fg(void);  /* full gradient, previous */
+gpair_buf *gpu_getp_dd(void);  /* descent direction */
+gpair_buf *gpu_getp_tg(void);  /* gradient at the trial image */
+gpair_buf *gpu_getp_eg(void);  /* entropy gradient */
+/* gpu.h:86-88 */
+void gpu_image2chi2(int nuv, int npow, int nbis, int data_alloc, int data_alloc_uv, gpair_buf *gpu_image);
+void gpu_image2vis(int nuv, int data_alloc_uv, gpair_buf *gpu_image);
+/* gpu.h:90  -- pick device 0 (or GPAIR_DEVICE), create the global context */
+void gpu_init(void);
+/* gpu.h:94  -- strong-Wolfe zoom between the two step lengths (gpair1/trunk/gpu.c:1947-2065) */
+float gpu_linesearch_zoom(int nuv, int npow, int nbis, int data_alloc, int data_alloc_uv, int image_width,
+                          float steplength_low, float steplength_high, float criterion_steplength_low,
+                          float wolfe_product1, float criterion_init, int *criterion_evals, int *grad_evals,
+                          gpair_buf *pDescent_direction, gpair_buf *pTemp_gradient, float hyperparameter_entropy);
+/* gpu.h:102 -- mock data + chi2 from the stored visibilities */
+void gpu_new_chi2(int nuv, int npow, int nbis, int data_alloc);
+/* gpu.h:104 -- V2 and T3 mock data from the stored visibilities */
+void gpu_vis2data(gpair_buf *gpu_vis, int nuv, int npow, int nbis);
+/* gpu.h:114 -- output = sum(array1 * array2) (device-resident) */
+void gpu_scalar_prod(int data_width, int data_height, gpair_buf *array1, gpair_buf *array2, gpair_buf *output);
+/* gpu.h:116 */
+void gpu_shutdown(void);
+/* gpu.h:118-119 -- image = max(image + steplength * d, minval); temp likewise into the temporary image */
+void gpu_update_image(int image_width, float steplength, float minval, gpair_buf *descent_direction);
+void gpu_update_tempimage(int image_width, float steplength, float minval, gpair_buf *descent_direction);
+
+/* =========================================================================
+ * Layer 2: extensions (status-returning, per-context)
+ * ========================================================================= */
+
+/* ---- host-side OIFITS indexing and setup (no device needed) ---- */
+
+/* OI_WAVELENGTH / OI_VIS2 / OI_T3 tables (gpair1/trunk/exchange.h:63-141);
+ * per-channel columns are row-major [numrec][nwave]. */
+typedef struct {
+    const char *insname;
+    int nwave;
+    const float *eff_wave, *eff_band;
+} gpair_oi_wavelength;
+typedef struct {
+    const char *insname;
+    long numrec;
+    int nwave;
+    const int *target_id;
+    const double *vis2data, *vis2err, *ucoord, *vcoord;
+    const char *flag;
+} gpair_oi_vis2;
+typedef struct {
+    const char *insname;
+    long numrec;
+    int nwave;
+    const int *target_id;
+    const double *t3amp, *t3amperr, *t3phi, *t3phierr, *u1coord, *v1coord, *u2coord, *v2coord;
+    const char *flag;
+} gpair_oi_t3;
+
+/* oi_data (gpair1/trunk/getoifits.h:61-75): arrays are malloc'd by
+ * gpair_get_oi_fits_data and released by gpair_free_oi_data. */
+typedef struct {
+    int npow, nbis, nuv;
+    float *pow, *powerr, *bisamp, *bisamperr, *bisphs, *bisphserr;
+    gpair_uv *uv;     /* [nuv] */
+    int64_t *uvpnt;   /* [nbis][3]: ab, bc, ca */
+    int16_t *sign;    /* [nbis][3]: +1, or -1 when the uv point is conjugated */
+} gpair_oi_data;
+
+/* get_oi_fits_data, gpair1/trunk/getoifits.c:65-357 (bit-exact, hashed matcher). */
+int gpair_get_oi_fits_data(int target_id, float minband, float maxband, int nwave_tables,
+                           const gpair_oi_wavelength *waves, int nvis2_tables, const gpair_oi_vis2 *vis2,
+                           int nt3_tables, const gpair_oi_t3 *t3, gpair_oi_data *out);
+void gpair_free_oi_data(gpair_oi_data *d);
+
+/* init_data, gpair1/trunk/gpair.c:997-1066. bisamp/bisamperr are updated in
+ * place on extrapolation. data/data_err hold npow + 2*nbis floats, phasor nbis
+ * complex values. Returns the change of ndof (<= 0). */
+int gpair_init_data(int do_extrapolation, int npow, int nbis, const float *pow, const float *powerr,
+                    float *bisamp, float *bisamperr, const float *bisphs, const float *bisphserr,
+                    const int64_t *uvpnt, float *data, float *data_err, gpair_float2 *phasor);
+
+/* set_model, gpair1/trunk/cpu.c:645-749 (types 0 flat, 1 Dirac, 2 disk, 3 Gaussian, 4 Lorentzian). */
+int gpair_set_model(int image_width, float image_pixellation, int modeltype, float modelwidth, float modelflux,
+                    float *default_model);
+
+/* DFT tables, gpair1/trunk/gpair.c:231-245 (CPU layout [nuv][N]) and, when
+ * dft_x_t/dft_y_t are non-NULL, the transposed device layout of
+ * gpair1/trunk/gpair.c:615-627 ([N][nuv], zero-padded to dft_alloc entries). */
+int gpair_dft_tables(int image_width, int nuv, const gpair_uv *uv, float pixellation, gpair_float2 *dft_x,
+                     gpair_float2 *dft_y, gpair_float2 *dft_x_t, gpair_float2 *dft_y_t, int dft_alloc);
+
+/* ---- device contexts ---- */
+
+#define GPAIR_PREC_FP32 0     /* CUDA-core FP32 DFT/adjoint (FP32 twiddles) */
+#define GPAIR_PREC_SPLIT16 1  /* tcgen05 f16 hi+lo split operands, 3 products, FP32 accumulate */
+#define GPAIR_PREC_TF32 2     /* tcgen05 TF32 operands, 1 product, FP32 accumulate */
+
+#define GPAIR_IMG_CURR 0
+#define GPAIR_IMG_TEMP 1
+
+int gpair_create(gpair_ctx **ctx, int device);
+int gpair_destroy(gpair_ctx *ctx);
+const char *gpair_strerror(int status);
+/* 1 = reference behaviour (layer 1 prints and exits on error), 0 = return */
+void gpair_set_exit_on_error(int on);
+/* the context used by layer 1 (created by gpu_init) */
+gpair_ctx *gpair_global_context(void);
+/* last CUDA error string seen by a context */
+const char *gpair_last_error(gpair_ctx *ctx);
+
+/* Load a problem. uv: nuv points; data/data_err: npow + 2*nbis; phasor: nbis;
+ * uvpnt/sign: [nbis][3]; default_model: N*N (copied). Twiddles are generated
+ * on the device from uv in FP64 phase with argument reduction. */
+int gpair_set_problem(gpair_ctx *ctx, int image_width, float pixellation, int nuv, const gpair_uv *uv, int npow,
+                      int nbis, const float *data, const float *data_err, const gpair_float2 *phasor,
+                      const int64_t *uvpnt, const int16_t *sign, const float *default_model);
+int gpair_set_precision(gpair_ctx *ctx, int mode);
+int gpair_get_precision(gpair_ctx *ctx);
+int gpair_set_image(gpair_ctx *ctx, int which, const float *image);
+int gpair_get_image(gpair_ctx *ctx, int which, float *image);
+
+/* One criterion evaluation on the current or temporary image:
+ * chi2 (FP64 sum), entropy S (FP64 sum); visibilities and mock data stay on the device. */
+int gpair_criterion(gpair_ctx *ctx, int which, double *chi2, double *entropy);
+/* Data gradient, entropy gradient and full gradient (data - alpha * entropy) of
+ * the image last passed to gpair_criterion. The full gradient goes to the new
+ * gradient (which = CURR) or the trial gradient (which = TEMP). */
+int gpair_gradient(gpair_ctx *ctx, int which, float alpha);
+/* read back device results of the last evaluation */
+int gpair_get_visibilities(gpair_ctx *ctx, gpair_float2 *visi);      /* nuv */
+int gpair_get_mock(gpair_ctx *ctx, float *mock);                     /* npow + 2*nbis */
+int gpair_get_data_gradient(gpair_ctx *ctx, float *grad);            /* N*N */
+int gpair_get_entropy_gradient(gpair_ctx *ctx, float *grad);         /* N*N */
+int gpair_get_full_gradient(gpair_ctx *ctx, int which, float *grad); /* N*N */
+
+/* Device-resident CG (reference control flow, FP64 scalars kept on the GPU). */
+typedef struct {
+    int method;       /* 0 SD, 1 FR, 2 PR+, 3 HS+ */
+    int iterations;
+    float alpha;      /* entropy hyperparameter */
+    double minvalue;  /* 1e-8 */
+    double wolfe1;    /* 1e-4 */
+    double wolfe2;    /* 0.1 */
+    double step_max;  /* 100 */
+    int max_zoom;     /* cap on zoom trials (reference: unbounded) */
+    int max_bracket;  /* cap on bracketing trials */
+} gpair_cg_params;
+
+typedef struct {
+    int iterations_done;
+    int criterion_evals;
+    int grad_evals;
+    double J, chi2, entropy; /* at the start of the last iteration */
+    double last_step, last_beta;
+    int status;
+} gpair_cg_result;
+
+void gpair_cg_default_params(gpair_cg_params *p);
+/* Runs p->iterations CG iterations from the current image. Per-iteration
+ * trace arrays (length p->iterations) may be NULL. */
+int gpair_cg_run(gpair_ctx *ctx, const gpair_cg_params *p, gpair_cg_result *res, double *trace_J,
+                 double *trace_chi2, double *trace_entropy, double *trace_step, double *trace_beta);
+
+/* Timing hooks for benchmarks: device time of the last gpair_cg_run (ms) and
+ * the algorithmic DFT + adjoint flop count it executed. */
+int gpair_last_run_stats(gpair_ctx *ctx, double *device_ms, double *dft_flops, int *kernel_launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GPAIR_B200_H */

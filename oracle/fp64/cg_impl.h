@@ -1,0 +1,161 @@
+/*
+ * cg_impl.h -- restatement of the reference's GPU-path nonlinear conjugate
+ * gradient with strong-Wolfe line search, instantiated for one scalar type.
+ *
+ * TEST INFRASTRUCTURE ONLY (oracle). Included by oracle_fp64.c twice:
+ *   REAL=double, CG(name)=o64_##name  -- the FP64 oracle's CG;
+ *   REAL=float,  CG(name)=o32_##name  -- the float CG that drives the
+ *                                        reference's own cpu.c functions
+ *                                        (the timed CPU baseline).
+ *
+ * Control flow follows, line by line in meaning:
+ *   main CG loop        gpair1/trunk/gpair.c:682-915
+ *   beta rules          gpair1/trunk/gpair.c:727-758 (0 SD, 1 FR, 2 PR+, 3 HS+,
+ *                       restart when |g_new.g_old|/|g_new|^2 > 0.5)
+ *   bracketing phase    gpair1/trunk/gpair.c:797-906
+ *   zoom                gpair1/trunk/gpu.c:1947-2065 (quadratic step with
+ *                       bisection fallback; J_lo is not updated inside zoom;
+ *                       acceptance when wolfe2 >= c2*wolfe1 or counter > 10)
+ *   image update        gpair1/trunk/gpair.c:910 (clamp at minvalue), then an
+ *                       unconditional gradient backup (gpair1/trunk/gpair.c:913)
+ * One deliberate difference: the zoom loop is capped at `max_zoom` trials.
+ * The reference loop has no cap and can spin forever once hi and lo are
+ * adjacent floating-point numbers; the cap only acts in that case.
+ */
+
+typedef struct {
+    void *ctx;
+    /* criterion J = chi2 - alpha*S of `image`; also returns chi2 and S */
+    REAL (*criterion)(void *ctx, const REAL *image, REAL *chi2, REAL *entropy);
+    /* full criterion gradient of `image` into `grad`; called only right after
+     * criterion() on the same image, as the reference requires */
+    void (*gradient)(void *ctx, const REAL *image, REAL *grad);
+} CG(evaluator);
+
+typedef struct {
+    int method;        /* 0 SD, 1 FR, 2 PR+, 3 HS+ */
+    int iterations;
+    REAL minvalue;     /* 1e-8 */
+    REAL wolfe1;       /* c1 = 1e-4 */
+    REAL wolfe2;       /* c2 = 0.1 */
+    REAL step_max;     /* 100 */
+    int max_zoom;
+} CG(params);
+
+typedef struct {
+    int criterion_evals, grad_evals;
+    /* per iteration (arrays of length iterations, may be NULL) */
+    REAL *J, *chi2, *entropy, *step, *beta;
+} CG(trace);
+
+static REAL CG(dot)(int n, const REAL *a, const REAL *b)
+{
+    REAL t = 0;
+    for (int i = 0; i < n; i++) t += a[i] * b[i];
+    return t;
+}
+
+static void CG(trial)(int n, const REAL *img, const REAL *d, REAL s, REAL minv, REAL *out)
+{
+    for (int i = 0; i < n; i++) {
+        REAL t = img[i] + s * d[i];
+        if (t < minv) t = minv;
+        out[i] = t;
+    }
+}
+
+static REAL CG(zoom)(const CG(evaluator) *ev, const CG(params) *p, int n, const REAL *img, const REAL *d,
+                      REAL lo, REAL hi, REAL J_lo, REAL wolfe_product1, REAL J_init,
+                      REAL *temp, REAL *tgrad, CG(trace) *tr)
+{
+    REAL s = 0, sel = 0, J = 0, J_old = 0, s_old = 0, chi2, S;
+    int counter = 0;
+    for (int guard = 0; guard < p->max_zoom; guard++) {
+        if (counter > 0 && (J_old - J_init - wolfe_product1 * s_old) != 0)
+            s = (REAL)fabs(wolfe_product1 * s_old * s_old / (2. * (J_old - J_init - wolfe_product1 * s_old)));
+        if (counter == 0 || s < lo || s > hi)
+            s = (hi - lo) / 2. + lo;
+        if (fabs(hi - lo) < 1e-14) return lo;
+        CG(trial)(n, img, d, s, p->minvalue, temp);
+        J = ev->criterion(ev->ctx, temp, &chi2, &S);
+        tr->criterion_evals++;
+        if ((J > (J_init + p->wolfe1 * s * wolfe_product1)) || (J >= J_lo)) {
+            hi = s;
+        } else {
+            ev->gradient(ev->ctx, temp, tgrad);
+            tr->grad_evals++;
+            REAL wolfe_product2 = CG(dot)(n, d, tgrad);
+            if ((wolfe_product2 >= p->wolfe2 * wolfe_product1) || (counter > 10)) {
+                sel = s;
+                return sel;
+            }
+            if (wolfe_product2 * (hi - lo) >= 0.) hi = lo;
+            lo = s;
+        }
+        s_old = s;
+        J_old = J;
+        counter++;
+    }
+    return lo;
+}
+
+/* Runs p->iterations CG iterations on `image` (updated in place). */
+static int CG(run)(const CG(evaluator) *ev, const CG(params) *p, int n, REAL *image, CG(trace) *tr)
+{
+    REAL *g_new = calloc(n, sizeof(REAL)), *g_old = calloc(n, sizeof(REAL));
+    REAL *d = calloc(n, sizeof(REAL)), *temp = calloc(n, sizeof(REAL)), *tgrad = calloc(n, sizeof(REAL));
+    if (!g_new || !g_old || !d || !temp || !tgrad) return -1;
+    REAL beta = 0, sel = 0, chi2, S;
+    tr->criterion_evals = tr->grad_evals = 0;
+    for (int it = 0; it < p->iterations; it++) {
+        REAL J = ev->criterion(ev->ctx, image, &chi2, &S);
+        tr->criterion_evals++;
+        ev->gradient(ev->ctx, image, g_new);
+        tr->grad_evals++;
+        if (it == 0 || p->method == 0) {
+            beta = 0.;
+        } else {
+            REAL nn = CG(dot)(n, g_new, g_new), no = CG(dot)(n, g_new, g_old), oo = CG(dot)(n, g_old, g_old);
+            if (p->method == 1) beta = nn / oo;
+            if (p->method == 2) { beta = (nn - no) / oo; if (beta < 0.) beta = 0.; }
+            if (p->method == 3) {
+                beta = (nn - no) / (CG(dot)(n, d, g_new) - CG(dot)(n, d, g_old));
+                if (beta < 0.) beta = 0.;
+            }
+            if (fabs(no / nn) > .5) beta = 0.;
+        }
+        if (tr->J) { tr->J[it] = J; tr->chi2[it] = chi2; tr->entropy[it] = S; tr->beta[it] = beta; }
+        for (int i = 0; i < n; i++) d[i] = beta * d[i] - g_new[i];
+        REAL wolfe_product1 = CG(dot)(n, d, g_new);
+        REAL s = 1., s_old = 0., J_init = J, J_old = J, Jt;
+        int ls_it = 1;
+        sel = 0.;
+        while (1) {
+            CG(trial)(n, image, d, s, p->minvalue, temp);
+            Jt = ev->criterion(ev->ctx, temp, &chi2, &S);
+            tr->criterion_evals++;
+            if ((Jt > (J_init + p->wolfe1 * s * wolfe_product1)) || ((Jt >= J_old) && (ls_it > 1))) {
+                sel = CG(zoom)(ev, p, n, image, d, s_old, s, J_old, wolfe_product1, J_init, temp, tgrad, tr);
+                break;
+            }
+            ev->gradient(ev->ctx, temp, tgrad);
+            tr->grad_evals++;
+            REAL wolfe_product2 = CG(dot)(n, d, tgrad);
+            if (fabs(wolfe_product2) <= -p->wolfe2 * wolfe_product1) { sel = s; break; }
+            if (wolfe_product2 >= 0.) {
+                sel = CG(zoom)(ev, p, n, image, d, s, s_old, Jt, wolfe_product1, J_init, temp, tgrad, tr);
+                break;
+            }
+            s_old = s;
+            J_old = Jt;
+            s = 10.0 * s;
+            if (s > p->step_max) s = p->step_max;
+            ls_it++;
+        }
+        if (tr->step) tr->step[it] = sel;
+        CG(trial)(n, image, d, sel, p->minvalue, image);
+        memcpy(g_old, g_new, sizeof(REAL) * n);
+    }
+    free(g_new); free(g_old); free(d); free(temp); free(tgrad);
+    return 0;
+}

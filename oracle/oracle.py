@@ -1,0 +1,284 @@
+"""CPU oracle of the reconstruction path -- TEST INFRASTRUCTURE ONLY.
+
+Loaded by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg as
+the checker; the product (gpair_b200) never imports it.
+
+Two native libraries, both built by oracle/Makefile:
+* lib/liboracle_fp64.so -- FP64 restatement of the reference's math and CG
+  (oracle/fp64/oracle_fp64.c), plus exact-float replicas of its setup code;
+* _ref/libgpair_ref.so  -- the reference's own gpair1/trunk/cpu.c and
+  gpair1/trunk/getoifits.c compiled unchanged, with an in-memory cfitsio shim
+  (oracle/shim), used to pin the restatement and as the timed CPU baseline.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+FP64_LIB = os.path.join(HERE, "lib", "liboracle_fp64.so")
+REF_LIB = os.path.join(HERE, "_ref", "libgpair_ref.so")
+
+_fp64 = None
+_ref = None
+
+
+def build():
+    """Build the oracle libraries (reference part only where its sources exist)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+def fp64() -> C.CDLL:
+    global _fp64
+    if _fp64 is None:
+        if not os.path.exists(FP64_LIB):
+            build()
+        L = C.CDLL(FP64_LIB)
+        vp, i, f, d = C.c_void_p, C.c_int, C.c_float, C.c_double
+        L.o_init_data.argtypes = [i, i, i, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+        L.o_dft_tables_f32.argtypes = [i, i, vp, f, vp, vp]
+        L.o64_image2vis.argtypes = [i, i, vp, vp, f, vp]
+        L.o64_vis2data.argtypes = [i, i, vp, vp, vp, vp, vp]
+        L.o64_data2chi2.argtypes = [i, vp, vp, vp]
+        L.o64_data2chi2.restype = d
+        L.o64_entropy.argtypes = [i, vp, vp]
+        L.o64_entropy.restype = d
+        L.o64_entropy_gradient.argtypes = [i, vp, vp, vp]
+        L.o64_data_gradient.argtypes = [i, i, i, vp, vp, f, vp, vp, vp, vp, vp, vp, vp, vp]
+        L.o64_evaluate.argtypes = [i, i, i, i, vp, f, vp, vp, vp, vp, vp, vp, vp, vp, vp, C.POINTER(d), vp]
+        L.o64_evaluate.restype = d
+        L.o64_reconstruct.argtypes = [i, i, i, i, vp, f, vp, vp, vp, vp, vp, vp, d, i, i, vp, C.POINTER(i),
+                                      C.POINTER(i), vp, vp, vp, vp, vp]
+        L.o32_ref_cg_run.argtypes = [vp, i, i, i, vp, f, i, i, vp, vp, vp, vp, vp, C.POINTER(i), C.POINTER(i), vp, vp,
+                                     vp, vp, vp]
+        L.o_set_threads.argtypes = [i]
+        _fp64 = L
+    return _fp64
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_LIB)
+
+
+class RefProblem(C.Structure):
+    _fields_ = [("image_width", C.c_int), ("nuv", C.c_int), ("npow", C.c_int), ("nbis", C.c_int),
+                ("data", C.c_void_p), ("data_err", C.c_void_p), ("phasor", C.c_void_p), ("uvpnt", C.c_void_p),
+                ("sign", C.c_void_p), ("dft_x", C.c_void_p), ("dft_y", C.c_void_p)]
+
+
+def ref() -> C.CDLL:
+    global _ref
+    if _ref is None:
+        if not ref_available():
+            build()
+        if not ref_available():
+            raise FileNotFoundError(f"{REF_LIB} not built (reference sources unavailable)")
+        L = C.CDLL(REF_LIB)
+        vp, i, f, d = C.c_void_p, C.c_int, C.c_float, C.c_double
+        L.oracle_shim_reset.argtypes = [i]
+        L.oracle_shim_add_wavelength.argtypes = [C.c_char_p, i, vp, vp]
+        L.oracle_shim_add_vis2.argtypes = [C.c_char_p, C.c_long, i, vp, vp, vp, vp, vp, vp]
+        L.oracle_shim_add_t3.argtypes = [C.c_char_p, C.c_long, i, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+        L.oracle_ref_get_oi_fits_data.argtypes = [i, f, f, C.c_long, C.c_long, C.POINTER(i), C.POINTER(i),
+                                                  C.POINTER(i), i]
+        L.oracle_ref_copy_oi_data.argtypes = [vp] * 9
+        L.oracle_ref_image2chi2.argtypes = [C.POINTER(RefProblem), vp, vp, vp, i]
+        L.oracle_ref_image2chi2.restype = f
+        L.oracle_ref_data_gradient.argtypes = [C.POINTER(RefProblem), vp, vp, vp, vp]
+        L.oracle_ref_entropy.argtypes = [i, vp, vp]
+        L.oracle_ref_entropy.restype = f
+        L.oracle_ref_entropy_gradient.argtypes = [i, vp, vp, vp]
+        L.oracle_ref_set_model.argtypes = [i, f, i, f, f, vp, i]
+        _ref = L
+    return _ref
+
+
+# ------------------------------------------------------------- indexing
+
+def ref_index(oi, minband: float = 0.0, maxband: float = 1e30, target_id: Optional[int] = None):
+    """Run the reference's get_oi_fits_data over OIFITS tables (gpair_b200.oifits.OIFits)."""
+    L = ref()
+    keep = []
+
+    def a(x, dt):
+        arr = np.ascontiguousarray(x, dtype=dt)
+        keep.append(arr)
+        return _p(arr)
+
+    L.oracle_shim_reset(oi.target_id)
+    for w in oi.wavelengths:
+        L.oracle_shim_add_wavelength(w.insname.encode(), len(w.eff_wave), a(w.eff_wave, np.float32),
+                                     a(w.eff_band, np.float32))
+    for t in oi.vis2:
+        L.oracle_shim_add_vis2(t.insname.encode(), len(t.ucoord), t.nwave, a(t.target_id, np.int32),
+                               a(t.vis2data, np.float64), a(t.vis2err, np.float64), a(t.ucoord, np.float64),
+                               a(t.vcoord, np.float64), a(t.flag, np.uint8))
+    for t in oi.t3:
+        L.oracle_shim_add_t3(t.insname.encode(), len(t.u1coord), t.nwave, a(t.target_id, np.int32),
+                             a(t.t3amp, np.float64), a(t.t3amperr, np.float64), a(t.t3phi, np.float64),
+                             a(t.t3phierr, np.float64), a(t.u1coord, np.float64), a(t.v1coord, np.float64),
+                             a(t.u2coord, np.float64), a(t.v2coord, np.float64), a(t.flag, np.uint8))
+    npow, nbis, nuv = C.c_int(), C.c_int(), C.c_int()
+    tid = oi.target_id if target_id is None else target_id
+    rc = L.oracle_ref_get_oi_fits_data(tid, minband, maxband, oi.num_vis2, oi.num_t3, C.byref(npow), C.byref(nbis),
+                                       C.byref(nuv), 1)
+    if rc:
+        raise RuntimeError(f"reference get_oi_fits_data status {rc}")
+    n, b, u = npow.value, nbis.value, nuv.value
+    out = dict(npow=n, nbis=b, nuv=u, pow=np.zeros(n, np.float32), powerr=np.zeros(n, np.float32),
+               bisamp=np.zeros(b, np.float32), bisamperr=np.zeros(b, np.float32), bisphs=np.zeros(b, np.float32),
+               bisphserr=np.zeros(b, np.float32), uv=np.zeros((u, 4), np.float32), uvpnt=np.zeros((b, 3), np.int64),
+               sign=np.zeros((b, 3), np.int16))
+    L.oracle_ref_copy_oi_data(*[_p(out[k]) for k in ("pow", "powerr", "bisamp", "bisamperr", "bisphs", "bisphserr",
+                                                     "uv", "uvpnt", "sign")])
+    return out
+
+
+# ----------------------------------------------------------- setup replicas
+
+def init_data(npow, nbis, pow_, powerr, bisamp, bisamperr, bisphs, bisphserr, uvpnt, do_extrapolation=1):
+    L = fp64()
+    nd = npow + 2 * nbis
+    data = np.zeros(max(nd, 1), np.float32)
+    err = np.zeros(max(nd, 1), np.float32)
+    ph = np.zeros(max(nbis, 1), np.complex64)
+    ba, be = np.array(bisamp, np.float32), np.array(bisamperr, np.float32)
+    uvpnt = np.ascontiguousarray(uvpnt, np.int64)
+    args = [np.ascontiguousarray(x, np.float32) for x in (pow_, powerr)]
+    args2 = [np.ascontiguousarray(x, np.float32) for x in (bisphs, bisphserr)]
+    delta = L.o_init_data(do_extrapolation, npow, nbis, _p(args[0]), _p(args[1]), _p(ba), _p(be), _p(args2[0]),
+                          _p(args2[1]), _p(uvpnt), _p(data), _p(err), _p(ph))
+    return data[:nd], err[:nd], ph[:nbis], int(delta)
+
+
+def dft_tables_f32(width, uv, pix):
+    uv = np.ascontiguousarray(uv, np.float32)
+    nuv = uv.shape[0]
+    tx = np.zeros(nuv * width, np.complex64)
+    ty = np.zeros(nuv * width, np.complex64)
+    fp64().o_dft_tables_f32(width, nuv, _p(uv), pix, _p(tx), _p(ty))
+    return tx, ty
+
+
+def ref_set_model(width, pix, modeltype, modelwidth, modelflux):
+    m = np.zeros(width * width, np.float32)
+    ref().oracle_ref_set_model(width, pix, modeltype, modelwidth, modelflux, _p(m), 1)
+    return m
+
+
+# -------------------------------------------------------------- FP64 math
+
+def evaluate64(p, image, want_grad=True, threads: int = 8):
+    """FP64 chi2, entropy, visibilities, mock and data gradient of `image` for a gpair_b200.Problem."""
+    L = fp64()
+    L.o_set_threads(threads)
+    img = np.ascontiguousarray(image, np.float64)
+    uv = np.ascontiguousarray(p.uv, np.float32)
+    visi = np.zeros(max(p.nuv, 1), np.complex128)
+    mock = np.zeros(max(p.npow + 2 * p.nbis, 1), np.float64)
+    grad = np.zeros(p.npix, np.float64) if want_grad else None
+    S = C.c_double()
+    keep = [np.ascontiguousarray(x) for x in (p.data.astype(np.float32), p.data_err.astype(np.float32),
+                                              p.phasor.astype(np.complex64), p.uvpnt.astype(np.int64),
+                                              p.sign.astype(np.int16), p.model.astype(np.float32))]
+    chi2 = L.o64_evaluate(p.width, p.nuv, p.npow, p.nbis, _p(uv), p.pixellation, _p(keep[0]), _p(keep[1]),
+                          _p(keep[2]), _p(keep[3]), _p(keep[4]), _p(keep[5]), _p(img), _p(visi), _p(mock),
+                          C.byref(S), _p(grad))
+    return dict(chi2=chi2, entropy=S.value, visi=visi[:p.nuv], mock=mock[:p.npow + 2 * p.nbis], data_grad=grad)
+
+
+def entropy_gradient64(image, model, prev=None):
+    g = np.zeros(len(image), np.float64) if prev is None else np.array(prev, np.float64)
+    img = np.ascontiguousarray(image, np.float64)
+    m = np.ascontiguousarray(model, np.float32)
+    fp64().o64_entropy_gradient(len(img), _p(img), _p(m), _p(g))
+    return g
+
+
+def reconstruct64(p, image, iterations, method=2, threads: int = 8):
+    """FP64 CG (reference GPU-path control flow) from `image`; returns (image, trace dict)."""
+    L = fp64()
+    L.o_set_threads(threads)
+    img = np.ascontiguousarray(image, np.float64).copy()
+    uv = np.ascontiguousarray(p.uv, np.float32)
+    tr = [np.zeros(iterations, np.float64) for _ in range(5)]
+    ce, ge = C.c_int(), C.c_int()
+    keep = [np.ascontiguousarray(x) for x in (p.data.astype(np.float32), p.data_err.astype(np.float32),
+                                              p.phasor.astype(np.complex64), p.uvpnt.astype(np.int64),
+                                              p.sign.astype(np.int16), p.model.astype(np.float32))]
+    rc = L.o64_reconstruct(p.width, p.nuv, p.npow, p.nbis, _p(uv), p.pixellation, _p(keep[0]), _p(keep[1]),
+                           _p(keep[2]), _p(keep[3]), _p(keep[4]), _p(keep[5]), p.alpha, method, iterations, _p(img),
+                           C.byref(ce), C.byref(ge), *[_p(t) for t in tr])
+    if rc:
+        raise RuntimeError("o64_reconstruct failed")
+    return img, dict(criterion_evals=ce.value, grad_evals=ge.value, J=tr[0], chi2=tr[1], entropy=tr[2], step=tr[3],
+                     beta=tr[4])
+
+
+# ------------------------------------------- the reference's own cpu.c
+
+class RefEvaluator:
+    """The reference's compiled cpu.c on one problem (float, CPU DFT tables)."""
+
+    def __init__(self, p, dft_x=None, dft_y=None):
+        L = ref()
+        self.p = p
+        if dft_x is None:
+            dft_x, dft_y = dft_tables_f32(p.width, p.uv, p.pixellation)
+        self._keep = [np.ascontiguousarray(p.data, np.float32), np.ascontiguousarray(p.data_err, np.float32),
+                      np.ascontiguousarray(p.phasor, np.complex64), np.ascontiguousarray(p.uvpnt, np.int64),
+                      np.ascontiguousarray(p.sign, np.int16), np.ascontiguousarray(dft_x, np.complex64),
+                      np.ascontiguousarray(dft_y, np.complex64)]
+        k = self._keep
+        self.prob = RefProblem(p.width, p.nuv, p.npow, p.nbis, _p(k[0]), _p(k[1]), _p(k[2]), _p(k[3]), _p(k[4]),
+                               _p(k[5]), _p(k[6]))
+        self.visi = np.zeros(max(p.nuv, 1), np.complex64)
+        self.mock = np.zeros(max(p.npow + 2 * p.nbis, 1), np.float32)
+        self.L = L
+
+    def chi2(self, image):
+        img = np.ascontiguousarray(image, np.float32).copy()
+        return float(self.L.oracle_ref_image2chi2(C.byref(self.prob), _p(img), _p(self.visi), _p(self.mock), 1))
+
+    def data_gradient(self, image):
+        img = np.ascontiguousarray(image, np.float32).copy()
+        g = np.zeros(self.p.npix, np.float32)
+        self.L.oracle_ref_data_gradient(C.byref(self.prob), _p(img), _p(self.visi), _p(self.mock), _p(g))
+        return g
+
+    def entropy(self, image):
+        img = np.ascontiguousarray(image, np.float32).copy()
+        m = np.ascontiguousarray(self.p.model, np.float32)
+        return float(self.L.oracle_ref_entropy(self.p.width, _p(img), _p(m)))
+
+    def entropy_gradient(self, image, prev=None):
+        img = np.ascontiguousarray(image, np.float32).copy()
+        m = np.ascontiguousarray(self.p.model, np.float32)
+        g = np.zeros(self.p.npix, np.float32) if prev is None else np.array(prev, np.float32)
+        self.L.oracle_ref_entropy_gradient(self.p.width, _p(img), _p(m), _p(g))
+        return g
+
+    def cg(self, image, iterations, method=2):
+        """Float CG (reference GPU-path control flow) over the reference's cpu.c. Returns (image, trace)."""
+        F = fp64()
+        img = np.ascontiguousarray(image, np.float32).copy()
+        m = np.ascontiguousarray(self.p.model, np.float32).copy()
+        tr = [np.zeros(iterations, np.float32) for _ in range(5)]
+        ce, ge = C.c_int(), C.c_int()
+        fn = lambda name: C.cast(getattr(self.L, name), C.c_void_p)  # noqa: E731
+        rc = F.o32_ref_cg_run(C.addressof(self.prob), self.p.width, self.p.nuv, self.p.npow + 2 * self.p.nbis, _p(m),
+                              self.p.alpha, method, iterations, _p(img), fn("oracle_ref_image2chi2"),
+                              fn("oracle_ref_data_gradient"), fn("oracle_ref_entropy"),
+                              fn("oracle_ref_entropy_gradient"), C.byref(ce), C.byref(ge), *[_p(t) for t in tr])
+        if rc:
+            raise RuntimeError("o32_ref_cg_run failed")
+        return img, dict(criterion_evals=ce.value, grad_evals=ge.value, J=tr[0], chi2=tr[1], entropy=tr[2],
+                         step=tr[3], beta=tr[4])
