@@ -1,0 +1,330 @@
+#!/usr/bin/env python
+"""Benchmark of the GPAIR reconstruction hot path on B200.
+
+Workload (default): the 256x256 "precision" reconstruction -- 0.05 mas/pixel,
+12 telescopes in a 400 m disk, 40 hour angles x 8 channels: 21,120 V2 points,
+70,400 closure triangles (nuv = 21,141 after the reference's uv matcher),
+seeded synthetic data (the reference publishes no data set of this size).
+
+A step is one plain PR+ nonlinear-CG iteration with the reference's strong
+Wolfe line search (criterion + gradient of the current image, direction
+update, bracketing/zoom trials, image update), continuing from the previous
+step. Metric: algorithmic DFT + adjoint TFLOP/s over the timed steps, i.e.
+(criterion + gradient evaluations) x (4 N^2 nuv + 8 N nuv) / time.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+`value` is timed with CUDA events on the library's stream (inputs resident in
+HBM, L2 flushed by a 512 MiB write before every step, outside the timed
+region); `e2e` times the same steps through the public C ABI with host
+buffers: image upload, one CG iteration, image read-back. With N > 1 each rank
+runs its own independent reconstruction (replicas, weak scaling); the time is
+the max over ranks. `--impl reference` times the reference's own compiled
+cpu.c (oracle/_ref) on a bounded sample of the same workload on all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "CG time-to-objective (learned warm-start vs plain) + DFT/grad TFLOP/s, 1 B200"
+UNIT = "TFLOP/s (algorithmic DFT+adjoint, plain PR+ CG iterations)"
+
+
+def _env_int(k, d):
+    try:
+        return int(os.environ.get(k, d))
+    except ValueError:
+        return d
+
+
+# ------------------------------------------------------------------ clocks
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.device)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ----------------------------------------------------------- measurements
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d["hbm_gbs"], d["bf16_tflops"], "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+def _traffic(kernel_key):
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f).get(kernel_key)
+    return None
+
+
+def cpu_sample_problem(p, width=32):
+    """Bounded CPU sample of the workload: the same data and uv coverage on a width x width image."""
+    import gpair_b200 as g
+    model = g.set_model(width, p.pixellation, 0, 0.0, 1.0)
+    return g.Problem(width, p.pixellation, p.uv, p.npow, p.nbis, p.data, p.data_err, p.phasor, p.uvpnt, p.sign,
+                     model, p.alpha)
+
+
+_SAMPLE_CACHE = {}
+
+
+def _ref_eval_worker(args):
+    """Criterion + gradient evaluations of the sample with the reference's own cpu.c (runs in a worker)."""
+    workload, width, reps = args
+    key = (workload, width)
+    if key not in _SAMPLE_CACHE:
+        import gpair_b200 as g
+        from oracle import oracle as O
+        s = cpu_sample_problem(g.workload_problem(workload), width)
+        _SAMPLE_CACHE[key] = (s, O.RefEvaluator(s))
+    s, ev = _SAMPLE_CACHE[key]
+    img = s.start_image()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        ev.chi2(img)
+        ev.data_gradient(img)
+        ev.entropy_gradient(img)
+    dt = time.perf_counter() - t0
+    flops = reps * 2 * s.dft_flops()
+    return flops, dt
+
+
+def cpu_baseline(workload, width=32, reps=3):
+    flops, dt = _ref_eval_worker((workload, width, reps))
+    return {"value": flops / dt / 1e12, "unit": UNIT, "cores": 1, "kind": "reference",
+            "sample": f"reference cpu.c criterion+gradient on a {width}x{width} image with the full data "
+                      f"({reps} evaluations, {dt:.1f} s)"}
+
+
+def run_reference(args, rank):
+    """The reference arm: the reference's own compiled cpu.c on all host cores."""
+    import multiprocessing as mp
+    if rank != 0:
+        return
+    import gpair_b200 as g
+    p = g.workload_problem(args.workload)
+    cores = os.cpu_count() or 1
+    width = 32
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        for _ in range(args.warmup):
+            pool.map(_ref_eval_worker, [(args.workload, width, 1)] * cores)
+        t0 = time.perf_counter()
+        tot = 0.0
+        for _ in range(args.steps):
+            res = pool.map(_ref_eval_worker, [(args.workload, width, 1)] * cores)
+            tot += sum(r[0] for r in res)
+        dt = time.perf_counter() - t0
+    value = tot / dt / 1e12
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": dt * 1e3 / max(args.steps, 1), "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32 (reference cpu.c, float complex)",
+           "data": "synthetic (seeded)", "impl": "reference",
+           "config": {"workload": f"{args.workload}: {p.width}x{p.width}, {p.npow} V2, {p.nbis} T3, nuv {p.nuv}",
+                      "sample": f"criterion+gradient on a {width}x{width} image with the full data, one per core"},
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                            "sample": f"{cores} processes x criterion+gradient on {width}x{width} with the full data"},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def run_ours(args, rank, world, local):
+    import numpy as np
+    import torch
+    import gpair_b200 as g
+
+    dist = world > 1
+    if dist:
+        import datetime
+        torch.cuda.set_device(local)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                             device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(local)
+    # one independent replica per rank: same array and scene, own noise seed
+    p = g.workload_problem(args.workload, scene_seed=1, noise_seed=2 + rank, array_seed=3)
+    prec = {"fp32": g.PREC_FP32, "split16": g.PREC_SPLIT16, "tf32": g.PREC_TF32}[args.precision]
+    rec = g.Reconstructor(local)
+    rec.set_problem(p)
+    rec.set_precision(prec)
+    rec.set_stage_timing(True)
+    rec.set_image(p.start_image())
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+
+    rec.cg(max(args.warmup, 1), method=2, resume=False)  # warm-up iterations (untimed)
+    sampler = ClockSampler(local)
+    if dist:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    time.sleep(0.5)  # let the sampler take its first sample before the timed steps
+    dev_ms, flops, launches, evals = 0.0, 0.0, 0, 0
+    stage_ms = {k: 0.0 for k in rec.STAGES}
+    stage_n = {k: 0 for k in rec.STAGES}
+    for k in range(args.steps):
+        flush.fill_(float(k))  # 512 MiB write: L2 (126 MB) holds none of the inputs at step start
+        torch.cuda.synchronize()
+        out = rec.cg(1, method=2, resume=True)
+        ms, fl, nl = rec.last_run_stats()
+        dev_ms += ms
+        flops += fl
+        launches += nl
+        evals += out["criterion_evals"] + out["grad_evals"]
+        for name, (t, n) in rec.last_run_stage_ms().items():
+            stage_ms[name] += t
+            stage_n[name] += n
+    torch.cuda.synchronize()
+    if dist:
+        torch.distributed.barrier()
+    clocks = sampler.stop()
+
+    # e2e: the same steps through the public API with host buffers
+    img = rec.get_image()
+    e2e_s, e2e_flops = 0.0, 0.0
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rec.set_image(img)  # H2D of the step's input image
+        rec.cg(1, method=2, resume=True)
+        img = rec.get_image()  # D2H of the step's result
+        e2e_s += time.perf_counter() - t0
+        e2e_flops += rec.last_run_stats()[1]
+
+    t = torch.tensor([dev_ms, e2e_s], dtype=torch.float64, device=f"cuda:{local}")
+    fsum = torch.tensor([flops, e2e_flops], dtype=torch.float64, device=f"cuda:{local}")
+    if dist:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        torch.distributed.all_reduce(fsum, op=torch.distributed.ReduceOp.SUM)
+    max_ms, max_e2e = float(t[0]), float(t[1])
+    tot_flops, tot_e2e_flops = float(fsum[0]), float(fsum[1])
+
+    if rank == 0:
+        hbm, tflops_peak, peak_kind = _peaks()
+        # dominant stage and its roofline
+        dom = max(stage_ms, key=lambda k: stage_ms[k])
+        per_launch_ms = stage_ms[dom] / max(stage_n[dom], 1)
+        N, nuv = p.width, p.nuv
+        if dom in ("forward_dft", "adjoint_dft"):
+            work = p.dft_flops()
+            achieved = work / (per_launch_ms * 1e-3) / 1e12
+            roof = {"bound": "tensor", "achieved": achieved, "peak": tflops_peak, "unit": "TFLOP/s",
+                    "frac": achieved / tflops_peak}
+        else:
+            bytes_per = {"prep": 8 * p.npix, "vis_data": 16 * p.npow + 60 * p.nbis,
+                         "adj_weights": 8 * p.npow + 24 * p.nbis, "grad_finalize": 16 * p.npix}[dom]
+            achieved = bytes_per / (per_launch_ms * 1e-3) / 1e9
+            roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm}
+        roof["kernel"] = dom
+        roof["peak_source"] = peak_kind
+        roof["traffic"] = _traffic(f"{dom}@{args.workload}@{args.precision}")
+        roof["stage_ms_per_launch"] = {k: stage_ms[k] / max(stage_n[k], 1) for k in stage_ms}
+        roof["stage_share"] = {k: stage_ms[k] / max(sum(stage_ms.values()), 1e-12) for k in stage_ms}
+        value = tot_flops / (max_ms * 1e-3) / 1e12
+        e2e = tot_e2e_flops / max_e2e / 1e12
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": {"fp32": "fp32", "split16": "f16 hi+lo split operands, fp32 accumulate",
+                          "tf32": "tf32 operands, fp32 accumulate"}[args.precision],
+                "data": "synthetic (seeded array, scene and noise; no public data set of this size)",
+                "config": {"workload": f"{args.workload}: {N}x{N} image, {p.npow} V2, {p.nbis} T3, nuv {nuv}",
+                           "step": "one PR+ CG iteration with strong-Wolfe line search (continuing)",
+                           "precision": args.precision, "evaluations": evals,
+                           "l2": "flushed (512 MiB write) before every timed step, outside the timed region",
+                           "parallelism": f"replicas x{world}"},
+                "gpu_launches": launches, "clocks": clocks, "roofline": roof,
+                "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 4 * p.npix,
+                        "d2h_bytes_per_step": 4 * p.npix}}
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(args.workload)
+        print(json.dumps(line), flush=True)
+    rec.close()
+    if dist:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="precision")
+    ap.add_argument("--precision", default=os.environ.get("GPAIR_BENCH_PRECISION", "fp32"),
+                    choices=["fp32", "split16", "tf32"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank, world, local = _env_int("RANK", 0), _env_int("WORLD_SIZE", 1), _env_int("LOCAL_RANK", 0)
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    run_ours(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -78,7 +78,7 @@ class OiData(C.Structure):
 class CgParams(C.Structure):
     _fields_ = [("method", C.c_int), ("iterations", C.c_int), ("alpha", C.c_float), ("minvalue", C.c_double),
                 ("wolfe1", C.c_double), ("wolfe2", C.c_double), ("step_max", C.c_double), ("max_zoom", C.c_int),
-                ("max_bracket", C.c_int)]
+                ("max_bracket", C.c_int), ("resume", C.c_int)]
 
 
 class CgResult(C.Structure):
@@ -116,6 +116,9 @@ def lib() -> C.CDLL:
         L.gpair_cg_default_params.argtypes = [C.POINTER(CgParams)]
         L.gpair_cg_run.argtypes = [vp, C.POINTER(CgParams), C.POINTER(CgResult), vp, vp, vp, vp, vp]
         L.gpair_last_run_stats.argtypes = [vp, C.POINTER(d), C.POINTER(d), C.POINTER(i)]
+        L.gpair_time_stages.argtypes = [vp, i, C.POINTER(d), i]
+        L.gpair_set_stage_timing.argtypes = [vp, i]
+        L.gpair_last_run_stage_ms.argtypes = [vp, C.POINTER(d), C.POINTER(i), i]
         L.gpair_get_oi_fits_data.argtypes = [i, f, f, i, vp, i, vp, i, vp, C.POINTER(OiData)]
         L.gpair_free_oi_data.argtypes = [C.POINTER(OiData)]
         L.gpair_init_data.argtypes = [i, i, i, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
@@ -123,8 +126,68 @@ def lib() -> C.CDLL:
         L.gpair_dft_tables.argtypes = [i, i, vp, f, vp, vp, vp, vp, i]
         L.gpair_set_exit_on_error.argtypes = [i]
         L.gpair_global_context.restype = vp
+        _declare_reference_boundary(L)
         _lib = L
     return _lib
+
+
+def _declare_reference_boundary(L):
+    """Prototypes of the reference-boundary functions (gpair1/trunk/gpu.h:5-120)."""
+    vp, i, f = C.c_void_p, C.c_int, C.c_float
+    proto = {
+        "print_opencl_error": (None, [C.c_char_p, i]),
+        "print_cl_errstring": (C.c_char_p, [i]),
+        "gpu_backup_gradient": (None, [i, vp, vp]),
+        "gpu_build_kernels": (None, [i, i, i]),
+        "gpu_check_data": (None, [vp, i, vp, i, vp, i, vp]),
+        "gpu_compare_data": (None, [i, vp, vp]),
+        "gpu_compare_complex_data": (None, [i, vp, vp]),
+        "gpu_compute_criterion_gradient": (None, [i, f, vp]),
+        "gpu_compute_criterion_gradient_curr": (None, [i, f]),
+        "gpu_compute_criterion_gradient_temp": (None, [i, f]),
+        "gpu_compute_criterion_step": (None, [i, f, f]),
+        "gpu_compute_entropy": (None, [i, vp, vp]),
+        "gpu_compute_entropy_gradient": (None, [i, vp]),
+        "gpu_compute_entropy_gradient_curr": (None, [i]),
+        "gpu_compute_entropy_gradient_temp": (None, [i]),
+        "gpu_compute_flux": (None, [vp, vp, vp]),
+        "gpu_compute_data_gradient": (None, [vp, i, i, i, i]),
+        "gpu_compute_data_gradient_curr": (None, [i, i, i, i]),
+        "gpu_compute_data_gradient_temp": (None, [i, i, i, i]),
+        "gpu_compute_descent_dir": (None, [i, f]),
+        "gpu_copy_data": (None, [vp, vp, i, i, vp, i, i, vp, vp, i, vp, i, i]),
+        "gpu_copy_dft": (None, [vp, vp, i]),
+        "gpu_copy_image": (None, [vp, i, i]),
+        "gpu_cleanup": (None, []),
+        "gpu_data2chi2": (None, [i]),
+        "gpu_error_callback": (i, [C.c_char_p]),
+        "gpu_get_chi2_curr": (f, [i, i, i, i, i]),
+        "gpu_get_chi2_temp": (f, [i, i, i, i, i]),
+        "gpu_get_chi2": (f, [i, i, i, i, i, vp]),
+        "gpu_get_entropy": (f, [i, vp]),
+        "gpu_get_entropy_curr": (f, [i]),
+        "gpu_get_entropy_temp": (f, [i]),
+        "gpu_get_image": (vp, [i, vp, vp]),
+        "gpu_get_scalprod": (f, [i, i, vp, vp]),
+        "gpu_image2chi2": (None, [i, i, i, i, i, vp]),
+        "gpu_image2vis": (None, [i, i, vp]),
+        "gpu_init": (None, []),
+        "gpu_linesearch_zoom": (f, [i, i, i, i, i, i, f, f, f, f, f, vp, vp, vp, vp, f]),
+        "gpu_new_chi2": (None, [i, i, i, i]),
+        "gpu_vis2data": (None, [vp, i, i, i]),
+        "gpu_scalar_prod": (None, [i, i, vp, vp, vp]),
+        "gpu_shutdown": (None, []),
+        "gpu_update_image": (None, [i, f, f, vp]),
+        "gpu_update_tempimage": (None, [i, f, f, vp]),
+    }
+    for name in ("gpu_getp_ci", "gpu_getp_ti", "gpu_getp_fgn", "gpu_getp_fg", "gpu_getp_dd", "gpu_getp_tg",
+                 "gpu_getp_eg"):
+        proto[name] = (vp, [])
+    for name, (res, args) in proto.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+
 
 
 def _p(a: np.ndarray) -> int:
@@ -392,11 +455,13 @@ class Reconstructor:
         self._c(self._L.gpair_get_full_gradient(self.h, which, _p(g)))
         return g
 
-    def cg(self, iterations: int, method: int = 2, alpha: Optional[float] = None, trace: bool = False, **kw):
+    def cg(self, iterations: int, method: int = 2, alpha: Optional[float] = None, trace: bool = False,
+           resume: bool = False, **kw):
         prm = CgParams()
         self._L.gpair_cg_default_params(C.byref(prm))
         prm.method = method
         prm.iterations = iterations
+        prm.resume = 1 if resume else 0
         prm.alpha = self.problem.alpha if alpha is None else alpha
         for k, v in kw.items():
             setattr(prm, k, v)
@@ -410,6 +475,24 @@ class Reconstructor:
         if trace:
             out.update(zip(("trace_J", "trace_chi2", "trace_entropy", "trace_step", "trace_beta"), tr))
         return out
+
+    STAGES = ("prep", "forward_dft", "vis_data", "adj_weights", "adjoint_dft", "grad_finalize")
+
+    def time_stages(self, reps: int = 10) -> dict:
+        ms = (C.c_double * 6)()
+        n = self._L.gpair_time_stages(self.h, reps, ms, 6)
+        if n < 0:
+            self._c(n)
+        return {k: ms[j] for j, k in enumerate(self.STAGES[:n])}
+
+    def set_stage_timing(self, on: bool = True):
+        self._c(self._L.gpair_set_stage_timing(self.h, 1 if on else 0))
+
+    def last_run_stage_ms(self) -> dict:
+        ms = (C.c_double * 6)()
+        cnt = (C.c_int * 6)()
+        n = self._L.gpair_last_run_stage_ms(self.h, ms, cnt, 6)
+        return {k: (ms[j], cnt[j]) for j, k in enumerate(self.STAGES[:n])}
 
     def last_run_stats(self):
         ms, fl, n = C.c_double(), C.c_double(), C.c_int()

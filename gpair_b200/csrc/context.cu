@@ -7,6 +7,7 @@
 // controller k_cg_ctrl, which holds every CG scalar in FP64 on the GPU; the
 // host only reads back the controller's next action (evaluate criterion,
 // evaluate gradient, or accept the step).
+#include <stddef.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -131,6 +132,12 @@ extern "C" int gpair_destroy(gpair_ctx *c)
     FREE_DEV(c->sc);
     FREE_DEV(c->partials);
     if (c->sc_host) cudaFreeHost(c->sc_host);
+    if (c->st_ev) {
+        for (int i = 0; i < 2 * GP_MAX_STAGE_REC; i++)
+            if (c->st_ev[i]) cudaEventDestroy(c->st_ev[i]);
+        free(c->st_ev);
+        free(c->st_stage);
+    }
     if (c->stream) cudaStreamDestroy(c->stream);
     free(c->ref_dft_x); free(c->ref_dft_y); free(c->ref_data); free(c->ref_data_err); free(c->ref_model);
     free(c->ref_phasor); free(c->ref_uvpnt); free(c->ref_sign);
@@ -287,14 +294,75 @@ int gp_sync_scalars(gpair_ctx *c)
     return GPAIR_OK;
 }
 
+// ----------------------------------------------------------- stage timing
+
+void gp_stage_begin(gpair_ctx *c, int stage)
+{
+    if (!c->stage_timing || !c->st_ev || c->st_n >= GP_MAX_STAGE_REC) return;
+    c->st_stage[c->st_n] = stage;
+    cudaEventRecord(c->st_ev[2 * c->st_n], c->stream);
+}
+
+void gp_stage_end(gpair_ctx *c)
+{
+    if (!c->stage_timing || !c->st_ev || c->st_n >= GP_MAX_STAGE_REC) return;
+    cudaEventRecord(c->st_ev[2 * c->st_n + 1], c->stream);
+    c->st_n++;
+}
+
+static void stage_collect(gpair_ctx *c)
+{
+    for (int i = 0; i < 8; i++) { c->stage_ms[i] = 0.0; c->stage_cnt[i] = 0; }
+    for (int r = 0; r < c->st_n; r++) {
+        float t = 0.f;
+        if (cudaEventElapsedTime(&t, c->st_ev[2 * r], c->st_ev[2 * r + 1]) == cudaSuccess) {
+            c->stage_ms[c->st_stage[r]] += t;
+            c->stage_cnt[c->st_stage[r]]++;
+        }
+    }
+    c->st_n = 0;
+}
+
+extern "C" int gpair_set_stage_timing(gpair_ctx *c, int on)
+{
+    if (!c) return GPAIR_ERR_INVALID;
+    if (on && !c->st_ev) {
+        GP_CUDA(c, cudaSetDevice(c->device));
+        c->st_ev = (cudaEvent_t *)calloc(2 * GP_MAX_STAGE_REC, sizeof(cudaEvent_t));
+        c->st_stage = (int *)calloc(GP_MAX_STAGE_REC, sizeof(int));
+        if (!c->st_ev || !c->st_stage) return GPAIR_ERR_ALLOC;
+        for (int i = 0; i < 2 * GP_MAX_STAGE_REC; i++) GP_CUDA(c, cudaEventCreate(&c->st_ev[i]));
+    }
+    c->stage_timing = on ? 1 : 0;
+    c->st_n = 0;
+    return GPAIR_OK;
+}
+
+extern "C" int gpair_last_run_stage_ms(gpair_ctx *c, double *ms, int *counts, int max_stages)
+{
+    if (!c || !ms) return GPAIR_ERR_INVALID;
+    int n = max_stages < GPAIR_NSTAGES ? max_stages : GPAIR_NSTAGES;
+    for (int i = 0; i < n; i++) {
+        ms[i] = c->stage_ms[i];
+        if (counts) counts[i] = c->stage_cnt[i];
+    }
+    return n;
+}
+
 // ----------------------------------------------------------- evaluations
 
 int gp_eval_criterion(gpair_ctx *c, int which, int trial)
 {
     int rc;
+    gp_stage_begin(c, 0);
     if ((rc = gp_prep_image(c, trial ? GPAIR_IMG_TEMP : which, trial, 0.0, trial))) return rc;
+    gp_stage_end(c);
+    gp_stage_begin(c, 1);
     if ((rc = gp_forward(c, trial ? GPAIR_IMG_TEMP : which))) return rc;
+    gp_stage_end(c);
+    gp_stage_begin(c, 2);
     if ((rc = gp_vis_data(c))) return rc;
+    gp_stage_end(c);
     c->last_image_src = trial ? GPAIR_IMG_TEMP : which;
     return GPAIR_OK;
 }
@@ -302,8 +370,16 @@ int gp_eval_criterion(gpair_ctx *c, int which, int trial)
 int gp_eval_gradient(gpair_ctx *c, int which, float alpha)
 {
     int rc;
-    if ((rc = gp_adjoint(c, which))) return rc;
-    return gp_grad_finalize(c, which, GRAD_FUSED, alpha);
+    gp_stage_begin(c, 3);
+    if ((rc = gp_adj_weights_only(c))) return rc;
+    gp_stage_end(c);
+    gp_stage_begin(c, 4);
+    if ((rc = gp_adjoint_contraction(c, which))) return rc;
+    gp_stage_end(c);
+    gp_stage_begin(c, 5);
+    rc = gp_grad_finalize(c, which, GRAD_FUSED, alpha);
+    gp_stage_end(c);
+    return rc;
 }
 
 extern "C" int gpair_criterion(gpair_ctx *c, int which, double *chi2, double *entropy)
@@ -367,6 +443,7 @@ extern "C" void gpair_cg_default_params(gpair_cg_params *p)
     p->step_max = 100.0;
     p->max_zoom = 200;
     p->max_bracket = 100;
+    p->resume = 0;
 }
 
 static int read_action(gpair_ctx *c, int *action)
@@ -395,9 +472,16 @@ extern "C" int gpair_cg_run(gpair_ctx *c, const gpair_cg_params *p, gpair_cg_res
     h.c1 = p->wolfe1;
     h.c2 = p->wolfe2;
     h.step_max = p->step_max;
-    GP_CUDA(c, cudaMemcpyAsync(&c->sc->cg, &h, sizeof(CgState), cudaMemcpyHostToDevice, c->stream));
-    int rc = gp_cg_kernel(c, CTRL_INIT);
-    if (rc) return rc;
+    int rc;
+    if (p->resume) {
+        // parameters only; the iteration state of the previous run is kept
+        GP_CUDA(c, cudaMemcpyAsync(&c->sc->cg, &h, offsetof(CgState, it), cudaMemcpyHostToDevice, c->stream));
+        if ((rc = gp_cg_kernel(c, CTRL_RESUME))) return rc;
+    } else {
+        GP_CUDA(c, cudaMemcpyAsync(&c->sc->cg, &h, sizeof(CgState), cudaMemcpyHostToDevice, c->stream));
+        if ((rc = gp_cg_kernel(c, CTRL_INIT))) return rc;
+    }
+    c->st_n = 0;
     cudaEvent_t e0, e1;
     GP_CUDA(c, cudaEventCreate(&e0));
     GP_CUDA(c, cudaEventCreate(&e1));
@@ -445,6 +529,7 @@ extern "C" int gpair_cg_run(gpair_ctx *c, const gpair_cg_params *p, gpair_cg_res
     GP_CUDA(c, cudaEventSynchronize(e1));
     float ms = 0.f;
     cudaEventElapsedTime(&ms, e0, e1);
+    if (c->stage_timing) stage_collect(c);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     int rc2 = gp_sync_scalars(c);
@@ -478,3 +563,40 @@ extern "C" int gpair_last_run_stats(gpair_ctx *c, double *ms, double *flops, int
 }
 
 double gp_adjoint_scale(gpair_ctx *c);
+
+extern "C" int gpair_time_stages(gpair_ctx *c, int reps, double *ms, int max_stages)
+{
+    if (!c || !c->have_problem || reps <= 0 || !ms) return GPAIR_ERR_INVALID;
+    GP_CUDA(c, cudaSetDevice(c->device));
+    const int ns = GPAIR_NSTAGES;
+    cudaEvent_t ev[GPAIR_NSTAGES + 1];
+    for (int i = 0; i <= ns; i++) GP_CUDA(c, cudaEventCreate(&ev[i]));
+    double acc[GPAIR_NSTAGES] = {0};
+    int rc = GPAIR_OK;
+    for (int r = 0; r < reps && !rc; r++) {
+        cudaEventRecord(ev[0], c->stream);
+        if ((rc = gp_prep_image(c, GPAIR_IMG_CURR, 0, 0.0, 0))) break;
+        cudaEventRecord(ev[1], c->stream);
+        if ((rc = gp_forward(c, GPAIR_IMG_CURR))) break;
+        cudaEventRecord(ev[2], c->stream);
+        if ((rc = gp_vis_data(c))) break;
+        cudaEventRecord(ev[3], c->stream);
+        if ((rc = gp_adj_weights_only(c))) break;
+        cudaEventRecord(ev[4], c->stream);
+        if ((rc = gp_adjoint_contraction(c, GPAIR_IMG_CURR))) break;
+        cudaEventRecord(ev[5], c->stream);
+        if ((rc = gp_grad_finalize(c, GPAIR_IMG_CURR, GRAD_FUSED, 1e-3f))) break;
+        cudaEventRecord(ev[6], c->stream);
+        if (cudaEventSynchronize(ev[6]) != cudaSuccess) { rc = GPAIR_ERR_CUDA; break; }
+        for (int i = 0; i < ns; i++) {
+            float t = 0.f;
+            cudaEventElapsedTime(&t, ev[i], ev[i + 1]);
+            acc[i] += t;
+        }
+    }
+    for (int i = 0; i <= ns; i++) cudaEventDestroy(ev[i]);
+    if (rc) return rc;
+    int n = max_stages < ns ? max_stages : ns;
+    for (int i = 0; i < n; i++) ms[i] = acc[i] / reps;
+    return n;
+}

@@ -25,6 +25,7 @@
 
 #define GP_THREADS 256
 #define GP_MAX_PARTIALS 4096
+#define GP_MAX_STAGE_REC 8192
 
 // Reduction slots (index into DevScalars::counter / partial areas)
 enum {
@@ -121,6 +122,14 @@ struct gpair_ctx {
     long long last_launches;  // launches of the last gpair_cg_run
     int last_image_src;  // which image the last criterion used (0/1), -1 none
 
+    // live stage timing inside gpair_cg_run (events on the context stream)
+    int stage_timing;
+    cudaEvent_t *st_ev;   // 2 * GP_MAX_STAGE_REC events
+    int *st_stage;        // stage id per record
+    int st_n;
+    double stage_ms[8];
+    int stage_cnt[8];
+
     // reference-boundary staging (layer 1)
     gpair_float2 *ref_dft_x, *ref_dft_y;  // host copies of the transposed tables
     int ref_dft_size;
@@ -156,6 +165,10 @@ struct gpair_ctx {
 
 static inline int gp_cdiv(long long a, long long b) { return (int)((a + b - 1) / b); }
 
+// stage timing (context.cu): bracket the launches of one stage
+void gp_stage_begin(gpair_ctx *c, int stage);
+void gp_stage_end(gpair_ctx *c);
+
 // kernel launchers (kernels_core.cu)
 int gp_gen_twiddles(gpair_ctx *c);
 int gp_twiddles_from_ref_tables(gpair_ctx *c, const float2 *dft_x_t, const float2 *dft_y_t);
@@ -164,6 +177,8 @@ int gp_prep_image(gpair_ctx *c, int which, int trial_mode, double step_host, int
 int gp_forward(gpair_ctx *c, int which);
 int gp_vis_data(gpair_ctx *c);
 int gp_adjoint(gpair_ctx *c, int which);
+int gp_adj_weights_only(gpair_ctx *c);
+int gp_adjoint_contraction(gpair_ctx *c, int which);
 int gp_grad_finalize(gpair_ctx *c, int which, int mode, float alpha);
 int gp_entropy_gradient(gpair_ctx *c, int which);
 int gp_criterion_gradient(gpair_ctx *c, float alpha, float *out);
@@ -175,7 +190,7 @@ int gp_cg_kernel(gpair_ctx *c, int which_ctrl);
 int gp_sync_scalars(gpair_ctx *c);
 
 enum { GRAD_FUSED = 0, GRAD_DATA_ONLY = 1 };
-enum { CTRL_BEGIN = 0, CTRL_AFTER_DIR = 1, CTRL_AFTER_CRIT = 2, CTRL_AFTER_GRAD = 3, CTRL_INIT = 4 };
+enum { CTRL_BEGIN = 0, CTRL_AFTER_DIR = 1, CTRL_AFTER_CRIT = 2, CTRL_AFTER_GRAD = 3, CTRL_INIT = 4, CTRL_RESUME = 5 };
 
 // tensor-core path (umma_dft.cu); return GPAIR_ERR_STATE when unavailable
 int gp_tc_prepare(gpair_ctx *c);

@@ -536,15 +536,26 @@ static int adj_splits(int N, int nuv)
     return s < 1 ? 1 : s;
 }
 
-int gp_adjoint(gpair_ctx *c, int which)
+int gp_adj_weights_only(gpair_ctx *c)
 {
-    (void)which;
     int nb = gp_cdiv(c->nuv, GP_THREADS);
     if (nb > 592) nb = 592;
     if (nb < 1) nb = 1;
     k_adj_weights<<<nb, GP_THREADS, 0, c->stream>>>(c->nuv, c->inc_off, c->inc_idx, c->trib, c->visd, c->cw,
                                                     slot_partials(c, RED_ADJ), c->sc);
     GP_LAUNCH_CHECK(c);
+    return GPAIR_OK;
+}
+
+int gp_adjoint(gpair_ctx *c, int which)
+{
+    int rc = gp_adj_weights_only(c);
+    if (rc) return rc;
+    return gp_adjoint_contraction(c, which);
+}
+
+int gp_adjoint_contraction(gpair_ctx *c, int which)
+{
     if (c->precision != GPAIR_PREC_FP32) return gp_tc_adjoint(c, which);
     int S = c->splits;
     int kchunk = gp_cdiv(c->nuv, S);
@@ -807,6 +818,11 @@ __global__ void k_cg_ctrl(DevScalars *__restrict__ sc, int what)
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     CgState &s = sc->cg;
     switch (what) {
+    case CTRL_RESUME:
+        // a continued run counts its own evaluations; the iteration state is kept
+        s.criterion_evals = s.grad_evals = 0;
+        sc->nonfinite = 0;
+        break;
     case CTRL_INIT:
         s.it = 0;
         s.criterion_evals = s.grad_evals = 0;

@@ -265,6 +265,8 @@ typedef struct {
     double step_max;  /* 100 */
     int max_zoom;     /* cap on zoom trials (reference: unbounded) */
     int max_bracket;  /* cap on bracketing trials */
+    int resume;       /* 0: start a new run; 1: continue the previous run's CG state
+                         (iteration count, previous gradient, descent direction) */
 } gpair_cg_params;
 
 typedef struct {
@@ -285,6 +287,21 @@ int gpair_cg_run(gpair_ctx *ctx, const gpair_cg_params *p, gpair_cg_result *res,
 /* Timing hooks for benchmarks: device time of the last gpair_cg_run (ms) and
  * the algorithmic DFT + adjoint flop count it executed. */
 int gpair_last_run_stats(gpair_ctx *ctx, double *device_ms, double *dft_flops, int *kernel_launches);
+
+/* Stages of one criterion + gradient evaluation, timed with CUDA events on
+ * the context's stream (average ms over `reps` repetitions, on the current
+ * image): [0] image prep (flux, entropy), [1] forward DFT, [2] V2/T3/chi2 and
+ * adjoint weights, [3] per-uv weight gather, [4] adjoint DFT, [5] gradient
+ * finalize. Returns the number of stages written (<= max_stages). */
+#define GPAIR_NSTAGES 6
+int gpair_time_stages(gpair_ctx *ctx, int reps, double *stage_ms, int max_stages);
+
+/* Live stage timing inside gpair_cg_run: when on, every stage launch of the
+ * run is bracketed by CUDA events on the context's stream;
+ * gpair_last_run_stage_ms returns the summed ms and launch count per stage
+ * (same stage order as gpair_time_stages) of the last run. */
+int gpair_set_stage_timing(gpair_ctx *ctx, int on);
+int gpair_last_run_stage_ms(gpair_ctx *ctx, double *stage_ms, int *stage_launches, int max_stages);
 
 #ifdef __cplusplus
 }

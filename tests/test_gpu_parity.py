@@ -1,0 +1,231 @@
+"""GPU parity: the CUDA path (through the C ABI) against the FP64 CPU oracle.
+
+Tolerances (against FP64, as the design states them):
+  visibilities        |V - V64| <= 1e-5 (V is normalised by the total flux)
+  chi2                <= 1e-5 relative
+  data gradient       <= 1e-5 relative (L2 over the image)
+  entropy, gradient   <= 1e-10 relative (FP64 sums, FP64 log per pixel)
+  CG trace            J <= 1e-5 relative per iteration, identical evaluation counts
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import gpair_b200 as g
+from gpair_b200 import synth
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+PRECISIONS = [g.PREC_FP32]
+
+
+def _problem(name, seeds=(1, 2, 3)):
+    w, oi = synth.make_workload_data(name, *seeds)
+    return g.problem_from_oifits(oi, w.image_width, w.pixellation_mas, w.alpha)
+
+
+@pytest.fixture(scope="module")
+def rec():
+    r = g.Reconstructor(0)
+    yield r
+    r.close()
+
+
+def _rand_image(p, seed):
+    rng = np.random.default_rng(seed)
+    return (p.start_image() * (1 + rng.uniform(0, 2, p.npix))).astype(np.float32)
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(np.asarray(a, np.float64) - b) / max(np.linalg.norm(b), 1e-300))
+
+
+@pytest.mark.parametrize("prec", PRECISIONS)
+@pytest.mark.parametrize("name", ["tiny", "small"])
+def test_criterion_and_gradient_match_fp64(rec, name, prec):
+    p = _problem(name)
+    rec.set_problem(p)
+    rec.set_precision(prec)
+    img = _rand_image(p, 7)
+    rec.set_image(img)
+    chi2, S = rec.criterion()
+    e = O.evaluate64(p, img)
+    assert abs(chi2 - e["chi2"]) / e["chi2"] <= 1e-5
+    assert abs(S - e["entropy"]) <= 1e-10 * max(1.0, abs(e["entropy"]))
+    assert np.abs(rec.visibilities() - e["visi"]).max() <= 1e-5
+    m = rec.mock()
+    assert np.allclose(m, e["mock"], rtol=1e-4, atol=2e-6)
+    rec.gradient()
+    assert _rel(rec.data_gradient(), e["data_grad"]) <= 1e-5
+    eg = O.entropy_gradient64(img, p.model)
+    assert np.allclose(rec.entropy_gradient(), eg, rtol=1e-6, atol=1e-7)
+    full = e["data_grad"] - np.float32(p.alpha) * eg
+    assert _rel(rec.full_gradient(), full) <= 1e-5
+
+
+def test_device_cg_matches_fp64_cg(rec):
+    p = _problem("tiny", (21, 22, 23))
+    rec.set_problem(p)
+    rec.set_precision(g.PREC_FP32)
+    img0 = p.start_image()
+    iters = 8
+    _, tr = O.reconstruct64(p, img0, iters)
+    rec.set_image(img0)
+    out = rec.cg(iters, method=2, trace=True)
+    # identical line-search decisions early on, FP64 objective within 1e-5
+    n = 4
+    assert np.allclose(out["trace_J"][:n], tr["J"][:n], rtol=1e-5)
+    assert np.allclose(out["trace_step"][:n], tr["step"][:n], rtol=1e-4)
+    assert out["trace_J"][-1] < out["trace_J"][0]
+    assert abs(out["trace_J"][-1] - tr["J"][-1]) / abs(tr["J"][-1]) < 1e-3
+
+
+def test_cg_methods_run_and_descend(rec):
+    p = _problem("tiny", (5, 6, 7))
+    rec.set_problem(p)
+    for method in (0, 1, 2, 3):
+        rec.set_image(p.start_image())
+        out = rec.cg(5, method=method, trace=True)
+        assert out["iterations"] == 5
+        assert out["trace_J"][-1] <= out["trace_J"][0]
+
+
+def _ref_boundary_run(p, iters, alpha):
+    """The reference's GPU-path main loop (gpair1/trunk/gpair.c:640-915) through the gpu_* C ABI."""
+    L = g.lib()  # prototypes of the gpu_* boundary are declared by gpair_b200.api
+    L.gpair_set_exit_on_error(0)
+    N, nuv, npow, nbis = p.width, p.nuv, p.npow, p.nbis
+    p2 = lambda n: 1 << int(np.ceil(np.log2(max(n, 1))))  # noqa: E731
+    alloc_uv, alloc_pow, alloc_bis = p2(nuv), p2(npow), p2(nbis)
+    data_alloc = alloc_pow + alloc_bis
+    data = np.zeros(data_alloc + 2 * nbis, np.float32)
+    err = np.zeros_like(data)
+    data[:npow + 2 * nbis] = p.data
+    err[:npow + 2 * nbis] = p.data_err
+    phasor = np.zeros(alloc_bis, np.complex64)
+    phasor[:nbis] = p.phasor
+    uvpnt = np.zeros((alloc_bis, 4), np.int64)
+    uvpnt[:nbis, :3] = p.uvpnt
+    sign = np.zeros((alloc_bis, 4), np.int16)
+    sign[:nbis, :3] = p.sign
+    _, _, gx, gy = g.dft_tables(N, p.uv, p.pixellation, transposed=True)
+    image = p.start_image()
+    L.gpu_init()
+    L.gpu_copy_data(data.ctypes.data, err.ctypes.data, len(data), alloc_uv, phasor.ctypes.data, alloc_bis, npow,
+                    uvpnt.ctypes.data, sign.ctypes.data, alloc_bis, p.model.ctypes.data, N * N, N)
+    L.gpu_copy_image(image.ctypes.data, N, N)
+    L.gpu_copy_dft(gx.ctypes.data, gy.ctypes.data, len(gx))
+    L.gpu_build_kernels(len(data), N, N * N)
+    fgn, fg, dd, tg, ci = L.gpu_getp_fgn(), L.gpu_getp_fg(), L.gpu_getp_dd(), L.gpu_getp_tg(), L.gpu_getp_ci()
+    Js = []
+    ce, ge = C.c_int(0), C.c_int(0)
+    beta = 0.0
+    for uu in range(iters):
+        chi2 = L.gpu_get_chi2_curr(nuv, npow, nbis, data_alloc, alloc_uv)
+        S = L.gpu_get_entropy_curr(N)
+        crit = np.float32(chi2) - np.float32(alpha) * np.float32(S)
+        Js.append(float(crit))
+        L.gpu_compute_data_gradient_curr(nuv, npow, nbis, N)
+        L.gpu_compute_entropy_gradient_curr(N)
+        L.gpu_compute_criterion_gradient_curr(N, alpha)
+        if uu == 0:
+            beta = 0.0
+        else:
+            nn = L.gpu_get_scalprod(N, N, fgn, fgn)
+            no = L.gpu_get_scalprod(N, N, fgn, fg)
+            oo = L.gpu_get_scalprod(N, N, fg, fg)
+            beta = max((nn - no) / oo, 0.0)
+            if abs(no / nn) > 0.5:
+                beta = 0.0
+        L.gpu_compute_descent_dir(N, beta)
+        w1 = L.gpu_get_scalprod(N, N, dd, fgn)
+        s, s_old, Jinit, Jold, it = np.float32(1.0), np.float32(0.0), crit, crit, 1
+        while True:
+            L.gpu_update_tempimage(N, s, 1e-8, dd)
+            chi2 = L.gpu_get_chi2_temp(nuv, npow, nbis, data_alloc, alloc_uv)
+            S = L.gpu_get_entropy_temp(N)
+            J = np.float32(chi2) - np.float32(alpha) * np.float32(S)
+            if J > Jinit + np.float32(1e-4) * s * np.float32(w1) or (J >= Jold and it > 1):
+                sel = L.gpu_linesearch_zoom(nuv, npow, nbis, data_alloc, alloc_uv, N, s_old, s, Jold, w1, Jinit,
+                                            C.byref(ce), C.byref(ge), dd, tg, alpha)
+                break
+            L.gpu_compute_data_gradient_temp(nuv, npow, nbis, N)
+            L.gpu_compute_entropy_gradient_temp(N)
+            L.gpu_compute_criterion_gradient_temp(N, alpha)
+            w2 = L.gpu_get_scalprod(N, N, dd, tg)
+            if abs(w2) <= -0.1 * w1:
+                sel = s
+                break
+            if w2 >= 0:
+                sel = L.gpu_linesearch_zoom(nuv, npow, nbis, data_alloc, alloc_uv, N, s, s_old, J, w1, Jinit,
+                                            C.byref(ce), C.byref(ge), dd, tg, alpha)
+                break
+            s_old, Jold = s, J
+            s = np.float32(min(10.0 * s, 100.0))
+            it += 1
+        L.gpu_update_image(N, sel, 1e-8, dd)
+        L.gpu_backup_gradient(N * N, fgn, fg)
+    out = np.zeros(N * N, np.float32)
+    L.gpu_get_image(N * N, out.ctypes.data, ci)
+    L.gpu_cleanup()
+    return np.array(Js), out
+
+
+def test_reference_boundary_loop_matches_fp64_cg():
+    p = _problem("tiny", (21, 22, 23))
+    iters = 5
+    Js, _ = _ref_boundary_run(p, iters, p.alpha)
+    _, tr = O.reconstruct64(p, p.start_image(), iters)
+    assert np.allclose(Js[:3], tr["J"][:3], rtol=1e-4)
+    assert Js[-1] < Js[0]
+
+
+def test_ragged_sizes_and_no_triangles(rec):
+    # odd image width, nuv not a multiple of any tile, no triangles
+    rng = np.random.default_rng(3)
+    N, nuv = 33, 37
+    uv = np.zeros((nuv, 4), np.float32)
+    uv[:, 0] = rng.uniform(0, 4e7, nuv)
+    uv[:, 1] = rng.uniform(-4e7, 4e7, nuv)
+    data = rng.uniform(0, 1, nuv).astype(np.float32)
+    err = np.full(nuv, 20.0, np.float32)
+    p = g.Problem(N, 0.1, uv, nuv, 0, data, err, np.zeros(0, np.complex64), np.zeros((0, 3), np.int64),
+                  np.zeros((0, 3), np.int16), np.full(N * N, 1.0 / N ** 2, np.float32), 1e-3)
+    rec.set_problem(p)
+    img = _rand_image(p, 1)
+    rec.set_image(img)
+    chi2, _ = rec.criterion()
+    rec.gradient()
+    e = O.evaluate64(p, img)
+    assert abs(chi2 - e["chi2"]) / e["chi2"] <= 1e-5
+    assert _rel(rec.data_gradient(), e["data_grad"]) <= 1e-5
+
+
+def test_invalid_problem_is_rejected_without_touching_the_gpu(rec):
+    p = _problem("tiny")
+    bad = g.Problem(p.width, p.pixellation, p.uv, p.npow, p.nbis, p.data, p.data_err, p.phasor,
+                    p.uvpnt.copy(), p.sign, p.model, p.alpha)
+    bad.uvpnt[0, 1] = p.nuv + 5  # index out of range
+    with pytest.raises(g.GpairError):
+        rec.set_problem(bad)
+    rec.set_problem(p)  # context still usable
+    rec.set_image(p.start_image())
+    rec.criterion()
+
+
+def test_resumed_cg_equals_uninterrupted_run(rec):
+    p = _problem("tiny", (8, 9, 10))
+    rec.set_problem(p)
+    rec.set_image(p.start_image())
+    full = rec.cg(4, method=2)
+    img_full = rec.get_image()
+    rec.set_problem(p)  # fresh device state
+    rec.set_image(p.start_image())
+    rec.cg(2, method=2)
+    part = rec.cg(1, method=2, resume=True)
+    part = rec.cg(1, method=2, resume=True)
+    img_part = rec.get_image()
+    assert np.array_equal(img_full, img_part)  # deterministic reductions: bit-identical
+    assert part["J"] == full["J"]

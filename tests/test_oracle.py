@@ -1,0 +1,217 @@
+"""The CPU oracle pinned against the reference's own compiled code, plus known-answer tests.
+
+The FP64 restatement (oracle/fp64) must agree with the reference's own
+gpair1/trunk/cpu.c (compiled unchanged into oracle/_ref) to FP32 accuracy; the
+exact-float setup replicas must agree bit for bit with the product's C setup
+code and with the reference's set_model.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import gpair_b200 as g
+from gpair_b200 import synth
+from oracle import oracle as O
+
+pytestmark = pytest.mark.skipif(not O.ref_available() and not __import__("os").path.exists(
+    "/root/reference/gpair1/trunk/cpu.c"), reason="reference build unavailable")
+
+
+@pytest.fixture(scope="module")
+def small():
+    w, oi = synth.make_workload_data("small", 11, 12, 13)
+    return g.problem_from_oifits(oi, w.image_width, w.pixellation_mas, w.alpha)
+
+
+@pytest.fixture(scope="module")
+def tiny():
+    w, oi = synth.make_workload_data("tiny", 21, 22, 23)
+    return g.problem_from_oifits(oi, w.image_width, w.pixellation_mas, w.alpha)
+
+
+def _rand_image(p, seed):
+    rng = np.random.default_rng(seed)
+    return (p.start_image() * (1 + rng.uniform(0, 2, p.npix))).astype(np.float32)
+
+
+@pytest.mark.parametrize("which", ["tiny", "small"])
+def test_fp64_oracle_matches_reference_cpu(which, request):
+    p = request.getfixturevalue(which)
+    img = _rand_image(p, 5)
+    ev = O.RefEvaluator(p)
+    chi2_ref = ev.chi2(img)
+    e = O.evaluate64(p, img)
+    assert abs(chi2_ref - e["chi2"]) / e["chi2"] < 2e-5
+    # visibilities: FP32 reference vs FP64, relative to total flux (V is flux-normalised)
+    assert np.abs(ev.visi[:p.nuv] - e["visi"]).max() < 2e-5
+    assert np.allclose(ev.mock[:p.npow + 2 * p.nbis], e["mock"], rtol=1e-4, atol=1e-5)
+    gref = ev.data_gradient(img)
+    assert np.linalg.norm(gref - e["data_grad"]) / np.linalg.norm(e["data_grad"]) < 1e-4
+    assert abs(ev.entropy(img) - e["entropy"]) <= 1e-4 * abs(e["entropy"]) + 1e-6
+    eg_ref = ev.entropy_gradient(img)
+    eg64 = O.entropy_gradient64(img, p.model)
+    assert np.allclose(eg_ref, eg64, rtol=1e-5, atol=1e-6)
+
+
+def test_entropy_gradient_keeps_previous_value_where_undefined(small):
+    p = small
+    img = _rand_image(p, 3)
+    img[:10] = 0.0  # image <= 0: gradient keeps its previous value
+    prev = np.full(p.npix, 7.0, np.float32)
+    ev = O.RefEvaluator(p)
+    got = ev.entropy_gradient(img, prev)
+    assert np.all(got[:10] == 7.0)
+    assert np.allclose(got[10:], -np.log(img[10:].astype(np.float64) / p.model[10:]), rtol=1e-6)
+
+
+def test_init_data_replica_bit_exact(small):
+    w, oi = synth.make_workload_data("small", 11, 12, 13)
+    ix = g.index_oifits(oi)
+    bisamperr = ix.bisamperr.copy()
+    bisamperr[::7] = -1.0  # missing triple amplitudes -> extrapolated from V2
+    bisamperr[::11] = 5e3
+    ix.bisamperr = bisamperr
+    d1, e1, p1, n1 = g.init_data(ix, 1)
+    d2, e2, p2, n2 = O.init_data(ix.npow, ix.nbis, ix.pow, ix.powerr, ix.bisamp, bisamperr, ix.bisphs, ix.bisphserr,
+                                 ix.uvpnt, 1)
+    assert n1 == n2
+    assert np.array_equal(d1.view(np.uint32), d2.view(np.uint32))
+    assert np.array_equal(e1.view(np.uint32), e2.view(np.uint32))
+    assert np.array_equal(p1.view(np.uint32), p2.view(np.uint32))
+
+
+@pytest.mark.parametrize("modeltype,width,mw", [(0, 64, 0.0), (1, 64, 0.0), (2, 64, 1.0), (3, 256, 5.0),
+                                                (4, 64, 2.0), (2, 33, 0.7)])
+def test_set_model_bit_exact_with_reference(modeltype, width, mw):
+    a = g.set_model(width, 0.1, modeltype, mw, 1.0)
+    b = O.ref_set_model(width, 0.1, modeltype, mw, 1.0)
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+def test_dft_tables_bit_exact(small):
+    p = small
+    a = g.dft_tables(p.width, p.uv, p.pixellation)
+    b = O.dft_tables_f32(p.width, p.uv, p.pixellation)
+    assert np.array_equal(a[0].view(np.uint32), b[0].view(np.uint32))
+    assert np.array_equal(a[1].view(np.uint32), b[1].view(np.uint32))
+    tx, ty, gx, gy = g.dft_tables(p.width, p.uv, p.pixellation, transposed=True)
+    nuv, N = p.nuv, p.width
+    assert np.array_equal(gx[:nuv * N].reshape(N, nuv), tx.reshape(nuv, N).T)
+    assert np.all(gx[nuv * N:] == 0)
+
+
+# ------------------------------------------------------------ known answers
+
+def _single_problem(width=16, nuv=7, seed=0):
+    rng = np.random.default_rng(seed)
+    uv = np.zeros((nuv, 4), np.float32)
+    uv[:, 0] = rng.uniform(0, 3e7, nuv)
+    uv[:, 1] = rng.uniform(-3e7, 3e7, nuv)
+    uv[:, 3] = 1.6e-6
+    tri = np.array([[0, 1, 2], [1, 2, 3], [3, 4, 5], [6, 0, 5]], np.int64)
+    sign = np.array([[1, -1, 1], [1, 1, -1], [-1, -1, 1], [1, 1, 1]], np.int16)
+    nb = len(tri)
+    data = np.abs(rng.normal(0.5, 0.2, nuv + 2 * nb)).astype(np.float32)
+    data[nuv + 1::2] = 0
+    err = rng.uniform(5, 20, nuv + 2 * nb).astype(np.float32)
+    ph = np.exp(-1j * rng.uniform(-np.pi, np.pi, nb)).astype(np.complex64)
+    model = np.full(width * width, 1.0 / (width * width), np.float32)
+    return g.Problem(width, 0.2, uv, nuv, nb, data, err, ph, tri, sign, model, 1e-2)
+
+
+def test_kat_point_source_at_origin_has_unit_visibility():
+    p = _single_problem()
+    img = np.zeros(p.npix)
+    img[0] = 3.0
+    e = O.evaluate64(p, img, want_grad=False)
+    assert np.allclose(e["visi"], 1.0, atol=1e-14)
+    assert np.allclose(e["mock"][:p.npow], 1.0, atol=1e-14)
+
+
+def test_kat_shifted_delta_is_a_phase_ramp_with_reference_signs():
+    p = _single_problem()
+    x0, y0 = 3, 5
+    img = np.zeros(p.npix)
+    img[x0 + y0 * p.width] = 1.0
+    e = O.evaluate64(p, img, want_grad=False)
+    rp = (math.pi / 180) / 3.6e6 * p.pixellation
+    u, v = p.uv[:, 0].astype(np.float64), p.uv[:, 1].astype(np.float64)
+    expect = np.exp(2j * np.pi * rp * (u * x0 - v * y0))
+    assert np.allclose(e["visi"], expect, atol=1e-12)
+
+
+def _closed_triangle_problem(width, ntri, seed=0):
+    """Triangles whose three uv points close (uv3 = -(uv1 + uv2)), folded to u >= 0 with signs."""
+    rng = np.random.default_rng(seed)
+    pts, tri, sign = [], [], []
+    for t in range(ntri):
+        a = rng.uniform(-3e7, 3e7, 2)
+        b = rng.uniform(-3e7, 3e7, 2)
+        row, srow = [], []
+        for q in (a, b, -(a + b)):
+            s = 1
+            if q[0] < 0:
+                q, s = -q, -1
+            row.append(len(pts))
+            srow.append(s)
+            pts.append(q)
+        tri.append(row)
+        sign.append(srow)
+    nuv = len(pts)
+    uv = np.zeros((nuv, 4), np.float32)
+    uv[:, :2] = np.array(pts)
+    uv[:, 3] = 1.6e-6
+    nd = nuv + 2 * ntri
+    p = g.Problem(width, 0.2, uv, nuv, ntri, np.ones(nd, np.float32), np.ones(nd, np.float32),
+                  np.ones(ntri, np.complex64), np.array(tri, np.int64), np.array(sign, np.int16),
+                  np.full(width * width, 1.0 / width ** 2, np.float32))
+    return p
+
+
+def test_kat_closure_phase_of_point_symmetric_image_is_zero_or_pi():
+    p = _closed_triangle_problem(17, 6)
+    img = np.random.default_rng(4).uniform(0.1, 1, (17, 17))
+    img = img + img[::-1, ::-1]  # symmetric about the centre pixel
+    p.phasor[:] = 1.0
+    e = O.evaluate64(p, img.ravel(), want_grad=False)
+    t3 = e["mock"][p.npow::2] + 1j * e["mock"][p.npow + 1::2]
+    # visibilities of a centro-symmetric image = real * phase ramp of the centre; closure removes the ramp
+    # float32 uv storage leaves a closure error of ~1e-7 relative in u, v
+    assert np.allclose(np.sin(np.angle(t3)), 0, atol=1e-6)
+
+
+def test_kat_gradient_matches_finite_differences():
+    p = _single_problem(width=8)
+    rng = np.random.default_rng(9)
+    img = rng.uniform(0.2, 1.0, p.npix)
+    e = O.evaluate64(p, img)
+    h = 1e-6
+    for pix in (0, 9, 37, 63):
+        ip, im = img.copy(), img.copy()
+        ip[pix] += h
+        im[pix] -= h
+        fd = (O.evaluate64(p, ip, False)["chi2"] - O.evaluate64(p, im, False)["chi2"]) / (2 * h)
+        assert abs(fd - e["data_grad"][pix]) <= 1e-6 * max(1.0, abs(fd))
+
+
+def test_kat_entropy_gradient_is_minus_log_ratio():
+    rng = np.random.default_rng(2)
+    img = rng.uniform(0.01, 2, 100)
+    m = rng.uniform(0.01, 2, 100).astype(np.float32)
+    gr = O.entropy_gradient64(img, m)
+    assert np.allclose(gr, -np.log(img / m.astype(np.float64)), rtol=0, atol=1e-14)
+
+
+def test_fp64_cg_decreases_objective_and_matches_float_reference_cg(tiny):
+    p = tiny
+    img0 = p.start_image()
+    _, tr64 = O.reconstruct64(p, img0, 12)
+    assert tr64["J"][-1] < tr64["J"][0]
+    assert np.all(np.diff(tr64["J"]) <= 1e-9 * np.abs(tr64["J"][:-1]))
+    ev = O.RefEvaluator(p)
+    _, tr32 = ev.cg(img0, 12)
+    # the float CG over the reference's cpu.c follows the same decisions early on
+    assert np.allclose(tr32["J"][:3], tr64["J"][:3], rtol=1e-4)
+    assert np.allclose(tr32["step"][:3], tr64["step"][:3], rtol=1e-3)
+    assert tr32["J"][-1] < tr32["J"][0]
