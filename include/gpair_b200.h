@@ -303,6 +303,29 @@ int gpair_time_stages(gpair_ctx *ctx, int reps, double *stage_ms, int max_stages
 int gpair_set_stage_timing(gpair_ctx *ctx, int on);
 int gpair_last_run_stage_ms(gpair_ctx *ctx, double *stage_ms, int *stage_launches, int max_stages);
 
+/* ---- allocation-free data stage ----
+ * No counterpart in the reference. For callers that cannot allocate device
+ * memory: programs whose own allocator owns the device heap, and latency-
+ * critical loops where a cudaMalloc could serialise the device. It computes
+ * the V2 / T3 mock data and chi2 (FP64 sum) from visibilities, like
+ * gpu_vis2data + gpu_data2chi2. It allocates nothing: every pointer is a
+ * caller-owned DEVICE buffer in the reference's layouts (visi float2[nuv],
+ * data/data_err/mock float[npow + 2*nbis], phasor float2[nbis], uvpnt
+ * long4[nbis], sign short4[nbis], chi2 one double). The reduction scratch is
+ * a fixed 64 KiB device array inside the library, held by every GPU that
+ * loads it until the process exits. Limits: npow + nbis <= 2,097,152,
+ * npow <= nuv; larger sizes return GPAIR_ERR_INVALID without launching.
+ * The first call on a device looks up the scratch address for that device
+ * (with it current); make that first call before any stream capture. The call
+ * is asynchronous on `stream` (a cudaStream_t, NULL = default stream); results
+ * are valid once the stream has reached it. All calls share the one scratch
+ * array, so calls that overlap on the GPU (other streams, other host threads)
+ * race and must be serialised by the caller. An out-of-range triangle
+ * reference is not read; the call then writes chi2 = NaN. */
+int gpair_vis2data_chi2_noalloc(const gpair_float2 *visi, int nuv, int npow, int nbis, const float *data,
+                                const float *data_err, const gpair_float2 *phasor, const gpair_long4 *uvpnt,
+                                const gpair_short4 *sign, float *mock, double *chi2, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
