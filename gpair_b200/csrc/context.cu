@@ -185,7 +185,12 @@ int gp_set_problem_core(gpair_ctx *c, int N, float pix, int nuv, const gpair_uv 
     c->ndata = npow + 2 * nbis;
     size_t nd = c->ndata ? c->ndata : 1, nt = nbis ? nbis : 1, nk = nuv ? nuv : 1;
     c->mt = gp_cdiv(N, 64);
-    c->splits = gp_default_splits(N, nuv ? nuv : 1);
+    c->splits_simt = gp_default_splits(N, nuv ? nuv : 1);
+    c->splits = c->splits_simt;
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
+    int max_splits = gp_tc_splits(N, nuv ? nuv : 1, nsm, nullptr);
+    if (max_splits < c->splits_simt) max_splits = c->splits_simt;
     GP_CUDA(c, cudaMalloc(&c->data, nd * sizeof(float)));
     GP_CUDA(c, cudaMalloc(&c->data_err, nd * sizeof(float)));
     GP_CUDA(c, cudaMalloc(&c->mock, nd * sizeof(float)));
@@ -199,7 +204,7 @@ int gp_set_problem_core(gpair_ctx *c, int N, float pix, int nuv, const gpair_uv 
     GP_CUDA(c, cudaMalloc(&c->visi, nk * sizeof(float2)));
     GP_CUDA(c, cudaMalloc(&c->cw, nk * sizeof(float2)));
     GP_CUDA(c, cudaMalloc(&c->trib, 3 * nt * sizeof(float2)));
-    GP_CUDA(c, cudaMalloc(&c->gpart, (size_t)c->splits * c->npix * sizeof(float)));
+    GP_CUDA(c, cudaMalloc(&c->gpart, (size_t)max_splits * c->npix * sizeof(float)));
     GP_CUDA(c, cudaMemsetAsync(c->mock, 0, nd * sizeof(float), c->stream));
     GP_CUDA(c, cudaMemsetAsync(c->visd, 0, nk * sizeof(double2), c->stream));
     GP_CUDA(c, cudaMemsetAsync(c->visi, 0, nk * sizeof(float2), c->stream));
@@ -231,7 +236,8 @@ int gp_set_problem_core(gpair_ctx *c, int N, float pix, int nuv, const gpair_uv 
     rc = gp_build_incidence(c, uvpnt);
     if (rc) return rc;
     c->have_problem = 1;
-    if (c->precision != GPAIR_PREC_FP32) {
+    if (c->precision != GPAIR_PREC_FP32 && uv) {
+        // with reference tables (uv == NULL) the operands are built lazily, once the tables are on the device
         rc = gp_tc_prepare(c);
         if (rc) return rc;
     }
@@ -291,6 +297,15 @@ int gp_sync_scalars(gpair_ctx *c)
 {
     GP_CUDA(c, cudaMemcpyAsync(c->sc_host, c->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, c->stream));
     GP_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (c->sc_host->tc_err) {
+        // a tensor-core kernel gave up a bounded wait; report it once and clear it
+        snprintf(c->last_error, sizeof(c->last_error), "tensor-core kernel wait timed out (code 0x%x)",
+                 c->sc_host->tc_err);
+        unsigned int zero = 0;
+        cudaMemcpyAsync(&c->sc->tc_err, &zero, sizeof(zero), cudaMemcpyHostToDevice, c->stream);
+        cudaStreamSynchronize(c->stream);
+        return GPAIR_ERR_TIMEOUT;
+    }
     return GPAIR_OK;
 }
 
@@ -400,8 +415,7 @@ extern "C" int gpair_gradient(gpair_ctx *c, int which, float alpha)
     GP_CUDA(c, cudaSetDevice(c->device));
     int rc = gp_eval_gradient(c, which, alpha);
     if (rc) return rc;
-    GP_CUDA(c, cudaStreamSynchronize(c->stream));
-    return GPAIR_OK;
+    return gp_sync_scalars(c);
 }
 
 extern "C" int gpair_get_visibilities(gpair_ctx *c, gpair_float2 *visi)
@@ -561,8 +575,6 @@ extern "C" int gpair_last_run_stats(gpair_ctx *c, double *ms, double *flops, int
     if (launches) *launches = (int)c->last_launches;
     return GPAIR_OK;
 }
-
-double gp_adjoint_scale(gpair_ctx *c);
 
 extern "C" int gpair_time_stages(gpair_ctx *c, int reps, double *ms, int max_stages)
 {

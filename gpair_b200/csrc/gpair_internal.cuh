@@ -62,14 +62,18 @@ struct CgState {
 
 struct DevScalars {
     double flux, invflux, entropy, chi2;
+    double imax;          // max |image| of the last prepared image
+    float fwd_inv_scale;  // tensor forward: 1 / (image scale * twiddle scale)
     double adj_c;      // C = Re sum_k c_k V_k
     double cmax;       // max |c_k| (scaling of split operands)
+    double gscale;     // factor applied to the summed adjoint partials (1, or 1/operand scales)
     double grad_dots[2][4];  // [CURR/TEMP]: g.g, g.g_old, g.d, d.g_old
     double dir_dot;    // d.g_new after the descent update
     double dot;        // generic scalar product
     float flux_f, invflux_f, chi2_f, entropy_f, dot_f;
     unsigned int counter[RED_NSLOTS];
     unsigned int nonfinite;  // set when a NaN/Inf reaches a reduction
+    unsigned int tc_err;     // tensor-core kernels: bounded wait gave up (bit = which wait)
     CgState cg;
 };
 
@@ -90,7 +94,8 @@ struct gpair_ctx {
     float pix;
     int have_problem, have_image;
     int mt;           // number of row tiles of the forward DFT
-    int splits;       // split-K factor of the adjoint
+    int splits;       // split-K factor of the last adjoint (number of partial images)
+    int splits_simt;  // split-K factor of the CUDA-core adjoint
 
     // buffers
     float *image, *image_temp, *model;
@@ -195,5 +200,6 @@ enum { CTRL_BEGIN = 0, CTRL_AFTER_DIR = 1, CTRL_AFTER_CRIT = 2, CTRL_AFTER_GRAD 
 // tensor-core path (umma_dft.cu); return GPAIR_ERR_STATE when unavailable
 int gp_tc_prepare(gpair_ctx *c);
 int gp_tc_forward(gpair_ctx *c, int which);
+int gp_tc_splits(int N, int nuv, int nsm, int *kb_per_out);
 int gp_tc_adjoint(gpair_ctx *c, int which);
 void gp_tc_free(gpair_ctx *c);

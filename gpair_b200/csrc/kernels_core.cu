@@ -170,6 +170,7 @@ __global__ void __launch_bounds__(GP_THREADS) k_prep(const float *__restrict__ s
     __shared__ double smem[2 * 32];
     double s = step_from_state ? sc->cg.s : step;
     double acc[2] = {0.0, 0.0};
+    double mx = 0.0;
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
         float I = src[p];
         if (trial) {
@@ -181,23 +182,33 @@ __global__ void __launch_bounds__(GP_THREADS) k_prep(const float *__restrict__ s
         double Id = I, m = model[p];
         acc[0] += Id;
         acc[1] += (Id > 0.0 && m > 0.0) ? (Id - m - Id * log(Id / m)) : -m;
+        mx = fmax(mx, fabs(Id));
     }
     block_sum<2>(acc, smem);
+    mx = block_max(mx, smem);
     if (threadIdx.x == 0) {
-        partials[2 * blockIdx.x] = acc[0];
-        partials[2 * blockIdx.x + 1] = acc[1];
+        partials[3 * blockIdx.x] = acc[0];
+        partials[3 * blockIdx.x + 1] = acc[1];
+        partials[3 * blockIdx.x + 2] = mx;
     }
     if (last_block(&sc->counter[RED_PREP])) {
-        double out[2];
-        finish_sum<2>(partials, gridDim.x, out, smem);
+        double v[2] = {0.0, 0.0}, m = 0.0;
+        for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
+            v[0] += __ldcg(&partials[3 * b]);
+            v[1] += __ldcg(&partials[3 * b + 1]);
+            m = fmax(m, __ldcg(&partials[3 * b + 2]));
+        }
+        block_sum<2>(v, smem);
+        m = block_max(m, smem);
         if (threadIdx.x == 0) {
-            sc->flux = out[0];
-            sc->invflux = 1.0 / out[0];
-            sc->entropy = out[1];
-            sc->flux_f = (float)out[0];
-            sc->invflux_f = (float)(1.0 / out[0]);
-            sc->entropy_f = (float)out[1];
-            if (!isfinite(out[0]) || !isfinite(out[1])) sc->nonfinite |= 1u;
+            sc->flux = v[0];
+            sc->invflux = 1.0 / v[0];
+            sc->entropy = v[1];
+            sc->imax = m;
+            sc->flux_f = (float)v[0];
+            sc->invflux_f = (float)(1.0 / v[0]);
+            sc->entropy_f = (float)v[1];
+            if (!isfinite(v[0]) || !isfinite(v[1])) sc->nonfinite |= 1u;
             sc->counter[RED_PREP] = 0;
         }
     }
@@ -456,6 +467,7 @@ __global__ void __launch_bounds__(GP_THREADS) k_adj_weights(int nuv, const int *
         if (threadIdx.x == 0) {
             sc->adj_c = sv[0];
             sc->cmax = m;
+            sc->gscale = 1.0;  // the tensor path's operand builder overrides this
             sc->counter[RED_ADJ] = 0;
         }
     }
@@ -557,11 +569,12 @@ int gp_adjoint(gpair_ctx *c, int which)
 int gp_adjoint_contraction(gpair_ctx *c, int which)
 {
     if (c->precision != GPAIR_PREC_FP32) return gp_tc_adjoint(c, which);
-    int S = c->splits;
+    int S = c->splits_simt;
     int kchunk = gp_cdiv(c->nuv, S);
     kchunk = gp_cdiv(kchunk, AB_K) * AB_K;
     S = gp_cdiv(c->nuv, kchunk);
     if (S < 1) S = 1;
+    c->splits_simt = S;
     c->splits = S;
     dim3 grid(gp_cdiv(c->N, AB_N), gp_cdiv(c->N, AB_M), S);
     if (c->nuv == 0) {
@@ -579,7 +592,7 @@ int gp_default_splits(int N, int nuv) { return adj_splits(N, nuv); }
 // ------------------------------------------------------ gradient finalize
 
 __global__ void __launch_bounds__(GP_THREADS) k_grad_finalize(const float *__restrict__ gpart, int splits,
-                                                              int npix, double gscale, int mode,
+                                                              int npix, int mode,
                                                               const float *__restrict__ img,
                                                               const float *__restrict__ model, float alpha,
                                                               float *__restrict__ data_grad,
@@ -591,11 +604,20 @@ __global__ void __launch_bounds__(GP_THREADS) k_grad_finalize(const float *__res
                                                               DevScalars *__restrict__ sc)
 {
     __shared__ double smem[4 * 32];
-    const double C = sc->adj_c;
+    const double C = sc->adj_c, gscale = sc->gscale;
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
         double g = 0.0;
-        for (int s = 0; s < splits; s++) g += gpart[(size_t)s * npix + p];
+        int s = 0;
+        for (; s + 4 <= splits; s += 4) {
+            float a0 = gpart[(size_t)s * npix + p], a1 = gpart[(size_t)(s + 1) * npix + p];
+            float a2 = gpart[(size_t)(s + 2) * npix + p], a3 = gpart[(size_t)(s + 3) * npix + p];
+            g += a0;
+            g += a1;
+            g += a2;
+            g += a3;
+        }
+        for (; s < splits; s++) g += gpart[(size_t)s * npix + p];
         float gd = (float)(g * gscale - C);
         data_grad[p] = gd;
         if (mode == GRAD_FUSED) {
@@ -627,14 +649,13 @@ __global__ void __launch_bounds__(GP_THREADS) k_grad_finalize(const float *__res
     }
 }
 
-double gp_adjoint_scale(gpair_ctx *c);
-
 int gp_grad_finalize(gpair_ctx *c, int which, int mode, float alpha)
 {
     const float *img = (which == GPAIR_IMG_TEMP) ? c->image_temp : c->image;
     float *out = (which == GPAIR_IMG_TEMP) ? c->grad_temp : c->full_grad_new;
-    int g = red_grid(c->npix);
-    k_grad_finalize<<<g, GP_THREADS, 0, c->stream>>>(c->gpart, c->splits, c->npix, gp_adjoint_scale(c), mode, img,
+    int g = gp_cdiv(c->npix, GP_THREADS);  // one pixel per thread: the split sum is latency-bound
+    if (g > GP_MAX_PARTIALS) g = GP_MAX_PARTIALS;
+    k_grad_finalize<<<g, GP_THREADS, 0, c->stream>>>(c->gpart, c->splits, c->npix, mode, img,
                                                      c->model, alpha, c->data_grad, c->entropy_grad, out,
                                                      c->full_grad, c->descent_dir, which == GPAIR_IMG_TEMP ? 1 : 0,
                                                      slot_partials(c, RED_GRAD), c->sc);
@@ -875,6 +896,11 @@ __global__ void k_cg_ctrl(DevScalars *__restrict__ sc, int what)
         s.action = CG_EVAL_CRIT;
         break;
     case CTRL_AFTER_CRIT: {
+        if (sc->tc_err) {  // a tensor-core kernel gave up a bounded wait: stop the run
+            s.sel = 0.0;
+            s.action = CG_DONE;
+            break;
+        }
         double Jt = sc->chi2 - s.alpha * sc->entropy;
         s.Jt = Jt;
         s.criterion_evals++;
@@ -904,6 +930,11 @@ __global__ void k_cg_ctrl(DevScalars *__restrict__ sc, int what)
         break;
     }
     case CTRL_AFTER_GRAD: {
+        if (sc->tc_err) {
+            s.sel = 0.0;
+            s.action = CG_DONE;
+            break;
+        }
         const double w2 = sc->grad_dots[1][2];  // d . g_trial
         s.grad_evals++;
         if (s.phase == CG_PH_BRACKET) {

@@ -1,15 +1,623 @@
-// umma_dft.cu -- tcgen05 (5th-generation tensor core) DFT and adjoint
-// contractions. Placeholder until the tensor path lands: every entry point
-// reports GPAIR_ERR_STATE so that a request for a tensor precision fails
-// loudly instead of silently running the CUDA-core path.
+// umma_dft.cu -- forward DFT and adjoint contraction on the 5th-generation
+// tensor cores (tcgen05, TMEM accumulators, TMA operand staging).
+//
+// Precision (GPAIR_PREC_SPLIT16): every operand x is stored as a pair of f16
+// values hi = f16(x), lo = f16(x - hi) after a power-of-two scaling that puts
+// the operand near the top of the f16 range; a product is formed as
+// A_hi B_hi + A_hi B_lo + A_lo B_hi with FP32 accumulation (the lo*lo term is
+// below 2^-22 of the result). Scales are exact powers of two and are removed
+// in the epilogues.
+//
+// Both contractions put the twiddle-side table in the M = 128 operand (TMEM
+// lanes) and the image-side operand in the N = 256 operand (TMEM columns).
+// Forward DFT (kernel_visi.cl / cpu.c:449-475):
+//   T[n][y] = sum_x Fx16[n][x] I[y][x],  row n = 2k+c holds (Re, Im) Fx[k][x]
+//   epilogue: the thread of row n sums over its 256 columns against one
+//   contiguous row of Fy (prefetched a chunk ahead); the Re/Im row pair is
+//   combined with one shuffle: Vpart[ytile][k] = sum_y (T[2k][y] + i T[2k+1][y]) Fy[k][y]
+// Adjoint (kernel_grad_pow.cl + kernel_grad_bis.cl / cpu.c:279-369):
+//   G[y][x] = sum_k' FxT[x][k'] W[y][k'],  W[y][2k] = Re(c_k Fy[k][y]),
+//   W[y][2k+1] = -Im(c_k Fy[k][y]),  FxT[x][2k+c] = (Re, Im) Fx[k][x]
+//   the thread of image column x stores G[y][x] for its 256 rows (consecutive
+//   lanes write consecutive x); split over k' into S partial images that
+//   k_grad_finalize sums in a fixed order
+//
+// One persistent CTA per SM, 192 threads: warp 0 issues TMA loads (2-stage
+// ring of 96 KB), warp 1 owns TMEM (512 columns = two 128x256 FP32
+// accumulators) and one of its threads issues tcgen05.mma; warps 2-5 drain
+// TMEM. All waits are bounded; a timeout sets an error code, the roles stop,
+// TMEM is released, and the host reports GPAIR_ERR_TIMEOUT.
+#include <cuda.h>
+#include <cuda_fp16.h>
+#include <cudaTypedefs.h>
+#include <stdlib.h>
+#include <string.h>
+
 #include "gpair_internal.cuh"
+#include "umma.cuh"
+
+#define TC_BM 128
+#define TC_BN 256
+#define TC_BK 64
+#define TC_STAGES 2
+#define TC_THREADS 192
+#define TC_TW_LOG2 10  // twiddle operands are scaled by 2^10
+#define TC_A_BYTES (TC_BM * TC_BK * 2)
+#define TC_B_BYTES (TC_BN * TC_BK * 2)
+#define TC_STAGE_BYTES (2 * TC_A_BYTES + 2 * TC_B_BYTES)
+#define TC_TMEM_COLS 512
+#define TC_SMEM_BYTES (1024 + TC_STAGES * TC_STAGE_BYTES + 256)
+#define TC_WAIT_BUDGET 4000000000LL  // clock cycles (~2 s) per wait
+
+enum { EPI_FWD = 0, EPI_STORE = 1 };
+
+struct TcArgs {
+    int m_tiles, n_tiles, kb_total, kb_per_split, units;
+    // forward epilogue: Fy[k][16 j] anchors, per-uv rotation e^{-2 pi i s v_k}
+    const float2 *fya, *fyr;
+    int nanc;
+    int N, nuv;
+    const DevScalars *sc;
+    float2 *vpart;
+    // store epilogue
+    float *gpart;
+    int out_ld, out_rows, out_cols;
+    unsigned int *err;
+};
+
+struct TcState {
+    // A side (M = 128 rows): forward twiddles [rows_pad][Kx_pad], adjoint twiddles [xrows_pad][K2_pad]
+    // B side (N = 256 rows): image [M_pad][Kx_pad], adjoint weights [M_pad][K2_pad]
+    int Kx_pad, M_pad, rows_pad, K2_pad, xrows_pad;
+    int splits, kb_per;
+    __half *img_hi, *img_lo, *fx_hi, *fx_lo, *fxt_hi, *fxt_lo, *w_hi, *w_lo;
+    float2 *fya, *fyr;
+    int nanc;
+    CUtensorMap m_img_hi, m_img_lo, m_fx_hi, m_fx_lo, m_w_hi, m_w_lo, m_fxt_hi, m_fxt_lo;
+    int nsm;
+};
+
+static inline int round_up(long long a, long long b) { return (int)(((a + b - 1) / b) * b); }
+
+// ------------------------------------------------------------------ GEMM
+
+__device__ __forceinline__ void tc_fail(unsigned int *err, volatile int *abort_flag, unsigned int code)
+{
+    atomicOr(err, code);
+    *abort_flag = 1;
+}
+
+template <int EPI>
+__device__ __forceinline__ void tc_decode(const TcArgs &a, int u, int &m, int &n, int &kb0, int &kb1, int &split)
+{
+    n = u % a.n_tiles;
+    int rest = u / a.n_tiles;
+    if (EPI == EPI_FWD) {
+        m = rest;
+        split = 0;
+        kb0 = 0;
+        kb1 = a.kb_total;
+    } else {
+        m = rest % a.m_tiles;
+        split = rest / a.m_tiles;
+        kb0 = split * a.kb_per_split;
+        kb1 = min(a.kb_total, kb0 + a.kb_per_split);
+    }
+}
+
+template <int EPI>
+__global__ void __launch_bounds__(TC_THREADS, 1)
+    k_tc_gemm(const __grid_constant__ CUtensorMap tA_hi, const __grid_constant__ CUtensorMap tA_lo,
+              const __grid_constant__ CUtensorMap tB_hi, const __grid_constant__ CUtensorMap tB_lo, const TcArgs a)
+{
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    unsigned char *stages = smem;
+    uint64_t *full = (uint64_t *)(smem + TC_STAGES * TC_STAGE_BYTES);
+    uint64_t *empty = full + TC_STAGES;
+    uint64_t *tfull = empty + TC_STAGES;
+    uint64_t *tempty = tfull + 2;
+    uint64_t *done_bar = tempty + 2;
+    uint32_t *tmem_slot = (uint32_t *)(done_bar + 1);
+    volatile int *abort_flag = (volatile int *)(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < TC_STAGES; s++) {
+            umma::mbar_init(&full[s], 1);
+            umma::mbar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; b++) {
+            umma::mbar_init(&tfull[b], 1);
+            umma::mbar_init(&tempty[b], 128);
+        }
+        umma::mbar_init(done_bar, 1);
+        *abort_flag = 0;
+        umma::fence_barrier_init();
+    }
+    if (warp == 1) {
+        umma::tmem_alloc(tmem_slot, TC_TMEM_COLS);
+        umma::tmem_relinquish();
+    }
+    umma::tc_fence_before();
+    __syncthreads();
+    umma::tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // ------------------------------------------------ TMA producer
+            umma::tma_prefetch(&tA_hi);
+            umma::tma_prefetch(&tA_lo);
+            umma::tma_prefetch(&tB_hi);
+            umma::tma_prefetch(&tB_lo);
+            int it = 0;
+            for (int u = blockIdx.x; u < a.units && !*abort_flag; u += gridDim.x) {
+                int m, n, kb0, kb1, split;
+                tc_decode<EPI>(a, u, m, n, kb0, kb1, split);
+                for (int kb = kb0; kb < kb1; kb++, it++) {
+                    const int s = it % TC_STAGES;
+                    const uint32_t ph = (uint32_t)(it / TC_STAGES) & 1u;
+                    if (!umma::mbar_wait(&empty[s], ph ^ 1u, TC_WAIT_BUDGET)) {
+                        tc_fail(a.err, abort_flag, 1u);
+                        break;
+                    }
+                    unsigned char *st = stages + s * TC_STAGE_BYTES;
+                    umma::mbar_arrive_expect_tx(&full[s], TC_STAGE_BYTES);
+                    umma::tma_load_2d(st, &tA_hi, &full[s], kb * TC_BK, m * TC_BM);
+                    umma::tma_load_2d(st + TC_A_BYTES, &tA_lo, &full[s], kb * TC_BK, m * TC_BM);
+                    umma::tma_load_2d(st + 2 * TC_A_BYTES, &tB_hi, &full[s], kb * TC_BK, n * TC_BN);
+                    umma::tma_load_2d(st + 2 * TC_A_BYTES + TC_B_BYTES, &tB_lo, &full[s], kb * TC_BK, n * TC_BN);
+                }
+            }
+            // no copy may be in flight when the CTA retires: wait for the last
+            // load issued into each stage (bounded)
+            for (int j = 1; j <= TC_STAGES && it - j >= 0; j++) {
+                const int i = it - j, s = i % TC_STAGES;
+                if (!umma::mbar_wait(&full[s], (uint32_t)(i / TC_STAGES) & 1u, TC_WAIT_BUDGET))
+                    tc_fail(a.err, abort_flag, 16u);
+            }
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // ------------------------------------------------ MMA issuer
+            const uint32_t idesc = umma::idesc_f16(TC_BM, TC_BN, 0);
+            int it = 0, t = 0;
+            bool ok = true;
+            for (int u = blockIdx.x; u < a.units && ok && !*abort_flag; u += gridDim.x, t++) {
+                int m, n, kb0, kb1, split;
+                tc_decode<EPI>(a, u, m, n, kb0, kb1, split);
+                const int b = t & 1;
+                if (!umma::mbar_wait(&tempty[b], ((uint32_t)(t >> 1) & 1u) ^ 1u, TC_WAIT_BUDGET)) {
+                    tc_fail(a.err, abort_flag, 2u);
+                    break;
+                }
+                umma::tc_fence_after();
+                const uint32_t d = tmem_base + (uint32_t)(b * TC_BN);
+                for (int kb = kb0; kb < kb1; kb++, it++) {
+                    const int s = it % TC_STAGES;
+                    if (!umma::mbar_wait(&full[s], (uint32_t)(it / TC_STAGES) & 1u, TC_WAIT_BUDGET)) {
+                        tc_fail(a.err, abort_flag, 4u);
+                        ok = false;
+                        break;
+                    }
+                    umma::tc_fence_after();
+                    unsigned char *st = stages + s * TC_STAGE_BYTES;
+                    const uint64_t dah = umma::smem_desc_k_sw128(st);
+                    const uint64_t dal = umma::smem_desc_k_sw128(st + TC_A_BYTES);
+                    const uint64_t dbh = umma::smem_desc_k_sw128(st + 2 * TC_A_BYTES);
+                    const uint64_t dbl = umma::smem_desc_k_sw128(st + 2 * TC_A_BYTES + TC_B_BYTES);
+#pragma unroll
+                    for (int kk = 0; kk < TC_BK / 16; kk++) {
+                        const uint64_t off = (uint64_t)(kk * 32) >> 4;  // 16 f16 = 32 B along K
+                        umma::mma_f16_ss(d, dah + off, dbh + off, idesc, (kb > kb0 || kk > 0) ? 1u : 0u);
+                        umma::mma_f16_ss(d, dah + off, dbl + off, idesc, 1u);
+                        umma::mma_f16_ss(d, dal + off, dbh + off, idesc, 1u);
+                    }
+                    umma::mma_commit(&empty[s]);  // stage reusable once these MMAs finish
+                }
+                if (!ok) break;
+                umma::mma_commit(&tfull[b]);  // accumulator ready for the epilogue
+            }
+            // every MMA of this CTA has completed before TMEM is released
+            umma::mma_commit(done_bar);
+            if (!umma::mbar_wait(done_bar, 0u, TC_WAIT_BUDGET)) tc_fail(a.err, abort_flag, 32u);
+        }
+        __syncwarp();
+    } else {
+        // ---------------------------------------------------- epilogue
+        const int q = warp & 3;  // TMEM lane quarter this warp may access
+        int t = 0;
+        for (int u = blockIdx.x; u < a.units; u += gridDim.x, t++) {
+            int m, n, kb0, kb1, split;
+            tc_decode<EPI>(a, u, m, n, kb0, kb1, split);
+            const int b = t & 1;
+            const int arow = m * TC_BM + q * 32 + lane;  // row of the twiddle-side operand
+            const int y0 = n * TC_BN;                   // first image row of the columns
+            const uint32_t taddr = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * TC_BN);
+            if (EPI == EPI_FWD) {
+                // Fy[k][y] along this thread's 256 columns: an FP64-accurate anchor every
+                // 16 rows, rotated by r_k = e^{-2 pi i s v_k} within the chunk (<= 15 steps)
+                const int k = arow >> 1;
+                const bool vk = k < a.nuv;
+                const float2 rot = vk ? __ldg(&a.fyr[k]) : make_float2(0.f, 0.f);
+                const float2 *anc = a.fya + (size_t)(vk ? k : 0) * a.nanc;
+                float2 an[TC_BN / 16];
+#pragma unroll
+                for (int c = 0; c < TC_BN / 16; c++) {
+                    const int j = (y0 >> 4) + c;
+                    an[c] = (vk && j < a.nanc) ? __ldg(&anc[j]) : make_float2(0.f, 0.f);
+                }
+                if (!umma::mbar_wait(&tfull[b], (uint32_t)(t >> 1) & 1u, TC_WAIT_BUDGET)) {
+                    tc_fail(a.err, abort_flag, 8u);
+                    break;
+                }
+                umma::tc_fence_after();
+                float sre = 0.f, sim = 0.f;
+#pragma unroll
+                for (int c = 0; c < TC_BN / 16; c++) {
+                    uint32_t r[16];
+                    umma::tmem_ld16(taddr + (uint32_t)(c * 16), r);
+                    umma::tmem_ld_wait();
+                    float2 w = an[c];
+#pragma unroll
+                    for (int j = 0; j < 16; j++) {
+                        const float tv = __uint_as_float(r[j]);
+                        sre = fmaf(tv, w.x, sre);
+                        sim = fmaf(tv, w.y, sim);
+                        const float wx = w.x * rot.x - w.y * rot.y;
+                        w.y = w.x * rot.y + w.y * rot.x;
+                        w.x = wx;
+                    }
+                }
+                umma::tc_fence_before();
+                umma::mbar_arrive(&tempty[b]);
+                const float fs = a.sc->fwd_inv_scale;
+                sre *= fs;
+                sim *= fs;
+                // even row: (sum T_re F_re, sum T_re F_im); odd row: (sum T_im F_re, sum T_im F_im)
+                const float ore = __shfl_xor_sync(0xffffffffu, sre, 1);
+                const float oim = __shfl_xor_sync(0xffffffffu, sim, 1);
+                if ((lane & 1) == 0 && vk) a.vpart[(size_t)n * a.nuv + k] = make_float2(sre - oim, sim + ore);
+            } else {
+                if (!umma::mbar_wait(&tfull[b], (uint32_t)(t >> 1) & 1u, TC_WAIT_BUDGET)) {
+                    tc_fail(a.err, abort_flag, 8u);
+                    break;
+                }
+                umma::tc_fence_after();
+                float *out = a.gpart + (size_t)split * a.out_rows * a.out_ld;
+                const int x = arow;
+                const bool xv = x < a.out_cols;
+#pragma unroll 1
+                for (int c = 0; c < TC_BN / 16; c++) {
+                    uint32_t r[16];
+                    umma::tmem_ld16(taddr + (uint32_t)(c * 16), r);
+                    umma::tmem_ld_wait();
+                    if (xv) {
+#pragma unroll
+                        for (int j = 0; j < 16; j++) {
+                            const int y = y0 + c * 16 + j;
+                            if (y < a.out_rows) out[(size_t)y * a.out_ld + x] = __uint_as_float(r[j]);
+                        }
+                    }
+                }
+                umma::tc_fence_before();
+                umma::mbar_arrive(&tempty[b]);
+            }
+        }
+    }
+    __syncthreads();
+    if (warp == 1) {
+        umma::tc_fence_after();
+        umma::tmem_dealloc(tmem_base, TC_TMEM_COLS);
+    }
+}
+
+// ------------------------------------------------------ operand kernels
+
+// Twiddle operands: forward B [rows_pad][Kx_pad] (row 2k+c = Re/Im of Fx[k][:])
+// and adjoint B [xrows_pad][K2_pad] (row x, column 2k+c), both scaled by 2^10.
+__global__ void k_tc_twiddle_ops(const float2 *__restrict__ fx, int nuv, int N, int Kx_pad, int rows_pad,
+                                 int K2_pad, int xrows_pad, __half *__restrict__ fx_hi, __half *__restrict__ fx_lo,
+                                 __half *__restrict__ fxt_hi, __half *__restrict__ fxt_lo)
+{
+    const float ts = (float)(1 << TC_TW_LOG2);
+    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    long long nf = (long long)rows_pad * Kx_pad;
+    if (idx < nf) {
+        int n = (int)(idx / Kx_pad), x = (int)(idx % Kx_pad), k = n >> 1;
+        float v = 0.f;
+        if (k < nuv && x < N) {
+            float2 f = fx[(size_t)k * N + x];
+            v = ((n & 1) ? f.y : f.x) * ts;
+        }
+        __half h = __float2half_rn(v);
+        fx_hi[idx] = h;
+        fx_lo[idx] = __float2half_rn(v - __half2float(h));
+        return;
+    }
+    idx -= nf;
+    if (idx < (long long)xrows_pad * K2_pad) {
+        int x = (int)(idx / K2_pad), kp = (int)(idx % K2_pad), k = kp >> 1;
+        float v = 0.f;
+        if (k < nuv && x < N) {
+            float2 f = fx[(size_t)k * N + x];
+            v = ((kp & 1) ? f.y : f.x) * ts;
+        }
+        __half h = __float2half_rn(v);
+        fxt_hi[idx] = h;
+        fxt_lo[idx] = __float2half_rn(v - __half2float(h));
+    }
+}
+
+// Image operand: one global power-of-two scale 2^(15 - e), e = exponent of
+// max |image| (reduced by k_prep), then an f16 hi/lo split; one block per
+// padded row. Block 0 publishes the factor the forward epilogue removes.
+__global__ void __launch_bounds__(256) k_tc_split_image(const float *__restrict__ img, int N, int Kx_pad,
+                                                        __half *__restrict__ hi, __half *__restrict__ lo,
+                                                        DevScalars *__restrict__ sc)
+{
+    const double mx = sc->imax;
+    int ex = 0;
+    float scale = 1.f;
+    if (mx > 0.0) {
+        frexp(mx, &ex);  // mx in [2^(ex-1), 2^ex)
+        scale = ldexpf(1.f, 15 - ex);
+    }
+    const int y = blockIdx.x;
+    for (int x = threadIdx.x; x < Kx_pad; x += blockDim.x) {
+        float v = (y < N && x < N) ? img[(size_t)y * N + x] * scale : 0.f;
+        __half h = __float2half_rn(v);
+        hi[(size_t)y * Kx_pad + x] = h;
+        lo[(size_t)y * Kx_pad + x] = __float2half_rn(v - __half2float(h));
+    }
+    if (y == 0 && threadIdx.x == 0) sc->fwd_inv_scale = mx > 0.0 ? ldexpf(1.f, ex - 15 - TC_TW_LOG2) : 0.f;
+}
+
+// Fy anchors every 16 image rows and the one-row rotation of every uv point
+__global__ void k_tc_fy_anchors(const float2 *__restrict__ fy, int nuv, int N, int nanc, float2 *__restrict__ fya,
+                                float2 *__restrict__ fyr)
+{
+    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)nuv * nanc) return;
+    int k = (int)(idx / nanc), j = (int)(idx % nanc);
+    fya[idx] = fy[(size_t)k * N + 16 * j];
+    if (j == 0) fyr[k] = N > 1 ? fy[(size_t)k * N + 1] : make_float2(1.f, 0.f);
+}
+
+// Adjoint A operand W[y][2k+c] from c_k and Fy[k][y], one global power-of-two
+// scale from max |c_k|; 32 uv x 32 rows per block, transposed through smem so
+// that reads of Fy and writes of W are both coalesced.
+__global__ void __launch_bounds__(256) k_tc_build_w(const float2 *__restrict__ cw, const float2 *__restrict__ fy,
+                                                    int nuv, int N, int K2_pad, __half *__restrict__ w_hi,
+                                                    __half *__restrict__ w_lo, DevScalars *__restrict__ sc)
+{
+    __shared__ float2 tile[32][33];
+    const double cmax = sc->cmax;
+    int ex = 0;
+    float wscale = 1.f;
+    if (cmax > 0.0) {
+        frexp(cmax * 1.4143, &ex);
+        wscale = ldexpf(1.f, 15 - ex);
+    }
+    if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0)
+        sc->gscale = 1.0 / ((double)wscale * (double)(1 << TC_TW_LOG2));
+    const int k0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
+    for (int j = ty; j < 32; j += 8) {
+        int k = k0 + j, y = y0 + tx;
+        float2 w = make_float2(0.f, 0.f);
+        if (k < nuv && y < N) {
+            float2 c = cw[k], f = fy[(size_t)k * N + y];
+            w = make_float2((c.x * f.x - c.y * f.y) * wscale, -(c.x * f.y + c.y * f.x) * wscale);
+        }
+        tile[j][tx] = w;  // [k][y]
+    }
+    __syncthreads();
+    for (int j = ty; j < 32; j += 8) {
+        int y = y0 + j;
+        if (y >= N) continue;
+        int kl = tx;  // one uv per thread: writes columns 2k, 2k+1
+        int k = k0 + kl;
+        if (2 * k + 1 >= K2_pad) continue;
+        float2 w = tile[kl][j];
+        __half h0 = __float2half_rn(w.x), h1 = __float2half_rn(w.y);
+        __half2 hv = __halves2half2(h0, h1);
+        __half2 lv = __halves2half2(__float2half_rn(w.x - __half2float(h0)), __float2half_rn(w.y - __half2float(h1)));
+        *reinterpret_cast<__half2 *>(&w_hi[(size_t)y * K2_pad + 2 * k]) = hv;
+        *reinterpret_cast<__half2 *>(&w_lo[(size_t)y * K2_pad + 2 * k]) = lv;
+    }
+}
+
+// ------------------------------------------------------------ host side
+
+static PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+
+static int tc_get_encode(gpair_ctx *c)
+{
+    if (g_encode) return GPAIR_OK;
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess
+        || q != cudaDriverEntryPointSuccess || !fn) {
+        snprintf(c->last_error, sizeof(c->last_error), "cuTensorMapEncodeTiled unavailable");
+        return GPAIR_ERR_CUDA;
+    }
+    g_encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    return GPAIR_OK;
+}
+
+// 2-D f16 tensor [rows][cols] (cols contiguous), 64 x box_rows boxes, 128 B swizzle
+static int tc_make_map(gpair_ctx *c, CUtensorMap *m, const void *base, long long rows, long long cols, int box_rows)
+{
+    if (cols % 64 || rows % box_rows || ((uintptr_t)base & 255)) {
+        snprintf(c->last_error, sizeof(c->last_error), "tensor map shape/alignment violates TMA rules");
+        return GPAIR_ERR_INVALID;
+    }
+    cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)cols * 2};
+    cuuint32_t box[2] = {64, (cuuint32_t)box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, const_cast<void *>(base), dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        snprintf(c->last_error, sizeof(c->last_error), "cuTensorMapEncodeTiled failed (%d)", (int)r);
+        return GPAIR_ERR_CUDA;
+    }
+    return GPAIR_OK;
+}
+
+int gp_tc_splits(int N, int nuv, int nsm, int *kb_per_out)
+{
+    int M_pad = round_up(N, TC_BN), xrows_pad = round_up(N, TC_BM), K2_pad = round_up(2LL * (nuv ? nuv : 1), TC_BK);
+    int tiles = (xrows_pad / TC_BM) * (M_pad / TC_BN);
+    int kb_total = K2_pad / TC_BK;
+    int want = (nsm + tiles - 1) / tiles;
+    if (want < 1) want = 1;
+    if (want > kb_total) want = kb_total;
+    int kb_per = (kb_total + want - 1) / want;
+    int splits = (kb_total + kb_per - 1) / kb_per;
+    if (kb_per_out) *kb_per_out = kb_per;
+    return splits;
+}
+
+void gp_tc_free(gpair_ctx *c)
+{
+    TcState *t = (TcState *)c->tc_state;
+    if (!t) return;
+    __half *bufs[] = {t->img_hi, t->img_lo, t->fx_hi, t->fx_lo, t->fxt_hi, t->fxt_lo, t->w_hi, t->w_lo};
+    for (__half *b : bufs)
+        if (b) cudaFree(b);
+    if (t->fya) cudaFree(t->fya);
+    if (t->fyr) cudaFree(t->fyr);
+    free(t);
+    c->tc_state = nullptr;
+}
 
 int gp_tc_prepare(gpair_ctx *c)
 {
-    snprintf(c->last_error, sizeof(c->last_error), "tensor-core precision modes are not built in this library");
-    return GPAIR_ERR_STATE;
+    if (c->precision == GPAIR_PREC_TF32) {
+        snprintf(c->last_error, sizeof(c->last_error), "the TF32 tensor path is not built in this library");
+        return GPAIR_ERR_STATE;
+    }
+    if (!c->have_problem) return GPAIR_OK;  // prepared when the problem is loaded
+    if (c->tc_state) return GPAIR_OK;
+    int rc = tc_get_encode(c);
+    if (rc) return rc;
+    TcState *t = (TcState *)calloc(1, sizeof(TcState));
+    if (!t) return GPAIR_ERR_ALLOC;
+    c->tc_state = t;
+    const int N = c->N, nuv = c->nuv ? c->nuv : 1;
+    t->Kx_pad = round_up(N, TC_BK);
+    t->M_pad = round_up(N, TC_BN);
+    t->rows_pad = round_up(2LL * nuv, TC_BM);
+    t->K2_pad = round_up(2LL * nuv, TC_BK);
+    t->xrows_pad = round_up(N, TC_BM);
+    GP_CUDA(c, cudaDeviceGetAttribute(&t->nsm, cudaDevAttrMultiProcessorCount, c->device));
+    t->splits = gp_tc_splits(N, nuv, t->nsm, &t->kb_per);
+    size_t img = (size_t)t->M_pad * t->Kx_pad, fxs = (size_t)t->rows_pad * t->Kx_pad;
+    size_t fxts = (size_t)t->xrows_pad * t->K2_pad, ws = (size_t)t->M_pad * t->K2_pad;
+    struct { __half **p; size_t n; } al[] = {{&t->img_hi, img}, {&t->img_lo, img}, {&t->fx_hi, fxs},
+                                             {&t->fx_lo, fxs},  {&t->fxt_hi, fxts}, {&t->fxt_lo, fxts},
+                                             {&t->w_hi, ws},    {&t->w_lo, ws}};
+    for (auto &x : al) {
+        GP_CUDA(c, cudaMalloc(x.p, x.n * sizeof(__half)));
+        GP_CUDA(c, cudaMemsetAsync(*x.p, 0, x.n * sizeof(__half), c->stream));
+    }
+    t->nanc = (N + 15) / 16;
+    GP_CUDA(c, cudaMalloc(&t->fya, sizeof(float2) * (size_t)nuv * t->nanc));
+    GP_CUDA(c, cudaMalloc(&t->fyr, sizeof(float2) * (size_t)nuv));
+    if (c->nuv) {
+        k_tc_fy_anchors<<<gp_cdiv((long long)c->nuv * t->nanc, 256), 256, 0, c->stream>>>(c->fy, c->nuv, N, t->nanc,
+                                                                                         t->fya, t->fyr);
+        GP_LAUNCH_CHECK(c);
+    }
+    long long n_all = (long long)fxs + (long long)fxts;
+    k_tc_twiddle_ops<<<gp_cdiv(n_all, 256), 256, 0, c->stream>>>(c->fx, c->nuv, N, t->Kx_pad, t->rows_pad, t->K2_pad,
+                                                                t->xrows_pad, t->fx_hi, t->fx_lo, t->fxt_hi,
+                                                                t->fxt_lo);
+    GP_LAUNCH_CHECK(c);
+    if ((rc = tc_make_map(c, &t->m_img_hi, t->img_hi, t->M_pad, t->Kx_pad, TC_BN))) return rc;
+    if ((rc = tc_make_map(c, &t->m_img_lo, t->img_lo, t->M_pad, t->Kx_pad, TC_BN))) return rc;
+    if ((rc = tc_make_map(c, &t->m_fx_hi, t->fx_hi, t->rows_pad, t->Kx_pad, TC_BM))) return rc;
+    if ((rc = tc_make_map(c, &t->m_fx_lo, t->fx_lo, t->rows_pad, t->Kx_pad, TC_BM))) return rc;
+    if ((rc = tc_make_map(c, &t->m_w_hi, t->w_hi, t->M_pad, t->K2_pad, TC_BN))) return rc;
+    if ((rc = tc_make_map(c, &t->m_w_lo, t->w_lo, t->M_pad, t->K2_pad, TC_BN))) return rc;
+    if ((rc = tc_make_map(c, &t->m_fxt_hi, t->fxt_hi, t->xrows_pad, t->K2_pad, TC_BM))) return rc;
+    if ((rc = tc_make_map(c, &t->m_fxt_lo, t->fxt_lo, t->xrows_pad, t->K2_pad, TC_BM))) return rc;
+    GP_CUDA(c, cudaFuncSetAttribute(k_tc_gemm<EPI_FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM_BYTES));
+    GP_CUDA(c, cudaFuncSetAttribute(k_tc_gemm<EPI_STORE>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM_BYTES));
+    GP_CUDA(c, cudaStreamSynchronize(c->stream));
+    return GPAIR_OK;
 }
-int gp_tc_forward(gpair_ctx *c, int) { return gp_tc_prepare(c); }
-int gp_tc_adjoint(gpair_ctx *c, int) { return gp_tc_prepare(c); }
-void gp_tc_free(gpair_ctx *) {}
-double gp_adjoint_scale(gpair_ctx *) { return 1.0; }
+
+int gp_tc_forward(gpair_ctx *c, int which)
+{
+    TcState *t = (TcState *)c->tc_state;
+    if (!t) {
+        int rc = gp_tc_prepare(c);
+        if (rc) return rc;
+        t = (TcState *)c->tc_state;
+        if (!t) return GPAIR_ERR_STATE;
+    }
+    const float *img = (which == GPAIR_IMG_TEMP) ? c->image_temp : c->image;
+    k_tc_split_image<<<t->M_pad, 256, 0, c->stream>>>(img, c->N, t->Kx_pad, t->img_hi, t->img_lo, c->sc);
+    GP_LAUNCH_CHECK(c);
+    TcArgs a;
+    memset(&a, 0, sizeof(a));
+    a.m_tiles = t->rows_pad / TC_BM;  // twiddle-row tiles
+    a.n_tiles = t->M_pad / TC_BN;     // image-row tiles
+    a.kb_total = t->Kx_pad / TC_BK;
+    a.kb_per_split = a.kb_total;
+    a.units = a.m_tiles * a.n_tiles;
+    a.fya = t->fya;
+    a.fyr = t->fyr;
+    a.nanc = t->nanc;
+    a.N = c->N;
+    a.nuv = c->nuv;
+    a.sc = c->sc;
+    a.vpart = c->vpart;
+    a.err = &c->sc->tc_err;
+    int grid = a.units < t->nsm ? a.units : t->nsm;
+    k_tc_gemm<EPI_FWD><<<grid, TC_THREADS, TC_SMEM_BYTES, c->stream>>>(t->m_fx_hi, t->m_fx_lo, t->m_img_hi,
+                                                                        t->m_img_lo, a);
+    GP_LAUNCH_CHECK(c);
+    c->mt = a.n_tiles;
+    return GPAIR_OK;
+}
+
+int gp_tc_adjoint(gpair_ctx *c, int which)
+{
+    (void)which;
+    TcState *t = (TcState *)c->tc_state;
+    if (!t) {
+        int rc = gp_tc_prepare(c);
+        if (rc) return rc;
+        t = (TcState *)c->tc_state;
+        if (!t) return GPAIR_ERR_STATE;
+    }
+    dim3 g(gp_cdiv(c->nuv ? c->nuv : 1, 32), gp_cdiv(c->N, 32));
+    k_tc_build_w<<<g, 256, 0, c->stream>>>(c->cw, c->fy, c->nuv, c->N, t->K2_pad, t->w_hi, t->w_lo, c->sc);
+    GP_LAUNCH_CHECK(c);
+    TcArgs a;
+    memset(&a, 0, sizeof(a));
+    a.m_tiles = t->xrows_pad / TC_BM;  // image-column tiles (twiddle side)
+    a.n_tiles = t->M_pad / TC_BN;      // image-row tiles (weight side)
+    a.kb_total = t->K2_pad / TC_BK;
+    a.kb_per_split = t->kb_per;
+    a.units = a.m_tiles * a.n_tiles * t->splits;
+    a.gpart = c->gpart;
+    a.out_ld = c->N;
+    a.out_rows = c->N;
+    a.out_cols = c->N;
+    a.err = &c->sc->tc_err;
+    int grid = a.units < t->nsm ? a.units : t->nsm;
+    k_tc_gemm<EPI_STORE><<<grid, TC_THREADS, TC_SMEM_BYTES, c->stream>>>(t->m_fxt_hi, t->m_fxt_lo, t->m_w_hi,
+                                                                          t->m_w_lo, a);
+    GP_LAUNCH_CHECK(c);
+    c->splits = t->splits;
+    return GPAIR_OK;
+}
+

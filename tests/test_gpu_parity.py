@@ -18,7 +18,7 @@ from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
-PRECISIONS = [g.PREC_FP32]
+PRECISIONS = [g.PREC_FP32, g.PREC_SPLIT16]
 
 
 def _problem(name, seeds=(1, 2, 3)):
@@ -65,10 +65,11 @@ def test_criterion_and_gradient_match_fp64(rec, name, prec):
     assert _rel(rec.full_gradient(), full) <= 1e-5
 
 
-def test_device_cg_matches_fp64_cg(rec):
+@pytest.mark.parametrize("prec", PRECISIONS)
+def test_device_cg_matches_fp64_cg(rec, prec):
     p = _problem("tiny", (21, 22, 23))
     rec.set_problem(p)
-    rec.set_precision(g.PREC_FP32)
+    rec.set_precision(prec)
     img0 = p.start_image()
     iters = 8
     _, tr = O.reconstruct64(p, img0, iters)
@@ -182,7 +183,8 @@ def test_reference_boundary_loop_matches_fp64_cg():
     assert Js[-1] < Js[0]
 
 
-def test_ragged_sizes_and_no_triangles(rec):
+@pytest.mark.parametrize("prec", PRECISIONS)
+def test_ragged_sizes_and_no_triangles(rec, prec):
     # odd image width, nuv not a multiple of any tile, no triangles
     rng = np.random.default_rng(3)
     N, nuv = 33, 37
@@ -194,6 +196,7 @@ def test_ragged_sizes_and_no_triangles(rec):
     p = g.Problem(N, 0.1, uv, nuv, 0, data, err, np.zeros(0, np.complex64), np.zeros((0, 3), np.int64),
                   np.zeros((0, 3), np.int16), np.full(N * N, 1.0 / N ** 2, np.float32), 1e-3)
     rec.set_problem(p)
+    rec.set_precision(prec)
     img = _rand_image(p, 1)
     rec.set_image(img)
     chi2, _ = rec.criterion()
