@@ -78,7 +78,7 @@ class OiData(C.Structure):
 class CgParams(C.Structure):
     _fields_ = [("method", C.c_int), ("iterations", C.c_int), ("alpha", C.c_float), ("minvalue", C.c_double),
                 ("wolfe1", C.c_double), ("wolfe2", C.c_double), ("step_max", C.c_double), ("max_zoom", C.c_int),
-                ("max_bracket", C.c_int), ("resume", C.c_int)]
+                ("max_bracket", C.c_int), ("resume", C.c_int), ("host_loop", C.c_int)]
 
 
 class CgResult(C.Structure):

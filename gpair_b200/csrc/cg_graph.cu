@@ -1,0 +1,211 @@
+// cg_graph.cu -- the CG iterations of gpair_cg_run as one CUDA graph with
+// conditional nodes, so that a run of any length is a single graph launch:
+// no host round trip per line-search trial.
+//
+//   WHILE (h_iter)                               one CG iteration per pass
+//     [pre ] criterion + gradient of the current image, beta, descent
+//            direction, wolfe1                    (gpair1/trunk/gpair.c:688-806)
+//     WHILE (h_ls)                               line-search trials
+//       [crit] trial image max(I + s d, minval), criterion, controller
+//       IF (h_grad)
+//         [grad] gradient of the trial image, controller
+//     [post] image update with the accepted step, gradient backup, trace
+//
+// The controller kernel (k_cg_ctrl_g) holds every decision of the reference's
+// line search (gpair1/trunk/gpair.c:832-903, gpair1/trunk/gpu.c:1947-2065) and
+// sets the three conditions with cudaGraphSetConditional. Loops are bounded:
+// the iteration count by run_limit, the trials by the controller's bracket
+// and zoom caps.
+#include <stdlib.h>
+#include <string.h>
+
+#include "gpair_internal.cuh"
+
+int gp_eval_criterion(gpair_ctx *c, int which, int trial);
+int gp_eval_gradient(gpair_ctx *c, int which, float alpha);
+
+struct CgGraph {
+    cudaGraph_t g;
+    cudaGraphExec_t exec;
+    int precision;
+    double *trace;
+    int trace_cap;
+    int n_pre, n_crit, n_grad, n_post;  // kernel launches per sequence
+};
+
+enum { SEQ_PRE = 0, SEQ_CRIT = 1, SEQ_GRAD = 2, SEQ_POST = 3 };
+
+static int emit(gpair_ctx *c, CgGraph *G, int seq, cudaGraphConditionalHandle hi, cudaGraphConditionalHandle hl,
+                cudaGraphConditionalHandle hg)
+{
+    int rc;
+    switch (seq) {
+    case SEQ_PRE:
+        if ((rc = gp_eval_criterion(c, GPAIR_IMG_CURR, 0))) return rc;
+        if ((rc = gp_eval_gradient(c, GPAIR_IMG_CURR, -1.f))) return rc;  // alpha from the device state
+        if ((rc = gp_cg_kernel_graph(c, CTRL_BEGIN, hi, hl, hg, G->trace, G->trace_cap))) return rc;
+        if ((rc = gp_descent_dir(c, 1, 0.0))) return rc;
+        return gp_cg_kernel_graph(c, CTRL_AFTER_DIR, hi, hl, hg, G->trace, G->trace_cap);
+    case SEQ_CRIT:
+        if ((rc = gp_eval_criterion(c, GPAIR_IMG_TEMP, 1))) return rc;
+        return gp_cg_kernel_graph(c, CTRL_AFTER_CRIT, hi, hl, hg, G->trace, G->trace_cap);
+    case SEQ_GRAD:
+        if ((rc = gp_eval_gradient(c, GPAIR_IMG_TEMP, -1.f))) return rc;
+        return gp_cg_kernel_graph(c, CTRL_AFTER_GRAD, hi, hl, hg, G->trace, G->trace_cap);
+    default:
+        if ((rc = gp_update_image(c, 1, 0.0, 1e-8, 1))) return rc;
+        return gp_cg_kernel_graph(c, CTRL_END, hi, hl, hg, G->trace, G->trace_cap);
+    }
+}
+
+static int capture(gpair_ctx *c, CgGraph *G, int seq, cudaGraphConditionalHandle hi, cudaGraphConditionalHandle hl,
+                   cudaGraphConditionalHandle hg, cudaGraph_t *out, int *nlaunch)
+{
+    const long long l0 = c->launches;
+    const int st = c->stage_timing;
+    c->stage_timing = 0;
+    GP_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = emit(c, G, seq, hi, hl, hg);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    c->stage_timing = st;
+    *nlaunch = (int)(c->launches - l0);
+    c->launches = l0;
+    if (rc || e != cudaSuccess || !g) {
+        if (g) cudaGraphDestroy(g);
+        if (!rc) snprintf(c->last_error, sizeof(c->last_error), "stream capture failed: %s", cudaGetErrorString(e));
+        return rc ? rc : GPAIR_ERR_CUDA;
+    }
+    *out = g;
+    return GPAIR_OK;
+}
+
+void gp_cg_graph_free(gpair_ctx *c)
+{
+    CgGraph *G = (CgGraph *)c->cg_graph;
+    if (!G) return;
+    if (G->exec) cudaGraphExecDestroy(G->exec);
+    if (G->g) cudaGraphDestroy(G->g);
+    if (G->trace) cudaFree(G->trace);
+    free(G);
+    c->cg_graph = nullptr;
+}
+
+static cudaGraphNode_t add_conditional(gpair_ctx *c, cudaGraph_t parent, cudaGraphConditionalHandle h,
+                                       cudaGraphConditionalNodeType type, cudaGraph_t *body, int *rc)
+{
+    cudaGraphNodeParams p = {cudaGraphNodeTypeConditional};  // remaining members zero
+    p.conditional.handle = h;
+    p.conditional.type = type;
+    p.conditional.size = 1;
+    cudaGraphNode_t n = nullptr;
+    cudaError_t e = cudaGraphAddNode(&n, parent, nullptr, 0, &p);
+    if (e != cudaSuccess) {
+        snprintf(c->last_error, sizeof(c->last_error), "cudaGraphAddNode(conditional): %s", cudaGetErrorString(e));
+        *rc = GPAIR_ERR_CUDA;
+        return nullptr;
+    }
+    *body = p.conditional.phGraph_out[0];
+    return n;
+}
+
+static int build(gpair_ctx *c, int trace_cap)
+{
+    gp_cg_graph_free(c);
+    if (c->precision != GPAIR_PREC_FP32) {
+        int rc = gp_tc_prepare(c);  // operand buffers must exist before capture
+        if (rc) return rc;
+    }
+    CgGraph *G = (CgGraph *)calloc(1, sizeof(CgGraph));
+    if (!G) return GPAIR_ERR_ALLOC;
+    c->cg_graph = G;
+    G->precision = c->precision;
+    G->trace_cap = trace_cap;
+    GP_CUDA(c, cudaMalloc(&G->trace, sizeof(double) * 5 * (size_t)trace_cap));
+    GP_CUDA(c, cudaGraphCreate(&G->g, 0));
+    int rc = GPAIR_OK;
+    cudaGraphConditionalHandle h_iter, h_ls, h_grad;
+    GP_CUDA(c, cudaGraphConditionalHandleCreate(&h_iter, G->g, 1, cudaGraphCondAssignDefault));
+    cudaGraph_t B1, B2, B3;
+    add_conditional(c, G->g, h_iter, cudaGraphCondTypeWhile, &B1, &rc);
+    if (rc) return rc;
+    GP_CUDA(c, cudaGraphConditionalHandleCreate(&h_ls, B1, 0, 0));
+    cudaGraphNode_t n_ls = add_conditional(c, B1, h_ls, cudaGraphCondTypeWhile, &B2, &rc);
+    if (rc) return rc;
+    GP_CUDA(c, cudaGraphConditionalHandleCreate(&h_grad, B2, 0, 0));
+    cudaGraphNode_t n_if = add_conditional(c, B2, h_grad, cudaGraphCondTypeIf, &B3, &rc);
+    if (rc) return rc;
+    cudaGraph_t S[4] = {nullptr, nullptr, nullptr, nullptr};
+    int *counts[4] = {&G->n_pre, &G->n_crit, &G->n_grad, &G->n_post};
+    for (int q = 0; q < 4 && !rc; q++) rc = capture(c, G, q, h_iter, h_ls, h_grad, &S[q], counts[q]);
+    if (!rc) {
+        cudaGraphNode_t n_pre, n_post, n_crit, n_grad;
+        cudaError_t e = cudaGraphAddChildGraphNode(&n_pre, B1, nullptr, 0, S[SEQ_PRE]);
+        if (e == cudaSuccess) e = cudaGraphAddChildGraphNode(&n_post, B1, nullptr, 0, S[SEQ_POST]);
+        if (e == cudaSuccess) e = cudaGraphAddDependencies(B1, &n_pre, &n_ls, 1);
+        if (e == cudaSuccess) e = cudaGraphAddDependencies(B1, &n_ls, &n_post, 1);
+        if (e == cudaSuccess) e = cudaGraphAddChildGraphNode(&n_crit, B2, nullptr, 0, S[SEQ_CRIT]);
+        if (e == cudaSuccess) e = cudaGraphAddDependencies(B2, &n_crit, &n_if, 1);
+        if (e == cudaSuccess) e = cudaGraphAddChildGraphNode(&n_grad, B3, nullptr, 0, S[SEQ_GRAD]);
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&G->exec, G->g, 0);
+        if (e != cudaSuccess) {
+            snprintf(c->last_error, sizeof(c->last_error), "CG graph assembly: %s", cudaGetErrorString(e));
+            rc = GPAIR_ERR_CUDA;
+        }
+    }
+    for (int q = 0; q < 4; q++)
+        if (S[q]) cudaGraphDestroy(S[q]);
+    if (rc) gp_cg_graph_free(c);
+    return rc;
+}
+
+// Launch `iterations` CG iterations as one graph. Returns the kernel launches
+// it executed through *launches (from the controller's evaluation counters).
+int gp_cg_graph_run(gpair_ctx *c, int iterations, int want_trace, long long *launches)
+{
+    CgGraph *G = (CgGraph *)c->cg_graph;
+    int cap = iterations > 4096 ? iterations : 4096;
+    if (!G || G->precision != c->precision || (want_trace && G->trace_cap < iterations)) {
+        int rc = build(c, cap);
+        if (rc) return rc;
+        G = (CgGraph *)c->cg_graph;
+    }
+    if (iterations > 0) GP_CUDA(c, cudaGraphLaunch(G->exec, c->stream));
+    *launches = 0;
+    return GPAIR_OK;
+}
+
+int gp_cg_graph_trace(gpair_ctx *c, int iterations, double *tJ, double *tchi2, double *tS, double *tstep,
+                      double *tbeta)
+{
+    CgGraph *G = (CgGraph *)c->cg_graph;
+    if (!G || iterations <= 0) return GPAIR_OK;
+    int n = iterations < G->trace_cap ? iterations : G->trace_cap;
+    double *h = (double *)malloc(sizeof(double) * 5 * (size_t)n);
+    if (!h) return GPAIR_ERR_ALLOC;
+    cudaError_t e = cudaMemcpyAsync(h, G->trace, sizeof(double) * 5 * (size_t)n, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) {
+        free(h);
+        snprintf(c->last_error, sizeof(c->last_error), "trace copy: %s", cudaGetErrorString(e));
+        return GPAIR_ERR_CUDA;
+    }
+    for (int i = 0; i < n; i++) {
+        if (tJ) tJ[i] = h[5 * i];
+        if (tchi2) tchi2[i] = h[5 * i + 1];
+        if (tS) tS[i] = h[5 * i + 2];
+        if (tstep) tstep[i] = h[5 * i + 3];
+        if (tbeta) tbeta[i] = h[5 * i + 4];
+    }
+    free(h);
+    return GPAIR_OK;
+}
+
+// kernel launches a finished graph run executed
+long long gp_cg_graph_launches(gpair_ctx *c, int iterations_done, int criterion_evals, int grad_evals)
+{
+    CgGraph *G = (CgGraph *)c->cg_graph;
+    if (!G) return 0;
+    long long trials_c = criterion_evals - iterations_done, trials_g = grad_evals - iterations_done;
+    return (long long)iterations_done * (G->n_pre + G->n_post) + trials_c * G->n_crit + trials_g * G->n_grad;
+}

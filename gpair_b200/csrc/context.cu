@@ -16,6 +16,11 @@
 #include "gpair_internal.cuh"
 
 int gp_default_splits(int N, int nuv);
+void gp_cg_graph_free(gpair_ctx *c);
+int gp_cg_graph_run(gpair_ctx *c, int iterations, int want_trace, long long *launches);
+int gp_cg_graph_trace(gpair_ctx *c, int iterations, double *tJ, double *tchi2, double *tS, double *tstep,
+                      double *tbeta);
+long long gp_cg_graph_launches(gpair_ctx *c, int iterations_done, int criterion_evals, int grad_evals);
 
 static const char *k_err_names[] = {"GPAIR_OK",      "GPAIR_ERR_INVALID", "GPAIR_ERR_ALLOC",     "GPAIR_ERR_CUDA",
                                     "GPAIR_ERR_STATE", "GPAIR_ERR_TIMEOUT", "GPAIR_ERR_NO_DEVICE", "GPAIR_ERR_NUMERIC"};
@@ -37,6 +42,7 @@ extern "C" const char *gpair_last_error(gpair_ctx *ctx) { return ctx ? ctx->last
 
 static void free_problem(gpair_ctx *c)
 {
+    gp_cg_graph_free(c);
     FREE_DEV(c->data); FREE_DEV(c->data_err); FREE_DEV(c->mock);
     FREE_DEV(c->tri); FREE_DEV(c->phasor); FREE_DEV(c->uvc);
     FREE_DEV(c->fx); FREE_DEV(c->fy); FREE_DEV(c->vpart); FREE_DEV(c->visd); FREE_DEV(c->visi);
@@ -47,6 +53,7 @@ static void free_problem(gpair_ctx *c)
 
 static void free_images(gpair_ctx *c)
 {
+    gp_cg_graph_free(c);
     FREE_DEV(c->image); FREE_DEV(c->image_temp); FREE_DEV(c->model);
     FREE_DEV(c->data_grad); FREE_DEV(c->entropy_grad); FREE_DEV(c->full_grad_new);
     FREE_DEV(c->full_grad); FREE_DEV(c->grad_temp); FREE_DEV(c->descent_dir);
@@ -458,6 +465,7 @@ extern "C" void gpair_cg_default_params(gpair_cg_params *p)
     p->max_zoom = 200;
     p->max_bracket = 100;
     p->resume = 0;
+    p->host_loop = 0;
 }
 
 static int read_action(gpair_ctx *c, int *action)
@@ -486,6 +494,7 @@ extern "C" int gpair_cg_run(gpair_ctx *c, const gpair_cg_params *p, gpair_cg_res
     h.c1 = p->wolfe1;
     h.c2 = p->wolfe2;
     h.step_max = p->step_max;
+    h.run_limit = p->iterations;
     int rc;
     if (p->resume) {
         // parameters only; the iteration state of the previous run is kept
@@ -500,8 +509,24 @@ extern "C" int gpair_cg_run(gpair_ctx *c, const gpair_cg_params *p, gpair_cg_res
     GP_CUDA(c, cudaEventCreate(&e0));
     GP_CUDA(c, cudaEventCreate(&e1));
     long long launches0 = c->launches;
+    const int want_trace = tJ || tchi2 || tS || tstep || tbeta;
+    if (!p->host_loop) {
+        // build (or reuse) the graph before the timed region
+        long long dummy = 0;
+        if ((rc = gp_cg_graph_run(c, 0, want_trace, &dummy))) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            return rc;
+        }
+        if (c->stage_timing) c->st_n = 0;
+    }
     GP_CUDA(c, cudaEventRecord(e0, c->stream));
-    int status = GPAIR_OK, it;
+    int status = GPAIR_OK, it = 0;
+    if (!p->host_loop) {
+        long long dummy = 0;
+        status = gp_cg_graph_run(c, p->iterations, want_trace, &dummy);
+        goto finished;
+    }
     for (it = 0; it < p->iterations && status == GPAIR_OK; it++) {
         if ((rc = gp_eval_criterion(c, GPAIR_IMG_CURR, 0)) || (rc = gp_eval_gradient(c, GPAIR_IMG_CURR, p->alpha))
             || (rc = gp_cg_kernel(c, CTRL_BEGIN)) || (rc = gp_descent_dir(c, 1, 0.0))
@@ -539,6 +564,7 @@ extern "C" int gpair_cg_run(gpair_ctx *c, const gpair_cg_params *p, gpair_cg_res
         }
         rc = 0;
     }
+finished:
     GP_CUDA(c, cudaEventRecord(e1, c->stream));
     GP_CUDA(c, cudaEventSynchronize(e1));
     float ms = 0.f;
@@ -549,6 +575,12 @@ extern "C" int gpair_cg_run(gpair_ctx *c, const gpair_cg_params *p, gpair_cg_res
     int rc2 = gp_sync_scalars(c);
     if (rc2 && !status) status = rc2;
     const CgState &s = c->sc_host->cg;
+    if (!p->host_loop) {
+        it = s.run_it;
+        if (want_trace && !status) status = gp_cg_graph_trace(c, it, tJ, tchi2, tS, tstep, tbeta);
+        if (!status && c->sc_host->nonfinite) status = GPAIR_ERR_NUMERIC;
+        c->launches = launches0 + gp_cg_graph_launches(c, it, s.criterion_evals, s.grad_evals);
+    }
     c->last_ms = ms;
     double per = 4.0 * (double)c->npix * c->nuv + 8.0 * c->N * (double)c->nuv;
     c->last_flops = per * (s.criterion_evals + s.grad_evals);

@@ -45,6 +45,7 @@ enum { CG_PH_BRACKET = 0, CG_PH_ZOOM = 1 };
 struct CgState {
     // parameters
     int method, max_zoom, max_bracket;
+    int run_limit;  // iterations this run performs (graph-captured runs)
     double alpha, minvalue, c1, c2, step_max;
     // per iteration
     int it;
@@ -58,6 +59,7 @@ struct CgState {
     double sel;
     // counters
     int criterion_evals, grad_evals;
+    int run_it;  // iterations completed in this run
 };
 
 struct DevScalars {
@@ -135,6 +137,9 @@ struct gpair_ctx {
     double stage_ms[8];
     int stage_cnt[8];
 
+    // graph-captured CG (cg_graph.cu)
+    void *cg_graph;
+
     // reference-boundary staging (layer 1)
     gpair_float2 *ref_dft_x, *ref_dft_y;  // host copies of the transposed tables
     int ref_dft_size;
@@ -192,10 +197,14 @@ int gp_descent_dir(gpair_ctx *c, int beta_from_state, double beta_host);
 int gp_update_image(gpair_ctx *c, int step_from_state, double step_host, double minval, int backup);
 int gp_update_temp(gpair_ctx *c, double step, double minval, int clamp);
 int gp_cg_kernel(gpair_ctx *c, int which_ctrl);
+// graph-captured controller: also sets the conditional handles of the CG graph
+int gp_cg_kernel_graph(gpair_ctx *c, int which_ctrl, unsigned long long h_iter, unsigned long long h_ls,
+                       unsigned long long h_grad, double *trace, int trace_cap);
 int gp_sync_scalars(gpair_ctx *c);
 
 enum { GRAD_FUSED = 0, GRAD_DATA_ONLY = 1 };
-enum { CTRL_BEGIN = 0, CTRL_AFTER_DIR = 1, CTRL_AFTER_CRIT = 2, CTRL_AFTER_GRAD = 3, CTRL_INIT = 4, CTRL_RESUME = 5 };
+enum { CTRL_BEGIN = 0, CTRL_AFTER_DIR = 1, CTRL_AFTER_CRIT = 2, CTRL_AFTER_GRAD = 3, CTRL_INIT = 4, CTRL_RESUME = 5,
+       CTRL_END = 6 };
 
 // tensor-core path (umma_dft.cu); return GPAIR_ERR_STATE when unavailable
 int gp_tc_prepare(gpair_ctx *c);

@@ -169,6 +169,7 @@ __global__ void __launch_bounds__(GP_THREADS) k_prep(const float *__restrict__ s
 {
     __shared__ double smem[2 * 32];
     double s = step_from_state ? sc->cg.s : step;
+    if (step_from_state) minval = sc->cg.minvalue;
     double acc[2] = {0.0, 0.0};
     double mx = 0.0;
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
@@ -219,7 +220,8 @@ static int red_grid(long long n) { int g = gp_cdiv(n, GP_THREADS * 4); return g 
 int gp_prep_image(gpair_ctx *c, int which, int trial_mode, double step_host, int step_from_state)
 {
     const float *src = (which == GPAIR_IMG_TEMP && !trial_mode) ? c->image_temp : c->image;
-    int g = red_grid(c->npix);
+    int g = gp_cdiv(c->npix, GP_THREADS);
+    if (g > GP_MAX_PARTIALS) g = GP_MAX_PARTIALS;
     k_prep<<<g, GP_THREADS, 0, c->stream>>>(src, c->descent_dir, c->image_temp, c->model, c->npix, trial_mode,
                                             step_host, step_from_state, (double)1e-8, slot_partials(c, RED_PREP),
                                             c->sc);
@@ -595,6 +597,7 @@ __global__ void __launch_bounds__(GP_THREADS) k_grad_finalize(const float *__res
                                                               int npix, int mode,
                                                               const float *__restrict__ img,
                                                               const float *__restrict__ model, float alpha,
+                                                              int alpha_from_state,
                                                               float *__restrict__ data_grad,
                                                               float *__restrict__ entropy_grad,
                                                               float *__restrict__ out,
@@ -605,6 +608,7 @@ __global__ void __launch_bounds__(GP_THREADS) k_grad_finalize(const float *__res
 {
     __shared__ double smem[4 * 32];
     const double C = sc->adj_c, gscale = sc->gscale;
+    if (alpha_from_state) alpha = (float)sc->cg.alpha;
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
         double g = 0.0;
@@ -651,12 +655,14 @@ __global__ void __launch_bounds__(GP_THREADS) k_grad_finalize(const float *__res
 
 int gp_grad_finalize(gpair_ctx *c, int which, int mode, float alpha)
 {
+    // alpha < 0 requests the value held in the device CG state (graph-captured runs)
+    const int alpha_from_state = alpha < 0.f;
     const float *img = (which == GPAIR_IMG_TEMP) ? c->image_temp : c->image;
     float *out = (which == GPAIR_IMG_TEMP) ? c->grad_temp : c->full_grad_new;
     int g = gp_cdiv(c->npix, GP_THREADS);  // one pixel per thread: the split sum is latency-bound
     if (g > GP_MAX_PARTIALS) g = GP_MAX_PARTIALS;
     k_grad_finalize<<<g, GP_THREADS, 0, c->stream>>>(c->gpart, c->splits, c->npix, mode, img,
-                                                     c->model, alpha, c->data_grad, c->entropy_grad, out,
+                                                     c->model, alpha, alpha_from_state, c->data_grad, c->entropy_grad, out,
                                                      c->full_grad, c->descent_dir, which == GPAIR_IMG_TEMP ? 1 : 0,
                                                      slot_partials(c, RED_GRAD), c->sc);
     GP_LAUNCH_CHECK(c);
@@ -767,6 +773,7 @@ __global__ void k_update_image(float *__restrict__ img, const float *__restrict_
     int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
     double s = step_from_state ? sc->cg.sel : step_host;
+    if (step_from_state) minval = sc->cg.minvalue;
     double t = (double)img[p] + s * (double)d[p];
     if (t < minval) t = minval;
     img[p] = (float)t;
@@ -834,17 +841,21 @@ __device__ void cg_zoom_enter(CgState &s, double lo, double hi, double J_lo)
     cg_zoom_next(s);
 }
 
-__global__ void k_cg_ctrl(DevScalars *__restrict__ sc, int what)
+__device__ void cg_control(DevScalars *__restrict__ sc, int what)
 {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
     CgState &s = sc->cg;
     switch (what) {
     case CTRL_RESUME:
         // a continued run counts its own evaluations; the iteration state is kept
         s.criterion_evals = s.grad_evals = 0;
+        s.run_it = 0;
         sc->nonfinite = 0;
         break;
+    case CTRL_END:
+        s.run_it++;
+        break;
     case CTRL_INIT:
+        s.run_it = 0;
         s.it = 0;
         s.criterion_evals = s.grad_evals = 0;
         s.beta = 0.0;
@@ -973,6 +984,62 @@ __global__ void k_cg_ctrl(DevScalars *__restrict__ sc, int what)
     default:
         break;
     }
+}
+
+__global__ void k_cg_ctrl(DevScalars *__restrict__ sc, int what)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    cg_control(sc, what);
+}
+
+// Graph-captured controller: runs the same state machine, then steers the CG
+// graph: h_ls keeps the line-search loop going, h_grad selects the gradient
+// branch of a trial, h_iter keeps the iteration loop going. At the end of an
+// iteration it appends (J, chi2, S, step, beta) to the device trace.
+__global__ void k_cg_ctrl_g(DevScalars *__restrict__ sc, int what, cudaGraphConditionalHandle h_iter,
+                            cudaGraphConditionalHandle h_ls, cudaGraphConditionalHandle h_grad,
+                            double *__restrict__ trace, int trace_cap)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    CgState &s = sc->cg;
+    if (what == CTRL_END) {
+        if (s.run_it < trace_cap) {
+            double *t = trace + 5 * (size_t)s.run_it;
+            t[0] = s.J;
+            t[1] = s.chi2;
+            t[2] = s.entropy;
+            t[3] = s.sel;
+            t[4] = s.beta;
+        }
+    }
+    cg_control(sc, what);
+    switch (what) {
+    case CTRL_AFTER_DIR:
+        cudaGraphSetConditional(h_ls, 1u);
+        break;
+    case CTRL_AFTER_CRIT:
+        cudaGraphSetConditional(h_grad, s.action == CG_EVAL_GRAD ? 1u : 0u);
+        cudaGraphSetConditional(h_ls, s.action != CG_DONE ? 1u : 0u);
+        break;
+    case CTRL_AFTER_GRAD:
+        cudaGraphSetConditional(h_ls, s.action != CG_DONE ? 1u : 0u);
+        break;
+    case CTRL_END: {
+        bool more = s.run_it < s.run_limit && !sc->nonfinite && !sc->tc_err;
+        cudaGraphSetConditional(h_iter, more ? 1u : 0u);
+        break;
+    }
+    default:
+        break;
+    }
+}
+
+int gp_cg_kernel_graph(gpair_ctx *c, int which_ctrl, unsigned long long h_iter, unsigned long long h_ls,
+                       unsigned long long h_grad, double *trace, int trace_cap)
+{
+    k_cg_ctrl_g<<<1, 32, 0, c->stream>>>(c->sc, which_ctrl, h_iter, h_ls, h_grad, trace, trace_cap);
+    GP_LAUNCH_CHECK(c);
+    return GPAIR_OK;
 }
 
 int gp_cg_kernel(gpair_ctx *c, int which_ctrl)

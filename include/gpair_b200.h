@@ -267,6 +267,9 @@ typedef struct {
     int max_bracket;  /* cap on bracketing trials */
     int resume;       /* 0: start a new run; 1: continue the previous run's CG state
                          (iteration count, previous gradient, descent direction) */
+    int host_loop;    /* 0 (default): the whole run is one CUDA graph launch (conditional
+                         nodes steer the line search on the device); 1: the host reads
+                         the controller's decision after every trial */
 } gpair_cg_params;
 
 typedef struct {

@@ -232,3 +232,20 @@ def test_resumed_cg_equals_uninterrupted_run(rec):
     img_part = rec.get_image()
     assert np.array_equal(img_full, img_part)  # deterministic reductions: bit-identical
     assert part["J"] == full["J"]
+
+
+@pytest.mark.parametrize("prec", PRECISIONS)
+def test_graph_run_equals_host_loop_run(rec, prec):
+    """The graph-captured CG (default) takes the same decisions as the host-driven loop."""
+    p = _problem("tiny", (12, 13, 14))
+    rec.set_problem(p)
+    rec.set_precision(prec)
+    rec.set_image(p.start_image())
+    a = rec.cg(6, method=2, trace=True)
+    img_a = rec.get_image()
+    rec.set_image(p.start_image())
+    b = rec.cg(6, method=2, trace=True, host_loop=1)
+    img_b = rec.get_image()
+    assert np.array_equal(img_a, img_b)
+    assert np.array_equal(a["trace_J"], b["trace_J"])
+    assert a["criterion_evals"] == b["criterion_evals"] and a["grad_evals"] == b["grad_evals"]
