@@ -38,24 +38,36 @@ enum { SEQ_PRE = 0, SEQ_CRIT = 1, SEQ_GRAD = 2, SEQ_POST = 3 };
 static int emit(gpair_ctx *c, CgGraph *G, int seq, cudaGraphConditionalHandle hi, cudaGraphConditionalHandle hl,
                 cudaGraphConditionalHandle hg)
 {
+    // the controller runs in the last block of the reduction kernel that precedes it
+    c->fuse_handles = 1;
+    c->fh_iter = hi;
+    c->fh_ls = hl;
+    c->fh_grad = hg;
     int rc;
     switch (seq) {
     case SEQ_PRE:
-        if ((rc = gp_eval_criterion(c, GPAIR_IMG_CURR, 0))) return rc;
-        if ((rc = gp_eval_gradient(c, GPAIR_IMG_CURR, -1.f))) return rc;  // alpha from the device state
-        if ((rc = gp_cg_kernel_graph(c, CTRL_BEGIN, hi, hl, hg, G->trace, G->trace_cap))) return rc;
-        if ((rc = gp_descent_dir(c, 1, 0.0))) return rc;
-        return gp_cg_kernel_graph(c, CTRL_AFTER_DIR, hi, hl, hg, G->trace, G->trace_cap);
+        if ((rc = gp_eval_criterion(c, GPAIR_IMG_CURR, 0))) break;
+        c->fuse_ctrl = CTRL_BEGIN;
+        if ((rc = gp_eval_gradient(c, GPAIR_IMG_CURR, -1.f))) break;  // alpha from the device state
+        c->fuse_ctrl = CTRL_AFTER_DIR;
+        rc = gp_descent_dir(c, 1, 0.0);
+        break;
     case SEQ_CRIT:
-        if ((rc = gp_eval_criterion(c, GPAIR_IMG_TEMP, 1))) return rc;
-        return gp_cg_kernel_graph(c, CTRL_AFTER_CRIT, hi, hl, hg, G->trace, G->trace_cap);
+        c->fuse_ctrl = CTRL_AFTER_CRIT;
+        rc = gp_eval_criterion(c, GPAIR_IMG_TEMP, 1);
+        break;
     case SEQ_GRAD:
-        if ((rc = gp_eval_gradient(c, GPAIR_IMG_TEMP, -1.f))) return rc;
-        return gp_cg_kernel_graph(c, CTRL_AFTER_GRAD, hi, hl, hg, G->trace, G->trace_cap);
+        c->fuse_ctrl = CTRL_AFTER_GRAD;
+        rc = gp_eval_gradient(c, GPAIR_IMG_TEMP, -1.f);
+        break;
     default:
-        if ((rc = gp_update_image(c, 1, 0.0, 1e-8, 1))) return rc;
-        return gp_cg_kernel_graph(c, CTRL_END, hi, hl, hg, G->trace, G->trace_cap);
+        if ((rc = gp_update_image(c, 1, 0.0, 1e-8, 1))) break;
+        rc = gp_cg_kernel_graph(c, CTRL_END, hi, hl, hg, G->trace, G->trace_cap);
+        break;
     }
+    c->fuse_ctrl = -1;
+    c->fuse_handles = 0;
+    return rc;
 }
 
 static int capture(gpair_ctx *c, CgGraph *G, int seq, cudaGraphConditionalHandle hi, cudaGraphConditionalHandle hl,

@@ -110,6 +110,7 @@ extern "C" int gpair_create(gpair_ctx **out, int device)
     if (!c) return GPAIR_ERR_ALLOC;
     c->device = device;
     c->precision = GPAIR_PREC_FP32;
+    c->fuse_ctrl = -1;
     c->last_image_src = -1;
     int rc = GPAIR_OK;
     do {
@@ -377,10 +378,15 @@ int gp_eval_criterion(gpair_ctx *c, int which, int trial)
 {
     int rc;
     gp_stage_begin(c, 0);
-    if ((rc = gp_prep_image(c, trial ? GPAIR_IMG_TEMP : which, trial, 0.0, trial))) return rc;
+    const bool fused_trial = trial && c->precision != GPAIR_PREC_FP32;
+    if (fused_trial) rc = gp_tc_prep_split_trial(c);  // trial image + f16 operand in one pass
+    else rc = gp_prep_image(c, trial ? GPAIR_IMG_TEMP : which, trial, 0.0, trial);
+    if (rc) return rc;
     gp_stage_end(c);
     gp_stage_begin(c, 1);
-    if ((rc = gp_forward(c, trial ? GPAIR_IMG_TEMP : which))) return rc;
+    if (fused_trial) rc = gp_tc_forward_gemm(c);
+    else rc = gp_forward(c, trial ? GPAIR_IMG_TEMP : which);
+    if (rc) return rc;
     gp_stage_end(c);
     gp_stage_begin(c, 2);
     if ((rc = gp_vis_data(c))) return rc;
@@ -483,6 +489,8 @@ extern "C" int gpair_cg_run(gpair_ctx *c, const gpair_cg_params *p, gpair_cg_res
     if (!c || !p || !c->have_problem) return GPAIR_ERR_STATE;
     if (p->iterations < 0 || p->method < 0 || p->method > 3) return GPAIR_ERR_INVALID;
     GP_CUDA(c, cudaSetDevice(c->device));
+    c->fuse_ctrl = -1;
+    c->fuse_handles = 0;
     // parameters into the device state
     CgState h;
     memset(&h, 0, sizeof(h));
@@ -528,30 +536,30 @@ extern "C" int gpair_cg_run(gpair_ctx *c, const gpair_cg_params *p, gpair_cg_res
         goto finished;
     }
     for (it = 0; it < p->iterations && status == GPAIR_OK; it++) {
-        if ((rc = gp_eval_criterion(c, GPAIR_IMG_CURR, 0)) || (rc = gp_eval_gradient(c, GPAIR_IMG_CURR, p->alpha))
-            || (rc = gp_cg_kernel(c, CTRL_BEGIN)) || (rc = gp_descent_dir(c, 1, 0.0))
-            || (rc = gp_cg_kernel(c, CTRL_AFTER_DIR))) {
-            status = rc;
-            break;
-        }
+        // the controller steps run in the last block of the preceding reduction kernel
+        if ((rc = gp_eval_criterion(c, GPAIR_IMG_CURR, 0))) { status = rc; break; }
+        c->fuse_ctrl = CTRL_BEGIN;
+        if ((rc = gp_eval_gradient(c, GPAIR_IMG_CURR, -1.f))) { status = rc; break; }
+        c->fuse_ctrl = CTRL_AFTER_DIR;
+        if ((rc = gp_descent_dir(c, 1, 0.0))) { status = rc; break; }
         int action = CG_EVAL_CRIT, trials = 0;
         while (action != CG_DONE) {
             if (++trials > 10000) { status = GPAIR_ERR_TIMEOUT; break; }
             if (action == CG_EVAL_CRIT) {
-                if ((rc = gp_eval_criterion(c, GPAIR_IMG_TEMP, 1)) || (rc = gp_cg_kernel(c, CTRL_AFTER_CRIT))) {
-                    status = rc;
-                    break;
-                }
+                c->fuse_ctrl = CTRL_AFTER_CRIT;
+                rc = gp_eval_criterion(c, GPAIR_IMG_TEMP, 1);
             } else {
-                if ((rc = gp_eval_gradient(c, GPAIR_IMG_TEMP, p->alpha)) || (rc = gp_cg_kernel(c, CTRL_AFTER_GRAD))) {
-                    status = rc;
-                    break;
-                }
+                c->fuse_ctrl = CTRL_AFTER_GRAD;
+                rc = gp_eval_gradient(c, GPAIR_IMG_TEMP, -1.f);
             }
+            if (rc) { status = rc; break; }
             if ((rc = read_action(c, &action))) { status = rc; break; }
         }
         if (status) break;
-        if ((rc = gp_update_image(c, 1, 0.0, p->minvalue, 1))) { status = rc; break; }
+        if ((rc = gp_update_image(c, 1, 0.0, p->minvalue, 1)) || (rc = gp_cg_kernel(c, CTRL_END))) {
+            status = rc;
+            break;
+        }
         if (tJ || tchi2 || tS || tstep || tbeta || it == p->iterations - 1) {
             if ((rc = gp_sync_scalars(c))) { status = rc; break; }
             const CgState &s = c->sc_host->cg;
@@ -613,32 +621,40 @@ extern "C" int gpair_time_stages(gpair_ctx *c, int reps, double *ms, int max_sta
     if (!c || !c->have_problem || reps <= 0 || !ms) return GPAIR_ERR_INVALID;
     GP_CUDA(c, cudaSetDevice(c->device));
     const int ns = GPAIR_NSTAGES;
-    cudaEvent_t ev[GPAIR_NSTAGES + 1];
-    for (int i = 0; i <= ns; i++) GP_CUDA(c, cudaEventCreate(&ev[i]));
-    double acc[GPAIR_NSTAGES] = {0};
+    std::vector<cudaEvent_t> ev((size_t)(ns + 1) * reps);
+    for (auto &e : ev) GP_CUDA(c, cudaEventCreate(&e));
+    const bool tc = c->precision != GPAIR_PREC_FP32;
     int rc = GPAIR_OK;
     for (int r = 0; r < reps && !rc; r++) {
-        cudaEventRecord(ev[0], c->stream);
+        // stages queued back to back: the events time kernels, not host launch gaps
+        cudaEvent_t *E = &ev[(size_t)r * (ns + 1)];
+        cudaEventRecord(E[0], c->stream);
         if ((rc = gp_prep_image(c, GPAIR_IMG_CURR, 0, 0.0, 0))) break;
-        cudaEventRecord(ev[1], c->stream);
-        if ((rc = gp_forward(c, GPAIR_IMG_CURR))) break;
-        cudaEventRecord(ev[2], c->stream);
+        if (tc && (rc = gp_tc_split(c, GPAIR_IMG_CURR))) break;
+        cudaEventRecord(E[1], c->stream);
+        if ((rc = tc ? gp_tc_forward_gemm(c) : gp_forward(c, GPAIR_IMG_CURR))) break;
+        cudaEventRecord(E[2], c->stream);
         if ((rc = gp_vis_data(c))) break;
-        cudaEventRecord(ev[3], c->stream);
+        cudaEventRecord(E[3], c->stream);
         if ((rc = gp_adj_weights_only(c))) break;
-        cudaEventRecord(ev[4], c->stream);
-        if ((rc = gp_adjoint_contraction(c, GPAIR_IMG_CURR))) break;
-        cudaEventRecord(ev[5], c->stream);
+        if (tc && (rc = gp_tc_build_w(c))) break;
+        cudaEventRecord(E[4], c->stream);
+        if ((rc = tc ? gp_tc_adjoint_gemm(c) : gp_adjoint_contraction(c, GPAIR_IMG_CURR))) break;
+        cudaEventRecord(E[5], c->stream);
         if ((rc = gp_grad_finalize(c, GPAIR_IMG_CURR, GRAD_FUSED, 1e-3f))) break;
-        cudaEventRecord(ev[6], c->stream);
-        if (cudaEventSynchronize(ev[6]) != cudaSuccess) { rc = GPAIR_ERR_CUDA; break; }
+        cudaEventRecord(E[6], c->stream);
+    }
+    double acc[GPAIR_NSTAGES] = {0};
+    if (!rc && cudaStreamSynchronize(c->stream) != cudaSuccess) rc = GPAIR_ERR_CUDA;
+    for (int r = 0; r < reps && !rc; r++) {
+        cudaEvent_t *E = &ev[(size_t)r * (ns + 1)];
         for (int i = 0; i < ns; i++) {
             float t = 0.f;
-            cudaEventElapsedTime(&t, ev[i], ev[i + 1]);
+            cudaEventElapsedTime(&t, E[i], E[i + 1]);
             acc[i] += t;
         }
     }
-    for (int i = 0; i <= ns; i++) cudaEventDestroy(ev[i]);
+    for (auto &e : ev) cudaEventDestroy(e);
     if (rc) return rc;
     int n = max_stages < ns ? max_stages : ns;
     for (int i = 0; i < n; i++) ms[i] = acc[i] / reps;

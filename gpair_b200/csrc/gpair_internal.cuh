@@ -65,6 +65,8 @@ struct CgState {
 struct DevScalars {
     double flux, invflux, entropy, chi2;
     double imax;          // max |image| of the last prepared image
+    double imax_curr;     // max |image| of the current CG image
+    unsigned int dmax_bits;  // max |descent direction| (float bits, atomic max)
     float fwd_inv_scale;  // tensor forward: 1 / (image scale * twiddle scale)
     double adj_c;      // C = Re sum_k c_k V_k
     double cmax;       // max |c_k| (scaling of split operands)
@@ -139,6 +141,9 @@ struct gpair_ctx {
 
     // graph-captured CG (cg_graph.cu)
     void *cg_graph;
+    // controller fused into the next reduction kernel launched (-1: none)
+    int fuse_ctrl, fuse_handles;
+    unsigned long long fh_iter, fh_ls, fh_grad;
 
     // reference-boundary staging (layer 1)
     gpair_float2 *ref_dft_x, *ref_dft_y;  // host copies of the transposed tables
@@ -209,6 +214,11 @@ enum { CTRL_BEGIN = 0, CTRL_AFTER_DIR = 1, CTRL_AFTER_CRIT = 2, CTRL_AFTER_GRAD 
 // tensor-core path (umma_dft.cu); return GPAIR_ERR_STATE when unavailable
 int gp_tc_prepare(gpair_ctx *c);
 int gp_tc_forward(gpair_ctx *c, int which);
+int gp_tc_forward_gemm(gpair_ctx *c);
+int gp_tc_split(gpair_ctx *c, int which);
+int gp_tc_build_w(gpair_ctx *c);
+int gp_tc_adjoint_gemm(gpair_ctx *c);
+int gp_tc_prep_split_trial(gpair_ctx *c);
 int gp_tc_splits(int N, int nuv, int nsm, int *kb_per_out);
 int gp_tc_adjoint(gpair_ctx *c, int which);
 void gp_tc_free(gpair_ctx *c);

@@ -32,70 +32,36 @@
 
 #define RPMAS_D ((3.14159265358979323 / 180.0) / 3600000.0)
 
-// ------------------------------------------------------------ reductions
+#include "reduce.cuh"
 
-template <int NV>
-__device__ __forceinline__ void block_sum(double (&v)[NV], double *smem)
+__device__ void cg_control(DevScalars *__restrict__ sc, int what);
+__device__ void cg_set_handles(DevScalars *__restrict__ sc, int what, cudaGraphConditionalHandle h_iter,
+                               cudaGraphConditionalHandle h_ls, cudaGraphConditionalHandle h_grad);
+
+// Controller fused into the last block of a reduction kernel (thread 0 only)
+struct FusedCtrl {
+    int what;         // CTRL_* to run after the reduction, or -1
+    int use_handles;  // set the CG graph's conditionals (graph-captured runs only)
+    cudaGraphConditionalHandle h_iter, h_ls, h_grad;
+};
+
+__device__ __forceinline__ void run_fused_ctrl(DevScalars *sc, const FusedCtrl &f)
 {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-#pragma unroll
-    for (int i = 0; i < NV; i++)
-        for (int off = 16; off > 0; off >>= 1) v[i] += __shfl_down_sync(0xffffffffu, v[i], off);
-    if (lane == 0)
-        for (int i = 0; i < NV; i++) smem[i * 32 + warp] = v[i];
-    __syncthreads();
-    if (warp == 0) {
-#pragma unroll
-        for (int i = 0; i < NV; i++) {
-            v[i] = lane < nw ? smem[i * 32 + lane] : 0.0;
-            for (int off = 16; off > 0; off >>= 1) v[i] += __shfl_down_sync(0xffffffffu, v[i], off);
-        }
-    }
-    __syncthreads();
+    if (f.what < 0) return;
+    cg_control(sc, f.what);
+    if (f.use_handles) cg_set_handles(sc, f.what, f.h_iter, f.h_ls, f.h_grad);
 }
 
-__device__ __forceinline__ double block_max(double v, double *smem)
+static FusedCtrl take_fused_ctrl(gpair_ctx *c)
 {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int off = 16; off > 0; off >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, off));
-    if (lane == 0) smem[warp] = v;
-    __syncthreads();
-    if (warp == 0) {
-        v = lane < nw ? smem[lane] : 0.0;
-        for (int off = 16; off > 0; off >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, off));
-    }
-    __syncthreads();
-    return v;
-}
-
-// True in exactly one block: the last to arrive. Partials written before the
-// call are visible to it. The counter is reset by that block.
-__device__ __forceinline__ bool last_block(unsigned int *counter)
-{
-    __shared__ bool am_last;
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        unsigned int prev = atomicAdd(counter, 1u);
-        am_last = (prev == gridDim.x - 1);
-    }
-    __syncthreads();
-    return am_last;
-}
-
-// Sum NV partial vectors (layout [block][NV]) in a fixed order.
-template <int NV>
-__device__ void finish_sum(const double *partials, int nblocks, double (&out)[NV], double *smem)
-{
-    double v[NV];
-#pragma unroll
-    for (int i = 0; i < NV; i++) v[i] = 0.0;
-    for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
-#pragma unroll
-        for (int i = 0; i < NV; i++) v[i] += __ldcg(&partials[(size_t)b * NV + i]);
-    block_sum<NV>(v, smem);
-#pragma unroll
-    for (int i = 0; i < NV; i++) out[i] = v[i];
+    FusedCtrl f;
+    f.what = c->fuse_ctrl;
+    f.use_handles = c->fuse_handles;
+    f.h_iter = c->fh_iter;
+    f.h_ls = c->fh_ls;
+    f.h_grad = c->fh_grad;
+    c->fuse_ctrl = -1;
+    return f;
 }
 
 static inline double *slot_partials(gpair_ctx *c, int slot) { return c->partials + (size_t)slot * GP_MAX_PARTIALS * 4; }
@@ -341,7 +307,7 @@ __global__ void __launch_bounds__(GP_THREADS) k_vis_data(const float2 *__restric
                                                          double2 *__restrict__ visd, float2 *__restrict__ visi,
                                                          float *__restrict__ mock, float2 *__restrict__ cw,
                                                          float2 *__restrict__ trib, double *__restrict__ partials,
-                                                         DevScalars *__restrict__ sc)
+                                                         DevScalars *__restrict__ sc, FusedCtrl fc)
 {
     __shared__ double smem[32];
     const double invF = sc->invflux;
@@ -408,6 +374,7 @@ __global__ void __launch_bounds__(GP_THREADS) k_vis_data(const float2 *__restric
             sc->chi2_f = (float)out[0];
             if (!isfinite(out[0])) sc->nonfinite |= 2u;
             sc->counter[RED_CHI2] = 0;
+            run_fused_ctrl(sc, fc);
         }
     }
 }
@@ -421,7 +388,8 @@ int gp_vis_data(gpair_ctx *c)
     if (nbt > 1536) nbt = 1536;
     k_vis_data<<<nbu + nbt, GP_THREADS, 0, c->stream>>>(c->vpart, c->mt, c->nuv, c->npow, c->nbis, c->data,
                                                         c->data_err, c->tri, c->phasor, nbu, c->visd, c->visi,
-                                                        c->mock, c->cw, c->trib, slot_partials(c, RED_CHI2), c->sc);
+                                                        c->mock, c->cw, c->trib, slot_partials(c, RED_CHI2), c->sc,
+                                                        take_fused_ctrl(c));
     GP_LAUNCH_CHECK(c);
     return GPAIR_OK;
 }
@@ -440,10 +408,21 @@ __global__ void __launch_bounds__(GP_THREADS) k_adj_weights(int nuv, const int *
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nuv; k += gridDim.x * blockDim.x) {
         float2 a = cw[k];
         double re = a.x, im = a.y;
-        for (int p = inc_off[k]; p < inc_off[k + 1]; p++) {
-            float2 b = trib[inc_idx[p]];
-            re += b.x;
-            im += b.y;
+        const int pe = inc_off[k + 1];
+        for (int p0 = inc_off[k]; p0 < pe; p0 += 8) {
+            // up to 8 independent index loads, then 8 independent weight loads;
+            // the sum keeps the ascending incidence order
+            int idx[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++) idx[j] = (p0 + j < pe) ? __ldg(&inc_idx[p0 + j]) : -1;
+            float2 b[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++) b[j] = idx[j] >= 0 ? __ldg(&trib[idx[j]]) : make_float2(0.f, 0.f);
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                re += b[j].x;
+                im += b[j].y;
+            }
         }
         float2 cf = make_float2((float)re, (float)im);
         cw[k] = cf;
@@ -604,7 +583,7 @@ __global__ void __launch_bounds__(GP_THREADS) k_grad_finalize(const float *__res
                                                               const float *__restrict__ g_old,
                                                               const float *__restrict__ d, int dot_slot,
                                                               double *__restrict__ partials,
-                                                              DevScalars *__restrict__ sc)
+                                                              DevScalars *__restrict__ sc, FusedCtrl fc)
 {
     __shared__ double smem[4 * 32];
     const double C = sc->adj_c, gscale = sc->gscale;
@@ -613,15 +592,14 @@ __global__ void __launch_bounds__(GP_THREADS) k_grad_finalize(const float *__res
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
         double g = 0.0;
         int s = 0;
-        for (; s + 4 <= splits; s += 4) {
-            float a0 = gpart[(size_t)s * npix + p], a1 = gpart[(size_t)(s + 1) * npix + p];
-            float a2 = gpart[(size_t)(s + 2) * npix + p], a3 = gpart[(size_t)(s + 3) * npix + p];
-            g += a0;
-            g += a1;
-            g += a2;
-            g += a3;
+        for (; s + 16 <= splits; s += 16) {  // 16 loads in flight, summed in split order
+            float a[16];
+#pragma unroll
+            for (int j = 0; j < 16; j++) a[j] = __ldcs(&gpart[(size_t)(s + j) * npix + p]);
+#pragma unroll
+            for (int j = 0; j < 16; j++) g += a[j];
         }
-        for (; s < splits; s++) g += gpart[(size_t)s * npix + p];
+        for (; s < splits; s++) g += __ldcs(&gpart[(size_t)s * npix + p]);
         float gd = (float)(g * gscale - C);
         data_grad[p] = gd;
         if (mode == GRAD_FUSED) {
@@ -649,6 +627,7 @@ __global__ void __launch_bounds__(GP_THREADS) k_grad_finalize(const float *__res
             for (int i = 0; i < 4; i++) sc->grad_dots[dot_slot][i] = o[i];
             if (!isfinite(o[0])) sc->nonfinite |= 4u;
             sc->counter[RED_GRAD] = 0;
+            run_fused_ctrl(sc, fc);
         }
     }
 }
@@ -664,7 +643,7 @@ int gp_grad_finalize(gpair_ctx *c, int which, int mode, float alpha)
     k_grad_finalize<<<g, GP_THREADS, 0, c->stream>>>(c->gpart, c->splits, c->npix, mode, img,
                                                      c->model, alpha, alpha_from_state, c->data_grad, c->entropy_grad, out,
                                                      c->full_grad, c->descent_dir, which == GPAIR_IMG_TEMP ? 1 : 0,
-                                                     slot_partials(c, RED_GRAD), c->sc);
+                                                     slot_partials(c, RED_GRAD), c->sc, take_fused_ctrl(c));
     GP_LAUNCH_CHECK(c);
     return GPAIR_OK;
 }
@@ -734,17 +713,23 @@ int gp_dot(gpair_ctx *c, const float *a, const float *b, int n)
 // d = beta d - g_new, and d.g_new (FP64)
 __global__ void __launch_bounds__(GP_THREADS) k_descent(float *__restrict__ d, const float *__restrict__ g, int n,
                                                         int beta_from_state, double beta_host,
-                                                        double *__restrict__ partials, DevScalars *__restrict__ sc)
+                                                        double *__restrict__ partials, DevScalars *__restrict__ sc,
+                                                        FusedCtrl fc)
 {
     __shared__ double smem[32];
     const double beta = beta_from_state ? sc->cg.beta : beta_host;
     double acc[1] = {0.0};
+    double dmax = 0.0;
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
         float dn = (float)(beta * (double)d[p] - (double)g[p]);
         d[p] = dn;
         acc[0] += (double)dn * (double)g[p];
+        dmax = fmax(dmax, fabs((double)dn));
     }
     block_sum<1>(acc, smem);
+    dmax = block_max(dmax, smem);
+    // max |d| bounds the trial images (order-independent, so an atomic max stays deterministic)
+    if (threadIdx.x == 0) atomicMax(&sc->dmax_bits, __float_as_uint((float)dmax));
     if (threadIdx.x == 0) partials[blockIdx.x] = acc[0];
     if (last_block(&sc->counter[RED_DIR])) {
         double o[1];
@@ -752,6 +737,7 @@ __global__ void __launch_bounds__(GP_THREADS) k_descent(float *__restrict__ d, c
         if (threadIdx.x == 0) {
             sc->dir_dot = o[0];
             sc->counter[RED_DIR] = 0;
+            run_fused_ctrl(sc, fc);
         }
     }
 }
@@ -760,7 +746,7 @@ int gp_descent_dir(gpair_ctx *c, int beta_from_state, double beta_host)
 {
     k_descent<<<red_grid(c->npix), GP_THREADS, 0, c->stream>>>(c->descent_dir, c->full_grad_new, c->npix,
                                                                beta_from_state, beta_host,
-                                                               slot_partials(c, RED_DIR), c->sc);
+                                                               slot_partials(c, RED_DIR), c->sc, take_fused_ctrl(c));
     GP_LAUNCH_CHECK(c);
     return GPAIR_OK;
 }
@@ -865,6 +851,8 @@ __device__ void cg_control(DevScalars *__restrict__ sc, int what)
         sc->nonfinite = 0;
         break;
     case CTRL_BEGIN: {
+        sc->imax_curr = sc->imax;  // exact max of the current image (its prep ran this iteration)
+        sc->dmax_bits = 0u;        // k_descent re-reduces max |d|
         // criterion and gradient of the current image are done (gpair.c:688-724);
         // beta from the FP64 dot products of the gradient finalize (gpair.c:727-758)
         s.J = sc->chi2 - s.alpha * sc->entropy;
@@ -996,23 +984,10 @@ __global__ void k_cg_ctrl(DevScalars *__restrict__ sc, int what)
 // graph: h_ls keeps the line-search loop going, h_grad selects the gradient
 // branch of a trial, h_iter keeps the iteration loop going. At the end of an
 // iteration it appends (J, chi2, S, step, beta) to the device trace.
-__global__ void k_cg_ctrl_g(DevScalars *__restrict__ sc, int what, cudaGraphConditionalHandle h_iter,
-                            cudaGraphConditionalHandle h_ls, cudaGraphConditionalHandle h_grad,
-                            double *__restrict__ trace, int trace_cap)
+__device__ void cg_set_handles(DevScalars *__restrict__ sc, int what, cudaGraphConditionalHandle h_iter,
+                               cudaGraphConditionalHandle h_ls, cudaGraphConditionalHandle h_grad)
 {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    CgState &s = sc->cg;
-    if (what == CTRL_END) {
-        if (s.run_it < trace_cap) {
-            double *t = trace + 5 * (size_t)s.run_it;
-            t[0] = s.J;
-            t[1] = s.chi2;
-            t[2] = s.entropy;
-            t[3] = s.sel;
-            t[4] = s.beta;
-        }
-    }
-    cg_control(sc, what);
+    const CgState &s = sc->cg;
     switch (what) {
     case CTRL_AFTER_DIR:
         cudaGraphSetConditional(h_ls, 1u);
@@ -1032,6 +1007,28 @@ __global__ void k_cg_ctrl_g(DevScalars *__restrict__ sc, int what, cudaGraphCond
     default:
         break;
     }
+}
+
+// Graph-captured controller: runs the same state machine, then steers the CG
+// graph: h_ls keeps the line-search loop going, h_grad selects the gradient
+// branch of a trial, h_iter keeps the iteration loop going. At the end of an
+// iteration it appends (J, chi2, S, step, beta) to the device trace.
+__global__ void k_cg_ctrl_g(DevScalars *__restrict__ sc, int what, cudaGraphConditionalHandle h_iter,
+                            cudaGraphConditionalHandle h_ls, cudaGraphConditionalHandle h_grad,
+                            double *__restrict__ trace, int trace_cap)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    CgState &s = sc->cg;
+    if (what == CTRL_END && s.run_it < trace_cap && trace) {
+        double *t = trace + 5 * (size_t)s.run_it;
+        t[0] = s.J;
+        t[1] = s.chi2;
+        t[2] = s.entropy;
+        t[3] = s.sel;
+        t[4] = s.beta;
+    }
+    cg_control(sc, what);
+    if (h_iter) cg_set_handles(sc, what, h_iter, h_ls, h_grad);
 }
 
 int gp_cg_kernel_graph(gpair_ctx *c, int which_ctrl, unsigned long long h_iter, unsigned long long h_ls,

@@ -34,6 +34,7 @@
 #include <string.h>
 
 #include "gpair_internal.cuh"
+#include "reduce.cuh"
 #include "umma.cuh"
 
 #define TC_BM 128
@@ -375,6 +376,72 @@ __global__ void __launch_bounds__(256) k_tc_split_image(const float *__restrict_
     if (y == 0 && threadIdx.x == 0) sc->fwd_inv_scale = mx > 0.0 ? ldexpf(1.f, ex - 15 - TC_TW_LOG2) : 0.f;
 }
 
+// Trial image + f16 split in one pass (line-search trials): I_t = max(I + s d,
+// minval), its flux / entropy / max reduced in FP64 like k_prep, and the f16
+// hi/lo image operand written with a power-of-two scale taken from the exact
+// bound max|I_t| <= max|I| + |s| max|d| (both maxima reduced earlier in the
+// iteration), so no separate pass over the trial image is needed.
+__global__ void __launch_bounds__(GP_THREADS) k_tc_prep_split_trial(
+    const float *__restrict__ img, const float *__restrict__ d, float *__restrict__ dst,
+    const float *__restrict__ model, int N, int npix, int Kx_pad, __half *__restrict__ hi, __half *__restrict__ lo,
+    double *__restrict__ partials, DevScalars *__restrict__ sc)
+{
+    __shared__ double smem[2 * 32];
+    const double s = sc->cg.s, minval = sc->cg.minvalue;
+    double bound = sc->imax_curr + fabs(s) * (double)__uint_as_float(sc->dmax_bits);
+    if (bound < minval) bound = minval;
+    int ex = 0;
+    frexp(bound, &ex);
+    const float scale = ldexpf(1.f, 15 - ex);
+    double acc[2] = {0.0, 0.0};
+    double mx = 0.0;
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < npix) {
+        double t = (double)img[p] + s * (double)d[p];
+        if (t < minval) t = minval;
+        const float I = (float)t;
+        dst[p] = I;
+        const double Id = I, m = model[p];
+        acc[0] = Id;
+        acc[1] = (Id > 0.0 && m > 0.0) ? (Id - m - Id * log(Id / m)) : -m;
+        mx = fabs(Id);
+        const int y = p / N, x = p - y * N;
+        const float v = I * scale;
+        const __half h = __float2half_rn(v);
+        hi[(size_t)y * Kx_pad + x] = h;
+        lo[(size_t)y * Kx_pad + x] = __float2half_rn(v - __half2float(h));
+    }
+    block_sum<2>(acc, smem);
+    mx = block_max(mx, smem);
+    if (threadIdx.x == 0) {
+        partials[3 * blockIdx.x] = acc[0];
+        partials[3 * blockIdx.x + 1] = acc[1];
+        partials[3 * blockIdx.x + 2] = mx;
+    }
+    if (last_block(&sc->counter[RED_PREP])) {
+        double v[2] = {0.0, 0.0}, m = 0.0;
+        for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
+            v[0] += __ldcg(&partials[3 * b]);
+            v[1] += __ldcg(&partials[3 * b + 1]);
+            m = fmax(m, __ldcg(&partials[3 * b + 2]));
+        }
+        block_sum<2>(v, smem);
+        m = block_max(m, smem);
+        if (threadIdx.x == 0) {
+            sc->flux = v[0];
+            sc->invflux = 1.0 / v[0];
+            sc->entropy = v[1];
+            sc->imax = m;
+            sc->flux_f = (float)v[0];
+            sc->invflux_f = (float)(1.0 / v[0]);
+            sc->entropy_f = (float)v[1];
+            sc->fwd_inv_scale = ldexpf(1.f, ex - 15 - TC_TW_LOG2);
+            if (!isfinite(v[0]) || !isfinite(v[1])) sc->nonfinite |= 1u;
+            sc->counter[RED_PREP] = 0;
+        }
+    }
+}
+
 // Fy anchors every 16 image rows and the one-row rotation of every uv point
 __global__ void k_tc_fy_anchors(const float2 *__restrict__ fy, int nuv, int N, int nanc, float2 *__restrict__ fya,
                                 float2 *__restrict__ fyr)
@@ -478,6 +545,10 @@ int gp_tc_splits(int N, int nuv, int nsm, int *kb_per_out)
     if (want < 1) want = 1;
     if (want > kb_total) want = kb_total;
     int kb_per = (kb_total + want - 1) / want;
+    // FP32 accumulation in TMEM: a running sum of n oscillating products carries a
+    // relative rounding error of about 2^-24 sqrt(n); at most 64 K-blocks (4096
+    // products) per split keeps it near 4e-6, the splits are summed in FP64
+    if (kb_per > 64) kb_per = 64;
     int splits = (kb_total + kb_per - 1) / kb_per;
     if (kb_per_out) *kb_per_out = kb_per;
     return splits;
@@ -553,18 +624,24 @@ int gp_tc_prepare(gpair_ctx *c)
     return GPAIR_OK;
 }
 
-int gp_tc_forward(gpair_ctx *c, int which)
+static TcState *tc_state_ready(gpair_ctx *c, int *rc)
 {
     TcState *t = (TcState *)c->tc_state;
+    *rc = GPAIR_OK;
     if (!t) {
-        int rc = gp_tc_prepare(c);
-        if (rc) return rc;
+        *rc = gp_tc_prepare(c);
         t = (TcState *)c->tc_state;
-        if (!t) return GPAIR_ERR_STATE;
+        if (!*rc && !t) *rc = GPAIR_ERR_STATE;
     }
-    const float *img = (which == GPAIR_IMG_TEMP) ? c->image_temp : c->image;
-    k_tc_split_image<<<t->M_pad, 256, 0, c->stream>>>(img, c->N, t->Kx_pad, t->img_hi, t->img_lo, c->sc);
-    GP_LAUNCH_CHECK(c);
+    return t;
+}
+
+// forward contraction on the already split image operand
+int gp_tc_forward_gemm(gpair_ctx *c)
+{
+    int rc;
+    TcState *t = tc_state_ready(c, &rc);
+    if (rc) return rc;
     TcArgs a;
     memset(&a, 0, sizeof(a));
     a.m_tiles = t->rows_pad / TC_BM;  // twiddle-row tiles
@@ -588,19 +665,57 @@ int gp_tc_forward(gpair_ctx *c, int which)
     return GPAIR_OK;
 }
 
-int gp_tc_adjoint(gpair_ctx *c, int which)
+// f16 hi/lo split of an image into the forward's image operand
+int gp_tc_split(gpair_ctx *c, int which)
 {
-    (void)which;
-    TcState *t = (TcState *)c->tc_state;
-    if (!t) {
-        int rc = gp_tc_prepare(c);
-        if (rc) return rc;
-        t = (TcState *)c->tc_state;
-        if (!t) return GPAIR_ERR_STATE;
-    }
+    int rc;
+    TcState *t = tc_state_ready(c, &rc);
+    if (rc) return rc;
+    const float *img = (which == GPAIR_IMG_TEMP) ? c->image_temp : c->image;
+    k_tc_split_image<<<t->M_pad, 256, 0, c->stream>>>(img, c->N, t->Kx_pad, t->img_hi, t->img_lo, c->sc);
+    GP_LAUNCH_CHECK(c);
+    return GPAIR_OK;
+}
+
+int gp_tc_forward(gpair_ctx *c, int which)
+{
+    int rc = gp_tc_split(c, which);
+    if (rc) return rc;
+    return gp_tc_forward_gemm(c);
+}
+
+// trial image + split in one kernel (reads s, minval, max|I|, max|d| from the device state)
+int gp_tc_prep_split_trial(gpair_ctx *c)
+{
+    int rc;
+    TcState *t = tc_state_ready(c, &rc);
+    if (rc) return rc;
+    int g = gp_cdiv(c->npix, GP_THREADS);
+    k_tc_prep_split_trial<<<g, GP_THREADS, 0, c->stream>>>(c->image, c->descent_dir, c->image_temp, c->model, c->N,
+                                                           c->npix, t->Kx_pad, t->img_hi, t->img_lo,
+                                                           c->partials, c->sc);
+    GP_LAUNCH_CHECK(c);
+    return GPAIR_OK;
+}
+
+// adjoint A-side weights W from c_k and Fy (f16 hi/lo, one global scale)
+int gp_tc_build_w(gpair_ctx *c)
+{
+    int rc;
+    TcState *t = tc_state_ready(c, &rc);
+    if (rc) return rc;
     dim3 g(gp_cdiv(c->nuv ? c->nuv : 1, 32), gp_cdiv(c->N, 32));
     k_tc_build_w<<<g, 256, 0, c->stream>>>(c->cw, c->fy, c->nuv, c->N, t->K2_pad, t->w_hi, t->w_lo, c->sc);
     GP_LAUNCH_CHECK(c);
+    return GPAIR_OK;
+}
+
+// adjoint contraction on the already built weights: S split-K partial images
+int gp_tc_adjoint_gemm(gpair_ctx *c)
+{
+    int rc;
+    TcState *t = tc_state_ready(c, &rc);
+    if (rc) return rc;
     TcArgs a;
     memset(&a, 0, sizeof(a));
     a.m_tiles = t->xrows_pad / TC_BM;  // image-column tiles (twiddle side)
@@ -621,3 +736,10 @@ int gp_tc_adjoint(gpair_ctx *c, int which)
     return GPAIR_OK;
 }
 
+int gp_tc_adjoint(gpair_ctx *c, int which)
+{
+    (void)which;
+    int rc = gp_tc_build_w(c);
+    if (rc) return rc;
+    return gp_tc_adjoint_gemm(c);
+}

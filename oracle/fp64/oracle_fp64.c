@@ -415,3 +415,75 @@ int o32_ref_cg_run(const void *problem, int N, int nuv, int ndata, float *model,
     free(c.visi); free(c.mock); free(c.dgrad); free(c.egrad);
     return rc;
 }
+
+/* The direct gradient (gpair1/trunk/cpu.c:303-368) at selected pixels only,
+ * for checks at sizes where the full O(N^2 (npow + nbis)) sum is too slow.
+ * pix_x/pix_y hold npx pixel coordinates; grad receives npx values. */
+void o64_data_gradient_pixels(int N, int npow, int nbis, int nuv, const double *image, const float *uv, float pix,
+                              const float *data, const float *data_err, const float *phasor_c64,
+                              const int64_t *uvpnt, const int16_t *sign, const double *visi, const double *mock,
+                              int npx, const int *pix_x, const int *pix_y, double *grad)
+{
+    const double complex *V = (const double complex *)visi;
+    double flux = 0;
+    for (int i = 0; i < N * N; i++) flux += image[i];
+    const double invflux = 1. / flux;
+    double complex *ex = malloc(sizeof(double complex) * (nuv ? nuv : 1));
+    double complex *ey = malloc(sizeof(double complex) * (nuv ? nuv : 1));
+    for (int q = 0; q < npx; q++) {
+        const int ii = pix_x[q], jj = pix_y[q];
+        for (int k = 0; k < nuv; k++) {
+            double px = o64_phase(pix, uv[4 * k], ii), py = o64_phase(pix, uv[4 * k + 1], jj);
+            ex[k] = cos(px) + I * sin(px);
+            ey[k] = cos(py) - I * sin(py);
+        }
+        double g = 0;
+        for (int k = 0; k < npow; k++) {
+            double complex e = ex[k] * ey[k];
+            g += 4.0 * (double)data_err[k] * data_err[k] * invflux * (mock[k] - data[k]) * creal(conj(V[k]) * (e - V[k]));
+        }
+        for (int t = 0; t < nbis; t++) {
+            int64_t a = uvpnt[3 * t], b = uvpnt[3 * t + 1], c = uvpnt[3 * t + 2];
+            double complex vab = V[a], vbc = V[b], vca = V[c];
+            double complex dab = ex[a] * ey[a], dbc = ex[b] * ey[b], dca = ex[c] * ey[c];
+            if (sign[3 * t] < 0) { vab = conj(vab); dab = conj(dab); }
+            if (sign[3 * t + 1] < 0) { vbc = conj(vbc); dbc = conj(dbc); }
+            if (sign[3 * t + 2] < 0) { vca = conj(vca); dca = conj(dca); }
+            double complex ph = phasor_c64[2 * t] + I * phasor_c64[2 * t + 1];
+            double complex t3der = ((dab - vab) * vbc * vca + vab * (dbc - vbc) * vca + vab * vbc * (dca - vca)) * ph * invflux;
+            int r = npow + 2 * t;
+            g += 2. * (double)data_err[r] * data_err[r] * (mock[r] - data[r]) * creal(t3der);
+            g += 2. * (double)data_err[r + 1] * data_err[r + 1] * mock[r + 1] * cimag(t3der);
+        }
+        grad[q] = g;
+    }
+    free(ex);
+    free(ey);
+}
+
+/* FP64 visibilities at selected uv points (same sum as o64_image2vis). */
+void o64_image2vis_subset(int N, const double *image, const float *uv, float pix, int nsel, const int *sel,
+                          double *visi)
+{
+    double F = 0;
+    for (int i = 0; i < N * N; i++) F += image[i];
+    double complex *V = (double complex *)visi;
+    double complex *ex = malloc(sizeof(double complex) * N), *ey = malloc(sizeof(double complex) * N);
+    for (int q = 0; q < nsel; q++) {
+        const int k = sel[q];
+        for (int i = 0; i < N; i++) {
+            double px = o64_phase(pix, uv[4 * k], i), py = o64_phase(pix, uv[4 * k + 1], i);
+            ex[i] = cos(px) + I * sin(px);
+            ey[i] = cos(py) - I * sin(py);
+        }
+        double complex acc = 0;
+        for (int y = 0; y < N; y++) {
+            double complex row = 0;
+            for (int x = 0; x < N; x++) row += image[y * N + x] * ex[x];
+            acc += row * ey[y];
+        }
+        V[q] = (F > 0.) ? acc / F : acc;
+    }
+    free(ex);
+    free(ey);
+}

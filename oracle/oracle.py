@@ -282,3 +282,35 @@ class RefEvaluator:
             raise RuntimeError("o32_ref_cg_run failed")
         return img, dict(criterion_evals=ce.value, grad_evals=ge.value, J=tr[0], chi2=tr[1], entropy=tr[2],
                          step=tr[3], beta=tr[4])
+
+
+def visibilities_subset64(p, image, sel):
+    """FP64 visibilities of `image` at uv indices `sel` (for checks at full problem size)."""
+    L = fp64()
+    L.o64_image2vis_subset.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_float, C.c_int, C.c_void_p, C.c_void_p]
+    img = np.ascontiguousarray(image, np.float64)
+    uv = np.ascontiguousarray(p.uv, np.float32)
+    sel = np.ascontiguousarray(sel, np.int32)
+    out = np.zeros(len(sel), np.complex128)
+    L.o64_image2vis_subset(p.width, _p(img), _p(uv), p.pixellation, len(sel), _p(sel), _p(out))
+    return out
+
+
+def data_gradient_pixels64(p, image, visi, mock, px, py):
+    """FP64 direct gradient (reference per-pixel sum) at pixels (px, py), given visibilities and mock data."""
+    L = fp64()
+    vp, i, f = C.c_void_p, C.c_int, C.c_float
+    L.o64_data_gradient_pixels.argtypes = [i, i, i, i, vp, vp, f, vp, vp, vp, vp, vp, vp, vp, i, vp, vp, vp]
+    img = np.ascontiguousarray(image, np.float64)
+    keep = [np.ascontiguousarray(x) for x in (p.uv.astype(np.float32), p.data.astype(np.float32),
+                                              p.data_err.astype(np.float32), p.phasor.astype(np.complex64),
+                                              p.uvpnt.astype(np.int64), p.sign.astype(np.int16))]
+    v = np.ascontiguousarray(visi, np.complex128)
+    m = np.ascontiguousarray(mock, np.float64)
+    px = np.ascontiguousarray(px, np.int32)
+    py = np.ascontiguousarray(py, np.int32)
+    out = np.zeros(len(px), np.float64)
+    L.o64_data_gradient_pixels(p.width, p.npow, p.nbis, p.nuv, _p(img), _p(keep[0]), p.pixellation, _p(keep[1]),
+                               _p(keep[2]), _p(keep[3]), _p(keep[4]), _p(keep[5]), _p(v), _p(m), len(px), _p(px),
+                               _p(py), _p(out))
+    return out
