@@ -160,6 +160,23 @@ def cpu_baseline(workload, width=32, reps=3):
                       f"({reps} evaluations, {dt:.1f} s)"}
 
 
+def replica_seeds(rank):
+    """Seeds of rank `rank`'s replica: the same array and scene on every rank, an own noise seed."""
+    return {"scene_seed": 1, "noise_seed": 2 + rank, "array_seed": 3}
+
+
+def combine_over_ranks(times, work, device=None):
+    """Whole-job figures of independent replicas: the slowest rank's times (max) and
+    the work of all ranks (sum). The only collective of a run, outside the timed region."""
+    import torch
+    t = torch.tensor(times, dtype=torch.float64, device=device)
+    w = torch.tensor(work, dtype=torch.float64, device=device)
+    if torch.distributed.is_available() and torch.distributed.is_initialized():
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        torch.distributed.all_reduce(w, op=torch.distributed.ReduceOp.SUM)
+    return [float(x) for x in t.tolist()], [float(x) for x in w.tolist()]
+
+
 def run_reference(args, rank):
     """The reference arm: the reference's own compiled cpu.c on all host cores."""
     import multiprocessing as mp
@@ -206,7 +223,7 @@ def run_ours(args, rank, world, local):
     else:
         torch.cuda.set_device(local)
     # one independent replica per rank: same array and scene, own noise seed
-    p = g.workload_problem(args.workload, scene_seed=1, noise_seed=2 + rank, array_seed=3)
+    p = g.workload_problem(args.workload, **replica_seeds(rank))
     prec = {"fp32": g.PREC_FP32, "split16": g.PREC_SPLIT16, "tf32": g.PREC_TF32}[args.precision]
     rec = g.Reconstructor(local)
     rec.set_problem(p)
@@ -260,13 +277,8 @@ def run_ours(args, rank, world, local):
         e2e_s += time.perf_counter() - t0
         e2e_flops += rec.last_run_stats()[1]
 
-    t = torch.tensor([dev_ms, e2e_s], dtype=torch.float64, device=f"cuda:{local}")
-    fsum = torch.tensor([flops, e2e_flops], dtype=torch.float64, device=f"cuda:{local}")
-    if dist:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        torch.distributed.all_reduce(fsum, op=torch.distributed.ReduceOp.SUM)
-    max_ms, max_e2e = float(t[0]), float(t[1])
-    tot_flops, tot_e2e_flops = float(fsum[0]), float(fsum[1])
+    (max_ms, max_e2e), (tot_flops, tot_e2e_flops) = combine_over_ranks(
+        [dev_ms, e2e_s], [flops, e2e_flops], f"cuda:{local}")
 
     if rank == 0:
         hbm, tflops_peak, peak_kind = _peaks()
@@ -322,7 +334,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="precision")
-    ap.add_argument("--precision", default=os.environ.get("GPAIR_BENCH_PRECISION", "fp32"),
+    ap.add_argument("--precision", default=os.environ.get("GPAIR_BENCH_PRECISION", "split16"),
                     choices=["fp32", "split16", "tf32"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--host-loop", action="store_true",
