@@ -78,13 +78,17 @@ class OiData(C.Structure):
 class CgParams(C.Structure):
     _fields_ = [("method", C.c_int), ("iterations", C.c_int), ("alpha", C.c_float), ("minvalue", C.c_double),
                 ("wolfe1", C.c_double), ("wolfe2", C.c_double), ("step_max", C.c_double), ("max_zoom", C.c_int),
-                ("max_bracket", C.c_int), ("resume", C.c_int), ("host_loop", C.c_int)]
+                ("max_bracket", C.c_int), ("resume", C.c_int), ("host_loop", C.c_int),
+                ("line_search", C.c_int), ("target_J", C.c_double), ("batch_step_max", C.c_double)]
+
+
+LS_WOLFE, LS_BATCH, LS_TRIALS = 0, 1, 8
 
 
 class CgResult(C.Structure):
     _fields_ = [("iterations_done", C.c_int), ("criterion_evals", C.c_int), ("grad_evals", C.c_int),
                 ("J", C.c_double), ("chi2", C.c_double), ("entropy", C.c_double), ("last_step", C.c_double),
-                ("last_beta", C.c_double), ("status", C.c_int)]
+                ("last_beta", C.c_double), ("status", C.c_int), ("reached", C.c_int)]
 
 
 _lib: Optional[C.CDLL] = None
@@ -471,7 +475,7 @@ class Reconstructor:
         self._c(self._L.gpair_cg_run(self.h, C.byref(prm), C.byref(res), *ptrs))
         out = {"iterations": res.iterations_done, "criterion_evals": res.criterion_evals,
                "grad_evals": res.grad_evals, "J": res.J, "chi2": res.chi2, "entropy": res.entropy,
-               "last_step": res.last_step, "last_beta": res.last_beta}
+               "last_step": res.last_step, "last_beta": res.last_beta, "reached": bool(res.reached)}
         if trace:
             out.update(zip(("trace_J", "trace_chi2", "trace_entropy", "trace_step", "trace_beta"), tr))
         return out

@@ -16,6 +16,16 @@
 // sets the three conditions with cudaGraphSetConditional. Loops are bounded:
 // the iteration count by run_limit, the trials by the controller's bracket
 // and zoom caps.
+//
+// With the batched line search (GPAIR_LS_BATCH) the inner loop body is one
+// batched evaluation of GPAIR_LS_TRIALS trial images and there is no gradient
+// branch:
+//
+//   WHILE (h_iter)
+//     [pre ] as above
+//     WHILE (h_ls)
+//       [batch] trial images, batched forward DFT, chi2 of each, controller
+//     [post] as above
 #include <stdlib.h>
 #include <string.h>
 
@@ -28,6 +38,7 @@ struct CgGraph {
     cudaGraph_t g;
     cudaGraphExec_t exec;
     int precision;
+    int ls_mode;
     double *trace;
     int trace_cap;
     int n_pre, n_crit, n_grad, n_post;  // kernel launches per sequence
@@ -53,8 +64,13 @@ static int emit(gpair_ctx *c, CgGraph *G, int seq, cudaGraphConditionalHandle hi
         rc = gp_descent_dir(c, 1, 0.0);
         break;
     case SEQ_CRIT:
-        c->fuse_ctrl = CTRL_AFTER_CRIT;
-        rc = gp_eval_criterion(c, GPAIR_IMG_TEMP, 1);
+        if (G->ls_mode == GPAIR_LS_BATCH) {
+            c->fuse_ctrl = CTRL_AFTER_BATCH;
+            rc = gp_eval_batch(c);
+        } else {
+            c->fuse_ctrl = CTRL_AFTER_CRIT;
+            rc = gp_eval_criterion(c, GPAIR_IMG_TEMP, 1);
+        }
         break;
     case SEQ_GRAD:
         c->fuse_ctrl = CTRL_AFTER_GRAD;
@@ -121,17 +137,22 @@ static cudaGraphNode_t add_conditional(gpair_ctx *c, cudaGraph_t parent, cudaGra
     return n;
 }
 
-static int build(gpair_ctx *c, int trace_cap)
+static int build(gpair_ctx *c, int trace_cap, int ls_mode)
 {
     gp_cg_graph_free(c);
     if (c->precision != GPAIR_PREC_FP32) {
         int rc = gp_tc_prepare(c);  // operand buffers must exist before capture
         if (rc) return rc;
     }
+    if (ls_mode == GPAIR_LS_BATCH) {
+        int rc = gp_batch_alloc(c);
+        if (rc) return rc;
+    }
     CgGraph *G = (CgGraph *)calloc(1, sizeof(CgGraph));
     if (!G) return GPAIR_ERR_ALLOC;
     c->cg_graph = G;
     G->precision = c->precision;
+    G->ls_mode = ls_mode;
     G->trace_cap = trace_cap;
     GP_CUDA(c, cudaMalloc(&G->trace, sizeof(double) * 5 * (size_t)trace_cap));
     GP_CUDA(c, cudaGraphCreate(&G->g, 0));
@@ -144,12 +165,20 @@ static int build(gpair_ctx *c, int trace_cap)
     GP_CUDA(c, cudaGraphConditionalHandleCreate(&h_ls, B1, 0, 0));
     cudaGraphNode_t n_ls = add_conditional(c, B1, h_ls, cudaGraphCondTypeWhile, &B2, &rc);
     if (rc) return rc;
-    GP_CUDA(c, cudaGraphConditionalHandleCreate(&h_grad, B2, 0, 0));
-    cudaGraphNode_t n_if = add_conditional(c, B2, h_grad, cudaGraphCondTypeIf, &B3, &rc);
-    if (rc) return rc;
+    const bool wolfe = ls_mode != GPAIR_LS_BATCH;
+    cudaGraphNode_t n_if = nullptr;
+    h_grad = 0;
+    if (wolfe) {
+        GP_CUDA(c, cudaGraphConditionalHandleCreate(&h_grad, B2, 0, 0));
+        n_if = add_conditional(c, B2, h_grad, cudaGraphCondTypeIf, &B3, &rc);
+        if (rc) return rc;
+    }
     cudaGraph_t S[4] = {nullptr, nullptr, nullptr, nullptr};
     int *counts[4] = {&G->n_pre, &G->n_crit, &G->n_grad, &G->n_post};
-    for (int q = 0; q < 4 && !rc; q++) rc = capture(c, G, q, h_iter, h_ls, h_grad, &S[q], counts[q]);
+    for (int q = 0; q < 4 && !rc; q++) {
+        if (q == SEQ_GRAD && !wolfe) continue;
+        rc = capture(c, G, q, h_iter, h_ls, h_grad, &S[q], counts[q]);
+    }
     if (!rc) {
         cudaGraphNode_t n_pre, n_post, n_crit, n_grad;
         cudaError_t e = cudaGraphAddChildGraphNode(&n_pre, B1, nullptr, 0, S[SEQ_PRE]);
@@ -157,8 +186,10 @@ static int build(gpair_ctx *c, int trace_cap)
         if (e == cudaSuccess) e = cudaGraphAddDependencies(B1, &n_pre, &n_ls, 1);
         if (e == cudaSuccess) e = cudaGraphAddDependencies(B1, &n_ls, &n_post, 1);
         if (e == cudaSuccess) e = cudaGraphAddChildGraphNode(&n_crit, B2, nullptr, 0, S[SEQ_CRIT]);
-        if (e == cudaSuccess) e = cudaGraphAddDependencies(B2, &n_crit, &n_if, 1);
-        if (e == cudaSuccess) e = cudaGraphAddChildGraphNode(&n_grad, B3, nullptr, 0, S[SEQ_GRAD]);
+        if (wolfe) {
+            if (e == cudaSuccess) e = cudaGraphAddDependencies(B2, &n_crit, &n_if, 1);
+            if (e == cudaSuccess) e = cudaGraphAddChildGraphNode(&n_grad, B3, nullptr, 0, S[SEQ_GRAD]);
+        }
         if (e == cudaSuccess) e = cudaGraphInstantiate(&G->exec, G->g, 0);
         if (e != cudaSuccess) {
             snprintf(c->last_error, sizeof(c->last_error), "CG graph assembly: %s", cudaGetErrorString(e));
@@ -173,12 +204,12 @@ static int build(gpair_ctx *c, int trace_cap)
 
 // Launch `iterations` CG iterations as one graph. Returns the kernel launches
 // it executed through *launches (from the controller's evaluation counters).
-int gp_cg_graph_run(gpair_ctx *c, int iterations, int want_trace, long long *launches)
+int gp_cg_graph_run(gpair_ctx *c, int iterations, int want_trace, int ls_mode, long long *launches)
 {
     CgGraph *G = (CgGraph *)c->cg_graph;
     int cap = iterations > 4096 ? iterations : 4096;
-    if (!G || G->precision != c->precision || (want_trace && G->trace_cap < iterations)) {
-        int rc = build(c, cap);
+    if (!G || G->precision != c->precision || G->ls_mode != ls_mode || (want_trace && G->trace_cap < iterations)) {
+        int rc = build(c, cap, ls_mode);
         if (rc) return rc;
         G = (CgGraph *)c->cg_graph;
     }
@@ -214,10 +245,12 @@ int gp_cg_graph_trace(gpair_ctx *c, int iterations, double *tJ, double *tchi2, d
 }
 
 // kernel launches a finished graph run executed
-long long gp_cg_graph_launches(gpair_ctx *c, int iterations_done, int criterion_evals, int grad_evals)
+long long gp_cg_graph_launches(gpair_ctx *c, int iterations_done, int criterion_evals, int grad_evals, int batches)
 {
     CgGraph *G = (CgGraph *)c->cg_graph;
     if (!G) return 0;
+    long long base = (long long)iterations_done * (G->n_pre + G->n_post);
+    if (G->ls_mode == GPAIR_LS_BATCH) return base + (long long)batches * G->n_crit;
     long long trials_c = criterion_evals - iterations_done, trials_g = grad_evals - iterations_done;
-    return (long long)iterations_done * (G->n_pre + G->n_post) + trials_c * G->n_crit + trials_g * G->n_grad;
+    return base + trials_c * G->n_crit + trials_g * G->n_grad;
 }

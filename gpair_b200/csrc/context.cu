@@ -17,10 +17,10 @@
 
 int gp_default_splits(int N, int nuv);
 void gp_cg_graph_free(gpair_ctx *c);
-int gp_cg_graph_run(gpair_ctx *c, int iterations, int want_trace, long long *launches);
+int gp_cg_graph_run(gpair_ctx *c, int iterations, int want_trace, int ls_mode, long long *launches);
 int gp_cg_graph_trace(gpair_ctx *c, int iterations, double *tJ, double *tchi2, double *tS, double *tstep,
                       double *tbeta);
-long long gp_cg_graph_launches(gpair_ctx *c, int iterations_done, int criterion_evals, int grad_evals);
+long long gp_cg_graph_launches(gpair_ctx *c, int iterations_done, int criterion_evals, int grad_evals, int batches);
 
 static const char *k_err_names[] = {"GPAIR_OK",      "GPAIR_ERR_INVALID", "GPAIR_ERR_ALLOC",     "GPAIR_ERR_CUDA",
                                     "GPAIR_ERR_STATE", "GPAIR_ERR_TIMEOUT", "GPAIR_ERR_NO_DEVICE", "GPAIR_ERR_NUMERIC"};
@@ -47,6 +47,7 @@ static void free_problem(gpair_ctx *c)
     FREE_DEV(c->tri); FREE_DEV(c->phasor); FREE_DEV(c->uvc);
     FREE_DEV(c->fx); FREE_DEV(c->fy); FREE_DEV(c->vpart); FREE_DEV(c->visd); FREE_DEV(c->visi);
     FREE_DEV(c->trib); FREE_DEV(c->cw); FREE_DEV(c->inc_off); FREE_DEV(c->inc_idx); FREE_DEV(c->gpart);
+    gp_batch_free(c);
     gp_tc_free(c);
     c->have_problem = 0;
 }
@@ -57,6 +58,7 @@ static void free_images(gpair_ctx *c)
     FREE_DEV(c->image); FREE_DEV(c->image_temp); FREE_DEV(c->model);
     FREE_DEV(c->data_grad); FREE_DEV(c->entropy_grad); FREE_DEV(c->full_grad_new);
     FREE_DEV(c->full_grad); FREE_DEV(c->grad_temp); FREE_DEV(c->descent_dir);
+    gp_batch_free(c);
     c->N = 0;
     c->npix = 0;
     c->have_image = 0;
@@ -472,6 +474,9 @@ extern "C" void gpair_cg_default_params(gpair_cg_params *p)
     p->max_bracket = 100;
     p->resume = 0;
     p->host_loop = 0;
+    p->line_search = GPAIR_LS_WOLFE;
+    p->target_J = 0.0;
+    p->batch_step_max = 1e12;
 }
 
 static int read_action(gpair_ctx *c, int *action)
@@ -488,6 +493,8 @@ extern "C" int gpair_cg_run(gpair_ctx *c, const gpair_cg_params *p, gpair_cg_res
 {
     if (!c || !p || !c->have_problem) return GPAIR_ERR_STATE;
     if (p->iterations < 0 || p->method < 0 || p->method > 3) return GPAIR_ERR_INVALID;
+    if (p->line_search != GPAIR_LS_WOLFE && p->line_search != GPAIR_LS_BATCH) return GPAIR_ERR_INVALID;
+    if (!(p->target_J >= 0.0)) return GPAIR_ERR_INVALID;
     GP_CUDA(c, cudaSetDevice(c->device));
     c->fuse_ctrl = -1;
     c->fuse_handles = 0;
@@ -503,7 +510,11 @@ extern "C" int gpair_cg_run(gpair_ctx *c, const gpair_cg_params *p, gpair_cg_res
     h.c2 = p->wolfe2;
     h.step_max = p->step_max;
     h.run_limit = p->iterations;
+    h.ls_mode = p->line_search;
+    h.target_J = p->target_J;
+    h.batch_step_max = p->batch_step_max > 0.0 ? p->batch_step_max : 1e12;
     int rc;
+    if (h.ls_mode == GPAIR_LS_BATCH && (rc = gp_batch_alloc(c))) return rc;
     if (p->resume) {
         // parameters only; the iteration state of the previous run is kept
         GP_CUDA(c, cudaMemcpyAsync(&c->sc->cg, &h, offsetof(CgState, it), cudaMemcpyHostToDevice, c->stream));
@@ -521,7 +532,7 @@ extern "C" int gpair_cg_run(gpair_ctx *c, const gpair_cg_params *p, gpair_cg_res
     if (!p->host_loop) {
         // build (or reuse) the graph before the timed region
         long long dummy = 0;
-        if ((rc = gp_cg_graph_run(c, 0, want_trace, &dummy))) {
+        if ((rc = gp_cg_graph_run(c, 0, want_trace, p->line_search, &dummy))) {
             cudaEventDestroy(e0);
             cudaEventDestroy(e1);
             return rc;
@@ -532,7 +543,7 @@ extern "C" int gpair_cg_run(gpair_ctx *c, const gpair_cg_params *p, gpair_cg_res
     int status = GPAIR_OK, it = 0;
     if (!p->host_loop) {
         long long dummy = 0;
-        status = gp_cg_graph_run(c, p->iterations, want_trace, &dummy);
+        status = gp_cg_graph_run(c, p->iterations, want_trace, p->line_search, &dummy);
         goto finished;
     }
     for (it = 0; it < p->iterations && status == GPAIR_OK; it++) {
@@ -543,9 +554,13 @@ extern "C" int gpair_cg_run(gpair_ctx *c, const gpair_cg_params *p, gpair_cg_res
         c->fuse_ctrl = CTRL_AFTER_DIR;
         if ((rc = gp_descent_dir(c, 1, 0.0))) { status = rc; break; }
         int action = CG_EVAL_CRIT, trials = 0;
+        if ((rc = read_action(c, &action))) { status = rc; break; }
         while (action != CG_DONE) {
             if (++trials > 10000) { status = GPAIR_ERR_TIMEOUT; break; }
-            if (action == CG_EVAL_CRIT) {
+            if (action == CG_EVAL_BATCH) {
+                c->fuse_ctrl = CTRL_AFTER_BATCH;
+                rc = gp_eval_batch(c);
+            } else if (action == CG_EVAL_CRIT) {
                 c->fuse_ctrl = CTRL_AFTER_CRIT;
                 rc = gp_eval_criterion(c, GPAIR_IMG_TEMP, 1);
             } else {
@@ -560,7 +575,7 @@ extern "C" int gpair_cg_run(gpair_ctx *c, const gpair_cg_params *p, gpair_cg_res
             status = rc;
             break;
         }
-        if (tJ || tchi2 || tS || tstep || tbeta || it == p->iterations - 1) {
+        if (tJ || tchi2 || tS || tstep || tbeta || it == p->iterations - 1 || p->target_J > 0.0) {
             if ((rc = gp_sync_scalars(c))) { status = rc; break; }
             const CgState &s = c->sc_host->cg;
             if (tJ) tJ[it] = s.J;
@@ -569,6 +584,7 @@ extern "C" int gpair_cg_run(gpair_ctx *c, const gpair_cg_params *p, gpair_cg_res
             if (tstep) tstep[it] = s.sel;
             if (tbeta) tbeta[it] = s.beta;
             if (c->sc_host->nonfinite) { status = GPAIR_ERR_NUMERIC; it++; break; }
+            if (s.reached) { it++; break; }
         }
         rc = 0;
     }
@@ -587,7 +603,7 @@ finished:
         it = s.run_it;
         if (want_trace && !status) status = gp_cg_graph_trace(c, it, tJ, tchi2, tS, tstep, tbeta);
         if (!status && c->sc_host->nonfinite) status = GPAIR_ERR_NUMERIC;
-        c->launches = launches0 + gp_cg_graph_launches(c, it, s.criterion_evals, s.grad_evals);
+        c->launches = launches0 + gp_cg_graph_launches(c, it, s.criterion_evals, s.grad_evals, s.batches);
     }
     c->last_ms = ms;
     double per = 4.0 * (double)c->npix * c->nuv + 8.0 * c->N * (double)c->nuv;
@@ -603,6 +619,7 @@ finished:
         res->last_step = s.sel;
         res->last_beta = s.beta;
         res->status = status;
+        res->reached = s.reached;
     }
     return status;
 }

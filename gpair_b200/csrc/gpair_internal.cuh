@@ -39,14 +39,24 @@ enum {
 };
 
 // CG line-search actions decided on the device
-enum { CG_EVAL_CRIT = 1, CG_EVAL_GRAD = 2, CG_DONE = 3 };
+enum { CG_EVAL_CRIT = 1, CG_EVAL_GRAD = 2, CG_DONE = 3, CG_EVAL_BATCH = 4 };
 enum { CG_PH_BRACKET = 0, CG_PH_ZOOM = 1 };
+
+// batched line search (GPAIR_LS_BATCH)
+#define GP_NTR GPAIR_LS_TRIALS  // trial images per batched evaluation
+#define GP_LS_RATIO 4.0         // step ratio of the geometric grid
+#define GP_LS_MAX_ROUNDS 6      // grid shifts + refine per iteration
+#define GP_LS_MAX_PTS (GP_LS_MAX_ROUNDS * GP_NTR)
+enum { BR_GRID = 0, BR_REFINE = 1 };
 
 struct CgState {
     // parameters
     int method, max_zoom, max_bracket;
     int run_limit;  // iterations this run performs (graph-captured runs)
     double alpha, minvalue, c1, c2, step_max;
+    int ls_mode;            // GPAIR_LS_WOLFE / GPAIR_LS_BATCH
+    double target_J;        // stop once the current image has J <= target_J (0: off)
+    double batch_step_max;  // largest batched trial step
     // per iteration
     int it;
     double J, chi2, entropy, beta, wolfe1;
@@ -60,6 +70,13 @@ struct CgState {
     // counters
     int criterion_evals, grad_evals;
     int run_it;  // iterations completed in this run
+    int batches;  // batched trial evaluations in this run
+    int reached;  // target objective reached
+    // batched line search
+    int bphase, bround, npts, force_sd;
+    double s_c;
+    double ts[GP_NTR];                 // steps of the batch being evaluated
+    double pts_s[GP_LS_MAX_PTS], pts_J[GP_LS_MAX_PTS];  // points evaluated this iteration
 };
 
 struct DevScalars {
@@ -78,6 +95,10 @@ struct DevScalars {
     unsigned int counter[RED_NSLOTS];
     unsigned int nonfinite;  // set when a NaN/Inf reaches a reduction
     unsigned int tc_err;     // tensor-core kernels: bounded wait gave up (bit = which wait)
+    // batched trials: per-trial flux, entropy, chi2 and tensor forward scale
+    double t_flux[GP_NTR], t_invflux[GP_NTR], t_entropy[GP_NTR], t_chi2[GP_NTR];
+    float t_scale[GP_NTR];
+    unsigned int t_counter[GP_NTR + 1];
     CgState cg;
 };
 
@@ -138,6 +159,13 @@ struct gpair_ctx {
     int st_n;
     double stage_ms[8];
     int stage_cnt[8];
+
+    // batched line-search trials: GP_NTR trial images, partial visibilities
+    // vpart_b[GP_NTR * epp][K] (epp row-tile entries per trial), reduction partials
+    float *image_trials;
+    float2 *vpart_b;
+    double *partials_b;
+    int epp;  // forward partial entries per trial image
 
     // graph-captured CG (cg_graph.cu)
     void *cg_graph;
@@ -209,7 +237,16 @@ int gp_sync_scalars(gpair_ctx *c);
 
 enum { GRAD_FUSED = 0, GRAD_DATA_ONLY = 1 };
 enum { CTRL_BEGIN = 0, CTRL_AFTER_DIR = 1, CTRL_AFTER_CRIT = 2, CTRL_AFTER_GRAD = 3, CTRL_INIT = 4, CTRL_RESUME = 5,
-       CTRL_END = 6 };
+       CTRL_END = 6, CTRL_AFTER_BATCH = 7 };
+
+// batched line-search trials (kernels_core.cu / umma_dft.cu)
+int gp_batch_alloc(gpair_ctx *c);
+void gp_batch_free(gpair_ctx *c);
+int gp_eval_batch(gpair_ctx *c);
+int gp_tc_batch_prepare(gpair_ctx *c, int *epp);
+int gp_trials_prep_launch(gpair_ctx *c, void *hi, void *lo, int Lpad, int Kx_pad, int tw_log2);
+int gp_tc_trials_prep_split(gpair_ctx *c, double *partials);
+int gp_tc_forward_batch_gemm(gpair_ctx *c);
 
 // tensor-core path (umma_dft.cu); return GPAIR_ERR_STATE when unavailable
 int gp_tc_prepare(gpair_ctx *c);

@@ -25,6 +25,7 @@
 //                    CG vectors and the line-search state machine of
 //                    gpair1/trunk/gpair.c:682-915 and gpair1/trunk/gpu.c:1947-2065,
 //                    with FP64 scalars that stay on the device.
+#include <cuda_fp16.h>
 #include <math.h>
 #include <string.h>
 
@@ -210,6 +211,9 @@ __global__ void __launch_bounds__(256) k_fwd_simt(const float *__restrict__ img,
     __shared__ float2 red[16][FB_K + 1];
     const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
     const int k0 = blockIdx.x * FB_K, y0 = blockIdx.y * FB_M;
+    // batched trials: image z of a stack, partials of image z after those of images < z
+    img += (size_t)blockIdx.z * N * N;
+    vpart += (size_t)blockIdx.z * gridDim.y * nuv;
     float2 acc[4][2];
 #pragma unroll
     for (int r = 0; r < 4; r++) acc[r][0] = acc[r][1] = make_float2(0.f, 0.f);
@@ -795,6 +799,207 @@ int gp_update_temp(gpair_ctx *c, double step, double minval, int clamp)
     return GPAIR_OK;
 }
 
+// ------------------------------------------- batched line-search trials
+
+// GP_NTR trial images I_j = max(I + s_j d, minval) (s_j = cg.ts[j], blockIdx.y
+// = j), each with its flux and entropy summed in FP64 (the trial part of
+// kernel_update_tempimage.cl + kernel_entropy_gs.cl, for a whole batch). On the
+// tensor path (hi != nullptr) the f16 hi/lo forward operand of trial j is
+// written to rows [j Lpad, j Lpad + N) with the power-of-two scale of the
+// bound max|I_j| <= max|I| + |s_j| max|d|.
+__global__ void __launch_bounds__(GP_THREADS) k_trials_prep(const float *__restrict__ img,
+                                                            const float *__restrict__ d, float *__restrict__ trials,
+                                                            const float *__restrict__ model, int N, int npix,
+                                                            __half *__restrict__ hi, __half *__restrict__ lo,
+                                                            int Lpad, int Kx_pad, int tw_log2,
+                                                            double *__restrict__ partials,
+                                                            DevScalars *__restrict__ sc)
+{
+    __shared__ double smem[2 * 32];
+    const int j = blockIdx.y;
+    const double s = sc->cg.ts[j], minval = sc->cg.minvalue;
+    int ex = 0;
+    float scale = 1.f;
+    if (hi) {
+        double bound = sc->imax_curr + fabs(s) * (double)__uint_as_float(sc->dmax_bits);
+        if (bound < minval) bound = minval;
+        frexp(bound, &ex);
+        scale = ldexpf(1.f, 15 - ex);
+    }
+    float *dst = trials + (size_t)j * npix;
+    double acc[2] = {0.0, 0.0};
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
+        double t = (double)img[p] + s * (double)d[p];
+        if (t < minval) t = minval;
+        const float I = (float)t;
+        dst[p] = I;
+        const double Id = I, m = model[p];
+        acc[0] += Id;
+        acc[1] += (Id > 0.0 && m > 0.0) ? (Id - m - Id * log(Id / m)) : -m;
+        if (hi) {
+            const int y = p / N, x = p - y * N;
+            const float v = I * scale;
+            const __half h = __float2half_rn(v);
+            const size_t o = ((size_t)j * Lpad + y) * Kx_pad + x;
+            hi[o] = h;
+            lo[o] = __float2half_rn(v - __half2float(h));
+        }
+    }
+    block_sum<2>(acc, smem);
+    double *pp = partials + (size_t)j * gridDim.x * 2;
+    if (threadIdx.x == 0) {
+        pp[2 * blockIdx.x] = acc[0];
+        pp[2 * blockIdx.x + 1] = acc[1];
+    }
+    if (last_block(&sc->t_counter[j])) {
+        double o[2];
+        finish_sum<2>(pp, gridDim.x, o, smem);
+        if (threadIdx.x == 0) {
+            sc->t_flux[j] = o[0];
+            sc->t_invflux[j] = 1.0 / o[0];
+            sc->t_entropy[j] = o[1];
+            sc->t_scale[j] = hi ? ldexpf(1.f, ex - 15 - tw_log2) : 1.f;
+            sc->t_counter[j] = 0;
+        }
+    }
+}
+
+// chi2 of every trial of a batch (blockIdx.y = trial): V = (sum of the trial's
+// epp partial entries) / F_j, then V2 and T3 residuals as in k_vis_data; mock
+// data and adjoint weights are not needed for trials. The last block of the
+// whole grid sums each trial's partials in block order and runs the controller.
+__global__ void __launch_bounds__(GP_THREADS) k_vis_chi2_batch(const float2 *__restrict__ vpart, int epp, int nuv,
+                                                               int npow, int nbis, const float *__restrict__ data,
+                                                               const float *__restrict__ data_err,
+                                                               const int4 *__restrict__ tri,
+                                                               const float2 *__restrict__ phasor,
+                                                               double *__restrict__ partials,
+                                                               DevScalars *__restrict__ sc, FusedCtrl fc)
+{
+    __shared__ double smem[32];
+    const int j = blockIdx.y;
+    const double invF = sc->t_invflux[j];
+    const float2 *vp = vpart + (size_t)j * epp * nuv;
+    double chi[1] = {0.0};
+    const int nitems = npow + nbis;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nitems; i += gridDim.x * blockDim.x) {
+        if (i < npow) {
+            double2 V = sum_vpart(vp, epp, nuv, i, invF);
+            double m2 = V.x * V.x + V.y * V.y;
+            double r = (m2 - (double)data[i]) * data_err[i];
+            chi[0] += r * r;
+        } else {
+            const int t = i - npow;
+            int4 q = tri[t];
+            double2 va = sum_vpart(vp, epp, nuv, q.x, invF);
+            double2 vb = sum_vpart(vp, epp, nuv, q.y, invF);
+            double2 vc = sum_vpart(vp, epp, nuv, q.z, invF);
+            if (q.w & 1) va = cconj(va);
+            if (q.w & 2) vb = cconj(vb);
+            if (q.w & 4) vc = cconj(vc);
+            float2 phf = phasor[t];
+            double2 t3 = cmul(cmul(cmul(va, vb), vc), make_double2(phf.x, phf.y));
+            const int r0 = npow + 2 * t;
+            double rre = (t3.x - (double)data[r0]) * data_err[r0];
+            double rim = (t3.y - (double)data[r0 + 1]) * data_err[r0 + 1];
+            chi[0] += rre * rre + rim * rim;
+        }
+    }
+    block_sum<1>(chi, smem);
+    if (threadIdx.x == 0) partials[(size_t)j * gridDim.x + blockIdx.x] = chi[0];
+    if (last_block_of(&sc->t_counter[GP_NTR], gridDim.x * gridDim.y)) {
+        for (int jj = 0; jj < (int)gridDim.y; jj++) {
+            double out[1];
+            finish_sum<1>(partials + (size_t)jj * gridDim.x, gridDim.x, out, smem);
+            if (threadIdx.x == 0) sc->t_chi2[jj] = out[0];
+        }
+        if (threadIdx.x == 0) {
+            sc->t_counter[GP_NTR] = 0;
+            run_fused_ctrl(sc, fc);
+        }
+    }
+}
+
+static int batch_blocks_per_trial(gpair_ctx *c)
+{
+    int g = gp_cdiv(c->npix, GP_THREADS * 2);
+    if (g > 256) g = 256;
+    return g < 1 ? 1 : g;
+}
+
+int gp_batch_alloc(gpair_ctx *c)
+{
+    if (c->image_trials) return GPAIR_OK;
+    const int mt_simt = gp_cdiv(c->N, FB_M);
+    int epp_tc = 0;
+    if (c->precision != GPAIR_PREC_FP32) {
+        int rc = gp_tc_batch_prepare(c, &epp_tc);
+        if (rc) return rc;
+    }
+    const int epp_max = mt_simt > epp_tc ? mt_simt : epp_tc;
+    GP_CUDA(c, cudaMalloc(&c->image_trials, sizeof(float) * (size_t)GP_NTR * c->npix));
+    GP_CUDA(c, cudaMalloc(&c->vpart_b, sizeof(float2) * (size_t)GP_NTR * epp_max * (c->nuv ? c->nuv : 1)));
+    GP_CUDA(c, cudaMalloc(&c->partials_b, sizeof(double) * (size_t)GP_NTR * 1024 * 2));
+    return GPAIR_OK;
+}
+
+void gp_batch_free(gpair_ctx *c)
+{
+    if (c->image_trials) cudaFree(c->image_trials);
+    if (c->vpart_b) cudaFree(c->vpart_b);
+    if (c->partials_b) cudaFree(c->partials_b);
+    c->image_trials = nullptr;
+    c->vpart_b = nullptr;
+    c->partials_b = nullptr;
+}
+
+int gp_trials_prep_launch(gpair_ctx *c, void *hi, void *lo, int Lpad, int Kx_pad, int tw_log2)
+{
+    dim3 g(batch_blocks_per_trial(c), GP_NTR);
+    k_trials_prep<<<g, GP_THREADS, 0, c->stream>>>(c->image, c->descent_dir, c->image_trials, c->model, c->N, c->npix,
+                                                  (__half *)hi, (__half *)lo, Lpad, Kx_pad, tw_log2, c->partials_b,
+                                                  c->sc);
+    GP_LAUNCH_CHECK(c);
+    return GPAIR_OK;
+}
+
+// One batched evaluation: GP_NTR trial images -> forward DFTs -> chi2 of each,
+// then the controller (fused into the last block of the chi2 kernel).
+int gp_eval_batch(gpair_ctx *c)
+{
+    int rc = gp_batch_alloc(c);
+    if (rc) return rc;
+    int epp;
+    gp_stage_begin(c, 0);
+    if (c->precision != GPAIR_PREC_FP32) {
+        if ((rc = gp_tc_trials_prep_split(c, c->partials_b))) return rc;
+        gp_stage_end(c);
+        gp_stage_begin(c, 1);
+        if ((rc = gp_tc_forward_batch_gemm(c))) return rc;
+        epp = c->epp;
+    } else {
+        if ((rc = gp_trials_prep_launch(c, nullptr, nullptr, 0, 0, 0))) return rc;
+        gp_stage_end(c);
+        gp_stage_begin(c, 1);
+        epp = gp_cdiv(c->N, FB_M);
+        dim3 grid(gp_cdiv(c->nuv, FB_K), epp, GP_NTR);
+        k_fwd_simt<<<grid, 256, 0, c->stream>>>(c->image_trials, c->fx, c->fy, c->N, c->nuv, c->vpart_b);
+        GP_LAUNCH_CHECK(c);
+    }
+    gp_stage_end(c);
+    gp_stage_begin(c, 2);
+    int nb = gp_cdiv(c->npow + c->nbis, GP_THREADS * 2);
+    if (nb > 1024) nb = 1024;
+    if (nb < 1) nb = 1;
+    dim3 g(nb, GP_NTR);
+    k_vis_chi2_batch<<<g, GP_THREADS, 0, c->stream>>>(c->vpart_b, epp, c->nuv, c->npow, c->nbis, c->data,
+                                                      c->data_err, c->tri, c->phasor, c->partials_b, c->sc,
+                                                      take_fused_ctrl(c));
+    GP_LAUNCH_CHECK(c);
+    gp_stage_end(c);
+    return GPAIR_OK;
+}
+
 // ------------------------------------------------------- CG controller
 
 __device__ void cg_zoom_next(CgState &s)
@@ -827,6 +1032,90 @@ __device__ void cg_zoom_enter(CgState &s, double lo, double hi, double J_lo)
     cg_zoom_next(s);
 }
 
+// Batched line search: a grid of GP_NTR steps s_c R^(j-3), R = GP_LS_RATIO
+__device__ void ls_batch_grid(CgState &s)
+{
+    for (int j = 0; j < GP_NTR; j++) {
+        double t = s.s_c * pow(GP_LS_RATIO, (double)(j - 3));
+        s.ts[j] = t < s.batch_step_max ? t : s.batch_step_max;
+    }
+    s.action = CG_EVAL_BATCH;
+}
+
+__device__ void ls_batch_accept(CgState &s, double sb, double Jb)
+{
+    s.sel = sb;
+    s.Jt = Jb;
+    if (sb > 0.0) s.s_c = sb;
+    s.action = CG_DONE;
+}
+
+// After a batch: record its points, then shift the grid (no decrease yet, or
+// the best step is the largest tried), refine inside the bracket of the best
+// point, or accept the best point.
+__device__ void ls_batch_after(DevScalars *__restrict__ sc, CgState &s)
+{
+    for (int j = 0; j < GP_NTR; j++) {
+        double J = sc->t_chi2[j] - s.alpha * sc->t_entropy[j];
+        if (!isfinite(J)) J = INFINITY;  // a trial that overflows is never the best
+        if (s.npts < GP_LS_MAX_PTS) {
+            s.pts_s[s.npts] = s.ts[j];
+            s.pts_J[s.npts] = J;
+            s.npts++;
+        }
+    }
+    s.criterion_evals += GP_NTR;
+    s.batches++;
+    s.bround++;
+    // best point (ties: the smaller step) against the current image (s = 0)
+    int b = -1;
+    double sb = 0.0, Jb = s.J_init;
+    for (int i = 0; i < s.npts; i++) {
+        const double Ji = s.pts_J[i], si = s.pts_s[i];
+        if (Ji < Jb || (Ji == Jb && b >= 0 && si < sb)) {
+            b = i;
+            sb = si;
+            Jb = Ji;
+        }
+    }
+    if (b < 0) {
+        // no trial decreased J: move the grid below the smallest step tried
+        double smin = s.pts_s[0];
+        for (int i = 1; i < s.npts; i++) smin = fmin(smin, s.pts_s[i]);
+        if (s.bround < GP_LS_MAX_ROUNDS && smin > 1e-300) {
+            s.s_c = smin / pow(GP_LS_RATIO, 5.0);
+            ls_batch_grid(s);
+        } else {
+            s.force_sd = 1;  // restart from steepest descent next iteration
+            ls_batch_accept(s, 0.0, s.J_init);
+        }
+        return;
+    }
+    double lo = 0.0, hi = INFINITY;
+    for (int i = 0; i < s.npts; i++) {
+        const double si = s.pts_s[i];
+        if (si < sb && si > lo) lo = si;
+        if (si > sb && si < hi) hi = si;
+    }
+    if (!(hi < INFINITY)) {
+        // the largest step tried is the best: extend the grid upwards
+        if (s.bround < GP_LS_MAX_ROUNDS - 1 && sb < s.batch_step_max) {
+            s.s_c = sb * pow(GP_LS_RATIO, 4.0);
+            ls_batch_grid(s);
+        } else {
+            ls_batch_accept(s, sb, Jb);
+        }
+        return;
+    }
+    if (s.bphase == BR_GRID && s.bround < GP_LS_MAX_ROUNDS) {
+        s.bphase = BR_REFINE;
+        for (int j = 0; j < GP_NTR; j++) s.ts[j] = lo + (hi - lo) * (double)(j + 1) / (double)(GP_NTR + 1);
+        s.action = CG_EVAL_BATCH;
+        return;
+    }
+    ls_batch_accept(s, sb, Jb);
+}
+
 __device__ void cg_control(DevScalars *__restrict__ sc, int what)
 {
     CgState &s = sc->cg;
@@ -834,8 +1123,18 @@ __device__ void cg_control(DevScalars *__restrict__ sc, int what)
     case CTRL_RESUME:
         // a continued run counts its own evaluations; the iteration state is kept
         s.criterion_evals = s.grad_evals = 0;
+        s.batches = 0;
         s.run_it = 0;
+        s.reached = 0;
         sc->nonfinite = 0;
+        break;
+    case CTRL_AFTER_BATCH:
+        if (sc->tc_err) {
+            s.sel = 0.0;
+            s.action = CG_DONE;
+            break;
+        }
+        ls_batch_after(sc, s);
         break;
     case CTRL_END:
         s.run_it++;
@@ -844,10 +1143,14 @@ __device__ void cg_control(DevScalars *__restrict__ sc, int what)
         s.run_it = 0;
         s.it = 0;
         s.criterion_evals = s.grad_evals = 0;
+        s.batches = 0;
         s.beta = 0.0;
         s.sel = 0.0;
         s.prev_nn = 0.0;
         s.action = CG_EVAL_CRIT;
+        s.s_c = 1.0;
+        s.reached = 0;
+        s.force_sd = 0;
         sc->nonfinite = 0;
         break;
     case CTRL_BEGIN: {
@@ -876,12 +1179,38 @@ __device__ void cg_control(DevScalars *__restrict__ sc, int what)
             }
             if (fabs(no / nn) > 0.5) beta = 0.0;
         }
+        if (s.force_sd) {
+            beta = 0.0;
+            s.force_sd = 0;
+        }
         s.beta = beta;
         s.prev_nn = nn;
         s.it++;
+        if (s.target_J > 0.0 && s.J <= s.target_J) s.reached = 1;
         break;
     }
     case CTRL_AFTER_DIR:
+        if (s.reached) {  // target objective reached: no line search, the run ends here
+            s.sel = 0.0;
+            s.action = CG_DONE;
+            break;
+        }
+        if (s.ls_mode == GPAIR_LS_BATCH) {
+            s.wolfe1 = sc->dir_dot;
+            s.J_init = s.J;
+            s.sel = 0.0;
+            s.npts = 0;
+            s.bround = 0;
+            s.bphase = BR_GRID;
+            if (!(s.wolfe1 < 0.0)) {  // not a descent direction: restart from -g
+                s.force_sd = 1;
+                s.action = CG_DONE;
+                break;
+            }
+            if (!(s.s_c > 0.0) || !isfinite(s.s_c)) s.s_c = 1.0;
+            ls_batch_grid(s);
+            break;
+        }
         // line search initialisation (gpair.c:792-806)
         s.wolfe1 = sc->dir_dot;
         s.sel = 0.0;
@@ -990,7 +1319,8 @@ __device__ void cg_set_handles(DevScalars *__restrict__ sc, int what, cudaGraphC
     const CgState &s = sc->cg;
     switch (what) {
     case CTRL_AFTER_DIR:
-        cudaGraphSetConditional(h_ls, 1u);
+    case CTRL_AFTER_BATCH:
+        cudaGraphSetConditional(h_ls, s.action != CG_DONE ? 1u : 0u);
         break;
     case CTRL_AFTER_CRIT:
         cudaGraphSetConditional(h_grad, s.action == CG_EVAL_GRAD ? 1u : 0u);
@@ -1000,7 +1330,7 @@ __device__ void cg_set_handles(DevScalars *__restrict__ sc, int what, cudaGraphC
         cudaGraphSetConditional(h_ls, s.action != CG_DONE ? 1u : 0u);
         break;
     case CTRL_END: {
-        bool more = s.run_it < s.run_limit && !sc->nonfinite && !sc->tc_err;
+        bool more = s.run_it < s.run_limit && !sc->nonfinite && !sc->tc_err && !s.reached;
         cudaGraphSetConditional(h_iter, more ? 1u : 0u);
         break;
     }

@@ -54,6 +54,20 @@ __device__ __forceinline__ bool last_block(unsigned int *counter)
     return am_last;
 }
 
+// last_block over an explicit number of participating blocks (2-D grids)
+__device__ __forceinline__ bool last_block_of(unsigned int *counter, unsigned int nblocks)
+{
+    __shared__ bool am_last_of;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned int prev = atomicAdd(counter, 1u);
+        am_last_of = (prev == nblocks - 1);
+    }
+    __syncthreads();
+    return am_last_of;
+}
+
 // Sum NV partial vectors (layout [block][NV]) in a fixed order.
 template <int NV>
 __device__ void finish_sum(const double *partials, int nblocks, double (&out)[NV], double *smem)

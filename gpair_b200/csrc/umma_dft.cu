@@ -58,6 +58,9 @@ struct TcArgs {
     const float2 *fya, *fyr;
     int nanc;
     int N, nuv;
+    // image-side rows: lpad rows per image, partial entries of 2^elog2 rows,
+    // epp entries per image; batch: per-image scales sc->t_scale[image]
+    int lpad, elog2, epp, batch;
     const DevScalars *sc;
     float2 *vpart;
     // store epilogue
@@ -69,7 +72,11 @@ struct TcArgs {
 struct TcState {
     // A side (M = 128 rows): forward twiddles [rows_pad][Kx_pad], adjoint twiddles [xrows_pad][K2_pad]
     // B side (N = 256 rows): image [M_pad][Kx_pad], adjoint weights [M_pad][K2_pad]
+    // batched trials: GP_NTR images stacked at Lb rows each, [GP_NTR Lb][Kx_pad]
     int Kx_pad, M_pad, rows_pad, K2_pad, xrows_pad;
+    int Lb, epp_b;
+    __half *imgb_hi, *imgb_lo;
+    CUtensorMap m_imgb_hi, m_imgb_lo;
     int splits, kb_per;
     __half *img_hi, *img_lo, *fx_hi, *fx_lo, *fxt_hi, *fxt_lo, *w_hi, *w_lo;
     float2 *fya, *fyr;
@@ -247,7 +254,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 float2 an[TC_BN / 16];
 #pragma unroll
                 for (int c = 0; c < TC_BN / 16; c++) {
-                    const int j = (y0 >> 4) + c;
+                    const int j = ((y0 + 16 * c) % a.lpad) >> 4;  // anchor of the row within its image
                     an[c] = (vk && j < a.nanc) ? __ldg(&anc[j]) : make_float2(0.f, 0.f);
                 }
                 if (!umma::mbar_wait(&tfull[b], (uint32_t)(t >> 1) & 1u, TC_WAIT_BUDGET)) {
@@ -255,6 +262,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     break;
                 }
                 umma::tc_fence_after();
+                const int emask = (1 << a.elog2) - 1;
                 float sre = 0.f, sim = 0.f;
 #pragma unroll
                 for (int c = 0; c < TC_BN / 16; c++) {
@@ -271,16 +279,22 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                         w.y = w.x * rot.y + w.y * rot.x;
                         w.x = wx;
                     }
+                    if (((y0 + 16 * c + 16) & emask) == 0) {
+                        // end of a partial entry (warp-uniform): scale, combine the Re/Im
+                        // row pair, store. even row: (sum T_re F_re, sum T_re F_im);
+                        // odd row: (sum T_im F_re, sum T_im F_im)
+                        const int entry = (y0 + 16 * c) >> a.elog2;
+                        const float fs = a.batch ? a.sc->t_scale[entry / a.epp] : a.sc->fwd_inv_scale;
+                        const float re = sre * fs, im = sim * fs;
+                        const float ore = __shfl_xor_sync(0xffffffffu, re, 1);
+                        const float oim = __shfl_xor_sync(0xffffffffu, im, 1);
+                        if ((lane & 1) == 0 && vk) a.vpart[(size_t)entry * a.nuv + k] = make_float2(re - oim, im + ore);
+                        sre = 0.f;
+                        sim = 0.f;
+                    }
                 }
                 umma::tc_fence_before();
                 umma::mbar_arrive(&tempty[b]);
-                const float fs = a.sc->fwd_inv_scale;
-                sre *= fs;
-                sim *= fs;
-                // even row: (sum T_re F_re, sum T_re F_im); odd row: (sum T_im F_re, sum T_im F_im)
-                const float ore = __shfl_xor_sync(0xffffffffu, sre, 1);
-                const float oim = __shfl_xor_sync(0xffffffffu, sim, 1);
-                if ((lane & 1) == 0 && vk) a.vpart[(size_t)n * a.nuv + k] = make_float2(sre - oim, sim + ore);
             } else {
                 if (!umma::mbar_wait(&tfull[b], (uint32_t)(t >> 1) & 1u, TC_WAIT_BUDGET)) {
                     tc_fail(a.err, abort_flag, 8u);
@@ -558,7 +572,8 @@ void gp_tc_free(gpair_ctx *c)
 {
     TcState *t = (TcState *)c->tc_state;
     if (!t) return;
-    __half *bufs[] = {t->img_hi, t->img_lo, t->fx_hi, t->fx_lo, t->fxt_hi, t->fxt_lo, t->w_hi, t->w_lo};
+    __half *bufs[] = {t->img_hi, t->img_lo, t->fx_hi, t->fx_lo, t->fxt_hi, t->fxt_lo, t->w_hi, t->w_lo,
+                      t->imgb_hi, t->imgb_lo};
     for (__half *b : bufs)
         if (b) cudaFree(b);
     if (t->fya) cudaFree(t->fya);
@@ -654,6 +669,10 @@ int gp_tc_forward_gemm(gpair_ctx *c)
     a.nanc = t->nanc;
     a.N = c->N;
     a.nuv = c->nuv;
+    a.lpad = t->M_pad;  // one image, partial entries of one 256-row tile each
+    a.elog2 = 8;
+    a.epp = a.n_tiles;
+    a.batch = 0;
     a.sc = c->sc;
     a.vpart = c->vpart;
     a.err = &c->sc->tc_err;
@@ -662,6 +681,78 @@ int gp_tc_forward_gemm(gpair_ctx *c)
                                                                         t->m_img_lo, a);
     GP_LAUNCH_CHECK(c);
     c->mt = a.n_tiles;
+    return GPAIR_OK;
+}
+
+// Operand stack of the batched line-search trials: GP_NTR images of Lb rows
+// (Lb = 32, 64 or 128 for small images so that 256-row tiles hold several
+// whole images, else N rounded up to 256); partial entries of min(Lb, 256) rows.
+int gp_tc_batch_prepare(gpair_ctx *c, int *epp)
+{
+    int rc;
+    TcState *t = tc_state_ready(c, &rc);
+    if (rc) return rc;
+    if (!t->imgb_hi) {
+        const int N = c->N;
+        t->Lb = N <= 32 ? 32 : N <= 64 ? 64 : N <= 128 ? 128 : round_up(N, TC_BN);
+        const int erows = t->Lb < TC_BN ? t->Lb : TC_BN;
+        t->epp_b = t->Lb / erows;
+        const size_t rows = (size_t)GP_NTR * t->Lb, n = rows * t->Kx_pad;
+        GP_CUDA(c, cudaMalloc(&t->imgb_hi, n * sizeof(__half)));
+        GP_CUDA(c, cudaMalloc(&t->imgb_lo, n * sizeof(__half)));
+        GP_CUDA(c, cudaMemsetAsync(t->imgb_hi, 0, n * sizeof(__half), c->stream));
+        GP_CUDA(c, cudaMemsetAsync(t->imgb_lo, 0, n * sizeof(__half), c->stream));
+        if ((rc = tc_make_map(c, &t->m_imgb_hi, t->imgb_hi, (long long)rows, t->Kx_pad, TC_BN))) return rc;
+        if ((rc = tc_make_map(c, &t->m_imgb_lo, t->imgb_lo, (long long)rows, t->Kx_pad, TC_BN))) return rc;
+    }
+    c->epp = t->epp_b;
+    if (epp) *epp = t->epp_b;
+    return GPAIR_OK;
+}
+
+// trial images + their f16 operands for a batch (steps from the device state)
+int gp_tc_trials_prep_split(gpair_ctx *c, double *partials)
+{
+    (void)partials;
+    int rc;
+    TcState *t = tc_state_ready(c, &rc);
+    if (rc) return rc;
+    if ((rc = gp_tc_batch_prepare(c, nullptr))) return rc;
+    return gp_trials_prep_launch(c, t->imgb_hi, t->imgb_lo, t->Lb, t->Kx_pad, TC_TW_LOG2);
+}
+
+// forward contraction of the GP_NTR trial images in one launch: every twiddle
+// tile is loaded once for the whole batch
+int gp_tc_forward_batch_gemm(gpair_ctx *c)
+{
+    int rc;
+    TcState *t = tc_state_ready(c, &rc);
+    if (rc) return rc;
+    if ((rc = gp_tc_batch_prepare(c, nullptr))) return rc;
+    TcArgs a;
+    memset(&a, 0, sizeof(a));
+    a.m_tiles = t->rows_pad / TC_BM;
+    a.n_tiles = (GP_NTR * t->Lb) / TC_BN;
+    a.kb_total = t->Kx_pad / TC_BK;
+    a.kb_per_split = a.kb_total;
+    a.units = a.m_tiles * a.n_tiles;
+    a.fya = t->fya;
+    a.fyr = t->fyr;
+    a.nanc = t->nanc;
+    a.N = c->N;
+    a.nuv = c->nuv;
+    a.lpad = t->Lb;
+    const int erows = t->Lb < TC_BN ? t->Lb : TC_BN;
+    a.elog2 = erows == 32 ? 5 : erows == 64 ? 6 : erows == 128 ? 7 : 8;
+    a.epp = t->epp_b;
+    a.batch = 1;
+    a.sc = c->sc;
+    a.vpart = c->vpart_b;
+    a.err = &c->sc->tc_err;
+    int grid = a.units < t->nsm ? a.units : t->nsm;
+    k_tc_gemm<EPI_FWD><<<grid, TC_THREADS, TC_SMEM_BYTES, c->stream>>>(t->m_fx_hi, t->m_fx_lo, t->m_imgb_hi,
+                                                                        t->m_imgb_lo, a);
+    GP_LAUNCH_CHECK(c);
     return GPAIR_OK;
 }
 

@@ -270,7 +270,21 @@ typedef struct {
     int host_loop;    /* 0 (default): the whole run is one CUDA graph launch (conditional
                          nodes steer the line search on the device); 1: the host reads
                          the controller's decision after every trial */
+    /* ---- extensions beyond the reference's CG ---- */
+    int line_search;  /* GPAIR_LS_WOLFE (default): the reference's strong-Wolfe bracketing
+                         and zoom, one trial image per evaluation. GPAIR_LS_BATCH: every
+                         round evaluates GPAIR_LS_TRIALS trial images in one batched
+                         evaluation (a geometric grid of steps around the last accepted
+                         step, shifted until it brackets the best step, then one refine
+                         round inside the bracket); the best trial is accepted */
+    double target_J;  /* > 0: the run stops at the first iteration whose current image has
+                         J <= target_J (time-to-objective runs); 0: off */
+    double batch_step_max; /* GPAIR_LS_BATCH: largest trial step (default 1e12) */
 } gpair_cg_params;
+
+#define GPAIR_LS_WOLFE 0
+#define GPAIR_LS_BATCH 1
+#define GPAIR_LS_TRIALS 8
 
 typedef struct {
     int iterations_done;
@@ -279,6 +293,7 @@ typedef struct {
     double J, chi2, entropy; /* at the start of the last iteration */
     double last_step, last_beta;
     int status;
+    int reached;  /* 1 when the run stopped at target_J */
 } gpair_cg_result;
 
 void gpair_cg_default_params(gpair_cg_params *p);

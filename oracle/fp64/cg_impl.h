@@ -99,6 +99,129 @@ static REAL CG(zoom)(const CG(evaluator) *ev, const CG(params) *p, int n, const 
     return lo;
 }
 
+/*
+ * Batched line search (the library's GPAIR_LS_BATCH extension; the reference
+ * has no counterpart). Same CG loop and beta rules as CG(run); each line
+ * search evaluates rounds of LSB_NTR trial steps:
+ *   grid round    s_c * 4^(j-3), j = 0..7 (s_c: the last accepted step, 1 at start)
+ *   no decrease   move the grid below the smallest step tried (s_c / 4^5 of it)
+ *   best = top    move the grid above the best step (s_c = best * 4^4)
+ *   bracketed     one refine round of 8 evenly spaced steps inside (lo, hi),
+ *                 the evaluated neighbours of the best step
+ *   accept        the best step over all rounds (ties: the smaller step)
+ * at most LSB_ROUNDS rounds; a direction that is not a descent direction, or
+ * a search without any decrease, takes no step and restarts from -g.
+ */
+#ifndef LSB_NTR
+#define LSB_NTR 8
+#define LSB_ROUNDS 6
+#define LSB_RATIO 4.0
+#endif
+
+static REAL CG(batch_search)(const CG(evaluator) *ev, const CG(params) *p, int n, const REAL *img, const REAL *d,
+                             REAL J_init, double *s_c, double step_cap, int *force_sd, REAL *temp, CG(trace) *tr)
+{
+    double ts[LSB_NTR], ps[LSB_NTR * LSB_ROUNDS], pJ[LSB_NTR * LSB_ROUNDS];
+    int npts = 0, round = 0, refine = 0;
+    for (int j = 0; j < LSB_NTR; j++) {
+        double t = *s_c * pow(LSB_RATIO, (double)(j - 3));
+        ts[j] = t < step_cap ? t : step_cap;
+    }
+    for (;;) {
+        for (int j = 0; j < LSB_NTR; j++) {
+            REAL chi2, S;
+            CG(trial)(n, img, d, (REAL)ts[j], p->minvalue, temp);
+            double J = ev->criterion(ev->ctx, temp, &chi2, &S);
+            if (!isfinite(J)) J = INFINITY;
+            ps[npts] = ts[j];
+            pJ[npts] = J;
+            npts++;
+        }
+        tr->criterion_evals += LSB_NTR;
+        round++;
+        int b = -1;
+        double sb = 0.0, Jb = J_init;
+        for (int i = 0; i < npts; i++)
+            if (pJ[i] < Jb || (pJ[i] == Jb && b >= 0 && ps[i] < sb)) { b = i; sb = ps[i]; Jb = pJ[i]; }
+        if (b < 0) {
+            double smin = ps[0];
+            for (int i = 1; i < npts; i++) smin = fmin(smin, ps[i]);
+            if (round < LSB_ROUNDS && smin > 1e-300) {
+                *s_c = smin / pow(LSB_RATIO, 5.0);
+                for (int j = 0; j < LSB_NTR; j++) {
+                    double t = *s_c * pow(LSB_RATIO, (double)(j - 3));
+                    ts[j] = t < step_cap ? t : step_cap;
+                }
+                continue;
+            }
+            *force_sd = 1;
+            return 0;
+        }
+        double lo = 0.0, hi = INFINITY;
+        for (int i = 0; i < npts; i++) {
+            if (ps[i] < sb && ps[i] > lo) lo = ps[i];
+            if (ps[i] > sb && ps[i] < hi) hi = ps[i];
+        }
+        if (!(hi < INFINITY)) {
+            if (round < LSB_ROUNDS - 1 && sb < step_cap) {
+                *s_c = sb * pow(LSB_RATIO, 4.0);
+                for (int j = 0; j < LSB_NTR; j++) {
+                    double t = *s_c * pow(LSB_RATIO, (double)(j - 3));
+                    ts[j] = t < step_cap ? t : step_cap;
+                }
+                continue;
+            }
+        } else if (!refine && round < LSB_ROUNDS) {
+            refine = 1;
+            for (int j = 0; j < LSB_NTR; j++) ts[j] = lo + (hi - lo) * (double)(j + 1) / (double)(LSB_NTR + 1);
+            continue;
+        }
+        if (sb > 0.0) *s_c = sb;
+        return (REAL)sb;
+    }
+}
+
+static int CG(run_batch)(const CG(evaluator) *ev, const CG(params) *p, int n, REAL *image, CG(trace) *tr,
+                         double step_cap)
+{
+    REAL *g_new = calloc(n, sizeof(REAL)), *g_old = calloc(n, sizeof(REAL));
+    REAL *d = calloc(n, sizeof(REAL)), *temp = calloc(n, sizeof(REAL));
+    if (!g_new || !g_old || !d || !temp) return -1;
+    REAL beta = 0, chi2, S;
+    double s_c = 1.0;
+    int force_sd = 0;
+    tr->criterion_evals = tr->grad_evals = 0;
+    for (int it = 0; it < p->iterations; it++) {
+        REAL J = ev->criterion(ev->ctx, image, &chi2, &S);
+        tr->criterion_evals++;
+        ev->gradient(ev->ctx, image, g_new);
+        tr->grad_evals++;
+        if (it == 0 || p->method == 0) {
+            beta = 0.;
+        } else {
+            REAL nn = CG(dot)(n, g_new, g_new), no = CG(dot)(n, g_new, g_old), oo = CG(dot)(n, g_old, g_old);
+            if (p->method == 1) beta = nn / oo;
+            if (p->method == 2) { beta = (nn - no) / oo; if (beta < 0.) beta = 0.; }
+            if (p->method == 3) {
+                beta = (nn - no) / (CG(dot)(n, d, g_new) - CG(dot)(n, d, g_old));
+                if (beta < 0.) beta = 0.;
+            }
+            if (fabs(no / nn) > .5) beta = 0.;
+        }
+        if (force_sd) { beta = 0.; force_sd = 0; }
+        if (tr->J) { tr->J[it] = J; tr->chi2[it] = chi2; tr->entropy[it] = S; tr->beta[it] = beta; }
+        for (int i = 0; i < n; i++) d[i] = beta * d[i] - g_new[i];
+        REAL w1 = CG(dot)(n, d, g_new), sel = 0;
+        if (!(w1 < 0)) force_sd = 1;
+        else sel = CG(batch_search)(ev, p, n, image, d, J, &s_c, step_cap, &force_sd, temp, tr);
+        if (tr->step) tr->step[it] = sel;
+        CG(trial)(n, image, d, sel, p->minvalue, image);
+        memcpy(g_old, g_new, sizeof(REAL) * n);
+    }
+    free(g_new); free(g_old); free(d); free(temp);
+    return 0;
+}
+
 /* Runs p->iterations CG iterations on `image` (updated in place). */
 static int CG(run)(const CG(evaluator) *ev, const CG(params) *p, int n, REAL *image, CG(trace) *tr)
 {

@@ -311,13 +311,14 @@ static void o64_eval_gradient(void *ctx, const double *image, double *grad)
     for (int i = 0; i < n; i++) grad[i] = p->dgrad[i] - p->alpha * p->egrad[i];
 }
 
-/* Full FP64 reconstruction: `iterations` CG iterations from `image`.
+/* Full FP64 reconstruction: `iterations` CG iterations from `image`, with the
+ * reference's line search (line_search 0) or the batched search (1).
  * trace arrays (length iterations) may be NULL. Returns 0 on success. */
 int o64_reconstruct(int N, int nuv, int npow, int nbis, const float *uv, float pix, const float *data,
                     const float *data_err, const float *phasor_c64, const int64_t *uvpnt, const int16_t *sign,
                     const float *model, double alpha, int method, int iterations, double *image,
                     int *criterion_evals, int *grad_evals, double *J, double *chi2, double *entropy,
-                    double *step, double *beta)
+                    double *step, double *beta, int line_search, double batch_step_max)
 {
     o64_problem p = {N, nuv, npow, nbis, uv, pix, data, data_err, NULL, uvpnt, sign, model, alpha};
     double *ph = malloc(sizeof(double) * 2 * (nbis ? nbis : 1));
@@ -330,7 +331,8 @@ int o64_reconstruct(int N, int nuv, int npow, int nbis, const float *uv, float p
     o64_evaluator ev = {&p, o64_eval_criterion, o64_eval_gradient};
     o64_params prm = {method, iterations, 1e-8, 1e-4, 0.1, 100., 200};
     o64_trace tr = {0, 0, J, chi2, entropy, step, beta};
-    int rc = o64_run(&ev, &prm, N * N, image, &tr);
+    int rc = line_search == 1 ? o64_run_batch(&ev, &prm, N * N, image, &tr, batch_step_max)
+                              : o64_run(&ev, &prm, N * N, image, &tr);
     *criterion_evals = tr.criterion_evals;
     *grad_evals = tr.grad_evals;
     free(ph); free(p.visi); free(p.mock); free(p.egrad); free(p.dgrad);

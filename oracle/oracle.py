@@ -56,7 +56,7 @@ def fp64() -> C.CDLL:
         L.o64_evaluate.argtypes = [i, i, i, i, vp, f, vp, vp, vp, vp, vp, vp, vp, vp, vp, C.POINTER(d), vp]
         L.o64_evaluate.restype = d
         L.o64_reconstruct.argtypes = [i, i, i, i, vp, f, vp, vp, vp, vp, vp, vp, d, i, i, vp, C.POINTER(i),
-                                      C.POINTER(i), vp, vp, vp, vp, vp]
+                                      C.POINTER(i), vp, vp, vp, vp, vp, i, d]
         L.o32_ref_cg_run.argtypes = [vp, i, i, i, vp, f, i, i, vp, vp, vp, vp, vp, C.POINTER(i), C.POINTER(i), vp, vp,
                                      vp, vp, vp]
         L.o_set_threads.argtypes = [i]
@@ -203,8 +203,10 @@ def entropy_gradient64(image, model, prev=None):
     return g
 
 
-def reconstruct64(p, image, iterations, method=2, threads: int = 8):
-    """FP64 CG (reference GPU-path control flow) from `image`; returns (image, trace dict)."""
+def reconstruct64(p, image, iterations, method=2, threads: int = 8, line_search: int = 0,
+                  batch_step_max: float = 1e12):
+    """FP64 CG from `image`; returns (image, trace dict). line_search 0: the
+    reference's GPU-path control flow; 1: the batched 8-trial search."""
     L = fp64()
     L.o_set_threads(threads)
     img = np.ascontiguousarray(image, np.float64).copy()
@@ -216,7 +218,8 @@ def reconstruct64(p, image, iterations, method=2, threads: int = 8):
                                               p.sign.astype(np.int16), p.model.astype(np.float32))]
     rc = L.o64_reconstruct(p.width, p.nuv, p.npow, p.nbis, _p(uv), p.pixellation, _p(keep[0]), _p(keep[1]),
                            _p(keep[2]), _p(keep[3]), _p(keep[4]), _p(keep[5]), p.alpha, method, iterations, _p(img),
-                           C.byref(ce), C.byref(ge), *[_p(t) for t in tr])
+                           C.byref(ce), C.byref(ge), *[_p(t) for t in tr], C.c_int(line_search),
+                           C.c_double(batch_step_max))
     if rc:
         raise RuntimeError("o64_reconstruct failed")
     return img, dict(criterion_evals=ce.value, grad_evals=ge.value, J=tr[0], chi2=tr[1], entropy=tr[2], step=tr[3],

@@ -249,3 +249,61 @@ def test_graph_run_equals_host_loop_run(rec, prec):
     assert np.array_equal(img_a, img_b)
     assert np.array_equal(a["trace_J"], b["trace_J"])
     assert a["criterion_evals"] == b["criterion_evals"] and a["grad_evals"] == b["grad_evals"]
+
+
+# ------------------------------------------------ batched line search
+
+@pytest.mark.parametrize("prec", PRECISIONS)
+@pytest.mark.parametrize("name,seeds", [("tiny", (21, 22, 23)), ("small", (1, 2, 3))])
+def test_batched_line_search_matches_fp64(rec, prec, name, seeds):
+    """GPAIR_LS_BATCH: 8 trial images per batched evaluation. The trial steps are
+    computed by the same FP64 rules on the device and in the oracle, so the
+    accepted steps agree exactly while no two trials tie within rounding."""
+    p = _problem(name, seeds)
+    rec.set_problem(p)
+    rec.set_precision(prec)
+    img0 = p.start_image()
+    iters = 6
+    _, tr = O.reconstruct64(p, img0, iters, line_search=1)
+    rec.set_image(img0)
+    out = rec.cg(iters, method=2, trace=True, line_search=g.LS_BATCH)
+    n = 3
+    assert np.allclose(out["trace_J"][:n], tr["J"][:n], rtol=1e-5)
+    assert np.allclose(out["trace_step"][:n], tr["step"][:n], rtol=1e-12)
+    assert np.all(np.diff(out["trace_J"]) <= 0)  # the best trial never increases J
+    assert abs(out["trace_J"][-1] - tr["J"][-1]) / abs(tr["J"][-1]) < 1e-3
+    assert out["criterion_evals"] % g.LS_TRIALS == iters % g.LS_TRIALS
+
+
+@pytest.mark.parametrize("prec", PRECISIONS)
+def test_batched_graph_equals_host_loop(rec, prec):
+    p = _problem("tiny", (12, 13, 14))
+    rec.set_problem(p)
+    rec.set_precision(prec)
+    rec.set_image(p.start_image())
+    a = rec.cg(5, method=2, trace=True, line_search=g.LS_BATCH)
+    img_a = rec.get_image()
+    rec.set_image(p.start_image())
+    b = rec.cg(5, method=2, trace=True, line_search=g.LS_BATCH, host_loop=1)
+    img_b = rec.get_image()
+    assert np.array_equal(img_a, img_b)
+    assert np.array_equal(a["trace_J"], b["trace_J"])
+    assert a["criterion_evals"] == b["criterion_evals"]
+
+
+@pytest.mark.parametrize("ls", [0, 1])
+def test_target_objective_stops_the_run(rec, ls):
+    p = _problem("tiny", (12, 13, 14))
+    rec.set_problem(p)
+    rec.set_precision(g.PREC_SPLIT16)
+    rec.set_image(p.start_image())
+    full = rec.cg(12, method=2, trace=True, line_search=ls)
+    target = float(full["trace_J"][5])
+    for host_loop in (0, 1):
+        rec.set_image(p.start_image())
+        out = rec.cg(12, method=2, trace=True, line_search=ls, target_J=target, host_loop=host_loop)
+        assert out["reached"]
+        # stops in the iteration whose current image first has J <= target
+        first = int(np.argmax(full["trace_J"] <= target))
+        assert out["iterations"] == first + 1
+        assert out["trace_J"][first] <= target

@@ -215,3 +215,16 @@ def test_fp64_cg_decreases_objective_and_matches_float_reference_cg(tiny):
     assert np.allclose(tr32["J"][:3], tr64["J"][:3], rtol=1e-4)
     assert np.allclose(tr32["step"][:3], tr64["step"][:3], rtol=1e-3)
     assert tr32["J"][-1] < tr32["J"][0]
+
+
+def test_batched_line_search_oracle_descends_and_counts():
+    """The FP64 restatement of the batched search: J never increases, each
+    iteration costs one criterion of the current image plus whole batches of 8."""
+    import gpair_b200 as g
+    p = g.workload_problem("tiny", 21, 22, 23)
+    iters = 5
+    _, tr = O.reconstruct64(p, p.start_image(), iters, line_search=1)
+    assert np.all(np.diff(tr["J"]) <= 0)
+    assert tr["grad_evals"] == iters
+    assert (tr["criterion_evals"] - iters) % 8 == 0
+    assert np.all(tr["step"] > 0)
