@@ -79,7 +79,8 @@ class CgParams(C.Structure):
     _fields_ = [("method", C.c_int), ("iterations", C.c_int), ("alpha", C.c_float), ("minvalue", C.c_double),
                 ("wolfe1", C.c_double), ("wolfe2", C.c_double), ("step_max", C.c_double), ("max_zoom", C.c_int),
                 ("max_bracket", C.c_int), ("resume", C.c_int), ("host_loop", C.c_int),
-                ("line_search", C.c_int), ("target_J", C.c_double), ("batch_step_max", C.c_double)]
+                ("line_search", C.c_int), ("target_J", C.c_double), ("batch_step_max", C.c_double),
+                ("stop_flag", C.c_void_p)]
 
 
 LS_WOLFE, LS_BATCH, LS_TRIALS = 0, 1, 8
@@ -88,7 +89,7 @@ LS_WOLFE, LS_BATCH, LS_TRIALS = 0, 1, 8
 class CgResult(C.Structure):
     _fields_ = [("iterations_done", C.c_int), ("criterion_evals", C.c_int), ("grad_evals", C.c_int),
                 ("J", C.c_double), ("chi2", C.c_double), ("entropy", C.c_double), ("last_step", C.c_double),
-                ("last_beta", C.c_double), ("status", C.c_int), ("reached", C.c_int)]
+                ("last_beta", C.c_double), ("status", C.c_int), ("reached", C.c_int), ("stopped", C.c_int)]
 
 
 _lib: Optional[C.CDLL] = None
@@ -109,6 +110,7 @@ def lib() -> C.CDLL:
         L.gpair_destroy.argtypes = [vp]
         L.gpair_set_problem.argtypes = [vp, i, f, i, vp, i, i, vp, vp, vp, vp, vp, vp]
         L.gpair_set_precision.argtypes = [vp, i]
+        L.gpair_get_precision.argtypes = [vp]
         L.gpair_set_image.argtypes = [vp, i, vp]
         L.gpair_get_image.argtypes = [vp, i, vp]
         L.gpair_criterion.argtypes = [vp, i, C.POINTER(d), C.POINTER(d)]
@@ -129,6 +131,10 @@ def lib() -> C.CDLL:
         L.gpair_set_model.argtypes = [i, f, i, f, f, vp]
         L.gpair_dft_tables.argtypes = [i, i, vp, f, vp, vp, vp, vp, i]
         L.gpair_set_exit_on_error.argtypes = [i]
+        L.gpair_adjoint_image.argtypes = [vp, vp, vp]
+        L.gpair_stop_flag_create.argtypes = [C.POINTER(vp)]
+        L.gpair_stop_flag_reset.argtypes = [vp]
+        L.gpair_stop_flag_destroy.argtypes = [vp]
         L.gpair_global_context.restype = vp
         _declare_reference_boundary(L)
         _lib = L
@@ -434,6 +440,13 @@ class Reconstructor:
         a = self.problem.alpha if alpha is None else alpha
         self._c(self._L.gpair_gradient(self.h, which, a))
 
+    def adjoint_image(self, weights: np.ndarray) -> np.ndarray:
+        """Re sum_k w_k Fx[k][x] Fy[k][y] for complex uv weights w (length nuv)."""
+        w = np.ascontiguousarray(weights, np.complex64)
+        out = np.empty(self.problem.npix, np.float32)
+        self._c(self._L.gpair_adjoint_image(self.h, _p(w), _p(out)))
+        return out
+
     def visibilities(self) -> np.ndarray:
         v = np.empty(self.problem.nuv, np.complex64)
         self._c(self._L.gpair_get_visibilities(self.h, _p(v)))
@@ -475,7 +488,8 @@ class Reconstructor:
         self._c(self._L.gpair_cg_run(self.h, C.byref(prm), C.byref(res), *ptrs))
         out = {"iterations": res.iterations_done, "criterion_evals": res.criterion_evals,
                "grad_evals": res.grad_evals, "J": res.J, "chi2": res.chi2, "entropy": res.entropy,
-               "last_step": res.last_step, "last_beta": res.last_beta, "reached": bool(res.reached)}
+               "last_step": res.last_step, "last_beta": res.last_beta, "reached": bool(res.reached),
+               "stopped": bool(res.stopped)}
         if trace:
             out.update(zip(("trace_J", "trace_chi2", "trace_entropy", "trace_step", "trace_beta"), tr))
         return out
@@ -502,3 +516,27 @@ class Reconstructor:
         ms, fl, n = C.c_double(), C.c_double(), C.c_int()
         self._c(self._L.gpair_last_run_stats(self.h, C.byref(ms), C.byref(fl), C.byref(n)))
         return ms.value, fl.value, n.value
+
+
+class StopFlag:
+    """Device flag shared by CG runs racing to a target objective."""
+
+    def __init__(self):
+        self._L = lib()
+        h = C.c_void_p()
+        _check(self._L.gpair_stop_flag_create(C.byref(h)))
+        self.ptr = h.value
+
+    def reset(self):
+        _check(self._L.gpair_stop_flag_reset(self.ptr))
+
+    def close(self):
+        if self.ptr:
+            self._L.gpair_stop_flag_destroy(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

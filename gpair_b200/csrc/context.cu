@@ -477,6 +477,35 @@ extern "C" void gpair_cg_default_params(gpair_cg_params *p)
     p->line_search = GPAIR_LS_WOLFE;
     p->target_J = 0.0;
     p->batch_step_max = 1e12;
+    p->stop_flag = nullptr;
+}
+
+extern "C" int gpair_adjoint_image(gpair_ctx *c, const gpair_float2 *weights, float *image)
+{
+    if (!c || !c->have_problem || !weights || !image) return GPAIR_ERR_STATE;
+    GP_CUDA(c, cudaSetDevice(c->device));
+    c->last_image_src = -1;  // the evaluation state (weights, data gradient) is overwritten
+    return gp_adjoint_image(c, (const float2 *)weights, image);
+}
+
+extern "C" int gpair_stop_flag_create(int **flag)
+{
+    if (!flag) return GPAIR_ERR_INVALID;
+    if (cudaMalloc(flag, sizeof(int)) != cudaSuccess) return GPAIR_ERR_ALLOC;
+    if (cudaMemset(*flag, 0, sizeof(int)) != cudaSuccess) return GPAIR_ERR_CUDA;
+    return GPAIR_OK;
+}
+
+extern "C" int gpair_stop_flag_reset(int *flag)
+{
+    if (!flag) return GPAIR_ERR_INVALID;
+    return cudaMemset(flag, 0, sizeof(int)) == cudaSuccess ? GPAIR_OK : GPAIR_ERR_CUDA;
+}
+
+extern "C" int gpair_stop_flag_destroy(int *flag)
+{
+    if (flag) cudaFree(flag);
+    return GPAIR_OK;
 }
 
 static int read_action(gpair_ctx *c, int *action)
@@ -514,6 +543,8 @@ extern "C" int gpair_cg_run(gpair_ctx *c, const gpair_cg_params *p, gpair_cg_res
     h.target_J = p->target_J;
     h.batch_step_max = p->batch_step_max > 0.0 ? p->batch_step_max : 1e12;
     int rc;
+    // stop flag shared with racing runs (device pointer or null)
+    GP_CUDA(c, cudaMemcpyAsync(&c->sc->stop_flag, &p->stop_flag, sizeof(int *), cudaMemcpyHostToDevice, c->stream));
     if (h.ls_mode == GPAIR_LS_BATCH && (rc = gp_batch_alloc(c))) return rc;
     if (p->resume) {
         // parameters only; the iteration state of the previous run is kept
@@ -575,7 +606,7 @@ extern "C" int gpair_cg_run(gpair_ctx *c, const gpair_cg_params *p, gpair_cg_res
             status = rc;
             break;
         }
-        if (tJ || tchi2 || tS || tstep || tbeta || it == p->iterations - 1 || p->target_J > 0.0) {
+        if (tJ || tchi2 || tS || tstep || tbeta || it == p->iterations - 1 || p->target_J > 0.0 || p->stop_flag) {
             if ((rc = gp_sync_scalars(c))) { status = rc; break; }
             const CgState &s = c->sc_host->cg;
             if (tJ) tJ[it] = s.J;
@@ -584,7 +615,7 @@ extern "C" int gpair_cg_run(gpair_ctx *c, const gpair_cg_params *p, gpair_cg_res
             if (tstep) tstep[it] = s.sel;
             if (tbeta) tbeta[it] = s.beta;
             if (c->sc_host->nonfinite) { status = GPAIR_ERR_NUMERIC; it++; break; }
-            if (s.reached) { it++; break; }
+            if (s.reached || s.stopped) { it++; break; }
         }
         rc = 0;
     }
@@ -620,6 +651,7 @@ finished:
         res->last_beta = s.beta;
         res->status = status;
         res->reached = s.reached;
+        res->stopped = s.stopped;
     }
     return status;
 }

@@ -72,6 +72,7 @@ struct CgState {
     int run_it;  // iterations completed in this run
     int batches;  // batched trial evaluations in this run
     int reached;  // target objective reached
+    int stopped;  // a racing run reached the target first
     // batched line search
     int bphase, bround, npts, force_sd;
     double s_c;
@@ -99,6 +100,7 @@ struct DevScalars {
     double t_flux[GP_NTR], t_invflux[GP_NTR], t_entropy[GP_NTR], t_chi2[GP_NTR];
     float t_scale[GP_NTR];
     unsigned int t_counter[GP_NTR + 1];
+    int *stop_flag;  // shared with racing runs (device memory), or null
     CgState cg;
 };
 
@@ -240,6 +242,7 @@ enum { CTRL_BEGIN = 0, CTRL_AFTER_DIR = 1, CTRL_AFTER_CRIT = 2, CTRL_AFTER_GRAD 
        CTRL_END = 6, CTRL_AFTER_BATCH = 7 };
 
 // batched line-search trials (kernels_core.cu / umma_dft.cu)
+int gp_adjoint_image(gpair_ctx *c, const float2 *cw_host, float *out_host);
 int gp_batch_alloc(gpair_ctx *c);
 void gp_batch_free(gpair_ctx *c);
 int gp_eval_batch(gpair_ctx *c);

@@ -544,6 +544,48 @@ int gp_adj_weights_only(gpair_ctx *c)
     return GPAIR_OK;
 }
 
+// Adjoint of caller-given uv weights (already in cw): C = 0, max |c_k| for the
+// tensor path's operand scale, unit adjoint scale.
+__global__ void __launch_bounds__(GP_THREADS) k_adj_given(int nuv, const float2 *__restrict__ cw,
+                                                          double *__restrict__ partials, DevScalars *__restrict__ sc)
+{
+    __shared__ double smem[32];
+    double cmax = 0.0;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nuv; k += gridDim.x * blockDim.x) {
+        const float2 cf = cw[k];
+        cmax = fmax(cmax, fmax(fabs((double)cf.x), fabs((double)cf.y)));
+    }
+    cmax = block_max(cmax, smem);
+    if (threadIdx.x == 0) partials[blockIdx.x] = cmax;
+    if (last_block(&sc->counter[RED_ADJ])) {
+        double m = 0.0;
+        for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) m = fmax(m, __ldcg(&partials[b]));
+        m = block_max(m, smem);
+        if (threadIdx.x == 0) {
+            sc->adj_c = 0.0;
+            sc->cmax = m;
+            sc->gscale = 1.0;
+            sc->counter[RED_ADJ] = 0;
+        }
+    }
+}
+
+int gp_adjoint_image(gpair_ctx *c, const float2 *cw_host, float *out_host)
+{
+    GP_CUDA(c, cudaMemcpyAsync(c->cw, cw_host, sizeof(float2) * c->nuv, cudaMemcpyHostToDevice, c->stream));
+    int nb = gp_cdiv(c->nuv, GP_THREADS);
+    if (nb > 592) nb = 592;
+    if (nb < 1) nb = 1;
+    k_adj_given<<<nb, GP_THREADS, 0, c->stream>>>(c->nuv, c->cw, slot_partials(c, RED_ADJ), c->sc);
+    GP_LAUNCH_CHECK(c);
+    int rc = gp_adjoint_contraction(c, GPAIR_IMG_CURR);
+    if (rc) return rc;
+    if ((rc = gp_grad_finalize(c, GPAIR_IMG_CURR, GRAD_DATA_ONLY, 0.f))) return rc;
+    GP_CUDA(c, cudaMemcpyAsync(out_host, c->data_grad, sizeof(float) * c->npix, cudaMemcpyDeviceToHost, c->stream));
+    GP_CUDA(c, cudaStreamSynchronize(c->stream));
+    return GPAIR_OK;
+}
+
 int gp_adjoint(gpair_ctx *c, int which)
 {
     int rc = gp_adj_weights_only(c);
@@ -1126,6 +1168,7 @@ __device__ void cg_control(DevScalars *__restrict__ sc, int what)
         s.batches = 0;
         s.run_it = 0;
         s.reached = 0;
+        s.stopped = 0;
         sc->nonfinite = 0;
         break;
     case CTRL_AFTER_BATCH:
@@ -1150,6 +1193,7 @@ __device__ void cg_control(DevScalars *__restrict__ sc, int what)
         s.action = CG_EVAL_CRIT;
         s.s_c = 1.0;
         s.reached = 0;
+        s.stopped = 0;
         s.force_sd = 0;
         sc->nonfinite = 0;
         break;
@@ -1186,11 +1230,16 @@ __device__ void cg_control(DevScalars *__restrict__ sc, int what)
         s.beta = beta;
         s.prev_nn = nn;
         s.it++;
-        if (s.target_J > 0.0 && s.J <= s.target_J) s.reached = 1;
+        if (s.target_J > 0.0 && s.J <= s.target_J) {
+            s.reached = 1;
+            if (sc->stop_flag) atomicExch(sc->stop_flag, 1);  // tell the runs racing this one
+        } else if (sc->stop_flag && *(volatile int *)sc->stop_flag) {
+            s.stopped = 1;
+        }
         break;
     }
     case CTRL_AFTER_DIR:
-        if (s.reached) {  // target objective reached: no line search, the run ends here
+        if (s.reached || s.stopped) {  // target reached here or by a racing run: the run ends here
             s.sel = 0.0;
             s.action = CG_DONE;
             break;
@@ -1330,7 +1379,7 @@ __device__ void cg_set_handles(DevScalars *__restrict__ sc, int what, cudaGraphC
         cudaGraphSetConditional(h_ls, s.action != CG_DONE ? 1u : 0u);
         break;
     case CTRL_END: {
-        bool more = s.run_it < s.run_limit && !sc->nonfinite && !sc->tc_err && !s.reached;
+        bool more = s.run_it < s.run_limit && !sc->nonfinite && !sc->tc_err && !s.reached && !s.stopped;
         cudaGraphSetConditional(h_iter, more ? 1u : 0u);
         break;
     }

@@ -1,0 +1,138 @@
+"""CG time-to-objective: wall time until a reconstruction reaches the plain
+method's converged objective.
+
+For one problem:
+  plain      CG from the flat prior with the reference's line search, run for
+             `iters` iterations; its converged objective J* is the lowest J it
+             reached. target = J* (1 + tol), tol = 1e-4 by default.
+  T_plain    the same run again, stopped on the device as soon as the current
+             image has J <= target (gpair_cg_params.target_J).
+  T_batch    flat start, batched line search, same target.
+  T_warm     features + network inference + CG with the batched line search
+             from the predicted image, same target; if it does not reach the
+             target within `iters` iterations the flat-start batched run is
+             added (the sequential fallback) and counted.
+  T_race     the flat-start fallback runs concurrently from t = 0 in a second
+             context (own stream) while the features, the network and the
+             warm-started CG run in the first; the first run to reach the
+             target sets a shared device flag that ends the other at its next
+             iteration (gpair_cg_params.stop_flag). Time until both returned.
+All times are host wall clock around the public calls, each call synchronised
+(gpair_cg_run returns after the device finished).
+"""
+from __future__ import annotations
+
+import threading
+import time
+from typing import Dict, List, Optional
+
+import numpy as np
+
+from . import api
+
+
+def _timed_cg(rec, start, iters, line_search, target):
+    rec.set_image(start)
+    t0 = time.perf_counter()
+    out = rec.cg(iters, method=2, line_search=line_search, target_J=target)
+    return time.perf_counter() - t0, out
+
+
+def race(rec: api.Reconstructor, rec2: api.Reconstructor, p: api.Problem, net, iters: int, target: float,
+         flag: api.StopFlag) -> Dict:
+    """Warm start in `rec` against the flat prior in `rec2` (both hold problem p)."""
+    import gpair_b200 as g
+    from .warmstart import features, warm_start
+    flag.reset()
+    res: Dict = {}
+
+    def flat():
+        rec2.set_image(p.start_image())
+        res["flat"] = rec2.cg(iters, method=2, line_search=g.LS_BATCH, target_J=target, stop_flag=flag.ptr)
+
+    t0 = time.perf_counter()
+    th = threading.Thread(target=flat)
+    th.start()
+    img = warm_start(net, rec, p, features(rec, p))
+    rec.set_image(img)
+    warm = rec.cg(iters, method=2, line_search=g.LS_BATCH, target_J=target, stop_flag=flag.ptr)
+    th.join()
+    dt = time.perf_counter() - t0
+    winner = "warm" if warm["reached"] else ("flat" if res["flat"]["reached"] else "none")
+    return {"race_s": dt, "race_winner": winner, "race_warm_iters": warm["iterations"],
+            "race_flat_iters": res["flat"]["iterations"]}
+
+
+def evaluate(rec: api.Reconstructor, p: api.Problem, net=None, iters: int = 1000, tol: float = 1e-4,
+             batch_iters: Optional[int] = None, objective_from: str = "plain",
+             rec2: Optional[api.Reconstructor] = None, flag: Optional[api.StopFlag] = None) -> Dict:
+    """objective_from "plain": J* from the reference line search (the headline
+    comparison); "batch": J* from the batched line search run for batch_iters
+    iterations from the flat prior (isolates what the network adds)."""
+    import gpair_b200 as g
+    from .warmstart import features, warm_start
+    rec.set_problem(p)
+    start = p.start_image()
+    bi = batch_iters or iters
+    rec.set_image(start)
+    if objective_from == "plain":
+        ref = rec.cg(iters, method=2, trace=True, line_search=g.LS_WOLFE)
+    else:
+        ref = rec.cg(bi, method=2, trace=True, line_search=g.LS_BATCH)
+    Jstar = float(np.min(ref["trace_J"][:ref["iterations"]]))
+    target = Jstar * (1.0 + tol) if Jstar > 0 else Jstar * (1.0 - tol)
+    res = {"width": p.width, "nuv": p.nuv, "J_star": Jstar, "target": target, "objective_from": objective_from}
+    if objective_from == "plain":
+        t_plain, o_plain = _timed_cg(rec, start, iters, g.LS_WOLFE, target)
+        res.update({"plain_s": t_plain, "plain_iters": o_plain["iterations"], "plain_reached": o_plain["reached"]})
+    t_batch, o_batch = _timed_cg(rec, start, bi, g.LS_BATCH, target)
+    res.update({"batch_s": t_batch, "batch_iters": o_batch["iterations"], "batch_reached": o_batch["reached"]})
+    if net is not None:
+        t0 = time.perf_counter()
+        f = features(rec, p)
+        img = warm_start(net, rec, p, f)
+        t_net = time.perf_counter() - t0
+        t_cg, o_warm = _timed_cg(rec, img, bi, g.LS_BATCH, target)
+        fell_back = not o_warm["reached"]
+        t_fb = 0.0
+        if fell_back:
+            t_fb, _ = _timed_cg(rec, start, bi, g.LS_BATCH, target)
+        res.update({"warm_s": t_net + t_cg + t_fb, "warm_net_s": t_net, "warm_iters": o_warm["iterations"],
+                    "warm_reached": o_warm["reached"], "fallback": fell_back})
+        if rec2 is not None and flag is not None:
+            rec2.set_problem(p)
+            rec2.set_precision(rec_precision(rec))
+            res.update(race(rec, rec2, p, net, bi, target, flag))
+    return res
+
+
+def rec_precision(rec: api.Reconstructor) -> int:
+    return int(rec._L.gpair_get_precision(rec.h))
+
+
+def summarize(rows: List[Dict]) -> Dict:
+    def tot(k):
+        return float(sum(r[k] for r in rows if k in r))
+
+    out = {"problems": len(rows), "batch_s": tot("batch_s"),
+           "batch_reached": int(sum(bool(r["batch_reached"]) for r in rows))}
+    has_plain = bool(rows) and "plain_s" in rows[0]
+    if has_plain:
+        out["plain_s"] = tot("plain_s")
+        out["plain_reached"] = int(sum(bool(r["plain_reached"]) for r in rows))
+        out["speedup_batch_vs_plain"] = out["plain_s"] / max(out["batch_s"], 1e-12)
+    if rows and "warm_s" in rows[0]:
+        out["warm_s"] = tot("warm_s")
+        out["warm_reached"] = int(sum(bool(r["warm_reached"]) for r in rows))
+        out["fallbacks"] = int(sum(bool(r["fallback"]) for r in rows))
+        out["speedup_warm_vs_batch"] = out["batch_s"] / max(out["warm_s"], 1e-12)
+        if "race_s" in rows[0]:
+            out["race_s"] = tot("race_s")
+            out["race_winners"] = {w: int(sum(r["race_winner"] == w for r in rows)) for w in ("warm", "flat", "none")}
+            out["speedup_race_vs_batch"] = out["batch_s"] / max(out["race_s"], 1e-12)
+            if has_plain:
+                out["speedup_race_vs_plain"] = out["plain_s"] / max(out["race_s"], 1e-12)
+        if has_plain:
+            out["speedup_warm_vs_plain"] = out["plain_s"] / max(out["warm_s"], 1e-12)
+            out["median_ratio_warm_vs_plain"] = float(np.median([r["plain_s"] / r["warm_s"] for r in rows]))
+    return out

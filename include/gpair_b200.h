@@ -280,6 +280,11 @@ typedef struct {
     double target_J;  /* > 0: the run stops at the first iteration whose current image has
                          J <= target_J (time-to-objective runs); 0: off */
     double batch_step_max; /* GPAIR_LS_BATCH: largest trial step (default 1e12) */
+    int *stop_flag;   /* device int shared by runs racing to target_J on one device (see
+                         gpair_stop_flag_create), or NULL: the run that reaches target_J
+                         first sets it; every run that sees it set ends at its next
+                         iteration (a start-image race: a warm start against the flat
+                         prior, each in its own context and stream) */
 } gpair_cg_params;
 
 #define GPAIR_LS_WOLFE 0
@@ -294,7 +299,46 @@ typedef struct {
     double last_step, last_beta;
     int status;
     int reached;  /* 1 when the run stopped at target_J */
+    int stopped;  /* 1 when a racing run reached target_J first */
 } gpair_cg_result;
+
+/* Stop flag for racing runs: a device int, zeroed at creation and by reset. */
+int gpair_stop_flag_create(int **flag);
+int gpair_stop_flag_reset(int *flag);
+int gpair_stop_flag_destroy(int *flag);
+
+/* Adjoint DFT of uv-plane weights: image[y*N + x] = Re sum_k w_k Fx[k][x] Fy[k][y]
+ * (the dirty image of the weights). Overwrites the evaluation state of the
+ * context (a gpair_gradient call must follow a new gpair_criterion). */
+int gpair_adjoint_image(gpair_ctx *ctx, const gpair_float2 *weights, float *image);
+
+/* ---- warm-start network kernels (no counterpart in the reference) ----
+ * Building blocks of the learned warm start: a 3x3-convolution encoder/decoder
+ * trained and run by the library's own kernels. Device pointers, float NCHW
+ * activations, 3x3 weights [Cout][Cin][3][3] as bfloat16 (uint16 storage),
+ * FP32 accumulation; `stream` is a cudaStream_t (NULL: the default stream).
+ * Every call returns GPAIR_OK, GPAIR_ERR_INVALID (bad sizes) or GPAIR_ERR_CUDA. */
+int gpair_cnn_conv3x3(const float *in, const void *w_bf16, const float *bias, const float *skip, float *out, int B,
+                      int Cin, int Cout, int H, int W, int relu, void *stream);
+int gpair_cnn_conv3x3_bwd_data(const float *gout, const void *w_bf16, float *gin, int B, int Cin, int Cout, int H,
+                               int W, int accumulate, void *stream);
+int gpair_cnn_conv3x3_bwd_weight(const float *in, const float *gpre, float *dw, float *db, float *scratch,
+                                 long long scratch_floats, int B, int Cin, int Cout, int H, int W, void *stream);
+int gpair_cnn_relu_mask(const float *y, float *g, long long n, void *stream);
+int gpair_cnn_pool2(const float *in, float *out, long long BC, int H, int W, void *stream);
+int gpair_cnn_pool2_bwd(const float *gout, float *gin, long long BC, int H, int W, int accumulate, void *stream);
+int gpair_cnn_up2(const float *in, float *out, long long BC, int H, int W, void *stream);
+int gpair_cnn_up2_bwd(const float *gout, float *gin, long long BC, int H, int W, void *stream);
+int gpair_cnn_head(const float *d, const float *w, const float *bias, float *z, float *out, float *asum, int B, int C,
+                   int HW, void *stream);
+int gpair_cnn_head_bwd(const float *d, const float *w, const float *z, const float *out, const float *asum,
+                       const float *gout, float *gd, float *dw, float *scratch, int B, int C, int HW, void *stream);
+/* mode 0: loss_b = HW sum (out - t)^2; mode 1: loss_b = sum (out - t)^2 / sum t^2 */
+int gpair_cnn_mse(const float *out, const float *target, float *gout, double *loss, int B, int HW, float gscale,
+                  int mode, void *stream);
+int gpair_cnn_adam(float *p, void *p_bf16, const float *g, float *m, float *v, int n, float lr, float b1, float b2,
+                   float eps, int step, void *stream);
+int gpair_cnn_to_bf16(const float *src, void *dst, int n, void *stream);
 
 void gpair_cg_default_params(gpair_cg_params *p);
 /* Runs p->iterations CG iterations from the current image. Per-iteration

@@ -307,3 +307,46 @@ def test_target_objective_stops_the_run(rec, ls):
         first = int(np.argmax(full["trace_J"] <= target))
         assert out["iterations"] == first + 1
         assert out["trace_J"][first] <= target
+
+
+def test_adjoint_image_matches_direct_sum(rec):
+    """gpair_adjoint_image: Re sum_k w_k Fx[k][x] Fy[k][y] (tables of gpair1/trunk/gpair.c:242-243)."""
+    p = _problem("tiny", (3, 4, 5))
+    rng = np.random.default_rng(9)
+    w = (rng.standard_normal(p.nuv) + 1j * rng.standard_normal(p.nuv)) / np.sqrt(p.nuv)
+    rpmas = (np.pi / 180.0) / 3600000.0
+    x = np.arange(p.width)
+    fx = np.exp(2j * np.pi * rpmas * p.pixellation * np.outer(p.uv[:, 0].astype(np.float64), x))
+    fy = np.exp(-2j * np.pi * rpmas * p.pixellation * np.outer(p.uv[:, 1].astype(np.float64), x))
+    ref = np.real(np.einsum("k,ky,kx->yx", w.astype(np.complex64).astype(np.complex128), fy, fx)).ravel()
+    for prec in PRECISIONS:
+        rec.set_problem(p)
+        rec.set_precision(prec)
+        got = rec.adjoint_image(w)
+        assert np.abs(got - ref).max() <= 1e-5 * np.abs(ref).max()
+
+
+def test_stop_flag_ends_a_racing_run(rec):
+    p = _problem("tiny", (12, 13, 14))
+    rec.set_problem(p)
+    rec.set_precision(g.PREC_SPLIT16)
+    rec.set_image(p.start_image())
+    full = rec.cg(10, method=2, trace=True, line_search=g.LS_BATCH)
+    target = float(full["trace_J"][4])
+    flag = g.api.StopFlag()
+    try:
+        with g.Reconstructor(0) as other:
+            other.set_problem(p)
+            other.set_precision(g.PREC_SPLIT16)
+            rec.set_image(p.start_image())
+            a = rec.cg(10, method=2, line_search=g.LS_BATCH, target_J=target, stop_flag=flag.ptr)
+            assert a["reached"] and not a["stopped"]
+            other.set_image(p.start_image())
+            b = other.cg(10, method=2, line_search=g.LS_BATCH, target_J=target, stop_flag=flag.ptr)
+            assert b["stopped"] and not b["reached"] and b["iterations"] == 1
+            flag.reset()
+            other.set_image(p.start_image())
+            c = other.cg(10, method=2, line_search=g.LS_BATCH, target_J=target, stop_flag=flag.ptr)
+            assert c["reached"] and c["iterations"] == a["iterations"]
+    finally:
+        flag.close()
