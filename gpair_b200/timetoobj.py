@@ -136,3 +136,43 @@ def summarize(rows: List[Dict]) -> Dict:
             out["speedup_warm_vs_plain"] = out["plain_s"] / max(out["warm_s"], 1e-12)
             out["median_ratio_warm_vs_plain"] = float(np.median([r["plain_s"] / r["warm_s"] for r in rows]))
     return out
+
+
+def main(argv=None):
+    """Evaluate held-out problems (seeds from gpair_b200.train_warmstart.SEED_HELD_OUT):
+    the first n64 at 64x64, the next n128 at 128x128; prints one JSON summary per
+    objective definition and writes the per-problem rows with --out."""
+    import argparse
+    import json
+    import gpair_b200 as g
+    from .train_warmstart import SEED_HELD_OUT
+    from .warmstart import DEFAULT_WEIGHTS, WarmStartNet, training_case
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--n64", type=int, default=16)
+    ap.add_argument("--n128", type=int, default=8)
+    ap.add_argument("--iters", type=int, default=1000)
+    ap.add_argument("--batch-iters", type=int, default=1500)
+    ap.add_argument("--weights", default=DEFAULT_WEIGHTS)
+    ap.add_argument("--out", default=None)
+    args = ap.parse_args(argv)
+    net = WarmStartNet.load(args.weights)
+    rows = {"plain": [], "batch": []}
+    flag = api.StopFlag()
+    with g.Reconstructor(0) as rec, g.Reconstructor(0) as rec2:
+        rec.set_precision(g.PREC_SPLIT16)
+        for k in range(args.n64 + args.n128):
+            p = training_case(SEED_HELD_OUT + k, 64 if k < args.n64 else 128).problem
+            rows["plain"].append(evaluate(rec, p, net, iters=args.iters, objective_from="plain", rec2=rec2,
+                                          flag=flag))
+            rows["batch"].append(evaluate(rec, p, net, iters=args.iters, batch_iters=args.batch_iters,
+                                          objective_from="batch", rec2=rec2, flag=flag))
+    flag.close()
+    for k in ("plain", "batch"):
+        print(f"SUMMARY {k}", json.dumps(summarize(rows[k])), flush=True)
+    if args.out:
+        with open(args.out, "w") as f:
+            json.dump(rows, f)
+
+
+if __name__ == "__main__":
+    main()
