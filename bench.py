@@ -104,6 +104,9 @@ class ClockSampler:
 
 # ----------------------------------------------------------- measurements
 
+LS = {"wolfe": 0, "batch": 1}
+
+
 def _peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -260,7 +263,7 @@ def run_ours(args, rank, world, local):
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
 
     # warm-up iterations (untimed); builds the CG graph
-    rec.cg(max(args.warmup, 1), method=2, resume=False, host_loop=int(args.host_loop))
+    rec.cg(max(args.warmup, 1), method=2, resume=False, host_loop=int(args.host_loop), line_search=LS[args.line_search])
     sampler = ClockSampler(local)
     if dist:
         torch.distributed.barrier()
@@ -271,7 +274,7 @@ def run_ours(args, rank, world, local):
     for k in range(args.steps):
         flush.fill_(float(k))  # 512 MiB write: L2 (126 MB) holds none of the inputs at step start
         torch.cuda.synchronize()
-        out = rec.cg(1, method=2, resume=True, host_loop=int(args.host_loop))  # one graph launch per CG iteration
+        out = rec.cg(1, method=2, resume=True, host_loop=int(args.host_loop), line_search=LS[args.line_search])  # one graph launch per CG iteration
         ms, fl, nl = rec.last_run_stats()
         dev_ms += ms
         flops += fl
@@ -304,7 +307,7 @@ def run_ours(args, rank, world, local):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         rec.set_image(img)  # H2D of the step's input image
-        rec.cg(1, method=2, resume=True, host_loop=int(args.host_loop))
+        rec.cg(1, method=2, resume=True, host_loop=int(args.host_loop), line_search=LS[args.line_search])
         img = rec.get_image()  # D2H of the step's result
         e2e_s += time.perf_counter() - t0
         e2e_flops += rec.last_run_stats()[1]
@@ -313,11 +316,11 @@ def run_ours(args, rank, world, local):
     # tcgen05 forward launch), device-timed like the headline steps
     bat_ms, bat_flops, bat_evals = 0.0, 0.0, 0
     rec.set_image(img)
-    rec.cg(max(args.warmup, 1), method=2, resume=False, line_search=g.LS_BATCH)
+    rec.cg(max(args.warmup, 1), method=2, resume=False, line_search=g.LS_BATCH, host_loop=int(args.host_loop))
     for k in range(args.steps):
         flush.fill_(float(k))
         torch.cuda.synchronize()
-        out_b = rec.cg(1, method=2, resume=True, line_search=g.LS_BATCH)
+        out_b = rec.cg(1, method=2, resume=True, line_search=g.LS_BATCH, host_loop=int(args.host_loop))
         ms_b, fl_b, _ = rec.last_run_stats()
         bat_ms += ms_b
         bat_flops += fl_b
@@ -358,7 +361,9 @@ def run_ours(args, rank, world, local):
                           "tf32": "tf32 operands, fp32 accumulate"}[args.precision],
                 "data": "synthetic (seeded array, scene and noise; no public data set of this size)",
                 "config": {"workload": f"{args.workload}: {N}x{N} image, {p.npow} V2, {p.nbis} T3, nuv {nuv}",
-                           "step": "one PR+ CG iteration with strong-Wolfe line search (continuing)",
+                           "step": ("one PR+ CG iteration with strong-Wolfe line search (continuing)"
+                                    if args.line_search == "wolfe" else
+                                    "one PR+ CG iteration with the batched 8-trial line search (continuing)"),
                            "precision": args.precision, "evaluations": evals,
                            "l2": "flushed (512 MiB write) before every timed step, outside the timed region",
                            "parallelism": f"replicas x{world}",
@@ -391,6 +396,8 @@ def main():
                     choices=["fp32", "split16", "tf32"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-time-to-objective", action="store_true")
+    ap.add_argument("--line-search", choices=["wolfe", "batch"], default="wolfe",
+                    help="line search of the headline steps: the reference's (default) or the batched one")
     ap.add_argument("--tto-problems", type=int, default=8,
                     help="held-out warm-start problems timed for the time-to-objective block")
     ap.add_argument("--host-loop", action="store_true",
