@@ -105,6 +105,8 @@ class ClockSampler:
 # ----------------------------------------------------------- measurements
 
 LS = {"wolfe": 0, "batch": 1}
+# independent contexts' streams should map to distinct hardware queues (default 8)
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 
 def _peaks():
@@ -178,6 +180,47 @@ def combine_over_ranks(times, work, device=None):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         torch.distributed.all_reduce(w, op=torch.distributed.ReduceOp.SUM)
     return [float(x) for x in t.tolist()], [float(x) for x in w.tolist()]
+
+
+def many_instances(n: int, iters: int) -> dict:
+    """n independent reconstructions of uneven size (widths 64-256, 500-8,000 uv)
+    for `iters` batched-line-search CG iterations each: one after another, then
+    all at once through gpair_cg_run_many (each context's graph on its own
+    stream). Host wall clock; problem loading is outside both timings."""
+    import gpair_b200 as g
+    from gpair_b200.instances import instances
+    ps = instances(n)
+    recs = [g.Reconstructor(0) for _ in ps]
+    try:
+        for r, p in zip(recs, ps):
+            r.set_problem(p)
+            r.set_precision(g.PREC_SPLIT16)
+            r.set_image(p.start_image())
+        g.cg_many(recs, 1, line_search=g.LS_BATCH)  # builds every graph
+        for r, p in zip(recs, ps):
+            r.set_image(p.start_image())
+        t0 = time.perf_counter()
+        for r in recs:
+            r.cg(iters, method=2, line_search=g.LS_BATCH)
+        t_seq = time.perf_counter() - t0
+        flops = sum(r.last_run_stats()[1] for r in recs)
+        for r, p in zip(recs, ps):
+            r.set_image(p.start_image())
+        t0 = time.perf_counter()
+        res = g.cg_many(recs, iters, line_search=g.LS_BATCH)
+        t_con = time.perf_counter() - t0
+        flops_con = sum(r.last_run_stats()[1] for r in recs)
+    finally:
+        for r in recs:
+            r.close()
+    return {"instances": n, "iterations": iters,
+            "widths": {w: sum(p.width == w for p in ps) for w in (64, 128, 192, 256)},
+            "uv_range": [min(p.nuv for p in ps), max(p.nuv for p in ps)],
+            "sequential_s": t_seq, "concurrent_s": t_con, "speedup": t_seq / max(t_con, 1e-12),
+            "instances_per_s": n / max(t_con, 1e-12), "tflops_concurrent": flops_con / max(t_con, 1e-12) / 1e12,
+            "tflops_sequential": flops / max(t_seq, 1e-12) / 1e12,
+            "all_ok": all(r_["status"] == 0 for r_ in res),
+            "unit": "s (host wall clock)", "line_search": "batched"}
 
 
 def time_to_objective(n_problems: int) -> dict:
@@ -379,6 +422,8 @@ def run_ours(args, rank, world, local):
             line["cpu_baseline"] = cpu_baseline(args.workload)
         if not args.no_time_to_objective:
             line["time_to_objective"] = time_to_objective(args.tto_problems)
+        if args.instances > 0:
+            line["many_instances"] = many_instances(args.instances, args.instance_iters)
         print(json.dumps(line), flush=True)
     rec.close()
     if dist:
@@ -396,6 +441,8 @@ def main():
                     choices=["fp32", "split16", "tf32"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-time-to-objective", action="store_true")
+    ap.add_argument("--instances", type=int, default=64, help="independent reconstructions run at once (0: skip)")
+    ap.add_argument("--instance-iters", type=int, default=30)
     ap.add_argument("--line-search", choices=["wolfe", "batch"], default="wolfe",
                     help="line search of the headline steps: the reference's (default) or the batched one")
     ap.add_argument("--tto-problems", type=int, default=8,

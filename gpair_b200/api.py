@@ -133,6 +133,7 @@ def lib() -> C.CDLL:
         L.gpair_set_exit_on_error.argtypes = [i]
         L.gpair_adjoint_image.argtypes = [vp, vp, vp]
         L.gpair_stop_flag_create.argtypes = [C.POINTER(vp)]
+        L.gpair_cg_run_many.argtypes = [C.POINTER(vp), i, C.POINTER(CgParams), C.POINTER(CgResult)]
         L.gpair_stop_flag_reset.argtypes = [vp]
         L.gpair_stop_flag_destroy.argtypes = [vp]
         L.gpair_global_context.restype = vp
@@ -540,3 +541,29 @@ class StopFlag:
             self.close()
         except Exception:
             pass
+
+
+def _result_dict(res: CgResult) -> dict:
+    return {"iterations": res.iterations_done, "criterion_evals": res.criterion_evals, "grad_evals": res.grad_evals,
+            "J": res.J, "chi2": res.chi2, "entropy": res.entropy, "last_step": res.last_step,
+            "last_beta": res.last_beta, "reached": bool(res.reached), "stopped": bool(res.stopped),
+            "status": res.status}
+
+
+def cg_many(recs, iterations: int, method: int = 2, alpha: Optional[float] = None, resume: bool = False, **kw):
+    """The same CG run on several contexts at once (gpair_cg_run_many): each
+    context's graph runs on its own stream. Returns one result dict per context."""
+    L = lib()
+    n = len(recs)
+    prm = CgParams()
+    L.gpair_cg_default_params(C.byref(prm))
+    prm.method = method
+    prm.iterations = iterations
+    prm.resume = 1 if resume else 0
+    prm.alpha = recs[0].problem.alpha if alpha is None else alpha
+    for k, v in kw.items():
+        setattr(prm, k, v)
+    handles = (C.c_void_p * n)(*[r.h.value for r in recs])
+    res = (CgResult * n)()
+    _check(L.gpair_cg_run_many(handles, n, C.byref(prm), res))
+    return [_result_dict(res[i]) for i in range(n)]

@@ -517,13 +517,28 @@ static int read_action(gpair_ctx *c, int *action)
     return GPAIR_OK;
 }
 
-extern "C" int gpair_cg_run(gpair_ctx *c, const gpair_cg_params *p, gpair_cg_result *res, double *tJ, double *tchi2,
-                            double *tS, double *tstep, double *tbeta)
+// One CG run in three phases, so that several contexts can have their runs in
+// flight at once (gpair_cg_run_many): prepare (parameters, controller reset,
+// graph build, start event), launch, finish (end event, wait, results).
+struct CgRun {
+    cudaEvent_t e0, e1;
+    long long launches0;
+    int want_trace;
+};
+
+static int cg_validate(gpair_ctx *c, const gpair_cg_params *p)
 {
     if (!c || !p || !c->have_problem) return GPAIR_ERR_STATE;
     if (p->iterations < 0 || p->method < 0 || p->method > 3) return GPAIR_ERR_INVALID;
     if (p->line_search != GPAIR_LS_WOLFE && p->line_search != GPAIR_LS_BATCH) return GPAIR_ERR_INVALID;
     if (!(p->target_J >= 0.0)) return GPAIR_ERR_INVALID;
+    return GPAIR_OK;
+}
+
+static int cg_prepare(gpair_ctx *c, const gpair_cg_params *p, int want_trace, CgRun *r)
+{
+    int rc = cg_validate(c, p);
+    if (rc) return rc;
     GP_CUDA(c, cudaSetDevice(c->device));
     c->fuse_ctrl = -1;
     c->fuse_handles = 0;
@@ -542,7 +557,6 @@ extern "C" int gpair_cg_run(gpair_ctx *c, const gpair_cg_params *p, gpair_cg_res
     h.ls_mode = p->line_search;
     h.target_J = p->target_J;
     h.batch_step_max = p->batch_step_max > 0.0 ? p->batch_step_max : 1e12;
-    int rc;
     // stop flag shared with racing runs (device pointer or null)
     GP_CUDA(c, cudaMemcpyAsync(&c->sc->stop_flag, &p->stop_flag, sizeof(int *), cudaMemcpyHostToDevice, c->stream));
     if (h.ls_mode == GPAIR_LS_BATCH && (rc = gp_batch_alloc(c))) return rc;
@@ -555,28 +569,34 @@ extern "C" int gpair_cg_run(gpair_ctx *c, const gpair_cg_params *p, gpair_cg_res
         if ((rc = gp_cg_kernel(c, CTRL_INIT))) return rc;
     }
     c->st_n = 0;
-    cudaEvent_t e0, e1;
-    GP_CUDA(c, cudaEventCreate(&e0));
-    GP_CUDA(c, cudaEventCreate(&e1));
-    long long launches0 = c->launches;
-    const int want_trace = tJ || tchi2 || tS || tstep || tbeta;
+    r->want_trace = want_trace;
+    r->launches0 = c->launches;
     if (!p->host_loop) {
         // build (or reuse) the graph before the timed region
         long long dummy = 0;
-        if ((rc = gp_cg_graph_run(c, 0, want_trace, p->line_search, &dummy))) {
-            cudaEventDestroy(e0);
-            cudaEventDestroy(e1);
-            return rc;
-        }
+        if ((rc = gp_cg_graph_run(c, 0, want_trace, p->line_search, &dummy))) return rc;
         if (c->stage_timing) c->st_n = 0;
     }
-    GP_CUDA(c, cudaEventRecord(e0, c->stream));
-    int status = GPAIR_OK, it = 0;
-    if (!p->host_loop) {
-        long long dummy = 0;
-        status = gp_cg_graph_run(c, p->iterations, want_trace, p->line_search, &dummy);
-        goto finished;
+    GP_CUDA(c, cudaEventCreate(&r->e0));
+    if (cudaEventCreate(&r->e1) != cudaSuccess) {
+        cudaEventDestroy(r->e0);
+        snprintf(c->last_error, sizeof(c->last_error), "cudaEventCreate failed");
+        return GPAIR_ERR_CUDA;
     }
+    if (cudaEventRecord(r->e0, c->stream) != cudaSuccess) {
+        cudaEventDestroy(r->e0);
+        cudaEventDestroy(r->e1);
+        snprintf(c->last_error, sizeof(c->last_error), "cudaEventRecord failed");
+        return GPAIR_ERR_CUDA;
+    }
+    return GPAIR_OK;
+}
+
+// host-driven iterations (host_loop = 1): the controller's decision is read after every trial
+static int cg_host_loop(gpair_ctx *c, const gpair_cg_params *p, double *tJ, double *tchi2, double *tS, double *tstep,
+                        double *tbeta, int *it_out)
+{
+    int status = GPAIR_OK, rc, it = 0;
     for (it = 0; it < p->iterations && status == GPAIR_OK; it++) {
         // the controller steps run in the last block of the preceding reduction kernel
         if ((rc = gp_eval_criterion(c, GPAIR_IMG_CURR, 0))) { status = rc; break; }
@@ -617,29 +637,39 @@ extern "C" int gpair_cg_run(gpair_ctx *c, const gpair_cg_params *p, gpair_cg_res
             if (c->sc_host->nonfinite) { status = GPAIR_ERR_NUMERIC; it++; break; }
             if (s.reached || s.stopped) { it++; break; }
         }
-        rc = 0;
     }
-finished:
-    GP_CUDA(c, cudaEventRecord(e1, c->stream));
-    GP_CUDA(c, cudaEventSynchronize(e1));
+    *it_out = it;
+    return status;
+}
+
+static void cg_mark_end(gpair_ctx *c, CgRun *r) { cudaEventRecord(r->e1, c->stream); }
+
+static int cg_finish(gpair_ctx *c, const gpair_cg_params *p, gpair_cg_result *res, double *tJ, double *tchi2,
+                     double *tS, double *tstep, double *tbeta, CgRun *r, int status, int it)
+{
+    cudaError_t e = cudaEventSynchronize(r->e1);
     float ms = 0.f;
-    cudaEventElapsedTime(&ms, e0, e1);
+    if (e == cudaSuccess) cudaEventElapsedTime(&ms, r->e0, r->e1);
+    cudaEventDestroy(r->e0);
+    cudaEventDestroy(r->e1);
+    if (e != cudaSuccess) {
+        snprintf(c->last_error, sizeof(c->last_error), "CG run: %s", cudaGetErrorString(e));
+        return GPAIR_ERR_CUDA;
+    }
     if (c->stage_timing) stage_collect(c);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     int rc2 = gp_sync_scalars(c);
     if (rc2 && !status) status = rc2;
     const CgState &s = c->sc_host->cg;
     if (!p->host_loop) {
         it = s.run_it;
-        if (want_trace && !status) status = gp_cg_graph_trace(c, it, tJ, tchi2, tS, tstep, tbeta);
+        if (r->want_trace && !status) status = gp_cg_graph_trace(c, it, tJ, tchi2, tS, tstep, tbeta);
         if (!status && c->sc_host->nonfinite) status = GPAIR_ERR_NUMERIC;
-        c->launches = launches0 + gp_cg_graph_launches(c, it, s.criterion_evals, s.grad_evals, s.batches);
+        c->launches = r->launches0 + gp_cg_graph_launches(c, it, s.criterion_evals, s.grad_evals, s.batches);
     }
     c->last_ms = ms;
     double per = 4.0 * (double)c->npix * c->nuv + 8.0 * c->N * (double)c->nuv;
     c->last_flops = per * (s.criterion_evals + s.grad_evals);
-    c->last_launches = c->launches - launches0;
+    c->last_launches = c->launches - r->launches0;
     if (res) {
         res->iterations_done = it;
         res->criterion_evals = s.criterion_evals;
@@ -654,6 +684,72 @@ finished:
         res->stopped = s.stopped;
     }
     return status;
+}
+
+extern "C" int gpair_cg_run(gpair_ctx *c, const gpair_cg_params *p, gpair_cg_result *res, double *tJ, double *tchi2,
+                            double *tS, double *tstep, double *tbeta)
+{
+    CgRun r;
+    int rc = cg_prepare(c, p, tJ || tchi2 || tS || tstep || tbeta, &r);
+    if (rc) return rc;
+    int status, it = 0;
+    if (!p->host_loop) {
+        long long dummy = 0;
+        status = gp_cg_graph_run(c, p->iterations, r.want_trace, p->line_search, &dummy);
+    } else {
+        status = cg_host_loop(c, p, tJ, tchi2, tS, tstep, tbeta, &it);
+    }
+    cg_mark_end(c, &r);
+    return cg_finish(c, p, res, tJ, tchi2, tS, tstep, tbeta, &r, status, it);
+}
+
+extern "C" int gpair_cg_run_many(gpair_ctx **ctx, int n, const gpair_cg_params *p, gpair_cg_result *res)
+{
+    if (!ctx || !p || n <= 0 || p->host_loop) return GPAIR_ERR_INVALID;
+    for (int i = 0; i < n; i++)
+        for (int j = 0; j < i; j++)
+            if (ctx[i] == ctx[j]) return GPAIR_ERR_INVALID;  // each run needs its own context and stream
+    for (int i = 0; i < n; i++) {
+        int rc = cg_validate(ctx[i], p);
+        if (rc) return rc;
+    }
+    CgRun *r = (CgRun *)calloc((size_t)n, sizeof(CgRun));
+    int *st = (int *)calloc((size_t)n, sizeof(int));
+    if (!r || !st) {
+        free(r);
+        free(st);
+        return GPAIR_ERR_ALLOC;
+    }
+    int first_err = GPAIR_OK, prepared = 0;
+    // every run is prepared (graphs built) before any is launched: a graph
+    // capture must not overlap another context's work on the legacy stream
+    for (; prepared < n; prepared++) {
+        int rc = cg_prepare(ctx[prepared], p, 0, &r[prepared]);
+        if (rc) {
+            first_err = rc;
+            break;
+        }
+    }
+    if (!first_err) {
+        for (int i = 0; i < n; i++) {
+            long long dummy = 0;
+            st[i] = gp_cg_graph_run(ctx[i], p->iterations, 0, p->line_search, &dummy);
+            cg_mark_end(ctx[i], &r[i]);
+        }
+    }
+    for (int i = 0; i < prepared; i++) {
+        if (first_err) {
+            cudaEventDestroy(r[i].e0);
+            cudaEventDestroy(r[i].e1);
+            continue;
+        }
+        int rc = cg_finish(ctx[i], p, res ? &res[i] : nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, &r[i],
+                           st[i], 0);
+        if (rc && !first_err) first_err = rc;
+    }
+    free(r);
+    free(st);
+    return first_err;
 }
 
 extern "C" int gpair_last_run_stats(gpair_ctx *c, double *ms, double *flops, int *launches)

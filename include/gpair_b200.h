@@ -302,6 +302,14 @@ typedef struct {
     int stopped;  /* 1 when a racing run reached target_J first */
 } gpair_cg_result;
 
+/* Runs the same CG parameters on n contexts (one problem each, distinct contexts)
+ * at once: every context's run is prepared, then every run's graph is launched on
+ * its context's stream, then the host waits for all. Small problems that each fill
+ * a few SMs run side by side this way (many independent reconstructions, e.g. a
+ * survey or a training set). host_loop must be 0; res (length n) may be NULL.
+ * Returns the first error; per-run status in res[i].status. */
+int gpair_cg_run_many(gpair_ctx **ctx, int n, const gpair_cg_params *p, gpair_cg_result *res);
+
 /* Stop flag for racing runs: a device int, zeroed at creation and by reset. */
 int gpair_stop_flag_create(int **flag);
 int gpair_stop_flag_reset(int *flag);

@@ -350,3 +350,30 @@ def test_stop_flag_ends_a_racing_run(rec):
             assert c["reached"] and c["iterations"] == a["iterations"]
     finally:
         flag.close()
+
+
+def test_cg_run_many_equals_separate_runs():
+    """gpair_cg_run_many: concurrent runs on several contexts give the results of
+    separate runs (deterministic kernels, no shared state between contexts)."""
+    from gpair_b200.instances import instance
+    ps = [instance(20_000_000 + k) for k in range(3)]
+    recs = [g.Reconstructor(0) for _ in ps]
+    try:
+        for r, p in zip(recs, ps):
+            r.set_problem(p)
+            r.set_precision(g.PREC_SPLIT16)
+        singles, imgs = [], []
+        for r, p in zip(recs, ps):
+            r.set_image(p.start_image())
+            singles.append(r.cg(6, method=2, line_search=g.LS_BATCH))
+            imgs.append(r.get_image())
+        for r, p in zip(recs, ps):
+            r.set_image(p.start_image())
+        many = g.cg_many(recs, 6, method=2, line_search=g.LS_BATCH)
+        for r, a, b, img in zip(recs, singles, many, imgs):
+            assert b["status"] == 0 and b["iterations"] == a["iterations"] == 6
+            assert a["J"] == b["J"] and a["criterion_evals"] == b["criterion_evals"]
+            assert np.array_equal(r.get_image(), img)
+    finally:
+        for r in recs:
+            r.close()
