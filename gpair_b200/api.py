@@ -27,6 +27,7 @@ LIB_PATH = os.path.join(_HERE, "libgpair_b200.so")
 
 GPAIR_OK = 0
 PREC_FP32, PREC_SPLIT16, PREC_TF32 = 0, 1, 2
+REG_GULL_SKILLING, REG_L2 = 0, 1
 IMG_CURR, IMG_TEMP = 0, 1
 
 
@@ -133,6 +134,8 @@ def lib() -> C.CDLL:
         L.gpair_set_exit_on_error.argtypes = [i]
         L.gpair_adjoint_image.argtypes = [vp, vp, vp]
         L.gpair_stop_flag_create.argtypes = [C.POINTER(vp)]
+        L.gpair_set_regularizer.argtypes = [vp, i]
+        L.gpair_update_pixel.argtypes = [vp, i, i, f, C.POINTER(d), C.POINTER(d)]
         L.gpair_cg_run_many.argtypes = [C.POINTER(vp), i, C.POINTER(CgParams), C.POINTER(CgResult)]
         L.gpair_stop_flag_reset.argtypes = [vp]
         L.gpair_stop_flag_destroy.argtypes = [vp]
@@ -440,6 +443,16 @@ class Reconstructor:
     def gradient(self, which: int = IMG_CURR, alpha: Optional[float] = None):
         a = self.problem.alpha if alpha is None else alpha
         self._c(self._L.gpair_gradient(self.h, which, a))
+
+    def set_regularizer(self, kind: int):
+        """REG_GULL_SKILLING (default) or REG_L2."""
+        self._c(self._L.gpair_set_regularizer(self.h, kind))
+
+    def update_pixel(self, x: int, y: int, value: float):
+        """Set pixel (x, y) of the current image; returns the updated (chi2, S)."""
+        chi2, S = C.c_double(), C.c_double()
+        self._c(self._L.gpair_update_pixel(self.h, x, y, value, C.byref(chi2), C.byref(S)))
+        return chi2.value, S.value
 
     def adjoint_image(self, weights: np.ndarray) -> np.ndarray:
         """Re sum_k w_k Fx[k][x] Fy[k][y] for complex uv weights w (length nuv)."""

@@ -488,6 +488,29 @@ extern "C" int gpair_adjoint_image(gpair_ctx *c, const gpair_float2 *weights, fl
     return gp_adjoint_image(c, (const float2 *)weights, image);
 }
 
+extern "C" int gpair_set_regularizer(gpair_ctx *c, int kind)
+{
+    if (!c || (kind != GPAIR_REG_GULL_SKILLING && kind != GPAIR_REG_L2)) return GPAIR_ERR_INVALID;
+    GP_CUDA(c, cudaSetDevice(c->device));
+    GP_CUDA(c, cudaMemcpyAsync(&c->sc->reg_kind, &kind, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    GP_CUDA(c, cudaStreamSynchronize(c->stream));
+    return GPAIR_OK;
+}
+
+extern "C" int gpair_update_pixel(gpair_ctx *c, int x, int y, float value, double *chi2, double *entropy)
+{
+    if (!c || !c->have_problem) return GPAIR_ERR_STATE;
+    if (c->last_image_src != GPAIR_IMG_CURR) return GPAIR_ERR_STATE;  // V must be the current image's
+    if (x < 0 || y < 0 || x >= c->N || y >= c->N || !(value == value)) return GPAIR_ERR_INVALID;
+    GP_CUDA(c, cudaSetDevice(c->device));
+    int rc = gp_update_pixel(c, x, y, value);
+    if (rc) return rc;
+    if ((rc = gp_sync_scalars(c))) return rc;
+    if (chi2) *chi2 = c->sc_host->chi2;
+    if (entropy) *entropy = c->sc_host->entropy;
+    return (c->sc_host->nonfinite & 3u) ? GPAIR_ERR_NUMERIC : GPAIR_OK;
+}
+
 extern "C" int gpair_stop_flag_create(int **flag)
 {
     if (!flag) return GPAIR_ERR_INVALID;

@@ -101,8 +101,28 @@ struct DevScalars {
     float t_scale[GP_NTR];
     unsigned int t_counter[GP_NTR + 1];
     int *stop_flag;  // shared with racing runs (device memory), or null
+    int reg_kind;    // GPAIR_REG_GULL_SKILLING / GPAIR_REG_L2
+    // single-pixel update: old total flux and flux change of the last update
+    double upd_flux_old, upd_delta;
     CgState cg;
 };
+
+// Regulariser term of one pixel and its gradient.
+//   Gull-Skilling (gpair1/trunk/cpu.c:385-412): I - m - I ln(I/m), or -m where I <= 0
+//   or m <= 0; gradient -ln(I/m), the previous value kept where I <= 0 or m <= 0.
+//   L2 (gpair1/trunk/cpu.c:508-521): -I^2 / (2m) where m > 0, else 0; gradient -I/m
+//   where m > 0, else 0 (the reference's L2_entropy_gradient returns only the sum
+//   of this field).
+__device__ __forceinline__ double reg_term(double I, double m, int kind)
+{
+    if (kind == GPAIR_REG_L2) return m > 0.0 ? -I * I / (2.0 * m) : 0.0;
+    return (I > 0.0 && m > 0.0) ? (I - m - I * log(I / m)) : -m;
+}
+__device__ __forceinline__ float reg_grad(float I, float m, float prev, int kind)
+{
+    if (kind == GPAIR_REG_L2) return m > 0.f ? (float)(-(double)I / (double)m) : 0.f;
+    return (I > 0.f && m > 0.f) ? (float)(-log((double)I / (double)m)) : prev;
+}
 
 struct gpair_buf {
     float *ptr;
@@ -243,6 +263,7 @@ enum { CTRL_BEGIN = 0, CTRL_AFTER_DIR = 1, CTRL_AFTER_CRIT = 2, CTRL_AFTER_GRAD 
 
 // batched line-search trials (kernels_core.cu / umma_dft.cu)
 int gp_adjoint_image(gpair_ctx *c, const float2 *cw_host, float *out_host);
+int gp_update_pixel(gpair_ctx *c, int x, int y, float value);
 int gp_batch_alloc(gpair_ctx *c);
 void gp_batch_free(gpair_ctx *c);
 int gp_eval_batch(gpair_ctx *c);

@@ -149,7 +149,7 @@ __global__ void __launch_bounds__(GP_THREADS) k_prep(const float *__restrict__ s
         }
         double Id = I, m = model[p];
         acc[0] += Id;
-        acc[1] += (Id > 0.0 && m > 0.0) ? (Id - m - Id * log(Id / m)) : -m;
+        acc[1] += reg_term(Id, m, sc->reg_kind);
         mx = fmax(mx, fabs(Id));
     }
     block_sum<2>(acc, smem);
@@ -311,14 +311,17 @@ __global__ void __launch_bounds__(GP_THREADS) k_vis_data(const float2 *__restric
                                                          double2 *__restrict__ visd, float2 *__restrict__ visi,
                                                          float *__restrict__ mock, float2 *__restrict__ cw,
                                                          float2 *__restrict__ trib, double *__restrict__ partials,
-                                                         DevScalars *__restrict__ sc, FusedCtrl fc)
+                                                         DevScalars *__restrict__ sc, FusedCtrl fc,
+                                                         int direct)
 {
+    // direct: the visibilities are already in visd (a single-pixel update), not in vpart
     __shared__ double smem[32];
     const double invF = sc->invflux;
+#define VIS_AT(k) (direct ? visd[(k)] : sum_vpart(vpart, mt, nuv, (k), invF))
     double chi[1] = {0.0};
     if ((int)blockIdx.x < nblk_uv) {
         for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nuv; k += nblk_uv * blockDim.x) {
-            double2 V = sum_vpart(vpart, mt, nuv, k, invF);
+            double2 V = VIS_AT(k);
             visd[k] = V;
             visi[k] = make_float2((float)V.x, (float)V.y);
             float2 a = make_float2(0.f, 0.f);
@@ -336,9 +339,9 @@ __global__ void __launch_bounds__(GP_THREADS) k_vis_data(const float2 *__restric
         const int nblk_tri = gridDim.x - nblk_uv;
         for (int t = (blockIdx.x - nblk_uv) * blockDim.x + threadIdx.x; t < nbis; t += nblk_tri * blockDim.x) {
             int4 q = tri[t];
-            double2 va = sum_vpart(vpart, mt, nuv, q.x, invF);
-            double2 vb = sum_vpart(vpart, mt, nuv, q.y, invF);
-            double2 vc = sum_vpart(vpart, mt, nuv, q.z, invF);
+            double2 va = VIS_AT(q.x);
+            double2 vb = VIS_AT(q.y);
+            double2 vc = VIS_AT(q.z);
             if (q.w & 1) va = cconj(va);
             if (q.w & 2) vb = cconj(vb);
             if (q.w & 4) vc = cconj(vc);
@@ -383,7 +386,13 @@ __global__ void __launch_bounds__(GP_THREADS) k_vis_data(const float2 *__restric
     }
 }
 
-int gp_vis_data(gpair_ctx *c)
+#undef VIS_AT
+
+static int vis_data_launch(gpair_ctx *c, int direct);
+
+int gp_vis_data(gpair_ctx *c) { return vis_data_launch(c, 0); }
+
+static int vis_data_launch(gpair_ctx *c, int direct)
 {
     int nbu = gp_cdiv(c->nuv, GP_THREADS);
     if (nbu > 512) nbu = 512;
@@ -393,7 +402,7 @@ int gp_vis_data(gpair_ctx *c)
     k_vis_data<<<nbu + nbt, GP_THREADS, 0, c->stream>>>(c->vpart, c->mt, c->nuv, c->npow, c->nbis, c->data,
                                                         c->data_err, c->tri, c->phasor, nbu, c->visd, c->visi,
                                                         c->mock, c->cw, c->trib, slot_partials(c, RED_CHI2), c->sc,
-                                                        take_fused_ctrl(c));
+                                                        take_fused_ctrl(c), direct);
     GP_LAUNCH_CHECK(c);
     return GPAIR_OK;
 }
@@ -633,6 +642,7 @@ __global__ void __launch_bounds__(GP_THREADS) k_grad_finalize(const float *__res
 {
     __shared__ double smem[4 * 32];
     const double C = sc->adj_c, gscale = sc->gscale;
+    const int reg_kind = sc->reg_kind;
     if (alpha_from_state) alpha = (float)sc->cg.alpha;
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
@@ -651,7 +661,7 @@ __global__ void __launch_bounds__(GP_THREADS) k_grad_finalize(const float *__res
         if (mode == GRAD_FUSED) {
             float I = img[p], m = model[p];
             float eg = entropy_grad[p];
-            if (I > 0.f && m > 0.f) eg = (float)(-log((double)I / (double)m));
+            eg = reg_grad(I, m, eg, reg_kind);
             entropy_grad[p] = eg;
             float fg = gd - alpha * eg;
             out[p] = fg;
@@ -696,18 +706,17 @@ int gp_grad_finalize(gpair_ctx *c, int which, int mode, float alpha)
 
 // entropy gradient alone (gpu_compute_entropy_gradient, kernel_entropy_gs_grad.cl)
 __global__ void k_entropy_grad(const float *__restrict__ img, const float *__restrict__ model, int npix,
-                               float *__restrict__ eg)
+                               float *__restrict__ eg, const DevScalars *__restrict__ sc)
 {
     int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= npix) return;
-    float I = img[p], m = model[p];
-    if (I > 0.f && m > 0.f) eg[p] = (float)(-log((double)I / (double)m));
+    eg[p] = reg_grad(img[p], model[p], eg[p], sc->reg_kind);
 }
 
 int gp_entropy_gradient(gpair_ctx *c, int which)
 {
     const float *img = (which == GPAIR_IMG_TEMP) ? c->image_temp : c->image;
-    k_entropy_grad<<<gp_cdiv(c->npix, 256), 256, 0, c->stream>>>(img, c->model, c->npix, c->entropy_grad);
+    k_entropy_grad<<<gp_cdiv(c->npix, 256), 256, 0, c->stream>>>(img, c->model, c->npix, c->entropy_grad, c->sc);
     GP_LAUNCH_CHECK(c);
     return GPAIR_OK;
 }
@@ -877,7 +886,7 @@ __global__ void __launch_bounds__(GP_THREADS) k_trials_prep(const float *__restr
         dst[p] = I;
         const double Id = I, m = model[p];
         acc[0] += Id;
-        acc[1] += (Id > 0.0 && m > 0.0) ? (Id - m - Id * log(Id / m)) : -m;
+        acc[1] += reg_term(Id, m, sc->reg_kind);
         if (hi) {
             const int y = p / N, x = p - y * N;
             const float v = I * scale;
@@ -1040,6 +1049,57 @@ int gp_eval_batch(gpair_ctx *c)
     GP_LAUNCH_CHECK(c);
     gp_stage_end(c);
     return GPAIR_OK;
+}
+
+// --------------------------------------------- single-pixel update
+
+// One pixel changes from I_old to `value`: the total flux, the regulariser
+// sum and the image are updated on one thread; V follows in k_update_pixel_vis.
+// Corrected form of the reference's single-pixel flux change
+// (gpair1/trunk/cpu.c:477-486, gpair1/trunk/gpu.c:2137-2182): with the total
+// flux going from F to F' = F + delta, V'_k = (F V_k + delta e_k(x, y)) / F'.
+__global__ void k_update_pixel_scalar(float *__restrict__ img, const float *__restrict__ model, int p, float value,
+                                      DevScalars *__restrict__ sc)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const double old = img[p], nv = value, m = model[p];
+    const double F = sc->flux, Fn = F + (nv - old);
+    sc->upd_flux_old = F;
+    sc->upd_delta = nv - old;
+    sc->flux = Fn;
+    sc->invflux = 1.0 / Fn;
+    sc->flux_f = (float)Fn;
+    sc->invflux_f = (float)(1.0 / Fn);
+    sc->entropy += reg_term(nv, m, sc->reg_kind) - reg_term(old, m, sc->reg_kind);
+    sc->entropy_f = (float)sc->entropy;
+    sc->imax = fmax(sc->imax, fabs(nv));
+    img[p] = value;
+}
+
+__global__ void k_update_pixel_vis(const float2 *__restrict__ fx, const float2 *__restrict__ fy, int N, int nuv,
+                                   int x, int y, double2 *__restrict__ visd, const DevScalars *__restrict__ sc)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nuv) return;
+    const float2 a = fx[(size_t)k * N + x], b = fy[(size_t)k * N + y];
+    const double er = (double)a.x * b.x - (double)a.y * b.y, ei = (double)a.x * b.y + (double)a.y * b.x;
+    const double F = sc->upd_flux_old, d = sc->upd_delta, inv = sc->invflux;
+    const double2 V = visd[k];
+    visd[k] = make_double2((F * V.x + d * er) * inv, (F * V.y + d * ei) * inv);
+}
+
+int gp_update_pixel(gpair_ctx *c, int x, int y, float value)
+{
+    const int p = x + y * c->N;
+    k_update_pixel_scalar<<<1, 32, 0, c->stream>>>(c->image, c->model, p, value, c->sc);
+    GP_LAUNCH_CHECK(c);
+    if (c->nuv) {
+        k_update_pixel_vis<<<gp_cdiv(c->nuv, 256), 256, 0, c->stream>>>(c->fx, c->fy, c->N, c->nuv, x, y, c->visd,
+                                                                       c->sc);
+        GP_LAUNCH_CHECK(c);
+    }
+    c->fuse_ctrl = -1;
+    return vis_data_launch(c, 1);  // V2, T3, chi2 and the adjoint weights from the updated V
 }
 
 // ------------------------------------------------------- CG controller

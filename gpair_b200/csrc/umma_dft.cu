@@ -417,7 +417,7 @@ __global__ void __launch_bounds__(GP_THREADS) k_tc_prep_split_trial(
         dst[p] = I;
         const double Id = I, m = model[p];
         acc[0] = Id;
-        acc[1] = (Id > 0.0 && m > 0.0) ? (Id - m - Id * log(Id / m)) : -m;
+        acc[1] = reg_term(Id, m, sc->reg_kind);
         mx = fabs(Id);
         const int y = p / N, x = p - y * N;
         const float v = I * scale;

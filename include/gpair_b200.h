@@ -310,6 +310,22 @@ typedef struct {
  * Returns the first error; per-run status in res[i].status. */
 int gpair_cg_run_many(gpair_ctx **ctx, int n, const gpair_cg_params *p, gpair_cg_result *res);
 
+/* Regulariser S of the criterion J = chi2 - alpha S (default Gull-Skilling entropy,
+ * gpair1/trunk/cpu.c:385-412). GPAIR_REG_L2: S = sum over m > 0 of -I^2/(2m), dS/dI =
+ * -I/m (gpair1/trunk/cpu.c:508-521; the reference's L2_entropy_gradient returns only
+ * the sum of this field). Applies to every evaluation and CG run of the context. */
+#define GPAIR_REG_GULL_SKILLING 0
+#define GPAIR_REG_L2 1
+int gpair_set_regularizer(gpair_ctx *ctx, int kind);
+
+/* Single-pixel update of the current image (the move of annealing / MCMC samplers;
+ * the corrected form of gpair1/trunk/gpu.c:2137-2182 and gpair1/trunk/cpu.c:477-486):
+ * pixel (x, y) becomes `value`, V_k <- (F V_k + delta e_k(x,y)) / (F + delta) in FP64,
+ * then V2/T3, chi2 and S are recomputed from V in O(nuv + nbis) work, no DFT. Needs a
+ * preceding gpair_criterion on the current image; a gpair_gradient may follow.
+ * Returns the new chi2 and regulariser S (either pointer may be NULL). */
+int gpair_update_pixel(gpair_ctx *ctx, int x, int y, float value, double *chi2, double *entropy);
+
 /* Stop flag for racing runs: a device int, zeroed at creation and by reset. */
 int gpair_stop_flag_create(int **flag);
 int gpair_stop_flag_reset(int *flag);

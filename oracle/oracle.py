@@ -317,3 +317,33 @@ def data_gradient_pixels64(p, image, visi, mock, px, py):
                                _p(keep[2]), _p(keep[3]), _p(keep[4]), _p(keep[5]), _p(v), _p(m), len(px), _p(px),
                                _p(py), _p(out))
     return out
+
+
+# ------------------------------------------------------------- regularisers
+
+def l2_entropy64(image, model):
+    """FP64 L2 regulariser, gpair1/trunk/cpu.c:508-521: sum over m > 0 of -I^2 / (2m)."""
+    I = np.asarray(image, np.float64)
+    m = np.asarray(model, np.float64)
+    ok = m > 0
+    return float(np.sum(np.where(ok, -I * I / (2.0 * np.where(ok, m, 1.0)), 0.0)))
+
+
+def l2_entropy_gradient64(image, model):
+    """Per-pixel gradient of l2_entropy64: -I/m where m > 0, else 0. The reference's
+    L2_entropy_gradient (gpair1/trunk/cpu.c:523-534) returns the sum of this field."""
+    I = np.asarray(image, np.float64)
+    m = np.asarray(model, np.float64)
+    ok = m > 0
+    return np.where(ok, -I / np.where(ok, m, 1.0), 0.0)
+
+
+def ref_l2(width, image, model):
+    """The reference's compiled L2_entropy and L2_entropy_gradient (a scalar sum)."""
+    L = ref()
+    for name in ("L2_entropy", "L2_entropy_gradient"):
+        getattr(L, name).restype = C.c_float
+        getattr(L, name).argtypes = [C.c_int, C.c_void_p, C.c_void_p]
+    img = np.ascontiguousarray(image, np.float32)
+    m = np.ascontiguousarray(model, np.float32)
+    return float(L.L2_entropy(width, _p(img), _p(m))), float(L.L2_entropy_gradient(width, _p(img), _p(m)))

@@ -377,3 +377,54 @@ def test_cg_run_many_equals_separate_runs():
     finally:
         for r in recs:
             r.close()
+
+
+@pytest.mark.parametrize("prec", PRECISIONS)
+def test_l2_regularizer_matches_fp64(rec, prec):
+    p = _problem("tiny", (21, 22, 23))
+    rec.set_problem(p)
+    rec.set_precision(prec)
+    rec.set_regularizer(g.REG_L2)
+    try:
+        img = _rand_image(p, 3)
+        rec.set_image(img)
+        chi2, S = rec.criterion()
+        rec.gradient()
+        S64 = O.l2_entropy64(img, p.model)
+        assert abs(S - S64) <= 1e-10 * abs(S64)
+        eg = rec.entropy_gradient().astype(np.float64)
+        assert _rel(eg, O.l2_entropy_gradient64(img, p.model)) <= 1e-6
+        rec.set_image(p.start_image())
+        out = rec.cg(5, method=2, trace=True)
+        assert out["trace_J"][-1] < out["trace_J"][0]
+    finally:
+        rec.set_regularizer(g.REG_GULL_SKILLING)
+
+
+@pytest.mark.parametrize("prec", PRECISIONS)
+def test_update_pixel_matches_full_recomputation(rec, prec):
+    """gpair_update_pixel: V, chi2 and S after single-pixel changes agree with a
+    full evaluation of the changed image (FP32 path in a second context)."""
+    p = _problem("small", (1, 2, 3))
+    rng = np.random.default_rng(11)
+    img = _rand_image(p, 7)
+    rec.set_problem(p)
+    rec.set_precision(prec)
+    rec.set_image(img)
+    rec.criterion()
+    with g.Reconstructor(0) as full:
+        full.set_problem(p)
+        for step in range(6):
+            x, y = int(rng.integers(0, p.width)), int(rng.integers(0, p.width))
+            v = float(img[y * p.width + x] * (20.0 if step == 2 else rng.uniform(0.2, 3.0)))
+            chi2_u, S_u = rec.update_pixel(x, y, v)
+            img[y * p.width + x] = np.float32(v)
+            full.set_image(img)
+            chi2_f, S_f = full.criterion()
+            assert abs(chi2_u - chi2_f) <= 1e-5 * chi2_f, (step, chi2_u, chi2_f)
+            assert abs(S_u - S_f) <= 1e-9 * abs(S_f)
+            assert np.abs(rec.visibilities() - full.visibilities()).max() <= 2e-6
+        assert np.array_equal(rec.get_image(), img)
+        rec.gradient()
+        full.gradient()
+        assert _rel(rec.data_gradient(), full.data_gradient().astype(np.float64)) <= 1e-5

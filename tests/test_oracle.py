@@ -228,3 +228,14 @@ def test_batched_line_search_oracle_descends_and_counts():
     assert tr["grad_evals"] == iters
     assert (tr["criterion_evals"] - iters) % 8 == 0
     assert np.all(tr["step"] > 0)
+
+
+def test_l2_regularizer_restatement_matches_reference():
+    rng = np.random.default_rng(4)
+    N = 24
+    img = rng.uniform(0, 2, N * N).astype(np.float32)
+    model = rng.uniform(0.5, 1.5, N * N).astype(np.float32)
+    model[::7] = 0.0  # pixels without prior are skipped
+    S_ref, gsum_ref = O.ref_l2(N, img, model)
+    assert abs(O.l2_entropy64(img, model) - S_ref) <= 1e-5 * abs(S_ref)
+    assert abs(O.l2_entropy_gradient64(img, model).sum() - gsum_ref) <= 1e-5 * abs(gsum_ref)
