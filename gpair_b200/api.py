@@ -124,6 +124,7 @@ def lib() -> C.CDLL:
         L.gpair_cg_run.argtypes = [vp, C.POINTER(CgParams), C.POINTER(CgResult), vp, vp, vp, vp, vp]
         L.gpair_last_run_stats.argtypes = [vp, C.POINTER(d), C.POINTER(d), C.POINTER(i)]
         L.gpair_time_stages.argtypes = [vp, i, C.POINTER(d), i]
+        L.gpair_time_batch_stages.argtypes = [vp, i, C.POINTER(d), i]
         L.gpair_set_stage_timing.argtypes = [vp, i]
         L.gpair_last_run_stage_ms.argtypes = [vp, C.POINTER(d), C.POINTER(i), i]
         L.gpair_get_oi_fits_data.argtypes = [i, f, f, i, vp, i, vp, i, vp, C.POINTER(OiData)]
@@ -516,6 +517,15 @@ class Reconstructor:
         if n < 0:
             self._c(n)
         return {k: ms[j] for j, k in enumerate(self.STAGES[:n])}
+
+    BATCH_STAGES = ("trials_prep", "forward_dft_batch", "vis_chi2_batch")
+
+    def time_batch_stages(self, reps: int = 10) -> dict:
+        ms = (C.c_double * 3)()
+        n = self._L.gpair_time_batch_stages(self.h, reps, ms, 3)
+        if n < 0:
+            self._c(n)
+        return {k: ms[j] for j, k in enumerate(self.BATCH_STAGES[:n])}
 
     def set_stage_timing(self, on: bool = True):
         self._c(self._L.gpair_set_stage_timing(self.h, 1 if on else 0))

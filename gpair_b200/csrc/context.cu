@@ -828,3 +828,41 @@ extern "C" int gpair_time_stages(gpair_ctx *c, int reps, double *ms, int max_sta
     for (int i = 0; i < n; i++) ms[i] = acc[i] / reps;
     return n;
 }
+
+// The three stages of one batched line-search evaluation (8 trial images), timed
+// like gpair_time_stages: [0] trial images + operands, [1] forward contraction
+// of the stack, [2] chi2 of every trial. The steps are the device state's last
+// batch (or the initial grid); the controller does not run.
+extern "C" int gpair_time_batch_stages(gpair_ctx *c, int reps, double *ms, int max_stages)
+{
+    if (!c || !c->have_problem || reps <= 0 || !ms) return GPAIR_ERR_INVALID;
+    GP_CUDA(c, cudaSetDevice(c->device));
+    int rc = gp_batch_alloc(c);
+    if (rc) return rc;
+    const int ns = 3;
+    std::vector<cudaEvent_t> ev((size_t)(ns + 1) * reps);
+    for (auto &e : ev) GP_CUDA(c, cudaEventCreate(&e));
+    const int st = c->stage_timing;
+    c->stage_timing = 0;
+    for (int r = 0; r < reps && !rc; r++) {
+        cudaEvent_t *E = &ev[(size_t)r * (ns + 1)];
+        c->fuse_ctrl = -1;
+        rc = gp_eval_batch_timed(c, E);
+    }
+    c->stage_timing = st;
+    double acc[3] = {0, 0, 0};
+    if (!rc && cudaStreamSynchronize(c->stream) != cudaSuccess) rc = GPAIR_ERR_CUDA;
+    for (int r = 0; r < reps && !rc; r++) {
+        cudaEvent_t *E = &ev[(size_t)r * (ns + 1)];
+        for (int i = 0; i < ns; i++) {
+            float t = 0.f;
+            cudaEventElapsedTime(&t, E[i], E[i + 1]);
+            acc[i] += t;
+        }
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+    if (rc) return rc;
+    int n = max_stages < ns ? max_stages : ns;
+    for (int i = 0; i < n; i++) ms[i] = acc[i] / reps;
+    return n;
+}

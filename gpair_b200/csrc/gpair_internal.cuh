@@ -267,6 +267,7 @@ int gp_update_pixel(gpair_ctx *c, int x, int y, float value);
 int gp_batch_alloc(gpair_ctx *c);
 void gp_batch_free(gpair_ctx *c);
 int gp_eval_batch(gpair_ctx *c);
+int gp_eval_batch_timed(gpair_ctx *c, cudaEvent_t *ev);
 int gp_tc_batch_prepare(gpair_ctx *c, int *epp);
 int gp_trials_prep_launch(gpair_ctx *c, void *hi, void *lo, int Lpad, int Kx_pad, int tw_log2);
 int gp_tc_trials_prep_split(gpair_ctx *c, double *partials);

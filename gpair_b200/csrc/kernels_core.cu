@@ -1015,22 +1015,26 @@ int gp_trials_prep_launch(gpair_ctx *c, void *hi, void *lo, int Lpad, int Kx_pad
 }
 
 // One batched evaluation: GP_NTR trial images -> forward DFTs -> chi2 of each,
-// then the controller (fused into the last block of the chi2 kernel).
-int gp_eval_batch(gpair_ctx *c)
+// then the controller (fused into the last block of the chi2 kernel). With
+// `ev` (4 events) the stage boundaries are recorded on the stream.
+static int eval_batch(gpair_ctx *c, cudaEvent_t *ev)
 {
     int rc = gp_batch_alloc(c);
     if (rc) return rc;
     int epp;
+    if (ev) cudaEventRecord(ev[0], c->stream);
     gp_stage_begin(c, 0);
     if (c->precision != GPAIR_PREC_FP32) {
         if ((rc = gp_tc_trials_prep_split(c, c->partials_b))) return rc;
         gp_stage_end(c);
+        if (ev) cudaEventRecord(ev[1], c->stream);
         gp_stage_begin(c, 1);
         if ((rc = gp_tc_forward_batch_gemm(c))) return rc;
         epp = c->epp;
     } else {
         if ((rc = gp_trials_prep_launch(c, nullptr, nullptr, 0, 0, 0))) return rc;
         gp_stage_end(c);
+        if (ev) cudaEventRecord(ev[1], c->stream);
         gp_stage_begin(c, 1);
         epp = gp_cdiv(c->N, FB_M);
         dim3 grid(gp_cdiv(c->nuv, FB_K), epp, GP_NTR);
@@ -1038,6 +1042,7 @@ int gp_eval_batch(gpair_ctx *c)
         GP_LAUNCH_CHECK(c);
     }
     gp_stage_end(c);
+    if (ev) cudaEventRecord(ev[2], c->stream);
     gp_stage_begin(c, 2);
     int nb = gp_cdiv(c->npow + c->nbis, GP_THREADS * 2);
     if (nb > 1024) nb = 1024;
@@ -1048,8 +1053,12 @@ int gp_eval_batch(gpair_ctx *c)
                                                       take_fused_ctrl(c));
     GP_LAUNCH_CHECK(c);
     gp_stage_end(c);
+    if (ev) cudaEventRecord(ev[3], c->stream);
     return GPAIR_OK;
 }
+
+int gp_eval_batch(gpair_ctx *c) { return eval_batch(c, nullptr); }
+int gp_eval_batch_timed(gpair_ctx *c, cudaEvent_t *ev) { return eval_batch(c, ev); }
 
 // --------------------------------------------- single-pixel update
 

@@ -382,6 +382,11 @@ int gpair_last_run_stats(gpair_ctx *ctx, double *device_ms, double *dft_flops, i
 #define GPAIR_NSTAGES 6
 int gpair_time_stages(gpair_ctx *ctx, int reps, double *stage_ms, int max_stages);
 
+/* The stages of one batched line-search evaluation (GPAIR_LS_TRIALS trial images),
+ * timed like gpair_time_stages: [0] trial images + operands, [1] forward contraction
+ * of the stack, [2] chi2 of every trial. Uses the steps of the last batch. */
+int gpair_time_batch_stages(gpair_ctx *ctx, int reps, double *stage_ms, int max_stages);
+
 /* Live stage timing inside gpair_cg_run: when on, every stage launch of the
  * run is bracketed by CUDA events on the context's stream;
  * gpair_last_run_stage_ms returns the summed ms and launch count per stage

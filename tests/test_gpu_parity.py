@@ -428,3 +428,18 @@ def test_update_pixel_matches_full_recomputation(rec, prec):
         rec.gradient()
         full.gradient()
         assert _rel(rec.data_gradient(), full.data_gradient().astype(np.float64)) <= 1e-5
+
+
+def test_stage_timing_hooks_return_positive_times(rec):
+    p = _problem("tiny", (1, 2, 3))
+    rec.set_problem(p)
+    rec.set_precision(g.PREC_SPLIT16)
+    rec.set_image(p.start_image())
+    rec.cg(2, method=2, line_search=g.LS_BATCH)
+    st = rec.time_stages(reps=2)
+    sb = rec.time_batch_stages(reps=2)
+    assert len(st) == 6 and all(v > 0 for v in st.values())
+    assert len(sb) == 3 and all(v > 0 for v in sb.values())
+    # timing runs no controller: the CG state is untouched
+    out = rec.cg(1, method=2, line_search=g.LS_BATCH, resume=True)
+    assert out["iterations"] == 1
