@@ -196,6 +196,13 @@ def many_instances(n: int, iters: int) -> dict:
             r.set_problem(p)
             r.set_precision(g.PREC_SPLIT16)
             r.set_image(p.start_image())
+        # autotuned configuration per instance shape (precision path, adjoint split-K),
+        # cached across instances of the same shape
+        t0 = time.perf_counter()
+        tuned = [r.autotune(g.api.TUNE_PRECISION | g.api.TUNE_SPLITS | g.api.TUNE_CACHE, reps=2) for r in recs]
+        t_tune = time.perf_counter() - t0
+        for r, p in zip(recs, ps):
+            r.set_image(p.start_image())
         g.cg_many(recs, 1, line_search=g.LS_BATCH)  # builds every graph
         for r, p in zip(recs, ps):
             r.set_image(p.start_image())
@@ -220,6 +227,9 @@ def many_instances(n: int, iters: int) -> dict:
             "instances_per_s": n / max(t_con, 1e-12), "tflops_concurrent": flops_con / max(t_con, 1e-12) / 1e12,
             "tflops_sequential": flops / max(t_seq, 1e-12) / 1e12,
             "all_ok": all(r_["status"] == 0 for r_ in res),
+            "autotune": {"s": t_tune, "tuned": sum(not t["from_cache"] for t in tuned),
+                         "fp32_path": sum(t["precision"] == g.PREC_FP32 for t in tuned),
+                         "split16_path": sum(t["precision"] == g.PREC_SPLIT16 for t in tuned)},
             "unit": "s (host wall clock)", "line_search": "batched"}
 
 

@@ -85,6 +85,13 @@ class CgParams(C.Structure):
 
 
 LS_WOLFE, LS_BATCH, LS_TRIALS = 0, 1, 8
+TUNE_PRECISION, TUNE_SPLITS, TUNE_CACHE = 1, 2, 4
+
+
+class TuneResult(C.Structure):
+    _fields_ = [("precision", C.c_int), ("adjoint_splits", C.c_int), ("ms_per_eval", C.c_double),
+                ("from_cache", C.c_int), ("n_candidates", C.c_int), ("cand_precision", C.c_int * 8),
+                ("cand_splits", C.c_int * 8), ("cand_ms", C.c_double * 8)]
 
 
 class CgResult(C.Structure):
@@ -136,6 +143,7 @@ def lib() -> C.CDLL:
         L.gpair_adjoint_image.argtypes = [vp, vp, vp]
         L.gpair_stop_flag_create.argtypes = [C.POINTER(vp)]
         L.gpair_set_regularizer.argtypes = [vp, i]
+        L.gpair_autotune.argtypes = [vp, i, i, C.POINTER(TuneResult)]
         L.gpair_update_pixel.argtypes = [vp, i, i, f, C.POINTER(d), C.POINTER(d)]
         L.gpair_cg_run_many.argtypes = [C.POINTER(vp), i, C.POINTER(CgParams), C.POINTER(CgResult)]
         L.gpair_stop_flag_reset.argtypes = [vp]
@@ -444,6 +452,15 @@ class Reconstructor:
     def gradient(self, which: int = IMG_CURR, alpha: Optional[float] = None):
         a = self.problem.alpha if alpha is None else alpha
         self._c(self._L.gpair_gradient(self.h, which, a))
+
+    def autotune(self, flags: int = 7, reps: int = 3) -> dict:
+        """Time criterion + gradient under candidate configurations (precision path,
+        adjoint split-K length) and keep the fastest (gpair_autotune)."""
+        r = TuneResult()
+        self._c(self._L.gpair_autotune(self.h, flags, reps, C.byref(r)))
+        return {"precision": r.precision, "adjoint_splits": r.adjoint_splits, "ms_per_eval": r.ms_per_eval,
+                "from_cache": bool(r.from_cache),
+                "candidates": [(r.cand_precision[i], r.cand_splits[i], r.cand_ms[i]) for i in range(r.n_candidates)]}
 
     def set_regularizer(self, kind: int):
         """REG_GULL_SKILLING (default) or REG_L2."""

@@ -1,0 +1,185 @@
+// autotune.cu -- per-problem choice of the precision path and of the adjoint's
+// split-K tile length, by timing criterion + gradient evaluations of the loaded
+// problem on the device (CUDA events on the context's stream).
+//
+// Candidates:
+//   precision  FP32 (CUDA-core contractions) and split-f16 (tcgen05); both meet
+//              the accuracy bounds, the faster one depends on the image width
+//              and the uv count (small problems leave the tensor GEMM's tiles
+//              mostly empty)
+//   splits     the adjoint's K-blocks per split (tensor) or split count
+//              (CUDA cores): the heuristic's value, half and double of it,
+//              within the FP32-accumulation cap and the partial-image buffer
+// Choices are cached per (device, width, uv count to 1/8) for the process.
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <map>
+#include <mutex>
+#include <tuple>
+#include <vector>
+
+#include "gpair_internal.cuh"
+
+namespace {
+
+struct Choice {
+    int precision, tc_kb_per, simt_splits;
+    double ms;
+};
+
+std::mutex g_mu;
+std::map<std::tuple<int, int, int>, Choice> g_cache;
+
+int uv_bucket(int nuv) { return nuv <= 0 ? 0 : (int)floor(log2((double)nuv) * 8.0); }
+
+// average ms of one criterion + gradient evaluation of the current image
+int time_evals(gpair_ctx *c, int reps, double *ms)
+{
+    cudaEvent_t e0, e1;
+    GP_CUDA(c, cudaEventCreate(&e0));
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return GPAIR_ERR_CUDA;
+    }
+    int rc = GPAIR_OK;
+    const int st = c->stage_timing;
+    c->stage_timing = 0;
+    c->fuse_ctrl = -1;
+    // one untimed evaluation: first-use costs (operand tables, function attributes)
+    rc = gp_eval_criterion(c, GPAIR_IMG_CURR, 0);
+    if (!rc) rc = gp_eval_gradient(c, GPAIR_IMG_CURR, 1e-3f);
+    cudaEventRecord(e0, c->stream);
+    for (int r = 0; r < reps && !rc; r++) {
+        rc = gp_eval_criterion(c, GPAIR_IMG_CURR, 0);
+        if (!rc) rc = gp_eval_gradient(c, GPAIR_IMG_CURR, 1e-3f);
+    }
+    cudaEventRecord(e1, c->stream);
+    c->stage_timing = st;
+    float t = 0.f;
+    if (!rc && cudaEventSynchronize(e1) != cudaSuccess) rc = GPAIR_ERR_CUDA;
+    if (!rc) cudaEventElapsedTime(&t, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (!rc) rc = gp_sync_scalars(c);  // a bounded-wait timeout surfaces here
+    *ms = t / reps;
+    return rc;
+}
+
+int apply(gpair_ctx *c, const Choice &ch)
+{
+    int rc = gpair_set_precision(c, ch.precision);
+    if (rc) return rc;
+    if (ch.precision != GPAIR_PREC_FP32) {
+        if ((rc = gp_tc_prepare(c))) return rc;
+        if ((rc = gp_tc_set_kb_per(c, ch.tc_kb_per))) return rc;
+    }
+    c->splits_simt = ch.simt_splits;
+    gp_cg_graph_free(c);  // a captured CG graph holds the old configuration
+    return GPAIR_OK;
+}
+
+}  // namespace
+
+extern "C" int gpair_autotune(gpair_ctx *c, int flags, int reps, gpair_tune_result *res)
+{
+    if (!c || !c->have_problem || !c->have_image) return GPAIR_ERR_STATE;
+    if (reps <= 0) reps = 3;
+    GP_CUDA(c, cudaSetDevice(c->device));
+    const auto key = std::make_tuple(c->device, c->N, uv_bucket(c->nuv));
+    if (res) memset(res, 0, sizeof(*res));
+    if (flags & GPAIR_TUNE_CACHE) {
+        Choice ch;
+        bool hit = false;
+        {
+            std::lock_guard<std::mutex> lk(g_mu);
+            auto it = g_cache.find(key);
+            if (it != g_cache.end()) {
+                ch = it->second;
+                hit = true;
+            }
+        }
+        bool applied = false;
+        if (hit) {
+            // a cached split-K length can exceed this problem's partial-image buffer
+            // (GPAIR_ERR_INVALID): then this problem is tuned afresh
+            int rc = apply(c, ch);
+            if (rc && rc != GPAIR_ERR_INVALID) return rc;
+            applied = rc == GPAIR_OK;
+        }
+        if (applied) {
+            if (res) {
+                res->precision = ch.precision;
+                res->adjoint_splits = ch.precision == GPAIR_PREC_FP32 ? ch.simt_splits : gp_tc_split_count(c, ch.tc_kb_per);
+                res->ms_per_eval = ch.ms;
+                res->from_cache = 1;
+            }
+            return GPAIR_OK;
+        }
+    }
+    std::vector<int> precs;
+    if (flags & GPAIR_TUNE_PRECISION) {
+        precs.push_back(GPAIR_PREC_SPLIT16);
+        precs.push_back(GPAIR_PREC_FP32);
+    } else {
+        precs.push_back(c->precision);
+    }
+    const int simt0 = c->splits_simt > 0 ? c->splits_simt : 1;
+    std::vector<Choice> cand;
+    for (int prec : precs) {
+        if (prec == GPAIR_PREC_FP32) {
+            std::vector<int> ss = {simt0};
+            if (flags & GPAIR_TUNE_SPLITS) {
+                if (simt0 / 2 >= 1) ss.push_back(simt0 / 2);
+                if (2 * simt0 <= c->gpart_cap && 2 * simt0 <= 64) ss.push_back(2 * simt0);
+            }
+            for (int s : ss) cand.push_back({prec, 0, s, 0.0});
+        } else {
+            int rc = gpair_set_precision(c, prec);
+            if (rc) return rc;
+            if ((rc = gp_tc_prepare(c))) return rc;
+            const int k0 = gp_tc_kb_per(c);
+            if (k0 <= 0) return GPAIR_ERR_STATE;
+            std::vector<int> ks = {k0};
+            if (flags & GPAIR_TUNE_SPLITS) {
+                if (k0 / 2 >= 1) ks.push_back(k0 / 2);
+                if (2 * k0 <= 64) ks.push_back(2 * k0);
+            }
+            for (int k : ks) cand.push_back({prec, k, simt0, 0.0});
+        }
+    }
+    if ((int)cand.size() > GPAIR_TUNE_MAX_CANDIDATES) cand.resize(GPAIR_TUNE_MAX_CANDIDATES);
+    int best = -1;
+    for (size_t i = 0; i < cand.size(); i++) {
+        int rc = apply(c, cand[i]);
+        if (rc == GPAIR_ERR_INVALID) {  // a split count beyond the partial-image buffer: skip it
+            cand[i].ms = INFINITY;
+            continue;
+        }
+        if (rc) return rc;
+        if ((rc = time_evals(c, reps, &cand[i].ms))) return rc;
+        if (best < 0 || cand[i].ms < cand[best].ms) best = (int)i;
+    }
+    if (best < 0) return GPAIR_ERR_STATE;
+    int rc = apply(c, cand[best]);
+    if (rc) return rc;
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        g_cache[key] = cand[best];
+    }
+    if (res) {
+        res->precision = cand[best].precision;
+        res->adjoint_splits = cand[best].precision == GPAIR_PREC_FP32 ? cand[best].simt_splits
+                                                                       : gp_tc_split_count(c, cand[best].tc_kb_per);
+        res->ms_per_eval = cand[best].ms;
+        res->n_candidates = (int)cand.size();
+        for (size_t i = 0; i < cand.size(); i++) {
+            res->cand_precision[i] = cand[i].precision;
+            res->cand_splits[i] = cand[i].precision == GPAIR_PREC_FP32 ? cand[i].simt_splits
+                                                                      : gp_tc_split_count(c, cand[i].tc_kb_per);
+            res->cand_ms[i] = cand[i].ms;
+        }
+    }
+    return GPAIR_OK;
+}

@@ -214,7 +214,9 @@ int gp_set_problem_core(gpair_ctx *c, int N, float pix, int nuv, const gpair_uv 
     GP_CUDA(c, cudaMalloc(&c->visi, nk * sizeof(float2)));
     GP_CUDA(c, cudaMalloc(&c->cw, nk * sizeof(float2)));
     GP_CUDA(c, cudaMalloc(&c->trib, 3 * nt * sizeof(float2)));
-    GP_CUDA(c, cudaMalloc(&c->gpart, (size_t)max_splits * c->npix * sizeof(float)));
+    // room for twice the default split count: the autotuner may shorten the split-K tiles
+    c->gpart_cap = 2 * max_splits;
+    GP_CUDA(c, cudaMalloc(&c->gpart, (size_t)c->gpart_cap * c->npix * sizeof(float)));
     GP_CUDA(c, cudaMemsetAsync(c->mock, 0, nd * sizeof(float), c->stream));
     GP_CUDA(c, cudaMemsetAsync(c->visd, 0, nk * sizeof(double2), c->stream));
     GP_CUDA(c, cudaMemsetAsync(c->visi, 0, nk * sizeof(float2), c->stream));

@@ -143,6 +143,7 @@ struct gpair_ctx {
     int mt;           // number of row tiles of the forward DFT
     int splits;       // split-K factor of the last adjoint (number of partial images)
     int splits_simt;  // split-K factor of the CUDA-core adjoint
+    int gpart_cap;    // partial images gpart holds
 
     // buffers
     float *image, *image_temp, *model;
@@ -284,3 +285,9 @@ int gp_tc_prep_split_trial(gpair_ctx *c);
 int gp_tc_splits(int N, int nuv, int nsm, int *kb_per_out);
 int gp_tc_adjoint(gpair_ctx *c, int which);
 void gp_tc_free(gpair_ctx *c);
+int gp_tc_kb_per(gpair_ctx *c);
+int gp_tc_set_kb_per(gpair_ctx *c, int kb_per);
+int gp_tc_split_count(gpair_ctx *c, int kb_per);
+int gp_eval_criterion(gpair_ctx *c, int which, int trial);
+int gp_eval_gradient(gpair_ctx *c, int which, float alpha);
+void gp_cg_graph_free(gpair_ctx *c);

@@ -639,6 +639,34 @@ int gp_tc_prepare(gpair_ctx *c)
     return GPAIR_OK;
 }
 
+// split-K tile length of the tensor adjoint (K-blocks per split): read / override
+int gp_tc_kb_per(gpair_ctx *c)
+{
+    TcState *t = (TcState *)c->tc_state;
+    return t ? t->kb_per : 0;
+}
+
+// split count of the tensor adjoint for a given split-K tile length
+int gp_tc_split_count(gpair_ctx *c, int kb_per)
+{
+    TcState *t = (TcState *)c->tc_state;
+    if (!t || kb_per <= 0) return 0;
+    return (t->K2_pad / TC_BK + kb_per - 1) / kb_per;
+}
+
+int gp_tc_set_kb_per(gpair_ctx *c, int kb_per)
+{
+    TcState *t = (TcState *)c->tc_state;
+    if (!t) return GPAIR_ERR_STATE;
+    const int kb_total = t->K2_pad / TC_BK;
+    if (kb_per < 1 || kb_per > 64) return GPAIR_ERR_INVALID;  // 64: the FP32 accumulation cap
+    const int splits = (kb_total + kb_per - 1) / kb_per;
+    if (splits > c->gpart_cap) return GPAIR_ERR_INVALID;
+    t->kb_per = kb_per;
+    t->splits = splits;
+    return GPAIR_OK;
+}
+
 static TcState *tc_state_ready(gpair_ctx *c, int *rc)
 {
     TcState *t = (TcState *)c->tc_state;

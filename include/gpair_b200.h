@@ -387,6 +387,29 @@ int gpair_time_stages(gpair_ctx *ctx, int reps, double *stage_ms, int max_stages
  * of the stack, [2] chi2 of every trial. Uses the steps of the last batch. */
 int gpair_time_batch_stages(gpair_ctx *ctx, int reps, double *stage_ms, int max_stages);
 
+/* Autotuner: times criterion + gradient evaluations of the loaded problem (current
+ * image) under candidate configurations and keeps the fastest. Candidates: the
+ * precision path (GPAIR_TUNE_PRECISION: FP32 CUDA cores vs split-f16 tensor cores;
+ * both meet the 1e-5 accuracy bounds) and the adjoint's split-K tile length
+ * (GPAIR_TUNE_SPLITS: half, default and double the heuristic's K-blocks per split,
+ * within the FP32-accumulation cap). GPAIR_TUNE_CACHE reuses the choice made for a
+ * problem of the same device, width and uv count (to 1/8) in this process. */
+#define GPAIR_TUNE_PRECISION 1
+#define GPAIR_TUNE_SPLITS 2
+#define GPAIR_TUNE_CACHE 4
+#define GPAIR_TUNE_MAX_CANDIDATES 8
+typedef struct {
+    int precision;       /* chosen precision mode */
+    int adjoint_splits;  /* chosen split-K count of the adjoint contraction */
+    double ms_per_eval;  /* criterion + gradient, chosen configuration */
+    int from_cache;
+    int n_candidates;
+    int cand_precision[GPAIR_TUNE_MAX_CANDIDATES];
+    int cand_splits[GPAIR_TUNE_MAX_CANDIDATES];
+    double cand_ms[GPAIR_TUNE_MAX_CANDIDATES];
+} gpair_tune_result;
+int gpair_autotune(gpair_ctx *ctx, int flags, int reps, gpair_tune_result *result);
+
 /* Live stage timing inside gpair_cg_run: when on, every stage launch of the
  * run is bracketed by CUDA events on the context's stream;
  * gpair_last_run_stage_ms returns the summed ms and launch count per stage

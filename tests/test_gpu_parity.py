@@ -443,3 +443,26 @@ def test_stage_timing_hooks_return_positive_times(rec):
     # timing runs no controller: the CG state is untouched
     out = rec.cg(1, method=2, line_search=g.LS_BATCH, resume=True)
     assert out["iterations"] == 1
+
+
+def test_autotune_keeps_accuracy_and_caches():
+    p = _problem("small", (1, 2, 3))
+    img = _rand_image(p, 2)
+    e = O.evaluate64(p, img)
+    with g.Reconstructor(0) as a, g.Reconstructor(0) as b:
+        a.set_problem(p)
+        a.set_image(img)
+        t = a.autotune(g.api.TUNE_PRECISION | g.api.TUNE_SPLITS, reps=2)
+        assert t["precision"] in (g.PREC_FP32, g.PREC_SPLIT16) and not t["from_cache"]
+        assert len(t["candidates"]) >= 4 and t["ms_per_eval"] > 0
+        assert t["ms_per_eval"] == min(ms for _, _, ms in t["candidates"])
+        chi2, _ = a.criterion()
+        a.gradient()
+        assert abs(chi2 - e["chi2"]) <= 1e-5 * e["chi2"]
+        assert _rel(a.data_gradient(), e["data_grad"]) <= 1e-5
+        assert a.cg(3, method=2)["iterations"] == 3  # the CG graph is rebuilt for the new configuration
+        b.set_problem(p)
+        b.set_image(img)
+        tb = b.autotune(g.api.TUNE_PRECISION | g.api.TUNE_SPLITS | g.api.TUNE_CACHE)
+        assert tb["from_cache"] and tb["precision"] == t["precision"]
+        assert tb["adjoint_splits"] == t["adjoint_splits"]
