@@ -199,7 +199,8 @@ def many_instances(n: int, iters: int) -> dict:
         # autotuned configuration per instance shape (precision path, adjoint split-K),
         # cached across instances of the same shape
         t0 = time.perf_counter()
-        tuned = [r.autotune(g.api.TUNE_PRECISION | g.api.TUNE_SPLITS | g.api.TUNE_CACHE, reps=2) for r in recs]
+        flags = g.api.TUNE_PRECISION | g.api.TUNE_SPLITS | g.api.TUNE_CACHE | g.api.TUNE_BATCHED
+        tuned = [r.autotune(flags, reps=2) for r in recs]
         t_tune = time.perf_counter() - t0
         for r, p in zip(recs, ps):
             r.set_image(p.start_image())

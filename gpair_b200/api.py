@@ -85,7 +85,7 @@ class CgParams(C.Structure):
 
 
 LS_WOLFE, LS_BATCH, LS_TRIALS = 0, 1, 8
-TUNE_PRECISION, TUNE_SPLITS, TUNE_CACHE = 1, 2, 4
+TUNE_PRECISION, TUNE_SPLITS, TUNE_CACHE, TUNE_BATCHED = 1, 2, 4, 8
 
 
 class TuneResult(C.Structure):

@@ -10,7 +10,9 @@
 //   splits     the adjoint's K-blocks per split (tensor) or split count
 //              (CUDA cores): the heuristic's value, half and double of it,
 //              within the FP32-accumulation cap and the partial-image buffer
-// Choices are cached per (device, width, uv count to 1/8) for the process.
+// Objective: one criterion + gradient evaluation, or (GPAIR_TUNE_BATCHED) that
+// plus two batched 8-trial evaluations, the work of a batched-line-search
+// iteration. Choices are cached per (device, width, uv count to 1/8, objective).
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
@@ -34,9 +36,15 @@ std::map<std::tuple<int, int, int>, Choice> g_cache;
 
 int uv_bucket(int nuv) { return nuv <= 0 ? 0 : (int)floor(log2((double)nuv) * 8.0); }
 
-// average ms of one criterion + gradient evaluation of the current image
-int time_evals(gpair_ctx *c, int reps, double *ms)
+// average ms of one criterion + gradient evaluation of the current image, plus
+// (batched) two evaluations of 8 trial images: the work of one iteration of the
+// batched line search
+int time_evals(gpair_ctx *c, int reps, int batched, double *ms)
 {
+    if (batched) {
+        int rc = gp_batch_alloc(c);
+        if (rc) return rc;
+    }
     cudaEvent_t e0, e1;
     GP_CUDA(c, cudaEventCreate(&e0));
     if (cudaEventCreate(&e1) != cudaSuccess) {
@@ -47,13 +55,15 @@ int time_evals(gpair_ctx *c, int reps, double *ms)
     const int st = c->stage_timing;
     c->stage_timing = 0;
     c->fuse_ctrl = -1;
-    // one untimed evaluation: first-use costs (operand tables, function attributes)
+    // one untimed pass: first-use costs (operand tables, function attributes)
     rc = gp_eval_criterion(c, GPAIR_IMG_CURR, 0);
     if (!rc) rc = gp_eval_gradient(c, GPAIR_IMG_CURR, 1e-3f);
+    if (!rc && batched) rc = gp_eval_batch(c);
     cudaEventRecord(e0, c->stream);
     for (int r = 0; r < reps && !rc; r++) {
         rc = gp_eval_criterion(c, GPAIR_IMG_CURR, 0);
         if (!rc) rc = gp_eval_gradient(c, GPAIR_IMG_CURR, 1e-3f);
+        for (int b = 0; b < 2 * batched && !rc; b++) rc = gp_eval_batch(c);  // no controller: fuse_ctrl = -1
     }
     cudaEventRecord(e1, c->stream);
     c->stage_timing = st;
@@ -87,7 +97,7 @@ extern "C" int gpair_autotune(gpair_ctx *c, int flags, int reps, gpair_tune_resu
     if (!c || !c->have_problem || !c->have_image) return GPAIR_ERR_STATE;
     if (reps <= 0) reps = 3;
     GP_CUDA(c, cudaSetDevice(c->device));
-    const auto key = std::make_tuple(c->device, c->N, uv_bucket(c->nuv));
+    const auto key = std::make_tuple(c->device, c->N, uv_bucket(c->nuv) * 2 + ((flags & GPAIR_TUNE_BATCHED) ? 1 : 0));
     if (res) memset(res, 0, sizeof(*res));
     if (flags & GPAIR_TUNE_CACHE) {
         Choice ch;
@@ -158,7 +168,7 @@ extern "C" int gpair_autotune(gpair_ctx *c, int flags, int reps, gpair_tune_resu
             continue;
         }
         if (rc) return rc;
-        if ((rc = time_evals(c, reps, &cand[i].ms))) return rc;
+        if ((rc = time_evals(c, reps, (flags & GPAIR_TUNE_BATCHED) ? 1 : 0, &cand[i].ms))) return rc;
         if (best < 0 || cand[i].ms < cand[best].ms) best = (int)i;
     }
     if (best < 0) return GPAIR_ERR_STATE;

@@ -393,10 +393,12 @@ int gpair_time_batch_stages(gpair_ctx *ctx, int reps, double *stage_ms, int max_
  * both meet the 1e-5 accuracy bounds) and the adjoint's split-K tile length
  * (GPAIR_TUNE_SPLITS: half, default and double the heuristic's K-blocks per split,
  * within the FP32-accumulation cap). GPAIR_TUNE_CACHE reuses the choice made for a
- * problem of the same device, width and uv count (to 1/8) in this process. */
+ * problem of the same device, width and uv count (to 1/8) and objective in this process. */
 #define GPAIR_TUNE_PRECISION 1
 #define GPAIR_TUNE_SPLITS 2
 #define GPAIR_TUNE_CACHE 4
+#define GPAIR_TUNE_BATCHED 8 /* objective: criterion + gradient + 2 batched 8-trial evaluations
+                                (one batched-line-search iteration) instead of criterion + gradient */
 #define GPAIR_TUNE_MAX_CANDIDATES 8
 typedef struct {
     int precision;       /* chosen precision mode */

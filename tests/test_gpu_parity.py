@@ -466,3 +466,9 @@ def test_autotune_keeps_accuracy_and_caches():
         tb = b.autotune(g.api.TUNE_PRECISION | g.api.TUNE_SPLITS | g.api.TUNE_CACHE)
         assert tb["from_cache"] and tb["precision"] == t["precision"]
         assert tb["adjoint_splits"] == t["adjoint_splits"]
+        # workload-matched objective (one batched-line-search iteration), then a batched run
+        tc = b.autotune(g.api.TUNE_PRECISION | g.api.TUNE_SPLITS | g.api.TUNE_BATCHED, reps=2)
+        assert not tc["from_cache"] and len(tc["candidates"]) >= 4
+        b.set_image(p.start_image())
+        out = b.cg(3, method=2, trace=True, line_search=g.LS_BATCH)
+        assert out["iterations"] == 3 and np.all(np.diff(out["trace_J"]) <= 0)
