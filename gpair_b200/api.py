@@ -143,6 +143,10 @@ def lib() -> C.CDLL:
         L.gpair_adjoint_image.argtypes = [vp, vp, vp]
         L.gpair_stop_flag_create.argtypes = [C.POINTER(vp)]
         L.gpair_set_regularizer.argtypes = [vp, i]
+        L.gpair_cg_checkpoint_size.argtypes = [vp]
+        L.gpair_cg_checkpoint_size.restype = C.c_size_t
+        L.gpair_cg_checkpoint_save.argtypes = [vp, vp, C.c_size_t]
+        L.gpair_cg_checkpoint_load.argtypes = [vp, vp, C.c_size_t]
         L.gpair_autotune.argtypes = [vp, i, i, C.POINTER(TuneResult)]
         L.gpair_update_pixel.argtypes = [vp, i, i, f, C.POINTER(d), C.POINTER(d)]
         L.gpair_cg_run_many.argtypes = [C.POINTER(vp), i, C.POINTER(CgParams), C.POINTER(CgResult)]
@@ -461,6 +465,35 @@ class Reconstructor:
         return {"precision": r.precision, "adjoint_splits": r.adjoint_splits, "ms_per_eval": r.ms_per_eval,
                 "from_cache": bool(r.from_cache),
                 "candidates": [(r.cand_precision[i], r.cand_splits[i], r.cand_ms[i]) for i in range(r.n_candidates)]}
+
+    def checkpoint(self) -> bytes:
+        """The CG state of this context (gpair_cg_checkpoint_save) as bytes."""
+        n = self._L.gpair_cg_checkpoint_size(self.h)
+        buf = C.create_string_buffer(n)
+        self._c(self._L.gpair_cg_checkpoint_save(self.h, buf, n))
+        return buf.raw
+
+    def restore(self, data: bytes):
+        """Load a checkpoint of the same problem; continue with cg(..., resume=True)."""
+        buf = C.create_string_buffer(data, len(data))
+        self._c(self._L.gpair_cg_checkpoint_load(self.h, buf, len(data)))
+
+    def save_checkpoint(self, path: str, meta: Optional[dict] = None):
+        """Raw checkpoint at `path` plus a JSON header at `path`.json (sizes, iteration, J)."""
+        import json
+        data = self.checkpoint()
+        with open(path, "wb") as f:
+            f.write(data)
+        p = self.problem
+        head = {"format": "gpair_b200 CG checkpoint v1", "bytes": len(data), "width": p.width, "nuv": p.nuv,
+                "npow": p.npow, "nbis": p.nbis}
+        head.update(meta or {})
+        with open(path + ".json", "w") as f:
+            json.dump(head, f, indent=1)
+
+    def load_checkpoint(self, path: str):
+        with open(path, "rb") as f:
+            self.restore(f.read())
 
     def set_regularizer(self, kind: int):
         """REG_GULL_SKILLING (default) or REG_L2."""

@@ -513,6 +513,89 @@ extern "C" int gpair_update_pixel(gpair_ctx *c, int x, int y, float value, doubl
     return (c->sc_host->nonfinite & 3u) ? GPAIR_ERR_NUMERIC : GPAIR_OK;
 }
 
+// ---------------------------------------------------------- checkpoints
+//
+// Layout: CheckpointHeader, CgState (the device controller state), then float
+// arrays of N*N: image, descent direction, previous gradient, current
+// gradient, entropy gradient (kept where the regulariser keeps old values).
+struct CheckpointHeader {
+    char magic[8];  // "GPAIRCK1"
+    int N, nuv, npow, nbis, precision, reg_kind;
+    unsigned int cgstate_bytes, arrays;
+};
+
+static const int kCkArrays = 5;
+
+extern "C" size_t gpair_cg_checkpoint_size(gpair_ctx *c)
+{
+    if (!c || !c->have_problem) return 0;
+    return sizeof(CheckpointHeader) + sizeof(CgState) + (size_t)kCkArrays * c->npix * sizeof(float);
+}
+
+static float *ck_array(gpair_ctx *c, int i)
+{
+    float *a[kCkArrays] = {c->image, c->descent_dir, c->full_grad, c->full_grad_new, c->entropy_grad};
+    return a[i];
+}
+
+extern "C" int gpair_cg_checkpoint_save(gpair_ctx *c, void *buf, size_t bytes)
+{
+    if (!c || !c->have_problem || !buf) return GPAIR_ERR_STATE;
+    if (bytes < gpair_cg_checkpoint_size(c)) return GPAIR_ERR_INVALID;
+    GP_CUDA(c, cudaSetDevice(c->device));
+    int rc = gp_sync_scalars(c);  // waits for the context's stream
+    if (rc) return rc;
+    CheckpointHeader h;
+    memset(&h, 0, sizeof(h));
+    memcpy(h.magic, "GPAIRCK1", 8);
+    h.N = c->N;
+    h.nuv = c->nuv;
+    h.npow = c->npow;
+    h.nbis = c->nbis;
+    h.precision = c->precision;
+    h.reg_kind = c->sc_host->reg_kind;
+    h.cgstate_bytes = sizeof(CgState);
+    h.arrays = kCkArrays;
+    unsigned char *p = (unsigned char *)buf;
+    memcpy(p, &h, sizeof(h));
+    p += sizeof(h);
+    memcpy(p, &c->sc_host->cg, sizeof(CgState));
+    p += sizeof(CgState);
+    for (int i = 0; i < kCkArrays; i++) {
+        GP_CUDA(c, cudaMemcpy(p, ck_array(c, i), sizeof(float) * c->npix, cudaMemcpyDeviceToHost));
+        p += sizeof(float) * c->npix;
+    }
+    return GPAIR_OK;
+}
+
+extern "C" int gpair_cg_checkpoint_load(gpair_ctx *c, const void *buf, size_t bytes)
+{
+    if (!c || !c->have_problem || !buf) return GPAIR_ERR_STATE;
+    if (bytes < gpair_cg_checkpoint_size(c)) return GPAIR_ERR_INVALID;
+    CheckpointHeader h;
+    memcpy(&h, buf, sizeof(h));
+    if (memcmp(h.magic, "GPAIRCK1", 8) || h.cgstate_bytes != sizeof(CgState) || h.arrays != (unsigned)kCkArrays ||
+        h.N != c->N || h.nuv != c->nuv || h.npow != c->npow || h.nbis != c->nbis) {
+        snprintf(c->last_error, sizeof(c->last_error), "checkpoint does not match this problem or build");
+        return GPAIR_ERR_INVALID;
+    }
+    GP_CUDA(c, cudaSetDevice(c->device));
+    int rc = gpair_set_precision(c, h.precision);
+    if (rc) return rc;
+    if ((rc = gpair_set_regularizer(c, h.reg_kind))) return rc;
+    const unsigned char *p = (const unsigned char *)buf + sizeof(h);
+    GP_CUDA(c, cudaMemcpy(&c->sc->cg, p, sizeof(CgState), cudaMemcpyHostToDevice));
+    p += sizeof(CgState);
+    for (int i = 0; i < kCkArrays; i++) {
+        GP_CUDA(c, cudaMemcpy(ck_array(c, i), p, sizeof(float) * c->npix, cudaMemcpyHostToDevice));
+        p += sizeof(float) * c->npix;
+    }
+    c->have_image = 1;
+    c->last_image_src = -1;
+    gp_cg_graph_free(c);
+    return GPAIR_OK;
+}
+
 extern "C" int gpair_stop_flag_create(int **flag)
 {
     if (!flag) return GPAIR_ERR_INVALID;

@@ -25,6 +25,7 @@
 #ifndef GPAIR_B200_H
 #define GPAIR_B200_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -325,6 +326,15 @@ int gpair_set_regularizer(gpair_ctx *ctx, int kind);
  * preceding gpair_criterion on the current image; a gpair_gradient may follow.
  * Returns the new chi2 and regulariser S (either pointer may be NULL). */
 int gpair_update_pixel(gpair_ctx *ctx, int x, int y, float value, double *chi2, double *entropy);
+
+/* Checkpoint / resume of a CG run: the device controller state (iteration, beta
+ * history, line-search state), the image, the descent direction and the gradients,
+ * as one host buffer of gpair_cg_checkpoint_size() bytes (a versioned header, then
+ * raw data). After gpair_cg_checkpoint_load on a context holding the same problem,
+ * gpair_cg_run with resume = 1 continues exactly where the saved run stopped. */
+size_t gpair_cg_checkpoint_size(gpair_ctx *ctx);
+int gpair_cg_checkpoint_save(gpair_ctx *ctx, void *buffer, size_t bytes);
+int gpair_cg_checkpoint_load(gpair_ctx *ctx, const void *buffer, size_t bytes);
 
 /* Stop flag for racing runs: a device int, zeroed at creation and by reset. */
 int gpair_stop_flag_create(int **flag);

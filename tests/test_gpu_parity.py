@@ -472,3 +472,28 @@ def test_autotune_keeps_accuracy_and_caches():
         b.set_image(p.start_image())
         out = b.cg(3, method=2, trace=True, line_search=g.LS_BATCH)
         assert out["iterations"] == 3 and np.all(np.diff(out["trace_J"]) <= 0)
+
+
+@pytest.mark.parametrize("ls", [0, 1])
+def test_checkpoint_resume_in_another_context_is_exact(rec, ls, tmp_path):
+    p = _problem("tiny", (8, 9, 10))
+    rec.set_problem(p)
+    rec.set_precision(g.PREC_SPLIT16)
+    rec.set_image(p.start_image())
+    rec.cg(3, method=2, line_search=ls)
+    path = str(tmp_path / "ck.bin")
+    rec.save_checkpoint(path, {"iteration": 3})
+    a = rec.cg(3, method=2, trace=True, resume=True, line_search=ls)
+    img_a = rec.get_image()
+    with g.Reconstructor(0) as other:
+        other.set_problem(p)
+        other.load_checkpoint(path)
+        b = other.cg(3, method=2, trace=True, resume=True, line_search=ls)
+        assert np.array_equal(a["trace_J"], b["trace_J"])
+        assert np.array_equal(img_a, other.get_image())
+    bad = g.workload_problem("tiny", 1, 2, 3)
+    with g.Reconstructor(0) as third:
+        third.set_problem(bad)
+        if bad.nuv != p.nuv or bad.nbis != p.nbis:
+            with pytest.raises(g.GpairError):
+                third.load_checkpoint(path)
