@@ -203,3 +203,53 @@ def read_oifits(path: str, target_id: int | None = None) -> OIFits:
                 cols["FLAG"].astype(np.uint8)))
     out.target_id = target_id if target_id is not None else (first_target if first_target is not None else 1)
     return out
+
+
+# ------------------------------------------------------------ FITS images
+
+def read_fits_image(path: str):
+    """Primary-HDU image of a FITS file as float32 [NAXIS2][NAXIS1] (x fastest), plus its header cards."""
+    with open(path, "rb") as f:
+        buf = f.read()
+    cards, pos = _parse_header(buf, 0)
+    bitpix = int(cards["BITPIX"])
+    naxis = int(cards.get("NAXIS", "0"))
+    if naxis != 2:
+        raise ValueError(f"{path}: expected a 2-D primary image, NAXIS = {naxis}")
+    nx, ny = int(cards["NAXIS1"]), int(cards["NAXIS2"])
+    dt = {8: "u1", 16: ">i2", 32: ">i4", 64: ">i8", -32: ">f4", -64: ">f8"}[bitpix]
+    data = np.frombuffer(buf, dtype=dt, count=nx * ny, offset=pos).reshape(ny, nx).astype(np.float64)
+    data = data * float(cards.get("BSCALE", "1")) + float(cards.get("BZERO", "0"))
+    return data.astype(np.float32), cards
+
+
+def _card(key: str, value) -> bytes:
+    if isinstance(value, bool):
+        v = "T" if value else "F"
+        s = f"{key:<8}= {v:>20}"
+    elif isinstance(value, (int, np.integer)):
+        s = f"{key:<8}= {int(value):>20}"
+    elif isinstance(value, (float, np.floating)):
+        s = f"{key:<8}= {float(value):>20.12G}"
+    else:
+        text = str(value).replace("'", "''")
+        s = f"{key:<8}= '{text:<8}'"
+    return s[:80].ljust(80).encode("ascii")
+
+
+def write_fits_image(path: str, image: np.ndarray, cards: Dict[str, object] | None = None):
+    """Write a float32 image [ny][nx] as a FITS primary HDU (BITPIX -32, big-endian)."""
+    img = np.asarray(image, np.float32)
+    if img.ndim != 2:
+        raise ValueError("image must be 2-D")
+    head = [_card("SIMPLE", True), _card("BITPIX", -32), _card("NAXIS", 2), _card("NAXIS1", img.shape[1]),
+            _card("NAXIS2", img.shape[0])]
+    for k, v in (cards or {}).items():
+        head.append(_card(k.upper()[:8], v))
+    head.append(b"END".ljust(80))
+    hdr = b"".join(head)
+    hdr += b" " * ((-len(hdr)) % _BLOCK)
+    data = img.astype(">f4").tobytes()
+    data += b"\0" * ((-len(data)) % _BLOCK)
+    with open(path, "wb") as f:
+        f.write(hdr + data)

@@ -497,3 +497,27 @@ def test_checkpoint_resume_in_another_context_is_exact(rec, ls, tmp_path):
         if bad.nuv != p.nuv or bad.nbis != p.nbis:
             with pytest.raises(g.GpairError):
                 third.load_checkpoint(path)
+
+
+def test_cli_reconstruction_writes_fits_log_and_checkpoint(tmp_path):
+    import json as _json
+    from gpair_b200 import reconstruct as R
+    from gpair_b200.oifits import read_fits_image
+    w, oi = synth.make_workload_data("tiny", 21, 22, 23)
+    args = R.build_parser().parse_args(["-s", str(w.pixellation_mas), "-w", str(w.image_width), "-mt", "0",
+                                        "-mf", "1", "-a", "0.001", "--iterations", "6", "--report-every", "3", "--line-search", "batch",
+                                        "--out", str(tmp_path / "r.fits"), "--log", str(tmp_path / "r.jsonl"),
+                                        "--checkpoint", str(tmp_path / "r.ck")])
+    out = R.run(args, oi=oi, quiet=True)
+    assert out["iterations"] == 6
+    img, cards = read_fits_image(str(tmp_path / "r.fits"))
+    assert img.shape == (w.image_width, w.image_width) and np.array_equal(img, out["image"])
+    lines = [_json.loads(l) for l in open(tmp_path / "r.jsonl")]
+    assert [l["iteration"] for l in lines] == list(range(1, 7))
+    assert lines[-1]["J"] < lines[0]["J"]
+    # resume from the checkpoint written after iteration 6: 3 more iterations
+    args2 = R.build_parser().parse_args(["-s", str(w.pixellation_mas), "-w", str(w.image_width), "-mt", "0",
+                                         "-mf", "1", "-a", "0.001", "--iterations", "3", "--line-search", "batch",
+                                         "--resume", str(tmp_path / "r.ck"), "--out", str(tmp_path / "r2.fits")])
+    out2 = R.run(args2, oi=oi, quiet=True)
+    assert out2["iterations"] == 3 and out2["final"]["J"] <= lines[-1]["J"]

@@ -150,3 +150,26 @@ def test_hash_candidates_cover_bucket_boundaries():
     v2 = base * 0.1
     oi = _tables(u1, v1, u2, v2, vis_u, vis_v)
     _same(g.index_oifits(oi), O.ref_index(oi))
+
+
+def test_fits_image_roundtrip(tmp_path):
+    from gpair_b200.oifits import read_fits_image, write_fits_image
+    rng = np.random.default_rng(0)
+    img = rng.uniform(0, 1, (16, 24)).astype(np.float32)
+    path = str(tmp_path / "img.fits")
+    write_fits_image(path, img, {"PIXSCALE": 0.15, "ORIGIN": "test"})
+    assert os.path.getsize(path) % 2880 == 0
+    back, cards = read_fits_image(path)
+    assert np.array_equal(back, img)
+    assert cards["BITPIX"] == "-32" and float(cards["PIXSCALE"]) == 0.15
+
+
+def test_cli_flags_mirror_the_reference_driver():
+    from gpair_b200.reconstruct import build_parser
+    a = build_parser().parse_args(["-d", "x.oifits", "-s", "0.2", "-w", "32", "-mt", "1", "-mw", "3", "-mf", "2",
+                                   "-a", "0.001", "-wavmin", "1.5", "-wavmax", "2.0"])
+    assert (a.data, a.pixellation, a.width, a.modeltype, a.modelwidth, a.modelflux) == ("x.oifits", 0.2, 32, 1, 3.0, 2.0)
+    assert (a.alpha, a.minband, a.maxband) == (0.001, 1.5, 2.0)
+    d = build_parser().parse_args([])
+    # the reference's defaults (gpair1/trunk/gpair.c:78-85)
+    assert (d.pixellation, d.modeltype, d.modelwidth, d.modelflux, d.alpha) == (0.15, 3, 5.0, 10.0, 1000.0)
