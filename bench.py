@@ -473,7 +473,7 @@ def main():
     ap.add_argument("--instance-iters", type=int, default=30)
     ap.add_argument("--line-search", choices=["wolfe", "batch"], default="wolfe",
                     help="line search of the headline steps: the reference's (default) or the batched one")
-    ap.add_argument("--tto-problems", type=int, default=8,
+    ap.add_argument("--tto-problems", type=int, default=16,
                     help="held-out warm-start problems timed for the time-to-objective block")
     ap.add_argument("--host-loop", action="store_true",
                     help="drive the line search from the host instead of the CUDA graph (for profilers that do "
