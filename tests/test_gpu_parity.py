@@ -521,3 +521,73 @@ def test_cli_reconstruction_writes_fits_log_and_checkpoint(tmp_path):
                                          "--resume", str(tmp_path / "r.ck"), "--out", str(tmp_path / "r2.fits")])
     out2 = R.run(args2, oi=oi, quiet=True)
     assert out2["iterations"] == 3 and out2["final"]["J"] <= lines[-1]["J"]
+
+
+# ---------------------------------------------- failures made on the host
+
+def test_nan_in_data_is_reported_not_propagated(rec):
+    """A NaN data value (a corrupt record) makes chi2 non-finite: the criterion
+    returns GPAIR_ERR_NUMERIC and a CG run stops with that status; the context
+    stays usable for the next problem."""
+    p = _problem("tiny", (3, 4, 5))
+    bad = g.Problem(p.width, p.pixellation, p.uv, p.npow, p.nbis, p.data.copy(), p.data_err, p.phasor,
+                    p.uvpnt, p.sign, p.model, p.alpha)
+    bad.data[3] = np.nan
+    rec.set_problem(bad)
+    rec.set_precision(g.PREC_SPLIT16)
+    rec.set_image(p.start_image())
+    with pytest.raises(g.GpairError, match="NUMERIC"):
+        rec.criterion()
+    rec.set_image(p.start_image())
+    with pytest.raises(g.GpairError, match="NUMERIC"):
+        rec.cg(5, method=2)
+    rec.set_problem(p)
+    rec.set_image(p.start_image())
+    chi2, _ = rec.criterion()
+    assert np.isfinite(chi2)
+
+
+def test_oversized_problem_is_rejected_before_allocating(rec):
+    p = _problem("tiny")
+    huge = g.Problem(40000, p.pixellation, p.uv, p.npow, p.nbis, p.data, p.data_err, p.phasor, p.uvpnt, p.sign,
+                     np.zeros(1, np.float32), p.alpha)
+    with pytest.raises(g.GpairError):
+        rec.set_problem(huge)
+    rec.set_problem(p)
+    rec.set_image(p.start_image())
+    assert np.isfinite(rec.criterion()[0])
+
+
+def test_race_falls_back_to_the_flat_start_when_the_warm_start_is_bad():
+    """A deliberately bad start image (all flux in one corner pixel) races the flat
+    prior: the flat-start run reaches the target, the bad run is stopped by the flag."""
+    p = _problem("small", (1, 2, 3))
+
+    with g.Reconstructor(0) as a, g.Reconstructor(0) as b:
+        for r in (a, b):
+            r.set_problem(p)
+            r.set_precision(g.PREC_SPLIT16)
+        b.set_image(p.start_image())
+        ref = b.cg(60, method=2, trace=True, line_search=g.LS_BATCH)
+        target = float(ref["trace_J"][40])
+        flag = g.api.StopFlag()
+        try:
+            spike = np.full(p.npix, 1e-8, np.float32)
+            spike[0] = np.float32(np.sum(p.start_image()))
+            import threading
+            res = {}
+
+            def flat():
+                b.set_image(p.start_image())
+                res["flat"] = b.cg(200, method=2, line_search=g.LS_BATCH, target_J=target, stop_flag=flag.ptr)
+
+            th = threading.Thread(target=flat)
+            th.start()
+            a.set_image(spike)
+            warm = a.cg(200, method=2, line_search=g.LS_BATCH, target_J=target, stop_flag=flag.ptr)
+            th.join()
+            assert res["flat"]["reached"]
+            assert warm["stopped"] or warm["reached"]
+            assert res["flat"]["iterations"] <= 42
+        finally:
+            flag.close()

@@ -63,3 +63,38 @@ def test_cnn_training_reduces_loss():
     for _ in range(30):
         last = float(net.train_step(xt, tt, 1e-3).mean())
     assert last < 0.5 * first
+
+
+def test_trained_network_gains_over_the_flat_start():
+    """What the trained network gains over plain CG's flat start, on held-out
+    problems (seeds never used in training): its start image has a lower
+    objective J than the flat prior, and CG started from it needs fewer
+    batched-line-search iterations to reach the objective that flat-start CG
+    reaches after 300 iterations (summed over the problems)."""
+    import gpair_b200 as g
+    from gpair_b200.train_warmstart import SEED_HELD_OUT
+    from gpair_b200.warmstart import WarmStartNet, training_case, warm_start
+    net = WarmStartNet.load()
+    better, it_flat, it_warm = 0, 0, 0
+    n = 8
+    with g.Reconstructor(0) as rec:
+        rec.set_precision(g.PREC_SPLIT16)
+        for k in range(n):
+            p = training_case(SEED_HELD_OUT + 100 + k, 64).problem
+            rec.set_problem(p)
+            rec.set_image(p.start_image())
+            chi2, S = rec.criterion()
+            J_flat = chi2 - p.alpha * S
+            img = warm_start(net, rec, p)
+            rec.set_image(img)
+            chi2, S = rec.criterion()
+            better += (chi2 - p.alpha * S) < J_flat
+            rec.set_image(p.start_image())
+            ref = rec.cg(300, method=2, trace=True, line_search=g.LS_BATCH)
+            target = float(ref["trace_J"][-1]) * (1 + 1e-4)
+            rec.set_image(p.start_image())
+            it_flat += rec.cg(300, method=2, line_search=g.LS_BATCH, target_J=target)["iterations"]
+            rec.set_image(img)
+            it_warm += rec.cg(300, method=2, line_search=g.LS_BATCH, target_J=target)["iterations"]
+    print(f"warm start better than flat on {better}/{n}; iterations to target: flat {it_flat}, warm {it_warm}")
+    assert better >= n - 1
