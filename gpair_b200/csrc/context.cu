@@ -188,6 +188,7 @@ int gp_set_problem_core(gpair_ctx *c, int N, float pix, int nuv, const gpair_uv 
     int rc = gp_alloc_images(c, N);
     if (rc) return rc;
     free_problem(c);
+    GP_CUDA(c, cudaMemsetAsync(&c->sc->nonfinite, 0, sizeof(unsigned int), c->stream));
     c->pix = pix;
     c->nuv = nuv;
     c->npow = npow;
@@ -418,6 +419,8 @@ extern "C" int gpair_criterion(gpair_ctx *c, int which, double *chi2, double *en
 {
     if (!c || !c->have_problem) return GPAIR_ERR_STATE;
     GP_CUDA(c, cudaSetDevice(c->device));
+    // the non-finite flag describes this evaluation, not an earlier one
+    GP_CUDA(c, cudaMemsetAsync(&c->sc->nonfinite, 0, sizeof(unsigned int), c->stream));
     int rc = gp_eval_criterion(c, which, 0);
     if (rc) return rc;
     if ((rc = gp_sync_scalars(c))) return rc;
@@ -505,6 +508,7 @@ extern "C" int gpair_update_pixel(gpair_ctx *c, int x, int y, float value, doubl
     if (c->last_image_src != GPAIR_IMG_CURR) return GPAIR_ERR_STATE;  // V must be the current image's
     if (x < 0 || y < 0 || x >= c->N || y >= c->N || !(value == value)) return GPAIR_ERR_INVALID;
     GP_CUDA(c, cudaSetDevice(c->device));
+    GP_CUDA(c, cudaMemsetAsync(&c->sc->nonfinite, 0, sizeof(unsigned int), c->stream));
     int rc = gp_update_pixel(c, x, y, value);
     if (rc) return rc;
     if ((rc = gp_sync_scalars(c))) return rc;
