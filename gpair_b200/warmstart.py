@@ -10,7 +10,7 @@ supplies the stream.
 Network (channels 16-32-64-128, 3x3 convolutions, ReLU, BF16 weights with
 FP32 accumulation):
 
-    x [3,H,W] -> e1 (2 convs, 16) -> pool -> e2 (32) -> pool -> e3 (64) -> pool -> e4 (128)
+    x [4,H,W] -> e1 (2 convs, 16) -> pool -> e2 (32) -> pool -> e3 (64) -> pool -> e4 (128)
     e4 -> up -> conv 64 + e3 -> conv 64 -> up -> conv 32 + e2 -> conv 32
        -> up -> conv 16 + e1 -> conv 16 -> 1x1 conv -> softplus -> / sum
 
@@ -24,7 +24,11 @@ Inputs of one problem (:func:`features`), each scaled to max |value| 1:
              the uv coverage samples it, centred (gpair_adjoint_image);
   channel 2  uv density: the (u, v) points and their conjugates gridded on the
              image's Fourier grid (cell = u * pixel size * N), log(1 + count),
-             zero frequency at the centre.
+             zero frequency at the centre;
+  channel 3  probe gradient: -d chi2 / dI at a centred Gaussian of FWHM N/4
+             pixels with the prior's flux. Its visibilities are non-zero on
+             every baseline, so the closure-phase residuals reach the gradient
+             (at the flat image they nearly vanish).
 """
 from __future__ import annotations
 
@@ -40,7 +44,7 @@ from . import api
 from .synth import ArrayConfig, Component, Scene, make_oifits
 
 RPMAS = (math.pi / 180.0) / 3600000.0
-N_FEATURES = 3
+N_FEATURES = 4
 LAYERS: Tuple[Tuple[str, int, int], ...] = (
     ("e1a", N_FEATURES, 16), ("e1b", 16, 16), ("e2a", 16, 32), ("e2b", 32, 32), ("e3a", 32, 64), ("e3b", 64, 64),
     ("e4a", 64, 128), ("e4b", 128, 128), ("d3a", 128, 64), ("d3b", 64, 64), ("d2a", 64, 32), ("d2b", 32, 32),
@@ -368,8 +372,23 @@ def v2_dirty_map(rec: api.Reconstructor, p: api.Problem) -> np.ndarray:
     return (img / m if m > 0 else img).reshape(N, N).astype(np.float32)
 
 
+def probe_gradient(rec: api.Reconstructor, p: api.Problem) -> np.ndarray:
+    """-d chi2/dI at a centred Gaussian (FWHM N/4 pixels, the prior's flux), max |value| 1."""
+    N = p.width
+    y, x = np.mgrid[0:N, 0:N].astype(np.float64)
+    sig = (N / 4.0) / 2.3548
+    gauss = np.exp(-((x - N // 2) ** 2 + (y - N // 2) ** 2) / (2 * sig * sig))
+    img = gauss / gauss.sum() * float(np.sum(p.start_image(), dtype=np.float64))
+    rec.set_image(np.maximum(img, 1e-8).astype(np.float32).ravel())
+    rec.criterion()
+    rec.gradient(alpha=0.0)
+    g = -rec.data_gradient().astype(np.float64)
+    m = np.abs(g).max()
+    return (g / m if m > 0 else g).reshape(N, N).astype(np.float32)
+
+
 def features(rec: api.Reconstructor, p: api.Problem) -> np.ndarray:
-    return np.stack([dirty_image(rec, p), v2_dirty_map(rec, p), uv_density(p)])
+    return np.stack([dirty_image(rec, p), v2_dirty_map(rec, p), uv_density(p), probe_gradient(rec, p)])
 
 
 def warm_start(net: WarmStartNet, rec: api.Reconstructor, p: api.Problem, feats: Optional[np.ndarray] = None):
