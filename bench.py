@@ -314,6 +314,9 @@ def run_ours(args, rank, world, local):
     rec.set_precision(prec)
     rec.set_stage_timing(True)
     rec.set_image(p.start_image())
+    # autotuned adjoint split-K length (precision stays as requested)
+    tune = rec.autotune(g.api.TUNE_SPLITS, reps=3)
+    rec.set_image(p.start_image())
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
 
     # warm-up iterations (untimed); builds the CG graph
@@ -422,6 +425,7 @@ def run_ours(args, rank, world, local):
                                     if args.line_search == "wolfe" else
                                     "one PR+ CG iteration with the batched 8-trial line search (continuing)"),
                            "precision": args.precision, "evaluations": evals,
+                           "autotuned_adjoint_splits": tune["adjoint_splits"],
                            "l2": "flushed (512 MiB write) before every timed step, outside the timed region",
                            "parallelism": f"replicas x{world}",
                            "cg_driver": "host loop" if args.host_loop else "one CUDA graph per step"},

@@ -469,12 +469,17 @@ __global__ void k_tc_fy_anchors(const float2 *__restrict__ fy, int nuv, int N, i
 
 // Adjoint A operand W[y][2k+c] from c_k and Fy[k][y], one global power-of-two
 // scale from max |c_k|; 32 uv x 32 rows per block, transposed through smem so
-// that reads of Fy and writes of W are both coalesced.
-__global__ void __launch_bounds__(256) k_tc_build_w(const float2 *__restrict__ cw, const float2 *__restrict__ fy,
-                                                    int nuv, int N, int K2_pad, __half *__restrict__ w_hi,
-                                                    __half *__restrict__ w_lo, DevScalars *__restrict__ sc)
+// that the writes of W are coalesced. Fy[k][y] is rebuilt from the forward's
+// FP64-accurate anchors Fy[k][16 j] and the per-uv rotation powers r_k^p,
+// p < 16 (formed in FP64 in shared memory), so the kernel reads 2.7 MB of
+// anchors instead of the full 43 MB table at 256^2.
+__global__ void __launch_bounds__(256) k_tc_build_w(const float2 *__restrict__ cw, const float2 *__restrict__ fya,
+                                                    const float2 *__restrict__ fyr, int nanc, int nuv, int N,
+                                                    int K2_pad, __half *__restrict__ w_hi, __half *__restrict__ w_lo,
+                                                    DevScalars *__restrict__ sc)
 {
     __shared__ float2 tile[32][33];
+    __shared__ float2 pw[32][16];
     const double cmax = sc->cmax;
     int ex = 0;
     float wscale = 1.f;
@@ -485,12 +490,27 @@ __global__ void __launch_bounds__(256) k_tc_build_w(const float2 *__restrict__ c
     if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0)
         sc->gscale = 1.0 / ((double)wscale * (double)(1 << TC_TW_LOG2));
     const int k0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
+    for (int i = threadIdx.x; i < 32 * 16; i += blockDim.x) {
+        const int kl = i >> 4, pp = i & 15, k = k0 + kl;
+        double zr = 1.0, zi = 0.0;
+        if (k < nuv) {
+            const float2 r = fyr[k];
+            for (int q = 0; q < pp; q++) {
+                const double t = zr * r.x - zi * r.y;
+                zi = zr * r.y + zi * r.x;
+                zr = t;
+            }
+        }
+        pw[kl][pp] = make_float2((float)zr, (float)zi);
+    }
+    __syncthreads();
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
     for (int j = ty; j < 32; j += 8) {
         int k = k0 + j, y = y0 + tx;
         float2 w = make_float2(0.f, 0.f);
         if (k < nuv && y < N) {
-            float2 c = cw[k], f = fy[(size_t)k * N + y];
+            const float2 c = cw[k], a = fya[(size_t)k * nanc + (y >> 4)], q = pw[j][y & 15];
+            const float2 f = make_float2(a.x * q.x - a.y * q.y, a.x * q.y + a.y * q.x);
             w = make_float2((c.x * f.x - c.y * f.y) * wscale, -(c.x * f.y + c.y * f.x) * wscale);
         }
         tile[j][tx] = w;  // [k][y]
@@ -824,7 +844,8 @@ int gp_tc_build_w(gpair_ctx *c)
     TcState *t = tc_state_ready(c, &rc);
     if (rc) return rc;
     dim3 g(gp_cdiv(c->nuv ? c->nuv : 1, 32), gp_cdiv(c->N, 32));
-    k_tc_build_w<<<g, 256, 0, c->stream>>>(c->cw, c->fy, c->nuv, c->N, t->K2_pad, t->w_hi, t->w_lo, c->sc);
+    k_tc_build_w<<<g, 256, 0, c->stream>>>(c->cw, t->fya, t->fyr, t->nanc, c->nuv, c->N, t->K2_pad, t->w_hi,
+                                           t->w_lo, c->sc);
     GP_LAUNCH_CHECK(c);
     return GPAIR_OK;
 }
