@@ -140,6 +140,7 @@ struct gpair_ctx {
     int N, npix, nuv, npow, nbis, ndata;
     float pix;
     int have_problem, have_image;
+    int have_uv;      // the problem came with (u, v) (else: the reference's DFT tables only)
     int mt;           // number of row tiles of the forward DFT
     int splits;       // split-K factor of the last adjoint (number of partial images)
     int splits_simt;  // split-K factor of the CUDA-core adjoint

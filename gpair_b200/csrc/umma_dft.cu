@@ -49,6 +49,7 @@
 #define TC_TMEM_COLS 512
 #define TC_SMEM_BYTES (1024 + TC_STAGES * TC_STAGE_BYTES + 256)
 #define TC_WAIT_BUDGET 4000000000LL  // clock cycles (~2 s) per wait
+#define RPMAS_TC ((3.14159265358979323 / 180.0) / 3600000.0)  // radians per milliarcsecond
 
 enum { EPI_FWD = 0, EPI_STORE = 1 };
 
@@ -469,17 +470,19 @@ __global__ void k_tc_fy_anchors(const float2 *__restrict__ fy, int nuv, int N, i
 
 // Adjoint A operand W[y][2k+c] from c_k and Fy[k][y], one global power-of-two
 // scale from max |c_k|; 32 uv x 32 rows per block, transposed through smem so
-// that the writes of W are coalesced. Fy[k][y] is rebuilt from the forward's
-// FP64-accurate anchors Fy[k][16 j] and the per-uv rotation powers r_k^p,
-// p < 16 (formed in FP64 in shared memory), so the kernel reads 2.7 MB of
-// anchors instead of the full 43 MB table at 256^2.
-__global__ void __launch_bounds__(256) k_tc_build_w(const float2 *__restrict__ cw, const float2 *__restrict__ fya,
-                                                    const float2 *__restrict__ fyr, int nanc, int nuv, int N,
+// that the writes of W are coalesced. Fy[k][y] = e^{-2 pi i s v_k y} is formed
+// in place, as k_gen_twiddles forms the table (phase in turns in FP64, reduced
+// to [-1/2, 1/2]) with the final sincos in FP32: the kernel reads no table and
+// writes only W. Problems given as the reference's tables (no (u, v)) read Fy
+// from the table instead (uvc == nullptr).
+__global__ void __launch_bounds__(256) k_tc_build_w(const float2 *__restrict__ cw, const float2 *__restrict__ uvc,
+                                                    const float2 *__restrict__ fy, float pix, int nuv, int N,
                                                     int K2_pad, __half *__restrict__ w_hi, __half *__restrict__ w_lo,
                                                     DevScalars *__restrict__ sc)
 {
     __shared__ float2 tile[32][33];
-    __shared__ float2 pw[32][16];
+    __shared__ double sv[32];
+    __shared__ float2 cs[32];
     const double cmax = sc->cmax;
     int ex = 0;
     float wscale = 1.f;
@@ -490,18 +493,10 @@ __global__ void __launch_bounds__(256) k_tc_build_w(const float2 *__restrict__ c
     if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0)
         sc->gscale = 1.0 / ((double)wscale * (double)(1 << TC_TW_LOG2));
     const int k0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
-    for (int i = threadIdx.x; i < 32 * 16; i += blockDim.x) {
-        const int kl = i >> 4, pp = i & 15, k = k0 + kl;
-        double zr = 1.0, zi = 0.0;
-        if (k < nuv) {
-            const float2 r = fyr[k];
-            for (int q = 0; q < pp; q++) {
-                const double t = zr * r.x - zi * r.y;
-                zi = zr * r.y + zi * r.x;
-                zr = t;
-            }
-        }
-        pw[kl][pp] = make_float2((float)zr, (float)zi);
+    if (threadIdx.x < 32) {
+        const int k = k0 + threadIdx.x;
+        sv[threadIdx.x] = (k < nuv && uvc) ? RPMAS_TC * (double)pix * (double)uvc[k].y : 0.0;
+        cs[threadIdx.x] = k < nuv ? cw[k] : make_float2(0.f, 0.f);
     }
     __syncthreads();
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
@@ -509,8 +504,17 @@ __global__ void __launch_bounds__(256) k_tc_build_w(const float2 *__restrict__ c
         int k = k0 + j, y = y0 + tx;
         float2 w = make_float2(0.f, 0.f);
         if (k < nuv && y < N) {
-            const float2 c = cw[k], a = fya[(size_t)k * nanc + (y >> 4)], q = pw[j][y & 15];
-            const float2 f = make_float2(a.x * q.x - a.y * q.y, a.x * q.y + a.y * q.x);
+            float2 f;
+            if (uvc) {
+                double t = sv[j] * (double)y;
+                t -= rint(t);
+                float sn, cn;
+                sincospif((float)(2.0 * t), &sn, &cn);
+                f = make_float2(cn, -sn);
+            } else {
+                f = fy[(size_t)k * N + y];
+            }
+            const float2 c = cs[j];
             w = make_float2((c.x * f.x - c.y * f.y) * wscale, -(c.x * f.y + c.y * f.x) * wscale);
         }
         tile[j][tx] = w;  // [k][y]
@@ -844,8 +848,8 @@ int gp_tc_build_w(gpair_ctx *c)
     TcState *t = tc_state_ready(c, &rc);
     if (rc) return rc;
     dim3 g(gp_cdiv(c->nuv ? c->nuv : 1, 32), gp_cdiv(c->N, 32));
-    k_tc_build_w<<<g, 256, 0, c->stream>>>(c->cw, t->fya, t->fyr, t->nanc, c->nuv, c->N, t->K2_pad, t->w_hi,
-                                           t->w_lo, c->sc);
+    k_tc_build_w<<<g, 256, 0, c->stream>>>(c->cw, c->have_uv ? c->uvc : nullptr, c->fy, c->pix, c->nuv, c->N,
+                                           t->K2_pad, t->w_hi, t->w_lo, c->sc);
     GP_LAUNCH_CHECK(c);
     return GPAIR_OK;
 }

@@ -93,8 +93,9 @@ def test_cg_methods_run_and_descend(rec):
         assert out["trace_J"][-1] <= out["trace_J"][0]
 
 
-def _ref_boundary_run(p, iters, alpha):
-    """The reference's GPU-path main loop (gpair1/trunk/gpair.c:640-915) through the gpu_* C ABI."""
+def _ref_boundary_run(p, iters, alpha, prec=g.PREC_FP32):
+    """The reference's GPU-path main loop (gpair1/trunk/gpair.c:640-915) through the gpu_* C ABI.
+    prec selects the global context's precision path (set through the layer-2 handle)."""
     L = g.lib()  # prototypes of the gpu_* boundary are declared by gpair_b200.api
     L.gpair_set_exit_on_error(0)
     N, nuv, npow, nbis = p.width, p.nuv, p.npow, p.nbis
@@ -119,6 +120,7 @@ def _ref_boundary_run(p, iters, alpha):
     L.gpu_copy_image(image.ctypes.data, N, N)
     L.gpu_copy_dft(gx.ctypes.data, gy.ctypes.data, len(gx))
     L.gpu_build_kernels(len(data), N, N * N)
+    assert L.gpair_set_precision(L.gpair_global_context(), prec) == 0
     fgn, fg, dd, tg, ci = L.gpu_getp_fgn(), L.gpu_getp_fg(), L.gpu_getp_dd(), L.gpu_getp_tg(), L.gpu_getp_ci()
     Js = []
     ce, ge = C.c_int(0), C.c_int(0)
@@ -170,14 +172,18 @@ def _ref_boundary_run(p, iters, alpha):
         L.gpu_backup_gradient(N * N, fgn, fg)
     out = np.zeros(N * N, np.float32)
     L.gpu_get_image(N * N, out.ctypes.data, ci)
+    L.gpair_set_precision(L.gpair_global_context(), g.PREC_FP32)
     L.gpu_cleanup()
     return np.array(Js), out
 
 
-def test_reference_boundary_loop_matches_fp64_cg():
+@pytest.mark.parametrize("prec", PRECISIONS)
+def test_reference_boundary_loop_matches_fp64_cg(prec):
+    """The reference's own loop through layer 1; with split16 the tensor path runs on
+    the reference's DFT tables (no (u, v) given)."""
     p = _problem("tiny", (21, 22, 23))
     iters = 5
-    Js, _ = _ref_boundary_run(p, iters, p.alpha)
+    Js, _ = _ref_boundary_run(p, iters, p.alpha, prec)
     _, tr = O.reconstruct64(p, p.start_image(), iters)
     assert np.allclose(Js[:3], tr["J"][:3], rtol=1e-4)
     assert Js[-1] < Js[0]
