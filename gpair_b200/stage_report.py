@@ -1,0 +1,102 @@
+"""Achieved bandwidth and FLOP rate of every stage of one criterion + gradient
+evaluation, for the named workloads.
+
+    python -m gpair_b200.stage_report [--workloads precision large] [--reps 10]
+
+Stages and time: `Reconstructor.time_stages` (CUDA events around the stages
+queued back to back), split-f16 tensor path.
+
+Bytes per stage are the stage's compulsory traffic, as its kernels move it:
+
+  prep           image + prior read for flux / entropy / max (8 B/px), image
+                 read again and the f16 hi/lo operand written (8 B/px)
+  vis_data       V2: partial visibilities (8 B per row tile), data + inverse
+                 error (8 B), visibilities written (16 + 8 B), mock (4 B), uv
+                 weight (8 B); T3: indices (16 B), three gathered visibilities
+                 (3 x 8 B per row tile), phasor (8 B), data + error (16 B),
+                 mock (8 B), vertex weights written (24 B)
+  adj_weights    uv weights + CSR gather of vertex weights (16 B per point +
+                 12 B per triangle vertex), then the adjoint's f16 hi/lo weight
+                 operand W written (8 B per pixel row per uv point: 8 N nuv)
+  grad_finalize  S split partial images read (4 S B/px), image, prior,
+                 previous gradient and direction read (16 B/px), data, entropy
+                 and full gradient written (12 B/px)
+  forward_dft / adjoint_dft  algorithmic FLOPs 4 N^2 nuv + 8 N nuv (TFLOP/s);
+                 executed = 3 x (three f16 products per algorithmic product)
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+
+from . import api
+
+
+def stage_bytes(p: api.Problem, splits: int, row_tiles: int) -> dict:
+    N, K, T = p.width, p.nuv, p.nbis
+    px = N * N
+    return {
+        "prep": 16 * px,
+        "vis_data": p.npow * (8 * row_tiles + 8 + 24 + 4 + 8) + T * (16 + 24 * row_tiles + 8 + 16 + 8 + 24),
+        "adj_weights": 16 * K + 12 * 3 * T + 8 * N * K,
+        "grad_finalize": (4 * splits + 28) * px,
+    }
+
+
+def report(name: str, reps: int = 10) -> dict:
+    p = api.workload_problem(name)
+    with api.Reconstructor(0) as rec:
+        rec.set_problem(p)
+        rec.set_precision(api.PREC_SPLIT16)
+        rec.set_image(p.start_image())
+        rec.criterion()
+        rec.gradient()
+        st = rec.time_stages(reps=reps)
+    peaks_path = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "MEASURED_PEAKS.json")
+    hbm, tf = 6650.0, 1590.0
+    if os.path.exists(peaks_path):
+        with open(peaks_path) as f:
+            d = json.load(f)
+        hbm, tf = d["hbm_gbs"], d["bf16_tflops"]
+    row_tiles = (p.width + 255) // 256
+    splits = _default_splits(p)
+    by = stage_bytes(p, splits, row_tiles)
+    out = {"workload": name, "N": p.width, "nuv": p.nuv, "npow": p.npow, "nbis": p.nbis, "splits": splits,
+           "hbm_peak_gbs": hbm, "tensor_peak_tflops": tf, "stages": {}}
+    for k, ms in st.items():
+        row = {"ms": ms}
+        if k in by:
+            gbs = by[k] / (ms * 1e-3) / 1e9
+            row.update({"bytes": by[k], "gbs": gbs, "hbm_frac": gbs / hbm})
+        else:
+            tfl = p.dft_flops() / (ms * 1e-3) / 1e12
+            row.update({"tflops": tfl, "frac": tfl / tf, "executed_frac": 3 * tfl / tf})
+        out["stages"][k] = row
+    return out
+
+
+def _default_splits(p: api.Problem) -> int:
+    """Split count of the tensor adjoint as the library chooses it (mirrors gp_tc_splits)."""
+    N, K = p.width, p.nuv
+    m_pad = -(-N // 256) * 256
+    xrows = -(-N // 128) * 128
+    k2 = -(-2 * K // 64) * 64
+    tiles = (xrows // 128) * (m_pad // 256)
+    kb_total = k2 // 64
+    want = max(1, min(kb_total, -(-148 // tiles)))
+    kb_per = min(64, -(-kb_total // want))
+    return -(-kb_total // kb_per)
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--workloads", nargs="+", default=["precision", "large"])
+    ap.add_argument("--reps", type=int, default=10)
+    args = ap.parse_args(argv)
+    for w in args.workloads:
+        print(json.dumps(report(w, args.reps)), flush=True)
+
+
+if __name__ == "__main__":
+    main()
