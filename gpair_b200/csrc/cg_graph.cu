@@ -108,15 +108,21 @@ static int capture(gpair_ctx *c, CgGraph *G, int seq, cudaGraphConditionalHandle
     return GPAIR_OK;
 }
 
-void gp_cg_graph_free(gpair_ctx *c)
+static void graph_free_one(gpair_ctx *c, int mode)
 {
-    CgGraph *G = (CgGraph *)c->cg_graph;
+    CgGraph *G = (CgGraph *)c->cg_graph[mode];
     if (!G) return;
     if (G->exec) cudaGraphExecDestroy(G->exec);
     if (G->g) cudaGraphDestroy(G->g);
     if (G->trace) cudaFree(G->trace);
     free(G);
-    c->cg_graph = nullptr;
+    c->cg_graph[mode] = nullptr;
+}
+
+void gp_cg_graph_free(gpair_ctx *c)
+{
+    graph_free_one(c, 0);
+    graph_free_one(c, 1);
 }
 
 static cudaGraphNode_t add_conditional(gpair_ctx *c, cudaGraph_t parent, cudaGraphConditionalHandle h,
@@ -139,7 +145,7 @@ static cudaGraphNode_t add_conditional(gpair_ctx *c, cudaGraph_t parent, cudaGra
 
 static int build(gpair_ctx *c, int trace_cap, int ls_mode)
 {
-    gp_cg_graph_free(c);
+    graph_free_one(c, ls_mode);
     if (c->precision != GPAIR_PREC_FP32) {
         int rc = gp_tc_prepare(c);  // operand buffers must exist before capture
         if (rc) return rc;
@@ -150,7 +156,7 @@ static int build(gpair_ctx *c, int trace_cap, int ls_mode)
     }
     CgGraph *G = (CgGraph *)calloc(1, sizeof(CgGraph));
     if (!G) return GPAIR_ERR_ALLOC;
-    c->cg_graph = G;
+    c->cg_graph[ls_mode] = G;
     G->precision = c->precision;
     G->ls_mode = ls_mode;
     G->trace_cap = trace_cap;
@@ -198,7 +204,7 @@ static int build(gpair_ctx *c, int trace_cap, int ls_mode)
     }
     for (int q = 0; q < 4; q++)
         if (S[q]) cudaGraphDestroy(S[q]);
-    if (rc) gp_cg_graph_free(c);
+    if (rc) graph_free_one(c, ls_mode);
     return rc;
 }
 
@@ -206,12 +212,14 @@ static int build(gpair_ctx *c, int trace_cap, int ls_mode)
 // it executed through *launches (from the controller's evaluation counters).
 int gp_cg_graph_run(gpair_ctx *c, int iterations, int want_trace, int ls_mode, long long *launches)
 {
-    CgGraph *G = (CgGraph *)c->cg_graph;
+    if (ls_mode < 0 || ls_mode > 1) return GPAIR_ERR_INVALID;
+    c->cg_graph_mode = ls_mode;
+    CgGraph *G = (CgGraph *)c->cg_graph[ls_mode];
     int cap = iterations > 4096 ? iterations : 4096;
-    if (!G || G->precision != c->precision || G->ls_mode != ls_mode || (want_trace && G->trace_cap < iterations)) {
+    if (!G || G->precision != c->precision || (want_trace && G->trace_cap < iterations)) {
         int rc = build(c, cap, ls_mode);
         if (rc) return rc;
-        G = (CgGraph *)c->cg_graph;
+        G = (CgGraph *)c->cg_graph[ls_mode];
     }
     if (iterations > 0) GP_CUDA(c, cudaGraphLaunch(G->exec, c->stream));
     *launches = 0;
@@ -221,7 +229,7 @@ int gp_cg_graph_run(gpair_ctx *c, int iterations, int want_trace, int ls_mode, l
 int gp_cg_graph_trace(gpair_ctx *c, int iterations, double *tJ, double *tchi2, double *tS, double *tstep,
                       double *tbeta)
 {
-    CgGraph *G = (CgGraph *)c->cg_graph;
+    CgGraph *G = (CgGraph *)c->cg_graph[c->cg_graph_mode];
     if (!G || iterations <= 0) return GPAIR_OK;
     int n = iterations < G->trace_cap ? iterations : G->trace_cap;
     double *h = (double *)malloc(sizeof(double) * 5 * (size_t)n);
@@ -247,7 +255,7 @@ int gp_cg_graph_trace(gpair_ctx *c, int iterations, double *tJ, double *tchi2, d
 // kernel launches a finished graph run executed
 long long gp_cg_graph_launches(gpair_ctx *c, int iterations_done, int criterion_evals, int grad_evals, int batches)
 {
-    CgGraph *G = (CgGraph *)c->cg_graph;
+    CgGraph *G = (CgGraph *)c->cg_graph[c->cg_graph_mode];
     if (!G) return 0;
     long long base = (long long)iterations_done * (G->n_pre + G->n_post);
     if (G->ls_mode == GPAIR_LS_BATCH) return base + (long long)batches * G->n_crit;

@@ -191,8 +191,10 @@ struct gpair_ctx {
     double *partials_b;
     int epp;  // forward partial entries per trial image
 
-    // graph-captured CG (cg_graph.cu)
-    void *cg_graph;
+    // graph-captured CG (cg_graph.cu): one graph per line-search mode, so that
+    // alternating modes does not re-capture; cg_graph_mode = the mode last run
+    void *cg_graph[2];
+    int cg_graph_mode;
     // controller fused into the next reduction kernel launched (-1: none)
     int fuse_ctrl, fuse_handles;
     unsigned long long fh_iter, fh_ls, fh_grad;

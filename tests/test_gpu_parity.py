@@ -597,3 +597,18 @@ def test_race_falls_back_to_the_flat_start_when_the_warm_start_is_bad():
             assert res["flat"]["iterations"] <= 42
         finally:
             flag.close()
+
+
+def test_alternating_line_searches_reuse_their_graphs(rec):
+    """One captured graph per line-search mode: alternating modes gives the same
+    results as fresh runs (the cache holds both)."""
+    p = _problem("tiny", (12, 13, 14))
+    rec.set_problem(p)
+    rec.set_precision(g.PREC_SPLIT16)
+    outs = []
+    for ls in (0, 1, 0, 1):
+        rec.set_image(p.start_image())
+        outs.append(rec.cg(3, method=2, trace=True, line_search=ls))
+    assert np.array_equal(outs[0]["trace_J"], outs[2]["trace_J"])
+    assert np.array_equal(outs[1]["trace_J"], outs[3]["trace_J"])
+    assert outs[1]["criterion_evals"] % g.LS_TRIALS == 3 % g.LS_TRIALS
