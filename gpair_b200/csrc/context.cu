@@ -239,6 +239,10 @@ int gp_set_problem_core(gpair_ctx *c, int N, float pix, int nuv, const gpair_uv 
     // the entropy-gradient buffer starts at zero: where image <= 0 or model <= 0
     // it keeps its previous value (gpair1/trunk/gpu.c:1332-1338, kernel_entropy_gs_grad.cl)
     GP_CUDA(c, cudaMemsetAsync(c->entropy_grad, 0, c->npix * sizeof(float), c->stream));
+    // a new problem starts without CG history (same-width image buffers are reused)
+    GP_CUDA(c, cudaMemsetAsync(c->descent_dir, 0, c->npix * sizeof(float), c->stream));
+    GP_CUDA(c, cudaMemsetAsync(c->full_grad, 0, c->npix * sizeof(float), c->stream));
+    GP_CUDA(c, cudaMemsetAsync(c->full_grad_new, 0, c->npix * sizeof(float), c->stream));
     c->have_uv = uv && nuv;
     if (uv && nuv) {
         std::vector<float2> uvc(nuv);

@@ -776,7 +776,9 @@ __global__ void __launch_bounds__(GP_THREADS) k_descent(float *__restrict__ d, c
     double acc[1] = {0.0};
     double dmax = 0.0;
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
-        float dn = (float)(beta * (double)d[p] - (double)g[p]);
+        // beta = 0 (first iteration, restarts) must not read the old direction:
+        // 0 * d_old is NaN when a previous run left non-finite values there
+        float dn = beta != 0.0 ? (float)(beta * (double)d[p] - (double)g[p]) : -g[p];
         d[p] = dn;
         acc[0] += (double)dn * (double)g[p];
         dmax = fmax(dmax, fabs((double)dn));
