@@ -184,9 +184,11 @@ def combine_over_ranks(times, work, device=None):
 
 def many_instances(n: int, iters: int) -> dict:
     """n independent reconstructions of uneven size (widths 64-256, 500-8,000 uv)
-    for `iters` batched-line-search CG iterations each: one after another, then
-    all at once through gpair_cg_run_many (each context's graph on its own
-    stream). Host wall clock; problem loading is outside both timings."""
+    for `iters` batched-line-search CG iterations each: one after another, all
+    at once through gpair_cg_run_many (each context's graph on its own stream),
+    and as one graph launch (gpair_batch_run: every CG loop a branch of one
+    graph). Host wall clock; problem loading and graph capture are outside the
+    timings."""
     import gpair_b200 as g
     from gpair_b200.instances import instances
     ps = instances(n)
@@ -218,6 +220,17 @@ def many_instances(n: int, iters: int) -> dict:
         res = g.cg_many(recs, iters, line_search=g.LS_BATCH)
         t_con = time.perf_counter() - t0
         flops_con = sum(r.last_run_stats()[1] for r in recs)
+        # all instances' CG loops as branches of one graph: one launch
+        with g.api.Batch(recs, line_search=g.LS_BATCH) as b:
+            for r, p in zip(recs, ps):
+                r.set_image(p.start_image())
+            b.run(1)  # first launch
+            for r, p in zip(recs, ps):
+                r.set_image(p.start_image())
+            t0 = time.perf_counter()
+            res_b = b.run(iters)
+            t_one = time.perf_counter() - t0
+            flops_one = sum(r.last_run_stats()[1] for r in recs)
     finally:
         for r in recs:
             r.close()
@@ -227,7 +240,9 @@ def many_instances(n: int, iters: int) -> dict:
             "sequential_s": t_seq, "concurrent_s": t_con, "speedup": t_seq / max(t_con, 1e-12),
             "instances_per_s": n / max(t_con, 1e-12), "tflops_concurrent": flops_con / max(t_con, 1e-12) / 1e12,
             "tflops_sequential": flops / max(t_seq, 1e-12) / 1e12,
-            "all_ok": all(r_["status"] == 0 for r_ in res),
+            "one_launch_s": t_one, "one_launch_speedup": t_seq / max(t_one, 1e-12),
+            "tflops_one_launch": flops_one / max(t_one, 1e-12) / 1e12,
+            "all_ok": all(r_["status"] == 0 for r_ in res) and all(r_["status"] == 0 for r_ in res_b),
             "autotune": {"s": t_tune, "tuned": sum(not t["from_cache"] for t in tuned),
                          "fp32_path": sum(t["precision"] == g.PREC_FP32 for t in tuned),
                          "split16_path": sum(t["precision"] == g.PREC_SPLIT16 for t in tuned)},

@@ -149,6 +149,9 @@ def lib() -> C.CDLL:
         L.gpair_cg_checkpoint_load.argtypes = [vp, vp, C.c_size_t]
         L.gpair_autotune.argtypes = [vp, i, i, C.POINTER(TuneResult)]
         L.gpair_update_pixel.argtypes = [vp, i, i, f, C.POINTER(d), C.POINTER(d)]
+        L.gpair_batch_create.argtypes = [C.POINTER(vp), C.POINTER(vp), i, i]
+        L.gpair_batch_run.argtypes = [vp, C.POINTER(CgParams), C.POINTER(CgResult)]
+        L.gpair_batch_destroy.argtypes = [vp]
         L.gpair_cg_run_many.argtypes = [C.POINTER(vp), i, C.POINTER(CgParams), C.POINTER(CgResult)]
         L.gpair_stop_flag_reset.argtypes = [vp]
         L.gpair_stop_flag_destroy.argtypes = [vp]
@@ -640,3 +643,49 @@ def cg_many(recs, iterations: int, method: int = 2, alpha: Optional[float] = Non
     res = (CgResult * n)()
     _check(L.gpair_cg_run_many(handles, n, C.byref(prm), res))
     return [_result_dict(res[i]) for i in range(n)]
+
+
+class Batch:
+    """Many reconstructions in one CUDA graph launch (gpair_batch_*): every
+    context's whole CG loop is a branch of one graph. Build after the contexts hold
+    their problems, images and configuration."""
+
+    def __init__(self, recs, line_search: int = LS_BATCH):
+        self._L = lib()
+        self.recs = list(recs)
+        self.line_search = line_search
+        h = C.c_void_p()
+        arr = (C.c_void_p * len(self.recs))(*[r.h.value for r in self.recs])
+        _check(self._L.gpair_batch_create(C.byref(h), arr, len(self.recs), line_search), self.recs[0].h)
+        self.h = h
+
+    def run(self, iterations: int, method: int = 2, alpha: Optional[float] = None, resume: bool = False, **kw):
+        prm = CgParams()
+        self._L.gpair_cg_default_params(C.byref(prm))
+        prm.method = method
+        prm.iterations = iterations
+        prm.resume = 1 if resume else 0
+        prm.alpha = self.recs[0].problem.alpha if alpha is None else alpha
+        prm.line_search = self.line_search
+        for k, v in kw.items():
+            setattr(prm, k, v)
+        res = (CgResult * len(self.recs))()
+        _check(self._L.gpair_batch_run(self.h, C.byref(prm), res), self.recs[0].h)
+        return [_result_dict(res[i]) for i in range(len(self.recs))]
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._L.gpair_batch_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -143,35 +143,28 @@ static cudaGraphNode_t add_conditional(gpair_ctx *c, cudaGraph_t parent, cudaGra
     return n;
 }
 
-static int build(gpair_ctx *c, int trace_cap, int ls_mode)
+// Adds one context's whole CG loop (the WHILE node and its bodies) to `parent`.
+// G carries the loop's line-search mode, trace buffer and launch counts.
+static int add_loop(gpair_ctx *c, CgGraph *G, cudaGraph_t parent)
 {
-    graph_free_one(c, ls_mode);
     if (c->precision != GPAIR_PREC_FP32) {
         int rc = gp_tc_prepare(c);  // operand buffers must exist before capture
         if (rc) return rc;
     }
-    if (ls_mode == GPAIR_LS_BATCH) {
+    if (G->ls_mode == GPAIR_LS_BATCH) {
         int rc = gp_batch_alloc(c);
         if (rc) return rc;
     }
-    CgGraph *G = (CgGraph *)calloc(1, sizeof(CgGraph));
-    if (!G) return GPAIR_ERR_ALLOC;
-    c->cg_graph[ls_mode] = G;
-    G->precision = c->precision;
-    G->ls_mode = ls_mode;
-    G->trace_cap = trace_cap;
-    GP_CUDA(c, cudaMalloc(&G->trace, sizeof(double) * 5 * (size_t)trace_cap));
-    GP_CUDA(c, cudaGraphCreate(&G->g, 0));
     int rc = GPAIR_OK;
     cudaGraphConditionalHandle h_iter, h_ls, h_grad;
-    GP_CUDA(c, cudaGraphConditionalHandleCreate(&h_iter, G->g, 1, cudaGraphCondAssignDefault));
+    GP_CUDA(c, cudaGraphConditionalHandleCreate(&h_iter, parent, 1, cudaGraphCondAssignDefault));
     cudaGraph_t B1, B2, B3;
-    add_conditional(c, G->g, h_iter, cudaGraphCondTypeWhile, &B1, &rc);
+    add_conditional(c, parent, h_iter, cudaGraphCondTypeWhile, &B1, &rc);
     if (rc) return rc;
     GP_CUDA(c, cudaGraphConditionalHandleCreate(&h_ls, B1, 0, 0));
     cudaGraphNode_t n_ls = add_conditional(c, B1, h_ls, cudaGraphCondTypeWhile, &B2, &rc);
     if (rc) return rc;
-    const bool wolfe = ls_mode != GPAIR_LS_BATCH;
+    const bool wolfe = G->ls_mode != GPAIR_LS_BATCH;
     cudaGraphNode_t n_if = nullptr;
     h_grad = 0;
     if (wolfe) {
@@ -196,7 +189,6 @@ static int build(gpair_ctx *c, int trace_cap, int ls_mode)
             if (e == cudaSuccess) e = cudaGraphAddDependencies(B2, &n_crit, &n_if, 1);
             if (e == cudaSuccess) e = cudaGraphAddChildGraphNode(&n_grad, B3, nullptr, 0, S[SEQ_GRAD]);
         }
-        if (e == cudaSuccess) e = cudaGraphInstantiate(&G->exec, G->g, 0);
         if (e != cudaSuccess) {
             snprintf(c->last_error, sizeof(c->last_error), "CG graph assembly: %s", cudaGetErrorString(e));
             rc = GPAIR_ERR_CUDA;
@@ -204,8 +196,114 @@ static int build(gpair_ctx *c, int trace_cap, int ls_mode)
     }
     for (int q = 0; q < 4; q++)
         if (S[q]) cudaGraphDestroy(S[q]);
+    return rc;
+}
+
+static int build(gpair_ctx *c, int trace_cap, int ls_mode)
+{
+    graph_free_one(c, ls_mode);
+    CgGraph *G = (CgGraph *)calloc(1, sizeof(CgGraph));
+    if (!G) return GPAIR_ERR_ALLOC;
+    c->cg_graph[ls_mode] = G;
+    G->precision = c->precision;
+    G->ls_mode = ls_mode;
+    G->trace_cap = trace_cap;
+    GP_CUDA(c, cudaMalloc(&G->trace, sizeof(double) * 5 * (size_t)trace_cap));
+    GP_CUDA(c, cudaGraphCreate(&G->g, 0));
+    int rc = add_loop(c, G, G->g);
+    if (!rc) {
+        cudaError_t e = cudaGraphInstantiate(&G->exec, G->g, 0);
+        if (e != cudaSuccess) {
+            snprintf(c->last_error, sizeof(c->last_error), "CG graph instantiate: %s", cudaGetErrorString(e));
+            rc = GPAIR_ERR_CUDA;
+        }
+    }
     if (rc) graph_free_one(c, ls_mode);
     return rc;
+}
+
+// ------------------------------------------------ many contexts, one graph
+//
+// One graph holding every context's whole CG loop as an independent branch
+// (each a WHILE node with its own conditional handles), so that one launch
+// runs all the reconstructions and the device schedules their kernels side
+// by side.
+struct BatchGraph {
+    int n;
+    cudaGraph_t g;
+    cudaGraphExec_t exec;
+    CgGraph *loops;  // per context: mode, trace buffer, launch counts (no graph of its own)
+};
+
+void gp_batch_graph_free(void *bg)
+{
+    BatchGraph *B = (BatchGraph *)bg;
+    if (!B) return;
+    if (B->exec) cudaGraphExecDestroy(B->exec);
+    if (B->g) cudaGraphDestroy(B->g);
+    if (B->loops) {
+        for (int i = 0; i < B->n; i++)
+            if (B->loops[i].trace) cudaFree(B->loops[i].trace);
+        free(B->loops);
+    }
+    free(B);
+}
+
+int gp_batch_graph_build(gpair_ctx **ctx, int n, int ls_mode, void **out)
+{
+    *out = nullptr;
+    BatchGraph *B = (BatchGraph *)calloc(1, sizeof(BatchGraph));
+    if (!B) return GPAIR_ERR_ALLOC;
+    B->n = n;
+    B->loops = (CgGraph *)calloc((size_t)n, sizeof(CgGraph));
+    if (!B->loops || cudaGraphCreate(&B->g, 0) != cudaSuccess) {
+        gp_batch_graph_free(B);
+        return GPAIR_ERR_ALLOC;
+    }
+    int rc = GPAIR_OK;
+    for (int i = 0; i < n && !rc; i++) {
+        CgGraph *G = &B->loops[i];
+        G->precision = ctx[i]->precision;
+        G->ls_mode = ls_mode;
+        G->trace_cap = 1;  // one row; batch runs return no trace
+        if (cudaMalloc(&G->trace, sizeof(double) * 5) != cudaSuccess) {
+            rc = GPAIR_ERR_ALLOC;
+            break;
+        }
+        rc = add_loop(ctx[i], G, B->g);
+    }
+    if (!rc) {
+        cudaError_t e = cudaGraphInstantiate(&B->exec, B->g, 0);
+        if (e != cudaSuccess) {
+            snprintf(ctx[0]->last_error, sizeof(ctx[0]->last_error), "batch graph instantiate: %s",
+                     cudaGetErrorString(e));
+            rc = GPAIR_ERR_CUDA;
+        }
+    }
+    if (rc) {
+        gp_batch_graph_free(B);
+        return rc;
+    }
+    *out = B;
+    return GPAIR_OK;
+}
+
+int gp_batch_graph_launch(void *bg, cudaStream_t stream)
+{
+    BatchGraph *B = (BatchGraph *)bg;
+    return cudaGraphLaunch(B->exec, stream) == cudaSuccess ? GPAIR_OK : GPAIR_ERR_CUDA;
+}
+
+int gp_batch_graph_precision(void *bg, int i) { return ((BatchGraph *)bg)->loops[i].precision; }
+
+long long gp_batch_graph_launches(void *bg, int i, int iterations_done, int criterion_evals, int grad_evals,
+                                  int batches)
+{
+    const CgGraph *G = &((BatchGraph *)bg)->loops[i];
+    long long base = (long long)iterations_done * (G->n_pre + G->n_post);
+    if (G->ls_mode == GPAIR_LS_BATCH) return base + (long long)batches * G->n_crit;
+    return base + (long long)(criterion_evals - iterations_done) * G->n_crit +
+           (long long)(grad_evals - iterations_done) * G->n_grad;
 }
 
 // Launch `iterations` CG iterations as one graph. Returns the kernel launches

@@ -21,6 +21,12 @@ int gp_cg_graph_run(gpair_ctx *c, int iterations, int want_trace, int ls_mode, l
 int gp_cg_graph_trace(gpair_ctx *c, int iterations, double *tJ, double *tchi2, double *tS, double *tstep,
                       double *tbeta);
 long long gp_cg_graph_launches(gpair_ctx *c, int iterations_done, int criterion_evals, int grad_evals, int batches);
+int gp_batch_graph_build(gpair_ctx **ctx, int n, int ls_mode, void **out);
+void gp_batch_graph_free(void *bg);
+int gp_batch_graph_launch(void *bg, cudaStream_t stream);
+int gp_batch_graph_precision(void *bg, int i);
+long long gp_batch_graph_launches(void *bg, int i, int iterations_done, int criterion_evals, int grad_evals,
+                                  int batches);
 
 static const char *k_err_names[] = {"GPAIR_OK",      "GPAIR_ERR_INVALID", "GPAIR_ERR_ALLOC",     "GPAIR_ERR_CUDA",
                                     "GPAIR_ERR_STATE", "GPAIR_ERR_TIMEOUT", "GPAIR_ERR_NO_DEVICE", "GPAIR_ERR_NUMERIC"};
@@ -652,7 +658,7 @@ static int cg_validate(gpair_ctx *c, const gpair_cg_params *p)
     return GPAIR_OK;
 }
 
-static int cg_prepare(gpair_ctx *c, const gpair_cg_params *p, int want_trace, CgRun *r)
+static int cg_prepare(gpair_ctx *c, const gpair_cg_params *p, int want_trace, CgRun *r, int build_graph = 1)
 {
     int rc = cg_validate(c, p);
     if (rc) return rc;
@@ -688,7 +694,7 @@ static int cg_prepare(gpair_ctx *c, const gpair_cg_params *p, int want_trace, Cg
     c->st_n = 0;
     r->want_trace = want_trace;
     r->launches0 = c->launches;
-    if (!p->host_loop) {
+    if (!p->host_loop && build_graph) {
         // build (or reuse) the graph before the timed region
         long long dummy = 0;
         if ((rc = gp_cg_graph_run(c, 0, want_trace, p->line_search, &dummy))) return rc;
@@ -762,7 +768,8 @@ static int cg_host_loop(gpair_ctx *c, const gpair_cg_params *p, double *tJ, doub
 static void cg_mark_end(gpair_ctx *c, CgRun *r) { cudaEventRecord(r->e1, c->stream); }
 
 static int cg_finish(gpair_ctx *c, const gpair_cg_params *p, gpair_cg_result *res, double *tJ, double *tchi2,
-                     double *tS, double *tstep, double *tbeta, CgRun *r, int status, int it)
+                     double *tS, double *tstep, double *tbeta, CgRun *r, int status, int it,
+                     void *batch_graph = nullptr, int batch_index = 0)
 {
     cudaError_t e = cudaEventSynchronize(r->e1);
     float ms = 0.f;
@@ -779,9 +786,13 @@ static int cg_finish(gpair_ctx *c, const gpair_cg_params *p, gpair_cg_result *re
     const CgState &s = c->sc_host->cg;
     if (!p->host_loop) {
         it = s.run_it;
-        if (r->want_trace && !status) status = gp_cg_graph_trace(c, it, tJ, tchi2, tS, tstep, tbeta);
+        if (r->want_trace && !status && !batch_graph) status = gp_cg_graph_trace(c, it, tJ, tchi2, tS, tstep, tbeta);
         if (!status && c->sc_host->nonfinite) status = GPAIR_ERR_NUMERIC;
-        c->launches = r->launches0 + gp_cg_graph_launches(c, it, s.criterion_evals, s.grad_evals, s.batches);
+        c->launches = r->launches0 + (batch_graph ? gp_batch_graph_launches(batch_graph, batch_index, it,
+                                                                            s.criterion_evals, s.grad_evals,
+                                                                            s.batches)
+                                                  : gp_cg_graph_launches(c, it, s.criterion_evals, s.grad_evals,
+                                                                         s.batches));
     }
     c->last_ms = ms;
     double per = 4.0 * (double)c->npix * c->nuv + 8.0 * c->N * (double)c->nuv;
@@ -818,6 +829,124 @@ extern "C" int gpair_cg_run(gpair_ctx *c, const gpair_cg_params *p, gpair_cg_res
     }
     cg_mark_end(c, &r);
     return cg_finish(c, p, res, tJ, tchi2, tS, tstep, tbeta, &r, status, it);
+}
+
+// ------------------------------------------------------- batched contexts
+
+struct gpair_batch {
+    int n, ls_mode, device;
+    gpair_ctx **ctx;
+    void *graph;
+    cudaStream_t stream;
+    cudaEvent_t *ready;
+    cudaEvent_t done, e0, e1;
+};
+
+extern "C" int gpair_batch_destroy(gpair_batch *b)
+{
+    if (!b) return GPAIR_OK;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    gp_batch_graph_free(b->graph);
+    if (b->ready)
+        for (int i = 0; i < b->n; i++)
+            if (b->ready[i]) cudaEventDestroy(b->ready[i]);
+    if (b->done) cudaEventDestroy(b->done);
+    if (b->e0) cudaEventDestroy(b->e0);
+    if (b->e1) cudaEventDestroy(b->e1);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    free(b->ready);
+    free(b->ctx);
+    free(b);
+    return GPAIR_OK;
+}
+
+extern "C" int gpair_batch_create(gpair_batch **out, gpair_ctx **ctx, int n, int line_search)
+{
+    if (!out || !ctx || n <= 0) return GPAIR_ERR_INVALID;
+    if (line_search != GPAIR_LS_WOLFE && line_search != GPAIR_LS_BATCH) return GPAIR_ERR_INVALID;
+    *out = nullptr;
+    for (int i = 0; i < n; i++) {
+        if (!ctx[i] || !ctx[i]->have_problem || !ctx[i]->have_image) return GPAIR_ERR_STATE;
+        if (ctx[i]->device != ctx[0]->device) return GPAIR_ERR_INVALID;
+        for (int j = 0; j < i; j++)
+            if (ctx[i] == ctx[j]) return GPAIR_ERR_INVALID;
+    }
+    gpair_batch *b = (gpair_batch *)calloc(1, sizeof(gpair_batch));
+    if (!b) return GPAIR_ERR_ALLOC;
+    b->n = n;
+    b->ls_mode = line_search;
+    b->device = ctx[0]->device;
+    b->ctx = (gpair_ctx **)calloc((size_t)n, sizeof(gpair_ctx *));
+    b->ready = (cudaEvent_t *)calloc((size_t)n, sizeof(cudaEvent_t));
+    if (!b->ctx || !b->ready) {
+        gpair_batch_destroy(b);
+        return GPAIR_ERR_ALLOC;
+    }
+    memcpy(b->ctx, ctx, sizeof(gpair_ctx *) * n);
+    int rc = GPAIR_OK;
+    if (cudaSetDevice(b->device) != cudaSuccess || cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) ||
+        cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming) || cudaEventCreate(&b->e0) ||
+        cudaEventCreate(&b->e1))
+        rc = GPAIR_ERR_CUDA;
+    for (int i = 0; i < n && !rc; i++)
+        if (cudaEventCreateWithFlags(&b->ready[i], cudaEventDisableTiming) != cudaSuccess) rc = GPAIR_ERR_CUDA;
+    for (int i = 0; i < n && !rc; i++) {
+        ctx[i]->fuse_ctrl = -1;
+        ctx[i]->fuse_handles = 0;
+    }
+    if (!rc) rc = gp_batch_graph_build(ctx, n, line_search, &b->graph);
+    if (rc) {
+        gpair_batch_destroy(b);
+        return rc;
+    }
+    *out = b;
+    return GPAIR_OK;
+}
+
+extern "C" int gpair_batch_run(gpair_batch *b, const gpair_cg_params *p, gpair_cg_result *res)
+{
+    if (!b || !p) return GPAIR_ERR_INVALID;
+    if (p->host_loop || p->line_search != b->ls_mode) return GPAIR_ERR_INVALID;
+    for (int i = 0; i < b->n; i++) {
+        int rc = cg_validate(b->ctx[i], p);
+        if (rc) return rc;
+        // the batch graph was captured with each context's precision path
+        if (gp_batch_graph_precision(b->graph, i) != b->ctx[i]->precision) return GPAIR_ERR_STATE;
+    }
+    std::vector<CgRun> r((size_t)b->n);
+    GP_CUDA(b->ctx[0], cudaSetDevice(b->device));
+    int prepared = 0, rc = GPAIR_OK;
+    for (; prepared < b->n; prepared++) {
+        gpair_ctx *c = b->ctx[prepared];
+        if ((rc = cg_prepare(c, p, 0, &r[prepared], 0))) break;
+        cudaEventRecord(b->ready[prepared], c->stream);
+        cudaStreamWaitEvent(b->stream, b->ready[prepared], 0);
+    }
+    float ms = 0.f;
+    if (!rc) {
+        cudaEventRecord(b->e0, b->stream);
+        rc = gp_batch_graph_launch(b->graph, b->stream);
+        cudaEventRecord(b->e1, b->stream);
+        cudaEventRecord(b->done, b->stream);
+        if (!rc && cudaEventSynchronize(b->e1) == cudaSuccess) cudaEventElapsedTime(&ms, b->e0, b->e1);
+    }
+    int first_err = rc;
+    for (int i = 0; i < prepared; i++) {
+        gpair_ctx *c = b->ctx[i];
+        if (rc) {
+            cudaEventDestroy(r[i].e0);
+            cudaEventDestroy(r[i].e1);
+            continue;
+        }
+        cudaStreamWaitEvent(c->stream, b->done, 0);
+        cg_mark_end(c, &r[i]);
+        int rci = cg_finish(c, p, res ? &res[i] : nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, &r[i],
+                            GPAIR_OK, 0, b->graph, i);
+        c->last_ms = ms;
+        if (rci && !first_err) first_err = rci;
+    }
+    return first_err;
 }
 
 extern "C" int gpair_cg_run_many(gpair_ctx **ctx, int n, const gpair_cg_params *p, gpair_cg_result *res)

@@ -336,6 +336,19 @@ size_t gpair_cg_checkpoint_size(gpair_ctx *ctx);
 int gpair_cg_checkpoint_save(gpair_ctx *ctx, void *buffer, size_t bytes);
 int gpair_cg_checkpoint_load(gpair_ctx *ctx, const void *buffer, size_t bytes);
 
+/* Batched reconstructions: one CUDA graph holds the whole CG loop of every context
+ * (each an independent branch with its own conditional nodes), so one graph launch
+ * runs all n reconstructions and the device schedules their kernels side by side.
+ * Create after every context holds its problem, image, precision and (optional)
+ * autotuned configuration; those are fixed into the graph: rebuild the batch after
+ * changing any of them. gpair_batch_run takes the same parameters as gpair_cg_run
+ * (line_search must match the batch's, host_loop must be 0; no traces) and returns
+ * per-context results; each context's last_run_stats holds the batch's device time. */
+typedef struct gpair_batch gpair_batch;
+int gpair_batch_create(gpair_batch **batch, gpair_ctx **ctx, int n, int line_search);
+int gpair_batch_run(gpair_batch *batch, const gpair_cg_params *p, gpair_cg_result *results);
+int gpair_batch_destroy(gpair_batch *batch);
+
 /* Stop flag for racing runs: a device int, zeroed at creation and by reset. */
 int gpair_stop_flag_create(int **flag);
 int gpair_stop_flag_reset(int *flag);

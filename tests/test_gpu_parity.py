@@ -612,3 +612,35 @@ def test_alternating_line_searches_reuse_their_graphs(rec):
     assert np.array_equal(outs[0]["trace_J"], outs[2]["trace_J"])
     assert np.array_equal(outs[1]["trace_J"], outs[3]["trace_J"])
     assert outs[1]["criterion_evals"] % g.LS_TRIALS == 3 % g.LS_TRIALS
+
+
+@pytest.mark.parametrize("ls", [0, 1])
+def test_batch_graph_equals_separate_runs(ls):
+    """gpair_batch_*: every context's CG loop in one graph, one launch; the results
+    are the separate runs' bit for bit, twice in a row (the graph is reused)."""
+    from gpair_b200.instances import instance
+    ps = [instance(20_000_000 + k) for k in range(4)]
+    recs = [g.Reconstructor(0) for _ in ps]
+    try:
+        for r, p in zip(recs, ps):
+            r.set_problem(p)
+            r.set_precision(g.PREC_SPLIT16)
+        singles, imgs = [], []
+        for r, p in zip(recs, ps):
+            r.set_image(p.start_image())
+            singles.append(r.cg(5, method=2, line_search=ls))
+            imgs.append(r.get_image())
+        for r, p in zip(recs, ps):
+            r.set_image(p.start_image())
+        with g.api.Batch(recs, line_search=ls) as b:
+            for rep in range(2):
+                for r, p in zip(recs, ps):
+                    r.set_image(p.start_image())
+                out = b.run(5)
+                for r, a, o, img in zip(recs, singles, out, imgs):
+                    assert o["status"] == 0 and o["iterations"] == 5
+                    assert o["J"] == a["J"] and o["criterion_evals"] == a["criterion_evals"]
+                    assert np.array_equal(r.get_image(), img)
+    finally:
+        for r in recs:
+            r.close()
