@@ -961,11 +961,16 @@ __global__ void __launch_bounds__(GP_THREADS) k_vis_chi2_batch(const float2 *__r
     block_sum<1>(chi, smem);
     if (threadIdx.x == 0) partials[(size_t)j * gridDim.x + blockIdx.x] = chi[0];
     if (last_block_of(&sc->t_counter[GP_NTR], gridDim.x * gridDim.y)) {
-        for (int jj = 0; jj < (int)gridDim.y; jj++) {
-            double out[1];
-            finish_sum<1>(partials + (size_t)jj * gridDim.x, gridDim.x, out, smem);
-            if (threadIdx.x == 0) sc->t_chi2[jj] = out[0];
+        // one warp per trial, all trials at once; fixed lane order and shuffle tree
+        const int lane = threadIdx.x & 31;
+        for (int jj = threadIdx.x >> 5; jj < (int)gridDim.y; jj += blockDim.x >> 5) {
+            const double *pp = partials + (size_t)jj * gridDim.x;
+            double v = 0.0;
+            for (int b = lane; b < (int)gridDim.x; b += 32) v += __ldcg(&pp[b]);
+            for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+            if (lane == 0) sc->t_chi2[jj] = v;
         }
+        __syncthreads();
         if (threadIdx.x == 0) {
             sc->t_counter[GP_NTR] = 0;
             run_fused_ctrl(sc, fc);

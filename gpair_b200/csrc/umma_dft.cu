@@ -410,16 +410,15 @@ __global__ void __launch_bounds__(GP_THREADS) k_tc_prep_split_trial(
     const float scale = ldexpf(1.f, 15 - ex);
     double acc[2] = {0.0, 0.0};
     double mx = 0.0;
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p < npix) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
         double t = (double)img[p] + s * (double)d[p];
         if (t < minval) t = minval;
         const float I = (float)t;
         dst[p] = I;
         const double Id = I, m = model[p];
-        acc[0] = Id;
-        acc[1] = reg_term(Id, m, sc->reg_kind);
-        mx = fabs(Id);
+        acc[0] += Id;
+        acc[1] += reg_term(Id, m, sc->reg_kind);
+        mx = fmax(mx, fabs(Id));
         const int y = p / N, x = p - y * N;
         const float v = I * scale;
         const __half h = __float2half_rn(v);
@@ -532,6 +531,101 @@ __global__ void __launch_bounds__(256) k_tc_build_w(const float2 *__restrict__ c
         __half2 lv = __halves2half2(__float2half_rn(w.x - __half2float(h0)), __float2half_rn(w.y - __half2float(h1)));
         *reinterpret_cast<__half2 *>(&w_hi[(size_t)y * K2_pad + 2 * k]) = hv;
         *reinterpret_cast<__half2 *>(&w_lo[(size_t)y * K2_pad + 2 * k]) = lv;
+    }
+}
+
+// The same W from the uv coordinates, without the transpose. A thread owns four
+// consecutive uv points (columns 8g .. 8g+7: one 16-byte store per row into
+// each of W hi and W lo, 512 contiguous bytes per warp) and BW_ROWS image rows.
+// Fy[k][y] = e^{-2 pi i t_k y}, t_k = pix v_k in turns, is evaluated as
+// A_k(y0) R_k(y - y0): the anchor A_k at every BW_SEG-th row and the
+// rotations R_k(j) = e^{-2 pi i j t_k}, j < BW_SEG (a shared table: the eight
+// warps of a block share their 128 uv points) both come from an FP64 phase
+// reduced to [-1/2, 1/2] and FP32 sincospif, so every element is one complex
+// product of two correctly rounded factors and no rounding error accumulates
+// along y. Columns of uv points >= nuv (up to K2_pad) are written as zeros;
+// rows >= N are not touched.
+#define BW_SEG 8
+#define BW_ROWS 16
+__global__ void __launch_bounds__(256) k_tc_build_w_uv(const float2 *__restrict__ cw,
+                                                        const float2 *__restrict__ uvc, float pix, int nuv, int N,
+                                                        int K2_pad, __half *__restrict__ w_hi,
+                                                        __half *__restrict__ w_lo, DevScalars *__restrict__ sc)
+{
+    __shared__ __align__(16) float2 rp[BW_SEG][128];
+    const double cmax = sc->cmax;
+    int ex = 0;
+    float wscale = 1.f;
+    if (cmax > 0.0) {
+        frexp(cmax * 1.4143, &ex);
+        wscale = ldexpf(1.f, 15 - ex);
+    }
+    if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0)
+        sc->gscale = 1.0 / ((double)wscale * (double)(1 << TC_TW_LOG2));
+    const int kbase = blockIdx.x * 128;
+    for (int e = threadIdx.x; e < BW_SEG * 128; e += blockDim.x) {
+        const int j = e >> 7, k = kbase + (e & 127);
+        float2 r = make_float2(1.f, 0.f);
+        if (j > 0 && k < nuv) {
+            double t = RPMAS_TC * (double)pix * (double)uvc[k].y * (double)j;
+            t -= rint(t);
+            float sn, cn;
+            sincospif((float)(2.0 * t), &sn, &cn);
+            r = make_float2(cn, -sn);
+        }
+        rp[j][e & 127] = r;
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int g = blockIdx.x * 32 + lane;
+    const int y0 = (blockIdx.y * 8 + (threadIdx.x >> 5)) * BW_ROWS;
+    if (8 * g >= K2_pad || y0 >= N) return;
+    float2 cs[4], an[4];
+    double tv[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const int k = 4 * g + i;
+        cs[i] = make_float2(0.f, 0.f);
+        tv[i] = 0.0;
+        if (k < nuv) {
+            const float2 c = cw[k];
+            cs[i] = make_float2(c.x * wscale, c.y * wscale);
+            tv[i] = RPMAS_TC * (double)pix * (double)uvc[k].y;
+        }
+    }
+    const int y1 = min(N, y0 + BW_ROWS);
+    uint4 *ph = reinterpret_cast<uint4 *>(w_hi + (size_t)y0 * K2_pad + 8 * g);
+    uint4 *pl = reinterpret_cast<uint4 *>(w_lo + (size_t)y0 * K2_pad + 8 * g);
+    const size_t step = (size_t)K2_pad / 8;  // uint4 per row
+    for (int y = y0; y < y1; y++) {
+        const int j = (y - y0) & (BW_SEG - 1);
+        if (j == 0) {
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                double t = tv[i] * (double)y;
+                t -= rint(t);
+                float sn, cn;
+                sincospif((float)(2.0 * t), &sn, &cn);
+                an[i] = make_float2(cn, -sn);
+            }
+        }
+        const float4 r01 = *reinterpret_cast<const float4 *>(&rp[j][4 * lane]);
+        const float4 r23 = *reinterpret_cast<const float4 *>(&rp[j][4 * lane + 2]);
+        const float2 r[4] = {make_float2(r01.x, r01.y), make_float2(r01.z, r01.w), make_float2(r23.x, r23.y),
+                             make_float2(r23.z, r23.w)};
+        __half2 hv[4], lv[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const float2 f = make_float2(an[i].x * r[i].x - an[i].y * r[i].y, an[i].x * r[i].y + an[i].y * r[i].x);
+            const float2 w = make_float2(cs[i].x * f.x - cs[i].y * f.y, -(cs[i].x * f.y + cs[i].y * f.x));
+            hv[i] = __float22half2_rn(w);
+            const float2 hb = __half22float2(hv[i]);
+            lv[i] = __float22half2_rn(make_float2(w.x - hb.x, w.y - hb.y));
+        }
+        *ph = *reinterpret_cast<const uint4 *>(hv);
+        *pl = *reinterpret_cast<const uint4 *>(lv);
+        ph += step;
+        pl += step;
     }
 }
 
@@ -833,7 +927,9 @@ int gp_tc_prep_split_trial(gpair_ctx *c)
     int rc;
     TcState *t = tc_state_ready(c, &rc);
     if (rc) return rc;
+    // at most GP_MAX_PARTIALS blocks: 3 partials each fit the RED_PREP slot
     int g = gp_cdiv(c->npix, GP_THREADS);
+    if (g > GP_MAX_PARTIALS) g = GP_MAX_PARTIALS;
     k_tc_prep_split_trial<<<g, GP_THREADS, 0, c->stream>>>(c->image, c->descent_dir, c->image_temp, c->model, c->N,
                                                            c->npix, t->Kx_pad, t->img_hi, t->img_lo,
                                                            c->partials, c->sc);
@@ -847,9 +943,16 @@ int gp_tc_build_w(gpair_ctx *c)
     int rc;
     TcState *t = tc_state_ready(c, &rc);
     if (rc) return rc;
-    dim3 g(gp_cdiv(c->nuv ? c->nuv : 1, 32), gp_cdiv(c->N, 32));
-    k_tc_build_w<<<g, 256, 0, c->stream>>>(c->cw, c->have_uv ? c->uvc : nullptr, c->fy, c->pix, c->nuv, c->N,
-                                           t->K2_pad, t->w_hi, t->w_lo, c->sc);
+    if (c->have_uv) {
+        // 32 groups of 4 uv points x 8 warps of BW_ROWS rows per block
+        dim3 g(gp_cdiv(t->K2_pad / 8, 32), gp_cdiv(c->N, 8 * BW_ROWS));
+        k_tc_build_w_uv<<<g, 256, 0, c->stream>>>(c->cw, c->uvc, c->pix, c->nuv, c->N, t->K2_pad, t->w_hi,
+                                                   t->w_lo, c->sc);
+    } else {
+        dim3 g(gp_cdiv(c->nuv ? c->nuv : 1, 32), gp_cdiv(c->N, 32));
+        k_tc_build_w<<<g, 256, 0, c->stream>>>(c->cw, nullptr, c->fy, c->pix, c->nuv, c->N, t->K2_pad, t->w_hi,
+                                               t->w_lo, c->sc);
+    }
     GP_LAUNCH_CHECK(c);
     return GPAIR_OK;
 }
