@@ -45,6 +45,7 @@ enum { CG_PH_BRACKET = 0, CG_PH_ZOOM = 1 };
 // batched line search (GPAIR_LS_BATCH)
 #define GP_NTR GPAIR_LS_TRIALS  // trial images per batched evaluation
 #define GP_LS_RATIO 4.0         // step ratio of the geometric grid
+#define GP_LS_RATIO_LOG2 2      // log2 of GP_LS_RATIO: grid steps are exact power-of-two multiples
 #define GP_LS_MAX_ROUNDS 6      // grid shifts + refine per iteration
 #define GP_LS_MAX_PTS (GP_LS_MAX_ROUNDS * GP_NTR)
 enum { BR_GRID = 0, BR_REFINE = 1 };
@@ -189,6 +190,7 @@ struct gpair_ctx {
     float *image_trials;
     float2 *vpart_b;
     double *partials_b;
+    int batch_wave[2];  // blocks per trial that fill one wave: [0] trial prep, [1] trial chi2
     int epp;  // forward partial entries per trial image
 
     // graph-captured CG (cg_graph.cu): one graph per line-search mode, so that

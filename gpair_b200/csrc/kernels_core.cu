@@ -978,11 +978,24 @@ __global__ void __launch_bounds__(GP_THREADS) k_vis_chi2_batch(const float2 *__r
     }
 }
 
+// Blocks per trial: at most one wave of resident blocks over the whole batch
+// (a partial second wave would leave most SMs idle while it runs), at most 256
+// (the per-trial partial-sum area), at least one.
 static int batch_blocks_per_trial(gpair_ctx *c)
 {
     int g = gp_cdiv(c->npix, GP_THREADS * 2);
+    if (g > c->batch_wave[0]) g = c->batch_wave[0];
     if (g > 256) g = 256;
     return g < 1 ? 1 : g;
+}
+
+static int batch_wave_blocks(const void *kernel, int nsm)
+{
+    int per_sm = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, GP_THREADS, 0) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    const int w = per_sm * nsm / GP_NTR;
+    return w < 1 ? 1 : w;
 }
 
 int gp_batch_alloc(gpair_ctx *c)
@@ -998,6 +1011,10 @@ int gp_batch_alloc(gpair_ctx *c)
     GP_CUDA(c, cudaMalloc(&c->image_trials, sizeof(float) * (size_t)GP_NTR * c->npix));
     GP_CUDA(c, cudaMalloc(&c->vpart_b, sizeof(float2) * (size_t)GP_NTR * epp_max * (c->nuv ? c->nuv : 1)));
     GP_CUDA(c, cudaMalloc(&c->partials_b, sizeof(double) * (size_t)GP_NTR * 1024 * 2));
+    int nsm = 148;
+    GP_CUDA(c, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
+    c->batch_wave[0] = batch_wave_blocks((const void *)k_trials_prep, nsm);
+    c->batch_wave[1] = batch_wave_blocks((const void *)k_vis_chi2_batch, nsm);
     return GPAIR_OK;
 }
 
@@ -1052,6 +1069,7 @@ static int eval_batch(gpair_ctx *c, cudaEvent_t *ev)
     if (ev) cudaEventRecord(ev[2], c->stream);
     gp_stage_begin(c, 2);
     int nb = gp_cdiv(c->npow + c->nbis, GP_THREADS * 2);
+    if (nb > c->batch_wave[1]) nb = c->batch_wave[1];  // one wave over the batch
     if (nb > 1024) nb = 1024;
     if (nb < 1) nb = 1;
     dim3 g(nb, GP_NTR);
@@ -1154,7 +1172,7 @@ __device__ void cg_zoom_enter(CgState &s, double lo, double hi, double J_lo)
 __device__ void ls_batch_grid(CgState &s)
 {
     for (int j = 0; j < GP_NTR; j++) {
-        double t = s.s_c * pow(GP_LS_RATIO, (double)(j - 3));
+        double t = ldexp(s.s_c, GP_LS_RATIO_LOG2 * (j - 3));  // s_c 4^(j-3), exact
         s.ts[j] = t < s.batch_step_max ? t : s.batch_step_max;
     }
     s.action = CG_EVAL_BATCH;
@@ -1201,7 +1219,7 @@ __device__ void ls_batch_after(DevScalars *__restrict__ sc, CgState &s)
         double smin = s.pts_s[0];
         for (int i = 1; i < s.npts; i++) smin = fmin(smin, s.pts_s[i]);
         if (s.bround < GP_LS_MAX_ROUNDS && smin > 1e-300) {
-            s.s_c = smin / pow(GP_LS_RATIO, 5.0);
+            s.s_c = ldexp(smin, -5 * GP_LS_RATIO_LOG2);  // smin / 4^5
             ls_batch_grid(s);
         } else {
             s.force_sd = 1;  // restart from steepest descent next iteration
@@ -1218,7 +1236,7 @@ __device__ void ls_batch_after(DevScalars *__restrict__ sc, CgState &s)
     if (!(hi < INFINITY)) {
         // the largest step tried is the best: extend the grid upwards
         if (s.bround < GP_LS_MAX_ROUNDS - 1 && sb < s.batch_step_max) {
-            s.s_c = sb * pow(GP_LS_RATIO, 4.0);
+            s.s_c = ldexp(sb, 4 * GP_LS_RATIO_LOG2);  // sb 4^4
             ls_batch_grid(s);
         } else {
             ls_batch_accept(s, sb, Jb);
@@ -1234,9 +1252,9 @@ __device__ void ls_batch_after(DevScalars *__restrict__ sc, CgState &s)
     ls_batch_accept(s, sb, Jb);
 }
 
-__device__ void cg_control(DevScalars *__restrict__ sc, int what)
+// One step of the state machine on a working copy of the CG state.
+__device__ __noinline__ static void cg_step(DevScalars *__restrict__ sc, CgState &s, int what)
 {
-    CgState &s = sc->cg;
     switch (what) {
     case CTRL_RESUME:
         // a continued run counts its own evaluations; the iteration state is kept
@@ -1426,6 +1444,18 @@ __device__ void cg_control(DevScalars *__restrict__ sc, int what)
     default:
         break;
     }
+}
+
+// The controller runs in one thread at the end of a reduction kernel, on the
+// critical path of every evaluation. It works on a copy of the CG state (read
+// once, held in registers and L1-cached local memory, written back once)
+// instead of on the device-global state, whose loads would each wait on L2
+// behind the controller's own stores.
+__device__ void cg_control(DevScalars *__restrict__ sc, int what)
+{
+    CgState s = sc->cg;
+    cg_step(sc, s, what);
+    sc->cg = s;
 }
 
 __global__ void k_cg_ctrl(DevScalars *__restrict__ sc, int what)

@@ -83,6 +83,22 @@ def test_device_cg_matches_fp64_cg(rec, prec):
     assert abs(out["trace_J"][-1] - tr["J"][-1]) / abs(tr["J"][-1]) < 1e-3
 
 
+def test_device_cg_above_one_megapixel(rec):
+    """1100^2 pixels (more than 4096 blocks x 256 threads): the trial-image prep
+    and the reductions run several pixels per thread on grids capped at their
+    partial-sum slots. Few uv points keep the FP64 oracle at seconds."""
+    w, oi = synth.make_workload_data("tiny", 21, 22, 23)
+    p = g.problem_from_oifits(oi, 1100, w.pixellation_mas * w.image_width / 1100, w.alpha)
+    rec.set_problem(p)
+    rec.set_precision(g.PREC_SPLIT16)
+    img0 = p.start_image()
+    _, tr = O.reconstruct64(p, img0, 2)
+    rec.set_image(img0)
+    out = rec.cg(2, method=2, trace=True)
+    assert np.allclose(out["trace_J"][:2], tr["J"][:2], rtol=1e-5)
+    assert np.allclose(out["trace_step"][:2], tr["step"][:2], rtol=1e-4)
+
+
 def test_cg_methods_run_and_descend(rec):
     p = _problem("tiny", (5, 6, 7))
     rec.set_problem(p)
