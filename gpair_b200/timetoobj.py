@@ -142,6 +142,12 @@ def summarize(rows: List[Dict]) -> Dict:
         if has_plain:
             out["speedup_warm_vs_plain"] = out["plain_s"] / max(out["warm_s"], 1e-12)
             out["median_ratio_warm_vs_plain"] = float(np.median([r["plain_s"] / r["warm_s"] for r in rows]))
+    # per problem: width, then iterations to the target (negative: not reached
+    # within the limit) of plain CG, the batched search and the warm start
+    cols = [k for k in ("plain", "batch", "warm") if f"{k}_iters" in (rows[0] if rows else {})]
+    out["per_problem_iters"] = {"columns": ["width"] + cols,
+                                "rows": [[int(r["width"])] + [int(r[f"{k}_iters"]) * (1 if r[f"{k}_reached"] else -1)
+                                                              for k in cols] for r in rows]}
     return out
 
 

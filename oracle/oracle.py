@@ -207,6 +207,8 @@ def reconstruct64(p, image, iterations, method=2, threads: int = 8, line_search:
                   batch_step_max: float = 1e12):
     """FP64 CG from `image`; returns (image, trace dict). line_search 0: the
     reference's GPU-path control flow; 1: the batched 8-trial search."""
+    if line_search not in (0, 1):
+        raise ValueError(f"line_search must be 0 (reference) or 1 (batched), got {line_search}")
     L = fp64()
     L.o_set_threads(threads)
     img = np.ascontiguousarray(image, np.float64).copy()
