@@ -248,7 +248,7 @@ def many_instances(n: int, iters: int) -> dict:
             "unit": "s (host wall clock)", "line_search": "batched"}
 
 
-def time_to_objective(n_problems: int) -> dict:
+def time_to_objective(n_problems: int, race_fr: bool = False) -> dict:
     """CG time-to-objective on held-out problems of the warm-start workload (3/4
     at 64x64, 1/4 at 128x128): wall time until J <= J* (1 + 1e-4), J* = plain
     CG's converged objective (reference line search, 1000 iterations), for plain
@@ -262,11 +262,12 @@ def time_to_objective(n_problems: int) -> dict:
     n64 = max(1, (3 * n_problems) // 4)
     rows = []
     flag = g.api.StopFlag()
-    with g.Reconstructor(0) as rec, g.Reconstructor(0) as rec2:
+    with g.Reconstructor(0) as rec, g.Reconstructor(0) as rec2, g.Reconstructor(0) as rec3:
         rec.set_precision(g.PREC_SPLIT16)
         for k in range(n_problems):
             p = training_case(SEED_HELD_OUT + k, 64 if k < n64 else 128).problem
-            rows.append(TT.evaluate(rec, p, net, iters=1000, objective_from="plain", rec2=rec2, flag=flag))
+            rows.append(TT.evaluate(rec, p, net, iters=1000, objective_from="plain", rec2=rec2, flag=flag,
+                                    rec3=rec3 if race_fr else None))
     flag.close()
     out = TT.summarize(rows)
     out["unit"] = "s (sum of host wall clock over the problems)"
@@ -467,7 +468,7 @@ def run_ours(args, rank, world, local):
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(args.workload)
         if not args.no_time_to_objective:
-            line["time_to_objective"] = time_to_objective(args.tto_problems)
+            line["time_to_objective"] = time_to_objective(args.tto_problems, race_fr=args.tto_race_fr)
         if args.instances > 0:
             line["many_instances"] = many_instances(args.instances, args.instance_iters)
         print(json.dumps(line), flush=True)
@@ -493,6 +494,8 @@ def main():
                     help="line search of the headline steps: the reference's (default) or the batched one")
     ap.add_argument("--tto-problems", type=int, default=16,
                     help="held-out warm-start problems timed for the time-to-objective block")
+    ap.add_argument("--tto-race-fr", action="store_true",
+                    help="add a flat-start Fletcher-Reeves runner to the time-to-objective race")
     ap.add_argument("--host-loop", action="store_true",
                     help="drive the line search from the host instead of the CUDA graph (for profilers that do "
                          "not see kernels inside conditional graph nodes)")

@@ -40,33 +40,48 @@ def _timed_cg(rec, start, iters, line_search, target):
 
 
 def race(rec: api.Reconstructor, rec2: api.Reconstructor, p: api.Problem, net, iters: int, target: float,
-         flag: api.StopFlag) -> Dict:
-    """Warm start in `rec` against the flat prior in `rec2` (both hold problem p)."""
+         flag: api.StopFlag, rec3: Optional[api.Reconstructor] = None) -> Dict:
+    """Warm start in `rec` against the flat prior in `rec2` (both hold problem p).
+    With `rec3` (also holding p), a third runner starts from the flat prior with
+    the Fletcher-Reeves beta: on ill-conditioned problems the beta rule moves
+    the iterations to the target by large factors either way, so each problem
+    takes whichever runner arrives first."""
     import gpair_b200 as g
     from .warmstart import features, warm_start
     flag.reset()
     res: Dict = {}
 
-    def flat():
-        rec2.set_image(p.start_image())
-        res["flat"] = rec2.cg(iters, method=2, line_search=g.LS_BATCH, target_J=target, stop_flag=flag.ptr)
+    def flat(r, key, method):
+        r.set_image(p.start_image())
+        res[key] = r.cg(iters, method=method, line_search=g.LS_BATCH, target_J=target, stop_flag=flag.ptr)
 
     t0 = time.perf_counter()
-    th = threading.Thread(target=flat)
-    th.start()
+    threads = [threading.Thread(target=flat, args=(rec2, "flat", 2))]
+    if rec3 is not None:
+        threads.append(threading.Thread(target=flat, args=(rec3, "flat_fr", 1)))
+    for th in threads:
+        th.start()
     img = warm_start(net, rec, p, features(rec, p))
     rec.set_image(img)
     warm = rec.cg(iters, method=2, line_search=g.LS_BATCH, target_J=target, stop_flag=flag.ptr)
-    th.join()
+    for th in threads:
+        th.join()
     dt = time.perf_counter() - t0
-    winner = "warm" if warm["reached"] else ("flat" if res["flat"]["reached"] else "none")
-    return {"race_s": dt, "race_winner": winner, "race_warm_iters": warm["iterations"],
-            "race_flat_iters": res["flat"]["iterations"]}
+    winner = "warm" if warm["reached"] else "none"
+    for key in ("flat", "flat_fr"):
+        if winner == "none" and key in res and res[key]["reached"]:
+            winner = key
+    out = {"race_s": dt, "race_winner": winner, "race_warm_iters": warm["iterations"],
+           "race_flat_iters": res["flat"]["iterations"]}
+    if "flat_fr" in res:
+        out["race_flat_fr_iters"] = res["flat_fr"]["iterations"]
+    return out
 
 
 def evaluate(rec: api.Reconstructor, p: api.Problem, net=None, iters: int = 1000, tol: float = 1e-4,
              batch_iters: Optional[int] = None, objective_from: str = "plain",
-             rec2: Optional[api.Reconstructor] = None, flag: Optional[api.StopFlag] = None) -> Dict:
+             rec2: Optional[api.Reconstructor] = None, flag: Optional[api.StopFlag] = None,
+             rec3: Optional[api.Reconstructor] = None) -> Dict:
     """objective_from "plain": J* from the reference line search (the headline
     comparison); "batch": J* from the batched line search run for batch_iters
     iterations from the flat prior (isolates what the network adds)."""
@@ -109,7 +124,12 @@ def evaluate(rec: api.Reconstructor, p: api.Problem, net=None, iters: int = 1000
             rec2.set_precision(rec_precision(rec))
             rec2.set_image(start)
             rec2.cg(1, method=2, line_search=g.LS_BATCH)  # graph capture outside the timed race
-            res.update(race(rec, rec2, p, net, bi, target, flag))
+            if rec3 is not None:
+                rec3.set_problem(p)
+                rec3.set_precision(rec_precision(rec))
+                rec3.set_image(start)
+                rec3.cg(1, method=1, line_search=g.LS_BATCH)
+            res.update(race(rec, rec2, p, net, bi, target, flag, rec3))
     return res
 
 
@@ -135,7 +155,8 @@ def summarize(rows: List[Dict]) -> Dict:
         out["speedup_warm_vs_batch"] = out["batch_s"] / max(out["warm_s"], 1e-12)
         if "race_s" in rows[0]:
             out["race_s"] = tot("race_s")
-            out["race_winners"] = {w: int(sum(r["race_winner"] == w for r in rows)) for w in ("warm", "flat", "none")}
+            out["race_winners"] = {w: int(sum(r["race_winner"] == w for r in rows))
+                                   for w in ("warm", "flat", "flat_fr", "none")}
             out["speedup_race_vs_batch"] = out["batch_s"] / max(out["race_s"], 1e-12)
             if has_plain:
                 out["speedup_race_vs_plain"] = out["plain_s"] / max(out["race_s"], 1e-12)

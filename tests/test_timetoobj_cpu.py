@@ -21,7 +21,7 @@ def test_summary_sums_ratios_and_rows():
     assert s["speedup_batch_vs_plain"] == pytest.approx(4.0 / 1.2)
     assert s["speedup_warm_vs_plain"] == pytest.approx(4.0 / 0.6)
     assert s["batch_reached"] == 1 and s["fallbacks"] == 1
-    assert s["race_winners"] == {"warm": 1, "flat": 1, "none": 0}
+    assert s["race_winners"] == {"warm": 1, "flat": 1, "flat_fr": 0, "none": 0}
     assert s["median_ratio_warm_vs_plain"] == pytest.approx((10.0 + 6.0) / 2)
     pp = s["per_problem_iters"]
     assert pp["columns"] == ["width", "plain", "batch", "warm"]
