@@ -27,3 +27,58 @@ def test_summary_sums_ratios_and_rows():
     assert pp["columns"] == ["width", "plain", "batch", "warm"]
     # a run that missed the target is reported with a negative iteration count
     assert pp["rows"] == [[64, 100, 30, 5], [128, 1000, -1000, 40]]
+
+
+class _FakeRec:
+    """Stands in for a Reconstructor: cg() returns a fixed outcome and records its arguments."""
+
+    def __init__(self, reached, iters):
+        self.reached, self.iters, self.calls = reached, iters, []
+
+    def set_image(self, img):
+        pass
+
+    def cg(self, iters, **kw):
+        self.calls.append(kw)
+        return {"reached": self.reached, "iterations": self.iters}
+
+
+class _FakeProblem:
+    def start_image(self):
+        return None
+
+
+class _FakeFlag:
+    ptr = 0
+
+    def reset(self):
+        pass
+
+
+@pytest.mark.parametrize("outcomes, expect", [
+    ((True, False, False), "warm"),
+    ((False, True, False), "flat"),
+    ((False, False, True), "flat_fr"),
+    ((False, False, False), "none"),
+])
+def test_race_winner_and_runner_settings(monkeypatch, outcomes, expect):
+    import gpair_b200.warmstart as W
+    monkeypatch.setattr(W, "features", lambda rec, p: None)
+    monkeypatch.setattr(W, "warm_start", lambda net, rec, p, f: None)
+    warm, flat, fr = (_FakeRec(r, 10 + i) for i, r in enumerate(outcomes))
+    out = T.race(warm, flat, _FakeProblem(), None, 100, 1.0, _FakeFlag(), rec3=fr)
+    assert out["race_winner"] == expect
+    assert (out["race_warm_iters"], out["race_flat_iters"], out["race_flat_fr_iters"]) == (10, 11, 12)
+    # every runner uses the batched search, the shared stop flag and the same target;
+    # the third runner alone uses the Fletcher-Reeves beta
+    for rec, method in ((warm, 2), (flat, 2), (fr, 1)):
+        (kw,) = rec.calls
+        assert kw["method"] == method and kw["target_J"] == 1.0 and kw["stop_flag"] == 0
+
+
+def test_race_without_third_runner(monkeypatch):
+    import gpair_b200.warmstart as W
+    monkeypatch.setattr(W, "features", lambda rec, p: None)
+    monkeypatch.setattr(W, "warm_start", lambda net, rec, p, f: None)
+    out = T.race(_FakeRec(False, 7), _FakeRec(True, 5), _FakeProblem(), None, 100, 1.0, _FakeFlag())
+    assert out["race_winner"] == "flat" and "race_flat_fr_iters" not in out
