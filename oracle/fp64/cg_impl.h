@@ -33,7 +33,7 @@ typedef struct {
 } CG(evaluator);
 
 typedef struct {
-    int method;        /* 0 SD, 1 FR, 2 PR+, 3 HS+ */
+    int method;        /* 0 SD, 1 FR, 2 PR+, 3 HS+; batched search only: 4 projected L-BFGS */
     int iterations;
     REAL minvalue;     /* 1e-8 */
     REAL wolfe1;       /* c1 = 1e-4 */
@@ -181,6 +181,71 @@ static REAL CG(batch_search)(const CG(evaluator) *ev, const CG(params) *p, int n
     }
 }
 
+/*
+ * Projected limited-memory BFGS direction (batched search, method 4; no
+ * counterpart in the reference or the library yet). Pixels on the positivity
+ * bound whose gradient points outward are held fixed: the gradient is zeroed
+ * there before the two-loop recursion (Nocedal & Wright, Algorithm 7.4) and
+ * the direction after it. The pairs s = x_new - x_old (the step actually
+ * taken, after the clamp) and y = g_new - g_old are kept when s.y > 1e-12 |s| |y|;
+ * H0 = (s.y / y.y) I from the newest pair.
+ */
+#define LBFGS_PAIRS 8
+
+typedef struct {
+    REAL *s, *y, *x_old;   /* LBFGS_PAIRS * n each for s and y; n for x_old */
+    double rho[LBFGS_PAIRS], gamma;
+    int head, count;       /* pairs stored: count <= LBFGS_PAIRS, newest at (head - 1) */
+} CG(lbfgs);
+
+static int CG(lbfgs_init)(CG(lbfgs) *L, int n)
+{
+    memset(L, 0, sizeof(*L));
+    L->gamma = 1.0;
+    L->s = calloc((size_t)LBFGS_PAIRS * n, sizeof(REAL));
+    L->y = calloc((size_t)LBFGS_PAIRS * n, sizeof(REAL));
+    L->x_old = calloc((size_t)n, sizeof(REAL));
+    return (L->s && L->y && L->x_old) ? 0 : -1;
+}
+
+static void CG(lbfgs_free)(CG(lbfgs) *L) { free(L->s); free(L->y); free(L->x_old); }
+
+/* new pair from the last step (x_old -> image, g_old -> g_new) */
+static void CG(lbfgs_update)(CG(lbfgs) *L, int n, const REAL *image, const REAL *g_new, const REAL *g_old)
+{
+    REAL *sk = L->s + (size_t)(L->head % LBFGS_PAIRS) * n, *yk = L->y + (size_t)(L->head % LBFGS_PAIRS) * n;
+    for (int i = 0; i < n; i++) { sk[i] = image[i] - L->x_old[i]; yk[i] = g_new[i] - g_old[i]; }
+    const double sy = CG(dot)(n, sk, yk), yy = CG(dot)(n, yk, yk), ss = CG(dot)(n, sk, sk);
+    if (yy > 0 && sy > 1e-12 * sqrt(ss * yy)) {
+        L->rho[L->head % LBFGS_PAIRS] = 1.0 / sy;
+        L->gamma = sy / yy;
+        L->head++;
+        if (L->count < LBFGS_PAIRS) L->count++;
+    }
+}
+
+static void CG(lbfgs_dir)(const CG(lbfgs) *L, int n, const REAL *image, const REAL *g, REAL minvalue, REAL *d)
+{
+    double al[LBFGS_PAIRS];
+    const REAL bound = minvalue * (REAL)1.000001;
+    for (int i = 0; i < n; i++) d[i] = (image[i] <= bound && g[i] > 0) ? 0 : g[i];
+    for (int j = 0; j < L->count; j++) {
+        const int slot = (L->head - 1 - j) % LBFGS_PAIRS;
+        const REAL *sk = L->s + (size_t)slot * n, *yk = L->y + (size_t)slot * n;
+        al[j] = L->rho[slot] * CG(dot)(n, sk, d);
+        for (int i = 0; i < n; i++) d[i] -= (REAL)al[j] * yk[i];
+    }
+    if (L->count)
+        for (int i = 0; i < n; i++) d[i] *= (REAL)L->gamma;
+    for (int j = L->count - 1; j >= 0; j--) {
+        const int slot = (L->head - 1 - j) % LBFGS_PAIRS;
+        const REAL *sk = L->s + (size_t)slot * n, *yk = L->y + (size_t)slot * n;
+        const double b = L->rho[slot] * CG(dot)(n, yk, d);
+        for (int i = 0; i < n; i++) d[i] += (REAL)(al[j] - b) * sk[i];
+    }
+    for (int i = 0; i < n; i++) d[i] = (image[i] <= bound && g[i] > 0) ? 0 : -d[i];
+}
+
 static int CG(run_batch)(const CG(evaluator) *ev, const CG(params) *p, int n, REAL *image, CG(trace) *tr,
                          double step_cap)
 {
@@ -190,13 +255,16 @@ static int CG(run_batch)(const CG(evaluator) *ev, const CG(params) *p, int n, RE
     REAL beta = 0, chi2, S;
     double s_c = 1.0;
     int force_sd = 0;
+    const int lbfgs = p->method == 4;
+    CG(lbfgs) L;
+    if (lbfgs && CG(lbfgs_init)(&L, n)) return -1;
     tr->criterion_evals = tr->grad_evals = 0;
     for (int it = 0; it < p->iterations; it++) {
         REAL J = ev->criterion(ev->ctx, image, &chi2, &S);
         tr->criterion_evals++;
         ev->gradient(ev->ctx, image, g_new);
         tr->grad_evals++;
-        if (it == 0 || p->method == 0) {
+        if (it == 0 || p->method == 0 || lbfgs) {
             beta = 0.;
         } else {
             REAL nn = CG(dot)(n, g_new, g_new), no = CG(dot)(n, g_new, g_old), oo = CG(dot)(n, g_old, g_old);
@@ -208,16 +276,24 @@ static int CG(run_batch)(const CG(evaluator) *ev, const CG(params) *p, int n, RE
             }
             if (fabs(no / nn) > .5) beta = 0.;
         }
-        if (force_sd) { beta = 0.; force_sd = 0; }
+        if (lbfgs) {
+            if (it > 0) CG(lbfgs_update)(&L, n, image, g_new, g_old);
+            if (force_sd) { L.count = 0; force_sd = 0; }  /* a failed search drops the history */
+            CG(lbfgs_dir)(&L, n, image, g_new, p->minvalue, d);
+        } else {
+            if (force_sd) { beta = 0.; force_sd = 0; }
+            for (int i = 0; i < n; i++) d[i] = beta * d[i] - g_new[i];
+        }
         if (tr->J) { tr->J[it] = J; tr->chi2[it] = chi2; tr->entropy[it] = S; tr->beta[it] = beta; }
-        for (int i = 0; i < n; i++) d[i] = beta * d[i] - g_new[i];
         REAL w1 = CG(dot)(n, d, g_new), sel = 0;
         if (!(w1 < 0)) force_sd = 1;
         else sel = CG(batch_search)(ev, p, n, image, d, J, &s_c, step_cap, &force_sd, temp, tr);
         if (tr->step) tr->step[it] = sel;
+        if (lbfgs) memcpy(L.x_old, image, sizeof(REAL) * n);
         CG(trial)(n, image, d, sel, p->minvalue, image);
         memcpy(g_old, g_new, sizeof(REAL) * n);
     }
+    if (lbfgs) CG(lbfgs_free)(&L);
     free(g_new); free(g_old); free(d); free(temp);
     return 0;
 }

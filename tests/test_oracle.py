@@ -230,6 +230,27 @@ def test_batched_line_search_oracle_descends_and_counts():
     assert np.all(tr["step"] > 0)
 
 
+def test_projected_lbfgs_oracle_direction():
+    """Method 4 of the batched search (projected L-BFGS, a candidate for the
+    device path): its first iteration is PR+'s (both start from -g with the same
+    search), J never increases, the image stays on or above the positivity
+    bound, and it exists only with the batched search."""
+    import gpair_b200 as g
+    p = g.workload_problem("tiny", 21, 22, 23)
+    iters = 30
+    img_pr, tr_pr = O.reconstruct64(p, p.start_image(), iters, method=2, line_search=1)
+    img_lb, tr_lb = O.reconstruct64(p, p.start_image(), iters, method=4, line_search=1)
+    assert tr_lb["J"][0] == tr_pr["J"][0] and tr_lb["J"][1] == tr_pr["J"][1]
+    assert tr_lb["step"][0] == tr_pr["step"][0]
+    assert np.all(np.diff(tr_lb["J"]) <= 0) and tr_lb["J"][-1] < tr_lb["J"][0]
+    assert tr_lb["grad_evals"] == iters and (tr_lb["criterion_evals"] - iters) % 8 == 0
+    assert img_lb.min() >= 1e-8 * (1 - 1e-12)
+    # a different direction from the second iteration on
+    assert tr_lb["J"][-1] != tr_pr["J"][-1]
+    with pytest.raises(ValueError):
+        O.reconstruct64(p, p.start_image(), 2, method=4, line_search=0)
+
+
 def test_l2_regularizer_restatement_matches_reference():
     rng = np.random.default_rng(4)
     N = 24
