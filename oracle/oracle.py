@@ -60,6 +60,7 @@ def fp64() -> C.CDLL:
         L.o32_ref_cg_run.argtypes = [vp, i, i, i, vp, f, i, i, vp, vp, vp, vp, vp, C.POINTER(i), C.POINTER(i), vp, vp,
                                      vp, vp, vp]
         L.o_set_threads.argtypes = [i]
+        L.o64_lbfgs_direction.argtypes = [i, i, vp, vp, d, vp, vp, d, vp]
         _fp64 = L
     return _fp64
 
@@ -354,3 +355,51 @@ def ref_l2(width, image, model):
     img = np.ascontiguousarray(image, np.float32)
     m = np.ascontiguousarray(model, np.float32)
     return float(L.L2_entropy(width, _p(img), _p(m))), float(L.L2_entropy_gradient(width, _p(img), _p(m)))
+
+
+# ------------------------------------------------ projected L-BFGS direction
+
+def _lbfgs_fixed(image, g, minvalue):
+    """Pixels held fixed: on the positivity bound with the gradient pointing outward."""
+    return (np.asarray(image, np.float64) <= minvalue * 1.000001) & (np.asarray(g, np.float64) > 0)
+
+
+def lbfgs_direction64(S, Y, gamma, image, g, minvalue=1e-8):
+    """The batched search's projected L-BFGS direction (method 4), by the C
+    oracle's two-loop recursion. S, Y: [count][n] pairs, oldest first."""
+    L = fp64()
+    S = np.ascontiguousarray(S, np.float64)
+    Y = np.ascontiguousarray(Y, np.float64)
+    img = np.ascontiguousarray(image, np.float64)
+    gr = np.ascontiguousarray(g, np.float64)
+    count, n = S.shape
+    d = np.zeros(n, np.float64)
+    L.o64_lbfgs_direction(n, count, _p(S), _p(Y), float(gamma), _p(img), _p(gr), float(minvalue), _p(d))
+    return d
+
+
+def lbfgs_direction_compact(S, Y, gamma, image, g, minvalue=1e-8):
+    """The same direction from the compact representation of the inverse BFGS
+    matrix (Byrd, Nocedal and Schnabel, 1994):
+        H q = gamma q + S^T t + gamma Y^T b,
+        b = -R^-1 u,  t = R^-T ((D + gamma Y Y^T) R^-1 u - v),
+    u = S q, v = gamma Y q, R = upper triangle of S Y^T, D its diagonal. It
+    needs the 2m dots S q, Y q (one pass over q), the m x m products S Y^T and
+    Y Y^T (kept as pairs arrive) and one combination pass: the formulation
+    for a device path, where the two-loop recursion would need 2m dependent
+    grid-wide reductions."""
+    S = np.asarray(S, np.float64)
+    Y = np.asarray(Y, np.float64)
+    fixed = _lbfgs_fixed(image, g, minvalue)
+    q = np.where(fixed, 0.0, np.asarray(g, np.float64))
+    if S.shape[0] == 0:
+        return np.where(fixed, 0.0, -q)
+    SY = S @ Y.T
+    R = np.triu(SY)
+    D = np.diag(np.diag(SY))
+    u = S @ q
+    v = gamma * (Y @ q)
+    Ru = np.linalg.solve(R, u)
+    t = np.linalg.solve(R.T, (D + gamma * (Y @ Y.T)) @ Ru - v)
+    Hq = gamma * q + S.T @ t - gamma * (Y.T @ Ru)
+    return np.where(fixed, 0.0, -Hq)

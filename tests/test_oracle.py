@@ -251,6 +251,45 @@ def test_projected_lbfgs_oracle_direction():
         O.reconstruct64(p, p.start_image(), 2, method=4, line_search=0)
 
 
+def _lbfgs_pairs(n, m, seed):
+    """Pairs with positive curvature from a random SPD quadratic (y = A s)."""
+    rng = np.random.default_rng(seed)
+    B = rng.standard_normal((n, n)) / np.sqrt(n)
+    A = B @ B.T + np.diag(rng.uniform(0.5, 2.0, n))
+    S = rng.standard_normal((m, n))
+    Y = S @ A.T
+    return S, Y
+
+
+@pytest.mark.parametrize("m", [0, 1, 3, 8])
+def test_lbfgs_compact_form_equals_two_loop(m):
+    """The compact form (the formulation for a device path) gives the two-loop
+    recursion's direction, with pixels on the bound held fixed."""
+    n = 300
+    S, Y = _lbfgs_pairs(n, m, seed=m)
+    rng = np.random.default_rng(100 + m)
+    image = rng.uniform(0.1, 2.0, n)
+    image[rng.choice(n, 40, replace=False)] = 1e-8
+    g = rng.standard_normal(n)
+    gamma = float(S[-1] @ Y[-1] / (Y[-1] @ Y[-1])) if m else 1.0
+    d2 = O.lbfgs_direction64(S, Y, gamma, image, g)
+    dc = O.lbfgs_direction_compact(S, Y, gamma, image, g)
+    assert np.linalg.norm(dc - d2) <= 1e-10 * np.linalg.norm(d2)
+    fixed = (image <= 1e-8 * 1.000001) & (g > 0)
+    assert np.all(d2[fixed] == 0) and fixed.any()
+    assert d2 @ g < 0  # a descent direction
+
+
+def test_lbfgs_direction_satisfies_newest_secant_equation():
+    """With no pixel on the bound, -d(g = y_newest) = H y_newest = s_newest."""
+    n, m = 200, 5
+    S, Y = _lbfgs_pairs(n, m, seed=7)
+    image = np.ones(n)
+    gamma = float(S[-1] @ Y[-1] / (Y[-1] @ Y[-1]))
+    d = O.lbfgs_direction64(S, Y, gamma, image, Y[-1])
+    assert np.allclose(-d, S[-1], rtol=0, atol=1e-9 * np.abs(S[-1]).max())
+
+
 def test_l2_regularizer_restatement_matches_reference():
     rng = np.random.default_rng(4)
     N = 24
