@@ -190,7 +190,7 @@ static REAL CG(batch_search)(const CG(evaluator) *ev, const CG(params) *p, int n
  * taken, after the clamp) and y = g_new - g_old are kept when s.y > 1e-12 |s| |y|;
  * H0 = (s.y / y.y) I from the newest pair.
  */
-#define LBFGS_PAIRS 8
+#define LBFGS_PAIRS 4
 
 typedef struct {
     REAL *s, *y, *x_old;   /* LBFGS_PAIRS * n each for s and y; n for x_old */

@@ -277,21 +277,23 @@ void o64_data_gradient(int N, int npow, int nbis, const double *image, const flo
 
 /* The projected L-BFGS direction of the batched search (two-loop recursion)
  * for caller-given pairs: S and Y hold `count` pairs of n values, oldest
- * first; rho[j] = 1 / (s_j . y_j); gamma scales the initial matrix. Lets the
- * tests check other formulations of the same direction against this one. */
+ * first, of which the newest LBFGS_PAIRS are used, as in the search; gamma
+ * scales the initial matrix. Lets the tests check other formulations of the
+ * same direction against this one. */
 void o64_lbfgs_direction(int n, int count, const double *S, const double *Y, double gamma, const double *image,
                          const double *g, double minvalue, double *d)
 {
     o64_lbfgs L;
     memset(&L, 0, sizeof(L));
-    L.s = (double *)S;
-    L.y = (double *)Y;
+    const int use = count < LBFGS_PAIRS ? count : LBFGS_PAIRS;
+    L.s = (double *)S + (size_t)(count - use) * n;
+    L.y = (double *)Y + (size_t)(count - use) * n;
     L.gamma = gamma;
-    L.count = count < LBFGS_PAIRS ? count : LBFGS_PAIRS;
-    L.head = L.count;  /* newest pair in slot count - 1 */
-    for (int j = 0; j < L.count; j++) {
+    L.count = use;
+    L.head = use;  /* newest pair in slot use - 1 */
+    for (int j = 0; j < use; j++) {
         double sy = 0;
-        for (int i = 0; i < n; i++) sy += S[(size_t)j * n + i] * Y[(size_t)j * n + i];
+        for (int i = 0; i < n; i++) sy += L.s[(size_t)j * n + i] * L.y[(size_t)j * n + i];
         L.rho[j] = 1.0 / sy;
     }
     o64_lbfgs_dir(&L, n, image, g, minvalue, d);

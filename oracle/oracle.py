@@ -209,7 +209,7 @@ def reconstruct64(p, image, iterations, method=2, threads: int = 8, line_search:
     """FP64 CG from `image`; returns (image, trace dict). line_search 0: the
     reference's GPU-path control flow; 1: the batched 8-trial search. method:
     0 SD, 1 FR, 2 PR+, 3 HS+ (the reference's beta rules); 4 projected L-BFGS
-    with 8 pairs, batched search only (a candidate direction for the device
+    with 4 pairs, batched search only (a candidate direction for the device
     path, not in the library yet)."""
     if line_search not in (0, 1):
         raise ValueError(f"line_search must be 0 (reference) or 1 (batched), got {line_search}")
@@ -366,7 +366,8 @@ def _lbfgs_fixed(image, g, minvalue):
 
 def lbfgs_direction64(S, Y, gamma, image, g, minvalue=1e-8):
     """The batched search's projected L-BFGS direction (method 4), by the C
-    oracle's two-loop recursion. S, Y: [count][n] pairs, oldest first."""
+    oracle's two-loop recursion. S, Y: [count][n] pairs, oldest first; the
+    newest LBFGS_PAIRS (4) of them are used, as in the search."""
     L = fp64()
     S = np.ascontiguousarray(S, np.float64)
     Y = np.ascontiguousarray(Y, np.float64)
@@ -385,7 +386,8 @@ def lbfgs_direction_compact(S, Y, gamma, image, g, minvalue=1e-8):
         b = -R^-1 u,  t = R^-T ((D + gamma Y Y^T) R^-1 u - v),
     u = S q, v = gamma Y q, R = upper triangle of S Y^T, D its diagonal. It
     needs the 2m dots S q, Y q (one pass over q), the m x m products S Y^T and
-    Y Y^T (kept as pairs arrive) and one combination pass: the formulation
+    Y Y^T (kept as pairs arrive) and one combination pass. All pairs given are
+    used (pass the newest LBFGS_PAIRS to match the search): the formulation
     for a device path, where the two-loop recursion would need 2m dependent
     grid-wide reductions."""
     S = np.asarray(S, np.float64)
