@@ -286,8 +286,16 @@ static int CG(run_batch)(const CG(evaluator) *ev, const CG(params) *p, int n, RE
         }
         if (tr->J) { tr->J[it] = J; tr->chi2[it] = chi2; tr->entropy[it] = S; tr->beta[it] = beta; }
         REAL w1 = CG(dot)(n, d, g_new), sel = 0;
-        if (!(w1 < 0)) force_sd = 1;
-        else sel = CG(batch_search)(ev, p, n, image, d, J, &s_c, step_cap, &force_sd, temp, tr);
+        if (!(w1 < 0)) {
+            force_sd = 1;
+        } else {
+            /* A quasi-Newton direction carries its own scale: centre the grid on
+             * step 1. Centred on the last CG-scale step instead, the trial images
+             * of a float evaluation round back to the current image, show no
+             * decrease, and the search moves the grid further down and fails. */
+            if (lbfgs && L.count > 0) s_c = 1.0;
+            sel = CG(batch_search)(ev, p, n, image, d, J, &s_c, step_cap, &force_sd, temp, tr);
+        }
         if (tr->step) tr->step[it] = sel;
         if (lbfgs) memcpy(L.x_old, image, sizeof(REAL) * n);
         CG(trial)(n, image, d, sel, p->minvalue, image);
