@@ -33,7 +33,7 @@ typedef struct {
 } CG(evaluator);
 
 typedef struct {
-    int method;        /* 0 SD, 1 FR, 2 PR+, 3 HS+; batched search only: 4 projected L-BFGS */
+    int method;        /* 0 SD, 1 FR, 2 PR+, 3 HS+; 4 projected L-BFGS (no reference counterpart) */
     int iterations;
     REAL minvalue;     /* 1e-8 */
     REAL wolfe1;       /* c1 = 1e-4 */
@@ -312,6 +312,8 @@ static int CG(run)(const CG(evaluator) *ev, const CG(params) *p, int n, REAL *im
     REAL *g_new = calloc(n, sizeof(REAL)), *g_old = calloc(n, sizeof(REAL));
     REAL *d = calloc(n, sizeof(REAL)), *temp = calloc(n, sizeof(REAL)), *tgrad = calloc(n, sizeof(REAL));
     if (!g_new || !g_old || !d || !temp || !tgrad) return -1;
+    CG(lbfgs) L;
+    if (p->method == 4 && CG(lbfgs_init)(&L, n)) return -1;
     REAL beta = 0, sel = 0, chi2, S;
     tr->criterion_evals = tr->grad_evals = 0;
     for (int it = 0; it < p->iterations; it++) {
@@ -332,7 +334,19 @@ static int CG(run)(const CG(evaluator) *ev, const CG(params) *p, int n, REAL *im
             if (fabs(no / nn) > .5) beta = 0.;
         }
         if (tr->J) { tr->J[it] = J; tr->chi2[it] = chi2; tr->entropy[it] = S; tr->beta[it] = beta; }
-        for (int i = 0; i < n; i++) d[i] = beta * d[i] - g_new[i];
+        if (p->method == 4) {
+            /* projected L-BFGS with the reference's search; a direction that is
+             * not a descent direction falls back to the projected -g */
+            if (it > 0) CG(lbfgs_update)(&L, n, image, g_new, g_old);
+            CG(lbfgs_dir)(&L, n, image, g_new, p->minvalue, d);
+            if (!(CG(dot)(n, d, g_new) < 0)) {
+                L.count = 0;
+                CG(lbfgs_dir)(&L, n, image, g_new, p->minvalue, d);
+            }
+            memcpy(L.x_old, image, sizeof(REAL) * n);
+        } else {
+            for (int i = 0; i < n; i++) d[i] = beta * d[i] - g_new[i];
+        }
         REAL wolfe_product1 = CG(dot)(n, d, g_new);
         REAL s = 1., s_old = 0., J_init = J, J_old = J, Jt;
         int ls_it = 1;
@@ -363,6 +377,7 @@ static int CG(run)(const CG(evaluator) *ev, const CG(params) *p, int n, REAL *im
         CG(trial)(n, image, d, sel, p->minvalue, image);
         memcpy(g_old, g_new, sizeof(REAL) * n);
     }
+    if (p->method == 4) CG(lbfgs_free)(&L);
     free(g_new); free(g_old); free(d); free(temp); free(tgrad);
     return 0;
 }

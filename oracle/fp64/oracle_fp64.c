@@ -353,7 +353,9 @@ int o64_reconstruct(int N, int nuv, int npow, int nbis, const float *uv, float p
     p.egrad = calloc((size_t)N * N, sizeof(double));
     p.dgrad = calloc((size_t)N * N, sizeof(double));
     o64_evaluator ev = {&p, o64_eval_criterion, o64_eval_gradient};
-    o64_params prm = {method, iterations, 1e-8, 1e-4, 0.1, 100., 200};
+    /* c2 = 0.1 is the reference's; projected L-BFGS (method 4, no reference
+     * counterpart) uses the usual quasi-Newton curvature constant 0.9 */
+    o64_params prm = {method, iterations, 1e-8, 1e-4, method == 4 ? 0.9 : 0.1, 100., 200};
     o64_trace tr = {0, 0, J, chi2, entropy, step, beta};
     int rc = line_search == 1 ? o64_run_batch(&ev, &prm, N * N, image, &tr, batch_step_max)
                               : o64_run(&ev, &prm, N * N, image, &tr);

@@ -209,12 +209,13 @@ def reconstruct64(p, image, iterations, method=2, threads: int = 8, line_search:
     """FP64 CG from `image`; returns (image, trace dict). line_search 0: the
     reference's GPU-path control flow; 1: the batched 8-trial search. method:
     0 SD, 1 FR, 2 PR+, 3 HS+ (the reference's beta rules); 4 projected L-BFGS
-    with 4 pairs, batched search only (a candidate direction for the device
-    path, not in the library yet)."""
+    with 4 pairs, with either search (with the reference's search it uses the
+    curvature constant c2 = 0.9 instead of 0.1; a candidate direction for the
+    device path, not in the library yet)."""
     if line_search not in (0, 1):
         raise ValueError(f"line_search must be 0 (reference) or 1 (batched), got {line_search}")
-    if method not in (0, 1, 2, 3, 4) or (method == 4 and line_search != 1):
-        raise ValueError(f"method {method} with line_search {line_search} is not available")
+    if method not in (0, 1, 2, 3, 4):
+        raise ValueError(f"method must be 0-4, got {method}")
     L = fp64()
     L.o_set_threads(threads)
     img = np.ascontiguousarray(image, np.float64).copy()

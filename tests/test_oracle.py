@@ -231,10 +231,10 @@ def test_batched_line_search_oracle_descends_and_counts():
 
 
 def test_projected_lbfgs_oracle_direction():
-    """Method 4 of the batched search (projected L-BFGS, a candidate for the
-    device path): its first iteration is PR+'s (both start from -g with the same
-    search), J never increases, the image stays on or above the positivity
-    bound, and it exists only with the batched search."""
+    """Method 4 (projected L-BFGS, a candidate for the device path): with the
+    batched search its first iteration is PR+'s (both start from -g with the
+    same search); with either search J never increases and the image stays on
+    or above the positivity bound."""
     import gpair_b200 as g
     p = g.workload_problem("tiny", 21, 22, 23)
     iters = 30
@@ -247,8 +247,12 @@ def test_projected_lbfgs_oracle_direction():
     assert img_lb.min() >= 1e-8 * (1 - 1e-12)
     # a different direction from the second iteration on
     assert tr_lb["J"][-1] != tr_pr["J"][-1]
+    # with the reference's search (curvature constant 0.9): Armijo steps, so J never increases
+    img_w, tr_w = O.reconstruct64(p, p.start_image(), iters, method=4, line_search=0)
+    assert np.all(np.diff(tr_w["J"]) <= 0) and tr_w["J"][-1] < tr_w["J"][0]
+    assert img_w.min() >= 1e-8 * (1 - 1e-12) and tr_w["grad_evals"] >= iters
     with pytest.raises(ValueError):
-        O.reconstruct64(p, p.start_image(), 2, method=4, line_search=0)
+        O.reconstruct64(p, p.start_image(), 2, method=5, line_search=1)
 
 
 def _lbfgs_pairs(n, m, seed):
