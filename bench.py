@@ -1,10 +1,14 @@
 #!/usr/bin/env python
 """Benchmark of the GPAIR reconstruction hot path on B200.
 
-Workload (default): the 256x256 "precision" reconstruction -- 0.05 mas/pixel,
-12 telescopes in a 400 m disk, 40 hour angles x 8 channels: 21,120 V2 points,
-70,400 closure triangles (nuv = 21,141 after the reference's uv matcher),
-seeded synthetic data (the reference publishes no data set of this size).
+Workload (default, `--workload large`): the 1024x1024 polychromatic
+reconstruction -- 0.02 mas/pixel, a limb-darkened 15 mas disk with 50 Gaussian
+spots (+-30 % contrast), 20 telescopes in a 400 m disk (190 baselines), 64 hour
+angles x 16 channels: 194,560 V2 points and 1,167,360 closure triangles
+(nuv = 195,021 after the reference's uv matcher), seeded synthetic data (the
+reference publishes no data set of this size). It is the largest
+configuration that fits one GPU (2.5 GB of HBM). The 256x256 "precision"
+workload (21,120 V2, 70,400 T3) is reported beside it under `precision_256`.
 
 A step is one plain PR+ nonlinear-CG iteration with the reference's strong
 Wolfe line search (criterion + gradient of the current image, direction
@@ -19,12 +23,18 @@ HBM, L2 flushed by a 512 MiB write before every step, outside the timed
 region); `e2e` times the same steps through the public C ABI with host
 buffers: image upload, one CG iteration, image read-back. With N > 1 each rank
 runs its own independent reconstruction (replicas, weak scaling); the time is
-the max over ranks. `--impl reference` times the reference's own compiled
-cpu.c (oracle/_ref) on a bounded sample of the same workload on all host cores.
+the max over ranks.
+
+`--impl reference` times the reference's own CPU code path on the host cores:
+its cpu.c criterion + gradient (compiled unchanged from the reference's
+sources into oracle/_ref) on a bounded sample of the same workload, whose uv
+and triangle indices come from the reference's own getoifits.c. That process
+never imports the gpair_b200 package and maps none of its libraries.
 """
 from __future__ import annotations
 
 import argparse
+import importlib.util
 import json
 import os
 import statistics
@@ -32,6 +42,7 @@ import subprocess
 import sys
 import threading
 import time
+import types
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
@@ -125,44 +136,217 @@ def _traffic(kernel_key):
     return None
 
 
-def cpu_sample_problem(p, width=32):
-    """Bounded CPU sample of the workload: the same data and uv coverage on a width x width image."""
-    import gpair_b200 as g
-    model = g.set_model(width, p.pixellation, 0, 0.0, 1.0)
-    return g.Problem(width, p.pixellation, p.uv, p.npow, p.nbis, p.data, p.data_err, p.phasor, p.uvpnt, p.sign,
-                     model, p.alpha)
+# ------------------------------------------------ the reference's CPU path
+
+def data_modules():
+    """The seeded data generator (gpair_b200/synth.py) and its OIFITS tables
+    (gpair_b200/oifits.py), loaded as plain modules under a private package
+    name: the gpair_b200 package, its ctypes layer and libgpair_b200.so are
+    not touched (the reference arm must run none of this project's code on
+    its measured path)."""
+    name = "_gpair_data_only"
+    if name in sys.modules:
+        pkg = sys.modules[name]
+        return pkg.synth, pkg.oifits
+    pkg = types.ModuleType(name)
+    pkg.__path__ = [os.path.join(ROOT, "gpair_b200")]
+    sys.modules[name] = pkg
+    for mod in ("oifits", "synth"):
+        spec = importlib.util.spec_from_file_location(f"{name}.{mod}", os.path.join(ROOT, "gpair_b200", f"{mod}.py"))
+        m = importlib.util.module_from_spec(spec)
+        sys.modules[f"{name}.{mod}"] = m
+        spec.loader.exec_module(m)
+        setattr(pkg, mod, m)
+    return pkg.synth, pkg.oifits
 
 
-_SAMPLE_CACHE = {}
+def subset_channels(oi, chans, oifits_mod):
+    """The same OIFITS tables restricted to the spectral channels `chans`."""
+    import numpy as np
+    ch = np.asarray(chans)
+    M = oifits_mod
+    wv = [M.WavelengthTable(x.insname, x.eff_wave[ch], x.eff_band[ch]) for x in oi.wavelengths]
+    v2 = [M.Vis2Table(t.insname, t.target_id, t.ucoord, t.vcoord, t.vis2data[:, ch], t.vis2err[:, ch],
+                      t.flag[:, ch]) for t in oi.vis2]
+    t3 = [M.T3Table(t.insname, t.target_id, t.u1coord, t.v1coord, t.u2coord, t.v2coord, t.t3amp[:, ch],
+                    t.t3amperr[:, ch], t.t3phi[:, ch], t.t3phierr[:, ch], t.flag[:, ch]) for t in oi.t3]
+    return M.OIFits(wv, v2, t3, oi.target_id)
 
 
-def _ref_eval_worker(args):
-    """Criterion + gradient evaluations of the sample with the reference's own cpu.c (runs in a worker)."""
-    workload, width, reps = args
-    key = (workload, width)
-    if key not in _SAMPLE_CACHE:
-        import gpair_b200 as g
-        from oracle import oracle as O
-        s = cpu_sample_problem(g.workload_problem(workload), width)
-        _SAMPLE_CACHE[key] = (s, O.RefEvaluator(s))
-    s, ev = _SAMPLE_CACHE[key]
-    img = s.start_image()
+# CPU sample of a workload: one spectral channel of its data (the middle one),
+# indexed by the reference's getoifits.c, on a SAMPLE_WIDTH^2 image. The
+# reference's criterion + gradient cost is linear in the pixel count and in the
+# V2 and triangle counts, and one channel keeps the workload's ratio of
+# triangles to uv points, so the per-FLOP rate carries over to the full size.
+SAMPLE_WIDTH = 32
+
+
+def reference_sample(workload: str, oi=None, width: int = SAMPLE_WIDTH) -> dict:
+    """Arrays of the CPU sample, built only by the reference's compiled code:
+    getoifits.c for the uv / triangle indices, gpair.c's init_data for the data
+    packing, cpu.c's set_model for the prior."""
+    import numpy as np
+    from oracle import oracle as O
+    synth, oifits_mod = data_modules()
+    w = synth.workload(workload)
+    if oi is None:
+        _, oi = synth.make_workload_data(workload)
+    nch = len(w.array.wavelengths_m)
+    ch = nch // 2
+    sub = subset_channels(oi, [ch], oifits_mod)
+    ix = O.ref_index(sub)
+    data, err, ph, _ = O.ref_init_data(ix["npow"], ix["nbis"], ix["pow"], ix["powerr"], ix["bisamp"],
+                                       ix["bisamperr"], ix["bisphs"], ix["bisphserr"], ix["uvpnt"], 1)
+    model = O.ref_set_model(width, w.pixellation_mas, 0, 0.0, 1.0)
+    full_nuv_est = ix["nuv"] * nch
+    return {"width": width, "pixellation": w.pixellation_mas, "uv": ix["uv"], "npow": ix["npow"],
+            "nbis": ix["nbis"], "data": data, "data_err": err, "phasor": ph, "uvpnt": ix["uvpnt"],
+            "sign": ix["sign"], "model": model, "alpha": w.alpha, "full_width": w.image_width, "channels": nch,
+            "channel": ch, "full_nuv_est": full_nuv_est,
+            "describe": (f"channel {ch + 1} of {nch} ({ix['npow']} V2, {ix['nbis']} T3, nuv {ix['nuv']}, indexed by "
+                         f"the reference's getoifits.c) on a {width}x{width} image")}
+
+
+class _SampleProblem:
+    def __init__(self, s):
+        self.__dict__.update(s)
+
+    @property
+    def nuv(self):
+        return int(self.uv.shape[0])
+
+    @property
+    def npix(self):
+        return self.width * self.width
+
+    def dft_flops(self):
+        return 4.0 * self.npix * self.nuv + 8.0 * self.width * self.nuv
+
+
+_WORKER = {}
+
+
+def _ref_worker_init(sample):
+    """Pool initializer: the reference's cpu.c evaluator on the sample arrays."""
+    from oracle import oracle as O
+    p = _SampleProblem(sample)
+    _WORKER["p"] = p
+    _WORKER["ev"] = O.RefEvaluator(p)
+    # cpu.c's image2vis prints on every call (gpair1/trunk/cpu.c:460)
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)
+
+
+def _ref_eval(reps):
+    """`reps` criterion + gradient evaluations with the reference's cpu.c."""
+    import numpy as np
+    p, ev = _WORKER["p"], _WORKER["ev"]
+    img = np.maximum(p.model, np.float32(1e-8)).astype(np.float32)
     t0 = time.perf_counter()
     for _ in range(reps):
         ev.chi2(img)
         ev.data_gradient(img)
         ev.entropy_gradient(img)
     dt = time.perf_counter() - t0
-    flops = reps * 2 * s.dft_flops()
-    return flops, dt
+    return reps * 2 * p.dft_flops(), dt
 
 
-def cpu_baseline(workload, width=32, reps=3):
-    flops, dt = _ref_eval_worker((workload, width, reps))
+def cpu_baseline(sample, reps=3):
+    """The reference's cpu.c on the sample, one core, in this process."""
+    import numpy as np
+    from oracle import oracle as O
+    p = _SampleProblem(sample)
+    ev = O.RefEvaluator(p)
+    img = np.maximum(p.model, np.float32(1e-8)).astype(np.float32)
+    sys.stdout.flush()
+    saved = os.dup(1)
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)  # cpu.c's image2vis prints on every call
+    try:
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            ev.chi2(img)
+            ev.data_gradient(img)
+            ev.entropy_gradient(img)
+        dt = time.perf_counter() - t0
+    finally:
+        os.dup2(saved, 1)
+        os.close(saved)
+        os.close(devnull)
+    flops = reps * 2 * p.dft_flops()
+    per_eval = dt / reps
+    scale = (sample["full_width"] / p.width) ** 2 * sample["channels"]
     return {"value": flops / dt / 1e12, "unit": UNIT, "cores": 1, "kind": "reference",
-            "sample": f"reference cpu.c criterion+gradient on a {width}x{width} image with the full data "
-                      f"({reps} evaluations, {dt:.1f} s)"}
+            "sample": f"reference cpu.c criterion+gradient, {sample['describe']}, {reps} evaluations ({dt:.1f} s)",
+            "extrapolated": True,
+            "extrapolated_full_evaluation_s": per_eval * scale,
+            "extrapolation": (f"per-evaluation time x (full width / sample width)^2 x channels = x{scale:.0f}; the "
+                              "reference's cost is linear in pixels, V2 points and triangles")}
 
+
+def run_reference(args, rank):
+    """The reference arm: the reference's own compiled cpu.c on all host cores,
+    on the CPU sample of the workload (see reference_sample)."""
+    import multiprocessing as mp
+    if rank != 0:
+        return
+    t_setup = time.perf_counter()
+    sample = reference_sample(args.workload)
+    t_setup = time.perf_counter() - t_setup
+    cores = os.cpu_count() or 1
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores, initializer=_ref_worker_init, initargs=(sample,)) as pool:
+        for _ in range(args.warmup):
+            pool.map(_ref_eval, [1] * cores)
+        t0 = time.perf_counter()
+        tot = 0.0
+        for _ in range(args.steps):
+            res = pool.map(_ref_eval, [1] * cores)
+            tot += sum(r[0] for r in res)
+        dt = time.perf_counter() - t0
+    value = tot / dt / 1e12
+    synth, _ = data_modules()
+    w = synth.workload(args.workload)
+    cfg = w.array
+    nbl = cfg.n_tel * (cfg.n_tel - 1) // 2
+    ntri = cfg.n_tel * (cfg.n_tel - 1) * (cfg.n_tel - 2) // 6 if cfg.triangles == "all" else (
+        (cfg.n_tel - 1) * (cfg.n_tel - 2) // 2)
+    nch = len(cfg.wavelengths_m)
+    maps = _mapped_libraries()
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": dt * 1e3 / max(args.steps, 1), "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32 (reference cpu.c, float complex)",
+           "data": "synthetic (seeded)", "impl": "reference",
+           "config": {"workload": (f"{args.workload}: {w.image_width}x{w.image_width} image, "
+                                   f"{nbl * cfg.n_ha * nch} V2, {ntri * cfg.n_ha * nch} T3"),
+                      "sample": (f"{sample['describe']}; one criterion+gradient evaluation per core per step; "
+                                 "throughput extrapolates to the full workload (cost linear in pixels, V2 points "
+                                 "and triangles)"),
+                      "setup_s": t_setup},
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                            "sample": f"{cores} processes x criterion+gradient, {sample['describe']}"},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+           "native_libraries": maps}
+    if any("libgpair_b200" in m for m in maps):
+        raise RuntimeError("the reference arm mapped this project's library")
+    print(json.dumps(out), flush=True)
+
+
+def _mapped_libraries():
+    """Shared objects of this repository mapped into this process."""
+    out = set()
+    try:
+        with open("/proc/self/maps") as f:
+            for ln in f:
+                parts = ln.split()
+                if len(parts) >= 6 and parts[-1].endswith(".so") and parts[-1].startswith(ROOT):
+                    out.add(os.path.relpath(parts[-1], ROOT))
+    except OSError:
+        pass
+    return sorted(out)
+
+
+# ----------------------------------------------------------- our arm
 
 def replica_seeds(rank):
     """Seeds of rank `rank`'s replica: the same array and scene on every rank, an own noise seed."""
@@ -276,87 +460,45 @@ def time_to_objective(n_problems: int, race_fr: bool = False) -> dict:
     return out
 
 
-def run_reference(args, rank):
-    """The reference arm: the reference's own compiled cpu.c on all host cores."""
-    import multiprocessing as mp
-    if rank != 0:
-        return
-    import gpair_b200 as g
-    p = g.workload_problem(args.workload)
-    cores = os.cpu_count() or 1
-    width = 32
-    ctx = mp.get_context("spawn")
-    with ctx.Pool(cores) as pool:
-        for _ in range(args.warmup):
-            pool.map(_ref_eval_worker, [(args.workload, width, 1)] * cores)
-        t0 = time.perf_counter()
-        tot = 0.0
-        for _ in range(args.steps):
-            res = pool.map(_ref_eval_worker, [(args.workload, width, 1)] * cores)
-            tot += sum(r[0] for r in res)
-        dt = time.perf_counter() - t0
-    value = tot / dt / 1e12
-    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-           "warmup": args.warmup, "ms_per_step": dt * 1e3 / max(args.steps, 1), "higher_is_better": True,
-           "scaling": "weak", "vs_baseline": None, "dtype": "f32 (reference cpu.c, float complex)",
-           "data": "synthetic (seeded)", "impl": "reference",
-           "config": {"workload": f"{args.workload}: {p.width}x{p.width}, {p.npow} V2, {p.nbis} T3, nuv {p.nuv}",
-                      "sample": f"criterion+gradient on a {width}x{width} image with the full data, one per core"},
-           "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
-                            "sample": f"{cores} processes x criterion+gradient on {width}x{width} with the full data"},
-           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(out), flush=True)
+def time_to_objective_workload(rec, p, iters: int, batch_iters: int) -> dict:
+    """Time-to-objective on the benchmark workload itself: plain CG (reference
+    line search) for `iters` iterations sets J*, then plain CG and the batched
+    line search are each timed from the flat prior to J* (1 + 1e-4)."""
+    from gpair_b200 import timetoobj as TT
+    row = TT.evaluate(rec, p, None, iters=iters, batch_iters=batch_iters, objective_from="plain")
+    row["speedup_batch_vs_plain"] = row["plain_s"] / max(row["batch_s"], 1e-12)
+    row["unit"] = "s (host wall clock)"
+    row["note"] = f"J* = lowest J of {iters} plain PR+ iterations with the reference's line search"
+    return row
 
 
-def run_ours(args, rank, world, local):
-    import numpy as np
+def measure_plain(rec, p, args, flush, local, dist):
+    """Timed plain CG iterations (device time, CUDA events inside the library),
+    their per-stage times and the e2e leg through the public API."""
     import torch
-    import gpair_b200 as g
-
-    dist = world > 1
-    if dist:
-        import datetime
-        torch.cuda.set_device(local)
-        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                             device_id=torch.device("cuda", local))
-    else:
-        torch.cuda.set_device(local)
-    # one independent replica per rank: same array and scene, own noise seed
-    p = g.workload_problem(args.workload, **replica_seeds(rank))
-    prec = {"fp32": g.PREC_FP32, "split16": g.PREC_SPLIT16, "tf32": g.PREC_TF32}[args.precision]
-    rec = g.Reconstructor(local)
-    rec.set_problem(p)
-    rec.set_precision(prec)
-    rec.set_stage_timing(True)
-    rec.set_image(p.start_image())
-    # autotuned adjoint split-K length (precision stays as requested)
-    tune = rec.autotune(g.api.TUNE_SPLITS, reps=3)
-    rec.set_image(p.start_image())
-    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
-
-    # warm-up iterations (untimed); builds the CG graph
-    rec.cg(max(args.warmup, 1), method=2, resume=False, host_loop=int(args.host_loop), line_search=LS[args.line_search])
+    rec.cg(max(args.warmup, 1), method=2, resume=False, host_loop=int(args.host_loop),
+           line_search=LS[args.line_search])  # untimed warm-up; builds the CG graph
     sampler = ClockSampler(local)
     if dist:
         torch.distributed.barrier()
     torch.cuda.synchronize()
     sampler.start()
     time.sleep(0.5)  # let the sampler take its first sample before the timed steps
-    dev_ms, flops, launches, evals, crit_evals, grad_evals = 0.0, 0.0, 0, 0, 0, 0
+    dev_ms, flops, launches, crit_evals, grad_evals = 0.0, 0.0, 0, 0, 0
     for k in range(args.steps):
         flush.fill_(float(k))  # 512 MiB write: L2 (126 MB) holds none of the inputs at step start
         torch.cuda.synchronize()
-        out = rec.cg(1, method=2, resume=True, host_loop=int(args.host_loop), line_search=LS[args.line_search])  # one graph launch per CG iteration
+        out = rec.cg(1, method=2, resume=True, host_loop=int(args.host_loop), line_search=LS[args.line_search])
         ms, fl, nl = rec.last_run_stats()
         dev_ms += ms
         flops += fl
         launches += nl
-        evals += out["criterion_evals"] + out["grad_evals"]
         crit_evals += out["criterion_evals"]
         grad_evals += out["grad_evals"]
     torch.cuda.synchronize()
     if dist:
         torch.distributed.barrier()
+    time.sleep(0.3)
     clocks = sampler.stop()
 
     # per-kernel times for the roofline: every stage of criterion + gradient
@@ -364,9 +506,7 @@ def run_ours(args, rank, world, local):
     # CUDA events (after an L2 flush), on the state the timed steps left
     flush.fill_(0.0)
     torch.cuda.synchronize()
-    st = rec.time_stages(reps=args.steps)
-    # each stage weighted by how often the timed steps ran it: the criterion
-    # stages once per criterion evaluation, the gradient stages once per gradient
+    st = rec.time_stages(reps=min(args.steps, 10))
     crit_stages = ("prep", "forward_dft", "vis_data")
     stage_n = {k: (crit_evals if k in crit_stages else grad_evals) for k in st}
     stage_ms = {k: st[k] * stage_n[k] for k in st}
@@ -383,9 +523,49 @@ def run_ours(args, rank, world, local):
         img = rec.get_image()  # D2H of the step's result
         e2e_s += time.perf_counter() - t0
         e2e_flops += rec.last_run_stats()[1]
+    return {"dev_ms": dev_ms, "flops": flops, "launches": launches, "evals": crit_evals + grad_evals,
+            "crit_evals": crit_evals, "grad_evals": grad_evals, "clocks": clocks, "stage_n": stage_n,
+            "stage_ms": stage_ms, "e2e_s": e2e_s, "e2e_flops": e2e_flops, "img": img}
 
-    # the same CG iterations with the batched line search (8 trial images per
-    # tcgen05 forward launch), device-timed like the headline steps
+
+def roofline(p, m, precision, workload):
+    """Roofline of the dominant stage (largest total time over the timed steps)."""
+    hbm, tflops_peak, peak_kind = _peaks()
+    stage_ms, stage_n = m["stage_ms"], m["stage_n"]
+    dom = max(stage_ms, key=lambda k: stage_ms[k])
+    per_launch_ms = stage_ms[dom] / max(stage_n[dom], 1)
+    if dom in ("forward_dft", "adjoint_dft"):
+        work = p.dft_flops()
+        achieved = work / (per_launch_ms * 1e-3) / 1e12
+        roof = {"bound": "tensor", "achieved": achieved, "peak": tflops_peak, "unit": "TFLOP/s",
+                "frac": achieved / tflops_peak, "work_per_launch": work,
+                "work_note": "algorithmic FLOPs 4 N^2 nuv + 8 N nuv per launch (one image)"}
+        mult = 3.0 if precision == "split16" else 1.0  # MMAs issued per algorithmic product
+        roof["executed_tflops"] = mult * achieved
+        roof["executed_frac"] = mult * achieved / tflops_peak
+        roof["executed_note"] = "split16 issues 3 f16 MMAs (hi*hi, hi*lo, lo*hi) per algorithmic product"
+    else:
+        bytes_per = {"prep": 8 * p.npix, "vis_data": 16 * p.npow + 60 * p.nbis,
+                     "adj_weights": 8 * p.npow + 24 * p.nbis, "grad_finalize": 16 * p.npix}[dom]
+        achieved = bytes_per / (per_launch_ms * 1e-3) / 1e9
+        roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                "work_per_launch": bytes_per}
+    roof["kernel"] = dom
+    roof["peak_source"] = peak_kind
+    roof["timing"] = ("per-stage CUDA events, stages queued back to back; stage totals = per-launch time x "
+                      "the timed steps' criterion (prep, forward, vis_data) or gradient evaluations")
+    roof["traffic"] = _traffic(f"{dom}@{workload}@{precision}")
+    roof["stage_ms_per_launch"] = {k: stage_ms[k] / max(stage_n[k], 1) for k in stage_ms}
+    roof["stage_share"] = {k: stage_ms[k] / max(sum(stage_ms.values()), 1e-12) for k in stage_ms}
+    return roof
+
+
+def batched_block(rec, p, args, flush, img, precision, workload):
+    """The same CG iterations with the batched line search (8 trial images per
+    tcgen05 forward launch), device-timed like the headline steps."""
+    import torch
+    import gpair_b200 as g
+    hbm, tflops_peak, peak_kind = _peaks()
     bat_ms, bat_flops, bat_evals = 0.0, 0.0, 0
     rec.set_image(img)
     rec.cg(max(args.warmup, 1), method=2, resume=False, line_search=g.LS_BATCH, host_loop=int(args.host_loop))
@@ -399,80 +579,117 @@ def run_ours(args, rank, world, local):
         bat_evals += out_b["criterion_evals"] + out_b["grad_evals"]
     flush.fill_(0.0)
     torch.cuda.synchronize()
-    st_b = rec.time_batch_stages(reps=args.steps)
-
-    (max_ms, max_e2e), (tot_flops, tot_e2e_flops) = combine_over_ranks(
-        [dev_ms, e2e_s], [flops, e2e_flops], f"cuda:{local}")
-
-    if rank == 0:
-        hbm, tflops_peak, peak_kind = _peaks()
-        # dominant stage and its roofline
-        dom = max(stage_ms, key=lambda k: stage_ms[k])
-        per_launch_ms = stage_ms[dom] / max(stage_n[dom], 1)
-        N, nuv = p.width, p.nuv
-        if dom in ("forward_dft", "adjoint_dft"):
-            work = p.dft_flops()
-            achieved = work / (per_launch_ms * 1e-3) / 1e12
-            roof = {"bound": "tensor", "achieved": achieved, "peak": tflops_peak, "unit": "TFLOP/s",
-                    "frac": achieved / tflops_peak}
-        else:
-            bytes_per = {"prep": 8 * p.npix, "vis_data": 16 * p.npow + 60 * p.nbis,
-                         "adj_weights": 8 * p.npow + 24 * p.nbis, "grad_finalize": 16 * p.npix}[dom]
-            achieved = bytes_per / (per_launch_ms * 1e-3) / 1e9
-            roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm}
-        roof["kernel"] = dom
-        roof["peak_source"] = peak_kind
-        roof["timing"] = ("per-stage CUDA events, stages queued back to back; stage totals = per-launch time x "
-                          "the timed steps' criterion (prep, forward, vis_data) or gradient evaluations")
-        roof["traffic"] = _traffic(f"{dom}@{args.workload}@{args.precision}")
-        roof["stage_ms_per_launch"] = {k: stage_ms[k] / max(stage_n[k], 1) for k in stage_ms}
-        roof["stage_share"] = {k: stage_ms[k] / max(sum(stage_ms.values()), 1e-12) for k in stage_ms}
-        value = tot_flops / (max_ms * 1e-3) / 1e12
-        e2e = tot_e2e_flops / max_e2e / 1e12
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None,
-                "dtype": {"fp32": "fp32", "split16": "f16 hi+lo split operands, fp32 accumulate",
-                          "tf32": "tf32 operands, fp32 accumulate"}[args.precision],
-                "data": "synthetic (seeded array, scene and noise; no public data set of this size)",
-                "config": {"workload": f"{args.workload}: {N}x{N} image, {p.npow} V2, {p.nbis} T3, nuv {nuv}",
-                           "step": ("one PR+ CG iteration with strong-Wolfe line search (continuing)"
-                                    if args.line_search == "wolfe" else
-                                    "one PR+ CG iteration with the batched 8-trial line search (continuing)"),
-                           "precision": args.precision, "evaluations": evals,
-                           "autotuned_adjoint_splits": tune["adjoint_splits"],
-                           "l2": "flushed (512 MiB write) before every timed step, outside the timed region",
-                           "parallelism": f"replicas x{world}",
-                           "cg_driver": "host loop" if args.host_loop else "one CUDA graph per step"},
-                "gpu_launches": launches, "clocks": clocks, "roofline": roof,
-                "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 4 * p.npix,
-                        "d2h_bytes_per_step": 4 * p.npix}}
-        mult = 3.0 if args.precision == "split16" else 1.0  # MMAs issued per algorithmic product
-        if dom in ("forward_dft", "adjoint_dft"):
-            roof["executed_tflops"] = mult * roof["achieved"]
-            roof["executed_frac"] = mult * roof["frac"]
-            roof["executed_note"] = "split16 issues 3 f16 MMAs (hi*hi, hi*lo, lo*hi) per algorithmic product"
-        fb_ms = st_b["forward_dft_batch"]
-        fb_ach = 8 * p.dft_flops() / (fb_ms * 1e-3) / 1e12
-        line["batched_line_search"] = {
-            "value": bat_flops / max(bat_ms * 1e-3, 1e-12) / 1e12, "unit": UNIT,
+    st_b = rec.time_batch_stages(reps=min(args.steps, 10))
+    mult = 3.0 if precision == "split16" else 1.0
+    fb_ms = st_b["forward_dft_batch"]
+    fb_ach = 8 * p.dft_flops() / (fb_ms * 1e-3) / 1e12
+    return {"value": bat_flops / max(bat_ms * 1e-3, 1e-12) / 1e12, "unit": UNIT,
             "ms_per_step": bat_ms / max(args.steps, 1), "evaluations": bat_evals,
             "note": "CG iterations with 8 trial images per batched evaluation (rank 0, device time)",
             "roofline": {"bound": "tensor", "kernel": "forward_dft_batch (8 stacked trial images)",
                          "achieved": fb_ach, "peak": tflops_peak, "unit": "TFLOP/s", "frac": fb_ach / tflops_peak,
                          "executed_tflops": mult * fb_ach, "executed_frac": mult * fb_ach / tflops_peak,
                          "peak_source": peak_kind,
-                         "traffic": _traffic(f"forward_dft_batch8@{args.workload}@{args.precision}"),
+                         "traffic": _traffic(f"forward_dft_batch8@{workload}@{precision}"),
                          "stage_ms_per_launch": st_b,
                          "timing": "CUDA events around the three batched stages queued back to back"}}
+
+
+def _describe(name, p):
+    return f"{name}: {p.width}x{p.width} image, {p.npow} V2, {p.nbis} T3, nuv {p.nuv}"
+
+
+def run_ours(args, rank, world, local):
+    import torch
+    import gpair_b200 as g
+    from gpair_b200 import synth
+
+    dist = world > 1
+    if dist:
+        import datetime
+        torch.cuda.set_device(local)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                             device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(local)
+    # one independent replica per rank: same array and scene, own noise seed
+    seeds = replica_seeds(rank)
+    w, oi = synth.make_workload_data(args.workload, **seeds)
+    p = g.problem_from_oifits(oi, w.image_width, w.pixellation_mas, w.alpha, modeltype=0, modelflux=w.prior_flux)
+    prec = {"fp32": g.PREC_FP32, "split16": g.PREC_SPLIT16}[args.precision]
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+    rec = g.Reconstructor(local)
+    rec.set_problem(p)
+    rec.set_precision(prec)
+    rec.set_stage_timing(True)
+    rec.set_image(p.start_image())
+    # autotuned adjoint split-K length (precision stays as requested)
+    tune = rec.autotune(g.api.TUNE_SPLITS, reps=3)
+    rec.set_image(p.start_image())
+
+    m = measure_plain(rec, p, args, flush, local, dist)
+    (max_ms, max_e2e), (tot_flops, tot_e2e_flops) = combine_over_ranks(
+        [m["dev_ms"], m["e2e_s"]], [m["flops"], m["e2e_flops"]], f"cuda:{local}")
+
+    if rank == 0:
+        roof = roofline(p, m, args.precision, args.workload)
+        value = tot_flops / (max_ms * 1e-3) / 1e12
+        e2e = tot_e2e_flops / max_e2e / 1e12
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": {"fp32": "fp32", "split16": "f16 hi+lo split operands, fp32 accumulate"}[args.precision],
+                "data": "synthetic (seeded array, scene and noise; no public data set of this size)",
+                "config": {"workload": _describe(args.workload, p),
+                           "step": ("one PR+ CG iteration with strong-Wolfe line search (continuing)"
+                                    if args.line_search == "wolfe" else
+                                    "one PR+ CG iteration with the batched 8-trial line search (continuing)"),
+                           "precision": args.precision, "evaluations": m["evals"],
+                           "criterion_evals": m["crit_evals"], "grad_evals": m["grad_evals"],
+                           "flop_per_evaluation": p.dft_flops(),
+                           "autotuned_adjoint_splits": tune["adjoint_splits"],
+                           "l2": "flushed (512 MiB write) before every timed step, outside the timed region",
+                           "parallelism": f"replicas x{world}", "seeds": seeds,
+                           "cg_driver": "host loop" if args.host_loop else "one CUDA graph per step"},
+                "gpu_launches": m["launches"], "clocks": m["clocks"], "roofline": roof,
+                "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 4 * p.npix,
+                        "d2h_bytes_per_step": 4 * p.npix}}
+        if not args.no_batched:
+            line["batched_line_search"] = batched_block(rec, p, args, flush, m["img"], args.precision, args.workload)
         if world == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(args.workload)
+            line["cpu_baseline"] = cpu_baseline(reference_sample(args.workload, oi))
+        if not args.no_time_to_objective and args.tto_workload_iters > 0:
+            line["time_to_objective_workload"] = time_to_objective_workload(
+                rec, p, args.tto_workload_iters, args.tto_workload_iters)
+    rec.close()
+    del oi, p
+
+    if rank == 0:
+        # the 256x256 precision workload beside the headline (context, same step)
+        if args.workload != "precision" and not args.no_precision_256:
+            p2 = g.workload_problem("precision", **seeds)
+            with g.Reconstructor(local) as r2:
+                r2.set_problem(p2)
+                r2.set_precision(prec)
+                r2.set_stage_timing(True)
+                r2.set_image(p2.start_image())
+                r2.autotune(g.api.TUNE_SPLITS, reps=3)
+                r2.set_image(p2.start_image())
+                m2 = measure_plain(r2, p2, args, flush, local, False)
+                blk = {"workload": _describe("precision", p2), "value": m2["flops"] / (m2["dev_ms"] * 1e-3) / 1e12,
+                       "unit": UNIT, "ms_per_step": m2["dev_ms"] / args.steps, "evaluations": m2["evals"],
+                       "gpu_launches": m2["launches"], "clocks": m2["clocks"],
+                       "e2e": {"value": m2["e2e_flops"] / m2["e2e_s"] / 1e12, "unit": UNIT},
+                       "roofline": roofline(p2, m2, args.precision, "precision")}
+                if not args.no_batched:
+                    blk["batched_line_search"] = batched_block(r2, p2, args, flush, m2["img"], args.precision,
+                                                               "precision")
+                line["precision_256"] = blk
         if not args.no_time_to_objective:
             line["time_to_objective"] = time_to_objective(args.tto_problems, race_fr=args.tto_race_fr)
         if args.instances > 0:
             line["many_instances"] = many_instances(args.instances, args.instance_iters)
         print(json.dumps(line), flush=True)
-    rec.close()
     if dist:
         torch.distributed.destroy_process_group()
 
@@ -480,20 +697,25 @@ def run_ours(args, rank, world, local):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="precision")
+    ap.add_argument("--workload", default="large", choices=["large", "precision", "small", "tiny"])
     ap.add_argument("--precision", default=os.environ.get("GPAIR_BENCH_PRECISION", "split16"),
-                    choices=["fp32", "split16", "tf32"])
+                    choices=["fp32", "split16"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-time-to-objective", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched line-search block")
+    ap.add_argument("--no-precision-256", action="store_true", help="skip the 256x256 context block")
     ap.add_argument("--instances", type=int, default=64, help="independent reconstructions run at once (0: skip)")
     ap.add_argument("--instance-iters", type=int, default=30)
     ap.add_argument("--line-search", choices=["wolfe", "batch"], default="wolfe",
                     help="line search of the headline steps: the reference's (default) or the batched one")
     ap.add_argument("--tto-problems", type=int, default=16,
                     help="held-out warm-start problems timed for the time-to-objective block")
+    ap.add_argument("--tto-workload-iters", type=int, default=60,
+                    help="plain-CG iterations that set J* for the time-to-objective block on the benchmark "
+                         "workload itself (0: skip)")
     ap.add_argument("--tto-race-fr", action="store_true",
                     help="add a flat-start Fletcher-Reeves runner to the time-to-objective race")
     ap.add_argument("--host-loop", action="store_true",

@@ -133,6 +133,7 @@ def lib() -> C.CDLL:
         L.gpair_time_stages.argtypes = [vp, i, C.POINTER(d), i]
         L.gpair_time_batch_stages.argtypes = [vp, i, C.POINTER(d), i]
         L.gpair_set_stage_timing.argtypes = [vp, i]
+        L.gpair_set_tc_wait.argtypes = [vp, C.c_longlong, i]
         L.gpair_last_run_stage_ms.argtypes = [vp, C.POINTER(d), C.POINTER(i), i]
         L.gpair_get_oi_fits_data.argtypes = [i, f, f, i, vp, i, vp, i, vp, C.POINTER(OiData)]
         L.gpair_free_oi_data.argtypes = [C.POINTER(OiData)]
@@ -213,6 +214,9 @@ def _declare_reference_boundary(L):
     for name in ("gpu_getp_ci", "gpu_getp_ti", "gpu_getp_fgn", "gpu_getp_fg", "gpu_getp_dd", "gpu_getp_tg",
                  "gpu_getp_eg"):
         proto[name] = (vp, [])
+    proto["gpair_set_zoom_trial_cap"] = (C.c_int, [i])
+    proto["gpair_zoom_cap_hits"] = (C.c_int, [])
+    proto["gpair_zoom_cap_hits_reset"] = (None, [])
     for name, (res, args) in proto.items():
         fn = getattr(L, name)
         fn.restype = res

@@ -34,18 +34,6 @@ def _nvcc() -> str:
     raise RuntimeError("nvcc not found")
 
 
-def _cutlass_include() -> str | None:
-    try:
-        import flashinfer  # noqa: F401  (only to locate the vendored CuTe headers)
-        base = os.path.dirname(flashinfer.__file__)
-    except Exception:
-        base = None
-    for cand in ([os.path.join(base, "data", "cutlass", "include")] if base else []):
-        if os.path.isdir(cand):
-            return cand
-    return None
-
-
 def _sources():
     cu = sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cu"))
     c = sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".c"))

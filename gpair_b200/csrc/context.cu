@@ -362,6 +362,14 @@ static void stage_collect(gpair_ctx *c)
     c->st_n = 0;
 }
 
+extern "C" int gpair_set_tc_wait(gpair_ctx *c, long long budget_cycles, int skip_loads)
+{
+    if (!c || budget_cycles < 0) return GPAIR_ERR_INVALID;
+    c->tc_wait_budget = budget_cycles;
+    c->tc_skip_loads = skip_loads ? 1 : 0;
+    return GPAIR_OK;
+}
+
 extern "C" int gpair_set_stage_timing(gpair_ctx *c, int on)
 {
     if (!c) return GPAIR_ERR_INVALID;
@@ -577,9 +585,10 @@ extern "C" int gpair_cg_checkpoint_save(gpair_ctx *c, void *buf, size_t bytes)
     memcpy(p, &c->sc_host->cg, sizeof(CgState));
     p += sizeof(CgState);
     for (int i = 0; i < kCkArrays; i++) {
-        GP_CUDA(c, cudaMemcpy(p, ck_array(c, i), sizeof(float) * c->npix, cudaMemcpyDeviceToHost));
+        GP_CUDA(c, cudaMemcpyAsync(p, ck_array(c, i), sizeof(float) * c->npix, cudaMemcpyDeviceToHost, c->stream));
         p += sizeof(float) * c->npix;
     }
+    GP_CUDA(c, cudaStreamSynchronize(c->stream));
     return GPAIR_OK;
 }
 
@@ -599,12 +608,16 @@ extern "C" int gpair_cg_checkpoint_load(gpair_ctx *c, const void *buf, size_t by
     if (rc) return rc;
     if ((rc = gpair_set_regularizer(c, h.reg_kind))) return rc;
     const unsigned char *p = (const unsigned char *)buf + sizeof(h);
-    GP_CUDA(c, cudaMemcpy(&c->sc->cg, p, sizeof(CgState), cudaMemcpyHostToDevice));
+    // every copy on the context's stream, after the work already queued there;
+    // the caller's buffer may be pageable, so wait until the last copy landed
+    GP_CUDA(c, cudaStreamSynchronize(c->stream));
+    GP_CUDA(c, cudaMemcpyAsync(&c->sc->cg, p, sizeof(CgState), cudaMemcpyHostToDevice, c->stream));
     p += sizeof(CgState);
     for (int i = 0; i < kCkArrays; i++) {
-        GP_CUDA(c, cudaMemcpy(ck_array(c, i), p, sizeof(float) * c->npix, cudaMemcpyHostToDevice));
+        GP_CUDA(c, cudaMemcpyAsync(ck_array(c, i), p, sizeof(float) * c->npix, cudaMemcpyHostToDevice, c->stream));
         p += sizeof(float) * c->npix;
     }
+    GP_CUDA(c, cudaStreamSynchronize(c->stream));
     c->have_image = 1;
     c->last_image_src = -1;
     gp_cg_graph_free(c);

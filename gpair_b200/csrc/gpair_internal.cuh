@@ -210,6 +210,12 @@ struct gpair_ctx {
     gpair_short4 *ref_sign;
     int ref_data_size, ref_phasor_size, ref_bsref_size, ref_npow;
     int bound_nuv, bound_npow, bound_nbis;
+
+    // tensor-core kernels: clock budget of each pipeline wait (0 = default)
+    // and a failure-path test switch: the TMA producer issues no loads, so
+    // the MMA and epilogue waits run out with no copy in flight
+    long long tc_wait_budget;
+    int tc_skip_loads;
 };
 
 // ---------------------------------------------------------------- helpers

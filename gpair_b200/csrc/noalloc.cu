@@ -132,6 +132,12 @@ extern "C" int gpair_vis2data_chi2_noalloc(const gpair_float2 *visi, int nuv, in
     int rc = noalloc_scratch_for_current_device(&scratch);
     if (rc) return rc;
     cudaStream_t s = (cudaStream_t)stream;
+    if (s) {
+        // the scratch address belongs to the current device: the stream must too
+        int cur = -1, sdev = -1;
+        if (cudaGetDevice(&cur) != cudaSuccess || cudaStreamGetDevice(s, &sdev) != cudaSuccess) return GPAIR_ERR_CUDA;
+        if (sdev != cur) return GPAIR_ERR_INVALID;
+    }
     // the counter and the error word must start at zero; the partials are overwritten
     if (cudaMemsetAsync(scratch, 0, 2 * sizeof(unsigned int), s) != cudaSuccess) return GPAIR_ERR_CUDA;
     int blocks = items > 0 ? (int)((items + NOALLOC_THREADS - 1) / NOALLOC_THREADS) : 1;

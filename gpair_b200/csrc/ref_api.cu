@@ -543,6 +543,26 @@ extern "C" gpair_buf *gpu_getp_eg(void) { return g_ctx ? &g_ctx->h_eg : nullptr;
 
 // ------------------------------------------------------------ line search
 
+// The reference's zoom can spin forever once steplength_low and
+// steplength_high are adjacent floats far from zero (their difference never
+// drops below 1e-14). This one stops after g_zoom_cap trials (200 unless set)
+// and returns steplength_low, like the reference's exit with no better point.
+// Each stop at the cap is counted and recorded in the global context's
+// last_error, so a caller of the drop-in layer can tell.
+static int g_zoom_cap = 200;
+static int g_zoom_cap_hits = 0;
+
+extern "C" int gpair_set_zoom_trial_cap(int cap)
+{
+    if (cap < 0) return GPAIR_ERR_INVALID;
+    g_zoom_cap = cap ? cap : 200;
+    return GPAIR_OK;
+}
+
+extern "C" int gpair_zoom_cap_hits(void) { return g_zoom_cap_hits; }
+
+extern "C" void gpair_zoom_cap_hits_reset(void) { g_zoom_cap_hits = 0; }
+
 // gpair1/trunk/gpu.c:1947-2065, float scalars as in the reference. The
 // reference's `*criterion_evals++` advances a local pointer and leaves the
 // counters untouched; the counters are left untouched here as well.
@@ -559,7 +579,7 @@ extern "C" float gpu_linesearch_zoom(int nuv, int npow, int nbis, int data_alloc
     int counter = 0;
     float minvalue = 1e-8;
     float wolfe_param1 = 1e-4, wolfe_param2 = 0.1;
-    for (int guard = 0; guard < 200; guard++) {
+    for (int guard = 0; guard < g_zoom_cap; guard++) {
         if ((counter > 0) && (criterion_old - criterion_init - wolfe_product1 * steplength_old) != 0.)
             steplength = fabs(wolfe_product1 * steplength_old * steplength_old
                               / (2. * (criterion_old - criterion_init - wolfe_product1 * steplength_old)));
@@ -589,6 +609,11 @@ extern "C" float gpu_linesearch_zoom(int nuv, int npow, int nbis, int data_alloc
         criterion_old = criterion;
         counter++;
     }
+    g_zoom_cap_hits++;
+    if (g_ctx)
+        snprintf(g_ctx->last_error, sizeof(g_ctx->last_error),
+                 "gpu_linesearch_zoom stopped at its %d-trial cap and returned steplength_low %.9g", g_zoom_cap,
+                 (double)steplength_low);
     return steplength_low;
 }
 

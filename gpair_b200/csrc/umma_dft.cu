@@ -48,7 +48,7 @@
 #define TC_STAGE_BYTES (2 * TC_A_BYTES + 2 * TC_B_BYTES)
 #define TC_TMEM_COLS 512
 #define TC_SMEM_BYTES (1024 + TC_STAGES * TC_STAGE_BYTES + 256)
-#define TC_WAIT_BUDGET 4000000000LL  // clock cycles (~2 s) per wait
+#define TC_WAIT_BUDGET 4000000000LL  // default clock cycles (~2 s) per pipeline wait
 #define RPMAS_TC ((3.14159265358979323 / 180.0) / 3600000.0)  // radians per milliarcsecond
 
 enum { EPI_FWD = 0, EPI_STORE = 1 };
@@ -68,6 +68,12 @@ struct TcArgs {
     float *gpart;
     int out_ld, out_rows, out_cols;
     unsigned int *err;
+    // clock budget of each pipeline wait; the drain of the TMA copies in
+    // flight always keeps TC_WAIT_BUDGET, so that no copy is outstanding when
+    // the CTA retires. skip_loads: the producer issues no TMA loads (used to
+    // make the other roles' waits run out with nothing in flight)
+    long long budget;
+    int skip_loads;
 };
 
 struct TcState {
@@ -164,23 +170,25 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             for (int u = blockIdx.x; u < a.units && !*abort_flag; u += gridDim.x) {
                 int m, n, kb0, kb1, split;
                 tc_decode<EPI>(a, u, m, n, kb0, kb1, split);
-                for (int kb = kb0; kb < kb1; kb++, it++) {
+                for (int kb = kb0; kb < kb1; kb++) {
                     const int s = it % TC_STAGES;
                     const uint32_t ph = (uint32_t)(it / TC_STAGES) & 1u;
-                    if (!umma::mbar_wait(&empty[s], ph ^ 1u, TC_WAIT_BUDGET)) {
+                    if (!umma::mbar_wait(&empty[s], ph ^ 1u, a.budget)) {
                         tc_fail(a.err, abort_flag, 1u);
                         break;
                     }
+                    if (a.skip_loads) continue;  // nothing issued: the stage never fills
                     unsigned char *st = stages + s * TC_STAGE_BYTES;
                     umma::mbar_arrive_expect_tx(&full[s], TC_STAGE_BYTES);
                     umma::tma_load_2d(st, &tA_hi, &full[s], kb * TC_BK, m * TC_BM);
                     umma::tma_load_2d(st + TC_A_BYTES, &tA_lo, &full[s], kb * TC_BK, m * TC_BM);
                     umma::tma_load_2d(st + 2 * TC_A_BYTES, &tB_hi, &full[s], kb * TC_BK, n * TC_BN);
                     umma::tma_load_2d(st + 2 * TC_A_BYTES + TC_B_BYTES, &tB_lo, &full[s], kb * TC_BK, n * TC_BN);
+                    it++;
                 }
             }
             // no copy may be in flight when the CTA retires: wait for the last
-            // load issued into each stage (bounded)
+            // load issued into each stage (bounded; `it` counts issued stages)
             for (int j = 1; j <= TC_STAGES && it - j >= 0; j++) {
                 const int i = it - j, s = i % TC_STAGES;
                 if (!umma::mbar_wait(&full[s], (uint32_t)(i / TC_STAGES) & 1u, TC_WAIT_BUDGET))
@@ -198,7 +206,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 int m, n, kb0, kb1, split;
                 tc_decode<EPI>(a, u, m, n, kb0, kb1, split);
                 const int b = t & 1;
-                if (!umma::mbar_wait(&tempty[b], ((uint32_t)(t >> 1) & 1u) ^ 1u, TC_WAIT_BUDGET)) {
+                if (!umma::mbar_wait(&tempty[b], ((uint32_t)(t >> 1) & 1u) ^ 1u, a.budget)) {
                     tc_fail(a.err, abort_flag, 2u);
                     break;
                 }
@@ -206,7 +214,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 const uint32_t d = tmem_base + (uint32_t)(b * TC_BN);
                 for (int kb = kb0; kb < kb1; kb++, it++) {
                     const int s = it % TC_STAGES;
-                    if (!umma::mbar_wait(&full[s], (uint32_t)(it / TC_STAGES) & 1u, TC_WAIT_BUDGET)) {
+                    if (!umma::mbar_wait(&full[s], (uint32_t)(it / TC_STAGES) & 1u, a.budget)) {
                         tc_fail(a.err, abort_flag, 4u);
                         ok = false;
                         break;
@@ -258,7 +266,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     const int j = ((y0 + 16 * c) % a.lpad) >> 4;  // anchor of the row within its image
                     an[c] = (vk && j < a.nanc) ? __ldg(&anc[j]) : make_float2(0.f, 0.f);
                 }
-                if (!umma::mbar_wait(&tfull[b], (uint32_t)(t >> 1) & 1u, TC_WAIT_BUDGET)) {
+                if (!umma::mbar_wait(&tfull[b], (uint32_t)(t >> 1) & 1u, a.budget)) {
                     tc_fail(a.err, abort_flag, 8u);
                     break;
                 }
@@ -297,7 +305,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 umma::tc_fence_before();
                 umma::mbar_arrive(&tempty[b]);
             } else {
-                if (!umma::mbar_wait(&tfull[b], (uint32_t)(t >> 1) & 1u, TC_WAIT_BUDGET)) {
+                if (!umma::mbar_wait(&tfull[b], (uint32_t)(t >> 1) & 1u, a.budget)) {
                     tc_fail(a.err, abort_flag, 8u);
                     break;
                 }
@@ -822,6 +830,8 @@ int gp_tc_forward_gemm(gpair_ctx *c)
     a.sc = c->sc;
     a.vpart = c->vpart;
     a.err = &c->sc->tc_err;
+    a.budget = c->tc_wait_budget > 0 ? c->tc_wait_budget : TC_WAIT_BUDGET;
+    a.skip_loads = c->tc_skip_loads;
     int grid = a.units < t->nsm ? a.units : t->nsm;
     k_tc_gemm<EPI_FWD><<<grid, TC_THREADS, TC_SMEM_BYTES, c->stream>>>(t->m_fx_hi, t->m_fx_lo, t->m_img_hi,
                                                                         t->m_img_lo, a);
@@ -895,6 +905,8 @@ int gp_tc_forward_batch_gemm(gpair_ctx *c)
     a.sc = c->sc;
     a.vpart = c->vpart_b;
     a.err = &c->sc->tc_err;
+    a.budget = c->tc_wait_budget > 0 ? c->tc_wait_budget : TC_WAIT_BUDGET;
+    a.skip_loads = c->tc_skip_loads;
     int grid = a.units < t->nsm ? a.units : t->nsm;
     k_tc_gemm<EPI_FWD><<<grid, TC_THREADS, TC_SMEM_BYTES, c->stream>>>(t->m_fx_hi, t->m_fx_lo, t->m_imgb_hi,
                                                                         t->m_imgb_lo, a);
@@ -975,6 +987,8 @@ int gp_tc_adjoint_gemm(gpair_ctx *c)
     a.out_rows = c->N;
     a.out_cols = c->N;
     a.err = &c->sc->tc_err;
+    a.budget = c->tc_wait_budget > 0 ? c->tc_wait_budget : TC_WAIT_BUDGET;
+    a.skip_loads = c->tc_skip_loads;
     int grid = a.units < t->nsm ? a.units : t->nsm;
     k_tc_gemm<EPI_STORE><<<grid, TC_THREADS, TC_SMEM_BYTES, c->stream>>>(t->m_fxt_hi, t->m_fxt_lo, t->m_w_hi,
                                                                           t->m_w_lo, a);

@@ -136,6 +136,15 @@ float gpu_linesearch_zoom(int nuv, int npow, int nbis, int data_alloc, int data_
                           float steplength_low, float steplength_high, float criterion_steplength_low,
                           float wolfe_product1, float criterion_init, int *criterion_evals, int *grad_evals,
                           gpair_buf *pDescent_direction, gpair_buf *pTemp_gradient, float hyperparameter_entropy);
+/* The reference's zoom can loop forever once its bracket is two adjacent
+ * floats; this one stops after a trial cap (200 by default) and returns
+ * steplength_low. No counterpart in the reference: gpair_set_zoom_trial_cap
+ * sets the cap (0 = 200), gpair_zoom_cap_hits counts the zoom calls that
+ * stopped at it (each also writes gpair_last_error of the global context),
+ * gpair_zoom_cap_hits_reset clears the count. */
+int gpair_set_zoom_trial_cap(int cap);
+int gpair_zoom_cap_hits(void);
+void gpair_zoom_cap_hits_reset(void);
 /* gpu.h:102 -- mock data + chi2 from the stored visibilities */
 void gpu_new_chi2(int nuv, int npow, int nbis, int data_alloc);
 /* gpu.h:104 -- V2 and T3 mock data from the stored visibilities */
@@ -440,6 +449,17 @@ int gpair_autotune(gpair_ctx *ctx, int flags, int reps, gpair_tune_result *resul
  * gpair_last_run_stage_ms returns the summed ms and launch count per stage
  * (same stage order as gpair_time_stages) of the last run. */
 int gpair_set_stage_timing(gpair_ctx *ctx, int on);
+
+/* ---- failure path of the tensor-core kernels ----
+ * No counterpart in the reference, which prints and exits on any device error
+ * (gpair1/trunk/gpu.c:186-202). Every pipeline wait of the tcgen05 kernels is
+ * bounded by a clock budget (default about 2 s: budget_cycles = 0); when one
+ * runs out the kernel stops its roles, waits for its TMA copies in flight,
+ * frees its tensor memory and returns, and the call reports GPAIR_ERR_TIMEOUT
+ * with the context still usable. skip_loads = 1 is a test switch: the TMA
+ * producer issues no loads, so the MMA and epilogue waits run out with no
+ * copy in flight. (0, 0) restores the defaults. */
+int gpair_set_tc_wait(gpair_ctx *ctx, long long budget_cycles, int skip_loads);
 int gpair_last_run_stage_ms(gpair_ctx *ctx, double *stage_ms, int *stage_launches, int max_stages);
 
 /* ---- allocation-free data stage ----
@@ -456,8 +476,9 @@ int gpair_last_run_stage_ms(gpair_ctx *ctx, double *stage_ms, int *stage_launche
  * npow <= nuv; larger sizes return GPAIR_ERR_INVALID without launching.
  * The first call on a device looks up the scratch address for that device
  * (with it current); make that first call before any stream capture. The call
- * is asynchronous on `stream` (a cudaStream_t, NULL = default stream); results
- * are valid once the stream has reached it. All calls share the one scratch
+ * is asynchronous on `stream` (a cudaStream_t of the current device, NULL =
+ * default stream; a stream of another device returns GPAIR_ERR_INVALID);
+ * results are valid once the stream has reached it. All calls share the one scratch
  * array, so calls that overlap on the GPU (other streams, other host threads)
  * race and must be serialised by the caller. An out-of-range triangle
  * reference is not read; the call then writes chi2 = NaN. */

@@ -20,16 +20,21 @@ from typing import Optional
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+# the reference's trunk sources, read in place (the one place this path is set;
+# oracle/Makefile's REF has the same default)
+REFERENCE_TRUNK = os.environ.get("GPAIR_REFERENCE_TRUNK", "/root/reference/gpair1/trunk")
 FP64_LIB = os.path.join(HERE, "lib", "liboracle_fp64.so")
 REF_LIB = os.path.join(HERE, "_ref", "libgpair_ref.so")
+REF_MAIN_LIB = os.path.join(HERE, "_ref", "libgpair_ref_main.so")
 
 _fp64 = None
 _ref = None
+_ref_main = None
 
 
 def build():
     """Build the oracle libraries (reference part only where its sources exist)."""
-    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    subprocess.run(["make", "-s", "-C", HERE, f"REF={REFERENCE_TRUNK}"], check=True)
 
 
 def _p(a):
@@ -141,6 +146,32 @@ def ref_index(oi, minband: float = 0.0, maxband: float = 1e30, target_id: Option
     L.oracle_ref_copy_oi_data(*[_p(out[k]) for k in ("pow", "powerr", "bisamp", "bisamperr", "bisphs", "bisphserr",
                                                      "uv", "uvpnt", "sign")])
     return out
+
+
+def ref_init_data(npow, nbis, pow_, powerr, bisamp, bisamperr, bisphs, bisphserr, uvpnt, do_extrapolation=1):
+    """The reference's own init_data (gpair1/trunk/gpair.c:997-1066, compiled with
+    main renamed into oracle/_ref/libgpair_ref_main.so). Returns data, data_err,
+    phasor (complex64) and the change of its global ndof."""
+    global _ref_main
+    if _ref_main is None:
+        if not os.path.exists(REF_MAIN_LIB):
+            build()
+        if not os.path.exists(REF_MAIN_LIB):
+            raise FileNotFoundError(f"{REF_MAIN_LIB} not built (reference sources unavailable)")
+        L = C.CDLL(REF_MAIN_LIB)
+        vp, i = C.c_void_p, C.c_int
+        L.oracle_ref_init_data.argtypes = [i, i, i, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+        L.oracle_ref_init_data.restype = i
+        _ref_main = L
+    nd = npow + 2 * nbis
+    data = np.zeros(max(nd, 1), np.float32)
+    err = np.zeros(max(nd, 1), np.float32)
+    ph = np.zeros(max(nbis, 1), np.complex64)
+    f32 = [np.ascontiguousarray(x, np.float32) for x in (pow_, powerr, bisamp, bisamperr, bisphs, bisphserr)]
+    uv = np.ascontiguousarray(np.asarray(uvpnt, np.int64).reshape(-1, 3))
+    delta = _ref_main.oracle_ref_init_data(do_extrapolation, npow, nbis, *[_p(x) for x in f32], _p(uv), _p(data),
+                                           _p(err), _p(ph))
+    return data[:nd], err[:nd], ph[:nbis], int(delta)
 
 
 # ----------------------------------------------------------- setup replicas

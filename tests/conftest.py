@@ -8,7 +8,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
-REFERENCE_TRUNK = "/root/reference/gpair1/trunk"
+from oracle.oracle import REFERENCE_TRUNK  # noqa: E402
 
 
 def pytest_configure(config):

@@ -28,7 +28,7 @@ from gpair_b200 import synth  # noqa: E402
 from gpair_b200.oifits import read_oifits  # noqa: E402
 from oracle import oracle as O  # noqa: E402
 
-FIXTURE = "/root/reference/gpair1/trunk/2004contest1.oifits"
+FIXTURE = os.path.join(O.REFERENCE_TRUNK, "2004contest1.oifits")
 KEYS = ["pow", "powerr", "bisamp", "bisamperr", "bisphs", "bisphserr", "uv", "uvpnt", "sign"]
 
 

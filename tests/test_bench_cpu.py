@@ -43,9 +43,58 @@ def test_clock_sampler_without_nvidia_smi():
     assert s.stop()["reasons"] == ["nvidia-smi unavailable"]
 
 
-def test_cpu_sample_problem_keeps_the_data():
+def test_reference_sample_is_one_channel_indexed_by_the_reference():
+    """The CPU sample holds the middle channel of the workload's tables, indexed by
+    the reference's own getoifits.c; this project's indexer gives the same indices."""
+    import os
+
+    import numpy as np
+    import pytest
+
     import gpair_b200 as g
-    p = g.workload_problem("tiny")
-    s = bench.cpu_sample_problem(p, 16)
-    assert s.width == 16 and s.nuv == p.nuv and s.npow == p.npow and s.nbis == p.nbis
-    assert (s.data == p.data).all() and s.model.shape == (16 * 16,)
+    from gpair_b200 import synth
+    from oracle import oracle as O
+
+    if not os.path.exists(O.REF_LIB):
+        pytest.skip("the reference's getoifits.c is not built here")
+    w, oi = synth.make_workload_data("tiny")
+    s = bench.reference_sample("tiny", oi, width=16)
+    _, oifits_mod = bench.data_modules()
+    sub = bench.subset_channels(oi, [s["channel"]], oifits_mod)
+    ix = g.index_oifits(sub)
+    assert s["channel"] == 1 and s["channels"] == 2 and s["width"] == 16
+    assert s["npow"] == ix.npow == oi.vis2[0].vis2data.shape[0]
+    assert s["nbis"] == ix.nbis == oi.t3[0].t3amp.shape[0]
+    assert np.array_equal(s["uv"], ix.uv) and np.array_equal(s["uvpnt"], ix.uvpnt)
+    assert np.array_equal(s["sign"], ix.sign)
+    assert s["model"].shape == (16 * 16,)
+
+
+def test_reference_arm_maps_no_library_of_this_project():
+    """`bench.py --impl reference` in a fresh process: the reference's compiled
+    cpu.c / getoifits.c run, libgpair_b200.so is never mapped."""
+    import json
+    import os
+    import subprocess
+    import sys
+
+    import pytest
+
+    from oracle import oracle as O
+
+    if not os.path.exists(O.REF_LIB):
+        pytest.skip("the reference's cpu.c is not built here")
+    r = subprocess.run([sys.executable, os.path.join(bench.ROOT, "bench.py"), "--impl", "reference", "--workload",
+                        "tiny", "--steps", "1", "--warmup", "0"], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["value"] > 0
+    libs = line["native_libraries"]
+    assert any(x.startswith("oracle/") for x in libs), libs
+    assert not any("libgpair_b200" in x for x in libs), libs
+    assert line["higher_is_better"] is True and line["unit"] == bench.UNIT and line["metric"] == bench.METRIC
+    assert line["cpu_baseline"]["kind"] == "reference"
+    assert line["cpu_baseline"]["cores"] == (os.cpu_count() or 1)
+    assert line["cpu_baseline"]["value"] == line["value"]
+    assert line["e2e"] == {"value": line["value"], "unit": line["unit"], "h2d_bytes_per_step": 0,
+                           "d2h_bytes_per_step": 0}

@@ -83,6 +83,27 @@ def test_device_cg_matches_fp64_cg(rec, prec):
     assert abs(out["trace_J"][-1] - tr["J"][-1]) / abs(tr["J"][-1]) < 1e-3
 
 
+@pytest.mark.parametrize("method", [1, 3])
+@pytest.mark.parametrize("prec", PRECISIONS)
+def test_device_cg_fr_and_hs_match_fp64_cg(rec, prec, method):
+    """Fletcher-Reeves (method 1) and Hestenes-Stiefel+ (method 3) beta rules of
+    gpair1/trunk/gpair.c:733-753: the device trace against the FP64 oracle's CG
+    with the same beta rule and the reference's line search."""
+    p = _problem("tiny", (21, 22, 23))
+    rec.set_problem(p)
+    rec.set_precision(prec)
+    img0 = p.start_image()
+    iters = 8
+    _, tr = O.reconstruct64(p, img0, iters, method=method)
+    rec.set_image(img0)
+    out = rec.cg(iters, method=method, trace=True)
+    n = 4
+    assert np.allclose(out["trace_J"][:n], tr["J"][:n], rtol=1e-5)
+    assert np.allclose(out["trace_step"][:n], tr["step"][:n], rtol=1e-4)
+    assert np.allclose(out["trace_beta"][1:n], tr["beta"][1:n], rtol=1e-3, atol=1e-6)
+    assert abs(out["trace_J"][-1] - tr["J"][-1]) / abs(tr["J"][-1]) < 1e-3
+
+
 def test_device_cg_above_one_megapixel(rec):
     """1100^2 pixels (more than 4096 blocks x 256 threads): the trial-image prep
     and the reductions run several pixels per thread on grids capped at their
@@ -203,6 +224,57 @@ def test_reference_boundary_loop_matches_fp64_cg(prec):
     _, tr = O.reconstruct64(p, p.start_image(), iters)
     assert np.allclose(Js[:3], tr["J"][:3], rtol=1e-4)
     assert Js[-1] < Js[0]
+
+
+def test_tensor_kernel_wait_timeout_is_reported_and_context_recovers(rec):
+    """The tcgen05 kernels' bounded waits run out (the producer issues no TMA
+    loads, so nothing ever fills a stage): the call returns GPAIR_ERR_TIMEOUT
+    instead of hanging, the kernel has freed its tensor memory (the next launch
+    allocates it again), and the same context then matches the FP64 oracle."""
+    p = _problem("tiny", (5, 6, 7))
+    rec.set_problem(p)
+    rec.set_precision(g.PREC_SPLIT16)
+    img = _rand_image(p, 3)
+    rec.set_image(img)
+    L = g.lib()
+    assert L.gpair_set_tc_wait(rec.h, -1, 0) != 0
+    assert L.gpair_set_tc_wait(rec.h, 20_000_000, 1) == 0  # about 10 ms per wait
+    try:
+        with pytest.raises(g.GpairError, match=r"\(-5\)"):
+            rec.criterion()
+        with pytest.raises(g.GpairError, match=r"\(-5\)"):
+            rec.gradient()
+    finally:
+        assert L.gpair_set_tc_wait(rec.h, 0, 0) == 0
+    e = O.evaluate64(p, img)
+    for _ in range(2):
+        rec.set_image(img)
+        chi2, _ = rec.criterion()
+        rec.gradient()
+        assert abs(chi2 - e["chi2"]) / e["chi2"] <= 1e-5
+        assert _rel(rec.data_gradient(), e["data_grad"]) <= 1e-5
+
+
+def test_boundary_zoom_reports_its_trial_cap():
+    """gpu_linesearch_zoom stops at its trial cap and says so: with the default cap
+    the reference loop's zooms all end on their own; with a cap of one trial the
+    zooms that need more stop there, are counted, and leave a message in the global
+    context's last error. The reference itself has no cap (gpair1/trunk/gpu.c:1947-2065)."""
+    L = g.lib()
+    p = _problem("tiny", (21, 22, 23))
+    L.gpair_zoom_cap_hits_reset()
+    Js, _ = _ref_boundary_run(p, 5, p.alpha)
+    assert L.gpair_zoom_cap_hits() == 0
+    try:
+        assert L.gpair_set_zoom_trial_cap(1) == 0
+        assert L.gpair_set_zoom_trial_cap(-1) != 0
+        L.gpair_zoom_cap_hits_reset()
+        Js1, _ = _ref_boundary_run(p, 5, p.alpha)
+        hits = L.gpair_zoom_cap_hits()
+    finally:
+        L.gpair_set_zoom_trial_cap(0)
+    assert hits >= 1
+    assert np.all(np.isfinite(Js1))
 
 
 @pytest.mark.parametrize("prec", PRECISIONS)
@@ -375,8 +447,9 @@ def test_stop_flag_ends_a_racing_run(rec):
 
 
 def test_cg_run_many_equals_separate_runs():
-    """gpair_cg_run_many: concurrent runs on several contexts give the results of
-    separate runs (deterministic kernels, no shared state between contexts)."""
+    """Consistency check (library against itself; single runs are oracle-pinned by
+    the CG tests above): gpair_cg_run_many's concurrent runs on several contexts
+    give the results of separate runs (deterministic kernels, no shared state)."""
     from gpair_b200.instances import instance
     ps = [instance(20_000_000 + k) for k in range(3)]
     recs = [g.Reconstructor(0) for _ in ps]
@@ -425,8 +498,9 @@ def test_l2_regularizer_matches_fp64(rec, prec):
 
 @pytest.mark.parametrize("prec", PRECISIONS)
 def test_update_pixel_matches_full_recomputation(rec, prec):
-    """gpair_update_pixel: V, chi2 and S after single-pixel changes agree with a
-    full evaluation of the changed image (FP32 path in a second context)."""
+    """Consistency check (library against itself; the oracle pin is
+    test_update_pixel_matches_fp64_oracle): V, chi2 and S after single-pixel
+    changes agree with a full evaluation of the changed image in a second context."""
     p = _problem("small", (1, 2, 3))
     rng = np.random.default_rng(11)
     img = _rand_image(p, 7)
@@ -450,6 +524,32 @@ def test_update_pixel_matches_full_recomputation(rec, prec):
         rec.gradient()
         full.gradient()
         assert _rel(rec.data_gradient(), full.data_gradient().astype(np.float64)) <= 1e-5
+
+
+@pytest.mark.parametrize("prec", PRECISIONS)
+def test_update_pixel_matches_fp64_oracle(rec, prec):
+    """gpair_update_pixel against the FP64 oracle: after each single-pixel change,
+    chi2, the visibilities and S of the changed image as the oracle evaluates it
+    from scratch (gpair1/trunk/cpu.c:449-475 restated in FP64), and the data
+    gradient after the last change."""
+    p = _problem("small", (1, 2, 3))
+    rng = np.random.default_rng(12)
+    img = _rand_image(p, 8)
+    rec.set_problem(p)
+    rec.set_precision(prec)
+    rec.set_image(img)
+    rec.criterion()
+    for step in range(5):
+        x, y = int(rng.integers(0, p.width)), int(rng.integers(0, p.width))
+        v = float(img[y * p.width + x] * (25.0 if step == 1 else rng.uniform(0.2, 3.0)))
+        chi2_u, S_u = rec.update_pixel(x, y, v)
+        img[y * p.width + x] = np.float32(v)
+        e = O.evaluate64(p, img, want_grad=(step == 4))
+        assert abs(chi2_u - e["chi2"]) <= 1e-5 * e["chi2"], (step, chi2_u, e["chi2"])
+        assert abs(S_u - e["entropy"]) <= 1e-9 * max(1.0, abs(e["entropy"]))
+        assert np.abs(rec.visibilities() - e["visi"]).max() <= 1e-5
+    rec.gradient()
+    assert _rel(rec.data_gradient(), e["data_grad"]) <= 1e-5
 
 
 def test_stage_timing_hooks_return_positive_times(rec):
@@ -632,8 +732,10 @@ def test_alternating_line_searches_reuse_their_graphs(rec):
 
 @pytest.mark.parametrize("ls", [0, 1])
 def test_batch_graph_equals_separate_runs(ls):
-    """gpair_batch_*: every context's CG loop in one graph, one launch; the results
-    are the separate runs' bit for bit, twice in a row (the graph is reused)."""
+    """Consistency check (library against itself; single runs are oracle-pinned by
+    the CG tests above): gpair_batch_*, every context's CG loop in one graph, one
+    launch; the results are the separate runs' bit for bit, twice in a row (the
+    graph is reused)."""
     from gpair_b200.instances import instance
     ps = [instance(20_000_000 + k) for k in range(4)]
     recs = [g.Reconstructor(0) for _ in ps]

@@ -15,7 +15,7 @@ from gpair_b200 import synth
 from oracle import oracle as O
 
 pytestmark = pytest.mark.skipif(not O.ref_available() and not __import__("os").path.exists(
-    "/root/reference/gpair1/trunk/cpu.c"), reason="reference build unavailable")
+    __import__("os").path.join(O.REFERENCE_TRUNK, "cpu.c")), reason="reference build unavailable")
 
 
 @pytest.fixture(scope="module")
@@ -76,6 +76,34 @@ def test_init_data_replica_bit_exact(small):
     d2, e2, p2, n2 = O.init_data(ix.npow, ix.nbis, ix.pow, ix.powerr, ix.bisamp, bisamperr, ix.bisphs, ix.bisphserr,
                                  ix.uvpnt, 1)
     assert n1 == n2
+    assert np.array_equal(d1.view(np.uint32), d2.view(np.uint32))
+    assert np.array_equal(e1.view(np.uint32), e2.view(np.uint32))
+    assert np.array_equal(p1.view(np.uint32), p2.view(np.uint32))
+
+
+@pytest.mark.parametrize("do_extrapolation", [1, 0])
+def test_init_data_bit_exact_with_reference(small, do_extrapolation):
+    """The product's gpair_init_data against the reference's own init_data
+    (gpair1/trunk/gpair.c:997-1066, compiled from its source): data packing,
+    inverse errors, phasors and the ndof change, including missing triple
+    amplitudes (extrapolated from V2), errors above 1e3, and triangles whose uv
+    points carry no V2 point (no extrapolation: amplitude 1, error 1e99)."""
+    if not __import__("os").path.exists(O.REF_MAIN_LIB):
+        O.build()
+    if not __import__("os").path.exists(O.REF_MAIN_LIB):
+        pytest.skip("the reference's gpair.c is not built here")
+    w, oi = synth.make_workload_data("small", 11, 12, 13)
+    ix = g.index_oifits(oi)
+    ix.bisamperr = ix.bisamperr.copy()
+    ix.bisamperr[::7] = -1.0
+    ix.bisamperr[::11] = 5e3
+    ix.uvpnt = ix.uvpnt.copy()
+    ix.uvpnt[3::13, 1] = ix.npow  # a uv point beyond the V2 points
+    ix.uvpnt[5::17, 2] = ix.npow + 1
+    d1, e1, p1, n1 = g.init_data(ix, do_extrapolation)
+    d2, e2, p2, n2 = O.ref_init_data(ix.npow, ix.nbis, ix.pow, ix.powerr, ix.bisamp, ix.bisamperr, ix.bisphs,
+                                     ix.bisphserr, ix.uvpnt, do_extrapolation)
+    assert n1 == n2 and (n1 < 0) == bool(do_extrapolation)
     assert np.array_equal(d1.view(np.uint32), d2.view(np.uint32))
     assert np.array_equal(e1.view(np.uint32), e2.view(np.uint32))
     assert np.array_equal(p1.view(np.uint32), p2.view(np.uint32))

@@ -74,32 +74,3 @@ def test_reference_arm_other_ranks_exit_without_work(capsys):
 
     bench.run_reference(A, rank=1)
     assert capsys.readouterr().out == ""
-
-
-def test_reference_arm_prints_its_line(capsys):
-    """Rank 0 times the reference's own compiled cpu.c on every host core (spawned
-    workers, no GPU) and prints the contract's JSON line."""
-    import json
-    import os
-
-    import bench
-    from oracle import oracle as O
-
-    if not os.path.exists(O.REF_LIB):
-        pytest.skip("the reference's cpu.c is not built here")
-
-    class A:
-        workload = "tiny"
-        warmup = 0
-        steps = 1
-        gpus = 1
-
-    bench.run_reference(A, rank=0)
-    line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
-    assert line["impl"] == "reference" and line["value"] > 0 and line["higher_is_better"] is True
-    assert line["unit"] == bench.UNIT and line["metric"] == bench.METRIC
-    assert line["cpu_baseline"]["kind"] == "reference"
-    assert line["cpu_baseline"]["cores"] == (os.cpu_count() or 1)
-    assert line["cpu_baseline"]["value"] == line["value"]
-    assert line["e2e"] == {"value": line["value"], "unit": line["unit"], "h2d_bytes_per_step": 0,
-                           "d2h_bytes_per_step": 0}

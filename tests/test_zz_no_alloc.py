@@ -29,6 +29,57 @@ def _entry():
     return f
 
 
+def _device_inputs(p, visi):
+    import torch
+
+    dev = torch.device("cuda", 0)
+    uv4 = np.zeros((p.nbis, 4), np.int64)
+    uv4[:, :3] = p.uvpnt
+    sg4 = np.zeros((p.nbis, 4), np.int16)
+    sg4[:, :3] = p.sign
+    return {"visi": torch.from_numpy(visi.view(np.float32).copy()).to(dev),
+            "data": torch.from_numpy(p.data.astype(np.float32)).to(dev),
+            "err": torch.from_numpy(p.data_err.astype(np.float32)).to(dev),
+            "ph": torch.from_numpy(p.phasor.astype(np.complex64).view(np.float32).copy()).to(dev),
+            "uv": torch.from_numpy(uv4).to(dev), "sg": torch.from_numpy(sg4).to(dev)}
+
+
+def _call(f, p, t):
+    import torch
+
+    dev = torch.device("cuda", 0)
+    nd = p.npow + 2 * p.nbis
+    t_mock = torch.full((nd,), float("nan"), dtype=torch.float32, device=dev)
+    t_chi2 = torch.full((1,), float("nan"), dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    rc = f(t["visi"].data_ptr(), p.nuv, p.npow, p.nbis, t["data"].data_ptr(), t["err"].data_ptr(),
+           t["ph"].data_ptr(), t["uv"].data_ptr(), t["sg"].data_ptr(), t_mock.data_ptr(), t_chi2.data_ptr(),
+           stream.cuda_stream)
+    stream.synchronize()
+    return rc, t_mock.cpu().numpy(), float(t_chi2.cpu().numpy()[0])
+
+
+def test_noalloc_flags_an_out_of_range_triangle_then_recovers():
+    """A triangle that names a uv point >= nuv is not read and makes chi2 NaN; the
+    next clean call starts from a cleared error word and returns a finite chi2."""
+    w, oi = synth.make_workload_data("tiny", 1, 2, 3)
+    p = g.problem_from_oifits(oi, w.image_width, w.pixellation_mas, w.alpha)
+    with g.Reconstructor(0) as rec:
+        rec.set_problem(p)
+        rec.set_image(p.start_image())
+        chi2_ref, _ = rec.criterion()
+        visi = rec.visibilities()
+    f = _entry()
+    t = _device_inputs(p, visi)
+    good = t["uv"].clone()
+    t["uv"][p.nbis // 2, 1] = p.nuv  # one past the end
+    rc, _, chi2 = _call(f, p, t)
+    assert rc == 0 and np.isnan(chi2)
+    t["uv"] = good
+    rc, _, chi2 = _call(f, p, t)
+    assert rc == 0 and np.isfinite(chi2) and abs(chi2 - chi2_ref) / chi2_ref <= 1e-5
+
+
 @pytest.mark.parametrize("name", ["tiny", "small"])
 def test_noalloc_matches_existing_entry_point_twice(name):
     import torch
