@@ -26,7 +26,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libgpair_b200.so")
 
 GPAIR_OK = 0
-PREC_FP32, PREC_SPLIT16, PREC_TF32 = 0, 1, 2
+PREC_FP32, PREC_SPLIT16, PREC_TF32, PREC_TF32X3 = 0, 1, 2, 3
 REG_GULL_SKILLING, REG_L2 = 0, 1
 IMG_CURR, IMG_TEMP = 0, 1
 
@@ -552,6 +552,8 @@ class Reconstructor:
         prm.iterations = iterations
         prm.resume = 1 if resume else 0
         prm.alpha = self.problem.alpha if alpha is None else alpha
+        if method == 4:
+            prm.wolfe2 = 0.9  # quasi-Newton curvature constant (the reference's 0.1 is for CG)
         for k, v in kw.items():
             setattr(prm, k, v)
         res = CgResult()

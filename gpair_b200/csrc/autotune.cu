@@ -154,7 +154,7 @@ extern "C" int gpair_autotune(gpair_ctx *c, int flags, int reps, gpair_tune_resu
             std::vector<int> ks = {k0};
             if (flags & GPAIR_TUNE_SPLITS) {
                 if (k0 / 2 >= 1) ks.push_back(k0 / 2);
-                if (2 * k0 <= 64) ks.push_back(2 * k0);
+                if (2 * k0 <= gp_tc_kb_cap(c)) ks.push_back(2 * k0);
             }
             for (int k : ks) cand.push_back({prec, k, simt0, 0.0});
         }

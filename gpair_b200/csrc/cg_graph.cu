@@ -39,6 +39,7 @@ struct CgGraph {
     cudaGraphExec_t exec;
     int precision;
     int ls_mode;
+    int lbfgs;  // direction by the projected L-BFGS passes (method 4) instead of the CG update
     double *trace;
     int trace_cap;
     int n_pre, n_crit, n_grad, n_post;  // kernel launches per sequence
@@ -61,7 +62,7 @@ static int emit(gpair_ctx *c, CgGraph *G, int seq, cudaGraphConditionalHandle hi
         c->fuse_ctrl = CTRL_BEGIN;
         if ((rc = gp_eval_gradient(c, GPAIR_IMG_CURR, -1.f))) break;  // alpha from the device state
         c->fuse_ctrl = CTRL_AFTER_DIR;
-        rc = gp_descent_dir(c, 1, 0.0);
+        rc = G->lbfgs ? gp_lbfgs_direction(c) : gp_descent_dir(c, 1, 0.0);
         break;
     case SEQ_CRIT:
         if (G->ls_mode == GPAIR_LS_BATCH) {
@@ -155,6 +156,10 @@ static int add_loop(gpair_ctx *c, CgGraph *G, cudaGraph_t parent)
         int rc = gp_batch_alloc(c);
         if (rc) return rc;
     }
+    if (G->lbfgs) {
+        int rc = gp_lbfgs_alloc(c);  // no allocation inside a capture
+        if (rc) return rc;
+    }
     int rc = GPAIR_OK;
     cudaGraphConditionalHandle h_iter, h_ls, h_grad;
     GP_CUDA(c, cudaGraphConditionalHandleCreate(&h_iter, parent, 1, cudaGraphCondAssignDefault));
@@ -207,6 +212,7 @@ static int build(gpair_ctx *c, int trace_cap, int ls_mode)
     c->cg_graph[ls_mode] = G;
     G->precision = c->precision;
     G->ls_mode = ls_mode;
+    G->lbfgs = c->cg_method == 4;
     G->trace_cap = trace_cap;
     GP_CUDA(c, cudaMalloc(&G->trace, sizeof(double) * 5 * (size_t)trace_cap));
     GP_CUDA(c, cudaGraphCreate(&G->g, 0));
@@ -314,7 +320,8 @@ int gp_cg_graph_run(gpair_ctx *c, int iterations, int want_trace, int ls_mode, l
     c->cg_graph_mode = ls_mode;
     CgGraph *G = (CgGraph *)c->cg_graph[ls_mode];
     int cap = iterations > 4096 ? iterations : 4096;
-    if (!G || G->precision != c->precision || (want_trace && G->trace_cap < iterations)) {
+    if (!G || G->precision != c->precision || G->lbfgs != (c->cg_method == 4) ||
+        (want_trace && G->trace_cap < iterations)) {
         int rc = build(c, cap, ls_mode);
         if (rc) return rc;
         G = (CgGraph *)c->cg_graph[ls_mode];

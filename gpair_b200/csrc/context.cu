@@ -65,6 +65,7 @@ static void free_images(gpair_ctx *c)
     FREE_DEV(c->data_grad); FREE_DEV(c->entropy_grad); FREE_DEV(c->full_grad_new);
     FREE_DEV(c->full_grad); FREE_DEV(c->grad_temp); FREE_DEV(c->descent_dir);
     gp_batch_free(c);
+    gp_lbfgs_free(c);
     c->N = 0;
     c->npix = 0;
     c->have_image = 0;
@@ -206,7 +207,7 @@ int gp_set_problem_core(gpair_ctx *c, int N, float pix, int nuv, const gpair_uv 
     c->splits = c->splits_simt;
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
-    int max_splits = gp_tc_splits(N, nuv ? nuv : 1, nsm, nullptr);
+    int max_splits = gp_tc_max_splits(N, nuv ? nuv : 1, nsm);
     if (max_splits < c->splits_simt) max_splits = c->splits_simt;
     GP_CUDA(c, cudaMalloc(&c->data, nd * sizeof(float)));
     GP_CUDA(c, cudaMalloc(&c->data_err, nd * sizeof(float)));
@@ -279,7 +280,7 @@ extern "C" int gpair_set_problem(gpair_ctx *c, int N, float pix, int nuv, const 
 
 extern "C" int gpair_set_precision(gpair_ctx *c, int mode)
 {
-    if (!c || mode < GPAIR_PREC_FP32 || mode > GPAIR_PREC_TF32) return GPAIR_ERR_INVALID;
+    if (!c || mode < GPAIR_PREC_FP32 || mode > GPAIR_PREC_TF32X3) return GPAIR_ERR_INVALID;
     int old = c->precision;
     c->precision = mode;
     if (mode != GPAIR_PREC_FP32 && c->have_problem) {
@@ -611,7 +612,13 @@ extern "C" int gpair_cg_checkpoint_load(gpair_ctx *c, const void *buf, size_t by
     // every copy on the context's stream, after the work already queued there;
     // the caller's buffer may be pageable, so wait until the last copy landed
     GP_CUDA(c, cudaStreamSynchronize(c->stream));
-    GP_CUDA(c, cudaMemcpyAsync(&c->sc->cg, p, sizeof(CgState), cudaMemcpyHostToDevice, c->stream));
+    // the projected L-BFGS pairs are not part of a checkpoint: a restored run
+    // starts its history afresh (its first direction is the projected -g)
+    memcpy(&c->sc_host->cg, p, sizeof(CgState));
+    c->sc_host->cg.lb_count = 0;
+    c->sc_host->cg.lb_xvalid = 0;
+    c->sc_host->cg.lb_drop = 0;
+    GP_CUDA(c, cudaMemcpyAsync(&c->sc->cg, &c->sc_host->cg, sizeof(CgState), cudaMemcpyHostToDevice, c->stream));
     p += sizeof(CgState);
     for (int i = 0; i < kCkArrays; i++) {
         GP_CUDA(c, cudaMemcpyAsync(ck_array(c, i), p, sizeof(float) * c->npix, cudaMemcpyHostToDevice, c->stream));
@@ -665,7 +672,7 @@ struct CgRun {
 static int cg_validate(gpair_ctx *c, const gpair_cg_params *p)
 {
     if (!c || !p || !c->have_problem) return GPAIR_ERR_STATE;
-    if (p->iterations < 0 || p->method < 0 || p->method > 3) return GPAIR_ERR_INVALID;
+    if (p->iterations < 0 || p->method < 0 || p->method > 4) return GPAIR_ERR_INVALID;
     if (p->line_search != GPAIR_LS_WOLFE && p->line_search != GPAIR_LS_BATCH) return GPAIR_ERR_INVALID;
     if (!(p->target_J >= 0.0)) return GPAIR_ERR_INVALID;
     return GPAIR_OK;
@@ -682,6 +689,8 @@ static int cg_prepare(gpair_ctx *c, const gpair_cg_params *p, int want_trace, Cg
     CgState h;
     memset(&h, 0, sizeof(h));
     h.method = p->method;
+    c->cg_method = p->method;
+    if (p->method == 4 && (rc = gp_lbfgs_alloc(c))) return rc;
     h.max_zoom = p->max_zoom > 0 ? p->max_zoom : 200;
     h.max_bracket = p->max_bracket > 0 ? p->max_bracket : 100;
     h.alpha = p->alpha;
@@ -739,7 +748,7 @@ static int cg_host_loop(gpair_ctx *c, const gpair_cg_params *p, double *tJ, doub
         c->fuse_ctrl = CTRL_BEGIN;
         if ((rc = gp_eval_gradient(c, GPAIR_IMG_CURR, -1.f))) { status = rc; break; }
         c->fuse_ctrl = CTRL_AFTER_DIR;
-        if ((rc = gp_descent_dir(c, 1, 0.0))) { status = rc; break; }
+        if ((rc = p->method == 4 ? gp_lbfgs_direction(c) : gp_descent_dir(c, 1, 0.0))) { status = rc; break; }
         int action = CG_EVAL_CRIT, trials = 0;
         if ((rc = read_action(c, &action))) { status = rc; break; }
         while (action != CG_DONE) {
@@ -920,7 +929,8 @@ extern "C" int gpair_batch_create(gpair_batch **out, gpair_ctx **ctx, int n, int
 extern "C" int gpair_batch_run(gpair_batch *b, const gpair_cg_params *p, gpair_cg_result *res)
 {
     if (!b || !p) return GPAIR_ERR_INVALID;
-    if (p->host_loop || p->line_search != b->ls_mode) return GPAIR_ERR_INVALID;
+    // the batch graph holds the CG direction update; projected L-BFGS runs per context
+    if (p->host_loop || p->line_search != b->ls_mode || p->method == 4) return GPAIR_ERR_INVALID;
     for (int i = 0; i < b->n; i++) {
         int rc = cg_validate(b->ctx[i], p);
         if (rc) return rc;

@@ -35,6 +35,8 @@ enum {
     RED_GRAD = 3,  // gradient finalize dots
     RED_DIR = 4,   // descent direction dot
     RED_DOT = 5,   // generic scalar product
+    RED_LBP = 6,   // projected L-BFGS: candidate pair dots
+    RED_LBD = 7,   // projected L-BFGS: dots of the projected gradient
     RED_NSLOTS = 8
 };
 
@@ -49,6 +51,13 @@ enum { CG_PH_BRACKET = 0, CG_PH_ZOOM = 1 };
 #define GP_LS_MAX_ROUNDS 6      // grid shifts + refine per iteration
 #define GP_LS_MAX_PTS (GP_LS_MAX_ROUNDS * GP_NTR)
 enum { BR_GRID = 0, BR_REFINE = 1 };
+
+// projected L-BFGS direction (method 4): pairs kept, and the dot products the
+// pair kernel (3 of the candidate, 2 per stored pair) and the direction-dots
+// kernel (q.q, 2 per stored pair) reduce
+#define GP_LB_PAIRS 4
+#define GP_LB_NPD (3 + 2 * GP_LB_PAIRS)
+#define GP_LB_NQD (1 + 2 * GP_LB_PAIRS)
 
 struct CgState {
     // parameters
@@ -79,6 +88,17 @@ struct CgState {
     double s_c;
     double ts[GP_NTR];                 // steps of the batch being evaluated
     double pts_s[GP_LS_MAX_PTS], pts_J[GP_LS_MAX_PTS];  // points evaluated this iteration
+    // projected L-BFGS (method 4): logical pairs 0 (oldest) .. lb_count - 1
+    // live in the buffers lb_slot[0 .. lb_count - 1] of the GP_LB_PAIRS + 1
+    // image-sized S and Y buffers; lb_slot[GP_LB_PAIRS] is the free buffer the
+    // next candidate pair is written to
+    int lb_count, lb_xvalid, lb_drop;
+    int lb_slot[GP_LB_PAIRS + 1];
+    double lb_sy[GP_LB_PAIRS][GP_LB_PAIRS];  // s_i . y_j (upper triangle used)
+    double lb_yy[GP_LB_PAIRS][GP_LB_PAIRS];  // y_i . y_j
+    double lb_gamma;                          // H0 = gamma I, from the newest accepted pair
+    // direction d = -(lb_cq q + sum_i lb_cs[i] s_i + sum_i lb_cy[i] y_i), q = projected gradient
+    double lb_cq, lb_cs[GP_LB_PAIRS], lb_cy[GP_LB_PAIRS];
 };
 
 struct DevScalars {
@@ -105,6 +125,8 @@ struct DevScalars {
     int reg_kind;    // GPAIR_REG_GULL_SKILLING / GPAIR_REG_L2
     // single-pixel update: old total flux and flux change of the last update
     double upd_flux_old, upd_delta;
+    // projected L-BFGS reductions
+    double lb_pdots[GP_LB_NPD], lb_qdots[GP_LB_NQD];
     CgState cg;
 };
 
@@ -188,6 +210,9 @@ struct gpair_ctx {
     // batched line-search trials: GP_NTR trial images, partial visibilities
     // vpart_b[GP_NTR * epp][K] (epp row-tile entries per trial), reduction partials
     float *image_trials;
+    // projected L-BFGS (method 4): GP_LB_PAIRS + 1 image-sized buffers each of
+    // steps s and gradient changes y, and the image the last direction started from
+    float *lb_s, *lb_y, *lb_xold;
     float2 *vpart_b;
     double *partials_b;
     int batch_wave[2];  // blocks per trial that fill one wave: [0] trial prep, [1] trial chi2
@@ -197,6 +222,7 @@ struct gpair_ctx {
     // alternating modes does not re-capture; cg_graph_mode = the mode last run
     void *cg_graph[2];
     int cg_graph_mode;
+    int cg_method;  // direction method of the current run (4: projected L-BFGS passes in the graph)
     // controller fused into the next reduction kernel launched (-1: none)
     int fuse_ctrl, fuse_handles;
     unsigned long long fh_iter, fh_ls, fh_grad;
@@ -271,7 +297,7 @@ int gp_sync_scalars(gpair_ctx *c);
 
 enum { GRAD_FUSED = 0, GRAD_DATA_ONLY = 1 };
 enum { CTRL_BEGIN = 0, CTRL_AFTER_DIR = 1, CTRL_AFTER_CRIT = 2, CTRL_AFTER_GRAD = 3, CTRL_INIT = 4, CTRL_RESUME = 5,
-       CTRL_END = 6, CTRL_AFTER_BATCH = 7 };
+       CTRL_END = 6, CTRL_AFTER_BATCH = 7, CTRL_LB_PAIR = 8, CTRL_LB_COEF = 9 };
 
 // batched line-search trials (kernels_core.cu / umma_dft.cu)
 int gp_adjoint_image(gpair_ctx *c, const float2 *cw_host, float *out_host);
@@ -281,7 +307,7 @@ void gp_batch_free(gpair_ctx *c);
 int gp_eval_batch(gpair_ctx *c);
 int gp_eval_batch_timed(gpair_ctx *c, cudaEvent_t *ev);
 int gp_tc_batch_prepare(gpair_ctx *c, int *epp);
-int gp_trials_prep_launch(gpair_ctx *c, void *hi, void *lo, int Lpad, int Kx_pad, int tw_log2);
+int gp_trials_prep_launch(gpair_ctx *c, void *hi, void *lo, int Lpad, int Kx_pad, int tw_log2, int tf32);
 int gp_tc_trials_prep_split(gpair_ctx *c, double *partials);
 int gp_tc_forward_batch_gemm(gpair_ctx *c);
 
@@ -293,7 +319,12 @@ int gp_tc_split(gpair_ctx *c, int which);
 int gp_tc_build_w(gpair_ctx *c);
 int gp_tc_adjoint_gemm(gpair_ctx *c);
 int gp_tc_prep_split_trial(gpair_ctx *c);
-int gp_tc_splits(int N, int nuv, int nsm, int *kb_per_out);
+int gp_tc_splits(int N, int nuv, int nsm, int bk, int *kb_per_out);
+int gp_lbfgs_alloc(gpair_ctx *c);
+void gp_lbfgs_free(gpair_ctx *c);
+int gp_lbfgs_direction(gpair_ctx *c);
+int gp_tc_max_splits(int N, int nuv, int nsm);
+int gp_tc_kb_cap(gpair_ctx *c);
 int gp_tc_adjoint(gpair_ctx *c, int which);
 void gp_tc_free(gpair_ctx *c);
 int gp_tc_kb_per(gpair_ctx *c);

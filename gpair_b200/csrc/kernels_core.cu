@@ -34,6 +34,7 @@
 #define RPMAS_D ((3.14159265358979323 / 180.0) / 3600000.0)
 
 #include "reduce.cuh"
+#include "umma.cuh"
 
 __device__ void cg_control(DevScalars *__restrict__ sc, int what);
 __device__ void cg_set_handles(DevScalars *__restrict__ sc, int what, cudaGraphConditionalHandle h_iter,
@@ -808,6 +809,233 @@ int gp_descent_dir(gpair_ctx *c, int beta_from_state, double beta_host)
     return GPAIR_OK;
 }
 
+// ------------------------------------------------ projected L-BFGS (method 4)
+//
+// No counterpart in the reference (its methods are the CG beta rules of
+// gpair1/trunk/gpair.c:733-753). Pixels on the positivity bound whose gradient
+// points outward are held fixed (q = g elsewhere, 0 there; the direction is 0
+// there too). The direction is the compact form of the inverse BFGS matrix
+// (Byrd, Nocedal and Schnabel, 1994) over the newest GP_LB_PAIRS pairs
+// s = x_new - x_old (the step taken, after the clamp), y = g_new - g_old:
+//   d = -(gamma q + S^T t - gamma Y^T R^-1 u),  u = S q,
+//   t = R^-T ((D + gamma Y Y^T) R^-1 u - gamma Y q),
+// R = upper triangle of S Y^T, D its diagonal, gamma = s.y / y.y of the newest
+// pair. The device needs three passes per iteration: the candidate pair and
+// its dots with the stored pairs, the 2m + 1 dots of q, and one combination
+// pass; the m x m algebra runs in the controller in FP64.
+
+__device__ __forceinline__ bool lb_fixed(float I, float g, double minvalue)
+{
+    return (double)I <= minvalue * 1.000001 && g > 0.f;
+}
+
+// Candidate pair (s, y) of the last step into the free buffer, with its dots
+// s.y, y.y, s.s and s_i.y, y_i.y against the stored pairs i (logical order).
+// Without a valid previous image (first iteration) it writes and sums nothing.
+__global__ void __launch_bounds__(GP_THREADS) k_lbfgs_pair(const float *__restrict__ img,
+                                                           const float *__restrict__ xold,
+                                                           const float *__restrict__ gnew,
+                                                           const float *__restrict__ gold, float *__restrict__ S,
+                                                           float *__restrict__ Y, int n, double *__restrict__ partials,
+                                                           DevScalars *__restrict__ sc, FusedCtrl fc)
+{
+    __shared__ double smem[GP_LB_NPD * 32];
+    const CgState &cs = sc->cg;
+    const int active = cs.lb_xvalid;
+    const int m = cs.lb_count;
+    float *sn = S + (size_t)cs.lb_slot[GP_LB_PAIRS] * n, *yn = Y + (size_t)cs.lb_slot[GP_LB_PAIRS] * n;
+    const float *si[GP_LB_PAIRS], *yi[GP_LB_PAIRS];
+#pragma unroll
+    for (int i = 0; i < GP_LB_PAIRS; i++) {
+        si[i] = S + (size_t)cs.lb_slot[i] * n;
+        yi[i] = Y + (size_t)cs.lb_slot[i] * n;
+    }
+    double acc[GP_LB_NPD];
+#pragma unroll
+    for (int k = 0; k < GP_LB_NPD; k++) acc[k] = 0.0;
+    if (active) {
+        for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+            const float s = img[p] - xold[p], y = gnew[p] - gold[p];
+            sn[p] = s;
+            yn[p] = y;
+            const double sd = s, yd = y;
+            acc[0] += sd * yd;
+            acc[1] += yd * yd;
+            acc[2] += sd * sd;
+#pragma unroll
+            for (int i = 0; i < GP_LB_PAIRS; i++) {
+                if (i < m) {
+                    acc[3 + i] += (double)si[i][p] * yd;
+                    acc[3 + GP_LB_PAIRS + i] += (double)yi[i][p] * yd;
+                }
+            }
+        }
+    }
+    block_sum<GP_LB_NPD>(acc, smem);
+    if (threadIdx.x == 0)
+        for (int k = 0; k < GP_LB_NPD; k++) partials[(size_t)blockIdx.x * GP_LB_NPD + k] = acc[k];
+    if (last_block(&sc->counter[RED_LBP])) {
+        double o[GP_LB_NPD];
+        finish_sum<GP_LB_NPD>(partials, gridDim.x, o, smem);
+        if (threadIdx.x == 0) {
+            for (int k = 0; k < GP_LB_NPD; k++) sc->lb_pdots[k] = o[k];
+            sc->counter[RED_LBP] = 0;
+            run_fused_ctrl(sc, fc);
+        }
+    }
+}
+
+// q = projected gradient; q.q, s_i.q, y_i.q over the stored pairs
+__global__ void __launch_bounds__(GP_THREADS) k_lbfgs_dots(const float *__restrict__ img, const float *__restrict__ g,
+                                                           const float *__restrict__ S, const float *__restrict__ Y,
+                                                           int n, double *__restrict__ partials,
+                                                           DevScalars *__restrict__ sc, FusedCtrl fc)
+{
+    __shared__ double smem[GP_LB_NQD * 32];
+    const CgState &cs = sc->cg;
+    const int m = cs.lb_count;
+    const double minvalue = cs.minvalue;
+    const float *si[GP_LB_PAIRS], *yi[GP_LB_PAIRS];
+#pragma unroll
+    for (int i = 0; i < GP_LB_PAIRS; i++) {
+        si[i] = S + (size_t)cs.lb_slot[i] * n;
+        yi[i] = Y + (size_t)cs.lb_slot[i] * n;
+    }
+    double acc[GP_LB_NQD];
+#pragma unroll
+    for (int k = 0; k < GP_LB_NQD; k++) acc[k] = 0.0;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        const float gp = g[p];
+        if (lb_fixed(img[p], gp, minvalue)) continue;
+        const double q = gp;
+        acc[0] += q * q;
+#pragma unroll
+        for (int i = 0; i < GP_LB_PAIRS; i++) {
+            if (i < m) {
+                acc[1 + i] += (double)si[i][p] * q;
+                acc[1 + GP_LB_PAIRS + i] += (double)yi[i][p] * q;
+            }
+        }
+    }
+    block_sum<GP_LB_NQD>(acc, smem);
+    if (threadIdx.x == 0)
+        for (int k = 0; k < GP_LB_NQD; k++) partials[(size_t)blockIdx.x * GP_LB_NQD + k] = acc[k];
+    if (last_block(&sc->counter[RED_LBD])) {
+        double o[GP_LB_NQD];
+        finish_sum<GP_LB_NQD>(partials, gridDim.x, o, smem);
+        if (threadIdx.x == 0) {
+            for (int k = 0; k < GP_LB_NQD; k++) sc->lb_qdots[k] = o[k];
+            if (!isfinite(o[0])) sc->nonfinite |= 4u;
+            sc->counter[RED_LBD] = 0;
+            run_fused_ctrl(sc, fc);
+        }
+    }
+}
+
+// d = -(cq q + sum cs_i s_i + sum cy_i y_i) on free pixels, 0 on fixed ones;
+// x_old = image; d.g and max |d|
+__global__ void __launch_bounds__(GP_THREADS) k_lbfgs_combine(const float *__restrict__ img,
+                                                              const float *__restrict__ g,
+                                                              const float *__restrict__ S,
+                                                              const float *__restrict__ Y, float *__restrict__ d,
+                                                              float *__restrict__ xold, int n,
+                                                              double *__restrict__ partials,
+                                                              DevScalars *__restrict__ sc, FusedCtrl fc)
+{
+    __shared__ double smem[32];
+    const CgState &cs = sc->cg;
+    const int m = cs.lb_count;
+    const double minvalue = cs.minvalue, cq = cs.lb_cq;
+    const float *si[GP_LB_PAIRS], *yi[GP_LB_PAIRS];
+    double ca[GP_LB_PAIRS], cb[GP_LB_PAIRS];
+#pragma unroll
+    for (int i = 0; i < GP_LB_PAIRS; i++) {
+        si[i] = S + (size_t)cs.lb_slot[i] * n;
+        yi[i] = Y + (size_t)cs.lb_slot[i] * n;
+        ca[i] = cs.lb_cs[i];
+        cb[i] = cs.lb_cy[i];
+    }
+    double acc[1] = {0.0};
+    double dmax = 0.0;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        const float I = img[p], gp = g[p];
+        xold[p] = I;
+        float dn = 0.f;
+        if (!lb_fixed(I, gp, minvalue)) {
+            double h = cq * (double)gp;
+#pragma unroll
+            for (int i = 0; i < GP_LB_PAIRS; i++)
+                if (i < m) h += ca[i] * (double)si[i][p] + cb[i] * (double)yi[i][p];
+            dn = (float)(-h);
+        }
+        d[p] = dn;
+        acc[0] += (double)dn * (double)gp;
+        dmax = fmax(dmax, fabs((double)dn));
+    }
+    block_sum<1>(acc, smem);
+    dmax = block_max(dmax, smem);
+    if (threadIdx.x == 0) atomicMax(&sc->dmax_bits, __float_as_uint((float)dmax));
+    if (threadIdx.x == 0) partials[blockIdx.x] = acc[0];
+    if (last_block(&sc->counter[RED_DIR])) {
+        double o[1];
+        finish_sum<1>(partials, gridDim.x, o, smem);
+        if (threadIdx.x == 0) {
+            sc->dir_dot = o[0];
+            sc->counter[RED_DIR] = 0;
+            run_fused_ctrl(sc, fc);
+        }
+    }
+}
+
+int gp_lbfgs_alloc(gpair_ctx *c)
+{
+    if (c->lb_s) return GPAIR_OK;
+    const size_t n = (size_t)(GP_LB_PAIRS + 1) * c->npix;
+    GP_CUDA(c, cudaMalloc(&c->lb_s, n * sizeof(float)));
+    GP_CUDA(c, cudaMalloc(&c->lb_y, n * sizeof(float)));
+    GP_CUDA(c, cudaMalloc(&c->lb_xold, (size_t)c->npix * sizeof(float)));
+    GP_CUDA(c, cudaMemsetAsync(c->lb_s, 0, n * sizeof(float), c->stream));
+    GP_CUDA(c, cudaMemsetAsync(c->lb_y, 0, n * sizeof(float), c->stream));
+    GP_CUDA(c, cudaMemsetAsync(c->lb_xold, 0, (size_t)c->npix * sizeof(float), c->stream));
+    return GPAIR_OK;
+}
+
+void gp_lbfgs_free(gpair_ctx *c)
+{
+    if (c->lb_s) cudaFree(c->lb_s);
+    if (c->lb_y) cudaFree(c->lb_y);
+    if (c->lb_xold) cudaFree(c->lb_xold);
+    c->lb_s = c->lb_y = c->lb_xold = nullptr;
+}
+
+// The direction of one iteration: candidate pair (controller: accept / drop),
+// dots of the projected gradient (controller: coefficients), combination
+// (controller: the line-search start, as after the CG descent update). The
+// controller steps run fused into the last block of each pass; the caller
+// sets the first one (CTRL_LB_PAIR) in c->fuse_ctrl.
+int gp_lbfgs_direction(gpair_ctx *c)
+{
+    const int last = c->fuse_ctrl;  // the controller step after the direction (CTRL_AFTER_DIR)
+    int rc = gp_lbfgs_alloc(c);
+    if (rc) return rc;
+    const int g = red_grid(c->npix);
+    c->fuse_ctrl = CTRL_LB_PAIR;
+    k_lbfgs_pair<<<g, GP_THREADS, 0, c->stream>>>(c->image, c->lb_xold, c->full_grad_new, c->full_grad, c->lb_s,
+                                                  c->lb_y, c->npix, slot_partials(c, RED_LBP), c->sc,
+                                                  take_fused_ctrl(c));
+    GP_LAUNCH_CHECK(c);
+    c->fuse_ctrl = CTRL_LB_COEF;
+    k_lbfgs_dots<<<g, GP_THREADS, 0, c->stream>>>(c->image, c->full_grad_new, c->lb_s, c->lb_y, c->npix,
+                                                  slot_partials(c, RED_LBD), c->sc, take_fused_ctrl(c));
+    GP_LAUNCH_CHECK(c);
+    c->fuse_ctrl = last;
+    k_lbfgs_combine<<<g, GP_THREADS, 0, c->stream>>>(c->image, c->full_grad_new, c->lb_s, c->lb_y,
+                                                     c->descent_dir, c->lb_xold, c->npix, slot_partials(c, RED_DIR),
+                                                     c->sc, take_fused_ctrl(c));
+    GP_LAUNCH_CHECK(c);
+    return GPAIR_OK;
+}
+
 // image = max(image + s d, minval); optionally full_grad = full_grad_new
 __global__ void k_update_image(float *__restrict__ img, const float *__restrict__ d, int n, int step_from_state,
                                double step_host, double minval, const float *__restrict__ gnew,
@@ -857,13 +1085,26 @@ int gp_update_temp(gpair_ctx *c, double step, double minval, int clamp)
 // GP_NTR trial images I_j = max(I + s_j d, minval) (s_j = cg.ts[j], blockIdx.y
 // = j), each with its flux and entropy summed in FP64 (the trial part of
 // kernel_update_tempimage.cl + kernel_entropy_gs.cl, for a whole batch). On the
-// tensor path (hi != nullptr) the f16 hi/lo forward operand of trial j is
-// written to rows [j Lpad, j Lpad + N) with the power-of-two scale of the
-// bound max|I_j| <= max|I| + |s_j| max|d|.
+// tensor path (hi != nullptr) the hi/lo forward operand of trial j (f16, or
+// TF32 held as FP32; lo == nullptr in one-product mode) is written to rows
+// [j Lpad, j Lpad + N) with the power-of-two scale of the bound
+// max|I_j| <= max|I| + |s_j| max|d|.
+__device__ __forceinline__ void trial_split(float v, __half &h, __half &l)
+{
+    h = __float2half_rn(v);
+    l = __float2half_rn(v - __half2float(h));
+}
+__device__ __forceinline__ void trial_split(float v, float &h, float &l)
+{
+    h = umma::tf32_rna(v);
+    l = umma::tf32_rna(v - h);
+}
+
+template <typename OT>
 __global__ void __launch_bounds__(GP_THREADS) k_trials_prep(const float *__restrict__ img,
                                                             const float *__restrict__ d, float *__restrict__ trials,
                                                             const float *__restrict__ model, int N, int npix,
-                                                            __half *__restrict__ hi, __half *__restrict__ lo,
+                                                            OT *__restrict__ hi, OT *__restrict__ lo,
                                                             int Lpad, int Kx_pad, int tw_log2,
                                                             double *__restrict__ partials,
                                                             DevScalars *__restrict__ sc)
@@ -892,10 +1133,11 @@ __global__ void __launch_bounds__(GP_THREADS) k_trials_prep(const float *__restr
         if (hi) {
             const int y = p / N, x = p - y * N;
             const float v = I * scale;
-            const __half h = __float2half_rn(v);
             const size_t o = ((size_t)j * Lpad + y) * Kx_pad + x;
+            OT h, l;
+            trial_split(v, h, l);
             hi[o] = h;
-            lo[o] = __float2half_rn(v - __half2float(h));
+            if (lo) lo[o] = l;
         }
     }
     block_sum<2>(acc, smem);
@@ -1013,7 +1255,10 @@ int gp_batch_alloc(gpair_ctx *c)
     GP_CUDA(c, cudaMalloc(&c->partials_b, sizeof(double) * (size_t)GP_NTR * 1024 * 2));
     int nsm = 148;
     GP_CUDA(c, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
-    c->batch_wave[0] = batch_wave_blocks((const void *)k_trials_prep, nsm);
+    // one wave of either operand kind's trial-prep kernel
+    const int w16 = batch_wave_blocks((const void *)k_trials_prep<__half>, nsm);
+    const int w32 = batch_wave_blocks((const void *)k_trials_prep<float>, nsm);
+    c->batch_wave[0] = w16 < w32 ? w16 : w32;
     c->batch_wave[1] = batch_wave_blocks((const void *)k_vis_chi2_batch, nsm);
     return GPAIR_OK;
 }
@@ -1028,12 +1273,17 @@ void gp_batch_free(gpair_ctx *c)
     c->partials_b = nullptr;
 }
 
-int gp_trials_prep_launch(gpair_ctx *c, void *hi, void *lo, int Lpad, int Kx_pad, int tw_log2)
+int gp_trials_prep_launch(gpair_ctx *c, void *hi, void *lo, int Lpad, int Kx_pad, int tw_log2, int tf32)
 {
     dim3 g(batch_blocks_per_trial(c), GP_NTR);
-    k_trials_prep<<<g, GP_THREADS, 0, c->stream>>>(c->image, c->descent_dir, c->image_trials, c->model, c->N, c->npix,
-                                                  (__half *)hi, (__half *)lo, Lpad, Kx_pad, tw_log2, c->partials_b,
-                                                  c->sc);
+    if (tf32)
+        k_trials_prep<float><<<g, GP_THREADS, 0, c->stream>>>(c->image, c->descent_dir, c->image_trials, c->model,
+                                                               c->N, c->npix, (float *)hi, (float *)lo, Lpad, Kx_pad,
+                                                               tw_log2, c->partials_b, c->sc);
+    else
+        k_trials_prep<__half><<<g, GP_THREADS, 0, c->stream>>>(c->image, c->descent_dir, c->image_trials, c->model,
+                                                                c->N, c->npix, (__half *)hi, (__half *)lo, Lpad,
+                                                                Kx_pad, tw_log2, c->partials_b, c->sc);
     GP_LAUNCH_CHECK(c);
     return GPAIR_OK;
 }
@@ -1056,7 +1306,7 @@ static int eval_batch(gpair_ctx *c, cudaEvent_t *ev)
         if ((rc = gp_tc_forward_batch_gemm(c))) return rc;
         epp = c->epp;
     } else {
-        if ((rc = gp_trials_prep_launch(c, nullptr, nullptr, 0, 0, 0))) return rc;
+        if ((rc = gp_trials_prep_launch(c, nullptr, nullptr, 0, 0, 0, 0))) return rc;
         gp_stage_end(c);
         if (ev) cudaEventRecord(ev[1], c->stream);
         gp_stage_begin(c, 1);
@@ -1252,6 +1502,109 @@ __device__ void ls_batch_after(DevScalars *__restrict__ sc, CgState &s)
     ls_batch_accept(s, sb, Jb);
 }
 
+// Projected L-BFGS, candidate pair: accept it when s.y > 1e-12 |s| |y| (the
+// newest GP_LB_PAIRS are kept, the oldest is evicted), record its dots in the
+// Gram matrices and take gamma from it; a failed batched search drops the
+// history afterwards.
+__device__ void lb_after_pair(DevScalars *__restrict__ sc, CgState &s)
+{
+    const double *pd = sc->lb_pdots;
+    if (s.lb_xvalid) {
+        const double sy = pd[0], yy = pd[1], ss = pd[2];
+        if (yy > 0.0 && sy > 1e-12 * sqrt(ss * yy)) {
+            const int m = s.lb_count;
+            double sy_col[GP_LB_PAIRS], yy_col[GP_LB_PAIRS];  // stored pair i with the new y
+            for (int i = 0; i < m; i++) {
+                sy_col[i] = pd[3 + i];
+                yy_col[i] = pd[3 + GP_LB_PAIRS + i];
+            }
+            const int cand = s.lb_slot[GP_LB_PAIRS];
+            int base = 0, mm = m;
+            if (m == GP_LB_PAIRS) {
+                // evict the oldest: its buffer becomes the free one
+                const int old = s.lb_slot[0];
+                for (int i = 0; i + 1 < GP_LB_PAIRS; i++) s.lb_slot[i] = s.lb_slot[i + 1];
+                s.lb_slot[GP_LB_PAIRS] = old;
+                for (int i = 0; i + 1 < GP_LB_PAIRS; i++)
+                    for (int j = 0; j + 1 < GP_LB_PAIRS; j++) {
+                        s.lb_sy[i][j] = s.lb_sy[i + 1][j + 1];
+                        s.lb_yy[i][j] = s.lb_yy[i + 1][j + 1];
+                    }
+                base = 1;
+                mm = GP_LB_PAIRS - 1;
+            } else {
+                s.lb_slot[GP_LB_PAIRS] = s.lb_slot[m];
+            }
+            s.lb_slot[mm] = cand;
+            for (int i = 0; i < mm; i++) {
+                s.lb_sy[i][mm] = sy_col[i + base];
+                s.lb_yy[i][mm] = yy_col[i + base];
+                s.lb_yy[mm][i] = yy_col[i + base];
+            }
+            s.lb_sy[mm][mm] = sy;
+            s.lb_yy[mm][mm] = yy;
+            s.lb_gamma = sy / yy;
+            s.lb_count = mm + 1;
+        }
+    }
+    if (s.lb_drop) {
+        s.lb_count = 0;
+        s.lb_drop = 0;
+    }
+}
+
+// Projected L-BFGS, direction coefficients from the compact form; with the
+// reference's search, a direction that is not a descent direction is replaced
+// by the projected -g at once (the batched search restarts the next iteration
+// instead, as for CG).
+__device__ void lb_coefficients(DevScalars *__restrict__ sc, CgState &s)
+{
+    const double *qd = sc->lb_qdots;
+    const int m = s.lb_count;
+    for (int i = 0; i < GP_LB_PAIRS; i++) {
+        s.lb_cs[i] = 0.0;
+        s.lb_cy[i] = 0.0;
+    }
+    s.lb_cq = 1.0;
+    if (m == 0) return;
+    const double gam = s.lb_gamma;
+    double x[GP_LB_PAIRS], z[GP_LB_PAIRS], t[GP_LB_PAIRS];
+    // R x = u (R upper triangular, R_ij = s_i.y_j for i <= j)
+    for (int i = m - 1; i >= 0; i--) {
+        double v = qd[1 + i];
+        for (int j = i + 1; j < m; j++) v -= s.lb_sy[i][j] * x[j];
+        x[i] = v / s.lb_sy[i][i];
+    }
+    // z = (D + gamma Y Y^T) x - gamma Y q
+    for (int i = 0; i < m; i++) {
+        double v = s.lb_sy[i][i] * x[i];
+        for (int j = 0; j < m; j++) v += gam * s.lb_yy[i][j] * x[j];
+        z[i] = v - gam * qd[1 + GP_LB_PAIRS + i];
+    }
+    // R^T t = z
+    for (int i = 0; i < m; i++) {
+        double v = z[i];
+        for (int j = 0; j < i; j++) v -= s.lb_sy[j][i] * t[j];
+        t[i] = v / s.lb_sy[i][i];
+    }
+    double w1 = gam * qd[0];
+    for (int i = 0; i < m; i++) {
+        s.lb_cs[i] = t[i];
+        s.lb_cy[i] = -gam * x[i];
+        w1 += t[i] * qd[1 + i] - gam * x[i] * qd[1 + GP_LB_PAIRS + i];
+    }
+    s.lb_cq = gam;
+    // d.g = -w1: not a descent direction (or not finite) with the reference's search -> projected -g
+    if (s.ls_mode != GPAIR_LS_BATCH && !(w1 > 0.0)) {
+        s.lb_count = 0;
+        for (int i = 0; i < GP_LB_PAIRS; i++) {
+            s.lb_cs[i] = 0.0;
+            s.lb_cy[i] = 0.0;
+        }
+        s.lb_cq = 1.0;
+    }
+}
+
 // One step of the CG state machine.
 __device__ __noinline__ static void cg_step(DevScalars *__restrict__ sc, CgState &s, int what)
 {
@@ -1276,6 +1629,12 @@ __device__ __noinline__ static void cg_step(DevScalars *__restrict__ sc, CgState
     case CTRL_END:
         s.run_it++;
         break;
+    case CTRL_LB_PAIR:
+        lb_after_pair(sc, s);
+        break;
+    case CTRL_LB_COEF:
+        lb_coefficients(sc, s);
+        break;
     case CTRL_INIT:
         s.run_it = 0;
         s.it = 0;
@@ -1290,6 +1649,11 @@ __device__ __noinline__ static void cg_step(DevScalars *__restrict__ sc, CgState
         s.stopped = 0;
         s.force_sd = 0;
         sc->nonfinite = 0;
+        s.lb_count = 0;
+        s.lb_xvalid = 0;
+        s.lb_drop = 0;
+        s.lb_gamma = 1.0;
+        for (int i = 0; i <= GP_LB_PAIRS; i++) s.lb_slot[i] = i;
         break;
     case CTRL_BEGIN: {
         sc->imax_curr = sc->imax;  // exact max of the current image (its prep ran this iteration)
@@ -1320,6 +1684,7 @@ __device__ __noinline__ static void cg_step(DevScalars *__restrict__ sc, CgState
         if (s.force_sd) {
             beta = 0.0;
             s.force_sd = 0;
+            if (s.method == 4) s.lb_drop = 1;  // projected L-BFGS: the history goes after this pair
         }
         s.beta = beta;
         s.prev_nn = nn;
@@ -1345,16 +1710,20 @@ __device__ __noinline__ static void cg_step(DevScalars *__restrict__ sc, CgState
             s.npts = 0;
             s.bround = 0;
             s.bphase = BR_GRID;
+            if (s.method == 4) s.lb_xvalid = 1;  // the combination pass saved x_old
             if (!(s.wolfe1 < 0.0)) {  // not a descent direction: restart from -g
                 s.force_sd = 1;
                 s.action = CG_DONE;
                 break;
             }
+            // a quasi-Newton direction carries its own scale: grid centred on step 1
+            if (s.method == 4 && s.lb_count > 0) s.s_c = 1.0;
             if (!(s.s_c > 0.0) || !isfinite(s.s_c)) s.s_c = 1.0;
             ls_batch_grid(s);
             break;
         }
         // line search initialisation (gpair.c:792-806)
+        if (s.method == 4) s.lb_xvalid = 1;
         s.wolfe1 = sc->dir_dot;
         s.sel = 0.0;
         s.s = 1.0;

@@ -122,6 +122,20 @@ __device__ __forceinline__ void mma_f16_ss(uint32_t d_tmem, uint64_t a_desc, uin
         : "memory");
 }
 
+// The same with kind::tf32: A and B hold FP32 bit patterns, of which the
+// tensor core uses the TF32 part (sign, exponent, 10 mantissa bits); K = 8
+// per instruction, i.e. 32 bytes of a K-major row as with kind::f16.
+__device__ __forceinline__ void mma_tf32_ss(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                            uint32_t accumulate)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+        ::"r"(d_tmem), "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+        : "memory");
+}
+
 // Arrive once on `bar` when all previously issued MMAs of this thread complete
 __device__ __forceinline__ void mma_commit(uint64_t *bar)
 {
@@ -160,7 +174,8 @@ __device__ __forceinline__ uint64_t smem_desc_k_sw128(const void *tile)
     return d;
 }
 
-// Instruction descriptor, kind::f16: D f32, A/B f16 (fmt 0) or bf16 (fmt 1), both K-major.
+// Instruction descriptor, kind::f16 / kind::tf32: D f32, A/B f16 (fmt 0), bf16
+// (fmt 1) or tf32 (fmt 2, with kind::tf32), both K-major.
 __host__ __device__ constexpr uint32_t idesc_f16(int M, int N, int ab_fmt)
 {
     return (1u << 4)                       // D format f32
@@ -168,6 +183,15 @@ __host__ __device__ constexpr uint32_t idesc_f16(int M, int N, int ab_fmt)
            | ((uint32_t)ab_fmt << 10)      // B format
            | ((uint32_t)(N >> 3) << 17)    // N / 8
            | ((uint32_t)(M >> 4) << 24);   // M / 16
+}
+
+// FP32 -> TF32, round to nearest (ties away from zero); the result is an FP32
+// bit pattern whose low 13 mantissa bits are zero
+__device__ __forceinline__ float tf32_rna(float x)
+{
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
 }
 
 }  // namespace umma

@@ -39,12 +39,12 @@
 
 #define TC_BM 128
 #define TC_BN 256
-#define TC_BK 64
+#define TC_ROWB 128  // bytes of one K-block row: 64 f16 or 32 TF32 elements
 #define TC_STAGES 2
 #define TC_THREADS 192
 #define TC_TW_LOG2 10  // twiddle operands are scaled by 2^10
-#define TC_A_BYTES (TC_BM * TC_BK * 2)
-#define TC_B_BYTES (TC_BN * TC_BK * 2)
+#define TC_A_BYTES (TC_BM * TC_ROWB)
+#define TC_B_BYTES (TC_BN * TC_ROWB)
 #define TC_STAGE_BYTES (2 * TC_A_BYTES + 2 * TC_B_BYTES)
 #define TC_TMEM_COLS 512
 #define TC_SMEM_BYTES (1024 + TC_STAGES * TC_STAGE_BYTES + 256)
@@ -52,6 +52,42 @@
 #define RPMAS_TC ((3.14159265358979323 / 180.0) / 3600000.0)  // radians per milliarcsecond
 
 enum { EPI_FWD = 0, EPI_STORE = 1 };
+
+// Operand element types: f16 (kind::f16, K = 16 per MMA) or TF32 held as FP32
+// bit patterns (kind::tf32, K = 8 per MMA). Both fill 128-byte K-block rows,
+// so the shared-memory stages, descriptors and TMA boxes are the same in bytes.
+enum { OP_F16 = 0, OP_TF32 = 1 };
+__host__ __device__ constexpr int tc_bk(int op) { return op == OP_F16 ? 64 : 32; }
+// products per K step: 3 = hi*hi + hi*lo + lo*hi of split operands, 1 = hi*hi
+// At most TC_SPLIT_PRODUCTS products per adjoint split-K partial (FP32 accumulation)
+#define TC_SPLIT_PRODUCTS 4096
+
+template <typename OT> struct OpSplit;
+template <> struct OpSplit<__half> {
+    // f16 hi = f16(v), lo = f16(v - hi)
+    static __device__ __forceinline__ void split(float v, __half &h, __half &l)
+    {
+        h = __float2half_rn(v);
+        l = __float2half_rn(v - __half2float(h));
+    }
+};
+template <> struct OpSplit<float> {
+    // TF32 hi = tf32(v), lo = tf32(v - hi) (v - hi is exact in FP32)
+    static __device__ __forceinline__ void split(float v, float &h, float &l)
+    {
+        h = umma::tf32_rna(v);
+        l = umma::tf32_rna(v - h);
+    }
+};
+
+template <typename OT>
+__device__ __forceinline__ void split_store(OT *__restrict__ hi, OT *__restrict__ lo, size_t i, float v)
+{
+    OT h, l;
+    OpSplit<OT>::split(v, h, l);
+    hi[i] = h;
+    if (lo) lo[i] = l;
+}
 
 struct TcArgs {
     int m_tiles, n_tiles, kb_total, kb_per_split, units;
@@ -80,12 +116,15 @@ struct TcState {
     // A side (M = 128 rows): forward twiddles [rows_pad][Kx_pad], adjoint twiddles [xrows_pad][K2_pad]
     // B side (N = 256 rows): image [M_pad][Kx_pad], adjoint weights [M_pad][K2_pad]
     // batched trials: GP_NTR images stacked at Lb rows each, [GP_NTR Lb][Kx_pad]
+    // op: OP_F16 or OP_TF32 (element size esz, bk elements per K-block);
+    // nprod: 3 (split operands; the lo buffers exist) or 1 (hi only)
+    int op, nprod, esz, bk;
     int Kx_pad, M_pad, rows_pad, K2_pad, xrows_pad;
     int Lb, epp_b;
-    __half *imgb_hi, *imgb_lo;
+    void *imgb_hi, *imgb_lo;
     CUtensorMap m_imgb_hi, m_imgb_lo;
     int splits, kb_per;
-    __half *img_hi, *img_lo, *fx_hi, *fx_lo, *fxt_hi, *fxt_lo, *w_hi, *w_lo;
+    void *img_hi, *img_lo, *fx_hi, *fx_lo, *fxt_hi, *fxt_lo, *w_hi, *w_lo;
     float2 *fya, *fyr;
     int nanc;
     CUtensorMap m_img_hi, m_img_lo, m_fx_hi, m_fx_lo, m_w_hi, m_w_lo, m_fxt_hi, m_fxt_lo;
@@ -120,7 +159,7 @@ __device__ __forceinline__ void tc_decode(const TcArgs &a, int u, int &m, int &n
     }
 }
 
-template <int EPI>
+template <int EPI, int OP, int NPROD>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     k_tc_gemm(const __grid_constant__ CUtensorMap tA_hi, const __grid_constant__ CUtensorMap tA_lo,
               const __grid_constant__ CUtensorMap tB_hi, const __grid_constant__ CUtensorMap tB_lo, const TcArgs a)
@@ -179,11 +218,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     }
                     if (a.skip_loads) continue;  // nothing issued: the stage never fills
                     unsigned char *st = stages + s * TC_STAGE_BYTES;
-                    umma::mbar_arrive_expect_tx(&full[s], TC_STAGE_BYTES);
-                    umma::tma_load_2d(st, &tA_hi, &full[s], kb * TC_BK, m * TC_BM);
-                    umma::tma_load_2d(st + TC_A_BYTES, &tA_lo, &full[s], kb * TC_BK, m * TC_BM);
-                    umma::tma_load_2d(st + 2 * TC_A_BYTES, &tB_hi, &full[s], kb * TC_BK, n * TC_BN);
-                    umma::tma_load_2d(st + 2 * TC_A_BYTES + TC_B_BYTES, &tB_lo, &full[s], kb * TC_BK, n * TC_BN);
+                    const int kx = kb * tc_bk(OP);
+                    umma::mbar_arrive_expect_tx(&full[s], NPROD == 3 ? TC_STAGE_BYTES : TC_A_BYTES + TC_B_BYTES);
+                    umma::tma_load_2d(st, &tA_hi, &full[s], kx, m * TC_BM);
+                    umma::tma_load_2d(st + 2 * TC_A_BYTES, &tB_hi, &full[s], kx, n * TC_BN);
+                    if (NPROD == 3) {
+                        umma::tma_load_2d(st + TC_A_BYTES, &tA_lo, &full[s], kx, m * TC_BM);
+                        umma::tma_load_2d(st + 2 * TC_A_BYTES + TC_B_BYTES, &tB_lo, &full[s], kx, n * TC_BN);
+                    }
                     it++;
                 }
             }
@@ -199,7 +241,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     } else if (warp == 1) {
         if (lane == 0) {
             // ------------------------------------------------ MMA issuer
-            const uint32_t idesc = umma::idesc_f16(TC_BM, TC_BN, 0);
+            const uint32_t idesc = umma::idesc_f16(TC_BM, TC_BN, OP == OP_F16 ? 0 : 2);
             int it = 0, t = 0;
             bool ok = true;
             for (int u = blockIdx.x; u < a.units && ok && !*abort_flag; u += gridDim.x, t++) {
@@ -226,11 +268,23 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     const uint64_t dbh = umma::smem_desc_k_sw128(st + 2 * TC_A_BYTES);
                     const uint64_t dbl = umma::smem_desc_k_sw128(st + 2 * TC_A_BYTES + TC_B_BYTES);
 #pragma unroll
-                    for (int kk = 0; kk < TC_BK / 16; kk++) {
-                        const uint64_t off = (uint64_t)(kk * 32) >> 4;  // 16 f16 = 32 B along K
-                        umma::mma_f16_ss(d, dah + off, dbh + off, idesc, (kb > kb0 || kk > 0) ? 1u : 0u);
-                        umma::mma_f16_ss(d, dah + off, dbl + off, idesc, 1u);
-                        umma::mma_f16_ss(d, dal + off, dbh + off, idesc, 1u);
+                    for (int kk = 0; kk < TC_ROWB / 32; kk++) {
+                        // one MMA covers 32 B along K: 16 f16 or 8 TF32 elements
+                        const uint64_t off = (uint64_t)(kk * 32) >> 4;
+                        const uint32_t acc = (kb > kb0 || kk > 0) ? 1u : 0u;
+                        if (OP == OP_F16) {
+                            umma::mma_f16_ss(d, dah + off, dbh + off, idesc, acc);
+                            if (NPROD == 3) {
+                                umma::mma_f16_ss(d, dah + off, dbl + off, idesc, 1u);
+                                umma::mma_f16_ss(d, dal + off, dbh + off, idesc, 1u);
+                            }
+                        } else {
+                            umma::mma_tf32_ss(d, dah + off, dbh + off, idesc, acc);
+                            if (NPROD == 3) {
+                                umma::mma_tf32_ss(d, dah + off, dbl + off, idesc, 1u);
+                                umma::mma_tf32_ss(d, dal + off, dbh + off, idesc, 1u);
+                            }
+                        }
                     }
                     umma::mma_commit(&empty[s]);  // stage reusable once these MMAs finish
                 }
@@ -342,9 +396,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 
 // Twiddle operands: forward B [rows_pad][Kx_pad] (row 2k+c = Re/Im of Fx[k][:])
 // and adjoint B [xrows_pad][K2_pad] (row x, column 2k+c), both scaled by 2^10.
+// lo == nullptr: hi only (one-product mode).
+template <typename OT>
 __global__ void k_tc_twiddle_ops(const float2 *__restrict__ fx, int nuv, int N, int Kx_pad, int rows_pad,
-                                 int K2_pad, int xrows_pad, __half *__restrict__ fx_hi, __half *__restrict__ fx_lo,
-                                 __half *__restrict__ fxt_hi, __half *__restrict__ fxt_lo)
+                                 int K2_pad, int xrows_pad, OT *__restrict__ fx_hi, OT *__restrict__ fx_lo,
+                                 OT *__restrict__ fxt_hi, OT *__restrict__ fxt_lo)
 {
     const float ts = (float)(1 << TC_TW_LOG2);
     long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -356,9 +412,7 @@ __global__ void k_tc_twiddle_ops(const float2 *__restrict__ fx, int nuv, int N, 
             float2 f = fx[(size_t)k * N + x];
             v = ((n & 1) ? f.y : f.x) * ts;
         }
-        __half h = __float2half_rn(v);
-        fx_hi[idx] = h;
-        fx_lo[idx] = __float2half_rn(v - __half2float(h));
+        split_store(fx_hi, fx_lo, (size_t)idx, v);
         return;
     }
     idx -= nf;
@@ -369,17 +423,16 @@ __global__ void k_tc_twiddle_ops(const float2 *__restrict__ fx, int nuv, int N, 
             float2 f = fx[(size_t)k * N + x];
             v = ((kp & 1) ? f.y : f.x) * ts;
         }
-        __half h = __float2half_rn(v);
-        fxt_hi[idx] = h;
-        fxt_lo[idx] = __float2half_rn(v - __half2float(h));
+        split_store(fxt_hi, fxt_lo, (size_t)idx, v);
     }
 }
 
 // Image operand: one global power-of-two scale 2^(15 - e), e = exponent of
 // max |image| (reduced by k_prep), then an f16 hi/lo split; one block per
 // padded row. Block 0 publishes the factor the forward epilogue removes.
+template <typename OT>
 __global__ void __launch_bounds__(256) k_tc_split_image(const float *__restrict__ img, int N, int Kx_pad,
-                                                        __half *__restrict__ hi, __half *__restrict__ lo,
+                                                        OT *__restrict__ hi, OT *__restrict__ lo,
                                                         DevScalars *__restrict__ sc)
 {
     const double mx = sc->imax;
@@ -392,9 +445,7 @@ __global__ void __launch_bounds__(256) k_tc_split_image(const float *__restrict_
     const int y = blockIdx.x;
     for (int x = threadIdx.x; x < Kx_pad; x += blockDim.x) {
         float v = (y < N && x < N) ? img[(size_t)y * N + x] * scale : 0.f;
-        __half h = __float2half_rn(v);
-        hi[(size_t)y * Kx_pad + x] = h;
-        lo[(size_t)y * Kx_pad + x] = __float2half_rn(v - __half2float(h));
+        split_store(hi, lo, (size_t)y * Kx_pad + x, v);
     }
     if (y == 0 && threadIdx.x == 0) sc->fwd_inv_scale = mx > 0.0 ? ldexpf(1.f, ex - 15 - TC_TW_LOG2) : 0.f;
 }
@@ -404,9 +455,10 @@ __global__ void __launch_bounds__(256) k_tc_split_image(const float *__restrict_
 // hi/lo image operand written with a power-of-two scale taken from the exact
 // bound max|I_t| <= max|I| + |s| max|d| (both maxima reduced earlier in the
 // iteration), so no separate pass over the trial image is needed.
+template <typename OT>
 __global__ void __launch_bounds__(GP_THREADS) k_tc_prep_split_trial(
     const float *__restrict__ img, const float *__restrict__ d, float *__restrict__ dst,
-    const float *__restrict__ model, int N, int npix, int Kx_pad, __half *__restrict__ hi, __half *__restrict__ lo,
+    const float *__restrict__ model, int N, int npix, int Kx_pad, OT *__restrict__ hi, OT *__restrict__ lo,
     double *__restrict__ partials, DevScalars *__restrict__ sc)
 {
     __shared__ double smem[2 * 32];
@@ -428,10 +480,7 @@ __global__ void __launch_bounds__(GP_THREADS) k_tc_prep_split_trial(
         acc[1] += reg_term(Id, m, sc->reg_kind);
         mx = fmax(mx, fabs(Id));
         const int y = p / N, x = p - y * N;
-        const float v = I * scale;
-        const __half h = __float2half_rn(v);
-        hi[(size_t)y * Kx_pad + x] = h;
-        lo[(size_t)y * Kx_pad + x] = __float2half_rn(v - __half2float(h));
+        split_store(hi, lo, (size_t)y * Kx_pad + x, I * scale);
     }
     block_sum<2>(acc, smem);
     mx = block_max(mx, smem);
@@ -482,9 +531,10 @@ __global__ void k_tc_fy_anchors(const float2 *__restrict__ fy, int nuv, int N, i
 // to [-1/2, 1/2]) with the final sincos in FP32: the kernel reads no table and
 // writes only W. Problems given as the reference's tables (no (u, v)) read Fy
 // from the table instead (uvc == nullptr).
+template <typename OT>
 __global__ void __launch_bounds__(256) k_tc_build_w(const float2 *__restrict__ cw, const float2 *__restrict__ uvc,
                                                     const float2 *__restrict__ fy, float pix, int nuv, int N,
-                                                    int K2_pad, __half *__restrict__ w_hi, __half *__restrict__ w_lo,
+                                                    int K2_pad, OT *__restrict__ w_hi, OT *__restrict__ w_lo,
                                                     DevScalars *__restrict__ sc)
 {
     __shared__ float2 tile[32][33];
@@ -534,11 +584,8 @@ __global__ void __launch_bounds__(256) k_tc_build_w(const float2 *__restrict__ c
         int k = k0 + kl;
         if (2 * k + 1 >= K2_pad) continue;
         float2 w = tile[kl][j];
-        __half h0 = __float2half_rn(w.x), h1 = __float2half_rn(w.y);
-        __half2 hv = __halves2half2(h0, h1);
-        __half2 lv = __halves2half2(__float2half_rn(w.x - __half2float(h0)), __float2half_rn(w.y - __half2float(h1)));
-        *reinterpret_cast<__half2 *>(&w_hi[(size_t)y * K2_pad + 2 * k]) = hv;
-        *reinterpret_cast<__half2 *>(&w_lo[(size_t)y * K2_pad + 2 * k]) = lv;
+        split_store(w_hi, w_lo, (size_t)y * K2_pad + 2 * k, w.x);
+        split_store(w_hi, w_lo, (size_t)y * K2_pad + 2 * k + 1, w.y);
     }
 }
 
@@ -555,10 +602,11 @@ __global__ void __launch_bounds__(256) k_tc_build_w(const float2 *__restrict__ c
 // rows >= N are not touched.
 #define BW_SEG 8
 #define BW_ROWS 16
+template <typename OT>
 __global__ void __launch_bounds__(256) k_tc_build_w_uv(const float2 *__restrict__ cw,
                                                         const float2 *__restrict__ uvc, float pix, int nuv, int N,
-                                                        int K2_pad, __half *__restrict__ w_hi,
-                                                        __half *__restrict__ w_lo, DevScalars *__restrict__ sc)
+                                                        int K2_pad, OT *__restrict__ w_hi,
+                                                        OT *__restrict__ w_lo, DevScalars *__restrict__ sc)
 {
     __shared__ __align__(16) float2 rp[BW_SEG][128];
     const double cmax = sc->cmax;
@@ -602,9 +650,11 @@ __global__ void __launch_bounds__(256) k_tc_build_w_uv(const float2 *__restrict_
         }
     }
     const int y1 = min(N, y0 + BW_ROWS);
+    // 8 values per row and thread: one 16-byte store (f16) or two (TF32)
+    constexpr int NV = sizeof(OT) * 8 / 16;
     uint4 *ph = reinterpret_cast<uint4 *>(w_hi + (size_t)y0 * K2_pad + 8 * g);
-    uint4 *pl = reinterpret_cast<uint4 *>(w_lo + (size_t)y0 * K2_pad + 8 * g);
-    const size_t step = (size_t)K2_pad / 8;  // uint4 per row
+    uint4 *pl = w_lo ? reinterpret_cast<uint4 *>(w_lo + (size_t)y0 * K2_pad + 8 * g) : nullptr;
+    const size_t step = (size_t)K2_pad * sizeof(OT) / 16;  // uint4 per row
     for (int y = y0; y < y1; y++) {
         const int j = (y - y0) & (BW_SEG - 1);
         if (j == 0) {
@@ -621,19 +671,23 @@ __global__ void __launch_bounds__(256) k_tc_build_w_uv(const float2 *__restrict_
         const float4 r23 = *reinterpret_cast<const float4 *>(&rp[j][4 * lane + 2]);
         const float2 r[4] = {make_float2(r01.x, r01.y), make_float2(r01.z, r01.w), make_float2(r23.x, r23.y),
                              make_float2(r23.z, r23.w)};
-        __half2 hv[4], lv[4];
+        __align__(16) OT hv[8];
+        __align__(16) OT lv[8];
 #pragma unroll
         for (int i = 0; i < 4; i++) {
             const float2 f = make_float2(an[i].x * r[i].x - an[i].y * r[i].y, an[i].x * r[i].y + an[i].y * r[i].x);
             const float2 w = make_float2(cs[i].x * f.x - cs[i].y * f.y, -(cs[i].x * f.y + cs[i].y * f.x));
-            hv[i] = __float22half2_rn(w);
-            const float2 hb = __half22float2(hv[i]);
-            lv[i] = __float22half2_rn(make_float2(w.x - hb.x, w.y - hb.y));
+            OpSplit<OT>::split(w.x, hv[2 * i], lv[2 * i]);
+            OpSplit<OT>::split(w.y, hv[2 * i + 1], lv[2 * i + 1]);
         }
-        *ph = *reinterpret_cast<const uint4 *>(hv);
-        *pl = *reinterpret_cast<const uint4 *>(lv);
+#pragma unroll
+        for (int v = 0; v < NV; v++) ph[v] = reinterpret_cast<const uint4 *>(hv)[v];
         ph += step;
-        pl += step;
+        if (pl) {
+#pragma unroll
+            for (int v = 0; v < NV; v++) pl[v] = reinterpret_cast<const uint4 *>(lv)[v];
+            pl += step;
+        }
     }
 }
 
@@ -655,20 +709,24 @@ static int tc_get_encode(gpair_ctx *c)
     return GPAIR_OK;
 }
 
-// 2-D f16 tensor [rows][cols] (cols contiguous), 64 x box_rows boxes, 128 B swizzle
-static int tc_make_map(gpair_ctx *c, CUtensorMap *m, const void *base, long long rows, long long cols, int box_rows)
+// 2-D operand tensor [rows][cols] (cols contiguous) of f16 (esz 2) or FP32/TF32
+// (esz 4) elements; boxes of one 128-byte K-block row x box_rows, 128 B swizzle
+static int tc_make_map(gpair_ctx *c, CUtensorMap *m, const void *base, long long rows, long long cols, int box_rows,
+                       int esz)
 {
-    if (cols % 64 || rows % box_rows || ((uintptr_t)base & 255)) {
+    const int bk = TC_ROWB / esz;
+    if (cols % bk || rows % box_rows || ((uintptr_t)base & 255)) {
         snprintf(c->last_error, sizeof(c->last_error), "tensor map shape/alignment violates TMA rules");
         return GPAIR_ERR_INVALID;
     }
     cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
-    cuuint64_t strides[1] = {(cuuint64_t)cols * 2};
-    cuuint32_t box[2] = {64, (cuuint32_t)box_rows};
+    cuuint64_t strides[1] = {(cuuint64_t)cols * esz};
+    cuuint32_t box[2] = {(cuuint32_t)bk, (cuuint32_t)box_rows};
     cuuint32_t estr[2] = {1, 1};
-    CUresult r = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, const_cast<void *>(base), dims, strides, box, estr,
-                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
-                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    CUresult r = g_encode(m, esz == 2 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+                          const_cast<void *>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) {
         snprintf(c->last_error, sizeof(c->last_error), "cuTensorMapEncodeTiled failed (%d)", (int)r);
         return GPAIR_ERR_CUDA;
@@ -676,31 +734,49 @@ static int tc_make_map(gpair_ctx *c, CUtensorMap *m, const void *base, long long
     return GPAIR_OK;
 }
 
-int gp_tc_splits(int N, int nuv, int nsm, int *kb_per_out)
+// operand kind and product count of a precision mode
+static void tc_mode(int precision, int *op, int *nprod)
 {
-    int M_pad = round_up(N, TC_BN), xrows_pad = round_up(N, TC_BM), K2_pad = round_up(2LL * (nuv ? nuv : 1), TC_BK);
+    *op = (precision == GPAIR_PREC_TF32 || precision == GPAIR_PREC_TF32X3) ? OP_TF32 : OP_F16;
+    *nprod = precision == GPAIR_PREC_TF32 ? 1 : 3;
+}
+
+// Split-K of the tensor adjoint for K-blocks of `bk` elements: enough splits to
+// fill the SMs, and at most TC_SPLIT_PRODUCTS products per split (FP32
+// accumulation in TMEM: a running sum of n oscillating products carries a
+// relative rounding error of about 2^-24 sqrt(n); 4096 keeps it near 4e-6; the
+// splits are summed in FP64)
+int gp_tc_splits(int N, int nuv, int nsm, int bk, int *kb_per_out)
+{
+    int M_pad = round_up(N, TC_BN), xrows_pad = round_up(N, TC_BM), K2_pad = round_up(2LL * (nuv ? nuv : 1), bk);
     int tiles = (xrows_pad / TC_BM) * (M_pad / TC_BN);
-    int kb_total = K2_pad / TC_BK;
+    int kb_total = K2_pad / bk;
     int want = (nsm + tiles - 1) / tiles;
     if (want < 1) want = 1;
     if (want > kb_total) want = kb_total;
     int kb_per = (kb_total + want - 1) / want;
-    // FP32 accumulation in TMEM: a running sum of n oscillating products carries a
-    // relative rounding error of about 2^-24 sqrt(n); at most 64 K-blocks (4096
-    // products) per split keeps it near 4e-6, the splits are summed in FP64
-    if (kb_per > 64) kb_per = 64;
+    const int cap = TC_SPLIT_PRODUCTS / bk;
+    if (kb_per > cap) kb_per = cap;
     int splits = (kb_total + kb_per - 1) / kb_per;
     if (kb_per_out) *kb_per_out = kb_per;
     return splits;
+}
+
+// the largest split count any tensor mode uses for this shape
+int gp_tc_max_splits(int N, int nuv, int nsm)
+{
+    int a = gp_tc_splits(N, nuv, nsm, tc_bk(OP_F16), nullptr);
+    int b = gp_tc_splits(N, nuv, nsm, tc_bk(OP_TF32), nullptr);
+    return a > b ? a : b;
 }
 
 void gp_tc_free(gpair_ctx *c)
 {
     TcState *t = (TcState *)c->tc_state;
     if (!t) return;
-    __half *bufs[] = {t->img_hi, t->img_lo, t->fx_hi, t->fx_lo, t->fxt_hi, t->fxt_lo, t->w_hi, t->w_lo,
-                      t->imgb_hi, t->imgb_lo};
-    for (__half *b : bufs)
+    void *bufs[] = {t->img_hi, t->img_lo, t->fx_hi, t->fx_lo, t->fxt_hi, t->fxt_lo, t->w_hi, t->w_lo,
+                    t->imgb_hi, t->imgb_lo};
+    for (void *b : bufs)
         if (b) cudaFree(b);
     if (t->fya) cudaFree(t->fya);
     if (t->fyr) cudaFree(t->fyr);
@@ -708,35 +784,65 @@ void gp_tc_free(gpair_ctx *c)
     c->tc_state = nullptr;
 }
 
+template <typename OT>
+static void launch_twiddle_ops(gpair_ctx *c, TcState *t, long long n_all)
+{
+    k_tc_twiddle_ops<OT><<<gp_cdiv(n_all, 256), 256, 0, c->stream>>>(
+        c->fx, c->nuv, c->N, t->Kx_pad, t->rows_pad, t->K2_pad, t->xrows_pad, (OT *)t->fx_hi, (OT *)t->fx_lo,
+        (OT *)t->fxt_hi, (OT *)t->fxt_lo);
+}
+
+template <int EPI>
+static int tc_set_smem(gpair_ctx *c)
+{
+    GP_CUDA(c, cudaFuncSetAttribute(k_tc_gemm<EPI, OP_F16, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    TC_SMEM_BYTES));
+    GP_CUDA(c, cudaFuncSetAttribute(k_tc_gemm<EPI, OP_TF32, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    TC_SMEM_BYTES));
+    GP_CUDA(c, cudaFuncSetAttribute(k_tc_gemm<EPI, OP_TF32, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    TC_SMEM_BYTES));
+    return GPAIR_OK;
+}
+
 int gp_tc_prepare(gpair_ctx *c)
 {
-    if (c->precision == GPAIR_PREC_TF32) {
-        snprintf(c->last_error, sizeof(c->last_error), "the TF32 tensor path is not built in this library");
-        return GPAIR_ERR_STATE;
-    }
     if (!c->have_problem) return GPAIR_OK;  // prepared when the problem is loaded
-    if (c->tc_state) return GPAIR_OK;
+    int op, nprod;
+    tc_mode(c->precision, &op, &nprod);
+    TcState *old = (TcState *)c->tc_state;
+    if (old && old->op == op && old->nprod == nprod) return GPAIR_OK;
+    if (old) {
+        // another operand kind: rebuild every operand buffer for this mode
+        GP_CUDA(c, cudaStreamSynchronize(c->stream));
+        gp_tc_free(c);
+    }
     int rc = tc_get_encode(c);
     if (rc) return rc;
     TcState *t = (TcState *)calloc(1, sizeof(TcState));
     if (!t) return GPAIR_ERR_ALLOC;
     c->tc_state = t;
+    t->op = op;
+    t->nprod = nprod;
+    t->esz = op == OP_F16 ? 2 : 4;
+    t->bk = tc_bk(op);
     const int N = c->N, nuv = c->nuv ? c->nuv : 1;
-    t->Kx_pad = round_up(N, TC_BK);
+    t->Kx_pad = round_up(N, t->bk);
     t->M_pad = round_up(N, TC_BN);
     t->rows_pad = round_up(2LL * nuv, TC_BM);
-    t->K2_pad = round_up(2LL * nuv, TC_BK);
+    t->K2_pad = round_up(2LL * nuv, t->bk);
     t->xrows_pad = round_up(N, TC_BM);
     GP_CUDA(c, cudaDeviceGetAttribute(&t->nsm, cudaDevAttrMultiProcessorCount, c->device));
-    t->splits = gp_tc_splits(N, nuv, t->nsm, &t->kb_per);
+    t->splits = gp_tc_splits(N, nuv, t->nsm, t->bk, &t->kb_per);
     size_t img = (size_t)t->M_pad * t->Kx_pad, fxs = (size_t)t->rows_pad * t->Kx_pad;
     size_t fxts = (size_t)t->xrows_pad * t->K2_pad, ws = (size_t)t->M_pad * t->K2_pad;
-    struct { __half **p; size_t n; } al[] = {{&t->img_hi, img}, {&t->img_lo, img}, {&t->fx_hi, fxs},
-                                             {&t->fx_lo, fxs},  {&t->fxt_hi, fxts}, {&t->fxt_lo, fxts},
-                                             {&t->w_hi, ws},    {&t->w_lo, ws}};
+    struct { void **p; size_t n; bool lo; } al[] = {{&t->img_hi, img, false}, {&t->img_lo, img, true},
+                                                    {&t->fx_hi, fxs, false},  {&t->fx_lo, fxs, true},
+                                                    {&t->fxt_hi, fxts, false}, {&t->fxt_lo, fxts, true},
+                                                    {&t->w_hi, ws, false},    {&t->w_lo, ws, true}};
     for (auto &x : al) {
-        GP_CUDA(c, cudaMalloc(x.p, x.n * sizeof(__half)));
-        GP_CUDA(c, cudaMemsetAsync(*x.p, 0, x.n * sizeof(__half), c->stream));
+        if (x.lo && nprod == 1) continue;  // one product: no lo operands
+        GP_CUDA(c, cudaMalloc(x.p, x.n * t->esz));
+        GP_CUDA(c, cudaMemsetAsync(*x.p, 0, x.n * t->esz, c->stream));
     }
     t->nanc = (N + 15) / 16;
     GP_CUDA(c, cudaMalloc(&t->fya, sizeof(float2) * (size_t)nuv * t->nanc));
@@ -747,20 +853,28 @@ int gp_tc_prepare(gpair_ctx *c)
         GP_LAUNCH_CHECK(c);
     }
     long long n_all = (long long)fxs + (long long)fxts;
-    k_tc_twiddle_ops<<<gp_cdiv(n_all, 256), 256, 0, c->stream>>>(c->fx, c->nuv, N, t->Kx_pad, t->rows_pad, t->K2_pad,
-                                                                t->xrows_pad, t->fx_hi, t->fx_lo, t->fxt_hi,
-                                                                t->fxt_lo);
+    if (op == OP_F16) launch_twiddle_ops<__half>(c, t, n_all);
+    else launch_twiddle_ops<float>(c, t, n_all);
     GP_LAUNCH_CHECK(c);
-    if ((rc = tc_make_map(c, &t->m_img_hi, t->img_hi, t->M_pad, t->Kx_pad, TC_BN))) return rc;
-    if ((rc = tc_make_map(c, &t->m_img_lo, t->img_lo, t->M_pad, t->Kx_pad, TC_BN))) return rc;
-    if ((rc = tc_make_map(c, &t->m_fx_hi, t->fx_hi, t->rows_pad, t->Kx_pad, TC_BM))) return rc;
-    if ((rc = tc_make_map(c, &t->m_fx_lo, t->fx_lo, t->rows_pad, t->Kx_pad, TC_BM))) return rc;
-    if ((rc = tc_make_map(c, &t->m_w_hi, t->w_hi, t->M_pad, t->K2_pad, TC_BN))) return rc;
-    if ((rc = tc_make_map(c, &t->m_w_lo, t->w_lo, t->M_pad, t->K2_pad, TC_BN))) return rc;
-    if ((rc = tc_make_map(c, &t->m_fxt_hi, t->fxt_hi, t->xrows_pad, t->K2_pad, TC_BM))) return rc;
-    if ((rc = tc_make_map(c, &t->m_fxt_lo, t->fxt_lo, t->xrows_pad, t->K2_pad, TC_BM))) return rc;
-    GP_CUDA(c, cudaFuncSetAttribute(k_tc_gemm<EPI_FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM_BYTES));
-    GP_CUDA(c, cudaFuncSetAttribute(k_tc_gemm<EPI_STORE>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM_BYTES));
+    const int e = t->esz;
+    if ((rc = tc_make_map(c, &t->m_img_hi, t->img_hi, t->M_pad, t->Kx_pad, TC_BN, e))) return rc;
+    if ((rc = tc_make_map(c, &t->m_fx_hi, t->fx_hi, t->rows_pad, t->Kx_pad, TC_BM, e))) return rc;
+    if ((rc = tc_make_map(c, &t->m_w_hi, t->w_hi, t->M_pad, t->K2_pad, TC_BN, e))) return rc;
+    if ((rc = tc_make_map(c, &t->m_fxt_hi, t->fxt_hi, t->xrows_pad, t->K2_pad, TC_BM, e))) return rc;
+    if (nprod == 3) {
+        if ((rc = tc_make_map(c, &t->m_img_lo, t->img_lo, t->M_pad, t->Kx_pad, TC_BN, e))) return rc;
+        if ((rc = tc_make_map(c, &t->m_fx_lo, t->fx_lo, t->rows_pad, t->Kx_pad, TC_BM, e))) return rc;
+        if ((rc = tc_make_map(c, &t->m_w_lo, t->w_lo, t->M_pad, t->K2_pad, TC_BN, e))) return rc;
+        if ((rc = tc_make_map(c, &t->m_fxt_lo, t->fxt_lo, t->xrows_pad, t->K2_pad, TC_BM, e))) return rc;
+    } else {
+        // the kernel never loads the lo maps in one-product mode; pass valid maps anyway
+        t->m_img_lo = t->m_img_hi;
+        t->m_fx_lo = t->m_fx_hi;
+        t->m_w_lo = t->m_w_hi;
+        t->m_fxt_lo = t->m_fxt_hi;
+    }
+    if ((rc = tc_set_smem<EPI_FWD>(c))) return rc;
+    if ((rc = tc_set_smem<EPI_STORE>(c))) return rc;
     GP_CUDA(c, cudaStreamSynchronize(c->stream));
     return GPAIR_OK;
 }
@@ -777,15 +891,22 @@ int gp_tc_split_count(gpair_ctx *c, int kb_per)
 {
     TcState *t = (TcState *)c->tc_state;
     if (!t || kb_per <= 0) return 0;
-    return (t->K2_pad / TC_BK + kb_per - 1) / kb_per;
+    return (t->K2_pad / t->bk + kb_per - 1) / kb_per;
+}
+
+// the largest split-K tile length the FP32 accumulation allows
+int gp_tc_kb_cap(gpair_ctx *c)
+{
+    TcState *t = (TcState *)c->tc_state;
+    return t ? TC_SPLIT_PRODUCTS / t->bk : 0;
 }
 
 int gp_tc_set_kb_per(gpair_ctx *c, int kb_per)
 {
     TcState *t = (TcState *)c->tc_state;
     if (!t) return GPAIR_ERR_STATE;
-    const int kb_total = t->K2_pad / TC_BK;
-    if (kb_per < 1 || kb_per > 64) return GPAIR_ERR_INVALID;  // 64: the FP32 accumulation cap
+    const int kb_total = t->K2_pad / t->bk;
+    if (kb_per < 1 || kb_per > TC_SPLIT_PRODUCTS / t->bk) return GPAIR_ERR_INVALID;
     const int splits = (kb_total + kb_per - 1) / kb_per;
     if (splits > c->gpart_cap) return GPAIR_ERR_INVALID;
     t->kb_per = kb_per;
@@ -805,6 +926,24 @@ static TcState *tc_state_ready(gpair_ctx *c, int *rc)
     return t;
 }
 
+// one launch of the contraction in the context's operand kind / product count
+template <int EPI>
+static int tc_launch(gpair_ctx *c, TcState *t, int grid, const CUtensorMap &A_hi, const CUtensorMap &A_lo,
+                     const CUtensorMap &B_hi, const CUtensorMap &B_lo, TcArgs &a)
+{
+    a.err = &c->sc->tc_err;
+    a.budget = c->tc_wait_budget > 0 ? c->tc_wait_budget : TC_WAIT_BUDGET;
+    a.skip_loads = c->tc_skip_loads;
+    if (t->op == OP_F16)
+        k_tc_gemm<EPI, OP_F16, 3><<<grid, TC_THREADS, TC_SMEM_BYTES, c->stream>>>(A_hi, A_lo, B_hi, B_lo, a);
+    else if (t->nprod == 3)
+        k_tc_gemm<EPI, OP_TF32, 3><<<grid, TC_THREADS, TC_SMEM_BYTES, c->stream>>>(A_hi, A_lo, B_hi, B_lo, a);
+    else
+        k_tc_gemm<EPI, OP_TF32, 1><<<grid, TC_THREADS, TC_SMEM_BYTES, c->stream>>>(A_hi, A_lo, B_hi, B_lo, a);
+    GP_LAUNCH_CHECK(c);
+    return GPAIR_OK;
+}
+
 // forward contraction on the already split image operand
 int gp_tc_forward_gemm(gpair_ctx *c)
 {
@@ -815,7 +954,7 @@ int gp_tc_forward_gemm(gpair_ctx *c)
     memset(&a, 0, sizeof(a));
     a.m_tiles = t->rows_pad / TC_BM;  // twiddle-row tiles
     a.n_tiles = t->M_pad / TC_BN;     // image-row tiles
-    a.kb_total = t->Kx_pad / TC_BK;
+    a.kb_total = t->Kx_pad / t->bk;
     a.kb_per_split = a.kb_total;
     a.units = a.m_tiles * a.n_tiles;
     a.fya = t->fya;
@@ -829,13 +968,8 @@ int gp_tc_forward_gemm(gpair_ctx *c)
     a.batch = 0;
     a.sc = c->sc;
     a.vpart = c->vpart;
-    a.err = &c->sc->tc_err;
-    a.budget = c->tc_wait_budget > 0 ? c->tc_wait_budget : TC_WAIT_BUDGET;
-    a.skip_loads = c->tc_skip_loads;
     int grid = a.units < t->nsm ? a.units : t->nsm;
-    k_tc_gemm<EPI_FWD><<<grid, TC_THREADS, TC_SMEM_BYTES, c->stream>>>(t->m_fx_hi, t->m_fx_lo, t->m_img_hi,
-                                                                        t->m_img_lo, a);
-    GP_LAUNCH_CHECK(c);
+    if ((rc = tc_launch<EPI_FWD>(c, t, grid, t->m_fx_hi, t->m_fx_lo, t->m_img_hi, t->m_img_lo, a))) return rc;
     c->mt = a.n_tiles;
     return GPAIR_OK;
 }
@@ -854,19 +988,24 @@ int gp_tc_batch_prepare(gpair_ctx *c, int *epp)
         const int erows = t->Lb < TC_BN ? t->Lb : TC_BN;
         t->epp_b = t->Lb / erows;
         const size_t rows = (size_t)GP_NTR * t->Lb, n = rows * t->Kx_pad;
-        GP_CUDA(c, cudaMalloc(&t->imgb_hi, n * sizeof(__half)));
-        GP_CUDA(c, cudaMalloc(&t->imgb_lo, n * sizeof(__half)));
-        GP_CUDA(c, cudaMemsetAsync(t->imgb_hi, 0, n * sizeof(__half), c->stream));
-        GP_CUDA(c, cudaMemsetAsync(t->imgb_lo, 0, n * sizeof(__half), c->stream));
-        if ((rc = tc_make_map(c, &t->m_imgb_hi, t->imgb_hi, (long long)rows, t->Kx_pad, TC_BN))) return rc;
-        if ((rc = tc_make_map(c, &t->m_imgb_lo, t->imgb_lo, (long long)rows, t->Kx_pad, TC_BN))) return rc;
+        GP_CUDA(c, cudaMalloc(&t->imgb_hi, n * t->esz));
+        GP_CUDA(c, cudaMemsetAsync(t->imgb_hi, 0, n * t->esz, c->stream));
+        if ((rc = tc_make_map(c, &t->m_imgb_hi, t->imgb_hi, (long long)rows, t->Kx_pad, TC_BN, t->esz))) return rc;
+        if (t->nprod == 3) {
+            GP_CUDA(c, cudaMalloc(&t->imgb_lo, n * t->esz));
+            GP_CUDA(c, cudaMemsetAsync(t->imgb_lo, 0, n * t->esz, c->stream));
+            if ((rc = tc_make_map(c, &t->m_imgb_lo, t->imgb_lo, (long long)rows, t->Kx_pad, TC_BN, t->esz)))
+                return rc;
+        } else {
+            t->m_imgb_lo = t->m_imgb_hi;
+        }
     }
     c->epp = t->epp_b;
     if (epp) *epp = t->epp_b;
     return GPAIR_OK;
 }
 
-// trial images + their f16 operands for a batch (steps from the device state)
+// trial images + their operands for a batch (steps from the device state)
 int gp_tc_trials_prep_split(gpair_ctx *c, double *partials)
 {
     (void)partials;
@@ -874,7 +1013,7 @@ int gp_tc_trials_prep_split(gpair_ctx *c, double *partials)
     TcState *t = tc_state_ready(c, &rc);
     if (rc) return rc;
     if ((rc = gp_tc_batch_prepare(c, nullptr))) return rc;
-    return gp_trials_prep_launch(c, t->imgb_hi, t->imgb_lo, t->Lb, t->Kx_pad, TC_TW_LOG2);
+    return gp_trials_prep_launch(c, t->imgb_hi, t->imgb_lo, t->Lb, t->Kx_pad, TC_TW_LOG2, t->op == OP_TF32);
 }
 
 // forward contraction of the GP_NTR trial images in one launch: every twiddle
@@ -889,7 +1028,7 @@ int gp_tc_forward_batch_gemm(gpair_ctx *c)
     memset(&a, 0, sizeof(a));
     a.m_tiles = t->rows_pad / TC_BM;
     a.n_tiles = (GP_NTR * t->Lb) / TC_BN;
-    a.kb_total = t->Kx_pad / TC_BK;
+    a.kb_total = t->Kx_pad / t->bk;
     a.kb_per_split = a.kb_total;
     a.units = a.m_tiles * a.n_tiles;
     a.fya = t->fya;
@@ -904,24 +1043,23 @@ int gp_tc_forward_batch_gemm(gpair_ctx *c)
     a.batch = 1;
     a.sc = c->sc;
     a.vpart = c->vpart_b;
-    a.err = &c->sc->tc_err;
-    a.budget = c->tc_wait_budget > 0 ? c->tc_wait_budget : TC_WAIT_BUDGET;
-    a.skip_loads = c->tc_skip_loads;
     int grid = a.units < t->nsm ? a.units : t->nsm;
-    k_tc_gemm<EPI_FWD><<<grid, TC_THREADS, TC_SMEM_BYTES, c->stream>>>(t->m_fx_hi, t->m_fx_lo, t->m_imgb_hi,
-                                                                        t->m_imgb_lo, a);
-    GP_LAUNCH_CHECK(c);
-    return GPAIR_OK;
+    return tc_launch<EPI_FWD>(c, t, grid, t->m_fx_hi, t->m_fx_lo, t->m_imgb_hi, t->m_imgb_lo, a);
 }
 
-// f16 hi/lo split of an image into the forward's image operand
+// split of an image into the forward's image operand
 int gp_tc_split(gpair_ctx *c, int which)
 {
     int rc;
     TcState *t = tc_state_ready(c, &rc);
     if (rc) return rc;
     const float *img = (which == GPAIR_IMG_TEMP) ? c->image_temp : c->image;
-    k_tc_split_image<<<t->M_pad, 256, 0, c->stream>>>(img, c->N, t->Kx_pad, t->img_hi, t->img_lo, c->sc);
+    if (t->op == OP_F16)
+        k_tc_split_image<__half><<<t->M_pad, 256, 0, c->stream>>>(img, c->N, t->Kx_pad, (__half *)t->img_hi,
+                                                                   (__half *)t->img_lo, c->sc);
+    else
+        k_tc_split_image<float><<<t->M_pad, 256, 0, c->stream>>>(img, c->N, t->Kx_pad, (float *)t->img_hi,
+                                                                  (float *)t->img_lo, c->sc);
     GP_LAUNCH_CHECK(c);
     return GPAIR_OK;
 }
@@ -942,29 +1080,41 @@ int gp_tc_prep_split_trial(gpair_ctx *c)
     // at most GP_MAX_PARTIALS blocks: 3 partials each fit the RED_PREP slot
     int g = gp_cdiv(c->npix, GP_THREADS);
     if (g > GP_MAX_PARTIALS) g = GP_MAX_PARTIALS;
-    k_tc_prep_split_trial<<<g, GP_THREADS, 0, c->stream>>>(c->image, c->descent_dir, c->image_temp, c->model, c->N,
-                                                           c->npix, t->Kx_pad, t->img_hi, t->img_lo,
-                                                           c->partials, c->sc);
+    if (t->op == OP_F16)
+        k_tc_prep_split_trial<__half><<<g, GP_THREADS, 0, c->stream>>>(
+            c->image, c->descent_dir, c->image_temp, c->model, c->N, c->npix, t->Kx_pad, (__half *)t->img_hi,
+            (__half *)t->img_lo, c->partials, c->sc);
+    else
+        k_tc_prep_split_trial<float><<<g, GP_THREADS, 0, c->stream>>>(
+            c->image, c->descent_dir, c->image_temp, c->model, c->N, c->npix, t->Kx_pad, (float *)t->img_hi,
+            (float *)t->img_lo, c->partials, c->sc);
     GP_LAUNCH_CHECK(c);
     return GPAIR_OK;
 }
 
-// adjoint A-side weights W from c_k and Fy (f16 hi/lo, one global scale)
+template <typename OT>
+static void launch_build_w(gpair_ctx *c, TcState *t)
+{
+    if (c->have_uv) {
+        // 32 groups of 4 uv points x 8 warps of BW_ROWS rows per block
+        dim3 g(gp_cdiv(t->K2_pad / 8, 32), gp_cdiv(c->N, 8 * BW_ROWS));
+        k_tc_build_w_uv<OT><<<g, 256, 0, c->stream>>>(c->cw, c->uvc, c->pix, c->nuv, c->N, t->K2_pad,
+                                                       (OT *)t->w_hi, (OT *)t->w_lo, c->sc);
+    } else {
+        dim3 g(gp_cdiv(c->nuv ? c->nuv : 1, 32), gp_cdiv(c->N, 32));
+        k_tc_build_w<OT><<<g, 256, 0, c->stream>>>(c->cw, nullptr, c->fy, c->pix, c->nuv, c->N, t->K2_pad,
+                                                    (OT *)t->w_hi, (OT *)t->w_lo, c->sc);
+    }
+}
+
+// adjoint A-side weights W from c_k and Fy (hi/lo, one global scale)
 int gp_tc_build_w(gpair_ctx *c)
 {
     int rc;
     TcState *t = tc_state_ready(c, &rc);
     if (rc) return rc;
-    if (c->have_uv) {
-        // 32 groups of 4 uv points x 8 warps of BW_ROWS rows per block
-        dim3 g(gp_cdiv(t->K2_pad / 8, 32), gp_cdiv(c->N, 8 * BW_ROWS));
-        k_tc_build_w_uv<<<g, 256, 0, c->stream>>>(c->cw, c->uvc, c->pix, c->nuv, c->N, t->K2_pad, t->w_hi,
-                                                   t->w_lo, c->sc);
-    } else {
-        dim3 g(gp_cdiv(c->nuv ? c->nuv : 1, 32), gp_cdiv(c->N, 32));
-        k_tc_build_w<<<g, 256, 0, c->stream>>>(c->cw, nullptr, c->fy, c->pix, c->nuv, c->N, t->K2_pad, t->w_hi,
-                                               t->w_lo, c->sc);
-    }
+    if (t->op == OP_F16) launch_build_w<__half>(c, t);
+    else launch_build_w<float>(c, t);
     GP_LAUNCH_CHECK(c);
     return GPAIR_OK;
 }
@@ -979,20 +1129,15 @@ int gp_tc_adjoint_gemm(gpair_ctx *c)
     memset(&a, 0, sizeof(a));
     a.m_tiles = t->xrows_pad / TC_BM;  // image-column tiles (twiddle side)
     a.n_tiles = t->M_pad / TC_BN;      // image-row tiles (weight side)
-    a.kb_total = t->K2_pad / TC_BK;
+    a.kb_total = t->K2_pad / t->bk;
     a.kb_per_split = t->kb_per;
     a.units = a.m_tiles * a.n_tiles * t->splits;
     a.gpart = c->gpart;
     a.out_ld = c->N;
     a.out_rows = c->N;
     a.out_cols = c->N;
-    a.err = &c->sc->tc_err;
-    a.budget = c->tc_wait_budget > 0 ? c->tc_wait_budget : TC_WAIT_BUDGET;
-    a.skip_loads = c->tc_skip_loads;
     int grid = a.units < t->nsm ? a.units : t->nsm;
-    k_tc_gemm<EPI_STORE><<<grid, TC_THREADS, TC_SMEM_BYTES, c->stream>>>(t->m_fxt_hi, t->m_fxt_lo, t->m_w_hi,
-                                                                          t->m_w_lo, a);
-    GP_LAUNCH_CHECK(c);
+    if ((rc = tc_launch<EPI_STORE>(c, t, grid, t->m_fxt_hi, t->m_fxt_lo, t->m_w_hi, t->m_w_lo, a))) return rc;
     c->splits = t->splits;
     return GPAIR_OK;
 }

@@ -224,7 +224,8 @@ int gpair_dft_tables(int image_width, int nuv, const gpair_uv *uv, float pixella
 
 #define GPAIR_PREC_FP32 0     /* CUDA-core FP32 DFT/adjoint (FP32 twiddles) */
 #define GPAIR_PREC_SPLIT16 1  /* tcgen05 f16 hi+lo split operands, 3 products, FP32 accumulate */
-#define GPAIR_PREC_TF32 2     /* tcgen05 TF32 operands, 1 product, FP32 accumulate */
+#define GPAIR_PREC_TF32 2     /* tcgen05 kind::tf32, TF32 operands, 1 product, FP32 accumulate */
+#define GPAIR_PREC_TF32X3 3   /* tcgen05 kind::tf32, TF32 hi+lo split operands, 3 products, FP32 accumulate */
 
 #define GPAIR_IMG_CURR 0
 #define GPAIR_IMG_TEMP 1
@@ -266,7 +267,12 @@ int gpair_get_full_gradient(gpair_ctx *ctx, int which, float *grad); /* N*N */
 
 /* Device-resident CG (reference control flow, FP64 scalars kept on the GPU). */
 typedef struct {
-    int method;       /* 0 SD, 1 FR, 2 PR+, 3 HS+ */
+    int method;       /* 0 SD, 1 FR, 2 PR+, 3 HS+ (the reference's beta rules, gpair.c:733-753);
+                         4 projected L-BFGS (no reference counterpart): the newest 4 (s, y)
+                         pairs in the compact form, pixels on the positivity bound with an
+                         outward gradient held fixed; use wolfe2 = 0.9 with GPAIR_LS_WOLFE.
+                         Not available in gpair_batch_run. A checkpoint does not hold the
+                         pairs: a restored run rebuilds its history. */
     int iterations;
     float alpha;      /* entropy hyperparameter */
     double minvalue;  /* 1e-8 */

@@ -210,13 +210,21 @@ static int CG(lbfgs_init)(CG(lbfgs) *L, int n)
 
 static void CG(lbfgs_free)(CG(lbfgs) *L) { free(L->s); free(L->y); free(L->x_old); }
 
-/* new pair from the last step (x_old -> image, g_old -> g_new) */
+/* new pair from the last step (x_old -> image, g_old -> g_new); a rejected pair
+ * leaves every stored pair untouched (the candidate is formed in place only
+ * once it is accepted) */
 static void CG(lbfgs_update)(CG(lbfgs) *L, int n, const REAL *image, const REAL *g_new, const REAL *g_old)
 {
-    REAL *sk = L->s + (size_t)(L->head % LBFGS_PAIRS) * n, *yk = L->y + (size_t)(L->head % LBFGS_PAIRS) * n;
-    for (int i = 0; i < n; i++) { sk[i] = image[i] - L->x_old[i]; yk[i] = g_new[i] - g_old[i]; }
-    const double sy = CG(dot)(n, sk, yk), yy = CG(dot)(n, yk, yk), ss = CG(dot)(n, sk, sk);
+    REAL sy = 0, yy = 0, ss = 0;
+    for (int i = 0; i < n; i++) {
+        const REAL si = image[i] - L->x_old[i], yi = g_new[i] - g_old[i];
+        sy += si * yi;
+        yy += yi * yi;
+        ss += si * si;
+    }
     if (yy > 0 && sy > 1e-12 * sqrt(ss * yy)) {
+        REAL *sk = L->s + (size_t)(L->head % LBFGS_PAIRS) * n, *yk = L->y + (size_t)(L->head % LBFGS_PAIRS) * n;
+        for (int i = 0; i < n; i++) { sk[i] = image[i] - L->x_old[i]; yk[i] = g_new[i] - g_old[i]; }
         L->rho[L->head % LBFGS_PAIRS] = 1.0 / sy;
         L->gamma = sy / yy;
         L->head++;

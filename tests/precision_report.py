@@ -46,8 +46,13 @@ def _entropy64(img, model):
     return float(np.sum(np.where(ok, img - m - img * np.log(np.where(ok, img / m, 1.0)), -m)))
 
 
+_PROBLEMS = {}
+
+
 def measure(name, prec, nsel=None, npx=24, seed=5):
-    p = g.workload_problem(name)
+    if name not in _PROBLEMS:
+        _PROBLEMS[name] = g.workload_problem(name)
+    p = _PROBLEMS[name]
     rng = np.random.default_rng(seed)
     img = (p.start_image() * (1 + rng.uniform(0, 2, p.npix))).astype(np.float32)
     with g.Reconstructor(0) as rec:
@@ -58,7 +63,9 @@ def measure(name, prec, nsel=None, npx=24, seed=5):
         V = rec.visibilities()
         rec.gradient()
         grad = rec.data_gradient().astype(np.float64)
-    out = {"workload": name, "N": p.width, "nuv": p.nuv}
+        st = rec.time_stages(reps=10)  # CUDA events, stages back to back
+    out = {"workload": name, "N": p.width, "nuv": p.nuv, "forward_ms": st["forward_dft"],
+           "adjoint_ms": st["adjoint_dft"]}
     if p.width <= 64:
         e = O.evaluate64(p, img)
         out["V"] = float(np.abs(V - e["visi"]).max())
@@ -84,28 +91,42 @@ def measure(name, prec, nsel=None, npx=24, seed=5):
     return out
 
 
+MODES = ((g.PREC_FP32, "fp32 (CUDA cores)"), (g.PREC_SPLIT16, "split16 (3 f16 products)"),
+         (g.PREC_TF32, "tf32 (1 TF32 product)"), (g.PREC_TF32X3, "tf32x3 (3 TF32 products)"))
+
+
 def main():
+    import bench  # clock sampler
+
     ap = argparse.ArgumentParser()
-    ap.add_argument("--large", action="store_true", help="also the 1024^2 workload (split16)")
+    ap.add_argument("--large", action="store_true", help="also the 1024^2 workload (tensor modes)")
     args = ap.parse_args()
     rows = []
+    sampler = bench.ClockSampler(0)
+    sampler.start()
     for name in ("small", "precision"):
-        for prec, pname in ((g.PREC_FP32, "fp32"), (g.PREC_SPLIT16, "split16")):
+        for prec, pname in MODES:
             r = measure(name, prec)
             r["precision"] = pname
             rows.append(r)
     if args.large:
-        r = measure("large", g.PREC_SPLIT16, nsel=256)
-        r["precision"] = "split16"
-        rows.append(r)
-    print("| workload | precision | max abs V error | chi2 rel. error | data gradient rel. L2 error | entropy rel. error |")
-    print("|---|---|---|---|---|---|")
+        for prec, pname in MODES[1:]:
+            r = measure("large", prec, nsel=256)
+            r["precision"] = pname
+            rows.append(r)
+    clocks = sampler.stop()
+    print("| workload | precision | max abs V error | chi2 rel. error | data gradient rel. L2 error | "
+          "entropy rel. error | forward | adjoint |")
+    print("|---|---|---|---|---|---|---|---|")
     for r in rows:
         v_on = f" ({r['V_on']})" if "V_on" in r else ""
         chi = f"{r['chi2']:.2e}" if "chi2" in r else "(consistency only)"
         print(f"| {r['workload']} {r['N']}², nuv {r['nuv']} | {r['precision']} | {r['V']:.2e}{v_on} | {chi} | "
-              f"{r['grad']:.2e} ({r['grad_on']}) | {r['entropy']:.1e} |")
-    print("\nTF32 path: not built (gpair_set_precision(GPAIR_PREC_TF32) returns GPAIR_ERR_STATE).")
+              f"{r['grad']:.2e} ({r['grad_on']}) | {r['entropy']:.1e} | {r['forward_ms'] * 1e3:.1f} µs | "
+              f"{r['adjoint_ms'] * 1e3:.1f} µs |")
+    print(f"\nSM clock during the run: median {clocks.get('sm_mhz')} MHz of max {clocks.get('sm_max_mhz')} MHz, "
+          f"throttle reasons {clocks.get('reasons')} ({clocks.get('samples')} samples). Stage times: CUDA events "
+          "around the stages queued back to back (gpair_time_stages, 10 repetitions).")
 
 
 if __name__ == "__main__":

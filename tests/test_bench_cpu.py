@@ -44,8 +44,9 @@ def test_clock_sampler_without_nvidia_smi():
 
 
 def test_reference_sample_is_one_channel_indexed_by_the_reference():
-    """The CPU sample holds the middle channel of the workload's tables, indexed by
-    the reference's own getoifits.c; this project's indexer gives the same indices."""
+    """The CPU sample holds the middle channel and every SAMPLE_HA_STRIDE-th hour
+    angle of the workload's tables, indexed by the reference's own getoifits.c;
+    this project's indexer gives the same indices."""
     import os
 
     import numpy as np
@@ -60,11 +61,17 @@ def test_reference_sample_is_one_channel_indexed_by_the_reference():
     w, oi = synth.make_workload_data("tiny")
     s = bench.reference_sample("tiny", oi, width=16)
     _, oifits_mod = bench.data_modules()
-    sub = bench.subset_channels(oi, [s["channel"]], oifits_mod)
+    cfg = w.array
+    nbl, ntr = cfg.n_tel * (cfg.n_tel - 1) // 2, oi.t3[0].t3amp.shape[0] // cfg.n_ha
+    ha = np.arange(0, cfg.n_ha, bench.SAMPLE_HA_STRIDE)
+    rows_v2 = (ha[:, None] * nbl + np.arange(nbl)[None, :]).ravel()
+    rows_t3 = (ha[:, None] * ntr + np.arange(ntr)[None, :]).ravel()
+    sub = bench.subset_channels(oi, [s["channel"]], oifits_mod, rows_v2, rows_t3)
     ix = g.index_oifits(sub)
     assert s["channel"] == 1 and s["channels"] == 2 and s["width"] == 16
-    assert s["npow"] == ix.npow == oi.vis2[0].vis2data.shape[0]
-    assert s["nbis"] == ix.nbis == oi.t3[0].t3amp.shape[0]
+    assert s["npow"] == ix.npow == len(ha) * nbl
+    assert s["nbis"] == ix.nbis == len(ha) * ntr
+    assert s["data_scale"] == 2 * cfg.n_ha / len(ha)
     assert np.array_equal(s["uv"], ix.uv) and np.array_equal(s["uvpnt"], ix.uvpnt)
     assert np.array_equal(s["sign"], ix.sign)
     assert s["model"].shape == (16 * 16,)

@@ -70,7 +70,7 @@ def precision_problem():
     return g.workload_problem("precision")
 
 
-@pytest.mark.parametrize("prec", [g.PREC_FP32, g.PREC_SPLIT16])
+@pytest.mark.parametrize("prec", [g.PREC_FP32, g.PREC_SPLIT16, g.PREC_TF32X3])
 def test_precision_workload_256(precision_problem, prec):
     _check(precision_problem, prec)
 
