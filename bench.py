@@ -37,10 +37,7 @@ import argparse
 import importlib.util
 import json
 import os
-import statistics
-import subprocess
 import sys
-import threading
 import time
 import types
 
@@ -56,60 +53,6 @@ def _env_int(k, d):
         return int(os.environ.get(k, d))
     except ValueError:
         return d
-
-
-# ------------------------------------------------------------------ clocks
-
-class ClockSampler:
-    """nvidia-smi clocks and throttle reasons, sampled during the timed region."""
-
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
-
-    def __init__(self, device: int):
-        self.device = device
-        self.proc = None
-        self.lines = []
-
-    def start(self):
-        try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                                          "-lms", "200", "-i", str(self.device)], stdout=subprocess.PIPE,
-                                         stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
-        except Exception:
-            self.proc = None
-
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
-
-    def stop(self):
-        if not self.proc:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            parts = [x.strip() for x in ln.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                mx = float(parts[2])
-            except ValueError:
-                continue
-            for n, v in zip(names, parts[5:9]):
-                if v.lower() == "active":
-                    reasons.add(n)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
 
 
 # ----------------------------------------------------------- measurements
@@ -453,7 +396,7 @@ def many_instances(n: int, iters: int) -> dict:
             "unit": "s (host wall clock)", "line_search": "batched"}
 
 
-def time_to_objective(n_problems: int, race_fr: bool = False) -> dict:
+def time_to_objective(n_problems: int, race_fr: bool = False, method: int = 2) -> dict:
     """CG time-to-objective on held-out problems of the warm-start workload (3/4
     at 64x64, 1/4 at 128x128): wall time until J <= J* (1 + 1e-4), J* = plain
     CG's converged objective (reference line search, 1000 iterations), for plain
@@ -472,21 +415,22 @@ def time_to_objective(n_problems: int, race_fr: bool = False) -> dict:
         for k in range(n_problems):
             p = training_case(SEED_HELD_OUT + k, 64 if k < n64 else 128).problem
             rows.append(TT.evaluate(rec, p, net, iters=1000, objective_from="plain", rec2=rec2, flag=flag,
-                                    rec3=rec3 if race_fr else None))
+                                    rec3=rec3 if race_fr else None, method=method))
     flag.close()
     out = TT.summarize(rows)
     out["unit"] = "s (sum of host wall clock over the problems)"
     out["workload"] = (f"{n_problems} held-out seeded problems ({n64} at 64x64 / 0.1 mas, {n_problems - n64} at "
                        "128x128 / 0.05 mas; 1-10 Gaussians/disks/points, 4-12 telescopes), tolerance 1e-4")
+    out["direction"] = {2: "PR+ CG", 4: "projected L-BFGS"}[method] + " with the batched line search (batch, warm, race)"
     return out
 
 
-def time_to_objective_workload(rec, p, iters: int, batch_iters: int) -> dict:
+def time_to_objective_workload(rec, p, iters: int, batch_iters: int, method: int = 2) -> dict:
     """Time-to-objective on the benchmark workload itself: plain CG (reference
     line search) for `iters` iterations sets J*, then plain CG and the batched
     line search are each timed from the flat prior to J* (1 + 1e-4)."""
     from gpair_b200 import timetoobj as TT
-    row = TT.evaluate(rec, p, None, iters=iters, batch_iters=batch_iters, objective_from="plain")
+    row = TT.evaluate(rec, p, None, iters=iters, batch_iters=batch_iters, objective_from="plain", method=method)
     row["speedup_batch_vs_plain"] = row["plain_s"] / max(row["batch_s"], 1e-12)
     row["unit"] = "s (host wall clock)"
     row["note"] = f"J* = lowest J of {iters} plain PR+ iterations with the reference's line search"
@@ -497,6 +441,7 @@ def measure_plain(rec, p, args, flush, local, dist):
     """Timed plain CG iterations (device time, CUDA events inside the library),
     their per-stage times and the e2e leg through the public API."""
     import torch
+    from gpair_b200.clocks import ClockSampler
     rec.cg(max(args.warmup, 1), method=2, resume=False, host_loop=int(args.host_loop),
            line_search=LS[args.line_search])  # untimed warm-up; builds the CG graph
     sampler = ClockSampler(local)
@@ -681,7 +626,7 @@ def run_ours(args, rank, world, local):
             line["cpu_baseline"] = cpu_baseline(reference_sample(args.workload, oi))
         if not args.no_time_to_objective and args.tto_workload_iters > 0:
             line["time_to_objective_workload"] = time_to_objective_workload(
-                rec, p, args.tto_workload_iters, args.tto_workload_iters)
+                rec, p, args.tto_workload_iters, args.tto_workload_iters, args.tto_method)
     rec.close()
     del oi, p
 
@@ -707,7 +652,8 @@ def run_ours(args, rank, world, local):
                                                                "precision")
                 line["precision_256"] = blk
         if not args.no_time_to_objective:
-            line["time_to_objective"] = time_to_objective(args.tto_problems, race_fr=args.tto_race_fr)
+            line["time_to_objective"] = time_to_objective(args.tto_problems, race_fr=args.tto_race_fr,
+                                                          method=args.tto_method)
         if args.instances > 0:
             line["many_instances"] = many_instances(args.instances, args.instance_iters)
         print(json.dumps(line), flush=True)
@@ -737,6 +683,9 @@ def main():
     ap.add_argument("--tto-workload-iters", type=int, default=60,
                     help="plain-CG iterations that set J* for the time-to-objective block on the benchmark "
                          "workload itself (0: skip)")
+    ap.add_argument("--tto-method", type=int, choices=[2, 4], default=2,
+                    help="direction of the batched / warm-start runs in the time-to-objective blocks: 2 PR+ CG, "
+                         "4 projected L-BFGS")
     ap.add_argument("--tto-race-fr", action="store_true",
                     help="add a flat-start Fletcher-Reeves runner to the time-to-objective race")
     ap.add_argument("--host-loop", action="store_true",

@@ -428,10 +428,30 @@ __global__ void k_tc_twiddle_ops(const float2 *__restrict__ fx, int nuv, int N, 
 }
 
 // Image operand: one global power-of-two scale 2^(15 - e), e = exponent of
-// max |image| (reduced by k_prep), then an f16 hi/lo split; one block per
-// padded row. Block 0 publishes the factor the forward epilogue removes.
+// max |image| (reduced by k_prep), then the hi/lo split. One thread per 8
+// consecutive elements of a padded row: 16-byte (f16) or 2 x 16-byte (TF32)
+// stores of hi and of lo. Thread 0 publishes the factor the forward epilogue
+// removes.
 template <typename OT>
-__global__ void __launch_bounds__(256) k_tc_split_image(const float *__restrict__ img, int N, int Kx_pad,
+__device__ __forceinline__ void split_store8(OT *__restrict__ hi, OT *__restrict__ lo, size_t off, const float (&v)[8])
+{
+    __align__(16) OT h[8];
+    __align__(16) OT l[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) OpSplit<OT>::split(v[j], h[j], l[j]);
+    constexpr int NV = sizeof(OT) * 8 / 16;
+    uint4 *ph = reinterpret_cast<uint4 *>(hi + off);
+#pragma unroll
+    for (int k = 0; k < NV; k++) ph[k] = reinterpret_cast<const uint4 *>(h)[k];
+    if (lo) {
+        uint4 *pl = reinterpret_cast<uint4 *>(lo + off);
+#pragma unroll
+        for (int k = 0; k < NV; k++) pl[k] = reinterpret_cast<const uint4 *>(l)[k];
+    }
+}
+
+template <typename OT>
+__global__ void __launch_bounds__(256) k_tc_split_image(const float *__restrict__ img, int N, int M_pad, int Kx_pad,
                                                         OT *__restrict__ hi, OT *__restrict__ lo,
                                                         DevScalars *__restrict__ sc)
 {
@@ -442,12 +462,17 @@ __global__ void __launch_bounds__(256) k_tc_split_image(const float *__restrict_
         frexp(mx, &ex);  // mx in [2^(ex-1), 2^ex)
         scale = ldexpf(1.f, 15 - ex);
     }
-    const int y = blockIdx.x;
-    for (int x = threadIdx.x; x < Kx_pad; x += blockDim.x) {
-        float v = (y < N && x < N) ? img[(size_t)y * N + x] * scale : 0.f;
-        split_store(hi, lo, (size_t)y * Kx_pad + x, v);
+    const int g8 = Kx_pad >> 3;  // groups of 8 per padded row
+    const long long total = (long long)M_pad * g8;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < total;
+         q += (long long)gridDim.x * blockDim.x) {
+        const int y = (int)(q / g8), x = (int)(q - (long long)y * g8) << 3;
+        float v[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) v[j] = (y < N && x + j < N) ? img[(size_t)y * N + x + j] * scale : 0.f;
+        split_store8(hi, lo, (size_t)y * Kx_pad + x, v);
     }
-    if (y == 0 && threadIdx.x == 0) sc->fwd_inv_scale = mx > 0.0 ? ldexpf(1.f, ex - 15 - TC_TW_LOG2) : 0.f;
+    if (blockIdx.x == 0 && threadIdx.x == 0) sc->fwd_inv_scale = mx > 0.0 ? ldexpf(1.f, ex - 15 - TC_TW_LOG2) : 0.f;
 }
 
 // Trial image + f16 split in one pass (line-search trials): I_t = max(I + s d,
@@ -470,17 +495,49 @@ __global__ void __launch_bounds__(GP_THREADS) k_tc_prep_split_trial(
     const float scale = ldexpf(1.f, 15 - ex);
     double acc[2] = {0.0, 0.0};
     double mx = 0.0;
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
-        double t = (double)img[p] + s * (double)d[p];
-        if (t < minval) t = minval;
-        const float I = (float)t;
-        dst[p] = I;
-        const double Id = I, m = model[p];
-        acc[0] += Id;
-        acc[1] += reg_term(Id, m, sc->reg_kind);
-        mx = fmax(mx, fabs(Id));
-        const int y = p / N, x = p - y * N;
-        split_store(hi, lo, (size_t)y * Kx_pad + x, I * scale);
+    const int reg_kind = sc->reg_kind;
+    if ((N & 7) == 0) {
+        // 8 consecutive pixels of one row per thread: 16-byte loads and stores
+        const int n8 = npix >> 3;
+        for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n8; q += gridDim.x * blockDim.x) {
+            const int p0 = q << 3;
+            float iv[8], dv[8], mv[8], out[8], v[8];
+            *reinterpret_cast<float4 *>(&iv[0]) = __ldg(reinterpret_cast<const float4 *>(img + p0));
+            *reinterpret_cast<float4 *>(&iv[4]) = __ldg(reinterpret_cast<const float4 *>(img + p0 + 4));
+            *reinterpret_cast<float4 *>(&dv[0]) = __ldg(reinterpret_cast<const float4 *>(d + p0));
+            *reinterpret_cast<float4 *>(&dv[4]) = __ldg(reinterpret_cast<const float4 *>(d + p0 + 4));
+            *reinterpret_cast<float4 *>(&mv[0]) = __ldg(reinterpret_cast<const float4 *>(model + p0));
+            *reinterpret_cast<float4 *>(&mv[4]) = __ldg(reinterpret_cast<const float4 *>(model + p0 + 4));
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                double t = (double)iv[j] + s * (double)dv[j];
+                if (t < minval) t = minval;
+                const float I = (float)t;
+                out[j] = I;
+                const double Id = I;
+                acc[0] += Id;
+                acc[1] += reg_term(Id, (double)mv[j], reg_kind);
+                mx = fmax(mx, fabs(Id));
+                v[j] = I * scale;
+            }
+            *reinterpret_cast<float4 *>(dst + p0) = *reinterpret_cast<const float4 *>(&out[0]);
+            *reinterpret_cast<float4 *>(dst + p0 + 4) = *reinterpret_cast<const float4 *>(&out[4]);
+            const int y = p0 / N, x = p0 - y * N;
+            split_store8(hi, lo, (size_t)y * Kx_pad + x, v);
+        }
+    } else {
+        for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
+            double t = (double)img[p] + s * (double)d[p];
+            if (t < minval) t = minval;
+            const float I = (float)t;
+            dst[p] = I;
+            const double Id = I, m = model[p];
+            acc[0] += Id;
+            acc[1] += reg_term(Id, m, reg_kind);
+            mx = fmax(mx, fabs(Id));
+            const int y = p / N, x = p - y * N;
+            split_store(hi, lo, (size_t)y * Kx_pad + x, I * scale);
+        }
     }
     block_sum<2>(acc, smem);
     mx = block_max(mx, smem);
@@ -1054,12 +1111,15 @@ int gp_tc_split(gpair_ctx *c, int which)
     TcState *t = tc_state_ready(c, &rc);
     if (rc) return rc;
     const float *img = (which == GPAIR_IMG_TEMP) ? c->image_temp : c->image;
+    long long groups = (long long)t->M_pad * (t->Kx_pad >> 3);
+    int grid = gp_cdiv(groups, 256);
+    if (grid > 8 * t->nsm) grid = 8 * t->nsm;
     if (t->op == OP_F16)
-        k_tc_split_image<__half><<<t->M_pad, 256, 0, c->stream>>>(img, c->N, t->Kx_pad, (__half *)t->img_hi,
-                                                                   (__half *)t->img_lo, c->sc);
+        k_tc_split_image<__half><<<grid, 256, 0, c->stream>>>(img, c->N, t->M_pad, t->Kx_pad, (__half *)t->img_hi,
+                                                               (__half *)t->img_lo, c->sc);
     else
-        k_tc_split_image<float><<<t->M_pad, 256, 0, c->stream>>>(img, c->N, t->Kx_pad, (float *)t->img_hi,
-                                                                  (float *)t->img_lo, c->sc);
+        k_tc_split_image<float><<<grid, 256, 0, c->stream>>>(img, c->N, t->M_pad, t->Kx_pad, (float *)t->img_hi,
+                                                              (float *)t->img_lo, c->sc);
     GP_LAUNCH_CHECK(c);
     return GPAIR_OK;
 }
@@ -1078,8 +1138,10 @@ int gp_tc_prep_split_trial(gpair_ctx *c)
     TcState *t = tc_state_ready(c, &rc);
     if (rc) return rc;
     // at most GP_MAX_PARTIALS blocks: 3 partials each fit the RED_PREP slot
-    int g = gp_cdiv(c->npix, GP_THREADS);
+    const int per_thread = (c->N & 7) == 0 ? 8 : 1;
+    int g = gp_cdiv(c->npix / per_thread, GP_THREADS);
     if (g > GP_MAX_PARTIALS) g = GP_MAX_PARTIALS;
+    if (g < 1) g = 1;
     if (t->op == OP_F16)
         k_tc_prep_split_trial<__half><<<g, GP_THREADS, 0, c->stream>>>(
             c->image, c->descent_dir, c->image_temp, c->model, c->N, c->npix, t->Kx_pad, (__half *)t->img_hi,

@@ -2,6 +2,12 @@
 evaluation, for the named workloads.
 
     python -m gpair_b200.stage_report [--workloads precision large] [--reps 10]
+    python -m gpair_b200.stage_report --workloads large --cg 1 [--method 2] [--line-search 0]
+
+With --cg N the module instead runs N CG iterations from the flat prior,
+driven from the host (every kernel a plain launch, so that a profiler's
+launch list shows each one), and prints the evaluation counts: the command
+for launch lists of one CG iteration.
 
 Stages and time: `Reconstructor.time_stages` (CUDA events around the stages
 queued back to back), split-f16 tensor path.
@@ -45,6 +51,7 @@ def stage_bytes(p: api.Problem, splits: int, row_tiles: int) -> dict:
 
 
 def report(name: str, reps: int = 10) -> dict:
+    from .clocks import ClockSampler
     p = api.workload_problem(name)
     with api.Reconstructor(0) as rec:
         rec.set_problem(p)
@@ -52,7 +59,13 @@ def report(name: str, reps: int = 10) -> dict:
         rec.set_image(p.start_image())
         rec.criterion()
         rec.gradient()
+        sampler = ClockSampler(0)
+        sampler.start()
         st = rec.time_stages(reps=reps)
+        for _ in range(4):  # long enough for a few 200 ms clock samples
+            st2 = rec.time_stages(reps=reps)
+            st = {k: min(st[k], st2[k]) for k in st}
+        clocks = sampler.stop()
     peaks_path = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "MEASURED_PEAKS.json")
     hbm, tf = 6650.0, 1590.0
     if os.path.exists(peaks_path):
@@ -63,7 +76,8 @@ def report(name: str, reps: int = 10) -> dict:
     splits = _default_splits(p)
     by = stage_bytes(p, splits, row_tiles)
     out = {"workload": name, "N": p.width, "nuv": p.nuv, "npow": p.npow, "nbis": p.nbis, "splits": splits,
-           "hbm_peak_gbs": hbm, "tensor_peak_tflops": tf, "stages": {}}
+           "hbm_peak_gbs": hbm, "tensor_peak_tflops": tf, "clocks": clocks,
+           "timing": f"CUDA events, stages back to back, best of 5 x {reps} repetitions", "stages": {}}
     for k, ms in st.items():
         row = {"ms": ms}
         if k in by:
@@ -93,8 +107,22 @@ def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--workloads", nargs="+", default=["precision", "large"])
     ap.add_argument("--reps", type=int, default=10)
+    ap.add_argument("--cg", type=int, default=0, help="run this many host-driven CG iterations instead")
+    ap.add_argument("--method", type=int, default=2)
+    ap.add_argument("--line-search", type=int, default=0, help="0 the reference's search, 1 batched")
+    ap.add_argument("--precision", type=int, default=api.PREC_SPLIT16)
     args = ap.parse_args(argv)
     for w in args.workloads:
+        if args.cg > 0:
+            p = api.workload_problem(w)
+            with api.Reconstructor(0) as rec:
+                rec.set_problem(p)
+                rec.set_precision(args.precision)
+                rec.set_image(p.start_image())
+                out = rec.cg(args.cg, method=args.method, line_search=args.line_search, host_loop=1)
+            print(json.dumps({"workload": w, "iterations": out["iterations"], "criterion_evals": out["criterion_evals"],
+                              "grad_evals": out["grad_evals"], "J": out["J"]}), flush=True)
+            continue
         print(json.dumps(report(w, args.reps)), flush=True)
 
 

@@ -32,15 +32,15 @@ import numpy as np
 from . import api
 
 
-def _timed_cg(rec, start, iters, line_search, target):
+def _timed_cg(rec, start, iters, line_search, target, method=2):
     rec.set_image(start)
     t0 = time.perf_counter()
-    out = rec.cg(iters, method=2, line_search=line_search, target_J=target)
+    out = rec.cg(iters, method=method, line_search=line_search, target_J=target)
     return time.perf_counter() - t0, out
 
 
 def race(rec: api.Reconstructor, rec2: api.Reconstructor, p: api.Problem, net, iters: int, target: float,
-         flag: api.StopFlag, rec3: Optional[api.Reconstructor] = None) -> Dict:
+         flag: api.StopFlag, rec3: Optional[api.Reconstructor] = None, method: int = 2) -> Dict:
     """Warm start in `rec` against the flat prior in `rec2` (both hold problem p).
     With `rec3` (also holding p), a third runner starts from the flat prior with
     the Fletcher-Reeves beta: on ill-conditioned problems the beta rule moves
@@ -56,14 +56,14 @@ def race(rec: api.Reconstructor, rec2: api.Reconstructor, p: api.Problem, net, i
         res[key] = r.cg(iters, method=method, line_search=g.LS_BATCH, target_J=target, stop_flag=flag.ptr)
 
     t0 = time.perf_counter()
-    threads = [threading.Thread(target=flat, args=(rec2, "flat", 2))]
+    threads = [threading.Thread(target=flat, args=(rec2, "flat", method))]
     if rec3 is not None:
         threads.append(threading.Thread(target=flat, args=(rec3, "flat_fr", 1)))
     for th in threads:
         th.start()
     img = warm_start(net, rec, p, features(rec, p))
     rec.set_image(img)
-    warm = rec.cg(iters, method=2, line_search=g.LS_BATCH, target_J=target, stop_flag=flag.ptr)
+    warm = rec.cg(iters, method=method, line_search=g.LS_BATCH, target_J=target, stop_flag=flag.ptr)
     for th in threads:
         th.join()
     dt = time.perf_counter() - t0
@@ -81,55 +81,57 @@ def race(rec: api.Reconstructor, rec2: api.Reconstructor, p: api.Problem, net, i
 def evaluate(rec: api.Reconstructor, p: api.Problem, net=None, iters: int = 1000, tol: float = 1e-4,
              batch_iters: Optional[int] = None, objective_from: str = "plain",
              rec2: Optional[api.Reconstructor] = None, flag: Optional[api.StopFlag] = None,
-             rec3: Optional[api.Reconstructor] = None) -> Dict:
+             rec3: Optional[api.Reconstructor] = None, method: int = 2) -> Dict:
     """objective_from "plain": J* from the reference line search (the headline
     comparison); "batch": J* from the batched line search run for batch_iters
-    iterations from the flat prior (isolates what the network adds)."""
+    iterations from the flat prior (isolates what the network adds). `method`
+    is the direction of the batched, warm and race runs (2: PR+ CG, 4:
+    projected L-BFGS); plain CG is always PR+ with the reference's search."""
     import gpair_b200 as g
     from .warmstart import features, warm_start
     rec.set_problem(p)
     start = p.start_image()
     bi = batch_iters or iters
     # capture both line-search graphs outside the timed runs (one CUDA graph per mode is cached)
-    for ls in (g.LS_WOLFE, g.LS_BATCH):
+    for ls, m in ((g.LS_WOLFE, 2), (g.LS_BATCH, method)):
         rec.set_image(start)
-        rec.cg(1, method=2, line_search=ls)
+        rec.cg(1, method=m, line_search=ls)
     rec.set_image(start)
     if objective_from == "plain":
         ref = rec.cg(iters, method=2, trace=True, line_search=g.LS_WOLFE)
     else:
-        ref = rec.cg(bi, method=2, trace=True, line_search=g.LS_BATCH)
+        ref = rec.cg(bi, method=method, trace=True, line_search=g.LS_BATCH)
     Jstar = float(np.min(ref["trace_J"][:ref["iterations"]]))
     target = Jstar * (1.0 + tol) if Jstar > 0 else Jstar * (1.0 - tol)
     res = {"width": p.width, "nuv": p.nuv, "J_star": Jstar, "target": target, "objective_from": objective_from}
     if objective_from == "plain":
         t_plain, o_plain = _timed_cg(rec, start, iters, g.LS_WOLFE, target)
         res.update({"plain_s": t_plain, "plain_iters": o_plain["iterations"], "plain_reached": o_plain["reached"]})
-    t_batch, o_batch = _timed_cg(rec, start, bi, g.LS_BATCH, target)
+    t_batch, o_batch = _timed_cg(rec, start, bi, g.LS_BATCH, target, method)
     res.update({"batch_s": t_batch, "batch_iters": o_batch["iterations"], "batch_reached": o_batch["reached"]})
     if net is not None:
         t0 = time.perf_counter()
         f = features(rec, p)
         img = warm_start(net, rec, p, f)
         t_net = time.perf_counter() - t0
-        t_cg, o_warm = _timed_cg(rec, img, bi, g.LS_BATCH, target)
+        t_cg, o_warm = _timed_cg(rec, img, bi, g.LS_BATCH, target, method)
         fell_back = not o_warm["reached"]
         t_fb = 0.0
         if fell_back:
-            t_fb, _ = _timed_cg(rec, start, bi, g.LS_BATCH, target)
+            t_fb, _ = _timed_cg(rec, start, bi, g.LS_BATCH, target, method)
         res.update({"warm_s": t_net + t_cg + t_fb, "warm_net_s": t_net, "warm_iters": o_warm["iterations"],
                     "warm_reached": o_warm["reached"], "fallback": fell_back})
         if rec2 is not None and flag is not None:
             rec2.set_problem(p)
             rec2.set_precision(rec_precision(rec))
             rec2.set_image(start)
-            rec2.cg(1, method=2, line_search=g.LS_BATCH)  # graph capture outside the timed race
+            rec2.cg(1, method=method, line_search=g.LS_BATCH)  # graph capture outside the timed race
             if rec3 is not None:
                 rec3.set_problem(p)
                 rec3.set_precision(rec_precision(rec))
                 rec3.set_image(start)
                 rec3.cg(1, method=1, line_search=g.LS_BATCH)
-            res.update(race(rec, rec2, p, net, bi, target, flag, rec3))
+            res.update(race(rec, rec2, p, net, bi, target, flag, rec3, method))
     return res
 
 
@@ -188,6 +190,12 @@ def main(argv=None):
     ap.add_argument("--batch-iters", type=int, default=1500)
     ap.add_argument("--weights", default=DEFAULT_WEIGHTS)
     ap.add_argument("--out", default=None)
+    ap.add_argument("--method", type=int, choices=[2, 4], default=2,
+                    help="direction of the batched, warm and race runs (2 PR+, 4 projected L-BFGS)")
+    ap.add_argument("--objectives", nargs="+", choices=["plain", "batch"], default=["plain", "batch"],
+                    help="J* definitions to evaluate: plain CG's converged objective (the headline) and/or the "
+                         "batched search's own (isolates what the network adds)")
+    ap.add_argument("--first", type=int, default=0, help="index of the first held-out problem")
     ap.add_argument("--workload", default=None,
                     help="a named workload (gpair_b200.synth) instead of the held-out warm-start problems: plain "
                          "CG against the batched line search, no network")
@@ -196,22 +204,25 @@ def main(argv=None):
         p = api.workload_problem(args.workload)
         with g.Reconstructor(0) as rec:
             rec.set_precision(g.PREC_SPLIT16)
-            row = evaluate(rec, p, None, iters=args.iters, batch_iters=args.batch_iters, objective_from="plain")
+            row = evaluate(rec, p, None, iters=args.iters, batch_iters=args.batch_iters, objective_from="plain",
+                           method=args.method)
         print("SUMMARY", json.dumps(row), flush=True)
         return
     net = WarmStartNet.load(args.weights)
-    rows = {"plain": [], "batch": []}
+    rows = {k: [] for k in args.objectives}
     flag = api.StopFlag()
     with g.Reconstructor(0) as rec, g.Reconstructor(0) as rec2:
         rec.set_precision(g.PREC_SPLIT16)
-        for k in range(args.n64 + args.n128):
-            p = training_case(SEED_HELD_OUT + k, 64 if k < args.n64 else 128).problem
-            rows["plain"].append(evaluate(rec, p, net, iters=args.iters, objective_from="plain", rec2=rec2,
-                                          flag=flag))
-            rows["batch"].append(evaluate(rec, p, net, iters=args.iters, batch_iters=args.batch_iters,
-                                          objective_from="batch", rec2=rec2, flag=flag))
+        for k in range(args.first, args.first + args.n64 + args.n128):
+            width = 64 if k - args.first < args.n64 else 128
+            p = training_case(SEED_HELD_OUT + k, width).problem
+            for obj in args.objectives:
+                r = evaluate(rec, p, net, iters=args.iters, batch_iters=args.batch_iters if obj == "batch" else None,
+                             objective_from=obj, rec2=rec2, flag=flag, method=args.method)
+                r["seed"] = SEED_HELD_OUT + k
+                rows[obj].append(r)
     flag.close()
-    for k in ("plain", "batch"):
+    for k in args.objectives:
         print(f"SUMMARY {k}", json.dumps(summarize(rows[k])), flush=True)
     if args.out:
         with open(args.out, "w") as f:

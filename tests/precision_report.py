@@ -96,13 +96,13 @@ MODES = ((g.PREC_FP32, "fp32 (CUDA cores)"), (g.PREC_SPLIT16, "split16 (3 f16 pr
 
 
 def main():
-    import bench  # clock sampler
+    from gpair_b200.clocks import ClockSampler
 
     ap = argparse.ArgumentParser()
     ap.add_argument("--large", action="store_true", help="also the 1024^2 workload (tensor modes)")
     args = ap.parse_args()
     rows = []
-    sampler = bench.ClockSampler(0)
+    sampler = ClockSampler(0)
     sampler.start()
     for name in ("small", "precision"):
         for prec, pname in MODES:

@@ -1,5 +1,6 @@
 """Host-side pieces of bench.py that need no GPU."""
 import bench
+from gpair_b200.clocks import ClockSampler
 
 
 class _FakeProc:
@@ -14,7 +15,7 @@ class _FakeProc:
 
 
 def _sampler(lines):
-    s = bench.ClockSampler(0)
+    s = ClockSampler(0)
     s.proc = _FakeProc()
     s.lines = list(lines)
     return s
@@ -39,7 +40,7 @@ def test_clock_sampler_reports_thermal_and_hw_slowdown():
 
 
 def test_clock_sampler_without_nvidia_smi():
-    s = bench.ClockSampler(0)
+    s = ClockSampler(0)
     assert s.stop()["reasons"] == ["nvidia-smi unavailable"]
 
 
