@@ -587,6 +587,7 @@ def run_ours(args, rank, world, local):
     rec = g.Reconstructor(local)
     rec.set_problem(p)
     rec.set_precision(prec)
+    rec.set_tc_pair(args.tc_pair)
     rec.set_stage_timing(True)
     rec.set_image(p.start_image())
     # autotuned adjoint split-K length (precision stays as requested)
@@ -611,6 +612,8 @@ def run_ours(args, rank, world, local):
                                     if args.line_search == "wolfe" else
                                     "one PR+ CG iteration with the batched 8-trial line search (continuing)"),
                            "precision": args.precision, "evaluations": m["evals"],
+                           "tensor_tiles": "CTA pairs (cta_group::2, 256x256)" if args.tc_pair else
+                           "single CTAs (128x256)",
                            "criterion_evals": m["crit_evals"], "grad_evals": m["grad_evals"],
                            "flop_per_evaluation": p.dft_flops(),
                            "autotuned_adjoint_splits": tune["adjoint_splits"],
@@ -637,6 +640,7 @@ def run_ours(args, rank, world, local):
             with g.Reconstructor(local) as r2:
                 r2.set_problem(p2)
                 r2.set_precision(prec)
+                r2.set_tc_pair(args.tc_pair)
                 r2.set_stage_timing(True)
                 r2.set_image(p2.start_image())
                 r2.autotune(g.api.TUNE_SPLITS, reps=3)
@@ -670,6 +674,8 @@ def main():
     ap.add_argument("--workload", default="large", choices=["large", "precision", "small", "tiny"])
     ap.add_argument("--precision", default=os.environ.get("GPAIR_BENCH_PRECISION", "split16"),
                     choices=["fp32", "split16"])
+    ap.add_argument("--tc-pair", type=int, choices=[0, 1], default=0,
+                    help="tensor-core contractions on CTA pairs (cta_group::2) instead of single CTAs")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-time-to-objective", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched line-search block")

@@ -134,6 +134,8 @@ def lib() -> C.CDLL:
         L.gpair_time_batch_stages.argtypes = [vp, i, C.POINTER(d), i]
         L.gpair_set_stage_timing.argtypes = [vp, i]
         L.gpair_set_tc_wait.argtypes = [vp, C.c_longlong, i]
+        L.gpair_set_tc_pair.argtypes = [vp, i]
+        L.gpair_get_tc_pair.argtypes = [vp]
         L.gpair_last_run_stage_ms.argtypes = [vp, C.POINTER(d), C.POINTER(i), i]
         L.gpair_get_oi_fits_data.argtypes = [i, f, f, i, vp, i, vp, i, vp, C.POINTER(OiData)]
         L.gpair_free_oi_data.argtypes = [C.POINTER(OiData)]
@@ -442,6 +444,10 @@ class Reconstructor:
         self._c(self._L.gpair_set_problem(self.h, p.width, p.pixellation, p.nuv, _p(k[0]), p.npow, p.nbis, _p(k[1]),
                                           _p(k[2]), _p(k[3]), _p(k[4]), _p(k[5]), _p(k[6])))
         self.problem = p
+
+    def set_tc_pair(self, on: bool = True):
+        """Tensor-core contractions on CTA pairs (cta_group::2) or single CTAs."""
+        self._c(self._L.gpair_set_tc_pair(self.h, 1 if on else 0))
 
     def set_precision(self, mode: int):
         self._c(self._L.gpair_set_precision(self.h, mode))

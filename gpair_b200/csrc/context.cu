@@ -363,6 +363,17 @@ static void stage_collect(gpair_ctx *c)
     c->st_n = 0;
 }
 
+extern "C" int gpair_set_tc_pair(gpair_ctx *c, int on)
+{
+    if (!c) return GPAIR_ERR_INVALID;
+    c->tc_pair = on ? 1 : 0;
+    gp_cg_graph_free(c);  // captured graphs hold the other kernel variant
+    if (c->precision != GPAIR_PREC_FP32 && c->have_problem && c->have_uv) return gp_tc_prepare(c);
+    return GPAIR_OK;
+}
+
+extern "C" int gpair_get_tc_pair(gpair_ctx *c) { return c ? c->tc_pair : -1; }
+
 extern "C" int gpair_set_tc_wait(gpair_ctx *c, long long budget_cycles, int skip_loads)
 {
     if (!c || budget_cycles < 0) return GPAIR_ERR_INVALID;

@@ -242,6 +242,8 @@ struct gpair_ctx {
     // the MMA and epilogue waits run out with no copy in flight
     long long tc_wait_budget;
     int tc_skip_loads;
+    // tensor-core contractions on CTA pairs (tcgen05 cta_group::2) instead of single CTAs
+    int tc_pair;
 };
 
 // ---------------------------------------------------------------- helpers
@@ -319,7 +321,7 @@ int gp_tc_split(gpair_ctx *c, int which);
 int gp_tc_build_w(gpair_ctx *c);
 int gp_tc_adjoint_gemm(gpair_ctx *c);
 int gp_tc_prep_split_trial(gpair_ctx *c);
-int gp_tc_splits(int N, int nuv, int nsm, int bk, int *kb_per_out);
+int gp_tc_splits(int N, int nuv, int nsm, int bk, int pair, int *kb_per_out);
 int gp_lbfgs_alloc(gpair_ctx *c);
 void gp_lbfgs_free(gpair_ctx *c);
 int gp_lbfgs_direction(gpair_ctx *c);

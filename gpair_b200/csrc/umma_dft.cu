@@ -129,6 +129,9 @@ struct TcState {
     int nanc;
     CUtensorMap m_img_hi, m_img_lo, m_fx_hi, m_fx_lo, m_w_hi, m_w_lo, m_fxt_hi, m_fxt_lo;
     int nsm;
+    // CTA pairs (cta_group::2): B maps with 128-row boxes, A row counts padded
+    // to 256; npairs = clusters of two that are resident at once
+    int pair, npairs;
 };
 
 static inline int round_up(long long a, long long b) { return (int)(((a + b - 1) / b) * b); }
@@ -159,42 +162,70 @@ __device__ __forceinline__ void tc_decode(const TcArgs &a, int u, int &m, int &n
     }
 }
 
-template <int EPI, int OP, int NPROD>
+// PAIR = 0: one CTA per tile of 128 (A rows) x 256 (B rows), 2 stages of 96 KB.
+// PAIR = 1: a cluster of two CTAs shares one tcgen05.mma.cta_group::2 tile of
+// 256 x 256: each CTA stages 128 rows of A and 128 rows of B (half of the tile's
+// B) per K-block in its own shared memory, 3 stages of 64 KB, and holds 128
+// TMEM lanes of the accumulator. The even CTA issues the MMAs; the odd CTA's
+// TMA loads report to the even CTA's full barriers, the MMA commits release
+// the stages of both CTAs, and both CTAs' epilogues release the even CTA's
+// accumulator buffers. Per SM the operand traffic per MMA drops by a third.
+template <int PAIR> struct TcGeo {
+    static constexpr int MT = PAIR ? 256 : 128;          // M rows per tile (per unit)
+    static constexpr int BROWS = PAIR ? 128 : 256;       // B rows staged per CTA
+    static constexpr int B_BYTES = BROWS * TC_ROWB;
+    static constexpr int STAGE = 2 * TC_A_BYTES + 2 * B_BYTES;
+    static constexpr int STAGES = PAIR ? 3 : 2;
+};
+static_assert(TcGeo<0>::STAGES * TcGeo<0>::STAGE == TcGeo<1>::STAGES * TcGeo<1>::STAGE, "same smem in both modes");
+
+template <int EPI, int OP, int NPROD, int PAIR>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     k_tc_gemm(const __grid_constant__ CUtensorMap tA_hi, const __grid_constant__ CUtensorMap tA_lo,
               const __grid_constant__ CUtensorMap tB_hi, const __grid_constant__ CUtensorMap tB_lo, const TcArgs a)
 {
+    using G = TcGeo<PAIR>;
     extern __shared__ unsigned char smem_raw[];
     unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     unsigned char *stages = smem;
-    uint64_t *full = (uint64_t *)(smem + TC_STAGES * TC_STAGE_BYTES);
-    uint64_t *empty = full + TC_STAGES;
-    uint64_t *tfull = empty + TC_STAGES;
+    uint64_t *full = (uint64_t *)(smem + G::STAGES * G::STAGE);
+    uint64_t *empty = full + G::STAGES;
+    uint64_t *tfull = empty + G::STAGES;
     uint64_t *tempty = tfull + 2;
     uint64_t *done_bar = tempty + 2;
     uint32_t *tmem_slot = (uint32_t *)(done_bar + 1);
     volatile int *abort_flag = (volatile int *)(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t rank = PAIR ? umma::cluster_ctarank() : 0u;
+    const bool leader = rank == 0;
+    const int unit0 = PAIR ? (int)(blockIdx.x >> 1) : (int)blockIdx.x;  // this CTA's (pair's) first unit
+    const int ustep = PAIR ? (int)(gridDim.x >> 1) : (int)gridDim.x;
     if (threadIdx.x == 0) {
-        for (int s = 0; s < TC_STAGES; s++) {
+        for (int s = 0; s < G::STAGES; s++) {
             umma::mbar_init(&full[s], 1);
             umma::mbar_init(&empty[s], 1);
         }
         for (int b = 0; b < 2; b++) {
             umma::mbar_init(&tfull[b], 1);
-            umma::mbar_init(&tempty[b], 128);
+            umma::mbar_init(&tempty[b], PAIR ? 256 : 128);  // pair: both CTAs' epilogues release
         }
         umma::mbar_init(done_bar, 1);
         *abort_flag = 0;
         umma::fence_barrier_init();
     }
     if (warp == 1) {
-        umma::tmem_alloc(tmem_slot, TC_TMEM_COLS);
-        umma::tmem_relinquish();
+        if (PAIR) {
+            umma::tmem_alloc_pair(tmem_slot, TC_TMEM_COLS);
+            umma::tmem_relinquish_pair();
+        } else {
+            umma::tmem_alloc(tmem_slot, TC_TMEM_COLS);
+            umma::tmem_relinquish();
+        }
     }
     umma::tc_fence_before();
     __syncthreads();
+    if (PAIR) umma::cluster_sync_all();  // both CTAs' barriers initialised before any remote arrival
     umma::tc_fence_after();
     const uint32_t tmem_base = *tmem_slot;
 
@@ -205,46 +236,63 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             umma::tma_prefetch(&tA_lo);
             umma::tma_prefetch(&tB_hi);
             umma::tma_prefetch(&tB_lo);
+            const uint32_t tx = (NPROD == 3 ? G::STAGE : TC_A_BYTES + G::B_BYTES) * (PAIR ? 2 : 1);
             int it = 0;
-            for (int u = blockIdx.x; u < a.units && !*abort_flag; u += gridDim.x) {
+            for (int u = unit0; u < a.units && !*abort_flag; u += ustep) {
                 int m, n, kb0, kb1, split;
                 tc_decode<EPI>(a, u, m, n, kb0, kb1, split);
+                const int arow0 = m * G::MT + (int)rank * 128, brow0 = n * TC_BN + (int)rank * G::BROWS;
                 for (int kb = kb0; kb < kb1; kb++) {
-                    const int s = it % TC_STAGES;
-                    const uint32_t ph = (uint32_t)(it / TC_STAGES) & 1u;
+                    const int s = it % G::STAGES;
+                    const uint32_t ph = (uint32_t)(it / G::STAGES) & 1u;
                     if (!umma::mbar_wait(&empty[s], ph ^ 1u, a.budget)) {
                         tc_fail(a.err, abort_flag, 1u);
                         break;
                     }
                     if (a.skip_loads) continue;  // nothing issued: the stage never fills
-                    unsigned char *st = stages + s * TC_STAGE_BYTES;
+                    unsigned char *st = stages + s * G::STAGE;
                     const int kx = kb * tc_bk(OP);
-                    umma::mbar_arrive_expect_tx(&full[s], NPROD == 3 ? TC_STAGE_BYTES : TC_A_BYTES + TC_B_BYTES);
-                    umma::tma_load_2d(st, &tA_hi, &full[s], kx, m * TC_BM);
-                    umma::tma_load_2d(st + 2 * TC_A_BYTES, &tB_hi, &full[s], kx, n * TC_BN);
-                    if (NPROD == 3) {
-                        umma::tma_load_2d(st + TC_A_BYTES, &tA_lo, &full[s], kx, m * TC_BM);
-                        umma::tma_load_2d(st + 2 * TC_A_BYTES + TC_B_BYTES, &tB_lo, &full[s], kx, n * TC_BN);
+                    if (PAIR) {
+                        // both CTAs' bytes are counted on the leader's barrier
+                        const uint32_t fb = umma::mapa_shared(umma::smem_u32(&full[s]), 0);
+                        if (leader) umma::mbar_arrive_expect_tx(&full[s], tx);
+                        umma::tma_load_2d_pair(st, &tA_hi, fb, kx, arow0);
+                        umma::tma_load_2d_pair(st + 2 * TC_A_BYTES, &tB_hi, fb, kx, brow0);
+                        if (NPROD == 3) {
+                            umma::tma_load_2d_pair(st + TC_A_BYTES, &tA_lo, fb, kx, arow0);
+                            umma::tma_load_2d_pair(st + 2 * TC_A_BYTES + G::B_BYTES, &tB_lo, fb, kx, brow0);
+                        }
+                    } else {
+                        umma::mbar_arrive_expect_tx(&full[s], tx);
+                        umma::tma_load_2d(st, &tA_hi, &full[s], kx, arow0);
+                        umma::tma_load_2d(st + 2 * TC_A_BYTES, &tB_hi, &full[s], kx, brow0);
+                        if (NPROD == 3) {
+                            umma::tma_load_2d(st + TC_A_BYTES, &tA_lo, &full[s], kx, arow0);
+                            umma::tma_load_2d(st + 2 * TC_A_BYTES + G::B_BYTES, &tB_lo, &full[s], kx, brow0);
+                        }
                     }
                     it++;
                 }
             }
             // no copy may be in flight when the CTA retires: wait for the last
-            // load issued into each stage (bounded; `it` counts issued stages)
-            for (int j = 1; j <= TC_STAGES && it - j >= 0; j++) {
-                const int i = it - j, s = i % TC_STAGES;
-                if (!umma::mbar_wait(&full[s], (uint32_t)(i / TC_STAGES) & 1u, TC_WAIT_BUDGET))
-                    tc_fail(a.err, abort_flag, 16u);
-            }
+            // load issued into each stage (bounded; `it` counts issued stages).
+            // With a pair the leader's barriers count both CTAs' copies, and the
+            // odd CTA retires only after the cluster barrier below.
+            if (leader)
+                for (int j = 1; j <= G::STAGES && it - j >= 0; j++) {
+                    const int i = it - j, s = i % G::STAGES;
+                    if (!umma::mbar_wait(&full[s], (uint32_t)(i / G::STAGES) & 1u, TC_WAIT_BUDGET))
+                        tc_fail(a.err, abort_flag, 16u);
+                }
         }
         __syncwarp();
     } else if (warp == 1) {
-        if (lane == 0) {
+        if (lane == 0 && leader) {
             // ------------------------------------------------ MMA issuer
-            const uint32_t idesc = umma::idesc_f16(TC_BM, TC_BN, OP == OP_F16 ? 0 : 2);
+            const uint32_t idesc = umma::idesc_f16(G::MT, TC_BN, OP == OP_F16 ? 0 : 2);
             int it = 0, t = 0;
             bool ok = true;
-            for (int u = blockIdx.x; u < a.units && ok && !*abort_flag; u += gridDim.x, t++) {
+            for (int u = unit0; u < a.units && ok && !*abort_flag; u += ustep, t++) {
                 int m, n, kb0, kb1, split;
                 tc_decode<EPI>(a, u, m, n, kb0, kb1, split);
                 const int b = t & 1;
@@ -255,24 +303,38 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 umma::tc_fence_after();
                 const uint32_t d = tmem_base + (uint32_t)(b * TC_BN);
                 for (int kb = kb0; kb < kb1; kb++, it++) {
-                    const int s = it % TC_STAGES;
-                    if (!umma::mbar_wait(&full[s], (uint32_t)(it / TC_STAGES) & 1u, a.budget)) {
+                    const int s = it % G::STAGES;
+                    if (!umma::mbar_wait(&full[s], (uint32_t)(it / G::STAGES) & 1u, a.budget)) {
                         tc_fail(a.err, abort_flag, 4u);
                         ok = false;
                         break;
                     }
                     umma::tc_fence_after();
-                    unsigned char *st = stages + s * TC_STAGE_BYTES;
+                    unsigned char *st = stages + s * G::STAGE;
                     const uint64_t dah = umma::smem_desc_k_sw128(st);
                     const uint64_t dal = umma::smem_desc_k_sw128(st + TC_A_BYTES);
                     const uint64_t dbh = umma::smem_desc_k_sw128(st + 2 * TC_A_BYTES);
-                    const uint64_t dbl = umma::smem_desc_k_sw128(st + 2 * TC_A_BYTES + TC_B_BYTES);
+                    const uint64_t dbl = umma::smem_desc_k_sw128(st + 2 * TC_A_BYTES + G::B_BYTES);
 #pragma unroll
                     for (int kk = 0; kk < TC_ROWB / 32; kk++) {
                         // one MMA covers 32 B along K: 16 f16 or 8 TF32 elements
                         const uint64_t off = (uint64_t)(kk * 32) >> 4;
                         const uint32_t acc = (kb > kb0 || kk > 0) ? 1u : 0u;
-                        if (OP == OP_F16) {
+                        if (PAIR) {
+                            if (OP == OP_F16) {
+                                umma::mma_f16_pair(d, dah + off, dbh + off, idesc, acc);
+                                if (NPROD == 3) {
+                                    umma::mma_f16_pair(d, dah + off, dbl + off, idesc, 1u);
+                                    umma::mma_f16_pair(d, dal + off, dbh + off, idesc, 1u);
+                                }
+                            } else {
+                                umma::mma_tf32_pair(d, dah + off, dbh + off, idesc, acc);
+                                if (NPROD == 3) {
+                                    umma::mma_tf32_pair(d, dah + off, dbl + off, idesc, 1u);
+                                    umma::mma_tf32_pair(d, dal + off, dbh + off, idesc, 1u);
+                                }
+                            }
+                        } else if (OP == OP_F16) {
                             umma::mma_f16_ss(d, dah + off, dbh + off, idesc, acc);
                             if (NPROD == 3) {
                                 umma::mma_f16_ss(d, dah + off, dbl + off, idesc, 1u);
@@ -286,26 +348,34 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                             }
                         }
                     }
-                    umma::mma_commit(&empty[s]);  // stage reusable once these MMAs finish
+                    // stage reusable (in both CTAs of a pair) once these MMAs finish
+                    if (PAIR) umma::mma_commit_pair(&empty[s], 0x3);
+                    else umma::mma_commit(&empty[s]);
                 }
                 if (!ok) break;
-                umma::mma_commit(&tfull[b]);  // accumulator ready for the epilogue
+                // accumulator ready for the epilogue(s)
+                if (PAIR) umma::mma_commit_pair(&tfull[b], 0x3);
+                else umma::mma_commit(&tfull[b]);
             }
-            // every MMA of this CTA has completed before TMEM is released
-            umma::mma_commit(done_bar);
+            // every MMA has completed before TMEM is released
+            if (PAIR) umma::mma_commit_pair(done_bar, 0x1);
+            else umma::mma_commit(done_bar);
             if (!umma::mbar_wait(done_bar, 0u, TC_WAIT_BUDGET)) tc_fail(a.err, abort_flag, 32u);
         }
         __syncwarp();
     } else {
         // ---------------------------------------------------- epilogue
         const int q = warp & 3;  // TMEM lane quarter this warp may access
+        // the accumulator buffers are released on the leader's barriers
+        const uint32_t te0 = PAIR ? umma::mapa_shared(umma::smem_u32(&tempty[0]), 0) : 0u;
+        const uint32_t te1 = PAIR ? umma::mapa_shared(umma::smem_u32(&tempty[1]), 0) : 0u;
         int t = 0;
-        for (int u = blockIdx.x; u < a.units; u += gridDim.x, t++) {
+        for (int u = unit0; u < a.units; u += ustep, t++) {
             int m, n, kb0, kb1, split;
             tc_decode<EPI>(a, u, m, n, kb0, kb1, split);
             const int b = t & 1;
-            const int arow = m * TC_BM + q * 32 + lane;  // row of the twiddle-side operand
-            const int y0 = n * TC_BN;                   // first image row of the columns
+            const int arow = m * G::MT + (int)rank * 128 + q * 32 + lane;  // row of the twiddle-side operand
+            const int y0 = n * TC_BN;                                      // first image row of the columns
             const uint32_t taddr = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * TC_BN);
             if (EPI == EPI_FWD) {
                 // Fy[k][y] along this thread's 256 columns: an FP64-accurate anchor every
@@ -356,8 +426,6 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                         sim = 0.f;
                     }
                 }
-                umma::tc_fence_before();
-                umma::mbar_arrive(&tempty[b]);
             } else {
                 if (!umma::mbar_wait(&tfull[b], (uint32_t)(t >> 1) & 1u, a.budget)) {
                     tc_fail(a.err, abort_flag, 8u);
@@ -380,15 +448,20 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                         }
                     }
                 }
-                umma::tc_fence_before();
-                umma::mbar_arrive(&tempty[b]);
             }
+            umma::tc_fence_before();
+            if (PAIR) umma::mbar_arrive_cluster(b ? te1 : te0);
+            else umma::mbar_arrive(&tempty[b]);
         }
     }
     __syncthreads();
+    // a pair retires together: no CTA leaves while the other may still touch its
+    // shared memory, barriers or tensor memory
+    if (PAIR) umma::cluster_sync_all();
     if (warp == 1) {
         umma::tc_fence_after();
-        umma::tmem_dealloc(tmem_base, TC_TMEM_COLS);
+        if (PAIR) umma::tmem_dealloc_pair(tmem_base, TC_TMEM_COLS);
+        else umma::tmem_dealloc(tmem_base, TC_TMEM_COLS);
     }
 }
 
@@ -803,12 +876,13 @@ static void tc_mode(int precision, int *op, int *nprod)
 // accumulation in TMEM: a running sum of n oscillating products carries a
 // relative rounding error of about 2^-24 sqrt(n); 4096 keeps it near 4e-6; the
 // splits are summed in FP64)
-int gp_tc_splits(int N, int nuv, int nsm, int bk, int *kb_per_out)
+int gp_tc_splits(int N, int nuv, int nsm, int bk, int pair, int *kb_per_out)
 {
-    int M_pad = round_up(N, TC_BN), xrows_pad = round_up(N, TC_BM), K2_pad = round_up(2LL * (nuv ? nuv : 1), bk);
-    int tiles = (xrows_pad / TC_BM) * (M_pad / TC_BN);
+    const int tm = pair ? 256 : TC_BM, slots = pair ? nsm / 2 : nsm;
+    int M_pad = round_up(N, TC_BN), xrows_pad = round_up(N, tm), K2_pad = round_up(2LL * (nuv ? nuv : 1), bk);
+    int tiles = (xrows_pad / tm) * (M_pad / TC_BN);
     int kb_total = K2_pad / bk;
-    int want = (nsm + tiles - 1) / tiles;
+    int want = (slots + tiles - 1) / tiles;
     if (want < 1) want = 1;
     if (want > kb_total) want = kb_total;
     int kb_per = (kb_total + want - 1) / want;
@@ -822,9 +896,13 @@ int gp_tc_splits(int N, int nuv, int nsm, int bk, int *kb_per_out)
 // the largest split count any tensor mode uses for this shape
 int gp_tc_max_splits(int N, int nuv, int nsm)
 {
-    int a = gp_tc_splits(N, nuv, nsm, tc_bk(OP_F16), nullptr);
-    int b = gp_tc_splits(N, nuv, nsm, tc_bk(OP_TF32), nullptr);
-    return a > b ? a : b;
+    int mx = 0;
+    for (int op = OP_F16; op <= OP_TF32; op++)
+        for (int pair = 0; pair <= 1; pair++) {
+            const int v = gp_tc_splits(N, nuv, nsm, tc_bk(op), pair, nullptr);
+            if (v > mx) mx = v;
+        }
+    return mx;
 }
 
 void gp_tc_free(gpair_ctx *c)
@@ -849,14 +927,14 @@ static void launch_twiddle_ops(gpair_ctx *c, TcState *t, long long n_all)
         (OT *)t->fxt_hi, (OT *)t->fxt_lo);
 }
 
-template <int EPI>
+template <int EPI, int PAIR>
 static int tc_set_smem(gpair_ctx *c)
 {
-    GP_CUDA(c, cudaFuncSetAttribute(k_tc_gemm<EPI, OP_F16, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    GP_CUDA(c, cudaFuncSetAttribute(k_tc_gemm<EPI, OP_F16, 3, PAIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     TC_SMEM_BYTES));
-    GP_CUDA(c, cudaFuncSetAttribute(k_tc_gemm<EPI, OP_TF32, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    GP_CUDA(c, cudaFuncSetAttribute(k_tc_gemm<EPI, OP_TF32, 3, PAIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     TC_SMEM_BYTES));
-    GP_CUDA(c, cudaFuncSetAttribute(k_tc_gemm<EPI, OP_TF32, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    GP_CUDA(c, cudaFuncSetAttribute(k_tc_gemm<EPI, OP_TF32, 1, PAIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     TC_SMEM_BYTES));
     return GPAIR_OK;
 }
@@ -866,8 +944,9 @@ int gp_tc_prepare(gpair_ctx *c)
     if (!c->have_problem) return GPAIR_OK;  // prepared when the problem is loaded
     int op, nprod;
     tc_mode(c->precision, &op, &nprod);
+    const int pair = c->tc_pair ? 1 : 0;
     TcState *old = (TcState *)c->tc_state;
-    if (old && old->op == op && old->nprod == nprod) return GPAIR_OK;
+    if (old && old->op == op && old->nprod == nprod && old->pair == pair) return GPAIR_OK;
     if (old) {
         // another operand kind: rebuild every operand buffer for this mode
         GP_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -880,16 +959,18 @@ int gp_tc_prepare(gpair_ctx *c)
     c->tc_state = t;
     t->op = op;
     t->nprod = nprod;
+    t->pair = pair;
     t->esz = op == OP_F16 ? 2 : 4;
     t->bk = tc_bk(op);
     const int N = c->N, nuv = c->nuv ? c->nuv : 1;
     t->Kx_pad = round_up(N, t->bk);
     t->M_pad = round_up(N, TC_BN);
-    t->rows_pad = round_up(2LL * nuv, TC_BM);
+    const int tm = pair ? 256 : TC_BM;  // A rows per tile
+    t->rows_pad = round_up(2LL * nuv, tm);
     t->K2_pad = round_up(2LL * nuv, t->bk);
-    t->xrows_pad = round_up(N, TC_BM);
+    t->xrows_pad = round_up(N, tm);
     GP_CUDA(c, cudaDeviceGetAttribute(&t->nsm, cudaDevAttrMultiProcessorCount, c->device));
-    t->splits = gp_tc_splits(N, nuv, t->nsm, t->bk, &t->kb_per);
+    t->splits = gp_tc_splits(N, nuv, t->nsm, t->bk, pair, &t->kb_per);
     size_t img = (size_t)t->M_pad * t->Kx_pad, fxs = (size_t)t->rows_pad * t->Kx_pad;
     size_t fxts = (size_t)t->xrows_pad * t->K2_pad, ws = (size_t)t->M_pad * t->K2_pad;
     struct { void **p; size_t n; bool lo; } al[] = {{&t->img_hi, img, false}, {&t->img_lo, img, true},
@@ -914,14 +995,15 @@ int gp_tc_prepare(gpair_ctx *c)
     else launch_twiddle_ops<float>(c, t, n_all);
     GP_LAUNCH_CHECK(c);
     const int e = t->esz;
-    if ((rc = tc_make_map(c, &t->m_img_hi, t->img_hi, t->M_pad, t->Kx_pad, TC_BN, e))) return rc;
+    const int bbox = pair ? 128 : TC_BN;  // B rows one CTA stages
+    if ((rc = tc_make_map(c, &t->m_img_hi, t->img_hi, t->M_pad, t->Kx_pad, bbox, e))) return rc;
     if ((rc = tc_make_map(c, &t->m_fx_hi, t->fx_hi, t->rows_pad, t->Kx_pad, TC_BM, e))) return rc;
-    if ((rc = tc_make_map(c, &t->m_w_hi, t->w_hi, t->M_pad, t->K2_pad, TC_BN, e))) return rc;
+    if ((rc = tc_make_map(c, &t->m_w_hi, t->w_hi, t->M_pad, t->K2_pad, bbox, e))) return rc;
     if ((rc = tc_make_map(c, &t->m_fxt_hi, t->fxt_hi, t->xrows_pad, t->K2_pad, TC_BM, e))) return rc;
     if (nprod == 3) {
-        if ((rc = tc_make_map(c, &t->m_img_lo, t->img_lo, t->M_pad, t->Kx_pad, TC_BN, e))) return rc;
+        if ((rc = tc_make_map(c, &t->m_img_lo, t->img_lo, t->M_pad, t->Kx_pad, bbox, e))) return rc;
         if ((rc = tc_make_map(c, &t->m_fx_lo, t->fx_lo, t->rows_pad, t->Kx_pad, TC_BM, e))) return rc;
-        if ((rc = tc_make_map(c, &t->m_w_lo, t->w_lo, t->M_pad, t->K2_pad, TC_BN, e))) return rc;
+        if ((rc = tc_make_map(c, &t->m_w_lo, t->w_lo, t->M_pad, t->K2_pad, bbox, e))) return rc;
         if ((rc = tc_make_map(c, &t->m_fxt_lo, t->fxt_lo, t->xrows_pad, t->K2_pad, TC_BM, e))) return rc;
     } else {
         // the kernel never loads the lo maps in one-product mode; pass valid maps anyway
@@ -930,8 +1012,32 @@ int gp_tc_prepare(gpair_ctx *c)
         t->m_w_lo = t->m_w_hi;
         t->m_fxt_lo = t->m_fxt_hi;
     }
-    if ((rc = tc_set_smem<EPI_FWD>(c))) return rc;
-    if ((rc = tc_set_smem<EPI_STORE>(c))) return rc;
+    if ((rc = tc_set_smem<EPI_FWD, 0>(c))) return rc;
+    if ((rc = tc_set_smem<EPI_STORE, 0>(c))) return rc;
+    if ((rc = tc_set_smem<EPI_FWD, 1>(c))) return rc;
+    if ((rc = tc_set_smem<EPI_STORE, 1>(c))) return rc;
+    t->npairs = t->nsm / 2;
+    if (pair) {
+        // clusters of two that can be resident at once (an SM left over in a GPC cannot host a pair)
+        cudaLaunchConfig_t cfg;
+        memset(&cfg, 0, sizeof(cfg));
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = 2;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3(2 * (unsigned)t->npairs, 1, 1);
+        cfg.blockDim = dim3(TC_THREADS, 1, 1);
+        cfg.dynamicSmemBytes = TC_SMEM_BYTES;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        int nclusters = 0;
+        if (cudaOccupancyMaxActiveClusters(&nclusters, (const void *)k_tc_gemm<EPI_FWD, OP_F16, 3, 1>, &cfg) ==
+                cudaSuccess &&
+            nclusters > 0 && nclusters < t->npairs)
+            t->npairs = nclusters;
+        cudaGetLastError();
+    }
     GP_CUDA(c, cudaStreamSynchronize(c->stream));
     return GPAIR_OK;
 }
@@ -983,21 +1089,51 @@ static TcState *tc_state_ready(gpair_ctx *c, int *rc)
     return t;
 }
 
-// one launch of the contraction in the context's operand kind / product count
+template <int EPI, int PAIR>
+static cudaError_t tc_launch_kind(TcState *t, dim3 grid, cudaStream_t st, const CUtensorMap &A_hi,
+                                  const CUtensorMap &A_lo, const CUtensorMap &B_hi, const CUtensorMap &B_lo,
+                                  const TcArgs &a)
+{
+    cudaLaunchConfig_t cfg;
+    memset(&cfg, 0, sizeof(cfg));
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = PAIR ? 2 : 1;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3(TC_THREADS, 1, 1);
+    cfg.dynamicSmemBytes = TC_SMEM_BYTES;
+    cfg.stream = st;
+    cfg.attrs = at;
+    cfg.numAttrs = PAIR ? 1 : 0;
+    if (t->op == OP_F16) return cudaLaunchKernelEx(&cfg, k_tc_gemm<EPI, OP_F16, 3, PAIR>, A_hi, A_lo, B_hi, B_lo, a);
+    if (t->nprod == 3) return cudaLaunchKernelEx(&cfg, k_tc_gemm<EPI, OP_TF32, 3, PAIR>, A_hi, A_lo, B_hi, B_lo, a);
+    return cudaLaunchKernelEx(&cfg, k_tc_gemm<EPI, OP_TF32, 1, PAIR>, A_hi, A_lo, B_hi, B_lo, a);
+}
+
+// one launch of the contraction in the context's operand kind / product count:
+// persistent CTAs (or CTA pairs), one per SM (pair of SMs) at most
 template <int EPI>
-static int tc_launch(gpair_ctx *c, TcState *t, int grid, const CUtensorMap &A_hi, const CUtensorMap &A_lo,
+static int tc_launch(gpair_ctx *c, TcState *t, const CUtensorMap &A_hi, const CUtensorMap &A_lo,
                      const CUtensorMap &B_hi, const CUtensorMap &B_lo, TcArgs &a)
 {
     a.err = &c->sc->tc_err;
     a.budget = c->tc_wait_budget > 0 ? c->tc_wait_budget : TC_WAIT_BUDGET;
     a.skip_loads = c->tc_skip_loads;
-    if (t->op == OP_F16)
-        k_tc_gemm<EPI, OP_F16, 3><<<grid, TC_THREADS, TC_SMEM_BYTES, c->stream>>>(A_hi, A_lo, B_hi, B_lo, a);
-    else if (t->nprod == 3)
-        k_tc_gemm<EPI, OP_TF32, 3><<<grid, TC_THREADS, TC_SMEM_BYTES, c->stream>>>(A_hi, A_lo, B_hi, B_lo, a);
-    else
-        k_tc_gemm<EPI, OP_TF32, 1><<<grid, TC_THREADS, TC_SMEM_BYTES, c->stream>>>(A_hi, A_lo, B_hi, B_lo, a);
-    GP_LAUNCH_CHECK(c);
+    cudaError_t e;
+    if (t->pair) {
+        const int np = a.units < t->npairs ? a.units : t->npairs;
+        e = tc_launch_kind<EPI, 1>(t, dim3(2 * np, 1, 1), c->stream, A_hi, A_lo, B_hi, B_lo, a);
+    } else {
+        const int g = a.units < t->nsm ? a.units : t->nsm;
+        e = tc_launch_kind<EPI, 0>(t, dim3(g, 1, 1), c->stream, A_hi, A_lo, B_hi, B_lo, a);
+    }
+    if (e != cudaSuccess) {
+        snprintf(c->last_error, sizeof(c->last_error), "tensor-core contraction launch: %s", cudaGetErrorString(e));
+        return GPAIR_ERR_CUDA;
+    }
+    c->launches++;
     return GPAIR_OK;
 }
 
@@ -1009,7 +1145,7 @@ int gp_tc_forward_gemm(gpair_ctx *c)
     if (rc) return rc;
     TcArgs a;
     memset(&a, 0, sizeof(a));
-    a.m_tiles = t->rows_pad / TC_BM;  // twiddle-row tiles
+    a.m_tiles = t->rows_pad / (t->pair ? 256 : TC_BM);  // twiddle-row tiles
     a.n_tiles = t->M_pad / TC_BN;     // image-row tiles
     a.kb_total = t->Kx_pad / t->bk;
     a.kb_per_split = a.kb_total;
@@ -1025,8 +1161,7 @@ int gp_tc_forward_gemm(gpair_ctx *c)
     a.batch = 0;
     a.sc = c->sc;
     a.vpart = c->vpart;
-    int grid = a.units < t->nsm ? a.units : t->nsm;
-    if ((rc = tc_launch<EPI_FWD>(c, t, grid, t->m_fx_hi, t->m_fx_lo, t->m_img_hi, t->m_img_lo, a))) return rc;
+    if ((rc = tc_launch<EPI_FWD>(c, t, t->m_fx_hi, t->m_fx_lo, t->m_img_hi, t->m_img_lo, a))) return rc;
     c->mt = a.n_tiles;
     return GPAIR_OK;
 }
@@ -1047,11 +1182,12 @@ int gp_tc_batch_prepare(gpair_ctx *c, int *epp)
         const size_t rows = (size_t)GP_NTR * t->Lb, n = rows * t->Kx_pad;
         GP_CUDA(c, cudaMalloc(&t->imgb_hi, n * t->esz));
         GP_CUDA(c, cudaMemsetAsync(t->imgb_hi, 0, n * t->esz, c->stream));
-        if ((rc = tc_make_map(c, &t->m_imgb_hi, t->imgb_hi, (long long)rows, t->Kx_pad, TC_BN, t->esz))) return rc;
+        const int bbox = t->pair ? 128 : TC_BN;
+        if ((rc = tc_make_map(c, &t->m_imgb_hi, t->imgb_hi, (long long)rows, t->Kx_pad, bbox, t->esz))) return rc;
         if (t->nprod == 3) {
             GP_CUDA(c, cudaMalloc(&t->imgb_lo, n * t->esz));
             GP_CUDA(c, cudaMemsetAsync(t->imgb_lo, 0, n * t->esz, c->stream));
-            if ((rc = tc_make_map(c, &t->m_imgb_lo, t->imgb_lo, (long long)rows, t->Kx_pad, TC_BN, t->esz)))
+            if ((rc = tc_make_map(c, &t->m_imgb_lo, t->imgb_lo, (long long)rows, t->Kx_pad, bbox, t->esz)))
                 return rc;
         } else {
             t->m_imgb_lo = t->m_imgb_hi;
@@ -1083,7 +1219,7 @@ int gp_tc_forward_batch_gemm(gpair_ctx *c)
     if ((rc = gp_tc_batch_prepare(c, nullptr))) return rc;
     TcArgs a;
     memset(&a, 0, sizeof(a));
-    a.m_tiles = t->rows_pad / TC_BM;
+    a.m_tiles = t->rows_pad / (t->pair ? 256 : TC_BM);
     a.n_tiles = (GP_NTR * t->Lb) / TC_BN;
     a.kb_total = t->Kx_pad / t->bk;
     a.kb_per_split = a.kb_total;
@@ -1100,8 +1236,7 @@ int gp_tc_forward_batch_gemm(gpair_ctx *c)
     a.batch = 1;
     a.sc = c->sc;
     a.vpart = c->vpart_b;
-    int grid = a.units < t->nsm ? a.units : t->nsm;
-    return tc_launch<EPI_FWD>(c, t, grid, t->m_fx_hi, t->m_fx_lo, t->m_imgb_hi, t->m_imgb_lo, a);
+    return tc_launch<EPI_FWD>(c, t, t->m_fx_hi, t->m_fx_lo, t->m_imgb_hi, t->m_imgb_lo, a);
 }
 
 // split of an image into the forward's image operand
@@ -1189,7 +1324,7 @@ int gp_tc_adjoint_gemm(gpair_ctx *c)
     if (rc) return rc;
     TcArgs a;
     memset(&a, 0, sizeof(a));
-    a.m_tiles = t->xrows_pad / TC_BM;  // image-column tiles (twiddle side)
+    a.m_tiles = t->xrows_pad / (t->pair ? 256 : TC_BM);  // image-column tiles (twiddle side)
     a.n_tiles = t->M_pad / TC_BN;      // image-row tiles (weight side)
     a.kb_total = t->K2_pad / t->bk;
     a.kb_per_split = t->kb_per;
@@ -1198,8 +1333,7 @@ int gp_tc_adjoint_gemm(gpair_ctx *c)
     a.out_ld = c->N;
     a.out_rows = c->N;
     a.out_cols = c->N;
-    int grid = a.units < t->nsm ? a.units : t->nsm;
-    if ((rc = tc_launch<EPI_STORE>(c, t, grid, t->m_fxt_hi, t->m_fxt_lo, t->m_w_hi, t->m_w_lo, a))) return rc;
+    if ((rc = tc_launch<EPI_STORE>(c, t, t->m_fxt_hi, t->m_fxt_lo, t->m_w_hi, t->m_w_lo, a))) return rc;
     c->splits = t->splits;
     return GPAIR_OK;
 }

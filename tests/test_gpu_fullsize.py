@@ -39,12 +39,13 @@ def _entropy64(img, model):
     return float(np.sum(np.where(ok, img - m - img * np.log(np.where(ok, img / m, 1.0)), -m)))
 
 
-def _check(p, prec, seed=5):
+def _check(p, prec, seed=5, pair=False):
     rng = np.random.default_rng(seed)
     img = (p.start_image() * (1 + rng.uniform(0, 2, p.npix))).astype(np.float32)
     with g.Reconstructor(0) as rec:
         rec.set_problem(p)
         rec.set_precision(prec)
+        rec.set_tc_pair(pair)
         rec.set_image(img)
         chi2, S = rec.criterion()
         V = rec.visibilities()
@@ -75,7 +76,17 @@ def test_precision_workload_256(precision_problem, prec):
     _check(precision_problem, prec)
 
 
-def test_large_workload_1024():
-    p = g.workload_problem("large")
+def test_precision_workload_256_cta_pairs(precision_problem):
+    _check(precision_problem, g.PREC_SPLIT16, pair=True)
+
+
+@pytest.fixture(scope="module")
+def large_problem():
+    return g.workload_problem("large")
+
+
+@pytest.mark.parametrize("pair", [False, True])
+def test_large_workload_1024(large_problem, pair):
+    p = large_problem
     assert (p.width, p.npow, p.nbis) == (1024, 194560, 1167360)
-    _check(p, g.PREC_SPLIT16)
+    _check(p, g.PREC_SPLIT16, pair=pair)

@@ -316,6 +316,69 @@ def test_tensor_kernel_wait_timeout_is_reported_and_context_recovers(rec):
         assert _rel(rec.data_gradient(), e["data_grad"]) <= 1e-5
 
 
+@pytest.mark.parametrize("prec", [g.PREC_SPLIT16, g.PREC_TF32X3, g.PREC_TF32])
+@pytest.mark.parametrize("name", ["tiny", "small"])
+def test_cta_pair_contractions_match_single_cta_and_fp64(name, prec):
+    """The contractions on CTA pairs (tcgen05.mma.cta_group::2, 256 x 256 tiles
+    over two SMs) against the single-CTA path and against the FP64 oracle:
+    visibilities, chi2, data gradient, and a batched line-search CG trace."""
+    p = _problem(name)
+    img = _rand_image(p, 7)
+    e = O.evaluate64(p, img)
+    out = {}
+    for pair in (0, 1):
+        with g.Reconstructor(0) as r:
+            r.set_problem(p)
+            r.set_precision(prec)
+            r.set_tc_pair(pair)
+            r.set_image(img)
+            chi2, _ = r.criterion()
+            V = r.visibilities()
+            r.gradient()
+            grad = r.data_gradient()
+            r.set_image(p.start_image())
+            tr = r.cg(3, method=2, trace=True, line_search=g.LS_BATCH)["trace_J"]
+            out[pair] = (chi2, V, grad, tr)
+    c0, V0, g0, t0 = out[0]
+    c1, V1, g1, t1 = out[1]
+    assert np.abs(V1 - V0).max() <= 1e-6
+    assert abs(c1 - c0) <= 1e-6 * c0
+    assert _rel(g1, g0.astype(np.float64)) <= 1e-6
+    assert np.allclose(t1, t0, rtol=1e-6)
+    if prec != g.PREC_TF32:
+        assert np.abs(V1 - e["visi"]).max() <= 1e-5
+        assert abs(c1 - e["chi2"]) / e["chi2"] <= 1e-5
+        assert _rel(g1, e["data_grad"]) <= 1e-5
+
+
+def test_cta_pair_wait_timeout_is_reported_and_context_recovers(rec):
+    """The bounded waits of the CTA-pair contraction run out (no TMA loads issued):
+    GPAIR_ERR_TIMEOUT, both CTAs retire and free their tensor memory, and the
+    same context then matches the FP64 oracle."""
+    p = _problem("tiny", (5, 6, 7))
+    rec.set_problem(p)
+    rec.set_precision(g.PREC_SPLIT16)
+    rec.set_tc_pair(True)
+    img = _rand_image(p, 3)
+    rec.set_image(img)
+    L = g.lib()
+    assert L.gpair_set_tc_wait(rec.h, 20_000_000, 1) == 0
+    try:
+        with pytest.raises(g.GpairError, match=r"\(-5\)"):
+            rec.criterion()
+        with pytest.raises(g.GpairError, match=r"\(-5\)"):
+            rec.gradient()
+    finally:
+        assert L.gpair_set_tc_wait(rec.h, 0, 0) == 0
+    e = O.evaluate64(p, img)
+    rec.set_image(img)
+    chi2, _ = rec.criterion()
+    rec.gradient()
+    assert abs(chi2 - e["chi2"]) / e["chi2"] <= 1e-5
+    assert _rel(rec.data_gradient(), e["data_grad"]) <= 1e-5
+    rec.set_tc_pair(False)
+
+
 def test_boundary_zoom_reports_its_trial_cap():
     """gpu_linesearch_zoom stops at its trial cap and says so: with the default cap
     the reference loop's zooms all end on their own; with a cap of one trial the
