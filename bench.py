@@ -427,10 +427,17 @@ def time_to_objective(n_problems: int, race_fr: bool = False, method: int = 2) -
 
 def time_to_objective_workload(rec, p, iters: int, batch_iters: int, method: int = 2) -> dict:
     """Time-to-objective on the benchmark workload itself: plain CG (reference
-    line search) for `iters` iterations sets J*, then plain CG and the batched
-    line search are each timed from the flat prior to J* (1 + 1e-4)."""
+    line search) for `iters` iterations sets J*, then plain CG, the batched line
+    search from the flat prior and the batched line search from the learned
+    warm start (the network applied at the workload's own size; the flat-prior
+    run is the fallback) are each timed to J* (1 + 1e-4)."""
     from gpair_b200 import timetoobj as TT
-    row = TT.evaluate(rec, p, None, iters=iters, batch_iters=batch_iters, objective_from="plain", method=method)
+    from gpair_b200.warmstart import WarmStartNet
+    net = WarmStartNet.load() if p.width % 8 == 0 else None
+    row = TT.evaluate(rec, p, net, iters=iters, batch_iters=batch_iters, objective_from="plain", method=method)
+    if net is not None:
+        row["speedup_warm_vs_plain"] = row["plain_s"] / max(row["warm_s"], 1e-12)
+        row["speedup_warm_vs_batch"] = row["batch_s"] / max(row["warm_s"], 1e-12)
     row["speedup_batch_vs_plain"] = row["plain_s"] / max(row["batch_s"], 1e-12)
     row["unit"] = "s (host wall clock)"
     row["note"] = f"J* = lowest J of {iters} plain PR+ iterations with the reference's line search"

@@ -646,17 +646,8 @@ __global__ void __launch_bounds__(GP_THREADS) k_grad_finalize(const float *__res
     const int reg_kind = sc->reg_kind;
     if (alpha_from_state) alpha = (float)sc->cg.alpha;
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
-        double g = 0.0;
-        int s = 0;
-        for (; s + 16 <= splits; s += 16) {  // 16 loads in flight, summed in split order
-            float a[16];
-#pragma unroll
-            for (int j = 0; j < 16; j++) a[j] = __ldcs(&gpart[(size_t)(s + j) * npix + p]);
-#pragma unroll
-            for (int j = 0; j < 16; j++) g += a[j];
-        }
-        for (; s < splits; s++) g += __ldcs(&gpart[(size_t)s * npix + p]);
+    // one pixel: the split sum in split order (FP64), then the gradient assembly
+    auto finish = [&](int p, double g) {
         float gd = (float)(g * gscale - C);
         data_grad[p] = gd;
         if (mode == GRAD_FUSED) {
@@ -671,6 +662,51 @@ __global__ void __launch_bounds__(GP_THREADS) k_grad_finalize(const float *__res
             acc[1] += fgd * go;
             acc[2] += fgd * dd;
             acc[3] += dd * go;
+        }
+    };
+    if ((npix & 3) == 0) {
+        // four consecutive pixels per thread: 16-byte loads, 8 splits (128 B) in flight
+        const int nq = npix >> 2;
+        for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
+            const float4 *g4 = reinterpret_cast<const float4 *>(gpart) + q;
+            const size_t stride = (size_t)nq;
+            double g[4] = {0.0, 0.0, 0.0, 0.0};
+            int s = 0;
+            for (; s + 8 <= splits; s += 8) {
+                float4 a[8];
+#pragma unroll
+                for (int j = 0; j < 8; j++) a[j] = __ldcs(g4 + (size_t)(s + j) * stride);
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    g[0] += a[j].x;
+                    g[1] += a[j].y;
+                    g[2] += a[j].z;
+                    g[3] += a[j].w;
+                }
+            }
+            for (; s < splits; s++) {
+                const float4 a = __ldcs(g4 + (size_t)s * stride);
+                g[0] += a.x;
+                g[1] += a.y;
+                g[2] += a.z;
+                g[3] += a.w;
+            }
+#pragma unroll
+            for (int j = 0; j < 4; j++) finish(4 * q + j, g[j]);
+        }
+    } else {
+        for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
+            double g = 0.0;
+            int s = 0;
+            for (; s + 16 <= splits; s += 16) {  // 16 loads in flight, summed in split order
+                float a[16];
+#pragma unroll
+                for (int j = 0; j < 16; j++) a[j] = __ldcs(&gpart[(size_t)(s + j) * npix + p]);
+#pragma unroll
+                for (int j = 0; j < 16; j++) g += a[j];
+            }
+            for (; s < splits; s++) g += __ldcs(&gpart[(size_t)s * npix + p]);
+            finish(p, g);
         }
     }
     if (mode != GRAD_FUSED) return;
@@ -695,8 +731,10 @@ int gp_grad_finalize(gpair_ctx *c, int which, int mode, float alpha)
     const int alpha_from_state = alpha < 0.f;
     const float *img = (which == GPAIR_IMG_TEMP) ? c->image_temp : c->image;
     float *out = (which == GPAIR_IMG_TEMP) ? c->grad_temp : c->full_grad_new;
-    int g = gp_cdiv(c->npix, GP_THREADS);  // one pixel per thread: the split sum is latency-bound
+    // one thread per pixel (per four pixels when the image size allows 16-byte loads)
+    int g = gp_cdiv((c->npix & 3) == 0 ? c->npix / 4 : c->npix, GP_THREADS);
     if (g > GP_MAX_PARTIALS) g = GP_MAX_PARTIALS;
+    if (g < 1) g = 1;
     k_grad_finalize<<<g, GP_THREADS, 0, c->stream>>>(c->gpart, c->splits, c->npix, mode, img,
                                                      c->model, alpha, alpha_from_state, c->data_grad, c->entropy_grad, out,
                                                      c->full_grad, c->descent_dir, which == GPAIR_IMG_TEMP ? 1 : 0,
@@ -1122,22 +1160,64 @@ __global__ void __launch_bounds__(GP_THREADS) k_trials_prep(const float *__restr
     }
     float *dst = trials + (size_t)j * npix;
     double acc[2] = {0.0, 0.0};
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
-        double t = (double)img[p] + s * (double)d[p];
-        if (t < minval) t = minval;
-        const float I = (float)t;
-        dst[p] = I;
-        const double Id = I, m = model[p];
-        acc[0] += Id;
-        acc[1] += reg_term(Id, m, sc->reg_kind);
-        if (hi) {
-            const int y = p / N, x = p - y * N;
-            const float v = I * scale;
-            const size_t o = ((size_t)j * Lpad + y) * Kx_pad + x;
-            OT h, l;
-            trial_split(v, h, l);
-            hi[o] = h;
-            if (lo) lo[o] = l;
+    const int reg_kind = sc->reg_kind;
+    if ((N & 7) == 0) {
+        // 8 consecutive pixels of one row per thread: 16-byte loads and stores
+        const int n8 = npix >> 3;
+        for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n8; q += gridDim.x * blockDim.x) {
+            const int p0 = q << 3;
+            __align__(16) float iv[8], dv[8], mv[8], out[8];
+            __align__(16) OT hv[8], lv[8];
+            *reinterpret_cast<float4 *>(&iv[0]) = __ldg(reinterpret_cast<const float4 *>(img + p0));
+            *reinterpret_cast<float4 *>(&iv[4]) = __ldg(reinterpret_cast<const float4 *>(img + p0 + 4));
+            *reinterpret_cast<float4 *>(&dv[0]) = __ldg(reinterpret_cast<const float4 *>(d + p0));
+            *reinterpret_cast<float4 *>(&dv[4]) = __ldg(reinterpret_cast<const float4 *>(d + p0 + 4));
+            *reinterpret_cast<float4 *>(&mv[0]) = __ldg(reinterpret_cast<const float4 *>(model + p0));
+            *reinterpret_cast<float4 *>(&mv[4]) = __ldg(reinterpret_cast<const float4 *>(model + p0 + 4));
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                double t = (double)iv[k] + s * (double)dv[k];
+                if (t < minval) t = minval;
+                const float I = (float)t;
+                out[k] = I;
+                const double Id = I;
+                acc[0] += Id;
+                acc[1] += reg_term(Id, (double)mv[k], reg_kind);
+                if (hi) trial_split(I * scale, hv[k], lv[k]);
+            }
+            *reinterpret_cast<float4 *>(dst + p0) = *reinterpret_cast<const float4 *>(&out[0]);
+            *reinterpret_cast<float4 *>(dst + p0 + 4) = *reinterpret_cast<const float4 *>(&out[4]);
+            if (hi) {
+                const int y = p0 / N, x = p0 - y * N;
+                const size_t o = ((size_t)j * Lpad + y) * Kx_pad + x;
+                constexpr int NV = sizeof(OT) * 8 / 16;
+#pragma unroll
+                for (int v = 0; v < NV; v++) reinterpret_cast<uint4 *>(hi + o)[v] = reinterpret_cast<const uint4 *>(hv)[v];
+                if (lo) {
+#pragma unroll
+                    for (int v = 0; v < NV; v++)
+                        reinterpret_cast<uint4 *>(lo + o)[v] = reinterpret_cast<const uint4 *>(lv)[v];
+                }
+            }
+        }
+    } else {
+        for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
+            double t = (double)img[p] + s * (double)d[p];
+            if (t < minval) t = minval;
+            const float I = (float)t;
+            dst[p] = I;
+            const double Id = I, m = model[p];
+            acc[0] += Id;
+            acc[1] += reg_term(Id, m, reg_kind);
+            if (hi) {
+                const int y = p / N, x = p - y * N;
+                const float v = I * scale;
+                const size_t o = ((size_t)j * Lpad + y) * Kx_pad + x;
+                OT h, l;
+                trial_split(v, h, l);
+                hi[o] = h;
+                if (lo) lo[o] = l;
+            }
         }
     }
     block_sum<2>(acc, smem);
