@@ -50,12 +50,13 @@ def stage_bytes(p: api.Problem, splits: int, row_tiles: int) -> dict:
     }
 
 
-def report(name: str, reps: int = 10) -> dict:
+def report(name: str, reps: int = 10, pair: bool = False) -> dict:
     from .clocks import ClockSampler
     p = api.workload_problem(name)
     with api.Reconstructor(0) as rec:
         rec.set_problem(p)
         rec.set_precision(api.PREC_SPLIT16)
+        rec.set_tc_pair(pair)
         rec.set_image(p.start_image())
         rec.criterion()
         rec.gradient()
@@ -73,10 +74,10 @@ def report(name: str, reps: int = 10) -> dict:
             d = json.load(f)
         hbm, tf = d["hbm_gbs"], d["bf16_tflops"]
     row_tiles = (p.width + 255) // 256
-    splits = _default_splits(p)
+    splits = _default_splits(p, pair)
     by = stage_bytes(p, splits, row_tiles)
     out = {"workload": name, "N": p.width, "nuv": p.nuv, "npow": p.npow, "nbis": p.nbis, "splits": splits,
-           "hbm_peak_gbs": hbm, "tensor_peak_tflops": tf, "clocks": clocks,
+           "hbm_peak_gbs": hbm, "tensor_peak_tflops": tf, "clocks": clocks, "cta_pairs": bool(pair),
            "timing": f"CUDA events, stages back to back, best of 5 x {reps} repetitions", "stages": {}}
     for k, ms in st.items():
         row = {"ms": ms}
@@ -90,15 +91,16 @@ def report(name: str, reps: int = 10) -> dict:
     return out
 
 
-def _default_splits(p: api.Problem) -> int:
-    """Split count of the tensor adjoint as the library chooses it (mirrors gp_tc_splits)."""
+def _default_splits(p: api.Problem, pair: bool = False) -> int:
+    """Split count of the tensor adjoint as the library chooses it (mirrors gp_tc_splits, f16 operands)."""
     N, K = p.width, p.nuv
+    tm, slots = (256, 74) if pair else (128, 148)
     m_pad = -(-N // 256) * 256
-    xrows = -(-N // 128) * 128
+    xrows = -(-N // tm) * tm
     k2 = -(-2 * K // 64) * 64
-    tiles = (xrows // 128) * (m_pad // 256)
+    tiles = (xrows // tm) * (m_pad // 256)
     kb_total = k2 // 64
-    want = max(1, min(kb_total, -(-148 // tiles)))
+    want = max(1, min(kb_total, -(-slots // tiles)))
     kb_per = min(64, -(-kb_total // want))
     return -(-kb_total // kb_per)
 
@@ -111,6 +113,7 @@ def main(argv=None):
     ap.add_argument("--method", type=int, default=2)
     ap.add_argument("--line-search", type=int, default=0, help="0 the reference's search, 1 batched")
     ap.add_argument("--precision", type=int, default=api.PREC_SPLIT16)
+    ap.add_argument("--tc-pair", type=int, default=0, help="1: contractions on CTA pairs (cta_group::2)")
     args = ap.parse_args(argv)
     for w in args.workloads:
         if args.cg > 0:
@@ -118,12 +121,13 @@ def main(argv=None):
             with api.Reconstructor(0) as rec:
                 rec.set_problem(p)
                 rec.set_precision(args.precision)
+                rec.set_tc_pair(bool(args.tc_pair))
                 rec.set_image(p.start_image())
                 out = rec.cg(args.cg, method=args.method, line_search=args.line_search, host_loop=1)
             print(json.dumps({"workload": w, "iterations": out["iterations"], "criterion_evals": out["criterion_evals"],
                               "grad_evals": out["grad_evals"], "J": out["J"]}), flush=True)
             continue
-        print(json.dumps(report(w, args.reps)), flush=True)
+        print(json.dumps(report(w, args.reps, bool(args.tc_pair))), flush=True)
 
 
 if __name__ == "__main__":
