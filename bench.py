@@ -696,7 +696,7 @@ def main():
     ap.add_argument("--tto-workload-iters", type=int, default=60,
                     help="plain-CG iterations that set J* for the time-to-objective block on the benchmark "
                          "workload itself (0: skip)")
-    ap.add_argument("--tto-method", type=int, choices=[2, 4], default=2,
+    ap.add_argument("--tto-method", type=int, choices=[2, 4], default=4,
                     help="direction of the batched / warm-start runs in the time-to-objective blocks: 2 PR+ CG, "
                          "4 projected L-BFGS")
     ap.add_argument("--tto-race-fr", action="store_true",
