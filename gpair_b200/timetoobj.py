@@ -190,6 +190,7 @@ def main(argv=None):
     ap.add_argument("--batch-iters", type=int, default=1500)
     ap.add_argument("--weights", default=DEFAULT_WEIGHTS)
     ap.add_argument("--out", default=None)
+    ap.add_argument("--rows", default=None, help="append each problem's row to this JSON-lines file as it finishes")
     ap.add_argument("--method", type=int, choices=[2, 4], default=2,
                     help="direction of the batched, warm and race runs (2 PR+, 4 projected L-BFGS)")
     ap.add_argument("--objectives", nargs="+", choices=["plain", "batch"], default=["plain", "batch"],
@@ -221,6 +222,9 @@ def main(argv=None):
                              objective_from=obj, rec2=rec2, flag=flag, method=args.method)
                 r["seed"] = SEED_HELD_OUT + k
                 rows[obj].append(r)
+                if args.rows:
+                    with open(args.rows, "a") as f:
+                        f.write(json.dumps({"objective": obj, **r}) + "\n")
     flag.close()
     for k in args.objectives:
         print(f"SUMMARY {k}", json.dumps(summarize(rows[k])), flush=True)
