@@ -681,7 +681,7 @@ def main():
     ap.add_argument("--workload", default="large", choices=["large", "precision", "small", "tiny"])
     ap.add_argument("--precision", default=os.environ.get("GPAIR_BENCH_PRECISION", "split16"),
                     choices=["fp32", "split16"])
-    ap.add_argument("--tc-pair", type=int, choices=[0, 1], default=0,
+    ap.add_argument("--tc-pair", type=int, choices=[0, 1], default=1,
                     help="tensor-core contractions on CTA pairs (cta_group::2) instead of single CTAs")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-time-to-objective", action="store_true")

@@ -119,6 +119,7 @@ extern "C" int gpair_create(gpair_ctx **out, int device)
     if (!c) return GPAIR_ERR_ALLOC;
     c->device = device;
     c->precision = GPAIR_PREC_FP32;
+    c->tc_pair = 1;  // tensor-core contractions on CTA pairs (gpair_set_tc_pair)
     c->fuse_ctrl = -1;
     c->last_image_src = -1;
     int rc = GPAIR_OK;

@@ -113,7 +113,7 @@ def main(argv=None):
     ap.add_argument("--method", type=int, default=2)
     ap.add_argument("--line-search", type=int, default=0, help="0 the reference's search, 1 batched")
     ap.add_argument("--precision", type=int, default=api.PREC_SPLIT16)
-    ap.add_argument("--tc-pair", type=int, default=0, help="1: contractions on CTA pairs (cta_group::2)")
+    ap.add_argument("--tc-pair", type=int, default=1, help="contractions on CTA pairs (cta_group::2, 1) or single CTAs (0)")
     args = ap.parse_args(argv)
     for w in args.workloads:
         if args.cg > 0:

@@ -468,10 +468,10 @@ int gpair_set_stage_timing(gpair_ctx *ctx, int on);
 int gpair_set_tc_wait(gpair_ctx *ctx, long long budget_cycles, int skip_loads);
 
 /* ---- tensor-core contraction layout ----
- * No counterpart in the reference. on = 1: the forward DFT and the adjoint run
- * on pairs of CTAs (a cluster of two SMs sharing one 256 x 256
+ * No counterpart in the reference. on = 1 (default): the forward DFT and the
+ * adjoint run on pairs of CTAs (a cluster of two SMs sharing one 256 x 256
  * tcgen05.mma.cta_group::2 tile, each SM staging half of the image-side
- * operand, 3 pipeline stages); on = 0 (default): one CTA per 128 x 256 tile.
+ * operand, 3 pipeline stages); on = 0: one CTA per 128 x 256 tile, 2 stages.
  * Results agree to rounding; the operands are rebuilt on a change. */
 int gpair_set_tc_pair(gpair_ctx *ctx, int on);
 int gpair_get_tc_pair(gpair_ctx *ctx);

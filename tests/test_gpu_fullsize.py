@@ -39,7 +39,7 @@ def _entropy64(img, model):
     return float(np.sum(np.where(ok, img - m - img * np.log(np.where(ok, img / m, 1.0)), -m)))
 
 
-def _check(p, prec, seed=5, pair=False):
+def _check(p, prec, seed=5, pair=True):
     rng = np.random.default_rng(seed)
     img = (p.start_image() * (1 + rng.uniform(0, 2, p.npix))).astype(np.float32)
     with g.Reconstructor(0) as rec:
@@ -76,8 +76,8 @@ def test_precision_workload_256(precision_problem, prec):
     _check(precision_problem, prec)
 
 
-def test_precision_workload_256_cta_pairs(precision_problem):
-    _check(precision_problem, g.PREC_SPLIT16, pair=True)
+def test_precision_workload_256_single_ctas(precision_problem):
+    _check(precision_problem, g.PREC_SPLIT16, pair=False)
 
 
 @pytest.fixture(scope="module")

@@ -295,6 +295,7 @@ def test_tensor_kernel_wait_timeout_is_reported_and_context_recovers(rec):
     p = _problem("tiny", (5, 6, 7))
     rec.set_problem(p)
     rec.set_precision(g.PREC_SPLIT16)
+    rec.set_tc_pair(False)  # single CTAs here; the CTA-pair kernel has its own timeout test
     img = _rand_image(p, 3)
     rec.set_image(img)
     L = g.lib()
@@ -314,6 +315,7 @@ def test_tensor_kernel_wait_timeout_is_reported_and_context_recovers(rec):
         rec.gradient()
         assert abs(chi2 - e["chi2"]) / e["chi2"] <= 1e-5
         assert _rel(rec.data_gradient(), e["data_grad"]) <= 1e-5
+    rec.set_tc_pair(True)
 
 
 @pytest.mark.parametrize("prec", [g.PREC_SPLIT16, g.PREC_TF32X3, g.PREC_TF32])
@@ -376,7 +378,6 @@ def test_cta_pair_wait_timeout_is_reported_and_context_recovers(rec):
     rec.gradient()
     assert abs(chi2 - e["chi2"]) / e["chi2"] <= 1e-5
     assert _rel(rec.data_gradient(), e["data_grad"]) <= 1e-5
-    rec.set_tc_pair(False)
 
 
 def test_boundary_zoom_reports_its_trial_cap():
