@@ -333,9 +333,10 @@ def many_instances(n: int, iters: int) -> dict:
     """n independent reconstructions of uneven size (widths 64-256, 500-8,000 uv)
     for `iters` batched-line-search CG iterations each: one after another, all
     at once through gpair_cg_run_many (each context's graph on its own stream),
-    and as one graph launch (gpair_batch_run: every CG loop a branch of one
-    graph). Host wall clock; problem loading and graph capture are outside the
-    timings."""
+    and as one graph launch (gpair_batch_run), both as a lockstep batch whose
+    batched evaluations run one grouped tcgen05 forward over all instances and
+    with every CG loop an independent branch of the graph. Host wall clock;
+    problem loading and graph capture are outside the timings."""
     import gpair_b200 as g
     from gpair_b200.instances import instances
     ps = instances(n)
@@ -345,10 +346,11 @@ def many_instances(n: int, iters: int) -> dict:
             r.set_problem(p)
             r.set_precision(g.PREC_SPLIT16)
             r.set_image(p.start_image())
-        # autotuned configuration per instance shape (precision path, adjoint split-K),
-        # cached across instances of the same shape
+        # autotuned configuration per instance shape (precision path, tensor-core tile,
+        # adjoint split-K), cached across instances of the same shape
         t0 = time.perf_counter()
-        flags = g.api.TUNE_PRECISION | g.api.TUNE_SPLITS | g.api.TUNE_CACHE | g.api.TUNE_BATCHED
+        flags = (g.api.TUNE_PRECISION | g.api.TUNE_SPLITS | g.api.TUNE_CACHE | g.api.TUNE_BATCHED |
+                 g.api.TUNE_TILE)
         tuned = [r.autotune(flags, reps=2) for r in recs]
         t_tune = time.perf_counter() - t0
         for r, p in zip(recs, ps):
@@ -367,17 +369,21 @@ def many_instances(n: int, iters: int) -> dict:
         res = g.cg_many(recs, iters, line_search=g.LS_BATCH)
         t_con = time.perf_counter() - t0
         flops_con = sum(r.last_run_stats()[1] for r in recs)
-        # all instances' CG loops as branches of one graph: one launch
-        with g.api.Batch(recs, line_search=g.LS_BATCH) as b:
-            for r, p in zip(recs, ps):
-                r.set_image(p.start_image())
-            b.run(1)  # first launch
-            for r, p in zip(recs, ps):
-                r.set_image(p.start_image())
-            t0 = time.perf_counter()
-            res_b = b.run(iters)
-            t_one = time.perf_counter() - t0
-            flops_one = sum(r.last_run_stats()[1] for r in recs)
+        # one graph launch: lockstep with grouped forwards, then independent branches
+        one = {}
+        for mode in ("grouped", "independent"):
+            with g.api.Batch(recs, line_search=g.LS_BATCH, independent=(mode == "independent")) as b:
+                for r, p in zip(recs, ps):
+                    r.set_image(p.start_image())
+                b.run(1)  # first launch
+                for r, p in zip(recs, ps):
+                    r.set_image(p.start_image())
+                t0 = time.perf_counter()
+                res_b = b.run(iters)
+                dt = time.perf_counter() - t0
+                one[mode] = {"s": dt, "grouped": b.grouped, "all_ok": all(r_["status"] == 0 for r_ in res_b),
+                             "tflops": sum(r.last_run_stats()[1] for r in recs) / max(dt, 1e-12) / 1e12}
+        t_one = one["grouped"]["s"]
     finally:
         for r in recs:
             r.close()
@@ -388,11 +394,15 @@ def many_instances(n: int, iters: int) -> dict:
             "instances_per_s": n / max(t_con, 1e-12), "tflops_concurrent": flops_con / max(t_con, 1e-12) / 1e12,
             "tflops_sequential": flops / max(t_seq, 1e-12) / 1e12,
             "one_launch_s": t_one, "one_launch_speedup": t_seq / max(t_one, 1e-12),
-            "tflops_one_launch": flops_one / max(t_one, 1e-12) / 1e12,
-            "all_ok": all(r_["status"] == 0 for r_ in res) and all(r_["status"] == 0 for r_ in res_b),
+            "tflops_one_launch": one["grouped"]["tflops"], "one_launch_grouped": one["grouped"]["grouped"],
+            "one_launch_independent_s": one["independent"]["s"],
+            "tflops_one_launch_independent": one["independent"]["tflops"],
+            "all_ok": all(r_["status"] == 0 for r_ in res) and all(v["all_ok"] for v in one.values()),
             "autotune": {"s": t_tune, "tuned": sum(not t["from_cache"] for t in tuned),
                          "fp32_path": sum(t["precision"] == g.PREC_FP32 for t in tuned),
-                         "split16_path": sum(t["precision"] == g.PREC_SPLIT16 for t in tuned)},
+                         "split16_path": sum(t["precision"] == g.PREC_SPLIT16 for t in tuned),
+                         "tile_256": sum(t["tile_m"] == 256 for t in tuned),
+                         "tile_128": sum(t["tile_m"] == 128 for t in tuned)},
             "unit": "s (host wall clock)", "line_search": "batched"}
 
 

@@ -85,13 +85,16 @@ class CgParams(C.Structure):
 
 
 LS_WOLFE, LS_BATCH, LS_TRIALS = 0, 1, 8
-TUNE_PRECISION, TUNE_SPLITS, TUNE_CACHE, TUNE_BATCHED = 1, 2, 4, 8
+BATCH_INDEPENDENT = 1  # gpair_batch_create_ex flag: independent branches, no lockstep grouping
+TUNE_PRECISION, TUNE_SPLITS, TUNE_CACHE, TUNE_BATCHED, TUNE_TILE = 1, 2, 4, 8, 16
+TUNE_MAX_CANDIDATES = 12
 
 
 class TuneResult(C.Structure):
     _fields_ = [("precision", C.c_int), ("adjoint_splits", C.c_int), ("ms_per_eval", C.c_double),
-                ("from_cache", C.c_int), ("n_candidates", C.c_int), ("cand_precision", C.c_int * 8),
-                ("cand_splits", C.c_int * 8), ("cand_ms", C.c_double * 8)]
+                ("from_cache", C.c_int), ("n_candidates", C.c_int), ("tile_m", C.c_int),
+                ("cand_precision", C.c_int * TUNE_MAX_CANDIDATES), ("cand_splits", C.c_int * TUNE_MAX_CANDIDATES),
+                ("cand_tile_m", C.c_int * TUNE_MAX_CANDIDATES), ("cand_ms", C.c_double * TUNE_MAX_CANDIDATES)]
 
 
 class CgResult(C.Structure):
@@ -153,6 +156,8 @@ def lib() -> C.CDLL:
         L.gpair_autotune.argtypes = [vp, i, i, C.POINTER(TuneResult)]
         L.gpair_update_pixel.argtypes = [vp, i, i, f, C.POINTER(d), C.POINTER(d)]
         L.gpair_batch_create.argtypes = [C.POINTER(vp), C.POINTER(vp), i, i]
+        L.gpair_batch_create_ex.argtypes = [C.POINTER(vp), C.POINTER(vp), i, i, i]
+        L.gpair_batch_grouped.argtypes = [vp]
         L.gpair_batch_run.argtypes = [vp, C.POINTER(CgParams), C.POINTER(CgResult)]
         L.gpair_batch_destroy.argtypes = [vp]
         L.gpair_cg_run_many.argtypes = [C.POINTER(vp), i, C.POINTER(CgParams), C.POINTER(CgResult)]
@@ -472,12 +477,13 @@ class Reconstructor:
 
     def autotune(self, flags: int = 7, reps: int = 3) -> dict:
         """Time criterion + gradient under candidate configurations (precision path,
-        adjoint split-K length) and keep the fastest (gpair_autotune)."""
+        adjoint split-K length, tensor-core tile) and keep the fastest (gpair_autotune)."""
         r = TuneResult()
         self._c(self._L.gpair_autotune(self.h, flags, reps, C.byref(r)))
         return {"precision": r.precision, "adjoint_splits": r.adjoint_splits, "ms_per_eval": r.ms_per_eval,
-                "from_cache": bool(r.from_cache),
-                "candidates": [(r.cand_precision[i], r.cand_splits[i], r.cand_ms[i]) for i in range(r.n_candidates)]}
+                "from_cache": bool(r.from_cache), "tile_m": r.tile_m,
+                "candidates": [(r.cand_precision[i], r.cand_splits[i], r.cand_tile_m[i], r.cand_ms[i])
+                               for i in range(r.n_candidates)]}
 
     def checkpoint(self) -> bytes:
         """The CG state of this context (gpair_cg_checkpoint_save) as bytes."""
@@ -658,18 +664,23 @@ def cg_many(recs, iterations: int, method: int = 2, alpha: Optional[float] = Non
 
 
 class Batch:
-    """Many reconstructions in one CUDA graph launch (gpair_batch_*): every
-    context's whole CG loop is a branch of one graph. Build after the contexts hold
-    their problems, images and configuration."""
+    """Many reconstructions in one CUDA graph launch (gpair_batch_*). With the
+    batched line search and every context on a tensor-core path the instances run
+    in lockstep and each batched evaluation's forwards are one grouped tcgen05
+    launch (`grouped` is True); otherwise (or with independent=True) every
+    context's whole CG loop is an independent branch of the graph. Build after the
+    contexts hold their problems, images and configuration."""
 
-    def __init__(self, recs, line_search: int = LS_BATCH):
+    def __init__(self, recs, line_search: int = LS_BATCH, independent: bool = False):
         self._L = lib()
         self.recs = list(recs)
         self.line_search = line_search
         h = C.c_void_p()
         arr = (C.c_void_p * len(self.recs))(*[r.h.value for r in self.recs])
-        _check(self._L.gpair_batch_create(C.byref(h), arr, len(self.recs), line_search), self.recs[0].h)
+        flags = BATCH_INDEPENDENT if independent else 0
+        _check(self._L.gpair_batch_create_ex(C.byref(h), arr, len(self.recs), line_search, flags), self.recs[0].h)
         self.h = h
+        self.grouped = bool(self._L.gpair_batch_grouped(self.h))
 
     def run(self, iterations: int, method: int = 2, alpha: Optional[float] = None, resume: bool = False, **kw):
         prm = CgParams()

@@ -1,12 +1,16 @@
-// autotune.cu -- per-problem choice of the precision path and of the adjoint's
-// split-K tile length, by timing criterion + gradient evaluations of the loaded
-// problem on the device (CUDA events on the context's stream).
+// autotune.cu -- per-problem choice of the precision path, the tensor-core tile
+// and the adjoint's split-K tile length, by timing criterion + gradient
+// evaluations of the loaded problem on the device (CUDA events on the
+// context's stream).
 //
 // Candidates:
 //   precision  FP32 (CUDA-core contractions) and split-f16 (tcgen05); both meet
 //              the accuracy bounds, the faster one depends on the image width
 //              and the uv count (small problems leave the tensor GEMM's tiles
 //              mostly empty)
+//   tile       (tensor) 256 x 256 output tiles on CTA pairs or 128 x 256 on
+//              single CTAs: pairs halve the operand traffic per MMA, single
+//              CTAs pad the uv rows less and give small problems more tiles
 //   splits     the adjoint's K-blocks per split (tensor) or split count
 //              (CUDA cores): the heuristic's value, half and double of it,
 //              within the FP32-accumulation cap and the partial-image buffer
@@ -27,7 +31,7 @@
 namespace {
 
 struct Choice {
-    int precision, tc_kb_per, simt_splits;
+    int precision, tc_kb_per, simt_splits, tc_pair;
     double ms;
 };
 
@@ -79,6 +83,10 @@ int time_evals(gpair_ctx *c, int reps, int batched, double *ms)
 
 int apply(gpair_ctx *c, const Choice &ch)
 {
+    if (c->tc_pair != ch.tc_pair) {
+        int rc = gpair_set_tc_pair(c, ch.tc_pair);  // rebuilds the tensor state on the tensor path
+        if (rc) return rc;
+    }
     int rc = gpair_set_precision(c, ch.precision);
     if (rc) return rc;
     if (ch.precision != GPAIR_PREC_FP32) {
@@ -97,7 +105,9 @@ extern "C" int gpair_autotune(gpair_ctx *c, int flags, int reps, gpair_tune_resu
     if (!c || !c->have_problem || !c->have_image) return GPAIR_ERR_STATE;
     if (reps <= 0) reps = 3;
     GP_CUDA(c, cudaSetDevice(c->device));
-    const auto key = std::make_tuple(c->device, c->N, uv_bucket(c->nuv) * 2 + ((flags & GPAIR_TUNE_BATCHED) ? 1 : 0));
+    const auto key = std::make_tuple(c->device, c->N,
+                                     uv_bucket(c->nuv) * 4 + ((flags & GPAIR_TUNE_BATCHED) ? 1 : 0) +
+                                         ((flags & GPAIR_TUNE_TILE) ? 2 : 0));
     if (res) memset(res, 0, sizeof(*res));
     if (flags & GPAIR_TUNE_CACHE) {
         Choice ch;
@@ -124,6 +134,7 @@ extern "C" int gpair_autotune(gpair_ctx *c, int flags, int reps, gpair_tune_resu
                 res->adjoint_splits = ch.precision == GPAIR_PREC_FP32 ? ch.simt_splits : gp_tc_split_count(c, ch.tc_kb_per);
                 res->ms_per_eval = ch.ms;
                 res->from_cache = 1;
+                res->tile_m = ch.precision == GPAIR_PREC_FP32 ? 0 : (ch.tc_pair ? 256 : 128);
             }
             return GPAIR_OK;
         }
@@ -144,19 +155,24 @@ extern "C" int gpair_autotune(gpair_ctx *c, int flags, int reps, gpair_tune_resu
                 if (simt0 / 2 >= 1) ss.push_back(simt0 / 2);
                 if (2 * simt0 <= c->gpart_cap && 2 * simt0 <= 64) ss.push_back(2 * simt0);
             }
-            for (int s : ss) cand.push_back({prec, 0, s, 0.0});
+            for (int s : ss) cand.push_back({prec, 0, s, c->tc_pair, 0.0});
         } else {
-            int rc = gpair_set_precision(c, prec);
-            if (rc) return rc;
-            if ((rc = gp_tc_prepare(c))) return rc;
-            const int k0 = gp_tc_kb_per(c);
-            if (k0 <= 0) return GPAIR_ERR_STATE;
-            std::vector<int> ks = {k0};
-            if (flags & GPAIR_TUNE_SPLITS) {
-                if (k0 / 2 >= 1) ks.push_back(k0 / 2);
-                if (2 * k0 <= gp_tc_kb_cap(c)) ks.push_back(2 * k0);
+            std::vector<int> pairs = {c->tc_pair};
+            if (flags & GPAIR_TUNE_TILE) pairs.push_back(!c->tc_pair);
+            for (int pr : pairs) {
+                int rc = gpair_set_tc_pair(c, pr);
+                if (rc) return rc;
+                if ((rc = gpair_set_precision(c, prec))) return rc;
+                if ((rc = gp_tc_prepare(c))) return rc;
+                const int k0 = gp_tc_kb_per(c);  // the heuristic's split for this tile
+                if (k0 <= 0) return GPAIR_ERR_STATE;
+                std::vector<int> ks = {k0};
+                if (flags & GPAIR_TUNE_SPLITS) {
+                    if (k0 / 2 >= 1) ks.push_back(k0 / 2);
+                    if (2 * k0 <= gp_tc_kb_cap(c)) ks.push_back(2 * k0);
+                }
+                for (int k : ks) cand.push_back({prec, k, simt0, pr, 0.0});
             }
-            for (int k : ks) cand.push_back({prec, k, simt0, 0.0});
         }
     }
     if ((int)cand.size() > GPAIR_TUNE_MAX_CANDIDATES) cand.resize(GPAIR_TUNE_MAX_CANDIDATES);
@@ -184,7 +200,9 @@ extern "C" int gpair_autotune(gpair_ctx *c, int flags, int reps, gpair_tune_resu
                                                                        : gp_tc_split_count(c, cand[best].tc_kb_per);
         res->ms_per_eval = cand[best].ms;
         res->n_candidates = (int)cand.size();
+        res->tile_m = cand[best].precision == GPAIR_PREC_FP32 ? 0 : (cand[best].tc_pair ? 256 : 128);
         for (size_t i = 0; i < cand.size(); i++) {
+            res->cand_tile_m[i] = cand[i].precision == GPAIR_PREC_FP32 ? 0 : (cand[i].tc_pair ? 256 : 128);
             res->cand_precision[i] = cand[i].precision;
             res->cand_splits[i] = cand[i].precision == GPAIR_PREC_FP32 ? cand[i].simt_splits
                                                                       : gp_tc_split_count(c, cand[i].tc_kb_per);

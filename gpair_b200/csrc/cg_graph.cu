@@ -29,6 +29,9 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
+#include <vector>
+
 #include "gpair_internal.cuh"
 
 int gp_eval_criterion(gpair_ctx *c, int which, int trial);
@@ -43,6 +46,7 @@ struct CgGraph {
     double *trace;
     int trace_cap;
     int n_pre, n_crit, n_grad, n_post;  // kernel launches per sequence
+    unsigned int buf_gen;                // the context's buffer generation at capture
 };
 
 enum { SEQ_PRE = 0, SEQ_CRIT = 1, SEQ_GRAD = 2, SEQ_POST = 3 };
@@ -50,8 +54,9 @@ enum { SEQ_PRE = 0, SEQ_CRIT = 1, SEQ_GRAD = 2, SEQ_POST = 3 };
 static int emit(gpair_ctx *c, CgGraph *G, int seq, cudaGraphConditionalHandle hi, cudaGraphConditionalHandle hl,
                 cudaGraphConditionalHandle hg)
 {
-    // the controller runs in the last block of the reduction kernel that precedes it
-    c->fuse_handles = 1;
+    // the controller runs in the last block of the reduction kernel that precedes it;
+    // it steers the graph when it has handles (a lockstep batch steers by routers)
+    c->fuse_handles = hi != 0;
     c->fh_iter = hi;
     c->fh_ls = hl;
     c->fh_grad = hg;
@@ -239,6 +244,14 @@ struct BatchGraph {
     cudaGraph_t g;
     cudaGraphExec_t exec;
     CgGraph *loops;  // per context: mode, trace buffer, launch counts (no graph of its own)
+    // lockstep batch with grouped forwards (instances in lockstep order: by class)
+    int grouped;
+    int ngrp;
+    void **grps;                      // one grouped forward per class of tensor instances (umma_dft.cu)
+    unsigned int *gerr;               // device: wait failures of the grouped forwards
+    int *flags;                       // device: act[n], ls[n], lockstep order
+    cudaGraphConditionalHandle *hd;   // device: h_pre[n], h_post[n], lockstep order
+    DevScalars **scs;                 // device: every instance's scalars, lockstep order
 };
 
 void gp_batch_graph_free(void *bg)
@@ -252,10 +265,310 @@ void gp_batch_graph_free(void *bg)
             if (B->loops[i].trace) cudaFree(B->loops[i].trace);
         free(B->loops);
     }
+    for (int k = 0; k < B->ngrp; k++) gp_tc_group_free(B->grps[k]);
+    free(B->grps);
+    if (B->gerr) cudaFree(B->gerr);
+    if (B->flags) cudaFree(B->flags);
+    if (B->hd) cudaFree(B->hd);
+    if (B->scs) cudaFree(B->scs);
     free(B);
 }
 
-int gp_batch_graph_build(gpair_ctx **ctx, int n, int ls_mode, void **out)
+// ----------------------------------------- lockstep batches, grouped forward
+//
+// With the batched line search the instances can advance in lockstep, so that
+// the batched-trial forwards of all of them run as one grouped tcgen05 launch
+// per class of tensor instances (same operand kind, product count and tile
+// layout; gp_tc_group_forward); instances on the CUDA cores keep their own
+// batched evaluation. In lockstep order (instances sorted by class):
+//
+//   [route INIT]   act[i] = 1
+//   WHILE (h_any_iter)
+//     [route BEGIN]  h_pre[i] = h_post[i] = act[i]
+//     IF (h_pre[i])  criterion + gradient + direction of instance i   (each i, side by side)
+//     [route LS0]    ls[i] = act[i] and the line search of i goes on; h_any_ls
+//     WHILE (h_any_ls)
+//       trial images + operands of instance i, if ls[i]              (each tensor i)
+//       one grouped forward per class over its instances with ls[i]
+//       chi2 of the trials + controller of instance i, if ls[i]      (each tensor i)
+//       the whole batched evaluation of instance i, if ls[i]         (each CUDA-core i)
+//       [route LSN]  ls[i] = ls[i] and the line search of i goes on; h_any_ls
+//     IF (h_post[i]) image update + end of the iteration of instance i
+//     [route END]    act[i] = act[i] and the run of i goes on; h_any_iter
+//
+// Each instance runs the kernels of its own graph with the same arguments
+// (its controllers steer nothing; the routers read their decisions), so its
+// results are bitwise those of a separate run.
+enum { GR_INIT = 0, GR_BEGIN = 1, GR_LS0 = 2, GR_LSN = 3, GR_END = 4 };
+
+__global__ void k_lockstep_route(int what, DevScalars *const *__restrict__ scs, int n, int *__restrict__ act,
+                                 int *__restrict__ ls, const cudaGraphConditionalHandle *__restrict__ h_pre,
+                                 const cudaGraphConditionalHandle *__restrict__ h_post,
+                                 cudaGraphConditionalHandle h_any, unsigned int *__restrict__ gerr)
+{
+    __shared__ int any;
+    if (threadIdx.x == 0) any = 0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        DevScalars *sc = scs[i];
+        int v = 0;
+        switch (what) {
+        case GR_INIT:
+            act[i] = 1;
+            if (i == 0) *gerr = 0u;  // wait failures of this launch's grouped forwards
+            break;
+        case GR_BEGIN:
+            cudaGraphSetConditional(h_pre[i], act[i] ? 1u : 0u);
+            cudaGraphSetConditional(h_post[i], act[i] ? 1u : 0u);
+            break;
+        case GR_LS0:
+            v = act[i] && sc->cg.action != CG_DONE;
+            ls[i] = v;
+            break;
+        case GR_LSN:
+            // a bounded wait of a grouped forward gave up: every instance stops
+            if (ls[i] && *gerr) sc->tc_err |= *gerr;
+            v = ls[i] && sc->cg.action != CG_DONE && !sc->tc_err;
+            ls[i] = v;
+            break;
+        default:  // GR_END
+            v = act[i] && cg_run_goes_on(sc);
+            act[i] = v;
+            break;
+        }
+        if (v) atomicOr(&any, 1);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && what >= GR_LS0) cudaGraphSetConditional(h_any, any ? 1u : 0u);
+}
+
+template <typename F>
+static int capture_fn(gpair_ctx *c, F f, cudaGraph_t *out, int *nlaunch)
+{
+    const long long l0 = c->launches;
+    const int st = c->stage_timing;
+    c->stage_timing = 0;
+    GP_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = f();
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    c->stage_timing = st;
+    if (nlaunch) *nlaunch = (int)(c->launches - l0);
+    c->launches = l0;
+    if (rc || e != cudaSuccess || !g) {
+        if (g) cudaGraphDestroy(g);
+        if (!rc) snprintf(c->last_error, sizeof(c->last_error), "stream capture failed: %s", cudaGetErrorString(e));
+        return rc ? rc : GPAIR_ERR_CUDA;
+    }
+    *out = g;
+    return GPAIR_OK;
+}
+
+// adds `child` (destroyed here) to `parent` after the nodes `deps`
+static int add_child(gpair_ctx *c, cudaGraph_t parent, cudaGraph_t child, const cudaGraphNode_t *deps, size_t ndeps,
+                     cudaGraphNode_t *node)
+{
+    cudaError_t e = cudaGraphAddChildGraphNode(node, parent, deps, ndeps, child);
+    cudaGraphDestroy(child);
+    if (e != cudaSuccess) {
+        snprintf(c->last_error, sizeof(c->last_error), "lockstep graph assembly: %s", cudaGetErrorString(e));
+        return GPAIR_ERR_CUDA;
+    }
+    return GPAIR_OK;
+}
+
+static int lockstep_route(BatchGraph *B, gpair_ctx *c, int what, cudaGraphConditionalHandle h_any, cudaGraph_t parent,
+                          const cudaGraphNode_t *deps, size_t ndeps, cudaGraphNode_t *node)
+{
+    const int n = B->n;
+    cudaGraph_t g = nullptr;
+    int rc = capture_fn(
+        c,
+        [&]() {
+            k_lockstep_route<<<1, 256, 0, c->stream>>>(what, B->scs, n, B->flags, B->flags + n, B->hd, B->hd + n,
+                                                       h_any, B->gerr);
+            GP_LAUNCH_CHECK(c);
+            return GPAIR_OK;
+        },
+        &g, nullptr);
+    if (rc) return rc;
+    return add_child(c, parent, g, deps, ndeps, node);
+}
+
+// GPAIR_ERR_STATE: no instance can take part in a grouped forward (the caller
+// builds the independent branches instead)
+static int build_lockstep(gpair_ctx **ctx_in, int n, BatchGraph *B)
+{
+    // lockstep order: tensor instances by class (stable), then the CUDA-core ones
+    std::vector<int> key((size_t)n), order((size_t)n);
+    for (int i = 0; i < n; i++) {
+        key[i] = gp_tc_group_key(ctx_in[i]);
+        order[i] = i;
+    }
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        const int ka = key[a] < 0 ? 1 << 30 : key[a], kb = key[b] < 0 ? 1 << 30 : key[b];
+        return ka < kb;
+    });
+    if (key[order[0]] < 0 || n > 4096) return GPAIR_ERR_STATE;
+    std::vector<gpair_ctx *> ctx((size_t)n);
+    for (int k = 0; k < n; k++) ctx[k] = ctx_in[order[k]];
+    gpair_ctx *c0 = ctx[0];
+    GP_CUDA(c0, cudaMalloc(&B->flags, sizeof(int) * 2 * (size_t)n));
+    GP_CUDA(c0, cudaMemset(B->flags, 0, sizeof(int) * 2 * (size_t)n));
+    GP_CUDA(c0, cudaMalloc(&B->gerr, sizeof(unsigned int)));
+    GP_CUDA(c0, cudaMemset(B->gerr, 0, sizeof(unsigned int)));
+    // classes: [cls_begin[q], cls_begin[q + 1]) in lockstep order; grouped launches hold
+    // at most 256 instances, a larger class is split
+    std::vector<int> cls_begin;
+    for (int k = 0; k < n; k++) {
+        if (key[order[k]] < 0) break;
+        if (cls_begin.empty() || key[order[k]] != key[order[k - 1]] || k - cls_begin.back() == 256)
+            cls_begin.push_back(k);
+    }
+    int ntc = 0;
+    while (ntc < n && key[order[ntc]] >= 0) ntc++;
+    cls_begin.push_back(ntc);
+    B->ngrp = (int)cls_begin.size() - 1;
+    B->grps = (void **)calloc((size_t)B->ngrp, sizeof(void *));
+    if (!B->grps) return GPAIR_ERR_ALLOC;
+    int rc = GPAIR_OK;
+    for (int q = 0; q < B->ngrp && !rc; q++) {
+        const int k0 = cls_begin[q], k1 = cls_begin[q + 1];
+        rc = gp_tc_group_build(&ctx[k0], k1 - k0, B->flags + n + k0, B->gerr, &B->grps[q]);
+    }
+    for (int k = ntc; k < n && !rc; k++) rc = gp_batch_alloc(ctx[k]);  // no allocation inside a capture
+    if (rc) return rc == GPAIR_ERR_STATE ? GPAIR_ERR_CUDA : rc;  // the instances were eligible
+    GP_CUDA(c0, cudaMalloc(&B->hd, sizeof(cudaGraphConditionalHandle) * 2 * (size_t)n));
+    GP_CUDA(c0, cudaMalloc(&B->scs, sizeof(DevScalars *) * (size_t)n));
+    std::vector<DevScalars *> hs((size_t)n);
+    for (int k = 0; k < n; k++) hs[k] = ctx[k]->sc;
+    GP_CUDA(c0, cudaMemcpy(B->scs, hs.data(), sizeof(DevScalars *) * (size_t)n, cudaMemcpyHostToDevice));
+
+    // loops and their handles
+    cudaGraphConditionalHandle h_iter, h_ls;
+    GP_CUDA(c0, cudaGraphConditionalHandleCreate(&h_iter, B->g, 1, cudaGraphCondAssignDefault));
+    cudaGraph_t B1, B2;
+    cudaGraphNode_t n_init;
+    if ((rc = lockstep_route(B, c0, GR_INIT, h_iter, B->g, nullptr, 0, &n_init))) return rc;
+    cudaGraphNode_t n_loop = add_conditional(c0, B->g, h_iter, cudaGraphCondTypeWhile, &B1, &rc);
+    if (rc) return rc;
+    GP_CUDA(c0, cudaGraphAddDependencies(B->g, &n_init, &n_loop, 1));
+    GP_CUDA(c0, cudaGraphConditionalHandleCreate(&h_ls, B1, 0, 0));
+    std::vector<cudaGraphConditionalHandle> hh(2 * (size_t)n);
+    for (size_t i = 0; i < hh.size(); i++) GP_CUDA(c0, cudaGraphConditionalHandleCreate(&hh[i], B1, 0, 0));
+    GP_CUDA(c0, cudaMemcpy(B->hd, hh.data(), sizeof(cudaGraphConditionalHandle) * hh.size(), cudaMemcpyHostToDevice));
+
+    // B1: BEGIN, IF(pre_k), LS0, WHILE(ls), IF(post_k), END
+    cudaGraphNode_t n_begin, n_ls0, n_lsw, n_end;
+    std::vector<cudaGraphNode_t> pre((size_t)n), post((size_t)n);
+    if ((rc = lockstep_route(B, c0, GR_BEGIN, h_iter, B1, nullptr, 0, &n_begin))) return rc;
+    for (int k = 0; k < n && !rc; k++) {
+        CgGraph *G = &B->loops[order[k]];
+        cudaGraph_t body, s = nullptr;
+        pre[k] = add_conditional(ctx[k], B1, hh[k], cudaGraphCondTypeIf, &body, &rc);
+        if (rc) return rc;
+        GP_CUDA(c0, cudaGraphAddDependencies(B1, &n_begin, &pre[k], 1));
+        if ((rc = capture(ctx[k], G, SEQ_PRE, 0, 0, 0, &s, &G->n_pre))) return rc;
+        cudaGraphNode_t nn;
+        if ((rc = add_child(ctx[k], body, s, nullptr, 0, &nn))) return rc;
+    }
+    if ((rc = lockstep_route(B, c0, GR_LS0, h_ls, B1, pre.data(), pre.size(), &n_ls0))) return rc;
+    n_lsw = add_conditional(c0, B1, h_ls, cudaGraphCondTypeWhile, &B2, &rc);
+    if (rc) return rc;
+    GP_CUDA(c0, cudaGraphAddDependencies(B1, &n_ls0, &n_lsw, 1));
+    for (int k = 0; k < n && !rc; k++) {
+        CgGraph *G = &B->loops[order[k]];
+        cudaGraph_t body, s = nullptr;
+        post[k] = add_conditional(ctx[k], B1, hh[n + k], cudaGraphCondTypeIf, &body, &rc);
+        if (rc) return rc;
+        GP_CUDA(c0, cudaGraphAddDependencies(B1, &n_lsw, &post[k], 1));
+        if ((rc = capture(ctx[k], G, SEQ_POST, 0, 0, 0, &s, &G->n_post))) return rc;
+        cudaGraphNode_t nn;
+        if ((rc = add_child(ctx[k], body, s, nullptr, 0, &nn))) return rc;
+    }
+    if ((rc = lockstep_route(B, c0, GR_END, h_iter, B1, post.data(), post.size(), &n_end))) return rc;
+
+    // B2: per class, the trial prep of its instances, its grouped forward, their
+    // chi2 + controller; the CUDA-core instances' whole evaluations; LSN after all
+    std::vector<cudaGraphNode_t> last;  // what LSN waits for
+    for (int q = 0; q < B->ngrp && !rc; q++) {
+        const int k0 = cls_begin[q], k1 = cls_begin[q + 1];
+        std::vector<cudaGraphNode_t> bprep;
+        for (int k = k0; k < k1 && !rc; k++) {
+            gpair_ctx *c = ctx[k];
+            CgGraph *G = &B->loops[order[k]];
+            const int *gate = B->flags + n + k;
+            cudaGraph_t s = nullptr;
+            cudaGraphNode_t nd;
+            rc = capture_fn(
+                c,
+                [&]() {
+                    c->gate = gate;
+                    int r = gp_eval_batch_part(c, 1);
+                    c->gate = nullptr;
+                    return r;
+                },
+                &s, &G->n_crit);
+            if (rc || (rc = add_child(c, B2, s, nullptr, 0, &nd))) return rc;
+            bprep.push_back(nd);
+        }
+        cudaGraphNode_t n_gemm;
+        {
+            gpair_ctx *c = ctx[k0];
+            cudaGraph_t s = nullptr;
+            rc = capture_fn(c, [&]() { return gp_tc_group_forward(B->grps[q], c); }, &s, nullptr);
+            if (rc || (rc = add_child(c, B2, s, bprep.data(), bprep.size(), &n_gemm))) return rc;
+        }
+        for (int k = k0; k < k1 && !rc; k++) {
+            gpair_ctx *c = ctx[k];
+            CgGraph *G = &B->loops[order[k]];
+            const int *gate = B->flags + n + k;
+            cudaGraph_t s = nullptr;
+            int n2 = 0;
+            cudaGraphNode_t nd;
+            rc = capture_fn(
+                c,
+                [&]() {
+                    c->gate = gate;
+                    c->fuse_ctrl = CTRL_AFTER_BATCH;
+                    c->fuse_handles = 0;
+                    int r = gp_eval_batch_part(c, 2);
+                    c->fuse_ctrl = -1;
+                    c->gate = nullptr;
+                    return r;
+                },
+                &s, &n2);
+            if (rc || (rc = add_child(c, B2, s, &n_gemm, 1, &nd))) return rc;
+            G->n_crit += n2;
+            last.push_back(nd);
+        }
+    }
+    for (int k = ntc; k < n && !rc; k++) {
+        gpair_ctx *c = ctx[k];
+        CgGraph *G = &B->loops[order[k]];
+        const int *gate = B->flags + n + k;
+        cudaGraph_t s = nullptr;
+        cudaGraphNode_t nd;
+        rc = capture_fn(
+            c,
+            [&]() {
+                c->gate = gate;
+                c->fuse_ctrl = CTRL_AFTER_BATCH;
+                c->fuse_handles = 0;
+                int r = gp_eval_batch(c);
+                c->fuse_ctrl = -1;
+                c->gate = nullptr;
+                return r;
+            },
+            &s, &G->n_crit);
+        if (rc || (rc = add_child(c, B2, s, nullptr, 0, &nd))) return rc;
+        last.push_back(nd);
+    }
+    cudaGraphNode_t n_lsn;
+    return lockstep_route(B, c0, GR_LSN, h_ls, B2, last.data(), last.size(), &n_lsn);
+}
+
+int gp_batch_graph_build(gpair_ctx **ctx, int n, int ls_mode, int allow_group, void **out)
 {
     *out = nullptr;
     BatchGraph *B = (BatchGraph *)calloc(1, sizeof(BatchGraph));
@@ -272,12 +585,21 @@ int gp_batch_graph_build(gpair_ctx **ctx, int n, int ls_mode, void **out)
         G->precision = ctx[i]->precision;
         G->ls_mode = ls_mode;
         G->trace_cap = 1;  // one row; batch runs return no trace
-        if (cudaMalloc(&G->trace, sizeof(double) * 5) != cudaSuccess) {
-            rc = GPAIR_ERR_ALLOC;
-            break;
-        }
-        rc = add_loop(ctx[i], G, B->g);
+        if (cudaMalloc(&G->trace, sizeof(double) * 5) != cudaSuccess) rc = GPAIR_ERR_ALLOC;
     }
+    if (!rc && allow_group && ls_mode == GPAIR_LS_BATCH) {
+        rc = build_lockstep(ctx, n, B);
+        if (rc == GPAIR_OK) {
+            B->grouped = 1;
+        } else if (rc == GPAIR_ERR_STATE) {
+            // no instance on the tensor path: independent branches
+            cudaGraphDestroy(B->g);
+            B->g = nullptr;
+            rc = cudaGraphCreate(&B->g, 0) == cudaSuccess ? GPAIR_OK : GPAIR_ERR_CUDA;
+        }
+    }
+    for (int i = 0; i < n && !rc && !B->grouped; i++) rc = add_loop(ctx[i], &B->loops[i], B->g);
+    for (int i = 0; i < n && !rc; i++) B->loops[i].buf_gen = ctx[i]->buf_gen;
     if (!rc) {
         cudaError_t e = cudaGraphInstantiate(&B->exec, B->g, 0);
         if (e != cudaSuccess) {
@@ -301,6 +623,8 @@ int gp_batch_graph_launch(void *bg, cudaStream_t stream)
 }
 
 int gp_batch_graph_precision(void *bg, int i) { return ((BatchGraph *)bg)->loops[i].precision; }
+unsigned int gp_batch_graph_buf_gen(void *bg, int i) { return ((BatchGraph *)bg)->loops[i].buf_gen; }
+int gp_batch_graph_grouped(void *bg) { return bg ? ((BatchGraph *)bg)->grouped : 0; }
 
 long long gp_batch_graph_launches(void *bg, int i, int iterations_done, int criterion_evals, int grad_evals,
                                   int batches)

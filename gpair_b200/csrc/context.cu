@@ -21,10 +21,12 @@ int gp_cg_graph_run(gpair_ctx *c, int iterations, int want_trace, int ls_mode, l
 int gp_cg_graph_trace(gpair_ctx *c, int iterations, double *tJ, double *tchi2, double *tS, double *tstep,
                       double *tbeta);
 long long gp_cg_graph_launches(gpair_ctx *c, int iterations_done, int criterion_evals, int grad_evals, int batches);
-int gp_batch_graph_build(gpair_ctx **ctx, int n, int ls_mode, void **out);
+int gp_batch_graph_build(gpair_ctx **ctx, int n, int ls_mode, int allow_group, void **out);
 void gp_batch_graph_free(void *bg);
 int gp_batch_graph_launch(void *bg, cudaStream_t stream);
 int gp_batch_graph_precision(void *bg, int i);
+unsigned int gp_batch_graph_buf_gen(void *bg, int i);
+int gp_batch_graph_grouped(void *bg);
 long long gp_batch_graph_launches(void *bg, int i, int iterations_done, int criterion_evals, int grad_evals,
                                   int batches);
 
@@ -415,13 +417,14 @@ int gp_eval_criterion(gpair_ctx *c, int which, int trial)
 {
     int rc;
     gp_stage_begin(c, 0);
-    const bool fused_trial = trial && c->precision != GPAIR_PREC_FP32;
-    if (fused_trial) rc = gp_tc_prep_split_trial(c);  // trial image + f16 operand in one pass
+    // tensor path: image (or trial image), its sums and its forward operand in one pass
+    const bool tc = c->precision != GPAIR_PREC_FP32;
+    if (tc) rc = trial ? gp_tc_prep_split_trial(c) : gp_tc_prep_image(c, which);
     else rc = gp_prep_image(c, trial ? GPAIR_IMG_TEMP : which, trial, 0.0, trial);
     if (rc) return rc;
     gp_stage_end(c);
     gp_stage_begin(c, 1);
-    if (fused_trial) rc = gp_tc_forward_gemm(c);
+    if (tc) rc = gp_tc_forward_gemm(c);
     else rc = gp_forward(c, trial ? GPAIR_IMG_TEMP : which);
     if (rc) return rc;
     gp_stage_end(c);
@@ -897,7 +900,15 @@ extern "C" int gpair_batch_destroy(gpair_batch *b)
 
 extern "C" int gpair_batch_create(gpair_batch **out, gpair_ctx **ctx, int n, int line_search)
 {
+    return gpair_batch_create_ex(out, ctx, n, line_search, 0);
+}
+
+extern "C" int gpair_batch_grouped(const gpair_batch *b) { return b ? gp_batch_graph_grouped(b->graph) : 0; }
+
+extern "C" int gpair_batch_create_ex(gpair_batch **out, gpair_ctx **ctx, int n, int line_search, int flags)
+{
     if (!out || !ctx || n <= 0) return GPAIR_ERR_INVALID;
+    if (flags & ~GPAIR_BATCH_INDEPENDENT) return GPAIR_ERR_INVALID;
     if (line_search != GPAIR_LS_WOLFE && line_search != GPAIR_LS_BATCH) return GPAIR_ERR_INVALID;
     *out = nullptr;
     for (int i = 0; i < n; i++) {
@@ -929,7 +940,7 @@ extern "C" int gpair_batch_create(gpair_batch **out, gpair_ctx **ctx, int n, int
         ctx[i]->fuse_ctrl = -1;
         ctx[i]->fuse_handles = 0;
     }
-    if (!rc) rc = gp_batch_graph_build(ctx, n, line_search, &b->graph);
+    if (!rc) rc = gp_batch_graph_build(ctx, n, line_search, !(flags & GPAIR_BATCH_INDEPENDENT), &b->graph);
     if (rc) {
         gpair_batch_destroy(b);
         return rc;
@@ -946,8 +957,10 @@ extern "C" int gpair_batch_run(gpair_batch *b, const gpair_cg_params *p, gpair_c
     for (int i = 0; i < b->n; i++) {
         int rc = cg_validate(b->ctx[i], p);
         if (rc) return rc;
-        // the batch graph was captured with each context's precision path
-        if (gp_batch_graph_precision(b->graph, i) != b->ctx[i]->precision) return GPAIR_ERR_STATE;
+        // the batch graph was captured with each context's precision path and buffers
+        if (gp_batch_graph_precision(b->graph, i) != b->ctx[i]->precision ||
+            gp_batch_graph_buf_gen(b->graph, i) != b->ctx[i]->buf_gen)
+            return GPAIR_ERR_STATE;
     }
     std::vector<CgRun> r((size_t)b->n);
     GP_CUDA(b->ctx[0], cudaSetDevice(b->device));
@@ -1055,8 +1068,7 @@ extern "C" int gpair_time_stages(gpair_ctx *c, int reps, double *ms, int max_sta
         // stages queued back to back: the events time kernels, not host launch gaps
         cudaEvent_t *E = &ev[(size_t)r * (ns + 1)];
         cudaEventRecord(E[0], c->stream);
-        if ((rc = gp_prep_image(c, GPAIR_IMG_CURR, 0, 0.0, 0))) break;
-        if (tc && (rc = gp_tc_split(c, GPAIR_IMG_CURR))) break;
+        if ((rc = tc ? gp_tc_prep_image(c, GPAIR_IMG_CURR) : gp_prep_image(c, GPAIR_IMG_CURR, 0, 0.0, 0))) break;
         cudaEventRecord(E[1], c->stream);
         if ((rc = tc ? gp_tc_forward_gemm(c) : gp_forward(c, GPAIR_IMG_CURR))) break;
         cudaEventRecord(E[2], c->stream);

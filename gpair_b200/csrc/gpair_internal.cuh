@@ -104,9 +104,6 @@ struct CgState {
 struct DevScalars {
     double flux, invflux, entropy, chi2;
     double imax;          // max |image| of the last prepared image
-    double imax_curr;     // max |image| of the current CG image
-    unsigned int dmax_bits;  // max |descent direction| (float bits, atomic max)
-    float fwd_inv_scale;  // tensor forward: 1 / (image scale * twiddle scale)
     double adj_c;      // C = Re sum_k c_k V_k
     double cmax;       // max |c_k| (scaling of split operands)
     double gscale;     // factor applied to the summed adjoint partials (1, or 1/operand scales)
@@ -117,9 +114,8 @@ struct DevScalars {
     unsigned int counter[RED_NSLOTS];
     unsigned int nonfinite;  // set when a NaN/Inf reaches a reduction
     unsigned int tc_err;     // tensor-core kernels: bounded wait gave up (bit = which wait)
-    // batched trials: per-trial flux, entropy, chi2 and tensor forward scale
+    // batched trials: per-trial flux, entropy and chi2
     double t_flux[GP_NTR], t_invflux[GP_NTR], t_entropy[GP_NTR], t_chi2[GP_NTR];
-    float t_scale[GP_NTR];
     unsigned int t_counter[GP_NTR + 1];
     int *stop_flag;  // shared with racing runs (device memory), or null
     int reg_kind;    // GPAIR_REG_GULL_SKILLING / GPAIR_REG_L2
@@ -141,6 +137,74 @@ __device__ __forceinline__ double reg_term(double I, double m, int kind)
     if (kind == GPAIR_REG_L2) return m > 0.0 ? -I * I / (2.0 * m) : 0.0;
     return (I > 0.0 && m > 0.0) ? (I - m - I * log(I / m)) : -m;
 }
+// The same term in FP32 without cancellation, for sums accumulated in FP64.
+// With r = (I - m) / m: I - m - I ln(I/m) = m g(r),
+//   g(r) = r - (1 + r) ln(1 + r) = -r^2 sum_{k>=0} (-r)^k / ((k + 1)(k + 2)),
+// evaluated by the series (Horner, k <= 18: truncation below 2^-26 of the sum)
+// for |r| < 1/2, where I - m is exact (Sterbenz); elsewhere the closed form
+// (I - m) - I ln(I/m), whose two terms cancel by at most a factor of 6.
+// Relative error of a term: a few units of 2^-24.
+__device__ __forceinline__ float reg_term_f(float I, float m, int kind)
+{
+    if (kind == GPAIR_REG_L2) return m > 0.f ? -I * I / (2.f * m) : 0.f;
+    if (!(I > 0.f && m > 0.f)) return -m;
+    const float dlt = I - m;
+    if (fabsf(dlt) < 0.5f * m) {
+        const float r = dlt / m, t = -r;
+        float p = 1.f / 380.f;  // k = 18: 1 / (19 * 20)
+#pragma unroll
+        for (int k = 17; k >= 0; k--) p = fmaf(p, t, 1.f / (float)((k + 1) * (k + 2)));
+        return m * (-(r * r) * p);
+    }
+    return dlt - I * logf(I / m);
+}
+// reg_term_f of eight pixels, summed into `acc` in pixel order: the series is
+// evaluated for all eight at once (independent FMA chains, no branch), the
+// closed form only for pixels far from the prior. Same values as reg_term_f.
+__device__ __forceinline__ void reg_terms8(const float (&I)[8], const float (&m)[8], int kind, double &acc)
+{
+    float term[8];
+    if (kind == GPAIR_REG_L2) {
+#pragma unroll
+        for (int k = 0; k < 8; k++) term[k] = m[k] > 0.f ? -I[k] * I[k] / (2.f * m[k]) : 0.f;
+    } else {
+        float r[8], p[8];
+        bool near[8];
+        bool any_far = false;
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            const float dlt = I[k] - m[k];
+            near[k] = I[k] > 0.f && m[k] > 0.f && fabsf(dlt) < 0.5f * m[k];
+            any_far |= !near[k];
+            r[k] = near[k] ? dlt / m[k] : 0.f;
+            p[k] = 1.f / 380.f;
+        }
+#pragma unroll
+        for (int j = 17; j >= 0; j--) {
+            const float cj = 1.f / (float)((j + 1) * (j + 2));
+#pragma unroll
+            for (int k = 0; k < 8; k++) p[k] = fmaf(p[k], -r[k], cj);
+        }
+#pragma unroll
+        for (int k = 0; k < 8; k++) term[k] = m[k] * (-(r[k] * r[k]) * p[k]);
+        if (any_far) {
+#pragma unroll
+            for (int k = 0; k < 8; k++)
+                if (!near[k]) term[k] = (I[k] > 0.f && m[k] > 0.f) ? (I[k] - m[k]) - I[k] * logf(I[k] / m[k]) : -m[k];
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 8; k++) acc += (double)term[k];
+}
+
+// A graph-captured CG run goes on after an iteration (the end-of-iteration
+// test of the controller)
+__device__ __forceinline__ bool cg_run_goes_on(const DevScalars *sc)
+{
+    const CgState &s = sc->cg;
+    return s.run_it < s.run_limit && !sc->nonfinite && !sc->tc_err && !s.reached && !s.stopped;
+}
+
 __device__ __forceinline__ float reg_grad(float I, float m, float prev, int kind)
 {
     if (kind == GPAIR_REG_L2) return m > 0.f ? (float)(-(double)I / (double)m) : 0.f;
@@ -242,6 +306,11 @@ struct gpair_ctx {
     // the MMA and epilogue waits run out with no copy in flight
     long long tc_wait_budget;
     int tc_skip_loads;
+    // lockstep batches: device flag gating this context's batched-trial kernels (or null)
+    const int *gate;
+    // bumped whenever the tensor operands or the batch buffers are freed: graphs
+    // captured before hold stale pointers
+    unsigned int buf_gen;
     // tensor-core contractions on CTA pairs (tcgen05 cta_group::2) instead of single CTAs
     int tc_pair;
 };
@@ -305,11 +374,12 @@ enum { CTRL_BEGIN = 0, CTRL_AFTER_DIR = 1, CTRL_AFTER_CRIT = 2, CTRL_AFTER_GRAD 
 int gp_adjoint_image(gpair_ctx *c, const float2 *cw_host, float *out_host);
 int gp_update_pixel(gpair_ctx *c, int x, int y, float value);
 int gp_batch_alloc(gpair_ctx *c);
+int gp_eval_batch_part(gpair_ctx *c, int part);
 void gp_batch_free(gpair_ctx *c);
 int gp_eval_batch(gpair_ctx *c);
 int gp_eval_batch_timed(gpair_ctx *c, cudaEvent_t *ev);
 int gp_tc_batch_prepare(gpair_ctx *c, int *epp);
-int gp_trials_prep_launch(gpair_ctx *c, void *hi, void *lo, int Lpad, int Kx_pad, int tw_log2, int tf32);
+int gp_trials_prep_launch(gpair_ctx *c);
 int gp_tc_trials_prep_split(gpair_ctx *c, double *partials);
 int gp_tc_forward_batch_gemm(gpair_ctx *c);
 
@@ -318,6 +388,12 @@ int gp_tc_prepare(gpair_ctx *c);
 int gp_tc_forward(gpair_ctx *c, int which);
 int gp_tc_forward_gemm(gpair_ctx *c);
 int gp_tc_split(gpair_ctx *c, int which);
+int gp_tc_prep_image(gpair_ctx *c, int which);
+// grouped forward over the batched trials of several instances (lockstep batches)
+int gp_tc_group_key(gpair_ctx *c);
+int gp_tc_group_build(gpair_ctx **ctx, int n, const int *gate, unsigned int *err, void **out);
+int gp_tc_group_forward(void *grp, gpair_ctx *c);
+void gp_tc_group_free(void *grp);
 int gp_tc_build_w(gpair_ctx *c);
 int gp_tc_adjoint_gemm(gpair_ctx *c);
 int gp_tc_prep_split_trial(gpair_ctx *c);

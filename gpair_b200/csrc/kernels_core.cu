@@ -188,8 +188,7 @@ static int red_grid(long long n) { int g = gp_cdiv(n, GP_THREADS * 4); return g 
 int gp_prep_image(gpair_ctx *c, int which, int trial_mode, double step_host, int step_from_state)
 {
     const float *src = (which == GPAIR_IMG_TEMP && !trial_mode) ? c->image_temp : c->image;
-    int g = gp_cdiv(c->npix, GP_THREADS);
-    if (g > GP_MAX_PARTIALS) g = GP_MAX_PARTIALS;
+    const int g = red_grid(c->npix);  // one wave, several pixels per thread: a short reduction tail
     k_prep<<<g, GP_THREADS, 0, c->stream>>>(src, c->descent_dir, c->image_temp, c->model, c->npix, trial_mode,
                                             step_host, step_from_state, (double)1e-8, slot_partials(c, RED_PREP),
                                             c->sc);
@@ -205,8 +204,9 @@ int gp_prep_image(gpair_ctx *c, int which, int trial_mode, double step_host, int
 
 __global__ void __launch_bounds__(256) k_fwd_simt(const float *__restrict__ img, const float2 *__restrict__ fx,
                                                   const float2 *__restrict__ fy, int N, int nuv,
-                                                  float2 *__restrict__ vpart)
+                                                  float2 *__restrict__ vpart, const int *__restrict__ gate)
 {
+    if (gate && !*gate) return;  // lockstep batches: this instance's line search is over
     __shared__ float As[FB_X][FB_M + 1];
     __shared__ float2 Bs[FB_X][FB_K + 1];
     __shared__ float2 red[16][FB_K + 1];
@@ -280,7 +280,7 @@ int gp_forward(gpair_ctx *c, int which)
     const float *img = (which == GPAIR_IMG_TEMP) ? c->image_temp : c->image;
     c->mt = gp_cdiv(c->N, FB_M);
     dim3 grid(gp_cdiv(c->nuv, FB_K), c->mt);
-    k_fwd_simt<<<grid, 256, 0, c->stream>>>(img, c->fx, c->fy, c->N, c->nuv, c->vpart);
+    k_fwd_simt<<<grid, 256, 0, c->stream>>>(img, c->fx, c->fy, c->N, c->nuv, c->vpart, nullptr);
     GP_LAUNCH_CHECK(c);
     return GPAIR_OK;
 }
@@ -813,19 +813,14 @@ __global__ void __launch_bounds__(GP_THREADS) k_descent(float *__restrict__ d, c
     __shared__ double smem[32];
     const double beta = beta_from_state ? sc->cg.beta : beta_host;
     double acc[1] = {0.0};
-    double dmax = 0.0;
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
         // beta = 0 (first iteration, restarts) must not read the old direction:
         // 0 * d_old is NaN when a previous run left non-finite values there
         float dn = beta != 0.0 ? (float)(beta * (double)d[p] - (double)g[p]) : -g[p];
         d[p] = dn;
         acc[0] += (double)dn * (double)g[p];
-        dmax = fmax(dmax, fabs((double)dn));
     }
     block_sum<1>(acc, smem);
-    dmax = block_max(dmax, smem);
-    // max |d| bounds the trial images (order-independent, so an atomic max stays deterministic)
-    if (threadIdx.x == 0) atomicMax(&sc->dmax_bits, __float_as_uint((float)dmax));
     if (threadIdx.x == 0) partials[blockIdx.x] = acc[0];
     if (last_block(&sc->counter[RED_DIR])) {
         double o[1];
@@ -994,7 +989,6 @@ __global__ void __launch_bounds__(GP_THREADS) k_lbfgs_combine(const float *__res
         cb[i] = cs.lb_cy[i];
     }
     double acc[1] = {0.0};
-    double dmax = 0.0;
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
         const float I = img[p], gp = g[p];
         xold[p] = I;
@@ -1008,11 +1002,8 @@ __global__ void __launch_bounds__(GP_THREADS) k_lbfgs_combine(const float *__res
         }
         d[p] = dn;
         acc[0] += (double)dn * (double)gp;
-        dmax = fmax(dmax, fabs((double)dn));
     }
     block_sum<1>(acc, smem);
-    dmax = block_max(dmax, smem);
-    if (threadIdx.x == 0) atomicMax(&sc->dmax_bits, __float_as_uint((float)dmax));
     if (threadIdx.x == 0) partials[blockIdx.x] = acc[0];
     if (last_block(&sc->counter[RED_DIR])) {
         double o[1];
@@ -1121,104 +1112,31 @@ int gp_update_temp(gpair_ctx *c, double step, double minval, int clamp)
 // ------------------------------------------- batched line-search trials
 
 // GP_NTR trial images I_j = max(I + s_j d, minval) (s_j = cg.ts[j], blockIdx.y
-// = j), each with its flux and entropy summed in FP64 (the trial part of
-// kernel_update_tempimage.cl + kernel_entropy_gs.cl, for a whole batch). On the
-// tensor path (hi != nullptr) the hi/lo forward operand of trial j (f16, or
-// TF32 held as FP32; lo == nullptr in one-product mode) is written to rows
-// [j Lpad, j Lpad + N) with the power-of-two scale of the bound
-// max|I_j| <= max|I| + |s_j| max|d|.
-__device__ __forceinline__ void trial_split(float v, __half &h, __half &l)
-{
-    h = __float2half_rn(v);
-    l = __float2half_rn(v - __half2float(h));
-}
-__device__ __forceinline__ void trial_split(float v, float &h, float &l)
-{
-    h = umma::tf32_rna(v);
-    l = umma::tf32_rna(v - h);
-}
-
-template <typename OT>
+// = j), each with its flux and regulariser summed in FP64 (the trial part of
+// kernel_update_tempimage.cl + kernel_entropy_gs.cl, for a whole batch), for
+// the CUDA-core forward; the tensor path prepares its trials row by row
+// together with their operands (k_tc_prep_rows).
 __global__ void __launch_bounds__(GP_THREADS) k_trials_prep(const float *__restrict__ img,
                                                             const float *__restrict__ d, float *__restrict__ trials,
-                                                            const float *__restrict__ model, int N, int npix,
-                                                            OT *__restrict__ hi, OT *__restrict__ lo,
-                                                            int Lpad, int Kx_pad, int tw_log2,
+                                                            const float *__restrict__ model, int npix,
                                                             double *__restrict__ partials,
-                                                            DevScalars *__restrict__ sc)
+                                                            DevScalars *__restrict__ sc, const int *__restrict__ gate)
 {
     __shared__ double smem[2 * 32];
+    if (gate && !*gate) return;  // lockstep batches: this instance's line search is over
     const int j = blockIdx.y;
     const double s = sc->cg.ts[j], minval = sc->cg.minvalue;
-    int ex = 0;
-    float scale = 1.f;
-    if (hi) {
-        double bound = sc->imax_curr + fabs(s) * (double)__uint_as_float(sc->dmax_bits);
-        if (bound < minval) bound = minval;
-        frexp(bound, &ex);
-        scale = ldexpf(1.f, 15 - ex);
-    }
     float *dst = trials + (size_t)j * npix;
     double acc[2] = {0.0, 0.0};
     const int reg_kind = sc->reg_kind;
-    if ((N & 7) == 0) {
-        // 8 consecutive pixels of one row per thread: 16-byte loads and stores
-        const int n8 = npix >> 3;
-        for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n8; q += gridDim.x * blockDim.x) {
-            const int p0 = q << 3;
-            __align__(16) float iv[8], dv[8], mv[8], out[8];
-            __align__(16) OT hv[8], lv[8];
-            *reinterpret_cast<float4 *>(&iv[0]) = __ldg(reinterpret_cast<const float4 *>(img + p0));
-            *reinterpret_cast<float4 *>(&iv[4]) = __ldg(reinterpret_cast<const float4 *>(img + p0 + 4));
-            *reinterpret_cast<float4 *>(&dv[0]) = __ldg(reinterpret_cast<const float4 *>(d + p0));
-            *reinterpret_cast<float4 *>(&dv[4]) = __ldg(reinterpret_cast<const float4 *>(d + p0 + 4));
-            *reinterpret_cast<float4 *>(&mv[0]) = __ldg(reinterpret_cast<const float4 *>(model + p0));
-            *reinterpret_cast<float4 *>(&mv[4]) = __ldg(reinterpret_cast<const float4 *>(model + p0 + 4));
-#pragma unroll
-            for (int k = 0; k < 8; k++) {
-                double t = (double)iv[k] + s * (double)dv[k];
-                if (t < minval) t = minval;
-                const float I = (float)t;
-                out[k] = I;
-                const double Id = I;
-                acc[0] += Id;
-                acc[1] += reg_term(Id, (double)mv[k], reg_kind);
-                if (hi) trial_split(I * scale, hv[k], lv[k]);
-            }
-            *reinterpret_cast<float4 *>(dst + p0) = *reinterpret_cast<const float4 *>(&out[0]);
-            *reinterpret_cast<float4 *>(dst + p0 + 4) = *reinterpret_cast<const float4 *>(&out[4]);
-            if (hi) {
-                const int y = p0 / N, x = p0 - y * N;
-                const size_t o = ((size_t)j * Lpad + y) * Kx_pad + x;
-                constexpr int NV = sizeof(OT) * 8 / 16;
-#pragma unroll
-                for (int v = 0; v < NV; v++) reinterpret_cast<uint4 *>(hi + o)[v] = reinterpret_cast<const uint4 *>(hv)[v];
-                if (lo) {
-#pragma unroll
-                    for (int v = 0; v < NV; v++)
-                        reinterpret_cast<uint4 *>(lo + o)[v] = reinterpret_cast<const uint4 *>(lv)[v];
-                }
-            }
-        }
-    } else {
-        for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
-            double t = (double)img[p] + s * (double)d[p];
-            if (t < minval) t = minval;
-            const float I = (float)t;
-            dst[p] = I;
-            const double Id = I, m = model[p];
-            acc[0] += Id;
-            acc[1] += reg_term(Id, m, reg_kind);
-            if (hi) {
-                const int y = p / N, x = p - y * N;
-                const float v = I * scale;
-                const size_t o = ((size_t)j * Lpad + y) * Kx_pad + x;
-                OT h, l;
-                trial_split(v, h, l);
-                hi[o] = h;
-                if (lo) lo[o] = l;
-            }
-        }
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
+        double t = (double)img[p] + s * (double)d[p];
+        if (t < minval) t = minval;
+        const float I = (float)t;
+        dst[p] = I;
+        const double Id = I, m = model[p];
+        acc[0] += Id;
+        acc[1] += reg_term(Id, m, reg_kind);
     }
     block_sum<2>(acc, smem);
     double *pp = partials + (size_t)j * gridDim.x * 2;
@@ -1233,7 +1151,6 @@ __global__ void __launch_bounds__(GP_THREADS) k_trials_prep(const float *__restr
             sc->t_flux[j] = o[0];
             sc->t_invflux[j] = 1.0 / o[0];
             sc->t_entropy[j] = o[1];
-            sc->t_scale[j] = hi ? ldexpf(1.f, ex - 15 - tw_log2) : 1.f;
             sc->t_counter[j] = 0;
         }
     }
@@ -1249,9 +1166,11 @@ __global__ void __launch_bounds__(GP_THREADS) k_vis_chi2_batch(const float2 *__r
                                                                const int4 *__restrict__ tri,
                                                                const float2 *__restrict__ phasor,
                                                                double *__restrict__ partials,
-                                                               DevScalars *__restrict__ sc, FusedCtrl fc)
+                                                               DevScalars *__restrict__ sc, FusedCtrl fc,
+                                                               const int *__restrict__ gate)
 {
     __shared__ double smem[32];
+    if (gate && !*gate) return;  // lockstep batches: this instance's line search is over
     const int j = blockIdx.y;
     const double invF = sc->t_invflux[j];
     const float2 *vp = vpart + (size_t)j * epp * nuv;
@@ -1322,29 +1241,29 @@ static int batch_wave_blocks(const void *kernel, int nsm)
 
 int gp_batch_alloc(gpair_ctx *c)
 {
-    if (c->image_trials) return GPAIR_OK;
-    const int mt_simt = gp_cdiv(c->N, FB_M);
     int epp_tc = 0;
     if (c->precision != GPAIR_PREC_FP32) {
+        // every time: the tensor state (and its trial operand stack) is rebuilt when
+        // the precision or the tile layout changes, the trial images are not
         int rc = gp_tc_batch_prepare(c, &epp_tc);
         if (rc) return rc;
     }
+    if (c->image_trials) return GPAIR_OK;
+    const int mt_simt = gp_cdiv(c->N, FB_M);
     const int epp_max = mt_simt > epp_tc ? mt_simt : epp_tc;
     GP_CUDA(c, cudaMalloc(&c->image_trials, sizeof(float) * (size_t)GP_NTR * c->npix));
     GP_CUDA(c, cudaMalloc(&c->vpart_b, sizeof(float2) * (size_t)GP_NTR * epp_max * (c->nuv ? c->nuv : 1)));
     GP_CUDA(c, cudaMalloc(&c->partials_b, sizeof(double) * (size_t)GP_NTR * 1024 * 2));
     int nsm = 148;
     GP_CUDA(c, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
-    // one wave of either operand kind's trial-prep kernel
-    const int w16 = batch_wave_blocks((const void *)k_trials_prep<__half>, nsm);
-    const int w32 = batch_wave_blocks((const void *)k_trials_prep<float>, nsm);
-    c->batch_wave[0] = w16 < w32 ? w16 : w32;
+    c->batch_wave[0] = batch_wave_blocks((const void *)k_trials_prep, nsm);
     c->batch_wave[1] = batch_wave_blocks((const void *)k_vis_chi2_batch, nsm);
     return GPAIR_OK;
 }
 
 void gp_batch_free(gpair_ctx *c)
 {
+    if (c->image_trials) c->buf_gen++;
     if (c->image_trials) cudaFree(c->image_trials);
     if (c->vpart_b) cudaFree(c->vpart_b);
     if (c->partials_b) cudaFree(c->partials_b);
@@ -1353,17 +1272,27 @@ void gp_batch_free(gpair_ctx *c)
     c->partials_b = nullptr;
 }
 
-int gp_trials_prep_launch(gpair_ctx *c, void *hi, void *lo, int Lpad, int Kx_pad, int tw_log2, int tf32)
+int gp_trials_prep_launch(gpair_ctx *c)
 {
     dim3 g(batch_blocks_per_trial(c), GP_NTR);
-    if (tf32)
-        k_trials_prep<float><<<g, GP_THREADS, 0, c->stream>>>(c->image, c->descent_dir, c->image_trials, c->model,
-                                                               c->N, c->npix, (float *)hi, (float *)lo, Lpad, Kx_pad,
-                                                               tw_log2, c->partials_b, c->sc);
-    else
-        k_trials_prep<__half><<<g, GP_THREADS, 0, c->stream>>>(c->image, c->descent_dir, c->image_trials, c->model,
-                                                                c->N, c->npix, (__half *)hi, (__half *)lo, Lpad,
-                                                                Kx_pad, tw_log2, c->partials_b, c->sc);
+    k_trials_prep<<<g, GP_THREADS, 0, c->stream>>>(c->image, c->descent_dir, c->image_trials, c->model, c->npix,
+                                                   c->partials_b, c->sc, c->gate);
+    GP_LAUNCH_CHECK(c);
+    return GPAIR_OK;
+}
+
+// chi2 of the GP_NTR trials of a batch from their partial visibilities (epp
+// entries per trial), then the fused controller
+static int batch_chi2(gpair_ctx *c, int epp)
+{
+    int nb = gp_cdiv(c->npow + c->nbis, GP_THREADS * 2);
+    if (nb > c->batch_wave[1]) nb = c->batch_wave[1];  // one wave over the batch
+    if (nb > 1024) nb = 1024;
+    if (nb < 1) nb = 1;
+    dim3 g(nb, GP_NTR);
+    k_vis_chi2_batch<<<g, GP_THREADS, 0, c->stream>>>(c->vpart_b, epp, c->nuv, c->npow, c->nbis, c->data,
+                                                      c->data_err, c->tri, c->phasor, c->partials_b, c->sc,
+                                                      take_fused_ctrl(c), c->gate);
     GP_LAUNCH_CHECK(c);
     return GPAIR_OK;
 }
@@ -1386,30 +1315,35 @@ static int eval_batch(gpair_ctx *c, cudaEvent_t *ev)
         if ((rc = gp_tc_forward_batch_gemm(c))) return rc;
         epp = c->epp;
     } else {
-        if ((rc = gp_trials_prep_launch(c, nullptr, nullptr, 0, 0, 0, 0))) return rc;
+        if ((rc = gp_trials_prep_launch(c))) return rc;
         gp_stage_end(c);
         if (ev) cudaEventRecord(ev[1], c->stream);
         gp_stage_begin(c, 1);
         epp = gp_cdiv(c->N, FB_M);
         dim3 grid(gp_cdiv(c->nuv, FB_K), epp, GP_NTR);
-        k_fwd_simt<<<grid, 256, 0, c->stream>>>(c->image_trials, c->fx, c->fy, c->N, c->nuv, c->vpart_b);
+        k_fwd_simt<<<grid, 256, 0, c->stream>>>(c->image_trials, c->fx, c->fy, c->N, c->nuv, c->vpart_b, c->gate);
         GP_LAUNCH_CHECK(c);
     }
     gp_stage_end(c);
     if (ev) cudaEventRecord(ev[2], c->stream);
     gp_stage_begin(c, 2);
-    int nb = gp_cdiv(c->npow + c->nbis, GP_THREADS * 2);
-    if (nb > c->batch_wave[1]) nb = c->batch_wave[1];  // one wave over the batch
-    if (nb > 1024) nb = 1024;
-    if (nb < 1) nb = 1;
-    dim3 g(nb, GP_NTR);
-    k_vis_chi2_batch<<<g, GP_THREADS, 0, c->stream>>>(c->vpart_b, epp, c->nuv, c->npow, c->nbis, c->data,
-                                                      c->data_err, c->tri, c->phasor, c->partials_b, c->sc,
-                                                      take_fused_ctrl(c));
-    GP_LAUNCH_CHECK(c);
+    if ((rc = batch_chi2(c, epp))) return rc;
     gp_stage_end(c);
     if (ev) cudaEventRecord(ev[3], c->stream);
     return GPAIR_OK;
+}
+
+// The parts of a batched evaluation around its forward, for lockstep batches
+// whose forwards run as one grouped launch (tensor path): 1 = trial images and
+// operands, 2 = chi2 of each trial and the controller.
+int gp_eval_batch_part(gpair_ctx *c, int part)
+{
+    int rc = gp_batch_alloc(c);
+    if (rc) return rc;
+    if (c->precision == GPAIR_PREC_FP32) return GPAIR_ERR_STATE;
+    if (part == 1) return gp_tc_trials_prep_split(c, c->partials_b);
+    if ((rc = gp_tc_batch_prepare(c, nullptr))) return rc;
+    return batch_chi2(c, c->epp);
 }
 
 int gp_eval_batch(gpair_ctx *c) { return eval_batch(c, nullptr); }
@@ -1736,8 +1670,6 @@ __device__ __noinline__ static void cg_step(DevScalars *__restrict__ sc, CgState
         for (int i = 0; i <= GP_LB_PAIRS; i++) s.lb_slot[i] = i;
         break;
     case CTRL_BEGIN: {
-        sc->imax_curr = sc->imax;  // exact max of the current image (its prep ran this iteration)
-        sc->dmax_bits = 0u;        // k_descent re-reduces max |d|
         // criterion and gradient of the current image are done (gpair.c:688-724);
         // beta from the FP64 dot products of the gradient finalize (gpair.c:727-758)
         s.J = sc->chi2 - s.alpha * sc->entropy;
@@ -1929,11 +1861,9 @@ __device__ void cg_set_handles(DevScalars *__restrict__ sc, int what, cudaGraphC
     case CTRL_AFTER_GRAD:
         cudaGraphSetConditional(h_ls, s.action != CG_DONE ? 1u : 0u);
         break;
-    case CTRL_END: {
-        bool more = s.run_it < s.run_limit && !sc->nonfinite && !sc->tc_err && !s.reached && !s.stopped;
-        cudaGraphSetConditional(h_iter, more ? 1u : 0u);
+    case CTRL_END:
+        cudaGraphSetConditional(h_iter, cg_run_goes_on(sc) ? 1u : 0u);
         break;
-    }
     default:
         break;
     }

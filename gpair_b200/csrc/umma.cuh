@@ -78,6 +78,14 @@ __device__ __forceinline__ void tma_prefetch(const CUtensorMap *map)
     asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
 }
 
+// A tensor map held in global memory (written before the launch) becomes
+// visible to the tensor-map proxy of this thread.
+__device__ __forceinline__ void tensormap_acquire(const CUtensorMap *map)
+{
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(reinterpret_cast<uint64_t>(map))
+                 : "memory");
+}
+
 // 2-D tiled load (no multicast): box at (x = inner coordinate, y) into smem,
 // completion reported as transaction bytes on `bar`.
 __device__ __forceinline__ void tma_load_2d(void *smem_dst, const CUtensorMap *map, uint64_t *bar, int x, int y)
@@ -174,6 +182,31 @@ __device__ __forceinline__ uint64_t smem_desc_k_sw128(const void *tile)
     return d;
 }
 
+// The same for a K-major tile whose rows are 64 B (64 x 8-bit) written by TMA
+// with 64-byte swizzling: 8-row core groups of 512 B (SBO), layout SWIZZLE_64B
+// (4). Advancing K by 32 elements within the row adds 32 B to the start.
+__device__ __forceinline__ uint64_t smem_desc_k_sw64(const void *tile)
+{
+    uint64_t addr = smem_u32(tile);
+    uint64_t d = 0;
+    d |= (addr >> 4) & 0x3FFFull;       // start address
+    d |= (uint64_t)1 << 16;             // leading byte offset (unused for swizzled K-major)
+    d |= (uint64_t)(512 >> 4) << 32;    // stride byte offset: 8 rows x 64 B
+    d |= (uint64_t)1 << 46;             // version
+    d |= (uint64_t)4 << 61;             // SWIZZLE_64B
+    return d;
+}
+
+// Instruction descriptor, kind::i8: D s32 (fmt 2), A/B signed 8-bit (fmt 1), both K-major.
+__host__ __device__ constexpr uint32_t idesc_i8(int M, int N)
+{
+    return (2u << 4)                       // D format s32
+           | (1u << 7)                     // A signed 8-bit
+           | (1u << 10)                    // B signed 8-bit
+           | ((uint32_t)(N >> 3) << 17)    // N / 8
+           | ((uint32_t)(M >> 4) << 24);   // M / 16
+}
+
 // Instruction descriptor, kind::f16 / kind::tf32: D f32, A/B f16 (fmt 0), bf16
 // (fmt 1) or tf32 (fmt 2, with kind::tf32), both K-major.
 __host__ __device__ constexpr uint32_t idesc_f16(int M, int N, int ab_fmt)
@@ -266,6 +299,18 @@ __device__ __forceinline__ void mma_tf32_pair(uint32_t d_tmem, uint64_t a_desc, 
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::2.kind::tf32 [%0], %1, %2, %3, {%5, %5, %5, %5, %5, %5, %5, %5}, p;\n\t}"
+        ::"r"(d_tmem), "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate), "r"(0u)
+        : "memory");
+}
+
+// D (+)= A * B^T over the CTA pair, kind::i8 (signed 8-bit operands, S32 accumulator)
+__device__ __forceinline__ void mma_i8_pair(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                            uint32_t accumulate)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, {%5, %5, %5, %5, %5, %5, %5, %5}, p;\n\t}"
         ::"r"(d_tmem), "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate), "r"(0u)
         : "memory");
 }

@@ -3,7 +3,9 @@
 //
 // Precision (GPAIR_PREC_SPLIT16): every operand x is stored as a pair of f16
 // values hi = f16(x), lo = f16(x - hi) after a power-of-two scaling that puts
-// the operand near the top of the f16 range; a product is formed as
+// the operand near the top of the f16 range (twiddles: 2^10; the forward's
+// image operand: one scale per image row, from the row's max; the adjoint's
+// weights: one scale from max |c_k|); a product is formed as
 // A_hi B_hi + A_hi B_lo + A_lo B_hi with FP32 accumulation (the lo*lo term is
 // below 2^-22 of the result). Scales are exact powers of two and are removed
 // in the epilogues.
@@ -48,6 +50,7 @@
 #define TC_STAGE_BYTES (2 * TC_A_BYTES + 2 * TC_B_BYTES)
 #define TC_TMEM_COLS 512
 #define TC_SMEM_BYTES (1024 + TC_STAGES * TC_STAGE_BYTES + 256)
+#define TC_SMEM_GROUP_BYTES (TC_SMEM_BYTES + 4 * 272)  // + unit prefix sums of up to TC_GROUP_MAX instances
 #define TC_WAIT_BUDGET 4000000000LL  // default clock cycles (~2 s) per pipeline wait
 #define RPMAS_TC ((3.14159265358979323 / 180.0) / 3600000.0)  // radians per milliarcsecond
 
@@ -95,10 +98,11 @@ struct TcArgs {
     const float2 *fya, *fyr;
     int nanc;
     int N, nuv;
-    // image-side rows: lpad rows per image, partial entries of 2^elog2 rows,
-    // epp entries per image; batch: per-image scales sc->t_scale[image]
-    int lpad, elog2, epp, batch;
-    const DevScalars *sc;
+    // image-side rows: lpad rows per image, partial entries of 2^elog2 rows;
+    // rsc[row]: power-of-two factor of every image-side row (operand scale and
+    // twiddle scale removed in the epilogue)
+    int lpad, elog2;
+    const float *rsc;
     float2 *vpart;
     // store epilogue
     float *gpart;
@@ -110,7 +114,26 @@ struct TcArgs {
     // make the other roles' waits run out with nothing in flight)
     long long budget;
     int skip_loads;
+    // grouped forward (GROUP = 1): ninst instances, the units of instance i
+    // taken when gate[i] != 0
+    const struct TcGroupInst *grp;
+    const int *gate;
+    int ninst;
 };
+
+// One instance of a grouped forward launch: its operand maps (the twiddles and
+// the stacked trial images of its batched line search) and its epilogue
+// arguments. Held in global memory; the maps are read through their generic
+// addresses.
+struct __align__(64) TcGroupInst {
+    CUtensorMap A_hi, A_lo, B_hi, B_lo;
+    int m_tiles, n_tiles, kb_total, units;
+    const float2 *fya, *fyr;
+    int nanc, nuv, lpad, elog2;
+    const float *rsc;
+    float2 *vpart;
+};
+#define TC_GROUP_MAX 256  // instances of one grouped launch (prefix sums in shared memory)
 
 struct TcState {
     // A side (M = 128 rows): forward twiddles [rows_pad][Kx_pad], adjoint twiddles [xrows_pad][K2_pad]
@@ -123,6 +146,9 @@ struct TcState {
     int Lb, epp_b;
     void *imgb_hi, *imgb_lo;
     CUtensorMap m_imgb_hi, m_imgb_lo;
+    // power-of-two factor of every image-side operand row: single image
+    // [M_pad], batch stack [GP_NTR Lb] (zero on padding rows)
+    float *rsc, *rscb;
     int splits, kb_per;
     void *img_hi, *img_lo, *fx_hi, *fx_lo, *fxt_hi, *fxt_lo, *w_hi, *w_lo;
     float2 *fya, *fyr;
@@ -162,6 +188,27 @@ __device__ __forceinline__ void tc_decode(const TcArgs &a, int u, int &m, int &n
     }
 }
 
+// Unit u of a launch: tile (m, n), K-blocks [kb0, kb1), split. GROUP = 1: u
+// counts the units of the gated instances in instance order (prefix sums
+// gpre[0..ninst]); `ci` is the caller's instance cursor, which only moves
+// forward because every role visits its units in increasing order.
+template <int EPI, int GROUP>
+__device__ __forceinline__ void tc_unit(const TcArgs &a, const int *gpre, int u, int &ci, int &m, int &n, int &kb0,
+                                        int &kb1, int &split)
+{
+    if (GROUP) {
+        while (gpre[ci + 1] <= u) ci++;
+        const int lu = u - gpre[ci], nt = a.grp[ci].n_tiles;
+        n = lu % nt;
+        m = lu / nt;
+        split = 0;
+        kb0 = 0;
+        kb1 = a.grp[ci].kb_total;
+    } else {
+        tc_decode<EPI>(a, u, m, n, kb0, kb1, split);
+    }
+}
+
 // PAIR = 0: one CTA per tile of 128 (A rows) x 256 (B rows), 2 stages of 96 KB.
 // PAIR = 1: a cluster of two CTAs shares one tcgen05.mma.cta_group::2 tile of
 // 256 x 256: each CTA stages 128 rows of A and 128 rows of B (half of the tile's
@@ -179,11 +226,15 @@ template <int PAIR> struct TcGeo {
 };
 static_assert(TcGeo<0>::STAGES * TcGeo<0>::STAGE == TcGeo<1>::STAGES * TcGeo<1>::STAGE, "same smem in both modes");
 
-template <int EPI, int OP, int NPROD, int PAIR>
+// GROUP = 1 (forward only): one launch over the units of several instances
+// (TcGroupInst), each with its own maps and epilogue arguments; the kernel's
+// map parameters are not used.
+template <int EPI, int OP, int NPROD, int PAIR, int GROUP>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     k_tc_gemm(const __grid_constant__ CUtensorMap tA_hi, const __grid_constant__ CUtensorMap tA_lo,
               const __grid_constant__ CUtensorMap tB_hi, const __grid_constant__ CUtensorMap tB_lo, const TcArgs a)
 {
+    static_assert(!GROUP || EPI == EPI_FWD, "grouped launches run the forward");
     using G = TcGeo<PAIR>;
     extern __shared__ unsigned char smem_raw[];
     unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -195,6 +246,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     uint64_t *done_bar = tempty + 2;
     uint32_t *tmem_slot = (uint32_t *)(done_bar + 1);
     volatile int *abort_flag = (volatile int *)(tmem_slot + 1);
+    int *gpre = (int *)(smem + G::STAGES * G::STAGE + 256);  // GROUP: unit prefix sums
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t rank = PAIR ? umma::cluster_ctarank() : 0u;
@@ -214,6 +266,25 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         *abort_flag = 0;
         umma::fence_barrier_init();
     }
+    if (GROUP) {
+        // units of the gated instances, then their prefix sums (warp 0, 32 at a time)
+        for (int i = threadIdx.x; i < a.ninst; i += blockDim.x) gpre[i + 1] = a.gate[i] ? a.grp[i].units : 0;
+        __syncthreads();
+        if (warp == 0) {
+            int carry = 0;
+            for (int b = 0; b < a.ninst; b += 32) {
+                int v = b + lane < a.ninst ? gpre[b + lane + 1] : 0;
+#pragma unroll
+                for (int off = 1; off < 32; off <<= 1) {
+                    const int o = __shfl_up_sync(0xffffffffu, v, off);
+                    if (lane >= off) v += o;
+                }
+                if (b + lane < a.ninst) gpre[b + lane + 1] = v + carry;
+                carry += __shfl_sync(0xffffffffu, v, 31);
+            }
+            if (lane == 0) gpre[0] = 0;
+        }
+    }
     if (warp == 1) {
         if (PAIR) {
             umma::tmem_alloc_pair(tmem_slot, TC_TMEM_COLS);
@@ -228,19 +299,35 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     if (PAIR) umma::cluster_sync_all();  // both CTAs' barriers initialised before any remote arrival
     umma::tc_fence_after();
     const uint32_t tmem_base = *tmem_slot;
+    const int units = GROUP ? gpre[a.ninst] : a.units;
 
     if (warp == 0) {
         if (lane == 0) {
             // ------------------------------------------------ TMA producer
-            umma::tma_prefetch(&tA_hi);
-            umma::tma_prefetch(&tA_lo);
-            umma::tma_prefetch(&tB_hi);
-            umma::tma_prefetch(&tB_lo);
+            const CUtensorMap *mAh = &tA_hi, *mAl = &tA_lo, *mBh = &tB_hi, *mBl = &tB_lo;
+            if (!GROUP) {
+                umma::tma_prefetch(mAh);
+                umma::tma_prefetch(mAl);
+                umma::tma_prefetch(mBh);
+                umma::tma_prefetch(mBl);
+            }
             const uint32_t tx = (NPROD == 3 ? G::STAGE : TC_A_BYTES + G::B_BYTES) * (PAIR ? 2 : 1);
-            int it = 0;
-            for (int u = unit0; u < a.units && !*abort_flag; u += ustep) {
+            int it = 0, ci = 0, cur = -1;
+            for (int u = unit0; u < units && !*abort_flag; u += ustep) {
                 int m, n, kb0, kb1, split;
-                tc_decode<EPI>(a, u, m, n, kb0, kb1, split);
+                tc_unit<EPI, GROUP>(a, gpre, u, ci, m, n, kb0, kb1, split);
+                if (GROUP && ci != cur) {
+                    // this instance's maps, written to global memory before the launch
+                    cur = ci;
+                    mAh = &a.grp[ci].A_hi;
+                    mAl = &a.grp[ci].A_lo;
+                    mBh = &a.grp[ci].B_hi;
+                    mBl = &a.grp[ci].B_lo;
+                    umma::tensormap_acquire(mAh);
+                    umma::tensormap_acquire(mAl);
+                    umma::tensormap_acquire(mBh);
+                    umma::tensormap_acquire(mBl);
+                }
                 const int arow0 = m * G::MT + (int)rank * 128, brow0 = n * TC_BN + (int)rank * G::BROWS;
                 for (int kb = kb0; kb < kb1; kb++) {
                     const int s = it % G::STAGES;
@@ -256,19 +343,19 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                         // both CTAs' bytes are counted on the leader's barrier
                         const uint32_t fb = umma::mapa_shared(umma::smem_u32(&full[s]), 0);
                         if (leader) umma::mbar_arrive_expect_tx(&full[s], tx);
-                        umma::tma_load_2d_pair(st, &tA_hi, fb, kx, arow0);
-                        umma::tma_load_2d_pair(st + 2 * TC_A_BYTES, &tB_hi, fb, kx, brow0);
+                        umma::tma_load_2d_pair(st, mAh, fb, kx, arow0);
+                        umma::tma_load_2d_pair(st + 2 * TC_A_BYTES, mBh, fb, kx, brow0);
                         if (NPROD == 3) {
-                            umma::tma_load_2d_pair(st + TC_A_BYTES, &tA_lo, fb, kx, arow0);
-                            umma::tma_load_2d_pair(st + 2 * TC_A_BYTES + G::B_BYTES, &tB_lo, fb, kx, brow0);
+                            umma::tma_load_2d_pair(st + TC_A_BYTES, mAl, fb, kx, arow0);
+                            umma::tma_load_2d_pair(st + 2 * TC_A_BYTES + G::B_BYTES, mBl, fb, kx, brow0);
                         }
                     } else {
                         umma::mbar_arrive_expect_tx(&full[s], tx);
-                        umma::tma_load_2d(st, &tA_hi, &full[s], kx, arow0);
-                        umma::tma_load_2d(st + 2 * TC_A_BYTES, &tB_hi, &full[s], kx, brow0);
+                        umma::tma_load_2d(st, mAh, &full[s], kx, arow0);
+                        umma::tma_load_2d(st + 2 * TC_A_BYTES, mBh, &full[s], kx, brow0);
                         if (NPROD == 3) {
-                            umma::tma_load_2d(st + TC_A_BYTES, &tA_lo, &full[s], kx, arow0);
-                            umma::tma_load_2d(st + 2 * TC_A_BYTES + G::B_BYTES, &tB_lo, &full[s], kx, brow0);
+                            umma::tma_load_2d(st + TC_A_BYTES, mAl, &full[s], kx, arow0);
+                            umma::tma_load_2d(st + 2 * TC_A_BYTES + G::B_BYTES, mBl, &full[s], kx, brow0);
                         }
                     }
                     it++;
@@ -290,11 +377,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         if (lane == 0 && leader) {
             // ------------------------------------------------ MMA issuer
             const uint32_t idesc = umma::idesc_f16(G::MT, TC_BN, OP == OP_F16 ? 0 : 2);
-            int it = 0, t = 0;
-            bool ok = true;
-            for (int u = unit0; u < a.units && ok && !*abort_flag; u += ustep, t++) {
+            int it = 0, t = 0, ci = 0;
+            bool ok = true, issued = false;
+            for (int u = unit0; u < units && ok && !*abort_flag; u += ustep, t++) {
                 int m, n, kb0, kb1, split;
-                tc_decode<EPI>(a, u, m, n, kb0, kb1, split);
+                tc_unit<EPI, GROUP>(a, gpre, u, ci, m, n, kb0, kb1, split);
                 const int b = t & 1;
                 if (!umma::mbar_wait(&tempty[b], ((uint32_t)(t >> 1) & 1u) ^ 1u, a.budget)) {
                     tc_fail(a.err, abort_flag, 2u);
@@ -348,6 +435,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                             }
                         }
                     }
+                    issued = true;
                     // stage reusable (in both CTAs of a pair) once these MMAs finish
                     if (PAIR) umma::mma_commit_pair(&empty[s], 0x3);
                     else umma::mma_commit(&empty[s]);
@@ -357,10 +445,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 if (PAIR) umma::mma_commit_pair(&tfull[b], 0x3);
                 else umma::mma_commit(&tfull[b]);
             }
-            // every MMA has completed before TMEM is released
-            if (PAIR) umma::mma_commit_pair(done_bar, 0x1);
-            else umma::mma_commit(done_bar);
-            if (!umma::mbar_wait(done_bar, 0u, TC_WAIT_BUDGET)) tc_fail(a.err, abort_flag, 32u);
+            // every MMA has completed before TMEM is released (a grouped launch can
+            // leave a CTA without units: then nothing was issued)
+            if (issued) {
+                if (PAIR) umma::mma_commit_pair(done_bar, 0x1);
+                else umma::mma_commit(done_bar);
+                if (!umma::mbar_wait(done_bar, 0u, TC_WAIT_BUDGET)) tc_fail(a.err, abort_flag, 32u);
+            }
         }
         __syncwarp();
     } else {
@@ -369,10 +460,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         // the accumulator buffers are released on the leader's barriers
         const uint32_t te0 = PAIR ? umma::mapa_shared(umma::smem_u32(&tempty[0]), 0) : 0u;
         const uint32_t te1 = PAIR ? umma::mapa_shared(umma::smem_u32(&tempty[1]), 0) : 0u;
-        int t = 0;
-        for (int u = unit0; u < a.units; u += ustep, t++) {
+        int t = 0, ci = 0;
+        for (int u = unit0; u < units; u += ustep, t++) {
             int m, n, kb0, kb1, split;
-            tc_decode<EPI>(a, u, m, n, kb0, kb1, split);
+            tc_unit<EPI, GROUP>(a, gpre, u, ci, m, n, kb0, kb1, split);
             const int b = t & 1;
             const int arow = m * G::MT + (int)rank * 128 + q * 32 + lane;  // row of the twiddle-side operand
             const int y0 = n * TC_BN;                                      // first image row of the columns
@@ -380,32 +471,52 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             if (EPI == EPI_FWD) {
                 // Fy[k][y] along this thread's 256 columns: an FP64-accurate anchor every
                 // 16 rows, rotated by r_k = e^{-2 pi i s v_k} within the chunk (<= 15 steps)
+                const float2 *fya = a.fya, *fyr = a.fyr;
+                const float *rsc = a.rsc;
+                float2 *vpart = a.vpart;
+                int nuv = a.nuv, nanc = a.nanc, lpad = a.lpad, elog2 = a.elog2;
+                if (GROUP) {
+                    const TcGroupInst &gi = a.grp[ci];
+                    fya = gi.fya;
+                    fyr = gi.fyr;
+                    rsc = gi.rsc;
+                    vpart = gi.vpart;
+                    nuv = gi.nuv;
+                    nanc = gi.nanc;
+                    lpad = gi.lpad;
+                    elog2 = gi.elog2;
+                }
                 const int k = arow >> 1;
-                const bool vk = k < a.nuv;
-                const float2 rot = vk ? __ldg(&a.fyr[k]) : make_float2(0.f, 0.f);
-                const float2 *anc = a.fya + (size_t)(vk ? k : 0) * a.nanc;
+                const bool vk = k < nuv;
+                const float2 rot = vk ? __ldg(&fyr[k]) : make_float2(0.f, 0.f);
+                const float2 *anc = fya + (size_t)(vk ? k : 0) * nanc;
                 float2 an[TC_BN / 16];
 #pragma unroll
                 for (int c = 0; c < TC_BN / 16; c++) {
-                    const int j = ((y0 + 16 * c) % a.lpad) >> 4;  // anchor of the row within its image
-                    an[c] = (vk && j < a.nanc) ? __ldg(&anc[j]) : make_float2(0.f, 0.f);
+                    const int j = ((y0 + 16 * c) % lpad) >> 4;  // anchor of the row within its image
+                    an[c] = (vk && j < nanc) ? __ldg(&anc[j]) : make_float2(0.f, 0.f);
                 }
                 if (!umma::mbar_wait(&tfull[b], (uint32_t)(t >> 1) & 1u, a.budget)) {
                     tc_fail(a.err, abort_flag, 8u);
                     break;
                 }
                 umma::tc_fence_after();
-                const int emask = (1 << a.elog2) - 1;
+                const int emask = (1 << elog2) - 1;
                 float sre = 0.f, sim = 0.f;
 #pragma unroll
                 for (int c = 0; c < TC_BN / 16; c++) {
                     uint32_t r[16];
                     umma::tmem_ld16(taddr + (uint32_t)(c * 16), r);
+                    // power-of-two scales of the 16 image rows (same address in every lane)
+                    float rs[16];
+                    const float4 *rp = reinterpret_cast<const float4 *>(rsc + y0 + 16 * c);
+#pragma unroll
+                    for (int v4 = 0; v4 < 4; v4++) *reinterpret_cast<float4 *>(&rs[4 * v4]) = __ldg(rp + v4);
                     umma::tmem_ld_wait();
                     float2 w = an[c];
 #pragma unroll
                     for (int j = 0; j < 16; j++) {
-                        const float tv = __uint_as_float(r[j]);
+                        const float tv = __uint_as_float(r[j]) * rs[j];
                         sre = fmaf(tv, w.x, sre);
                         sim = fmaf(tv, w.y, sim);
                         const float wx = w.x * rot.x - w.y * rot.y;
@@ -413,15 +524,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                         w.x = wx;
                     }
                     if (((y0 + 16 * c + 16) & emask) == 0) {
-                        // end of a partial entry (warp-uniform): scale, combine the Re/Im
-                        // row pair, store. even row: (sum T_re F_re, sum T_re F_im);
+                        // end of a partial entry (warp-uniform): combine the Re/Im row
+                        // pair, store. even row: (sum T_re F_re, sum T_re F_im);
                         // odd row: (sum T_im F_re, sum T_im F_im)
-                        const int entry = (y0 + 16 * c) >> a.elog2;
-                        const float fs = a.batch ? a.sc->t_scale[entry / a.epp] : a.sc->fwd_inv_scale;
-                        const float re = sre * fs, im = sim * fs;
+                        const int entry = (y0 + 16 * c) >> elog2;
+                        const float re = sre, im = sim;
                         const float ore = __shfl_xor_sync(0xffffffffu, re, 1);
                         const float oim = __shfl_xor_sync(0xffffffffu, im, 1);
-                        if ((lane & 1) == 0 && vk) a.vpart[(size_t)entry * a.nuv + k] = make_float2(re - oim, im + ore);
+                        if ((lane & 1) == 0 && vk) vpart[(size_t)entry * nuv + k] = make_float2(re - oim, im + ore);
                         sre = 0.f;
                         sim = 0.f;
                     }
@@ -500,11 +610,8 @@ __global__ void k_tc_twiddle_ops(const float2 *__restrict__ fx, int nuv, int N, 
     }
 }
 
-// Image operand: one global power-of-two scale 2^(15 - e), e = exponent of
-// max |image| (reduced by k_prep), then the hi/lo split. One thread per 8
-// consecutive elements of a padded row: 16-byte (f16) or 2 x 16-byte (TF32)
-// stores of hi and of lo. Thread 0 publishes the factor the forward epilogue
-// removes.
+// Eight consecutive values of one operand row: hi (and lo) with 16-byte (f16)
+// or 2 x 16-byte (TF32) stores.
 template <typename OT>
 __device__ __forceinline__ void split_store8(OT *__restrict__ hi, OT *__restrict__ lo, size_t off, const float (&v)[8])
 {
@@ -523,121 +630,201 @@ __device__ __forceinline__ void split_store8(OT *__restrict__ hi, OT *__restrict
     }
 }
 
-template <typename OT>
-__global__ void __launch_bounds__(256) k_tc_split_image(const float *__restrict__ img, int N, int M_pad, int Kx_pad,
-                                                        OT *__restrict__ hi, OT *__restrict__ lo,
-                                                        DevScalars *__restrict__ sc)
+// f16 operands: the same split with paired conversions
+template <>
+__device__ __forceinline__ void split_store8<__half>(__half *__restrict__ hi, __half *__restrict__ lo, size_t off,
+                                                     const float (&v)[8])
 {
-    const double mx = sc->imax;
-    int ex = 0;
-    float scale = 1.f;
-    if (mx > 0.0) {
-        frexp(mx, &ex);  // mx in [2^(ex-1), 2^ex)
-        scale = ldexpf(1.f, 15 - ex);
-    }
-    const int g8 = Kx_pad >> 3;  // groups of 8 per padded row
-    const long long total = (long long)M_pad * g8;
-    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < total;
-         q += (long long)gridDim.x * blockDim.x) {
-        const int y = (int)(q / g8), x = (int)(q - (long long)y * g8) << 3;
-        float v[8];
+    __align__(16) __half2 h[4];
+    __align__(16) __half2 l[4];
 #pragma unroll
-        for (int j = 0; j < 8; j++) v[j] = (y < N && x + j < N) ? img[(size_t)y * N + x + j] * scale : 0.f;
-        split_store8(hi, lo, (size_t)y * Kx_pad + x, v);
+    for (int j = 0; j < 4; j++) {
+        h[j] = __floats2half2_rn(v[2 * j], v[2 * j + 1]);
+        const float2 b = __half22float2(h[j]);
+        l[j] = __floats2half2_rn(v[2 * j] - b.x, v[2 * j + 1] - b.y);
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) sc->fwd_inv_scale = mx > 0.0 ? ldexpf(1.f, ex - 15 - TC_TW_LOG2) : 0.f;
+    *reinterpret_cast<uint4 *>(hi + off) = *reinterpret_cast<const uint4 *>(h);
+    if (lo) *reinterpret_cast<uint4 *>(lo + off) = *reinterpret_cast<const uint4 *>(l);
 }
 
-// Trial image + f16 split in one pass (line-search trials): I_t = max(I + s d,
-// minval), its flux / entropy / max reduced in FP64 like k_prep, and the f16
-// hi/lo image operand written with a power-of-two scale taken from the exact
-// bound max|I_t| <= max|I| + |s| max|d| (both maxima reduced earlier in the
-// iteration), so no separate pass over the trial image is needed.
-template <typename OT>
-__global__ void __launch_bounds__(GP_THREADS) k_tc_prep_split_trial(
-    const float *__restrict__ img, const float *__restrict__ d, float *__restrict__ dst,
-    const float *__restrict__ model, int N, int npix, int Kx_pad, OT *__restrict__ hi, OT *__restrict__ lo,
-    double *__restrict__ partials, DevScalars *__restrict__ sc)
+__device__ __forceinline__ float warp_max_f(float v)
 {
-    __shared__ double smem[2 * 32];
-    const double s = sc->cg.s, minval = sc->cg.minvalue;
-    double bound = sc->imax_curr + fabs(s) * (double)__uint_as_float(sc->dmax_bits);
-    if (bound < minval) bound = minval;
-    int ex = 0;
-    frexp(bound, &ex);
-    const float scale = ldexpf(1.f, 15 - ex);
-    double acc[2] = {0.0, 0.0};
-    double mx = 0.0;
-    const int reg_kind = sc->reg_kind;
-    if ((N & 7) == 0) {
-        // 8 consecutive pixels of one row per thread: 16-byte loads and stores
-        const int n8 = npix >> 3;
-        for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n8; q += gridDim.x * blockDim.x) {
-            const int p0 = q << 3;
-            float iv[8], dv[8], mv[8], out[8], v[8];
-            *reinterpret_cast<float4 *>(&iv[0]) = __ldg(reinterpret_cast<const float4 *>(img + p0));
-            *reinterpret_cast<float4 *>(&iv[4]) = __ldg(reinterpret_cast<const float4 *>(img + p0 + 4));
-            *reinterpret_cast<float4 *>(&dv[0]) = __ldg(reinterpret_cast<const float4 *>(d + p0));
-            *reinterpret_cast<float4 *>(&dv[4]) = __ldg(reinterpret_cast<const float4 *>(d + p0 + 4));
-            *reinterpret_cast<float4 *>(&mv[0]) = __ldg(reinterpret_cast<const float4 *>(model + p0));
-            *reinterpret_cast<float4 *>(&mv[4]) = __ldg(reinterpret_cast<const float4 *>(model + p0 + 4));
 #pragma unroll
-            for (int j = 0; j < 8; j++) {
-                double t = (double)iv[j] + s * (double)dv[j];
-                if (t < minval) t = minval;
-                const float I = (float)t;
-                out[j] = I;
-                const double Id = I;
-                acc[0] += Id;
-                acc[1] += reg_term(Id, (double)mv[j], reg_kind);
-                mx = fmax(mx, fabs(Id));
-                v[j] = I * scale;
+    for (int off = 16; off > 0; off >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, off));
+    return v;
+}
+
+// Row-wise prep of the forward's image operand. A block of PR_THREADS threads
+// works on R = 8 / W image rows at a time, W warps (a power of two) per row:
+//   MODE 0  the image as it is; with `reduce`, its flux, regulariser and max
+//   MODE 1  the line-search trial I = max(I + s d, minval), s = cg.s, written to
+//           dst, with its flux, regulariser and max
+//   MODE 2  trial j = blockIdx.y of a batched search, s = cg.ts[j], written to
+//           dst + j npix and to operand rows j Lpad + y, with its flux and
+//           regulariser; nothing when `gate` is set and *gate is 0
+// Every row gets its own power-of-two scale 2^(15 - e), e the exponent of the
+// row's max |I| (a reduction over the row's warps: no pass over the whole image
+// has to end before the split), and the forward epilogue multiplies
+// accumulator column y by rsc[row] = 2^(e - 15 - TC_TW_LOG2), exactly. With N a
+// multiple of 8 and N <= 256 W every lane holds 8 consecutive pixels of its row
+// in registers between the max and the split (16-byte loads and stores); other
+// shapes take a scalar path that reads the row twice. Per-pixel regulariser
+// terms in FP32 (reg_term_f); flux and regulariser are summed in FP64 in a
+// fixed order (kernel_update_tempimage.cl, kernel_entropy_gs.cl;
+// gpu.c:860-884).
+#define PR_THREADS 256
+#define PR_WARPS_MAX (PR_THREADS / 32)
+
+// warps per image row: a power of two, at most PR_WARPS_MAX
+static inline int pr_warps_per_row(int N)
+{
+    int w = 1;
+    while (w < PR_WARPS_MAX && 256 * w < N) w <<= 1;
+    return w;
+}
+
+template <typename OT, int MODE>
+__global__ void __launch_bounds__(PR_THREADS)
+    k_tc_prep_rows(const float *__restrict__ img, const float *__restrict__ d, float *__restrict__ dst,
+                   const float *__restrict__ model, int N, int W, int Lpad, int Kx_pad, OT *__restrict__ hi,
+                   OT *__restrict__ lo, float *__restrict__ rsc, int reduce, double *__restrict__ partials,
+                   DevScalars *__restrict__ sc, const int *__restrict__ gate)
+{
+    __shared__ double smem[3 * 32];
+    __shared__ float wmax[PR_WARPS_MAX];
+    if (gate && !*gate) return;  // lockstep batches: this instance's line search is over
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int j = MODE == 2 ? (int)blockIdx.y : 0;
+    const double s = MODE == 1 ? sc->cg.s : MODE == 2 ? sc->cg.ts[j] : 0.0;
+    const double minval = MODE ? sc->cg.minvalue : 0.0;
+    const int reg_kind = sc->reg_kind;
+    const bool red = MODE ? true : reduce != 0;
+    if (MODE == 2) dst += (size_t)j * N * N;
+    const size_t row0 = (size_t)j * Lpad;
+    const int R = PR_WARPS_MAX / W;            // rows per block and pass
+    const int sub = warp % W, rw = warp / W;   // this warp's part of its row, row within the pass
+    const int t = sub * 32 + lane, nt = 32 * W;  // thread within the row's group
+    double acc[2] = {0.0, 0.0};
+    float mx = 0.f;
+    const bool vec = (N & 7) == 0 && N <= 8 * nt;
+    for (int ybase = blockIdx.x * R; ybase < N; ybase += gridDim.x * R) {  // block-uniform
+        const int y = ybase + rw;
+        const bool yv = y < N;
+        const size_t rp = (size_t)(yv ? y : 0) * N;
+        float rmax = 0.f;
+        float v[8];
+        const int x = 8 * t;
+        const bool xv = vec && yv && x < N;
+        if (vec) {
+            if (xv) {
+                *reinterpret_cast<float4 *>(&v[0]) = __ldg(reinterpret_cast<const float4 *>(img + rp + x));
+                *reinterpret_cast<float4 *>(&v[4]) = __ldg(reinterpret_cast<const float4 *>(img + rp + x + 4));
+                if (MODE) {
+                    float dv[8];
+                    *reinterpret_cast<float4 *>(&dv[0]) = __ldg(reinterpret_cast<const float4 *>(d + rp + x));
+                    *reinterpret_cast<float4 *>(&dv[4]) = __ldg(reinterpret_cast<const float4 *>(d + rp + x + 4));
+#pragma unroll
+                    for (int k = 0; k < 8; k++) {
+                        double tt = (double)v[k] + s * (double)dv[k];
+                        if (tt < minval) tt = minval;
+                        v[k] = (float)tt;
+                    }
+                    *reinterpret_cast<float4 *>(dst + rp + x) = *reinterpret_cast<const float4 *>(&v[0]);
+                    *reinterpret_cast<float4 *>(dst + rp + x + 4) = *reinterpret_cast<const float4 *>(&v[4]);
+                }
+                if (red) {
+                    float mv[8];
+                    *reinterpret_cast<float4 *>(&mv[0]) = __ldg(reinterpret_cast<const float4 *>(model + rp + x));
+                    *reinterpret_cast<float4 *>(&mv[4]) = __ldg(reinterpret_cast<const float4 *>(model + rp + x + 4));
+#pragma unroll
+                    for (int k = 0; k < 8; k++) acc[0] += (double)v[k];
+                    reg_terms8(v, mv, reg_kind, acc[1]);
+                }
+#pragma unroll
+                for (int k = 0; k < 8; k++) rmax = fmaxf(rmax, fabsf(v[k]));
             }
-            *reinterpret_cast<float4 *>(dst + p0) = *reinterpret_cast<const float4 *>(&out[0]);
-            *reinterpret_cast<float4 *>(dst + p0 + 4) = *reinterpret_cast<const float4 *>(&out[4]);
-            const int y = p0 / N, x = p0 - y * N;
-            split_store8(hi, lo, (size_t)y * Kx_pad + x, v);
+        } else if (yv) {
+            for (int xx = t; xx < N; xx += nt) {
+                float I = __ldg(&img[rp + xx]);
+                if (MODE) {
+                    double tt = (double)I + s * (double)__ldg(&d[rp + xx]);
+                    if (tt < minval) tt = minval;
+                    I = (float)tt;
+                    dst[rp + xx] = I;
+                }
+                if (red) {
+                    acc[0] += (double)I;
+                    acc[1] += (double)reg_term_f(I, __ldg(&model[rp + xx]), reg_kind);
+                }
+                rmax = fmaxf(rmax, fabsf(I));
+            }
         }
-    } else {
-        for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
-            double t = (double)img[p] + s * (double)d[p];
-            if (t < minval) t = minval;
-            const float I = (float)t;
-            dst[p] = I;
-            const double Id = I, m = model[p];
-            acc[0] += Id;
-            acc[1] += reg_term(Id, m, reg_kind);
-            mx = fmax(mx, fabs(Id));
-            const int y = p / N, x = p - y * N;
-            split_store(hi, lo, (size_t)y * Kx_pad + x, I * scale);
+        // max over the row's W warps
+        rmax = warp_max_f(rmax);
+        if (lane == 0) wmax[warp] = rmax;
+        __syncthreads();
+        rmax = 0.f;
+        for (int q = 0; q < W; q++) rmax = fmaxf(rmax, wmax[rw * W + q]);
+        __syncthreads();  // wmax is rewritten by the next pass
+        int ex = 0;
+        frexpf(rmax, &ex);
+        const float scale = ldexpf(1.f, 15 - ex);
+        if (xv) {
+#pragma unroll
+            for (int k = 0; k < 8; k++) v[k] *= scale;
+            split_store8(hi, lo, (row0 + y) * Kx_pad + x, v);
+        } else if (!vec && yv) {
+            // second pass: each thread reads back the values it wrote (or the image)
+            for (int xx = t; xx < N; xx += nt) {
+                const float I = MODE ? dst[rp + xx] : __ldg(&img[rp + xx]);
+                split_store(hi, lo, (row0 + y) * Kx_pad + xx, I * scale);
+            }
         }
+        if (yv && t == 0) rsc[row0 + y] = ldexpf(1.f, ex - 15 - TC_TW_LOG2);
+        mx = fmaxf(mx, rmax);
     }
+    if (!red) return;  // uniform over the grid
     block_sum<2>(acc, smem);
-    mx = block_max(mx, smem);
+    const double bmax = block_max((double)mx, smem);
+    if (MODE == 2) {
+        double *pp = partials + (size_t)j * gridDim.x * 2;
+        if (threadIdx.x == 0) {
+            pp[2 * blockIdx.x] = acc[0];
+            pp[2 * blockIdx.x + 1] = acc[1];
+        }
+        if (last_block(&sc->t_counter[j])) {
+            double o[2];
+            finish_sum<2>(pp, gridDim.x, o, smem);
+            if (threadIdx.x == 0) {
+                sc->t_flux[j] = o[0];
+                sc->t_invflux[j] = 1.0 / o[0];
+                sc->t_entropy[j] = o[1];
+                sc->t_counter[j] = 0;
+            }
+        }
+        return;
+    }
     if (threadIdx.x == 0) {
         partials[3 * blockIdx.x] = acc[0];
         partials[3 * blockIdx.x + 1] = acc[1];
-        partials[3 * blockIdx.x + 2] = mx;
+        partials[3 * blockIdx.x + 2] = bmax;
     }
     if (last_block(&sc->counter[RED_PREP])) {
-        double v[2] = {0.0, 0.0}, m = 0.0;
-        for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
-            v[0] += __ldcg(&partials[3 * b]);
-            v[1] += __ldcg(&partials[3 * b + 1]);
-            m = fmax(m, __ldcg(&partials[3 * b + 2]));
-        }
-        block_sum<2>(v, smem);
+        double v3[3];
+        finish_sum<3>(partials, gridDim.x, v3, smem);
+        // max over the blocks' maxima (any order gives the same value)
+        double m = 0.0;
+        for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) m = fmax(m, __ldcg(&partials[3 * b + 2]));
         m = block_max(m, smem);
         if (threadIdx.x == 0) {
-            sc->flux = v[0];
-            sc->invflux = 1.0 / v[0];
-            sc->entropy = v[1];
+            sc->flux = v3[0];
+            sc->invflux = 1.0 / v3[0];
+            sc->entropy = v3[1];
             sc->imax = m;
-            sc->flux_f = (float)v[0];
-            sc->invflux_f = (float)(1.0 / v[0]);
-            sc->entropy_f = (float)v[1];
-            sc->fwd_inv_scale = ldexpf(1.f, ex - 15 - TC_TW_LOG2);
-            if (!isfinite(v[0]) || !isfinite(v[1])) sc->nonfinite |= 1u;
+            sc->flux_f = (float)v3[0];
+            sc->invflux_f = (float)(1.0 / v3[0]);
+            sc->entropy_f = (float)v3[1];
+            if (!isfinite(v3[0]) || !isfinite(v3[1])) sc->nonfinite |= 1u;
             sc->counter[RED_PREP] = 0;
         }
     }
@@ -909,12 +1096,15 @@ void gp_tc_free(gpair_ctx *c)
 {
     TcState *t = (TcState *)c->tc_state;
     if (!t) return;
+    c->buf_gen++;
     void *bufs[] = {t->img_hi, t->img_lo, t->fx_hi, t->fx_lo, t->fxt_hi, t->fxt_lo, t->w_hi, t->w_lo,
                     t->imgb_hi, t->imgb_lo};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (t->fya) cudaFree(t->fya);
     if (t->fyr) cudaFree(t->fyr);
+    if (t->rsc) cudaFree(t->rsc);
+    if (t->rscb) cudaFree(t->rscb);
     free(t);
     c->tc_state = nullptr;
 }
@@ -927,15 +1117,16 @@ static void launch_twiddle_ops(gpair_ctx *c, TcState *t, long long n_all)
         (OT *)t->fxt_hi, (OT *)t->fxt_lo);
 }
 
-template <int EPI, int PAIR>
+template <int EPI, int PAIR, int GROUP>
 static int tc_set_smem(gpair_ctx *c)
 {
-    GP_CUDA(c, cudaFuncSetAttribute(k_tc_gemm<EPI, OP_F16, 3, PAIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    TC_SMEM_BYTES));
-    GP_CUDA(c, cudaFuncSetAttribute(k_tc_gemm<EPI, OP_TF32, 3, PAIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    TC_SMEM_BYTES));
-    GP_CUDA(c, cudaFuncSetAttribute(k_tc_gemm<EPI, OP_TF32, 1, PAIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    TC_SMEM_BYTES));
+    const int bytes = GROUP ? TC_SMEM_GROUP_BYTES : TC_SMEM_BYTES;
+    GP_CUDA(c, cudaFuncSetAttribute(k_tc_gemm<EPI, OP_F16, 3, PAIR, GROUP>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    GP_CUDA(c, cudaFuncSetAttribute(k_tc_gemm<EPI, OP_TF32, 3, PAIR, GROUP>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    GP_CUDA(c, cudaFuncSetAttribute(k_tc_gemm<EPI, OP_TF32, 1, PAIR, GROUP>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     return GPAIR_OK;
 }
 
@@ -982,6 +1173,8 @@ int gp_tc_prepare(gpair_ctx *c)
         GP_CUDA(c, cudaMalloc(x.p, x.n * t->esz));
         GP_CUDA(c, cudaMemsetAsync(*x.p, 0, x.n * t->esz, c->stream));
     }
+    GP_CUDA(c, cudaMalloc(&t->rsc, sizeof(float) * (size_t)t->M_pad));
+    GP_CUDA(c, cudaMemsetAsync(t->rsc, 0, sizeof(float) * (size_t)t->M_pad, c->stream));
     t->nanc = (N + 15) / 16;
     GP_CUDA(c, cudaMalloc(&t->fya, sizeof(float2) * (size_t)nuv * t->nanc));
     GP_CUDA(c, cudaMalloc(&t->fyr, sizeof(float2) * (size_t)nuv));
@@ -1012,10 +1205,12 @@ int gp_tc_prepare(gpair_ctx *c)
         t->m_w_lo = t->m_w_hi;
         t->m_fxt_lo = t->m_fxt_hi;
     }
-    if ((rc = tc_set_smem<EPI_FWD, 0>(c))) return rc;
-    if ((rc = tc_set_smem<EPI_STORE, 0>(c))) return rc;
-    if ((rc = tc_set_smem<EPI_FWD, 1>(c))) return rc;
-    if ((rc = tc_set_smem<EPI_STORE, 1>(c))) return rc;
+    if ((rc = tc_set_smem<EPI_FWD, 0, 0>(c))) return rc;
+    if ((rc = tc_set_smem<EPI_STORE, 0, 0>(c))) return rc;
+    if ((rc = tc_set_smem<EPI_FWD, 1, 0>(c))) return rc;
+    if ((rc = tc_set_smem<EPI_STORE, 1, 0>(c))) return rc;
+    if ((rc = tc_set_smem<EPI_FWD, 0, 1>(c))) return rc;
+    if ((rc = tc_set_smem<EPI_FWD, 1, 1>(c))) return rc;
     t->npairs = t->nsm / 2;
     if (pair) {
         // clusters of two that can be resident at once (an SM left over in a GPC cannot host a pair)
@@ -1032,7 +1227,7 @@ int gp_tc_prepare(gpair_ctx *c)
         cfg.attrs = at;
         cfg.numAttrs = 1;
         int nclusters = 0;
-        if (cudaOccupancyMaxActiveClusters(&nclusters, (const void *)k_tc_gemm<EPI_FWD, OP_F16, 3, 1>, &cfg) ==
+        if (cudaOccupancyMaxActiveClusters(&nclusters, (const void *)k_tc_gemm<EPI_FWD, OP_F16, 3, 1, 0>, &cfg) ==
                 cudaSuccess &&
             nclusters > 0 && nclusters < t->npairs)
             t->npairs = nclusters;
@@ -1107,9 +1302,10 @@ static cudaError_t tc_launch_kind(TcState *t, dim3 grid, cudaStream_t st, const 
     cfg.stream = st;
     cfg.attrs = at;
     cfg.numAttrs = PAIR ? 1 : 0;
-    if (t->op == OP_F16) return cudaLaunchKernelEx(&cfg, k_tc_gemm<EPI, OP_F16, 3, PAIR>, A_hi, A_lo, B_hi, B_lo, a);
-    if (t->nprod == 3) return cudaLaunchKernelEx(&cfg, k_tc_gemm<EPI, OP_TF32, 3, PAIR>, A_hi, A_lo, B_hi, B_lo, a);
-    return cudaLaunchKernelEx(&cfg, k_tc_gemm<EPI, OP_TF32, 1, PAIR>, A_hi, A_lo, B_hi, B_lo, a);
+    if (t->op == OP_F16) return cudaLaunchKernelEx(&cfg, k_tc_gemm<EPI, OP_F16, 3, PAIR, 0>, A_hi, A_lo, B_hi, B_lo, a);
+    if (t->nprod == 3)
+        return cudaLaunchKernelEx(&cfg, k_tc_gemm<EPI, OP_TF32, 3, PAIR, 0>, A_hi, A_lo, B_hi, B_lo, a);
+    return cudaLaunchKernelEx(&cfg, k_tc_gemm<EPI, OP_TF32, 1, PAIR, 0>, A_hi, A_lo, B_hi, B_lo, a);
 }
 
 // one launch of the contraction in the context's operand kind / product count:
@@ -1137,6 +1333,43 @@ static int tc_launch(gpair_ctx *c, TcState *t, const CUtensorMap &A_hi, const CU
     return GPAIR_OK;
 }
 
+// Row-wise prep launches (k_tc_prep_rows): PR_THREADS threads per block, R rows
+// per block and pass; at most GP_MAX_PARTIALS blocks (three partials each fit
+// the RED_PREP slot), a batch at most 1024 per trial (two partials each).
+template <typename OT, int MODE>
+static void tc_prep_rows_kernel(gpair_ctx *c, TcState *t, dim3 g, int W, const float *img, float *dst, int reduce,
+                                double *partials)
+{
+    const bool b = MODE == 2;
+    k_tc_prep_rows<OT, MODE><<<g, PR_THREADS, 0, c->stream>>>(
+        img, c->descent_dir, dst, c->model, c->N, W, b ? t->Lb : 0, t->Kx_pad, (OT *)(b ? t->imgb_hi : t->img_hi),
+        (OT *)(b ? t->imgb_lo : t->img_lo), b ? t->rscb : t->rsc, reduce, partials, c->sc, b ? c->gate : nullptr);
+}
+
+static int tc_prep_rows_launch(gpair_ctx *c, TcState *t, int mode, int reduce, double *partials,
+                               const float *img = nullptr)
+{
+    const int W = pr_warps_per_row(c->N), R = PR_WARPS_MAX / W;
+    int gx = gp_cdiv(c->N, R);
+    const int cap = mode == 2 ? 1024 : GP_MAX_PARTIALS;
+    if (gx > cap) gx = cap;
+    if (gx < 1) gx = 1;
+    const dim3 g(gx, mode == 2 ? GP_NTR : 1, 1);
+    const bool f16 = t->op == OP_F16;
+    if (mode == 0) {
+        if (f16) tc_prep_rows_kernel<__half, 0>(c, t, g, W, img, nullptr, reduce, partials);
+        else tc_prep_rows_kernel<float, 0>(c, t, g, W, img, nullptr, reduce, partials);
+    } else if (mode == 1) {
+        if (f16) tc_prep_rows_kernel<__half, 1>(c, t, g, W, c->image, c->image_temp, 1, partials);
+        else tc_prep_rows_kernel<float, 1>(c, t, g, W, c->image, c->image_temp, 1, partials);
+    } else {
+        if (f16) tc_prep_rows_kernel<__half, 2>(c, t, g, W, c->image, c->image_trials, 1, partials);
+        else tc_prep_rows_kernel<float, 2>(c, t, g, W, c->image, c->image_trials, 1, partials);
+    }
+    GP_LAUNCH_CHECK(c);
+    return GPAIR_OK;
+}
+
 // forward contraction on the already split image operand
 int gp_tc_forward_gemm(gpair_ctx *c)
 {
@@ -1157,9 +1390,7 @@ int gp_tc_forward_gemm(gpair_ctx *c)
     a.nuv = c->nuv;
     a.lpad = t->M_pad;  // one image, partial entries of one 256-row tile each
     a.elog2 = 8;
-    a.epp = a.n_tiles;
-    a.batch = 0;
-    a.sc = c->sc;
+    a.rsc = t->rsc;
     a.vpart = c->vpart;
     if ((rc = tc_launch<EPI_FWD>(c, t, t->m_fx_hi, t->m_fx_lo, t->m_img_hi, t->m_img_lo, a))) return rc;
     c->mt = a.n_tiles;
@@ -1180,6 +1411,8 @@ int gp_tc_batch_prepare(gpair_ctx *c, int *epp)
         const int erows = t->Lb < TC_BN ? t->Lb : TC_BN;
         t->epp_b = t->Lb / erows;
         const size_t rows = (size_t)GP_NTR * t->Lb, n = rows * t->Kx_pad;
+        GP_CUDA(c, cudaMalloc(&t->rscb, sizeof(float) * rows));
+        GP_CUDA(c, cudaMemsetAsync(t->rscb, 0, sizeof(float) * rows, c->stream));
         GP_CUDA(c, cudaMalloc(&t->imgb_hi, n * t->esz));
         GP_CUDA(c, cudaMemsetAsync(t->imgb_hi, 0, n * t->esz, c->stream));
         const int bbox = t->pair ? 128 : TC_BN;
@@ -1201,12 +1434,11 @@ int gp_tc_batch_prepare(gpair_ctx *c, int *epp)
 // trial images + their operands for a batch (steps from the device state)
 int gp_tc_trials_prep_split(gpair_ctx *c, double *partials)
 {
-    (void)partials;
     int rc;
     TcState *t = tc_state_ready(c, &rc);
     if (rc) return rc;
     if ((rc = gp_tc_batch_prepare(c, nullptr))) return rc;
-    return gp_trials_prep_launch(c, t->imgb_hi, t->imgb_lo, t->Lb, t->Kx_pad, TC_TW_LOG2, t->op == OP_TF32);
+    return tc_prep_rows_launch(c, t, 2, 1, partials);
 }
 
 // forward contraction of the GP_NTR trial images in one launch: every twiddle
@@ -1232,31 +1464,19 @@ int gp_tc_forward_batch_gemm(gpair_ctx *c)
     a.lpad = t->Lb;
     const int erows = t->Lb < TC_BN ? t->Lb : TC_BN;
     a.elog2 = erows == 32 ? 5 : erows == 64 ? 6 : erows == 128 ? 7 : 8;
-    a.epp = t->epp_b;
-    a.batch = 1;
-    a.sc = c->sc;
+    a.rsc = t->rscb;
     a.vpart = c->vpart_b;
     return tc_launch<EPI_FWD>(c, t, t->m_fx_hi, t->m_fx_lo, t->m_imgb_hi, t->m_imgb_lo, a);
 }
 
-// split of an image into the forward's image operand
+// split of an image into the forward's image operand (its flux and regulariser
+// already reduced)
 int gp_tc_split(gpair_ctx *c, int which)
 {
     int rc;
     TcState *t = tc_state_ready(c, &rc);
     if (rc) return rc;
-    const float *img = (which == GPAIR_IMG_TEMP) ? c->image_temp : c->image;
-    long long groups = (long long)t->M_pad * (t->Kx_pad >> 3);
-    int grid = gp_cdiv(groups, 256);
-    if (grid > 8 * t->nsm) grid = 8 * t->nsm;
-    if (t->op == OP_F16)
-        k_tc_split_image<__half><<<grid, 256, 0, c->stream>>>(img, c->N, t->M_pad, t->Kx_pad, (__half *)t->img_hi,
-                                                               (__half *)t->img_lo, c->sc);
-    else
-        k_tc_split_image<float><<<grid, 256, 0, c->stream>>>(img, c->N, t->M_pad, t->Kx_pad, (float *)t->img_hi,
-                                                              (float *)t->img_lo, c->sc);
-    GP_LAUNCH_CHECK(c);
-    return GPAIR_OK;
+    return tc_prep_rows_launch(c, t, 0, 0, nullptr, which == GPAIR_IMG_TEMP ? c->image_temp : c->image);
 }
 
 int gp_tc_forward(gpair_ctx *c, int which)
@@ -1266,27 +1486,22 @@ int gp_tc_forward(gpair_ctx *c, int which)
     return gp_tc_forward_gemm(c);
 }
 
-// trial image + split in one kernel (reads s, minval, max|I|, max|d| from the device state)
+// flux, regulariser and max of an image, and its forward operand, in one pass
+int gp_tc_prep_image(gpair_ctx *c, int which)
+{
+    int rc;
+    TcState *t = tc_state_ready(c, &rc);
+    if (rc) return rc;
+    return tc_prep_rows_launch(c, t, 0, 1, c->partials, which == GPAIR_IMG_TEMP ? c->image_temp : c->image);
+}
+
+// trial image + split in one kernel (reads s and minval from the device state)
 int gp_tc_prep_split_trial(gpair_ctx *c)
 {
     int rc;
     TcState *t = tc_state_ready(c, &rc);
     if (rc) return rc;
-    // at most GP_MAX_PARTIALS blocks: 3 partials each fit the RED_PREP slot
-    const int per_thread = (c->N & 7) == 0 ? 8 : 1;
-    int g = gp_cdiv(c->npix / per_thread, GP_THREADS);
-    if (g > GP_MAX_PARTIALS) g = GP_MAX_PARTIALS;
-    if (g < 1) g = 1;
-    if (t->op == OP_F16)
-        k_tc_prep_split_trial<__half><<<g, GP_THREADS, 0, c->stream>>>(
-            c->image, c->descent_dir, c->image_temp, c->model, c->N, c->npix, t->Kx_pad, (__half *)t->img_hi,
-            (__half *)t->img_lo, c->partials, c->sc);
-    else
-        k_tc_prep_split_trial<float><<<g, GP_THREADS, 0, c->stream>>>(
-            c->image, c->descent_dir, c->image_temp, c->model, c->N, c->npix, t->Kx_pad, (float *)t->img_hi,
-            (float *)t->img_lo, c->partials, c->sc);
-    GP_LAUNCH_CHECK(c);
-    return GPAIR_OK;
+    return tc_prep_rows_launch(c, t, 1, 1, c->partials);
 }
 
 template <typename OT>
@@ -1344,4 +1559,156 @@ int gp_tc_adjoint(gpair_ctx *c, int which)
     int rc = gp_tc_build_w(c);
     if (rc) return rc;
     return gp_tc_adjoint_gemm(c);
+}
+
+// ------------------------------------------------------ grouped forward
+//
+// One tcgen05 launch over the batched-trial forwards of several instances
+// (many independent reconstructions advancing in lockstep): the units of every
+// gated instance, each with its own maps and epilogue arguments from a
+// TcGroupInst array in global memory, share the persistent CTAs (or CTA pairs).
+// All instances use the same operand kind, product count and tile layout.
+struct TcGroup {
+    int n, op, nprod, pair, npairs, nsm;
+    TcGroupInst *d_inst;  // [n], device
+    CUtensorMap map0;     // a valid map for the kernel's unused map parameters
+    const int *gate;      // [n], device, owned by the caller
+    unsigned int *err;    // bounded-wait failures of the grouped launches (device word of the caller)
+};
+
+void gp_tc_group_free(void *grp)
+{
+    TcGroup *G = (TcGroup *)grp;
+    if (!G) return;
+    if (G->d_inst) cudaFree(G->d_inst);
+    free(G);
+}
+
+// the operand kind, product count and tile layout of a context's tensor path
+// (instances with equal keys can share a grouped launch), or -1 on the CUDA cores
+int gp_tc_group_key(gpair_ctx *c)
+{
+    if (c->precision == GPAIR_PREC_FP32) return -1;
+    int op, nprod;
+    tc_mode(c->precision, &op, &nprod);
+    return (op * 4 + nprod) * 2 + (c->tc_pair ? 1 : 0);
+}
+
+// Builds the group of ctx[0..n-1] (their tensor state and batch buffers are
+// allocated here if needed). GPAIR_ERR_STATE when the instances cannot share
+// one launch (a CUDA-core instance, or another operand kind or tile layout).
+int gp_tc_group_build(gpair_ctx **ctx, int n, const int *gate, unsigned int *err, void **out)
+{
+    *out = nullptr;
+    if (n <= 0 || n > TC_GROUP_MAX) return GPAIR_ERR_STATE;
+    TcGroupInst *h = (TcGroupInst *)calloc((size_t)n, sizeof(TcGroupInst));
+    if (!h) return GPAIR_ERR_ALLOC;
+    int rc = GPAIR_OK;
+    TcState *t0 = nullptr;
+    for (int i = 0; i < n && !rc; i++) {
+        gpair_ctx *c = ctx[i];
+        if (c->precision == GPAIR_PREC_FP32) {
+            rc = GPAIR_ERR_STATE;
+            break;
+        }
+        TcState *t = tc_state_ready(c, &rc);
+        if (rc) break;
+        if ((rc = gp_batch_alloc(c))) break;
+        if (t0 && (t->op != t0->op || t->nprod != t0->nprod || t->pair != t0->pair)) {
+            rc = GPAIR_ERR_STATE;
+            break;
+        }
+        if (!t0) t0 = t;
+        TcGroupInst &g = h[i];
+        g.A_hi = t->m_fx_hi;
+        g.A_lo = t->m_fx_lo;
+        g.B_hi = t->m_imgb_hi;
+        g.B_lo = t->m_imgb_lo;
+        g.m_tiles = t->rows_pad / (t->pair ? 256 : TC_BM);
+        g.n_tiles = (GP_NTR * t->Lb) / TC_BN;
+        g.kb_total = t->Kx_pad / t->bk;
+        g.units = g.m_tiles * g.n_tiles;
+        g.fya = t->fya;
+        g.fyr = t->fyr;
+        g.nanc = t->nanc;
+        g.nuv = c->nuv;
+        g.lpad = t->Lb;
+        const int erows = t->Lb < TC_BN ? t->Lb : TC_BN;
+        g.elog2 = erows == 32 ? 5 : erows == 64 ? 6 : erows == 128 ? 7 : 8;
+        g.rsc = t->rscb;
+        g.vpart = c->vpart_b;
+    }
+    TcGroup *G = nullptr;
+    if (!rc) {
+        G = (TcGroup *)calloc(1, sizeof(TcGroup));
+        if (!G) rc = GPAIR_ERR_ALLOC;
+    }
+    if (!rc) {
+        G->n = n;
+        G->op = t0->op;
+        G->nprod = t0->nprod;
+        G->pair = t0->pair;
+        G->npairs = t0->npairs;
+        G->nsm = t0->nsm;
+        G->map0 = h[0].A_hi;
+        G->gate = gate;
+        G->err = err;
+        gpair_ctx *c = ctx[0];
+        if (cudaMalloc(&G->d_inst, sizeof(TcGroupInst) * (size_t)n) != cudaSuccess ||
+            cudaMemcpy(G->d_inst, h, sizeof(TcGroupInst) * (size_t)n, cudaMemcpyHostToDevice) != cudaSuccess) {
+            snprintf(c->last_error, sizeof(c->last_error), "grouped forward: device arrays");
+            rc = GPAIR_ERR_CUDA;
+        }
+    }
+    free(h);
+    if (rc) {
+        gp_tc_group_free(G);
+        return rc;
+    }
+    *out = G;
+    return GPAIR_OK;
+}
+
+template <int PAIR>
+static cudaError_t tc_group_launch_kind(TcGroup *G, cudaStream_t st, const TcArgs &a)
+{
+    cudaLaunchConfig_t cfg;
+    memset(&cfg, 0, sizeof(cfg));
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = PAIR ? 2 : 1;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(PAIR ? 2 * (unsigned)G->npairs : (unsigned)G->nsm, 1, 1);
+    cfg.blockDim = dim3(TC_THREADS, 1, 1);
+    cfg.dynamicSmemBytes = TC_SMEM_GROUP_BYTES;
+    cfg.stream = st;
+    cfg.attrs = at;
+    cfg.numAttrs = PAIR ? 1 : 0;
+    const CUtensorMap &m = G->map0;
+    if (G->op == OP_F16) return cudaLaunchKernelEx(&cfg, k_tc_gemm<EPI_FWD, OP_F16, 3, PAIR, 1>, m, m, m, m, a);
+    if (G->nprod == 3) return cudaLaunchKernelEx(&cfg, k_tc_gemm<EPI_FWD, OP_TF32, 3, PAIR, 1>, m, m, m, m, a);
+    return cudaLaunchKernelEx(&cfg, k_tc_gemm<EPI_FWD, OP_TF32, 1, PAIR, 1>, m, m, m, m, a);
+}
+
+// the grouped forward of every gated instance, on c's stream (persistent: one
+// CTA per SM or one pair per two SMs, whatever the number of gated units)
+int gp_tc_group_forward(void *grp, gpair_ctx *c)
+{
+    TcGroup *G = (TcGroup *)grp;
+    TcArgs a;
+    memset(&a, 0, sizeof(a));
+    a.grp = G->d_inst;
+    a.gate = G->gate;
+    a.ninst = G->n;
+    a.err = G->err;
+    a.budget = c->tc_wait_budget > 0 ? c->tc_wait_budget : TC_WAIT_BUDGET;
+    a.skip_loads = c->tc_skip_loads;
+    cudaError_t e = G->pair ? tc_group_launch_kind<1>(G, c->stream, a) : tc_group_launch_kind<0>(G, c->stream, a);
+    if (e != cudaSuccess) {
+        snprintf(c->last_error, sizeof(c->last_error), "grouped contraction launch: %s", cudaGetErrorString(e));
+        return GPAIR_ERR_CUDA;
+    }
+    c->launches++;
+    return GPAIR_OK;
 }

@@ -358,9 +358,24 @@ int gpair_cg_checkpoint_load(gpair_ctx *ctx, const void *buffer, size_t bytes);
  * autotuned configuration; those are fixed into the graph: rebuild the batch after
  * changing any of them. gpair_batch_run takes the same parameters as gpair_cg_run
  * (line_search must match the batch's, host_loop must be 0; no traces) and returns
- * per-context results; each context's last_run_stats holds the batch's device time. */
+ * per-context results; each context's last_run_stats holds the batch's device time.
+ *
+ * Lockstep batches (the default of gpair_batch_create when line_search is
+ * GPAIR_LS_BATCH, every context is on a tensor-core path with the same operand kind
+ * and tile layout, and n <= 256): the reconstructions advance one CG step at a
+ * time together, and each batched line-search evaluation runs the forward DFTs of
+ * the trial images of every instance still searching as ONE grouped tcgen05 launch
+ * (per-instance operand maps and epilogue arguments in device memory). Each
+ * instance's results are bitwise those of its separate run. Otherwise, or with
+ * GPAIR_BATCH_INDEPENDENT, every context's loop is an independent graph branch.
+ * gpair_batch_grouped tells which one was built. gpair_batch_run returns
+ * GPAIR_ERR_STATE when a context's operand or batch buffers were rebuilt since the
+ * batch was created (another precision, tile layout, problem or image size). */
 typedef struct gpair_batch gpair_batch;
+#define GPAIR_BATCH_INDEPENDENT 1
 int gpair_batch_create(gpair_batch **batch, gpair_ctx **ctx, int n, int line_search);
+int gpair_batch_create_ex(gpair_batch **batch, gpair_ctx **ctx, int n, int line_search, int flags);
+int gpair_batch_grouped(const gpair_batch *batch);
 int gpair_batch_run(gpair_batch *batch, const gpair_cg_params *p, gpair_cg_result *results);
 int gpair_batch_destroy(gpair_batch *batch);
 
@@ -428,24 +443,29 @@ int gpair_time_batch_stages(gpair_ctx *ctx, int reps, double *stage_ms, int max_
 /* Autotuner: times criterion + gradient evaluations of the loaded problem (current
  * image) under candidate configurations and keeps the fastest. Candidates: the
  * precision path (GPAIR_TUNE_PRECISION: FP32 CUDA cores vs split-f16 tensor cores;
- * both meet the 1e-5 accuracy bounds) and the adjoint's split-K tile length
+ * both meet the 1e-5 accuracy bounds), the adjoint's split-K tile length
  * (GPAIR_TUNE_SPLITS: half, default and double the heuristic's K-blocks per split,
- * within the FP32-accumulation cap). GPAIR_TUNE_CACHE reuses the choice made for a
+ * within the FP32-accumulation cap) and the tensor-core tile (GPAIR_TUNE_TILE:
+ * 256 x 256 output tiles on CTA pairs or 128 x 256 on single CTAs, as
+ * gpair_set_tc_pair selects). GPAIR_TUNE_CACHE reuses the choice made for a
  * problem of the same device, width and uv count (to 1/8) and objective in this process. */
 #define GPAIR_TUNE_PRECISION 1
 #define GPAIR_TUNE_SPLITS 2
 #define GPAIR_TUNE_CACHE 4
 #define GPAIR_TUNE_BATCHED 8 /* objective: criterion + gradient + 2 batched 8-trial evaluations
                                 (one batched-line-search iteration) instead of criterion + gradient */
-#define GPAIR_TUNE_MAX_CANDIDATES 8
+#define GPAIR_TUNE_TILE 16
+#define GPAIR_TUNE_MAX_CANDIDATES 12
 typedef struct {
     int precision;       /* chosen precision mode */
     int adjoint_splits;  /* chosen split-K count of the adjoint contraction */
     double ms_per_eval;  /* criterion + gradient, chosen configuration */
     int from_cache;
     int n_candidates;
+    int tile_m;          /* chosen tensor-core tile rows: 256 (CTA pairs), 128, or 0 (CUDA cores) */
     int cand_precision[GPAIR_TUNE_MAX_CANDIDATES];
     int cand_splits[GPAIR_TUNE_MAX_CANDIDATES];
+    int cand_tile_m[GPAIR_TUNE_MAX_CANDIDATES];
     double cand_ms[GPAIR_TUNE_MAX_CANDIDATES];
 } gpair_tune_result;
 int gpair_autotune(gpair_ctx *ctx, int flags, int reps, gpair_tune_result *result);

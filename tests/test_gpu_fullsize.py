@@ -8,7 +8,7 @@ consistency relations.
   gradient       device data gradient on 24 random pixels against the reference's
                  direct per-pixel sum in FP64, evaluated with the device's
                  visibilities: relative L2 error <= 1e-5
-  entropy        FP64 sums, 1e-12 relative
+  entropy        FP64 sums of FP32 per-pixel terms (tensor paths): 1e-6 relative
 """
 import numpy as np
 import pytest
@@ -58,7 +58,7 @@ def _check(p, prec, seed=5, pair=True):
     mock64, chi2_host = _host_mock_chi2(p, V)
     assert abs(chi2 - chi2_host) <= 1e-6 * chi2_host
     assert np.allclose(mock, mock64, rtol=2e-6, atol=1e-6)
-    assert abs(S - _entropy64(img, p.model)) <= 1e-12 * max(1.0, abs(S))
+    assert abs(S - _entropy64(img, p.model)) <= (1e-12 if prec == g.PREC_FP32 else 1e-6) * max(1.0, abs(S))
     px = rng.integers(0, p.width, 24)
     py = rng.integers(0, p.width, 24)
     g64 = O.data_gradient_pixels64(p, img, V, mock64, px, py)

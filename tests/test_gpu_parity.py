@@ -4,7 +4,10 @@ Tolerances (against FP64, as the design states them):
   visibilities        |V - V64| <= 1e-5 (V is normalised by the total flux)
   chi2                <= 1e-5 relative
   data gradient       <= 1e-5 relative (L2 over the image)
-  entropy, gradient   <= 1e-10 relative (FP64 sums, FP64 log per pixel)
+  entropy             <= 1e-10 relative on the CUDA-core path (FP64 term per pixel);
+                      <= 1e-6 on the tensor paths (FP32 term per pixel without
+                      cancellation, reg_term_f; FP64 sums)
+  entropy gradient    rtol 1e-6
   CG trace            J <= 1e-5 relative per iteration, identical evaluation counts
 """
 import ctypes as C
@@ -19,6 +22,11 @@ from oracle import oracle as O
 pytestmark = pytest.mark.gpu
 
 PRECISIONS = [g.PREC_FP32, g.PREC_SPLIT16, g.PREC_TF32X3]
+
+
+def _s_tol(prec):
+    """Relative tolerance of the regulariser sum against FP64 (see the module docstring)."""
+    return 1e-10 if prec == g.PREC_FP32 else 1e-6
 
 
 def _problem(name, seeds=(1, 2, 3)):
@@ -53,7 +61,7 @@ def test_criterion_and_gradient_match_fp64(rec, name, prec):
     chi2, S = rec.criterion()
     e = O.evaluate64(p, img)
     assert abs(chi2 - e["chi2"]) / e["chi2"] <= 1e-5
-    assert abs(S - e["entropy"]) <= 1e-10 * max(1.0, abs(e["entropy"]))
+    assert abs(S - e["entropy"]) <= _s_tol(prec) * max(1.0, abs(e["entropy"]))
     assert np.abs(rec.visibilities() - e["visi"]).max() <= 1e-5
     m = rec.mock()
     assert np.allclose(m, e["mock"], rtol=1e-4, atol=2e-6)
@@ -63,6 +71,32 @@ def test_criterion_and_gradient_match_fp64(rec, name, prec):
     assert np.allclose(rec.entropy_gradient(), eg, rtol=1e-6, atol=1e-7)
     full = e["data_grad"] - np.float32(p.alpha) * eg
     assert _rel(rec.full_gradient(), full) <= 1e-5
+
+
+@pytest.mark.parametrize("prec", [g.PREC_SPLIT16, g.PREC_TF32X3])
+@pytest.mark.parametrize("regime", ["near", "far", "mixed"])
+def test_regulariser_sum_near_and_far_from_the_prior(rec, prec, regime):
+    """The tensor paths' one-pass image prep sums FP32 per-pixel Gull-Skilling
+    terms in FP64. Near the prior (I/m - 1 ~ 1e-4, where I - m - I ln(I/m) cancels
+    to -m r^2/2) the series branch keeps the relative accuracy; far from it
+    (I/m from 1e-6 to 1e3) the closed form does. Against the FP64 oracle: 1e-6."""
+    p = _problem("small")
+    rec.set_problem(p)
+    rec.set_precision(prec)
+    rng = np.random.default_rng(17)
+    m = p.model.astype(np.float64)
+    if regime == "near":
+        img = m * (1 + 1e-4 * rng.standard_normal(p.npix))
+    elif regime == "far":
+        img = m * 10.0 ** rng.uniform(-6, 3, p.npix)
+    else:
+        img = m * np.where(rng.random(p.npix) < 0.5, 1 + 0.49 * rng.uniform(-1, 1, p.npix),
+                           10.0 ** rng.uniform(-3, 2, p.npix))
+    img = img.astype(np.float32)
+    rec.set_image(img)
+    chi2, S = rec.criterion()
+    S64 = O.evaluate64(p, img)["entropy"]
+    assert abs(S - S64) <= 1e-6 * abs(S64), (S, S64)
 
 
 @pytest.mark.parametrize("name", ["tiny", "small"])
@@ -611,7 +645,7 @@ def test_l2_regularizer_matches_fp64(rec, prec):
         chi2, S = rec.criterion()
         rec.gradient()
         S64 = O.l2_entropy64(img, p.model)
-        assert abs(S - S64) <= 1e-10 * abs(S64)
+        assert abs(S - S64) <= _s_tol(prec) * abs(S64)
         eg = rec.entropy_gradient().astype(np.float64)
         assert _rel(eg, O.l2_entropy_gradient64(img, p.model)) <= 1e-6
         rec.set_image(p.start_image())
@@ -643,7 +677,7 @@ def test_update_pixel_matches_full_recomputation(rec, prec):
             full.set_image(img)
             chi2_f, S_f = full.criterion()
             assert abs(chi2_u - chi2_f) <= 1e-5 * chi2_f, (step, chi2_u, chi2_f)
-            assert abs(S_u - S_f) <= 1e-9 * abs(S_f)
+            assert abs(S_u - S_f) <= max(1e-9, _s_tol(prec)) * abs(S_f)
             assert np.abs(rec.visibilities() - full.visibilities()).max() <= 2e-6
         assert np.array_equal(rec.get_image(), img)
         rec.gradient()
@@ -671,7 +705,7 @@ def test_update_pixel_matches_fp64_oracle(rec, prec):
         img[y * p.width + x] = np.float32(v)
         e = O.evaluate64(p, img, want_grad=(step == 4))
         assert abs(chi2_u - e["chi2"]) <= 1e-5 * e["chi2"], (step, chi2_u, e["chi2"])
-        assert abs(S_u - e["entropy"]) <= 1e-9 * max(1.0, abs(e["entropy"]))
+        assert abs(S_u - e["entropy"]) <= max(1e-9, _s_tol(prec)) * max(1.0, abs(e["entropy"]))
         assert np.abs(rec.visibilities() - e["visi"]).max() <= 1e-5
     rec.gradient()
     assert _rel(rec.data_gradient(), e["data_grad"]) <= 1e-5
@@ -702,7 +736,7 @@ def test_autotune_keeps_accuracy_and_caches():
         t = a.autotune(g.api.TUNE_PRECISION | g.api.TUNE_SPLITS, reps=2)
         assert t["precision"] in (g.PREC_FP32, g.PREC_SPLIT16) and not t["from_cache"]
         assert len(t["candidates"]) >= 4 and t["ms_per_eval"] > 0
-        assert t["ms_per_eval"] == min(ms for _, _, ms in t["candidates"])
+        assert t["ms_per_eval"] == min(cand[-1] for cand in t["candidates"])
         chi2, _ = a.criterion()
         a.gradient()
         assert abs(chi2 - e["chi2"]) <= 1e-5 * e["chi2"]
@@ -719,6 +753,15 @@ def test_autotune_keeps_accuracy_and_caches():
         b.set_image(p.start_image())
         out = b.cg(3, method=2, trace=True, line_search=g.LS_BATCH)
         assert out["iterations"] == 3 and np.all(np.diff(out["trace_J"]) <= 0)
+        # the tensor-core tile: CTA pairs (256 rows) against single CTAs (128 rows)
+        b.set_precision(g.PREC_SPLIT16)
+        td = b.autotune(g.api.TUNE_SPLITS | g.api.TUNE_TILE | g.api.TUNE_BATCHED, reps=2)
+        assert {cand[2] for cand in td["candidates"]} == {128, 256} and td["tile_m"] in (128, 256)
+        b.set_image(img)
+        chi2, _ = b.criterion()
+        b.gradient()
+        assert abs(chi2 - e["chi2"]) <= 1e-5 * e["chi2"]
+        assert _rel(b.data_gradient(), e["data_grad"]) <= 1e-5
 
 
 @pytest.mark.parametrize("ls", [0, 1])
@@ -855,19 +898,26 @@ def test_alternating_line_searches_reuse_their_graphs(rec):
     assert outs[1]["criterion_evals"] % g.LS_TRIALS == 3 % g.LS_TRIALS
 
 
-@pytest.mark.parametrize("ls", [0, 1])
-def test_batch_graph_equals_separate_runs(ls):
+@pytest.mark.parametrize("ls,independent,pair,mixed", [(0, False, True, False), (1, True, True, False),
+                                                       (1, False, True, False), (1, False, False, False),
+                                                       (1, False, True, True)])
+def test_batch_graph_equals_separate_runs(ls, independent, pair, mixed):
     """Consistency check (library against itself; single runs are oracle-pinned by
-    the CG tests above): gpair_batch_*, every context's CG loop in one graph, one
-    launch; the results are the separate runs' bit for bit, twice in a row (the
-    graph is reused)."""
+    the CG tests above): gpair_batch_*, one graph, one launch; the results are the
+    separate runs' bit for bit, twice in a row (the graph is reused). With the
+    batched line search the instances run in lockstep and each batched evaluation's
+    forwards are one grouped tcgen05 launch per class of tensor instances (CTA
+    pairs or single CTAs); an instance on the CUDA-core path (mixed) keeps its own
+    evaluation in the lockstep graph; with independent=True every CG loop is an
+    independent branch."""
     from gpair_b200.instances import instance
     ps = [instance(20_000_000 + k) for k in range(4)]
     recs = [g.Reconstructor(0) for _ in ps]
     try:
-        for r, p in zip(recs, ps):
+        for k, (r, p) in enumerate(zip(recs, ps)):
+            r.set_tc_pair(pair)
             r.set_problem(p)
-            r.set_precision(g.PREC_SPLIT16)
+            r.set_precision(g.PREC_FP32 if (mixed and k == 1) else g.PREC_SPLIT16)
         singles, imgs = [], []
         for r, p in zip(recs, ps):
             r.set_image(p.start_image())
@@ -875,7 +925,8 @@ def test_batch_graph_equals_separate_runs(ls):
             imgs.append(r.get_image())
         for r, p in zip(recs, ps):
             r.set_image(p.start_image())
-        with g.api.Batch(recs, line_search=ls) as b:
+        with g.api.Batch(recs, line_search=ls, independent=independent) as b:
+            assert b.grouped == (ls == 1 and not independent)
             for rep in range(2):
                 for r, p in zip(recs, ps):
                     r.set_image(p.start_image())
@@ -884,6 +935,46 @@ def test_batch_graph_equals_separate_runs(ls):
                     assert o["status"] == 0 and o["iterations"] == 5
                     assert o["J"] == a["J"] and o["criterion_evals"] == a["criterion_evals"]
                     assert np.array_equal(r.get_image(), img)
+    finally:
+        for r in recs:
+            r.close()
+
+
+def test_grouped_batch_wait_timeout_is_reported_and_recovers():
+    """The grouped forward's bounded waits run out (built from a first context whose
+    producer issues no TMA loads): every instance's run ends with GPAIR_ERR_TIMEOUT
+    instead of hanging; rebuilt with the normal wait, the same contexts give the
+    separate runs' results bit for bit."""
+    from gpair_b200.instances import instance
+    ps = [instance(20_000_100 + k) for k in range(3)]
+    recs = [g.Reconstructor(0) for _ in ps]
+    L = g.lib()
+    try:
+        for r, p in zip(recs, ps):
+            r.set_problem(p)
+            r.set_precision(g.PREC_SPLIT16)
+        singles, imgs = [], []
+        for r, p in zip(recs, ps):
+            r.set_image(p.start_image())
+            singles.append(r.cg(3, method=2, line_search=g.LS_BATCH))
+            imgs.append(r.get_image())
+        assert L.gpair_set_tc_wait(recs[0].h, 20_000_000, 1) == 0  # about 10 ms per wait
+        try:
+            for r, p in zip(recs, ps):
+                r.set_image(p.start_image())
+            with g.api.Batch(recs, line_search=g.LS_BATCH) as b:
+                assert b.grouped
+                with pytest.raises(g.GpairError, match=r"\(-5\)"):
+                    b.run(3)
+        finally:
+            assert L.gpair_set_tc_wait(recs[0].h, 0, 0) == 0
+        for r, p in zip(recs, ps):
+            r.set_image(p.start_image())
+        with g.api.Batch(recs, line_search=g.LS_BATCH) as b:
+            out = b.run(3)
+            for r, a, o, img in zip(recs, singles, out, imgs):
+                assert o["status"] == 0 and o["J"] == a["J"]
+                assert np.array_equal(r.get_image(), img)
     finally:
         for r in recs:
             r.close()
