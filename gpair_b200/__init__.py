@@ -7,5 +7,5 @@ this package holds the ctypes mirror of that ABI (api), OIFITS tables (oifits),
 the seeded synthetic data generator (synth) and the build script (build).
 """
 from .api import (IMG_CURR, IMG_TEMP, LS_BATCH, LS_TRIALS, LS_WOLFE, PREC_FP32, PREC_SPLIT16,  # noqa: F401
-                  PREC_TF32, PREC_TF32X3, REG_GULL_SKILLING, REG_L2, GpairError, Indexed, Problem, Reconstructor, cg_many, dft_tables, index_oifits, init_data, lib, problem_from_oifits, set_model,
+                  PREC_TF32, PREC_TF32X3, PREC_SPLIT16F8, REG_GULL_SKILLING, REG_L2, GpairError, Indexed, Problem, Reconstructor, cg_many, dft_tables, index_oifits, init_data, lib, problem_from_oifits, set_model,
                   workload_problem)

@@ -26,7 +26,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libgpair_b200.so")
 
 GPAIR_OK = 0
-PREC_FP32, PREC_SPLIT16, PREC_TF32, PREC_TF32X3 = 0, 1, 2, 3
+PREC_FP32, PREC_SPLIT16, PREC_TF32, PREC_TF32X3, PREC_SPLIT16F8 = 0, 1, 2, 3, 4
 REG_GULL_SKILLING, REG_L2 = 0, 1
 IMG_CURR, IMG_TEMP = 0, 1
 

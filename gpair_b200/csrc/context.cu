@@ -283,7 +283,7 @@ extern "C" int gpair_set_problem(gpair_ctx *c, int N, float pix, int nuv, const 
 
 extern "C" int gpair_set_precision(gpair_ctx *c, int mode)
 {
-    if (!c || mode < GPAIR_PREC_FP32 || mode > GPAIR_PREC_TF32X3) return GPAIR_ERR_INVALID;
+    if (!c || mode < GPAIR_PREC_FP32 || mode > GPAIR_PREC_SPLIT16F8) return GPAIR_ERR_INVALID;
     int old = c->precision;
     c->precision = mode;
     if (mode != GPAIR_PREC_FP32 && c->have_problem) {

@@ -144,6 +144,19 @@ __device__ __forceinline__ void mma_tf32_ss(uint32_t d_tmem, uint64_t a_desc, ui
         : "memory");
 }
 
+// The same with kind::f8f6f4: 8-bit float operands (E4M3 by the instruction
+// descriptor), K = 32 per MMA, FP32 accumulation
+__device__ __forceinline__ void mma_f8_ss(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                          uint32_t accumulate)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+        ::"r"(d_tmem), "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+        : "memory");
+}
+
 // Arrive once on `bar` when all previously issued MMAs of this thread complete
 __device__ __forceinline__ void mma_commit(uint64_t *bar)
 {
@@ -197,18 +210,9 @@ __device__ __forceinline__ uint64_t smem_desc_k_sw64(const void *tile)
     return d;
 }
 
-// Instruction descriptor, kind::i8: D s32 (fmt 2), A/B signed 8-bit (fmt 1), both K-major.
-__host__ __device__ constexpr uint32_t idesc_i8(int M, int N)
-{
-    return (2u << 4)                       // D format s32
-           | (1u << 7)                     // A signed 8-bit
-           | (1u << 10)                    // B signed 8-bit
-           | ((uint32_t)(N >> 3) << 17)    // N / 8
-           | ((uint32_t)(M >> 4) << 24);   // M / 16
-}
-
-// Instruction descriptor, kind::f16 / kind::tf32: D f32, A/B f16 (fmt 0), bf16
-// (fmt 1) or tf32 (fmt 2, with kind::tf32), both K-major.
+// Instruction descriptor, kind::f16 / kind::tf32 / kind::f8f6f4: D f32, A/B f16
+// (fmt 0), bf16 (fmt 1) or tf32 (fmt 2, with kind::tf32); with kind::f8f6f4,
+// fmt 0 is E4M3. Both operands K-major.
 __host__ __device__ constexpr uint32_t idesc_f16(int M, int N, int ab_fmt)
 {
     return (1u << 4)                       // D format f32
@@ -303,14 +307,15 @@ __device__ __forceinline__ void mma_tf32_pair(uint32_t d_tmem, uint64_t a_desc, 
         : "memory");
 }
 
-// D (+)= A * B^T over the CTA pair, kind::i8 (signed 8-bit operands, S32 accumulator)
-__device__ __forceinline__ void mma_i8_pair(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+// D (+)= A * B^T over the CTA pair, kind::f8f6f4 (8-bit float operands, K = 32
+// per MMA, FP32 accumulator)
+__device__ __forceinline__ void mma_f8_pair(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
                                             uint32_t accumulate)
 {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, {%5, %5, %5, %5, %5, %5, %5, %5}, p;\n\t}"
+        "tcgen05.mma.cta_group::2.kind::f8f6f4 [%0], %1, %2, %3, {%5, %5, %5, %5, %5, %5, %5, %5}, p;\n\t}"
         ::"r"(d_tmem), "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate), "r"(0u)
         : "memory");
 }

@@ -31,6 +31,7 @@
 // TMEM is released, and the host reports GPAIR_ERR_TIMEOUT.
 #include <cuda.h>
 #include <cuda_fp16.h>
+#include <cuda_fp8.h>
 #include <cudaTypedefs.h>
 #include <stdlib.h>
 #include <string.h>
@@ -59,8 +60,36 @@ enum { EPI_FWD = 0, EPI_STORE = 1 };
 // Operand element types: f16 (kind::f16, K = 16 per MMA) or TF32 held as FP32
 // bit patterns (kind::tf32, K = 8 per MMA). Both fill 128-byte K-block rows,
 // so the shared-memory stages, descriptors and TMA boxes are the same in bytes.
-enum { OP_F16 = 0, OP_TF32 = 1 };
-__host__ __device__ constexpr int tc_bk(int op) { return op == OP_F16 ? 64 : 32; }
+// OP_F16F8 (forward only): f16 hi operands for hi*hi (kind::f16) and 8-bit
+// E4M3 operands for the two cross terms (kind::f8f6f4, K = 32 per MMA, twice
+// the f16 rate), 64-byte rows with 64-byte swizzling; a K-block is 64 elements
+// of each.
+enum { OP_F16 = 0, OP_TF32 = 1, OP_F16F8 = 2 };
+__host__ __device__ constexpr int tc_bk(int op) { return op == OP_TF32 ? 32 : 64; }
+
+// E4M3 (round to nearest even, saturating at 448) of x
+__device__ __forceinline__ uint8_t to_e4m3(float x)
+{
+    return (uint8_t)__nv_cvt_float_to_fp8(x, __NV_SATFINITE, __NV_E4M3);
+}
+// Power-of-two scales of the 8-bit cross-term operands (E4M3 holds |x| <= 448
+// with 3 mantissa bits): twiddle hi / 4 (|hi| <= 2^10), twiddle lo * 2^10
+// (|lo| <= 2^-2), image hi / 2^10 (|hi| <= 2^15), image lo * 4 (|lo| <= 2^3).
+// (A_hi / 4)(4 B_lo) = A_hi B_lo and (2^10 A_lo)(B_hi / 2^10) = A_lo B_hi, so the
+// cross terms accumulate in the same FP32 accumulator as A_hi B_hi.
+#define F8_A_HI 0.25f
+#define F8_A_LO 1024.f
+#define F8_B_HI (1.f / 1024.f)
+#define F8_B_LO 4.f
+
+// f16 hi of v and the 8-bit pair (hi * s_hi, (v - hi) * s_lo)
+__device__ __forceinline__ void split_f8(float v, float s_hi, float s_lo, __half &h, uint8_t &q_hi, uint8_t &q_lo)
+{
+    h = __float2half_rn(v);
+    const float hf = __half2float(h);
+    q_hi = to_e4m3(hf * s_hi);
+    q_lo = to_e4m3((v - hf) * s_lo);
+}
 // products per K step: 3 = hi*hi + hi*lo + lo*hi of split operands, 1 = hi*hi
 // At most TC_SPLIT_PRODUCTS products per adjoint split-K partial (FP32 accumulation)
 #define TC_SPLIT_PRODUCTS 4096
@@ -126,7 +155,7 @@ struct TcArgs {
 // arguments. Held in global memory; the maps are read through their generic
 // addresses.
 struct __align__(64) TcGroupInst {
-    CUtensorMap A_hi, A_lo, B_hi, B_lo;
+    CUtensorMap A_hi, A_lo, A_x, B_hi, B_lo, B_x;  // A_x, B_x: OP_F16F8's second 8-bit operands
     int m_tiles, n_tiles, kb_total, units;
     const float2 *fya, *fyr;
     int nanc, nuv, lpad, elog2;
@@ -140,8 +169,12 @@ struct TcState {
     // B side (N = 256 rows): image [M_pad][Kx_pad], adjoint weights [M_pad][K2_pad]
     // batched trials: GP_NTR images stacked at Lb rows each, [GP_NTR Lb][Kx_pad]
     // op: OP_F16 or OP_TF32 (element size esz, bk elements per K-block);
-    // nprod: 3 (split operands; the lo buffers exist) or 1 (hi only)
-    int op, nprod, esz, bk;
+    // nprod: 3 (split operands; the lo buffers exist) or 1 (hi only);
+    // fop: the forward's operand kind (op, or OP_F16F8: the forward's lo
+    // operands are the E4M3 buffers *8h / *8l, its f16 lo buffers do not exist)
+    int op, nprod, esz, bk, fop;
+    void *fx8h, *fx8l, *img8h, *img8l, *imgb8h, *imgb8l;
+    CUtensorMap m_fx8h, m_fx8l, m_img8h, m_img8l, m_imgb8h, m_imgb8l;
     int Kx_pad, M_pad, rows_pad, K2_pad, xrows_pad;
     int Lb, epp_b;
     void *imgb_hi, *imgb_lo;
@@ -229,12 +262,21 @@ static_assert(TcGeo<0>::STAGES * TcGeo<0>::STAGE == TcGeo<1>::STAGES * TcGeo<1>:
 // GROUP = 1 (forward only): one launch over the units of several instances
 // (TcGroupInst), each with its own maps and epilogue arguments; the kernel's
 // map parameters are not used.
+//
+// OP_F16F8: each stage holds A_hi (f16, 128-byte rows), A8_hi and A8_lo (E4M3,
+// 64-byte rows), B_hi, B8_hi and B8_lo; per K-block 4 kind::f16 MMAs (A_hi B_hi)
+// and 2 x 2 kind::f8f6f4 MMAs (A8_hi B8_lo, A8_lo B8_hi), same stage bytes as
+// the three f16 products. Maps: (A_hi, A_lo, A_x) = (f16 hi, E4M3 hi, E4M3 lo)
+// and likewise for B; A_x and B_x are not used by the other operand kinds.
 template <int EPI, int OP, int NPROD, int PAIR, int GROUP>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     k_tc_gemm(const __grid_constant__ CUtensorMap tA_hi, const __grid_constant__ CUtensorMap tA_lo,
-              const __grid_constant__ CUtensorMap tB_hi, const __grid_constant__ CUtensorMap tB_lo, const TcArgs a)
+              const __grid_constant__ CUtensorMap tA_x, const __grid_constant__ CUtensorMap tB_hi,
+              const __grid_constant__ CUtensorMap tB_lo, const __grid_constant__ CUtensorMap tB_x, const TcArgs a)
 {
     static_assert(!GROUP || EPI == EPI_FWD, "grouped launches run the forward");
+    static_assert(OP != OP_F16F8 || (EPI == EPI_FWD && NPROD == 3), "the 8-bit cross terms serve the forward");
+    constexpr bool F8 = OP == OP_F16F8;
     using G = TcGeo<PAIR>;
     extern __shared__ unsigned char smem_raw[];
     unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -304,12 +346,16 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     if (warp == 0) {
         if (lane == 0) {
             // ------------------------------------------------ TMA producer
-            const CUtensorMap *mAh = &tA_hi, *mAl = &tA_lo, *mBh = &tB_hi, *mBl = &tB_lo;
+            const CUtensorMap *mAh = &tA_hi, *mAl = &tA_lo, *mAx = &tA_x, *mBh = &tB_hi, *mBl = &tB_lo, *mBx = &tB_x;
             if (!GROUP) {
                 umma::tma_prefetch(mAh);
                 umma::tma_prefetch(mAl);
                 umma::tma_prefetch(mBh);
                 umma::tma_prefetch(mBl);
+                if (F8) {
+                    umma::tma_prefetch(mAx);
+                    umma::tma_prefetch(mBx);
+                }
             }
             const uint32_t tx = (NPROD == 3 ? G::STAGE : TC_A_BYTES + G::B_BYTES) * (PAIR ? 2 : 1);
             int it = 0, ci = 0, cur = -1;
@@ -321,12 +367,18 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     cur = ci;
                     mAh = &a.grp[ci].A_hi;
                     mAl = &a.grp[ci].A_lo;
+                    mAx = &a.grp[ci].A_x;
                     mBh = &a.grp[ci].B_hi;
                     mBl = &a.grp[ci].B_lo;
+                    mBx = &a.grp[ci].B_x;
                     umma::tensormap_acquire(mAh);
                     umma::tensormap_acquire(mAl);
                     umma::tensormap_acquire(mBh);
                     umma::tensormap_acquire(mBl);
+                    if (F8) {
+                        umma::tensormap_acquire(mAx);
+                        umma::tensormap_acquire(mBx);
+                    }
                 }
                 const int arow0 = m * G::MT + (int)rank * 128, brow0 = n * TC_BN + (int)rank * G::BROWS;
                 for (int kb = kb0; kb < kb1; kb++) {
@@ -345,7 +397,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                         if (leader) umma::mbar_arrive_expect_tx(&full[s], tx);
                         umma::tma_load_2d_pair(st, mAh, fb, kx, arow0);
                         umma::tma_load_2d_pair(st + 2 * TC_A_BYTES, mBh, fb, kx, brow0);
-                        if (NPROD == 3) {
+                        if (F8) {
+                            // the 8-bit tiles: 64-byte rows, half the bytes of an f16 tile
+                            umma::tma_load_2d_pair(st + TC_A_BYTES, mAl, fb, kx, arow0);
+                            umma::tma_load_2d_pair(st + TC_A_BYTES + TC_A_BYTES / 2, mAx, fb, kx, arow0);
+                            umma::tma_load_2d_pair(st + 2 * TC_A_BYTES + G::B_BYTES, mBl, fb, kx, brow0);
+                            umma::tma_load_2d_pair(st + 2 * TC_A_BYTES + G::B_BYTES + G::B_BYTES / 2, mBx, fb, kx,
+                                                   brow0);
+                        } else if (NPROD == 3) {
                             umma::tma_load_2d_pair(st + TC_A_BYTES, mAl, fb, kx, arow0);
                             umma::tma_load_2d_pair(st + 2 * TC_A_BYTES + G::B_BYTES, mBl, fb, kx, brow0);
                         }
@@ -353,7 +412,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                         umma::mbar_arrive_expect_tx(&full[s], tx);
                         umma::tma_load_2d(st, mAh, &full[s], kx, arow0);
                         umma::tma_load_2d(st + 2 * TC_A_BYTES, mBh, &full[s], kx, brow0);
-                        if (NPROD == 3) {
+                        if (F8) {
+                            umma::tma_load_2d(st + TC_A_BYTES, mAl, &full[s], kx, arow0);
+                            umma::tma_load_2d(st + TC_A_BYTES + TC_A_BYTES / 2, mAx, &full[s], kx, arow0);
+                            umma::tma_load_2d(st + 2 * TC_A_BYTES + G::B_BYTES, mBl, &full[s], kx, brow0);
+                            umma::tma_load_2d(st + 2 * TC_A_BYTES + G::B_BYTES + G::B_BYTES / 2, mBx, &full[s], kx,
+                                              brow0);
+                        } else if (NPROD == 3) {
                             umma::tma_load_2d(st + TC_A_BYTES, mAl, &full[s], kx, arow0);
                             umma::tma_load_2d(st + 2 * TC_A_BYTES + G::B_BYTES, mBl, &full[s], kx, brow0);
                         }
@@ -376,7 +441,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     } else if (warp == 1) {
         if (lane == 0 && leader) {
             // ------------------------------------------------ MMA issuer
-            const uint32_t idesc = umma::idesc_f16(G::MT, TC_BN, OP == OP_F16 ? 0 : 2);
+            const uint32_t idesc = umma::idesc_f16(G::MT, TC_BN, OP == OP_TF32 ? 2 : 0);  // f16, tf32; E4M3 for f8f6f4
             int it = 0, t = 0, ci = 0;
             bool ok = true, issued = false;
             for (int u = unit0; u < units && ok && !*abort_flag; u += ustep, t++) {
@@ -402,36 +467,62 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     const uint64_t dal = umma::smem_desc_k_sw128(st + TC_A_BYTES);
                     const uint64_t dbh = umma::smem_desc_k_sw128(st + 2 * TC_A_BYTES);
                     const uint64_t dbl = umma::smem_desc_k_sw128(st + 2 * TC_A_BYTES + G::B_BYTES);
+                    if (F8) {
+                        // hi*hi in f16, then the cross terms A8_hi B8_lo + A8_lo B8_hi in E4M3
+                        const uint64_t qah = umma::smem_desc_k_sw64(st + TC_A_BYTES);
+                        const uint64_t qal = umma::smem_desc_k_sw64(st + TC_A_BYTES + TC_A_BYTES / 2);
+                        const uint64_t qbh = umma::smem_desc_k_sw64(st + 2 * TC_A_BYTES + G::B_BYTES);
+                        const uint64_t qbl = umma::smem_desc_k_sw64(st + 2 * TC_A_BYTES + G::B_BYTES + G::B_BYTES / 2);
 #pragma unroll
-                    for (int kk = 0; kk < TC_ROWB / 32; kk++) {
-                        // one MMA covers 32 B along K: 16 f16 or 8 TF32 elements
-                        const uint64_t off = (uint64_t)(kk * 32) >> 4;
-                        const uint32_t acc = (kb > kb0 || kk > 0) ? 1u : 0u;
-                        if (PAIR) {
-                            if (OP == OP_F16) {
-                                umma::mma_f16_pair(d, dah + off, dbh + off, idesc, acc);
+                        for (int kk = 0; kk < TC_ROWB / 32; kk++) {
+                            const uint64_t off = (uint64_t)(kk * 32) >> 4;
+                            const uint32_t acc = (kb > kb0 || kk > 0) ? 1u : 0u;
+                            if (PAIR) umma::mma_f16_pair(d, dah + off, dbh + off, idesc, acc);
+                            else umma::mma_f16_ss(d, dah + off, dbh + off, idesc, acc);
+                        }
+#pragma unroll
+                        for (int kk = 0; kk < 2; kk++) {  // 32 E4M3 elements (32 B) per MMA
+                            const uint64_t off = (uint64_t)(kk * 32) >> 4;
+                            if (PAIR) {
+                                umma::mma_f8_pair(d, qah + off, qbl + off, idesc, 1u);
+                                umma::mma_f8_pair(d, qal + off, qbh + off, idesc, 1u);
+                            } else {
+                                umma::mma_f8_ss(d, qah + off, qbl + off, idesc, 1u);
+                                umma::mma_f8_ss(d, qal + off, qbh + off, idesc, 1u);
+                            }
+                        }
+                    } else {
+#pragma unroll
+                        for (int kk = 0; kk < TC_ROWB / 32; kk++) {
+                            // one MMA covers 32 B along K: 16 f16 or 8 TF32 elements
+                            const uint64_t off = (uint64_t)(kk * 32) >> 4;
+                            const uint32_t acc = (kb > kb0 || kk > 0) ? 1u : 0u;
+                            if (PAIR) {
+                                if (OP == OP_F16) {
+                                    umma::mma_f16_pair(d, dah + off, dbh + off, idesc, acc);
+                                    if (NPROD == 3) {
+                                        umma::mma_f16_pair(d, dah + off, dbl + off, idesc, 1u);
+                                        umma::mma_f16_pair(d, dal + off, dbh + off, idesc, 1u);
+                                    }
+                                } else {
+                                    umma::mma_tf32_pair(d, dah + off, dbh + off, idesc, acc);
+                                    if (NPROD == 3) {
+                                        umma::mma_tf32_pair(d, dah + off, dbl + off, idesc, 1u);
+                                        umma::mma_tf32_pair(d, dal + off, dbh + off, idesc, 1u);
+                                    }
+                                }
+                            } else if (OP == OP_F16) {
+                                umma::mma_f16_ss(d, dah + off, dbh + off, idesc, acc);
                                 if (NPROD == 3) {
-                                    umma::mma_f16_pair(d, dah + off, dbl + off, idesc, 1u);
-                                    umma::mma_f16_pair(d, dal + off, dbh + off, idesc, 1u);
+                                    umma::mma_f16_ss(d, dah + off, dbl + off, idesc, 1u);
+                                    umma::mma_f16_ss(d, dal + off, dbh + off, idesc, 1u);
                                 }
                             } else {
-                                umma::mma_tf32_pair(d, dah + off, dbh + off, idesc, acc);
+                                umma::mma_tf32_ss(d, dah + off, dbh + off, idesc, acc);
                                 if (NPROD == 3) {
-                                    umma::mma_tf32_pair(d, dah + off, dbl + off, idesc, 1u);
-                                    umma::mma_tf32_pair(d, dal + off, dbh + off, idesc, 1u);
+                                    umma::mma_tf32_ss(d, dah + off, dbl + off, idesc, 1u);
+                                    umma::mma_tf32_ss(d, dal + off, dbh + off, idesc, 1u);
                                 }
-                            }
-                        } else if (OP == OP_F16) {
-                            umma::mma_f16_ss(d, dah + off, dbh + off, idesc, acc);
-                            if (NPROD == 3) {
-                                umma::mma_f16_ss(d, dah + off, dbl + off, idesc, 1u);
-                                umma::mma_f16_ss(d, dal + off, dbh + off, idesc, 1u);
-                            }
-                        } else {
-                            umma::mma_tf32_ss(d, dah + off, dbh + off, idesc, acc);
-                            if (NPROD == 3) {
-                                umma::mma_tf32_ss(d, dah + off, dbl + off, idesc, 1u);
-                                umma::mma_tf32_ss(d, dal + off, dbh + off, idesc, 1u);
                             }
                         }
                     }
@@ -579,11 +670,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 
 // Twiddle operands: forward B [rows_pad][Kx_pad] (row 2k+c = Re/Im of Fx[k][:])
 // and adjoint B [xrows_pad][K2_pad] (row x, column 2k+c), both scaled by 2^10.
-// lo == nullptr: hi only (one-product mode).
+// lo == nullptr: hi only (one-product mode). fx8 != nullptr (OP_F16F8): the
+// forward's E4M3 pair (hi / 4, lo * 2^10) instead of its f16 lo.
 template <typename OT>
 __global__ void k_tc_twiddle_ops(const float2 *__restrict__ fx, int nuv, int N, int Kx_pad, int rows_pad,
                                  int K2_pad, int xrows_pad, OT *__restrict__ fx_hi, OT *__restrict__ fx_lo,
-                                 OT *__restrict__ fxt_hi, OT *__restrict__ fxt_lo)
+                                 uint8_t *__restrict__ fx8h, uint8_t *__restrict__ fx8l, OT *__restrict__ fxt_hi,
+                                 OT *__restrict__ fxt_lo)
 {
     const float ts = (float)(1 << TC_TW_LOG2);
     long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -595,7 +688,15 @@ __global__ void k_tc_twiddle_ops(const float2 *__restrict__ fx, int nuv, int N, 
             float2 f = fx[(size_t)k * N + x];
             v = ((n & 1) ? f.y : f.x) * ts;
         }
-        split_store(fx_hi, fx_lo, (size_t)idx, v);
+        if (fx8h) {
+            if constexpr (sizeof(OT) == 2) {
+                __half h;
+                split_f8(v, F8_A_HI, F8_A_LO, h, fx8h[idx], fx8l[idx]);
+                fx_hi[idx] = h;
+            }
+        } else {
+            split_store(fx_hi, fx_lo, (size_t)idx, v);
+        }
         return;
     }
     idx -= nf;
@@ -687,7 +788,8 @@ template <typename OT, int MODE>
 __global__ void __launch_bounds__(PR_THREADS)
     k_tc_prep_rows(const float *__restrict__ img, const float *__restrict__ d, float *__restrict__ dst,
                    const float *__restrict__ model, int N, int W, int Lpad, int Kx_pad, OT *__restrict__ hi,
-                   OT *__restrict__ lo, float *__restrict__ rsc, int reduce, double *__restrict__ partials,
+                   OT *__restrict__ lo, uint8_t *__restrict__ h8, uint8_t *__restrict__ l8,
+                   float *__restrict__ rsc, int reduce, double *__restrict__ partials,
                    DevScalars *__restrict__ sc, const int *__restrict__ gate)
 {
     __shared__ double smem[3 * 32];
@@ -772,12 +874,35 @@ __global__ void __launch_bounds__(PR_THREADS)
         if (xv) {
 #pragma unroll
             for (int k = 0; k < 8; k++) v[k] *= scale;
-            split_store8(hi, lo, (row0 + y) * Kx_pad + x, v);
+            const size_t o = (row0 + y) * Kx_pad + x;
+            if (h8) {
+                if constexpr (sizeof(OT) == 2) {
+                    // f16 hi plus the E4M3 pair (hi / 2^10, lo * 4): 16 + 8 + 8 bytes
+                    __align__(16) __half hh[8];
+                    __align__(8) uint8_t qh[8], ql[8];
+#pragma unroll
+                    for (int k = 0; k < 8; k++) split_f8(v[k], F8_B_HI, F8_B_LO, hh[k], qh[k], ql[k]);
+                    *reinterpret_cast<uint4 *>(hi + o) = *reinterpret_cast<const uint4 *>(hh);
+                    *reinterpret_cast<uint2 *>(h8 + o) = *reinterpret_cast<const uint2 *>(qh);
+                    *reinterpret_cast<uint2 *>(l8 + o) = *reinterpret_cast<const uint2 *>(ql);
+                }
+            } else {
+                split_store8(hi, lo, o, v);
+            }
         } else if (!vec && yv) {
             // second pass: each thread reads back the values it wrote (or the image)
             for (int xx = t; xx < N; xx += nt) {
                 const float I = MODE ? dst[rp + xx] : __ldg(&img[rp + xx]);
-                split_store(hi, lo, (row0 + y) * Kx_pad + xx, I * scale);
+                const size_t o = (row0 + y) * Kx_pad + xx;
+                if (h8) {
+                    if constexpr (sizeof(OT) == 2) {
+                        __half hh;
+                        split_f8(I * scale, F8_B_HI, F8_B_LO, hh, h8[o], l8[o]);
+                        hi[o] = hh;
+                    }
+                } else {
+                    split_store(hi, lo, o, I * scale);
+                }
             }
         }
         if (yv && t == 0) rsc[row0 + y] = ldexpf(1.f, ex - 15 - TC_TW_LOG2);
@@ -1051,11 +1176,33 @@ static int tc_make_map(gpair_ctx *c, CUtensorMap *m, const void *base, long long
     return GPAIR_OK;
 }
 
-// operand kind and product count of a precision mode
-static void tc_mode(int precision, int *op, int *nprod)
+// operand kind and product count of a precision mode, and the forward's operand kind
+static void tc_mode(int precision, int *op, int *nprod, int *fop = nullptr)
 {
     *op = (precision == GPAIR_PREC_TF32 || precision == GPAIR_PREC_TF32X3) ? OP_TF32 : OP_F16;
     *nprod = precision == GPAIR_PREC_TF32 ? 1 : 3;
+    if (fop) *fop = precision == GPAIR_PREC_SPLIT16F8 ? OP_F16F8 : *op;
+}
+
+// 2-D tensor [rows][cols] of bytes (E4M3), boxes of 64 bytes x box_rows, 64 B swizzle
+static int tc_make_map8(gpair_ctx *c, CUtensorMap *m, const void *base, long long rows, long long cols, int box_rows)
+{
+    if (cols % 64 || rows % box_rows || ((uintptr_t)base & 255)) {
+        snprintf(c->last_error, sizeof(c->last_error), "tensor map shape/alignment violates TMA rules");
+        return GPAIR_ERR_INVALID;
+    }
+    cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)cols};
+    cuuint32_t box[2] = {64u, (cuuint32_t)box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void *>(base), dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        snprintf(c->last_error, sizeof(c->last_error), "cuTensorMapEncodeTiled (8-bit) failed (%d)", (int)r);
+        return GPAIR_ERR_CUDA;
+    }
+    return GPAIR_OK;
 }
 
 // Split-K of the tensor adjoint for K-blocks of `bk` elements: enough splits to
@@ -1098,7 +1245,7 @@ void gp_tc_free(gpair_ctx *c)
     if (!t) return;
     c->buf_gen++;
     void *bufs[] = {t->img_hi, t->img_lo, t->fx_hi, t->fx_lo, t->fxt_hi, t->fxt_lo, t->w_hi, t->w_lo,
-                    t->imgb_hi, t->imgb_lo};
+                    t->imgb_hi, t->imgb_lo, t->fx8h, t->fx8l, t->img8h, t->img8l, t->imgb8h, t->imgb8l};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (t->fya) cudaFree(t->fya);
@@ -1114,7 +1261,7 @@ static void launch_twiddle_ops(gpair_ctx *c, TcState *t, long long n_all)
 {
     k_tc_twiddle_ops<OT><<<gp_cdiv(n_all, 256), 256, 0, c->stream>>>(
         c->fx, c->nuv, c->N, t->Kx_pad, t->rows_pad, t->K2_pad, t->xrows_pad, (OT *)t->fx_hi, (OT *)t->fx_lo,
-        (OT *)t->fxt_hi, (OT *)t->fxt_lo);
+        (uint8_t *)t->fx8h, (uint8_t *)t->fx8l, (OT *)t->fxt_hi, (OT *)t->fxt_lo);
 }
 
 template <int EPI, int PAIR, int GROUP>
@@ -1127,17 +1274,20 @@ static int tc_set_smem(gpair_ctx *c)
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     GP_CUDA(c, cudaFuncSetAttribute(k_tc_gemm<EPI, OP_TF32, 1, PAIR, GROUP>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    if (EPI == EPI_FWD)
+        GP_CUDA(c, cudaFuncSetAttribute(k_tc_gemm<EPI_FWD, OP_F16F8, 3, PAIR, GROUP>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     return GPAIR_OK;
 }
 
 int gp_tc_prepare(gpair_ctx *c)
 {
     if (!c->have_problem) return GPAIR_OK;  // prepared when the problem is loaded
-    int op, nprod;
-    tc_mode(c->precision, &op, &nprod);
+    int op, nprod, fop;
+    tc_mode(c->precision, &op, &nprod, &fop);
     const int pair = c->tc_pair ? 1 : 0;
     TcState *old = (TcState *)c->tc_state;
-    if (old && old->op == op && old->nprod == nprod && old->pair == pair) return GPAIR_OK;
+    if (old && old->op == op && old->nprod == nprod && old->fop == fop && old->pair == pair) return GPAIR_OK;
     if (old) {
         // another operand kind: rebuild every operand buffer for this mode
         GP_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -1150,6 +1300,7 @@ int gp_tc_prepare(gpair_ctx *c)
     c->tc_state = t;
     t->op = op;
     t->nprod = nprod;
+    t->fop = fop;
     t->pair = pair;
     t->esz = op == OP_F16 ? 2 : 4;
     t->bk = tc_bk(op);
@@ -1164,14 +1315,19 @@ int gp_tc_prepare(gpair_ctx *c)
     t->splits = gp_tc_splits(N, nuv, t->nsm, t->bk, pair, &t->kb_per);
     size_t img = (size_t)t->M_pad * t->Kx_pad, fxs = (size_t)t->rows_pad * t->Kx_pad;
     size_t fxts = (size_t)t->xrows_pad * t->K2_pad, ws = (size_t)t->M_pad * t->K2_pad;
-    struct { void **p; size_t n; bool lo; } al[] = {{&t->img_hi, img, false}, {&t->img_lo, img, true},
-                                                    {&t->fx_hi, fxs, false},  {&t->fx_lo, fxs, true},
-                                                    {&t->fxt_hi, fxts, false}, {&t->fxt_lo, fxts, true},
-                                                    {&t->w_hi, ws, false},    {&t->w_lo, ws, true}};
+    const bool f8 = fop == OP_F16F8;
+    // f8: the forward's lo operands are E4M3 pairs (1 byte per element each)
+    struct { void **p; size_t n; bool lo; int esz; } al[] = {
+        {&t->img_hi, img, false, t->esz},  {&t->img_lo, f8 ? 0 : img, true, t->esz},
+        {&t->fx_hi, fxs, false, t->esz},   {&t->fx_lo, f8 ? 0 : fxs, true, t->esz},
+        {&t->fxt_hi, fxts, false, t->esz}, {&t->fxt_lo, fxts, true, t->esz},
+        {&t->w_hi, ws, false, t->esz},     {&t->w_lo, ws, true, t->esz},
+        {&t->img8h, f8 ? img : 0, true, 1}, {&t->img8l, f8 ? img : 0, true, 1},
+        {&t->fx8h, f8 ? fxs : 0, true, 1},  {&t->fx8l, f8 ? fxs : 0, true, 1}};
     for (auto &x : al) {
-        if (x.lo && nprod == 1) continue;  // one product: no lo operands
-        GP_CUDA(c, cudaMalloc(x.p, x.n * t->esz));
-        GP_CUDA(c, cudaMemsetAsync(*x.p, 0, x.n * t->esz, c->stream));
+        if ((x.lo && nprod == 1) || x.n == 0) continue;  // one product: no lo operands
+        GP_CUDA(c, cudaMalloc(x.p, x.n * x.esz));
+        GP_CUDA(c, cudaMemsetAsync(*x.p, 0, x.n * x.esz, c->stream));
     }
     GP_CUDA(c, cudaMalloc(&t->rsc, sizeof(float) * (size_t)t->M_pad));
     GP_CUDA(c, cudaMemsetAsync(t->rsc, 0, sizeof(float) * (size_t)t->M_pad, c->stream));
@@ -1194,8 +1350,17 @@ int gp_tc_prepare(gpair_ctx *c)
     if ((rc = tc_make_map(c, &t->m_w_hi, t->w_hi, t->M_pad, t->K2_pad, bbox, e))) return rc;
     if ((rc = tc_make_map(c, &t->m_fxt_hi, t->fxt_hi, t->xrows_pad, t->K2_pad, TC_BM, e))) return rc;
     if (nprod == 3) {
-        if ((rc = tc_make_map(c, &t->m_img_lo, t->img_lo, t->M_pad, t->Kx_pad, bbox, e))) return rc;
-        if ((rc = tc_make_map(c, &t->m_fx_lo, t->fx_lo, t->rows_pad, t->Kx_pad, TC_BM, e))) return rc;
+        if (f8) {
+            if ((rc = tc_make_map8(c, &t->m_img8h, t->img8h, t->M_pad, t->Kx_pad, bbox))) return rc;
+            if ((rc = tc_make_map8(c, &t->m_img8l, t->img8l, t->M_pad, t->Kx_pad, bbox))) return rc;
+            if ((rc = tc_make_map8(c, &t->m_fx8h, t->fx8h, t->rows_pad, t->Kx_pad, TC_BM))) return rc;
+            if ((rc = tc_make_map8(c, &t->m_fx8l, t->fx8l, t->rows_pad, t->Kx_pad, TC_BM))) return rc;
+            t->m_img_lo = t->m_img_hi;  // not loaded by the OP_F16F8 forward
+            t->m_fx_lo = t->m_fx_hi;
+        } else {
+            if ((rc = tc_make_map(c, &t->m_img_lo, t->img_lo, t->M_pad, t->Kx_pad, bbox, e))) return rc;
+            if ((rc = tc_make_map(c, &t->m_fx_lo, t->fx_lo, t->rows_pad, t->Kx_pad, TC_BM, e))) return rc;
+        }
         if ((rc = tc_make_map(c, &t->m_w_lo, t->w_lo, t->M_pad, t->K2_pad, bbox, e))) return rc;
         if ((rc = tc_make_map(c, &t->m_fxt_lo, t->fxt_lo, t->xrows_pad, t->K2_pad, TC_BM, e))) return rc;
     } else {
@@ -1284,10 +1449,14 @@ static TcState *tc_state_ready(gpair_ctx *c, int *rc)
     return t;
 }
 
+// The maps of one contraction: (A_hi, A_lo, A_x, B_hi, B_lo, B_x); A_x and B_x
+// are read by the OP_F16F8 forward only
+struct TcMaps {
+    const CUtensorMap *a_hi, *a_lo, *a_x, *b_hi, *b_lo, *b_x;
+};
+
 template <int EPI, int PAIR>
-static cudaError_t tc_launch_kind(TcState *t, dim3 grid, cudaStream_t st, const CUtensorMap &A_hi,
-                                  const CUtensorMap &A_lo, const CUtensorMap &B_hi, const CUtensorMap &B_lo,
-                                  const TcArgs &a)
+static cudaError_t tc_launch_kind(TcState *t, dim3 grid, cudaStream_t st, const TcMaps &m, const TcArgs &a)
 {
     cudaLaunchConfig_t cfg;
     memset(&cfg, 0, sizeof(cfg));
@@ -1302,17 +1471,23 @@ static cudaError_t tc_launch_kind(TcState *t, dim3 grid, cudaStream_t st, const 
     cfg.stream = st;
     cfg.attrs = at;
     cfg.numAttrs = PAIR ? 1 : 0;
-    if (t->op == OP_F16) return cudaLaunchKernelEx(&cfg, k_tc_gemm<EPI, OP_F16, 3, PAIR, 0>, A_hi, A_lo, B_hi, B_lo, a);
+    if (EPI == EPI_FWD && t->fop == OP_F16F8)
+        return cudaLaunchKernelEx(&cfg, k_tc_gemm<EPI_FWD, OP_F16F8, 3, PAIR, 0>, *m.a_hi, *m.a_lo, *m.a_x, *m.b_hi,
+                                  *m.b_lo, *m.b_x, a);
+    if (t->op == OP_F16)
+        return cudaLaunchKernelEx(&cfg, k_tc_gemm<EPI, OP_F16, 3, PAIR, 0>, *m.a_hi, *m.a_lo, *m.a_x, *m.b_hi,
+                                  *m.b_lo, *m.b_x, a);
     if (t->nprod == 3)
-        return cudaLaunchKernelEx(&cfg, k_tc_gemm<EPI, OP_TF32, 3, PAIR, 0>, A_hi, A_lo, B_hi, B_lo, a);
-    return cudaLaunchKernelEx(&cfg, k_tc_gemm<EPI, OP_TF32, 1, PAIR, 0>, A_hi, A_lo, B_hi, B_lo, a);
+        return cudaLaunchKernelEx(&cfg, k_tc_gemm<EPI, OP_TF32, 3, PAIR, 0>, *m.a_hi, *m.a_lo, *m.a_x, *m.b_hi,
+                                  *m.b_lo, *m.b_x, a);
+    return cudaLaunchKernelEx(&cfg, k_tc_gemm<EPI, OP_TF32, 1, PAIR, 0>, *m.a_hi, *m.a_lo, *m.a_x, *m.b_hi,
+                              *m.b_lo, *m.b_x, a);
 }
 
 // one launch of the contraction in the context's operand kind / product count:
 // persistent CTAs (or CTA pairs), one per SM (pair of SMs) at most
 template <int EPI>
-static int tc_launch(gpair_ctx *c, TcState *t, const CUtensorMap &A_hi, const CUtensorMap &A_lo,
-                     const CUtensorMap &B_hi, const CUtensorMap &B_lo, TcArgs &a)
+static int tc_launch(gpair_ctx *c, TcState *t, const TcMaps &m, TcArgs &a)
 {
     a.err = &c->sc->tc_err;
     a.budget = c->tc_wait_budget > 0 ? c->tc_wait_budget : TC_WAIT_BUDGET;
@@ -1320,10 +1495,10 @@ static int tc_launch(gpair_ctx *c, TcState *t, const CUtensorMap &A_hi, const CU
     cudaError_t e;
     if (t->pair) {
         const int np = a.units < t->npairs ? a.units : t->npairs;
-        e = tc_launch_kind<EPI, 1>(t, dim3(2 * np, 1, 1), c->stream, A_hi, A_lo, B_hi, B_lo, a);
+        e = tc_launch_kind<EPI, 1>(t, dim3(2 * np, 1, 1), c->stream, m, a);
     } else {
         const int g = a.units < t->nsm ? a.units : t->nsm;
-        e = tc_launch_kind<EPI, 0>(t, dim3(g, 1, 1), c->stream, A_hi, A_lo, B_hi, B_lo, a);
+        e = tc_launch_kind<EPI, 0>(t, dim3(g, 1, 1), c->stream, m, a);
     }
     if (e != cudaSuccess) {
         snprintf(c->last_error, sizeof(c->last_error), "tensor-core contraction launch: %s", cudaGetErrorString(e));
@@ -1331,6 +1506,20 @@ static int tc_launch(gpair_ctx *c, TcState *t, const CUtensorMap &A_hi, const CU
     }
     c->launches++;
     return GPAIR_OK;
+}
+
+// the forward's maps over an image-side operand (single image or batch stack)
+static TcMaps tc_fwd_maps(const TcState *t, bool batch)
+{
+    const bool f8 = t->fop == OP_F16F8;
+    TcMaps m;
+    m.a_hi = &t->m_fx_hi;
+    m.a_lo = f8 ? &t->m_fx8h : &t->m_fx_lo;
+    m.a_x = f8 ? &t->m_fx8l : &t->m_fx_hi;
+    m.b_hi = batch ? &t->m_imgb_hi : &t->m_img_hi;
+    m.b_lo = f8 ? (batch ? &t->m_imgb8h : &t->m_img8h) : (batch ? &t->m_imgb_lo : &t->m_img_lo);
+    m.b_x = f8 ? (batch ? &t->m_imgb8l : &t->m_img8l) : m.b_hi;
+    return m;
 }
 
 // Row-wise prep launches (k_tc_prep_rows): PR_THREADS threads per block, R rows
@@ -1343,7 +1532,9 @@ static void tc_prep_rows_kernel(gpair_ctx *c, TcState *t, dim3 g, int W, const f
     const bool b = MODE == 2;
     k_tc_prep_rows<OT, MODE><<<g, PR_THREADS, 0, c->stream>>>(
         img, c->descent_dir, dst, c->model, c->N, W, b ? t->Lb : 0, t->Kx_pad, (OT *)(b ? t->imgb_hi : t->img_hi),
-        (OT *)(b ? t->imgb_lo : t->img_lo), b ? t->rscb : t->rsc, reduce, partials, c->sc, b ? c->gate : nullptr);
+        (OT *)(b ? t->imgb_lo : t->img_lo), (uint8_t *)(b ? t->imgb8h : t->img8h),
+        (uint8_t *)(b ? t->imgb8l : t->img8l), b ? t->rscb : t->rsc, reduce, partials, c->sc,
+        b ? c->gate : nullptr);
 }
 
 static int tc_prep_rows_launch(gpair_ctx *c, TcState *t, int mode, int reduce, double *partials,
@@ -1392,7 +1583,7 @@ int gp_tc_forward_gemm(gpair_ctx *c)
     a.elog2 = 8;
     a.rsc = t->rsc;
     a.vpart = c->vpart;
-    if ((rc = tc_launch<EPI_FWD>(c, t, t->m_fx_hi, t->m_fx_lo, t->m_img_hi, t->m_img_lo, a))) return rc;
+    if ((rc = tc_launch<EPI_FWD>(c, t, tc_fwd_maps(t, false), a))) return rc;
     c->mt = a.n_tiles;
     return GPAIR_OK;
 }
@@ -1417,7 +1608,15 @@ int gp_tc_batch_prepare(gpair_ctx *c, int *epp)
         GP_CUDA(c, cudaMemsetAsync(t->imgb_hi, 0, n * t->esz, c->stream));
         const int bbox = t->pair ? 128 : TC_BN;
         if ((rc = tc_make_map(c, &t->m_imgb_hi, t->imgb_hi, (long long)rows, t->Kx_pad, bbox, t->esz))) return rc;
-        if (t->nprod == 3) {
+        if (t->fop == OP_F16F8) {
+            GP_CUDA(c, cudaMalloc(&t->imgb8h, n));
+            GP_CUDA(c, cudaMemsetAsync(t->imgb8h, 0, n, c->stream));
+            GP_CUDA(c, cudaMalloc(&t->imgb8l, n));
+            GP_CUDA(c, cudaMemsetAsync(t->imgb8l, 0, n, c->stream));
+            if ((rc = tc_make_map8(c, &t->m_imgb8h, t->imgb8h, (long long)rows, t->Kx_pad, bbox))) return rc;
+            if ((rc = tc_make_map8(c, &t->m_imgb8l, t->imgb8l, (long long)rows, t->Kx_pad, bbox))) return rc;
+            t->m_imgb_lo = t->m_imgb_hi;  // not loaded by the OP_F16F8 forward
+        } else if (t->nprod == 3) {
             GP_CUDA(c, cudaMalloc(&t->imgb_lo, n * t->esz));
             GP_CUDA(c, cudaMemsetAsync(t->imgb_lo, 0, n * t->esz, c->stream));
             if ((rc = tc_make_map(c, &t->m_imgb_lo, t->imgb_lo, (long long)rows, t->Kx_pad, bbox, t->esz)))
@@ -1466,7 +1665,7 @@ int gp_tc_forward_batch_gemm(gpair_ctx *c)
     a.elog2 = erows == 32 ? 5 : erows == 64 ? 6 : erows == 128 ? 7 : 8;
     a.rsc = t->rscb;
     a.vpart = c->vpart_b;
-    return tc_launch<EPI_FWD>(c, t, t->m_fx_hi, t->m_fx_lo, t->m_imgb_hi, t->m_imgb_lo, a);
+    return tc_launch<EPI_FWD>(c, t, tc_fwd_maps(t, true), a);
 }
 
 // split of an image into the forward's image operand (its flux and regulariser
@@ -1548,7 +1747,8 @@ int gp_tc_adjoint_gemm(gpair_ctx *c)
     a.out_ld = c->N;
     a.out_rows = c->N;
     a.out_cols = c->N;
-    if ((rc = tc_launch<EPI_STORE>(c, t, t->m_fxt_hi, t->m_fxt_lo, t->m_w_hi, t->m_w_lo, a))) return rc;
+    const TcMaps m = {&t->m_fxt_hi, &t->m_fxt_lo, &t->m_fxt_hi, &t->m_w_hi, &t->m_w_lo, &t->m_w_hi};
+    if ((rc = tc_launch<EPI_STORE>(c, t, m, a))) return rc;
     c->splits = t->splits;
     return GPAIR_OK;
 }
@@ -1569,7 +1769,7 @@ int gp_tc_adjoint(gpair_ctx *c, int which)
 // TcGroupInst array in global memory, share the persistent CTAs (or CTA pairs).
 // All instances use the same operand kind, product count and tile layout.
 struct TcGroup {
-    int n, op, nprod, pair, npairs, nsm;
+    int n, op, nprod, pair, npairs, nsm;  // op: the forward's operand kind
     TcGroupInst *d_inst;  // [n], device
     CUtensorMap map0;     // a valid map for the kernel's unused map parameters
     const int *gate;      // [n], device, owned by the caller
@@ -1589,9 +1789,9 @@ void gp_tc_group_free(void *grp)
 int gp_tc_group_key(gpair_ctx *c)
 {
     if (c->precision == GPAIR_PREC_FP32) return -1;
-    int op, nprod;
-    tc_mode(c->precision, &op, &nprod);
-    return (op * 4 + nprod) * 2 + (c->tc_pair ? 1 : 0);
+    int op, nprod, fop;
+    tc_mode(c->precision, &op, &nprod, &fop);
+    return (fop * 4 + nprod) * 2 + (c->tc_pair ? 1 : 0);
 }
 
 // Builds the group of ctx[0..n-1] (their tensor state and batch buffers are
@@ -1614,16 +1814,19 @@ int gp_tc_group_build(gpair_ctx **ctx, int n, const int *gate, unsigned int *err
         TcState *t = tc_state_ready(c, &rc);
         if (rc) break;
         if ((rc = gp_batch_alloc(c))) break;
-        if (t0 && (t->op != t0->op || t->nprod != t0->nprod || t->pair != t0->pair)) {
+        if (t0 && (t->fop != t0->fop || t->nprod != t0->nprod || t->pair != t0->pair)) {
             rc = GPAIR_ERR_STATE;
             break;
         }
         if (!t0) t0 = t;
         TcGroupInst &g = h[i];
-        g.A_hi = t->m_fx_hi;
-        g.A_lo = t->m_fx_lo;
-        g.B_hi = t->m_imgb_hi;
-        g.B_lo = t->m_imgb_lo;
+        const TcMaps fm = tc_fwd_maps(t, true);
+        g.A_hi = *fm.a_hi;
+        g.A_lo = *fm.a_lo;
+        g.A_x = *fm.a_x;
+        g.B_hi = *fm.b_hi;
+        g.B_lo = *fm.b_lo;
+        g.B_x = *fm.b_x;
         g.m_tiles = t->rows_pad / (t->pair ? 256 : TC_BM);
         g.n_tiles = (GP_NTR * t->Lb) / TC_BN;
         g.kb_total = t->Kx_pad / t->bk;
@@ -1645,7 +1848,7 @@ int gp_tc_group_build(gpair_ctx **ctx, int n, const int *gate, unsigned int *err
     }
     if (!rc) {
         G->n = n;
-        G->op = t0->op;
+        G->op = t0->fop;
         G->nprod = t0->nprod;
         G->pair = t0->pair;
         G->npairs = t0->npairs;
@@ -1686,9 +1889,12 @@ static cudaError_t tc_group_launch_kind(TcGroup *G, cudaStream_t st, const TcArg
     cfg.attrs = at;
     cfg.numAttrs = PAIR ? 1 : 0;
     const CUtensorMap &m = G->map0;
-    if (G->op == OP_F16) return cudaLaunchKernelEx(&cfg, k_tc_gemm<EPI_FWD, OP_F16, 3, PAIR, 1>, m, m, m, m, a);
-    if (G->nprod == 3) return cudaLaunchKernelEx(&cfg, k_tc_gemm<EPI_FWD, OP_TF32, 3, PAIR, 1>, m, m, m, m, a);
-    return cudaLaunchKernelEx(&cfg, k_tc_gemm<EPI_FWD, OP_TF32, 1, PAIR, 1>, m, m, m, m, a);
+    if (G->op == OP_F16F8)
+        return cudaLaunchKernelEx(&cfg, k_tc_gemm<EPI_FWD, OP_F16F8, 3, PAIR, 1>, m, m, m, m, m, m, a);
+    if (G->op == OP_F16) return cudaLaunchKernelEx(&cfg, k_tc_gemm<EPI_FWD, OP_F16, 3, PAIR, 1>, m, m, m, m, m, m, a);
+    if (G->nprod == 3)
+        return cudaLaunchKernelEx(&cfg, k_tc_gemm<EPI_FWD, OP_TF32, 3, PAIR, 1>, m, m, m, m, m, m, a);
+    return cudaLaunchKernelEx(&cfg, k_tc_gemm<EPI_FWD, OP_TF32, 1, PAIR, 1>, m, m, m, m, m, m, a);
 }
 
 // the grouped forward of every gated instance, on c's stream (persistent: one

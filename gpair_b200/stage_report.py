@@ -28,7 +28,10 @@ Bytes per stage are the stage's compulsory traffic, as its kernels move it:
                  previous gradient and direction read (16 B/px), data, entropy
                  and full gradient written (12 B/px)
   forward_dft / adjoint_dft  algorithmic FLOPs 4 N^2 nuv + 8 N nuv (TFLOP/s);
-                 executed = 3 x (three f16 products per algorithmic product)
+                 executed = the MMA work in f16-rate units per algorithmic
+                 product: 3 for split-f16 (three f16 products); for
+                 split-f16/E4M3 the forward is 2 (one f16 product and two E4M3
+                 products at twice the rate), the adjoint 3
 """
 from __future__ import annotations
 
@@ -50,12 +53,12 @@ def stage_bytes(p: api.Problem, splits: int, row_tiles: int) -> dict:
     }
 
 
-def report(name: str, reps: int = 10, pair: bool = False) -> dict:
+def report(name: str, reps: int = 10, pair: bool = False, precision: int = api.PREC_SPLIT16) -> dict:
     from .clocks import ClockSampler
     p = api.workload_problem(name)
     with api.Reconstructor(0) as rec:
         rec.set_problem(p)
-        rec.set_precision(api.PREC_SPLIT16)
+        rec.set_precision(precision)
         rec.set_tc_pair(pair)
         rec.set_image(p.start_image())
         rec.criterion()
@@ -76,7 +79,8 @@ def report(name: str, reps: int = 10, pair: bool = False) -> dict:
     row_tiles = (p.width + 255) // 256
     splits = _default_splits(p, pair)
     by = stage_bytes(p, splits, row_tiles)
-    out = {"workload": name, "N": p.width, "nuv": p.nuv, "npow": p.npow, "nbis": p.nbis, "splits": splits,
+    out = {"workload": name, "precision": precision, "N": p.width, "nuv": p.nuv, "npow": p.npow, "nbis": p.nbis,
+           "splits": splits,
            "hbm_peak_gbs": hbm, "tensor_peak_tflops": tf, "clocks": clocks, "cta_pairs": bool(pair),
            "timing": f"CUDA events, stages back to back, best of 5 x {reps} repetitions", "stages": {}}
     for k, ms in st.items():
@@ -86,7 +90,8 @@ def report(name: str, reps: int = 10, pair: bool = False) -> dict:
             row.update({"bytes": by[k], "gbs": gbs, "hbm_frac": gbs / hbm})
         else:
             tfl = p.dft_flops() / (ms * 1e-3) / 1e12
-            row.update({"tflops": tfl, "frac": tfl / tf, "executed_frac": 3 * tfl / tf})
+            mult = 2.0 if (precision == api.PREC_SPLIT16F8 and k == "forward_dft") else 3.0
+            row.update({"tflops": tfl, "frac": tfl / tf, "executed_frac": mult * tfl / tf})
         out["stages"][k] = row
     return out
 
@@ -127,7 +132,7 @@ def main(argv=None):
             print(json.dumps({"workload": w, "iterations": out["iterations"], "criterion_evals": out["criterion_evals"],
                               "grad_evals": out["grad_evals"], "J": out["J"]}), flush=True)
             continue
-        print(json.dumps(report(w, args.reps, bool(args.tc_pair))), flush=True)
+        print(json.dumps(report(w, args.reps, bool(args.tc_pair), args.precision)), flush=True)
 
 
 if __name__ == "__main__":

@@ -226,6 +226,9 @@ int gpair_dft_tables(int image_width, int nuv, const gpair_uv *uv, float pixella
 #define GPAIR_PREC_SPLIT16 1  /* tcgen05 f16 hi+lo split operands, 3 products, FP32 accumulate */
 #define GPAIR_PREC_TF32 2     /* tcgen05 kind::tf32, TF32 operands, 1 product, FP32 accumulate */
 #define GPAIR_PREC_TF32X3 3   /* tcgen05 kind::tf32, TF32 hi+lo split operands, 3 products, FP32 accumulate */
+#define GPAIR_PREC_SPLIT16F8 4 /* forward: f16 hi*hi (kind::f16) plus the two hi*lo cross terms as E4M3
+                                  products (kind::f8f6f4, twice the f16 rate) into the same FP32
+                                  accumulator; adjoint: as GPAIR_PREC_SPLIT16 */
 
 #define GPAIR_IMG_CURR 0
 #define GPAIR_IMG_TEMP 1

@@ -71,7 +71,7 @@ def precision_problem():
     return g.workload_problem("precision")
 
 
-@pytest.mark.parametrize("prec", [g.PREC_FP32, g.PREC_SPLIT16, g.PREC_TF32X3])
+@pytest.mark.parametrize("prec", [g.PREC_FP32, g.PREC_SPLIT16, g.PREC_TF32X3, g.PREC_SPLIT16F8])
 def test_precision_workload_256(precision_problem, prec):
     _check(precision_problem, prec)
 
@@ -85,8 +85,8 @@ def large_problem():
     return g.workload_problem("large")
 
 
-@pytest.mark.parametrize("pair", [False, True])
-def test_large_workload_1024(large_problem, pair):
+@pytest.mark.parametrize("pair,prec", [(False, g.PREC_SPLIT16), (True, g.PREC_SPLIT16), (True, g.PREC_SPLIT16F8)])
+def test_large_workload_1024(large_problem, pair, prec):
     p = large_problem
     assert (p.width, p.npow, p.nbis) == (1024, 194560, 1167360)
-    _check(p, g.PREC_SPLIT16, pair=pair)
+    _check(p, prec, pair=pair)

@@ -21,7 +21,7 @@ from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
-PRECISIONS = [g.PREC_FP32, g.PREC_SPLIT16, g.PREC_TF32X3]
+PRECISIONS = [g.PREC_FP32, g.PREC_SPLIT16, g.PREC_TF32X3, g.PREC_SPLIT16F8]
 
 
 def _s_tol(prec):
@@ -73,7 +73,7 @@ def test_criterion_and_gradient_match_fp64(rec, name, prec):
     assert _rel(rec.full_gradient(), full) <= 1e-5
 
 
-@pytest.mark.parametrize("prec", [g.PREC_SPLIT16, g.PREC_TF32X3])
+@pytest.mark.parametrize("prec", [g.PREC_SPLIT16, g.PREC_TF32X3, g.PREC_SPLIT16F8])
 @pytest.mark.parametrize("regime", ["near", "far", "mixed"])
 def test_regulariser_sum_near_and_far_from_the_prior(rec, prec, regime):
     """The tensor paths' one-pass image prep sums FP32 per-pixel Gull-Skilling
@@ -352,7 +352,7 @@ def test_tensor_kernel_wait_timeout_is_reported_and_context_recovers(rec):
     rec.set_tc_pair(True)
 
 
-@pytest.mark.parametrize("prec", [g.PREC_SPLIT16, g.PREC_TF32X3, g.PREC_TF32])
+@pytest.mark.parametrize("prec", [g.PREC_SPLIT16, g.PREC_TF32X3, g.PREC_TF32, g.PREC_SPLIT16F8])
 @pytest.mark.parametrize("name", ["tiny", "small"])
 def test_cta_pair_contractions_match_single_cta_and_fp64(name, prec):
     """The contractions on CTA pairs (tcgen05.mma.cta_group::2, 256 x 256 tiles
