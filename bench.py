@@ -401,6 +401,7 @@ def many_instances(n: int, iters: int) -> dict:
             "autotune": {"s": t_tune, "tuned": sum(not t["from_cache"] for t in tuned),
                          "fp32_path": sum(t["precision"] == g.PREC_FP32 for t in tuned),
                          "split16_path": sum(t["precision"] == g.PREC_SPLIT16 for t in tuned),
+                         "split16f8_path": sum(t["precision"] == g.PREC_SPLIT16F8 for t in tuned),
                          "tile_256": sum(t["tile_m"] == 256 for t in tuned),
                          "tile_128": sum(t["tile_m"] == 128 for t in tuned)},
             "unit": "s (host wall clock)", "line_search": "batched"}

@@ -87,7 +87,7 @@ class CgParams(C.Structure):
 LS_WOLFE, LS_BATCH, LS_TRIALS = 0, 1, 8
 BATCH_INDEPENDENT = 1  # gpair_batch_create_ex flag: independent branches, no lockstep grouping
 TUNE_PRECISION, TUNE_SPLITS, TUNE_CACHE, TUNE_BATCHED, TUNE_TILE = 1, 2, 4, 8, 16
-TUNE_MAX_CANDIDATES = 12
+TUNE_MAX_CANDIDATES = 16
 
 
 class TuneResult(C.Structure):

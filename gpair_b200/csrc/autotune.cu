@@ -4,10 +4,10 @@
 // context's stream).
 //
 // Candidates:
-//   precision  FP32 (CUDA-core contractions) and split-f16 (tcgen05); both meet
-//              the accuracy bounds, the faster one depends on the image width
-//              and the uv count (small problems leave the tensor GEMM's tiles
-//              mostly empty)
+//   precision  FP32 (CUDA-core contractions), split-f16 and split-f16/E4M3
+//              (tcgen05); all meet the accuracy bounds, the fastest depends on
+//              the image width and the uv count (small problems leave the
+//              tensor GEMM's tiles mostly empty)
 //   tile       (tensor) 256 x 256 output tiles on CTA pairs or 128 x 256 on
 //              single CTAs: pairs halve the operand traffic per MMA, single
 //              CTAs pad the uv rows less and give small problems more tiles
@@ -142,6 +142,7 @@ extern "C" int gpair_autotune(gpair_ctx *c, int flags, int reps, gpair_tune_resu
     std::vector<int> precs;
     if (flags & GPAIR_TUNE_PRECISION) {
         precs.push_back(GPAIR_PREC_SPLIT16);
+        precs.push_back(GPAIR_PREC_SPLIT16F8);
         precs.push_back(GPAIR_PREC_FP32);
     } else {
         precs.push_back(c->precision);

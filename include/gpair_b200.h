@@ -445,8 +445,8 @@ int gpair_time_batch_stages(gpair_ctx *ctx, int reps, double *stage_ms, int max_
 
 /* Autotuner: times criterion + gradient evaluations of the loaded problem (current
  * image) under candidate configurations and keeps the fastest. Candidates: the
- * precision path (GPAIR_TUNE_PRECISION: FP32 CUDA cores vs split-f16 tensor cores;
- * both meet the 1e-5 accuracy bounds), the adjoint's split-K tile length
+ * precision path (GPAIR_TUNE_PRECISION: FP32 CUDA cores, split-f16 or split-f16/E4M3
+ * tensor cores; all meet the 1e-5 accuracy bounds), the adjoint's split-K tile length
  * (GPAIR_TUNE_SPLITS: half, default and double the heuristic's K-blocks per split,
  * within the FP32-accumulation cap) and the tensor-core tile (GPAIR_TUNE_TILE:
  * 256 x 256 output tiles on CTA pairs or 128 x 256 on single CTAs, as
@@ -458,7 +458,7 @@ int gpair_time_batch_stages(gpair_ctx *ctx, int reps, double *stage_ms, int max_
 #define GPAIR_TUNE_BATCHED 8 /* objective: criterion + gradient + 2 batched 8-trial evaluations
                                 (one batched-line-search iteration) instead of criterion + gradient */
 #define GPAIR_TUNE_TILE 16
-#define GPAIR_TUNE_MAX_CANDIDATES 12
+#define GPAIR_TUNE_MAX_CANDIDATES 16
 typedef struct {
     int precision;       /* chosen precision mode */
     int adjoint_splits;  /* chosen split-K count of the adjoint contraction */
