@@ -92,6 +92,7 @@ def measure(name, prec, nsel=None, npx=24, seed=5):
 
 
 MODES = ((g.PREC_FP32, "fp32 (CUDA cores)"), (g.PREC_SPLIT16, "split16 (3 f16 products)"),
+         (g.PREC_SPLIT16F8, "split16f8 (forward: f16 hi*hi + 2 E4M3 cross products)"),
          (g.PREC_TF32, "tf32 (1 TF32 product)"), (g.PREC_TF32X3, "tf32x3 (3 TF32 products)"))
 
 
