@@ -898,10 +898,11 @@ def test_alternating_line_searches_reuse_their_graphs(rec):
     assert outs[1]["criterion_evals"] % g.LS_TRIALS == 3 % g.LS_TRIALS
 
 
-@pytest.mark.parametrize("ls,independent,pair,mixed", [(0, False, True, False), (1, True, True, False),
-                                                       (1, False, True, False), (1, False, False, False),
-                                                       (1, False, True, True)])
-def test_batch_graph_equals_separate_runs(ls, independent, pair, mixed):
+@pytest.mark.parametrize("ls,independent,pair,mixed,prec", [
+    (0, False, True, False, g.PREC_SPLIT16), (1, True, True, False, g.PREC_SPLIT16),
+    (1, False, True, False, g.PREC_SPLIT16), (1, False, False, False, g.PREC_SPLIT16),
+    (1, False, True, True, g.PREC_SPLIT16), (1, False, True, False, g.PREC_SPLIT16F8)])
+def test_batch_graph_equals_separate_runs(ls, independent, pair, mixed, prec):
     """Consistency check (library against itself; single runs are oracle-pinned by
     the CG tests above): gpair_batch_*, one graph, one launch; the results are the
     separate runs' bit for bit, twice in a row (the graph is reused). With the
@@ -917,7 +918,7 @@ def test_batch_graph_equals_separate_runs(ls, independent, pair, mixed):
         for k, (r, p) in enumerate(zip(recs, ps)):
             r.set_tc_pair(pair)
             r.set_problem(p)
-            r.set_precision(g.PREC_FP32 if (mixed and k == 1) else g.PREC_SPLIT16)
+            r.set_precision(g.PREC_FP32 if (mixed and k == 1) else prec)
         singles, imgs = [], []
         for r, p in zip(recs, ps):
             r.set_image(p.start_image())
