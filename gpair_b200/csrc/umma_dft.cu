@@ -8,10 +8,12 @@
 // weights: one scale from max |c_k|); a product is formed as
 // A_hi B_hi + A_hi B_lo + A_lo B_hi with FP32 accumulation (the lo*lo term is
 // below 2^-22 of the result). Scales are exact powers of two and are removed
-// in the epilogues.
+// in the epilogues. GPAIR_PREC_SPLIT16F8: the forward forms the two cross
+// terms as E4M3 products (kind::f8f6f4) into the same accumulator (OP_F16F8).
 //
-// Both contractions put the twiddle-side table in the M = 128 operand (TMEM
-// lanes) and the image-side operand in the N = 256 operand (TMEM columns).
+// Both contractions put the twiddle-side table in the M operand (TMEM lanes:
+// 128 rows on one CTA, 256 on a CTA pair) and the image-side operand in the
+// N = 256 operand (TMEM columns).
 // Forward DFT (kernel_visi.cl / cpu.c:449-475):
 //   T[n][y] = sum_x Fx16[n][x] I[y][x],  row n = 2k+c holds (Re, Im) Fx[k][x]
 //   epilogue: the thread of row n sums over its 256 columns against one
@@ -24,11 +26,12 @@
 //   lanes write consecutive x); split over k' into S partial images that
 //   k_grad_finalize sums in a fixed order
 //
-// One persistent CTA per SM, 192 threads: warp 0 issues TMA loads (2-stage
-// ring of 96 KB), warp 1 owns TMEM (512 columns = two 128x256 FP32
-// accumulators) and one of its threads issues tcgen05.mma; warps 2-5 drain
-// TMEM. All waits are bounded; a timeout sets an error code, the roles stop,
-// TMEM is released, and the host reports GPAIR_ERR_TIMEOUT.
+// One persistent CTA per SM (or CTA pair per two SMs), 192 threads: warp 0
+// issues TMA loads (a ring of 2 stages of 96 KB, or 3 of 64 KB per CTA of a
+// pair), warp 1 owns TMEM (512 columns = two FP32 accumulators of 256
+// columns) and one of its threads issues tcgen05.mma; warps 2-5 drain TMEM.
+// All waits are bounded; a timeout sets an error code, the roles stop, TMEM is
+// released, and the host reports GPAIR_ERR_TIMEOUT.
 #include <cuda.h>
 #include <cuda_fp16.h>
 #include <cuda_fp8.h>
