@@ -47,7 +47,8 @@ def build_parser() -> argparse.ArgumentParser:
     ap.add_argument("--iterations", type=int, default=500)
     ap.add_argument("--method", type=int, default=2, help="0 SD, 1 FR, 2 PR+, 3 HS+")
     ap.add_argument("--line-search", choices=["wolfe", "batch"], default="wolfe")
-    ap.add_argument("--precision", choices=["split16", "fp32"], default="split16")
+    ap.add_argument("--precision", choices=["split16", "split16f8", "fp32"], default="split16",
+                    help="split16: three f16 products; split16f8: E4M3 cross terms in the forward; fp32: CUDA cores")
     ap.add_argument("--regularizer", choices=["gs", "l2"], default="gs")
     ap.add_argument("--warm-start", action="store_true", help="start from the learned warm start")
     ap.add_argument("--out", default="reconst.fits")
@@ -87,7 +88,8 @@ def run(args, oi: Optional[OIFits] = None, quiet: bool = False) -> dict:
     t0 = time.perf_counter()
     with api.Reconstructor(args.device) as rec:
         rec.set_problem(p)
-        rec.set_precision({"split16": api.PREC_SPLIT16, "fp32": api.PREC_FP32}[args.precision])
+        rec.set_precision({"split16": api.PREC_SPLIT16, "split16f8": api.PREC_SPLIT16F8,
+                           "fp32": api.PREC_FP32}[args.precision])
         rec.set_regularizer({"gs": api.REG_GULL_SKILLING, "l2": api.REG_L2}[args.regularizer])
         resume = False
         if args.resume:
