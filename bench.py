@@ -441,14 +441,29 @@ def time_to_objective_workload(rec, p, iters: int, batch_iters: int, method: int
     line search) for `iters` iterations sets J*, then plain CG, the batched line
     search from the flat prior and the batched line search from the learned
     warm start (the network applied at the workload's own size; the flat-prior
-    run is the fallback) are each timed to J* (1 + 1e-4)."""
+    run is the fallback) are each timed to J* (1 + 1e-4); then the warm start
+    raced against the flat prior in a second context sharing a stop flag."""
+    import gpair_b200 as g
     from gpair_b200 import timetoobj as TT
     from gpair_b200.warmstart import WarmStartNet
     net = WarmStartNet.load() if p.width % 8 == 0 else None
-    row = TT.evaluate(rec, p, net, iters=iters, batch_iters=batch_iters, objective_from="plain", method=method)
+    flag = g.api.StopFlag() if net is not None else None
+    rec2 = g.Reconstructor(rec.device) if net is not None else None
+    try:
+        if rec2 is not None:
+            rec2.set_tc_pair(True)
+        row = TT.evaluate(rec, p, net, iters=iters, batch_iters=batch_iters, objective_from="plain", method=method,
+                          rec2=rec2, flag=flag)
+    finally:
+        if rec2 is not None:
+            rec2.close()
+        if flag is not None:
+            flag.close()
     if net is not None:
         row["speedup_warm_vs_plain"] = row["plain_s"] / max(row["warm_s"], 1e-12)
         row["speedup_warm_vs_batch"] = row["batch_s"] / max(row["warm_s"], 1e-12)
+        row["speedup_race_vs_plain"] = row["plain_s"] / max(row["race_s"], 1e-12)
+        row["speedup_race_vs_batch"] = row["batch_s"] / max(row["race_s"], 1e-12)
     row["speedup_batch_vs_plain"] = row["plain_s"] / max(row["batch_s"], 1e-12)
     row["unit"] = "s (host wall clock)"
     row["note"] = f"J* = lowest J of {iters} plain PR+ iterations with the reference's line search"

@@ -418,6 +418,7 @@ class Reconstructor:
         h = C.c_void_p()
         _check(self._L.gpair_create(C.byref(h), device))
         self.h = h
+        self.device = device
         self.problem: Optional[Problem] = None
 
     def close(self):
