@@ -171,6 +171,24 @@ def reference_sample(workload: str, oi=None, width: int = SAMPLE_WIDTH) -> dict:
                          f"{width}x{width} image")}
 
 
+def reference_problem(workload: str, oi=None) -> dict:
+    """The whole workload's arrays, built only by the reference's compiled code
+    (getoifits.c indices, gpair.c init_data packing, cpu.c set_model prior), at
+    the workload's own image size."""
+    from oracle import oracle as O
+    synth, _ = data_modules()
+    w = synth.workload(workload)
+    if oi is None:
+        _, oi = synth.make_workload_data(workload)
+    ix = O.ref_index(oi)
+    data, err, ph, _ = O.ref_init_data(ix["npow"], ix["nbis"], ix["pow"], ix["powerr"], ix["bisamp"],
+                                       ix["bisamperr"], ix["bisphs"], ix["bisphserr"], ix["uvpnt"], 1)
+    model = O.ref_set_model(w.image_width, w.pixellation_mas, 0, 0.0, 1.0)
+    return {"width": w.image_width, "pixellation": w.pixellation_mas, "uv": ix["uv"], "npow": ix["npow"],
+            "nbis": ix["nbis"], "data": data, "data_err": err, "phasor": ph, "uvpnt": ix["uvpnt"],
+            "sign": ix["sign"], "model": model, "alpha": w.alpha}
+
+
 class _SampleProblem:
     def __init__(self, s):
         self.__dict__.update(s)
@@ -333,10 +351,12 @@ def many_instances(n: int, iters: int) -> dict:
     """n independent reconstructions of uneven size (widths 64-256, 500-8,000 uv)
     for `iters` batched-line-search CG iterations each: one after another, all
     at once through gpair_cg_run_many (each context's graph on its own stream),
-    and as one graph launch (gpair_batch_run), both as a lockstep batch whose
-    batched evaluations run one grouped tcgen05 forward over all instances and
-    with every CG loop an independent branch of the graph. Host wall clock;
-    problem loading and graph capture are outside the timings."""
+    and as one graph launch (gpair_batch_run) in three layouts: the staged lockstep
+    batch (every stage of an iteration one launch over all instances, every
+    contraction one grouped tcgen05 launch per class), the lockstep batch with
+    grouped trial forwards only, and every CG loop an independent branch of the
+    graph. Host wall clock; problem loading and graph capture are outside the
+    timings."""
     import gpair_b200 as g
     from gpair_b200.instances import instances
     ps = instances(n)
@@ -369,10 +389,11 @@ def many_instances(n: int, iters: int) -> dict:
         res = g.cg_many(recs, iters, line_search=g.LS_BATCH)
         t_con = time.perf_counter() - t0
         flops_con = sum(r.last_run_stats()[1] for r in recs)
-        # one graph launch: lockstep with grouped forwards, then independent branches
+        # one graph launch: staged lockstep, lockstep with grouped forwards only, independent branches
         one = {}
-        for mode in ("grouped", "independent"):
-            with g.api.Batch(recs, line_search=g.LS_BATCH, independent=(mode == "independent")) as b:
+        for mode in ("staged", "forwards_only", "independent"):
+            with g.api.Batch(recs, line_search=g.LS_BATCH, independent=(mode == "independent"),
+                             forwards_only=(mode == "forwards_only")) as b:
                 for r, p in zip(recs, ps):
                     r.set_image(p.start_image())
                 b.run(1)  # first launch
@@ -383,7 +404,7 @@ def many_instances(n: int, iters: int) -> dict:
                 dt = time.perf_counter() - t0
                 one[mode] = {"s": dt, "grouped": b.grouped, "all_ok": all(r_["status"] == 0 for r_ in res_b),
                              "tflops": sum(r.last_run_stats()[1] for r in recs) / max(dt, 1e-12) / 1e12}
-        t_one = one["grouped"]["s"]
+        t_one = one["staged"]["s"]
     finally:
         for r in recs:
             r.close()
@@ -394,7 +415,9 @@ def many_instances(n: int, iters: int) -> dict:
             "instances_per_s": n / max(t_con, 1e-12), "tflops_concurrent": flops_con / max(t_con, 1e-12) / 1e12,
             "tflops_sequential": flops / max(t_seq, 1e-12) / 1e12,
             "one_launch_s": t_one, "one_launch_speedup": t_seq / max(t_one, 1e-12),
-            "tflops_one_launch": one["grouped"]["tflops"], "one_launch_grouped": one["grouped"]["grouped"],
+            "tflops_one_launch": one["staged"]["tflops"], "one_launch_grouped": one["staged"]["grouped"],
+            "one_launch_forwards_only_s": one["forwards_only"]["s"],
+            "tflops_one_launch_forwards_only": one["forwards_only"]["tflops"],
             "one_launch_independent_s": one["independent"]["s"],
             "tflops_one_launch_independent": one["independent"]["tflops"],
             "all_ok": all(r_["status"] == 0 for r_ in res) and all(v["all_ok"] for v in one.values()),
@@ -405,6 +428,61 @@ def many_instances(n: int, iters: int) -> dict:
                          "tile_256": sum(t["tile_m"] == 256 for t in tuned),
                          "tile_128": sum(t["tile_m"] == 128 for t in tuned)},
             "unit": "s (host wall clock)", "line_search": "batched"}
+
+
+def small_plain_cg_cpu(iters: int) -> dict:
+    """The reference's side of small_plain_cg: `iters` PR+ CG iterations with the
+    reference's line search on one host core through the reference's own compiled
+    cpu.c (float; the CG control flow of gpair1/trunk/gpair.c:682-915 restated in
+    the oracle; data built by the reference's getoifits.c, init_data and
+    set_model). Runs in a worker thread beside the GPU blocks: the foreign calls
+    release the GIL."""
+    import numpy as np
+    from oracle import oracle as O
+    synth, _ = data_modules()
+    _, oi = synth.make_workload_data("small")
+    ref = _SampleProblem(reference_problem("small", oi))
+    ev = O.RefEvaluator(ref)
+    t0 = time.perf_counter()
+    _, tr = ev.cg(np.maximum(ref.model, np.float32(1e-8)).astype(np.float32), iters, method=2)
+    dt = time.perf_counter() - t0
+    return {"s": dt, "cores": 1, "kind": "reference", "J": float(tr["J"][-1]),
+            "criterion_evals": tr["criterion_evals"], "grad_evals": tr["grad_evals"],
+            "note": "the reference's cpu.c criterion and gradients in float, one core"}
+
+
+def small_plain_cg(iters: int, device: int, precisions, cpu=None) -> dict:
+    """The plain method on the small workload (64x64, 0.1 mas/pixel, 900 V2, 600
+    closure phases, MEM against a flat prior, alpha 1e-3): `iters` PR+ CG
+    iterations with the reference's line search from the flat start on the GPU
+    (one CUDA graph per run; device time and host wall clock, per precision
+    path), beside `cpu` (small_plain_cg_cpu) when given."""
+    import gpair_b200 as g
+    p = g.workload_problem("small")
+    img0 = p.start_image()
+    names = {v: k for k, v in PRECISION_MODES.items()}
+    out = {"workload": _describe("small", p), "iterations": iters, "method": "PR+, reference line search"}
+    for prec in precisions:
+        with g.Reconstructor(device) as r:
+            r.set_problem(p)
+            r.set_precision(prec)
+            r.set_image(img0)
+            r.cg(1, method=2)  # graph capture outside the timing
+            r.set_image(img0)
+            t0 = time.perf_counter()
+            o = r.cg(iters, method=2)
+            dt = time.perf_counter() - t0
+            ms = r.last_run_stats()[0]
+            out["gpu_" + names[prec]] = {"s": dt, "device_ms": ms, "J": o["J"], "criterion_evals": o["criterion_evals"],
+                                         "grad_evals": o["grad_evals"]}
+    if cpu is not None:
+        out["cpu_reference"] = cpu
+        for k, v in list(out.items()):
+            if k.startswith("gpu_"):
+                v["speedup_vs_cpu_reference"] = cpu["s"] / max(v["s"], 1e-12)
+                v["rel_J_vs_cpu_reference"] = abs(v["J"] - cpu["J"]) / abs(cpu["J"])
+    out["unit"] = "s (host wall clock of the whole run)"
+    return out
 
 
 def time_to_objective(n_problems: int, race_fr: bool = False, method: int = 2) -> dict:
@@ -704,6 +782,15 @@ def run_ours(args, rank, world, local):
     del oi, p
 
     if rank == 0:
+        # the reference's cpu.c on the small workload, in a worker thread beside the GPU blocks
+        cpu_pool = cpu_small = None
+        if args.small_iters > 0 and not args.no_cpu_baseline:
+            import concurrent.futures
+            cpu_pool = concurrent.futures.ThreadPoolExecutor(1)
+            sys.stdout.flush()
+            saved_fd, devnull_fd = os.dup(1), os.open(os.devnull, os.O_WRONLY)
+            os.dup2(devnull_fd, 1)  # cpu.c's image2vis prints on every call
+            cpu_small = cpu_pool.submit(small_plain_cg_cpu, args.small_iters)
         # the 256x256 precision workload beside the headline (context, same step)
         if args.workload != "precision" and not args.no_precision_256:
             p2 = g.workload_problem("precision", **seeds)
@@ -730,6 +817,17 @@ def run_ours(args, rank, world, local):
                                                           method=args.tto_method)
         if args.instances > 0:
             line["many_instances"] = many_instances(args.instances, args.instance_iters)
+        if args.small_iters > 0:
+            cpu = None
+            if cpu_small is not None:
+                try:
+                    cpu = cpu_small.result()
+                finally:
+                    cpu_pool.shutdown()
+                    os.dup2(saved_fd, 1)
+                    os.close(saved_fd)
+                    os.close(devnull_fd)
+            line["small_plain_cg"] = small_plain_cg(args.small_iters, local, (g.PREC_FP32, prec), cpu)
         print(json.dumps(line), flush=True)
     if dist:
         torch.distributed.destroy_process_group()
@@ -754,6 +852,8 @@ def main():
     ap.add_argument("--no-precision-256", action="store_true", help="skip the 256x256 context block")
     ap.add_argument("--instances", type=int, default=64, help="independent reconstructions run at once (0: skip)")
     ap.add_argument("--instance-iters", type=int, default=30)
+    ap.add_argument("--small-iters", type=int, default=200,
+                    help="plain CG iterations of the 64x64 workload on the GPU and the reference's cpu.c (0: skip)")
     ap.add_argument("--line-search", choices=["wolfe", "batch"], default="wolfe",
                     help="line search of the headline steps: the reference's (default) or the batched one")
     ap.add_argument("--tto-problems", type=int, default=16,

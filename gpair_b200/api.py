@@ -86,6 +86,7 @@ class CgParams(C.Structure):
 
 LS_WOLFE, LS_BATCH, LS_TRIALS = 0, 1, 8
 BATCH_INDEPENDENT = 1  # gpair_batch_create_ex flag: independent branches, no lockstep grouping
+BATCH_FORWARDS_ONLY = 2  # gpair_batch_create_ex flag: lockstep with grouped trial forwards only
 TUNE_PRECISION, TUNE_SPLITS, TUNE_CACHE, TUNE_BATCHED, TUNE_TILE = 1, 2, 4, 8, 16
 TUNE_MAX_CANDIDATES = 16
 
@@ -666,22 +667,24 @@ def cg_many(recs, iterations: int, method: int = 2, alpha: Optional[float] = Non
 
 class Batch:
     """Many reconstructions in one CUDA graph launch (gpair_batch_*). With the
-    batched line search and every context on a tensor-core path the instances run
-    in lockstep and each batched evaluation's forwards are one grouped tcgen05
-    launch (`grouped` is True); otherwise (or with independent=True) every
-    context's whole CG loop is an independent branch of the graph. Build after the
-    contexts hold their problems, images and configuration."""
+    batched line search and the contexts on tensor-core paths the instances run in
+    lockstep: `grouped` is 2 when every stage of an iteration is one launch over all
+    instances and every contraction one grouped tcgen05 launch per class (staged),
+    1 when only the trial forwards are grouped (forwards_only=True, or instances
+    that cannot all be staged), 0 when every context's whole CG loop is an
+    independent branch of the graph (independent=True, or no tensor-core context).
+    Build after the contexts hold their problems, images and configuration."""
 
-    def __init__(self, recs, line_search: int = LS_BATCH, independent: bool = False):
+    def __init__(self, recs, line_search: int = LS_BATCH, independent: bool = False, forwards_only: bool = False):
         self._L = lib()
         self.recs = list(recs)
         self.line_search = line_search
         h = C.c_void_p()
         arr = (C.c_void_p * len(self.recs))(*[r.h.value for r in self.recs])
-        flags = BATCH_INDEPENDENT if independent else 0
+        flags = (BATCH_INDEPENDENT if independent else 0) | (BATCH_FORWARDS_ONLY if forwards_only else 0)
         _check(self._L.gpair_batch_create_ex(C.byref(h), arr, len(self.recs), line_search, flags), self.recs[0].h)
         self.h = h
-        self.grouped = bool(self._L.gpair_batch_grouped(self.h))
+        self.grouped = int(self._L.gpair_batch_grouped(self.h))
 
     def run(self, iterations: int, method: int = 2, alpha: Optional[float] = None, resume: bool = False, **kw):
         prm = CgParams()

@@ -252,6 +252,12 @@ struct BatchGraph {
     int *flags;                       // device: act[n], ls[n], lockstep order
     cudaGraphConditionalHandle *hd;   // device: h_pre[n], h_post[n], lockstep order
     DevScalars **scs;                 // device: every instance's scalars, lockstep order
+    // staged lockstep: every stage grouped (per class: the image forward and the adjoint)
+    int staged;
+    void **grps_img, **grps_adj;
+    void *stg_args[GS_COUNT];  // device: argument structs of every instance, lockstep order
+    int *stg_start[GS_COUNT];  // device: block starts [n + 1]
+    int stg_total[GS_COUNT];
 };
 
 void gp_batch_graph_free(void *bg)
@@ -265,8 +271,18 @@ void gp_batch_graph_free(void *bg)
             if (B->loops[i].trace) cudaFree(B->loops[i].trace);
         free(B->loops);
     }
-    for (int k = 0; k < B->ngrp; k++) gp_tc_group_free(B->grps[k]);
+    for (int k = 0; k < B->ngrp; k++) {
+        gp_tc_group_free(B->grps[k]);
+        if (B->grps_img) gp_tc_group_free(B->grps_img[k]);
+        if (B->grps_adj) gp_tc_group_free(B->grps_adj[k]);
+    }
     free(B->grps);
+    free(B->grps_img);
+    free(B->grps_adj);
+    for (int s = 0; s < GS_COUNT; s++) {
+        if (B->stg_args[s]) cudaFree(B->stg_args[s]);
+        if (B->stg_start[s]) cudaFree(B->stg_start[s]);
+    }
     if (B->gerr) cudaFree(B->gerr);
     if (B->flags) cudaFree(B->flags);
     if (B->hd) cudaFree(B->hd);
@@ -299,7 +315,9 @@ void gp_batch_graph_free(void *bg)
 // Each instance runs the kernels of its own graph with the same arguments
 // (its controllers steer nothing; the routers read their decisions), so its
 // results are bitwise those of a separate run.
-enum { GR_INIT = 0, GR_BEGIN = 1, GR_LS0 = 2, GR_LSN = 3, GR_END = 4 };
+// GR_LS0S: LS0 of a staged batch, whose criterion and gradient contractions are
+// grouped too: a wait failure of those stops every active instance
+enum { GR_INIT = 0, GR_BEGIN = 1, GR_LS0 = 2, GR_LSN = 3, GR_END = 4, GR_LS0S = 5 };
 
 __global__ void k_lockstep_route(int what, DevScalars *const *__restrict__ scs, int n, int *__restrict__ act,
                                  int *__restrict__ ls, const cudaGraphConditionalHandle *__restrict__ h_pre,
@@ -323,6 +341,11 @@ __global__ void k_lockstep_route(int what, DevScalars *const *__restrict__ scs, 
             break;
         case GR_LS0:
             v = act[i] && sc->cg.action != CG_DONE;
+            ls[i] = v;
+            break;
+        case GR_LS0S:
+            if (act[i] && *gerr) sc->tc_err |= *gerr;
+            v = act[i] && sc->cg.action != CG_DONE && !sc->tc_err;
             ls[i] = v;
             break;
         case GR_LSN:
@@ -568,6 +591,212 @@ static int build_lockstep(gpair_ctx **ctx_in, int n, BatchGraph *B)
     return lockstep_route(B, c0, GR_LSN, h_ls, B2, last.data(), last.size(), &n_lsn);
 }
 
+// --------------------------------- staged lockstep batches (every stage grouped)
+//
+// With every instance on the tensor path (one operand element type, (u, v)
+// given), every stage of an iteration is ONE launch over all instances
+// (group.cuh), and every contraction one grouped tcgen05 launch per class:
+//
+//   [route INIT]   act[i] = 1
+//   WHILE (h_any_iter)
+//     prep | forward (per class) | V2/T3/chi2 | c_k | W | adjoint (per class)
+//       | gradient, CTRL_BEGIN | direction, CTRL_AFTER_DIR           (gate act[i])
+//     [route LS0S]   ls[i] = act[i] and the line search of i goes on; h_any_ls
+//     WHILE (h_any_ls)
+//       trial prep | trial forward (per class) | trial chi2, CTRL_AFTER_BATCH   (gate ls[i])
+//       [route LSN]
+//     image update | CTRL_END                                          (gate act[i])
+//     [route END]    act[i] = act[i] and the run of i goes on; h_any_iter
+//
+// An instance's part of every launch has the arguments and the block grid of
+// its own single launch, so its results are bitwise those of a separate run.
+
+// argument structs and block starts of one stage over the instances ctx[0..n-1]
+static int stage_table(BatchGraph *B, gpair_ctx **ctx, int n, int stage, double *const *trace, int *op_out)
+{
+    const bool tc = stage == GS_PREP_IMAGE || stage == GS_PREP_TRIALS || stage == GS_BUILD_W;
+    const size_t sz = tc ? gp_tc_stage_args_size(stage) : gp_stage_args_size(stage);
+    std::vector<unsigned char> h(sz * (size_t)n);
+    std::vector<int> start((size_t)n + 1, 0);
+    int op0 = -1;
+    for (int k = 0; k < n; k++) {
+        int nb = 0, op = -1, rc;
+        if (tc) {
+            rc = gp_tc_stage_args(ctx[k], stage, h.data() + sz * k, &nb, &op);
+            if (!rc && op0 >= 0 && op != op0) rc = GPAIR_ERR_STATE;  // one operand element type per launch
+            op0 = op;
+        } else {
+            rc = gp_stage_args(ctx[k], stage, trace[k], h.data() + sz * k, &nb);
+        }
+        if (rc) return rc;
+        if (nb < 1 || (long long)start[k] + nb > (1LL << 30)) return GPAIR_ERR_STATE;
+        start[k + 1] = start[k] + nb;
+    }
+    gpair_ctx *c0 = ctx[0];
+    GP_CUDA(c0, cudaMalloc(&B->stg_args[stage], sz * (size_t)n));
+    GP_CUDA(c0, cudaMemcpy(B->stg_args[stage], h.data(), sz * (size_t)n, cudaMemcpyHostToDevice));
+    GP_CUDA(c0, cudaMalloc(&B->stg_start[stage], sizeof(int) * ((size_t)n + 1)));
+    GP_CUDA(c0, cudaMemcpy(B->stg_start[stage], start.data(), sizeof(int) * ((size_t)n + 1), cudaMemcpyHostToDevice));
+    B->stg_total[stage] = start[(size_t)n];
+    if (op_out) *op_out = op0;
+    return GPAIR_OK;
+}
+
+// GPAIR_ERR_STATE: the instances cannot run fully staged (the caller builds the
+// lockstep with grouped trial forwards only, or independent branches)
+static int build_lockstep_staged(gpair_ctx **ctx_in, int n, BatchGraph *B)
+{
+    if (n > 4096) return GPAIR_ERR_STATE;
+    std::vector<int> key((size_t)n), order((size_t)n);
+    for (int i = 0; i < n; i++) {
+        key[i] = gp_tc_group_key(ctx_in[i]);
+        if (key[i] < 0 || !ctx_in[i]->have_uv) return GPAIR_ERR_STATE;
+        order[i] = i;
+    }
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return key[a] < key[b]; });
+    std::vector<gpair_ctx *> ctx((size_t)n);
+    for (int k = 0; k < n; k++) ctx[k] = ctx_in[order[k]];
+    gpair_ctx *c0 = ctx[0];
+    // classes of the contractions, at most 256 instances per grouped launch
+    std::vector<int> cls_begin;
+    for (int k = 0; k < n; k++)
+        if (cls_begin.empty() || key[order[k]] != key[order[k - 1]] || k - cls_begin.back() == 256)
+            cls_begin.push_back(k);
+    cls_begin.push_back(n);
+    const int ngrp = (int)cls_begin.size() - 1;
+    // every instance's tensor state and batch buffers (no allocation inside a capture)
+    for (int k = 0; k < n; k++) {
+        int rc = gp_batch_alloc(ctx[k]);
+        if (!rc) rc = gp_tc_stage_sizes(ctx[k], &ctx[k]->mt, &ctx[k]->splits);
+        if (rc) return rc == GPAIR_ERR_STATE ? GPAIR_ERR_CUDA : rc;
+    }
+    // the prep and W stages need one operand element type for all instances
+    int op_prep = -1;
+    {
+        std::vector<unsigned char> tmp(gp_tc_stage_args_size(GS_PREP_IMAGE));
+        for (int k = 0; k < n; k++) {
+            int nb = 0, op = -1;
+            int rc = gp_tc_stage_args(ctx[k], GS_PREP_IMAGE, tmp.data(), &nb, &op);
+            if (rc) return rc == GPAIR_ERR_STATE ? GPAIR_ERR_CUDA : rc;
+            if (op_prep >= 0 && op != op_prep) return GPAIR_ERR_STATE;
+            op_prep = op;
+        }
+    }
+    GP_CUDA(c0, cudaMalloc(&B->flags, sizeof(int) * 2 * (size_t)n));
+    GP_CUDA(c0, cudaMemset(B->flags, 0, sizeof(int) * 2 * (size_t)n));
+    GP_CUDA(c0, cudaMalloc(&B->gerr, sizeof(unsigned int)));
+    GP_CUDA(c0, cudaMemset(B->gerr, 0, sizeof(unsigned int)));
+    const int *act = B->flags, *lsg = B->flags + n;
+    B->ngrp = ngrp;
+    B->grps = (void **)calloc((size_t)ngrp, sizeof(void *));
+    B->grps_img = (void **)calloc((size_t)ngrp, sizeof(void *));
+    B->grps_adj = (void **)calloc((size_t)ngrp, sizeof(void *));
+    if (!B->grps || !B->grps_img || !B->grps_adj) return GPAIR_ERR_ALLOC;
+    int rc = GPAIR_OK;
+    for (int q = 0; q < ngrp && !rc; q++) {
+        const int k0 = cls_begin[q], k1 = cls_begin[q + 1];
+        rc = gp_tc_group_build_kind(&ctx[k0], k1 - k0, GP_TCG_TRIALS, lsg + k0, B->gerr, &B->grps[q]);
+        if (!rc) rc = gp_tc_group_build_kind(&ctx[k0], k1 - k0, GP_TCG_IMAGE, act + k0, B->gerr, &B->grps_img[q]);
+        if (!rc) rc = gp_tc_group_build_kind(&ctx[k0], k1 - k0, GP_TCG_ADJOINT, act + k0, B->gerr, &B->grps_adj[q]);
+    }
+    if (rc) return rc == GPAIR_ERR_STATE ? GPAIR_ERR_CUDA : rc;  // the instances were eligible
+    std::vector<double *> trace((size_t)n);
+    for (int k = 0; k < n; k++) trace[k] = B->loops[order[k]].trace;
+    int op = -1;
+    for (int st = 0; st < GS_COUNT && !rc; st++) rc = stage_table(B, ctx.data(), n, st, trace.data(), &op);
+    if (rc) return rc == GPAIR_ERR_STATE ? GPAIR_ERR_CUDA : rc;
+    GP_CUDA(c0, cudaMalloc(&B->scs, sizeof(DevScalars *) * (size_t)n));
+    std::vector<DevScalars *> hs((size_t)n);
+    for (int k = 0; k < n; k++) hs[k] = ctx[k]->sc;
+    GP_CUDA(c0, cudaMemcpy(B->scs, hs.data(), sizeof(DevScalars *) * (size_t)n, cudaMemcpyHostToDevice));
+
+    auto stage = [&](int st, const int *gate) {
+        const bool tc = st == GS_PREP_IMAGE || st == GS_PREP_TRIALS || st == GS_BUILD_W;
+        return tc ? gp_tc_stage_group_launch(c0, st, op_prep, B->stg_args[st], B->stg_start[st], n, B->stg_total[st],
+                                             gate)
+                  : gp_stage_group_launch(c0, st, B->stg_args[st], B->stg_start[st], n, B->stg_total[st], gate);
+    };
+    // grouped contractions: each class on c0's stream, with the wait budget of its first instance
+    auto gemms = [&](void **grps) {
+        for (int q = 0; q < ngrp; q++) {
+            int r = gp_tc_group_run(grps[q], ctx[cls_begin[q]], c0->stream);
+            if (r) return r;
+        }
+        return GPAIR_OK;
+    };
+    auto route = [&](int what, cudaGraphConditionalHandle h) {
+        k_lockstep_route<<<1, 256, 0, c0->stream>>>(what, B->scs, n, B->flags, B->flags + n, nullptr, nullptr, h,
+                                                     B->gerr);
+        GP_LAUNCH_CHECK(c0);
+        return GPAIR_OK;
+    };
+
+    cudaGraphConditionalHandle h_iter, h_ls;
+    GP_CUDA(c0, cudaGraphConditionalHandleCreate(&h_iter, B->g, 1, cudaGraphCondAssignDefault));
+    cudaGraph_t g_init = nullptr, B1, B2;
+    if ((rc = capture_fn(c0, [&]() { return route(GR_INIT, h_iter); }, &g_init, nullptr))) return rc;
+    cudaGraphNode_t n_init, n_loop, n_pre, n_lsw, n_post, n_ls;
+    if ((rc = add_child(c0, B->g, g_init, nullptr, 0, &n_init))) return rc;
+    n_loop = add_conditional(c0, B->g, h_iter, cudaGraphCondTypeWhile, &B1, &rc);
+    if (rc) return rc;
+    GP_CUDA(c0, cudaGraphAddDependencies(B->g, &n_init, &n_loop, 1));
+    GP_CUDA(c0, cudaGraphConditionalHandleCreate(&h_ls, B1, 0, 0));
+
+    // B1: pre-phase + LS0S, WHILE (h_ls), post-phase + END
+    int npre = 0, nls = 0, npost = 0;
+    cudaGraph_t g_pre = nullptr, g_post = nullptr, g_ls = nullptr;
+    rc = capture_fn(
+        c0,
+        [&]() {
+            int r;
+            if ((r = stage(GS_PREP_IMAGE, act))) return r;
+            if ((r = gemms(B->grps_img))) return r;
+            if ((r = stage(GS_VIS_DATA, act))) return r;
+            if ((r = stage(GS_ADJ_WEIGHTS, act))) return r;
+            if ((r = stage(GS_BUILD_W, act))) return r;
+            if ((r = gemms(B->grps_adj))) return r;
+            if ((r = stage(GS_GRAD_FINALIZE, act))) return r;
+            if ((r = stage(GS_DESCENT, act))) return r;
+            return route(GR_LS0S, h_ls);
+        },
+        &g_pre, &npre);
+    if (rc || (rc = add_child(c0, B1, g_pre, nullptr, 0, &n_pre))) return rc;
+    n_lsw = add_conditional(c0, B1, h_ls, cudaGraphCondTypeWhile, &B2, &rc);
+    if (rc) return rc;
+    GP_CUDA(c0, cudaGraphAddDependencies(B1, &n_pre, &n_lsw, 1));
+    rc = capture_fn(
+        c0,
+        [&]() {
+            int r;
+            if ((r = stage(GS_UPDATE, act))) return r;
+            if ((r = stage(GS_CTRL_END, act))) return r;
+            return route(GR_END, h_iter);
+        },
+        &g_post, &npost);
+    if (rc || (rc = add_child(c0, B1, g_post, &n_lsw, 1, &n_post))) return rc;
+    // B2: one batched evaluation of every searching instance
+    rc = capture_fn(
+        c0,
+        [&]() {
+            int r;
+            if ((r = stage(GS_PREP_TRIALS, lsg))) return r;
+            if ((r = gemms(B->grps))) return r;
+            if ((r = stage(GS_CHI2_BATCH, lsg))) return r;
+            return route(GR_LSN, h_ls);
+        },
+        &g_ls, &nls);
+    if (rc || (rc = add_child(c0, B2, g_ls, nullptr, 0, &n_ls))) return rc;
+    // launches an instance takes part in (shared with the other instances)
+    for (int i = 0; i < n; i++) {
+        B->loops[i].n_pre = npre;
+        B->loops[i].n_post = npost;
+        B->loops[i].n_crit = nls;
+        B->loops[i].n_grad = 0;
+    }
+    B->staged = 1;
+    return GPAIR_OK;
+}
+
 int gp_batch_graph_build(gpair_ctx **ctx, int n, int ls_mode, int allow_group, void **out)
 {
     *out = nullptr;
@@ -587,7 +816,17 @@ int gp_batch_graph_build(gpair_ctx **ctx, int n, int ls_mode, int allow_group, v
         G->trace_cap = 1;  // one row; batch runs return no trace
         if (cudaMalloc(&G->trace, sizeof(double) * 5) != cudaSuccess) rc = GPAIR_ERR_ALLOC;
     }
-    if (!rc && allow_group && ls_mode == GPAIR_LS_BATCH) {
+    if (!rc && allow_group >= 2 && ls_mode == GPAIR_LS_BATCH) {
+        rc = build_lockstep_staged(ctx, n, B);
+        if (rc == GPAIR_OK) {
+            B->grouped = 2;
+        } else if (rc == GPAIR_ERR_STATE) {
+            // not every instance can take part in every grouped stage (nothing was
+            // built yet): the lockstep with grouped forwards only
+            rc = GPAIR_OK;
+        }
+    }
+    if (!rc && !B->grouped && allow_group && ls_mode == GPAIR_LS_BATCH) {
         rc = build_lockstep(ctx, n, B);
         if (rc == GPAIR_OK) {
             B->grouped = 1;

@@ -908,7 +908,7 @@ extern "C" int gpair_batch_grouped(const gpair_batch *b) { return b ? gp_batch_g
 extern "C" int gpair_batch_create_ex(gpair_batch **out, gpair_ctx **ctx, int n, int line_search, int flags)
 {
     if (!out || !ctx || n <= 0) return GPAIR_ERR_INVALID;
-    if (flags & ~GPAIR_BATCH_INDEPENDENT) return GPAIR_ERR_INVALID;
+    if (flags & ~(GPAIR_BATCH_INDEPENDENT | GPAIR_BATCH_FORWARDS_ONLY)) return GPAIR_ERR_INVALID;
     if (line_search != GPAIR_LS_WOLFE && line_search != GPAIR_LS_BATCH) return GPAIR_ERR_INVALID;
     *out = nullptr;
     for (int i = 0; i < n; i++) {
@@ -940,7 +940,9 @@ extern "C" int gpair_batch_create_ex(gpair_batch **out, gpair_ctx **ctx, int n, 
         ctx[i]->fuse_ctrl = -1;
         ctx[i]->fuse_handles = 0;
     }
-    if (!rc) rc = gp_batch_graph_build(ctx, n, line_search, !(flags & GPAIR_BATCH_INDEPENDENT), &b->graph);
+    // 2: every stage grouped where the instances allow it, 1: grouped forwards only, 0: independent
+    const int group = (flags & GPAIR_BATCH_INDEPENDENT) ? 0 : (flags & GPAIR_BATCH_FORWARDS_ONLY) ? 1 : 2;
+    if (!rc) rc = gp_batch_graph_build(ctx, n, line_search, group, &b->graph);
     if (rc) {
         gpair_batch_destroy(b);
         return rc;

@@ -389,11 +389,48 @@ int gp_tc_forward(gpair_ctx *c, int which);
 int gp_tc_forward_gemm(gpair_ctx *c);
 int gp_tc_split(gpair_ctx *c, int which);
 int gp_tc_prep_image(gpair_ctx *c, int which);
-// grouped forward over the batched trials of several instances (lockstep batches)
+// grouped contractions over several instances (lockstep batches): the forward of
+// the batched trials (GP_TCG_TRIALS), the forward of the current image
+// (GP_TCG_IMAGE) or the adjoint into split-K partial images (GP_TCG_ADJOINT)
+enum { GP_TCG_TRIALS = 0, GP_TCG_IMAGE = 1, GP_TCG_ADJOINT = 2 };
 int gp_tc_group_key(gpair_ctx *c);
 int gp_tc_group_build(gpair_ctx **ctx, int n, const int *gate, unsigned int *err, void **out);
+int gp_tc_group_build_kind(gpair_ctx **ctx, int n, int kind, const int *gate, unsigned int *err, void **out);
 int gp_tc_group_forward(void *grp, gpair_ctx *c);
+int gp_tc_group_run(void *grp, gpair_ctx *c, cudaStream_t st);
 void gp_tc_group_free(void *grp);
+// forward row tiles and adjoint split count of a context's tensor state (what
+// its forward and adjoint launches would set in c->mt and c->splits)
+int gp_tc_stage_sizes(gpair_ctx *c, int *mt, int *splits);
+
+// Grouped stage kernels (group.cuh): the argument struct of one instance for
+// stage GS_* (host memory, gp_stage_args_size bytes) and its virtual grid's
+// block count; one launch over n instances whose argument structs are at
+// d_args (device) with block starts d_start[0..n], gated by gate[i].
+// GS_CTRL_END writes its trace row to `trace` (capacity 1).
+enum {
+    GS_PREP_IMAGE = 0,   // current image: flux, regulariser, max, forward operand (umma_dft.cu)
+    GS_VIS_DATA = 1,     // V, V2/T3, chi2, adjoint weights (no controller)
+    GS_ADJ_WEIGHTS = 2,  // c_k and C
+    GS_BUILD_W = 3,      // adjoint weight operand (umma_dft.cu)
+    GS_GRAD_FINALIZE = 4,  // gradient of the current image, then CTRL_BEGIN
+    GS_DESCENT = 5,      // CG direction, then CTRL_AFTER_DIR
+    GS_PREP_TRIALS = 6,  // batched trial images and their operands (umma_dft.cu)
+    GS_CHI2_BATCH = 7,   // chi2 of every trial, then CTRL_AFTER_BATCH
+    GS_UPDATE = 8,       // image update with the accepted step, gradient backup
+    GS_CTRL_END = 9,     // end of the iteration (trace row)
+    GS_COUNT = 10
+};
+size_t gp_stage_args_size(int stage);
+int gp_stage_args(gpair_ctx *c, int stage, double *trace, void *out, int *nblocks);
+int gp_stage_group_launch(gpair_ctx *c, int stage, const void *d_args, const int *d_start, int n, int total,
+                          const int *gate);
+// the umma_dft.cu stages (GS_PREP_IMAGE, GS_PREP_TRIALS, GS_BUILD_W); `op` is the
+// operand kind of every instance in the launch
+size_t gp_tc_stage_args_size(int stage);
+int gp_tc_stage_args(gpair_ctx *c, int stage, void *out, int *nblocks, int *op);
+int gp_tc_stage_group_launch(gpair_ctx *c, int stage, int op, const void *d_args, const int *d_start, int n,
+                             int total, const int *gate);
 int gp_tc_build_w(gpair_ctx *c);
 int gp_tc_adjoint_gemm(gpair_ctx *c);
 int gp_tc_prep_split_trial(gpair_ctx *c);

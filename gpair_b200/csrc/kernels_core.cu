@@ -33,6 +33,7 @@
 
 #define RPMAS_D ((3.14159265358979323 / 180.0) / 3600000.0)
 
+#include "group.cuh"
 #include "reduce.cuh"
 #include "umma.cuh"
 
@@ -304,24 +305,46 @@ __device__ __forceinline__ double2 sum_vpart(const float2 *__restrict__ vpart, i
     return make_double2(re * invF, im * invF);
 }
 
-__global__ void __launch_bounds__(GP_THREADS) k_vis_data(const float2 *__restrict__ vpart, int mt, int nuv,
-                                                         int npow, int nbis, const float *__restrict__ data,
-                                                         const float *__restrict__ data_err,
-                                                         const int4 *__restrict__ tri,
-                                                         const float2 *__restrict__ phasor, int nblk_uv,
-                                                         double2 *__restrict__ visd, float2 *__restrict__ visi,
-                                                         float *__restrict__ mock, float2 *__restrict__ cw,
-                                                         float2 *__restrict__ trib, double *__restrict__ partials,
-                                                         DevScalars *__restrict__ sc, FusedCtrl fc,
-                                                         int direct)
+struct VisDataArgs {
+    const float2 *vpart;
+    int mt, nuv, npow, nbis;
+    const float *data, *data_err;
+    const int4 *tri;
+    const float2 *phasor;
+    int nblk_uv;
+    double2 *visd;
+    float2 *visi;
+    float *mock;
+    float2 *cw, *trib;
+    double *partials;
+    DevScalars *sc;
+    FusedCtrl fc;
+    int direct;
+    GP_VGRID_FIELDS;
+};
+
+__device__ __forceinline__ void vis_data_body(const VisDataArgs &A, const GpVGrid &vg)
 {
+    const float2 *__restrict__ vpart = A.vpart;
+    const int mt = A.mt, nuv = A.nuv, npow = A.npow, nbis = A.nbis, nblk_uv = A.nblk_uv, direct = A.direct;
+    const float *__restrict__ data = A.data;
+    const float *__restrict__ data_err = A.data_err;
+    const int4 *__restrict__ tri = A.tri;
+    const float2 *__restrict__ phasor = A.phasor;
+    double2 *__restrict__ visd = A.visd;
+    float2 *__restrict__ visi = A.visi;
+    float *__restrict__ mock = A.mock;
+    float2 *__restrict__ cw = A.cw;
+    float2 *__restrict__ trib = A.trib;
+    double *__restrict__ partials = A.partials;
+    DevScalars *__restrict__ sc = A.sc;
     // direct: the visibilities are already in visd (a single-pixel update), not in vpart
     __shared__ double smem[32];
     const double invF = sc->invflux;
 #define VIS_AT(k) (direct ? visd[(k)] : sum_vpart(vpart, mt, nuv, (k), invF))
     double chi[1] = {0.0};
-    if ((int)blockIdx.x < nblk_uv) {
-        for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nuv; k += nblk_uv * blockDim.x) {
+    if (vg.bx < nblk_uv) {
+        for (int k = vg.bx * blockDim.x + threadIdx.x; k < nuv; k += nblk_uv * blockDim.x) {
             double2 V = VIS_AT(k);
             visd[k] = V;
             visi[k] = make_float2((float)V.x, (float)V.y);
@@ -337,8 +360,8 @@ __global__ void __launch_bounds__(GP_THREADS) k_vis_data(const float2 *__restric
             cw[k] = a;
         }
     } else {
-        const int nblk_tri = gridDim.x - nblk_uv;
-        for (int t = (blockIdx.x - nblk_uv) * blockDim.x + threadIdx.x; t < nbis; t += nblk_tri * blockDim.x) {
+        const int nblk_tri = vg.nbx - nblk_uv;
+        for (int t = (vg.bx - nblk_uv) * blockDim.x + threadIdx.x; t < nbis; t += nblk_tri * blockDim.x) {
             int4 q = tri[t];
             double2 va = VIS_AT(q.x);
             double2 vb = VIS_AT(q.y);
@@ -373,21 +396,41 @@ __global__ void __launch_bounds__(GP_THREADS) k_vis_data(const float2 *__restric
         }
     }
     block_sum<1>(chi, smem);
-    if (threadIdx.x == 0) partials[blockIdx.x] = chi[0];
-    if (last_block(&sc->counter[RED_CHI2])) {
+    if (threadIdx.x == 0) partials[vg.bx] = chi[0];
+    if (last_block_of(&sc->counter[RED_CHI2], vg.nbx)) {
         double out[1];
-        finish_sum<1>(partials, gridDim.x, out, smem);
+        finish_sum<1>(partials, vg.nbx, out, smem);
         if (threadIdx.x == 0) {
             sc->chi2 = out[0];
             sc->chi2_f = (float)out[0];
             if (!isfinite(out[0])) sc->nonfinite |= 2u;
             sc->counter[RED_CHI2] = 0;
-            run_fused_ctrl(sc, fc);
+            run_fused_ctrl(sc, A.fc);
         }
     }
 }
 
 #undef VIS_AT
+
+__global__ void __launch_bounds__(GP_THREADS) k_vis_data(const VisDataArgs a) { vis_data_body(a, gp_vgrid_hw()); }
+
+struct VisDataOp {
+    using Args = VisDataArgs;
+    static __device__ __forceinline__ void run(const Args &a, const GpVGrid &v) { vis_data_body(a, v); }
+};
+
+static VisDataArgs vis_data_args(gpair_ctx *c, int direct, FusedCtrl fc)
+{
+    int nbu = gp_cdiv(c->nuv, GP_THREADS);
+    if (nbu > 512) nbu = 512;
+    if (nbu < 1) nbu = 1;
+    int nbt = gp_cdiv(c->nbis, GP_THREADS);
+    if (nbt > 1536) nbt = 1536;
+    VisDataArgs a = {c->vpart, c->mt, c->nuv, c->npow, c->nbis, c->data, c->data_err, c->tri, c->phasor, nbu,
+                     c->visd, c->visi, c->mock, c->cw, c->trib, slot_partials(c, RED_CHI2), c->sc, fc, direct,
+                     nbu + nbt, 1};
+    return a;
+}
 
 static int vis_data_launch(gpair_ctx *c, int direct);
 
@@ -395,31 +438,39 @@ int gp_vis_data(gpair_ctx *c) { return vis_data_launch(c, 0); }
 
 static int vis_data_launch(gpair_ctx *c, int direct)
 {
-    int nbu = gp_cdiv(c->nuv, GP_THREADS);
-    if (nbu > 512) nbu = 512;
-    if (nbu < 1) nbu = 1;
-    int nbt = gp_cdiv(c->nbis, GP_THREADS);
-    if (nbt > 1536) nbt = 1536;
-    k_vis_data<<<nbu + nbt, GP_THREADS, 0, c->stream>>>(c->vpart, c->mt, c->nuv, c->npow, c->nbis, c->data,
-                                                        c->data_err, c->tri, c->phasor, nbu, c->visd, c->visi,
-                                                        c->mock, c->cw, c->trib, slot_partials(c, RED_CHI2), c->sc,
-                                                        take_fused_ctrl(c), direct);
+    const VisDataArgs a = vis_data_args(c, direct, take_fused_ctrl(c));
+    k_vis_data<<<a.nbx, GP_THREADS, 0, c->stream>>>(a);
     GP_LAUNCH_CHECK(c);
     return GPAIR_OK;
 }
 
 // ----------------------------------------------------- adjoint weights
 
-__global__ void __launch_bounds__(GP_THREADS) k_adj_weights(int nuv, const int *__restrict__ inc_off,
-                                                            const int *__restrict__ inc_idx,
-                                                            const float2 *__restrict__ trib,
-                                                            const double2 *__restrict__ visd, float2 *__restrict__ cw,
-                                                            double *__restrict__ partials, DevScalars *__restrict__ sc)
+struct AdjWeightsArgs {
+    int nuv;
+    const int *inc_off, *inc_idx;
+    const float2 *trib;
+    const double2 *visd;
+    float2 *cw;
+    double *partials;
+    DevScalars *sc;
+    GP_VGRID_FIELDS;
+};
+
+__device__ __forceinline__ void adj_weights_body(const AdjWeightsArgs &A, const GpVGrid &vg)
 {
+    const int nuv = A.nuv;
+    const int *__restrict__ inc_off = A.inc_off;
+    const int *__restrict__ inc_idx = A.inc_idx;
+    const float2 *__restrict__ trib = A.trib;
+    const double2 *__restrict__ visd = A.visd;
+    float2 *__restrict__ cw = A.cw;
+    double *__restrict__ partials = A.partials;
+    DevScalars *__restrict__ sc = A.sc;
     __shared__ double smem[32];
     double acc[1] = {0.0};
     double cmax = 0.0;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nuv; k += gridDim.x * blockDim.x) {
+    for (int k = vg.bx * blockDim.x + threadIdx.x; k < nuv; k += vg.nbx * blockDim.x) {
         float2 a = cw[k];
         double re = a.x, im = a.y;
         const int pe = inc_off[k + 1];
@@ -447,12 +498,12 @@ __global__ void __launch_bounds__(GP_THREADS) k_adj_weights(int nuv, const int *
     block_sum<1>(acc, smem);
     cmax = block_max(cmax, smem);
     if (threadIdx.x == 0) {
-        partials[2 * blockIdx.x] = acc[0];
-        partials[2 * blockIdx.x + 1] = cmax;
+        partials[2 * vg.bx] = acc[0];
+        partials[2 * vg.bx + 1] = cmax;
     }
-    if (last_block(&sc->counter[RED_ADJ])) {
+    if (last_block_of(&sc->counter[RED_ADJ], vg.nbx)) {
         double s = 0.0, m = 0.0;
-        for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
+        for (int b = threadIdx.x; b < vg.nbx; b += blockDim.x) {
             s += __ldcg(&partials[2 * b]);
             m = fmax(m, __ldcg(&partials[2 * b + 1]));
         }
@@ -466,6 +517,26 @@ __global__ void __launch_bounds__(GP_THREADS) k_adj_weights(int nuv, const int *
             sc->counter[RED_ADJ] = 0;
         }
     }
+}
+
+__global__ void __launch_bounds__(GP_THREADS) k_adj_weights(const AdjWeightsArgs a)
+{
+    adj_weights_body(a, gp_vgrid_hw());
+}
+
+struct AdjWeightsOp {
+    using Args = AdjWeightsArgs;
+    static __device__ __forceinline__ void run(const Args &a, const GpVGrid &v) { adj_weights_body(a, v); }
+};
+
+static AdjWeightsArgs adj_weights_args(gpair_ctx *c)
+{
+    int nb = gp_cdiv(c->nuv, GP_THREADS);
+    if (nb > 592) nb = 592;
+    if (nb < 1) nb = 1;
+    AdjWeightsArgs a = {c->nuv, c->inc_off, c->inc_idx, c->trib, c->visd, c->cw, slot_partials(c, RED_ADJ), c->sc,
+                        nb, 1};
+    return a;
 }
 
 // ----------------------------------------------------- adjoint, CUDA cores
@@ -545,11 +616,8 @@ static int adj_splits(int N, int nuv)
 
 int gp_adj_weights_only(gpair_ctx *c)
 {
-    int nb = gp_cdiv(c->nuv, GP_THREADS);
-    if (nb > 592) nb = 592;
-    if (nb < 1) nb = 1;
-    k_adj_weights<<<nb, GP_THREADS, 0, c->stream>>>(c->nuv, c->inc_off, c->inc_idx, c->trib, c->visd, c->cw,
-                                                    slot_partials(c, RED_ADJ), c->sc);
+    const AdjWeightsArgs a = adj_weights_args(c);
+    k_adj_weights<<<a.nbx, GP_THREADS, 0, c->stream>>>(a);
     GP_LAUNCH_CHECK(c);
     return GPAIR_OK;
 }
@@ -628,19 +696,36 @@ int gp_default_splits(int N, int nuv) { return adj_splits(N, nuv); }
 
 // ------------------------------------------------------ gradient finalize
 
-__global__ void __launch_bounds__(GP_THREADS) k_grad_finalize(const float *__restrict__ gpart, int splits,
-                                                              int npix, int mode,
-                                                              const float *__restrict__ img,
-                                                              const float *__restrict__ model, float alpha,
-                                                              int alpha_from_state,
-                                                              float *__restrict__ data_grad,
-                                                              float *__restrict__ entropy_grad,
-                                                              float *__restrict__ out,
-                                                              const float *__restrict__ g_old,
-                                                              const float *__restrict__ d, int dot_slot,
-                                                              double *__restrict__ partials,
-                                                              DevScalars *__restrict__ sc, FusedCtrl fc)
+struct GradFinalizeArgs {
+    const float *gpart;
+    int splits, npix, mode;
+    const float *img, *model;
+    float alpha;
+    int alpha_from_state;
+    float *data_grad, *entropy_grad, *out;
+    const float *g_old, *d;
+    int dot_slot;
+    double *partials;
+    DevScalars *sc;
+    FusedCtrl fc;
+    GP_VGRID_FIELDS;
+};
+
+__device__ __forceinline__ void grad_finalize_body(const GradFinalizeArgs &A, const GpVGrid &vg)
 {
+    const float *__restrict__ gpart = A.gpart;
+    const int splits = A.splits, npix = A.npix, mode = A.mode, dot_slot = A.dot_slot;
+    const float *__restrict__ img = A.img;
+    const float *__restrict__ model = A.model;
+    float alpha = A.alpha;
+    const int alpha_from_state = A.alpha_from_state;
+    float *__restrict__ data_grad = A.data_grad;
+    float *__restrict__ entropy_grad = A.entropy_grad;
+    float *__restrict__ out = A.out;
+    const float *__restrict__ g_old = A.g_old;
+    const float *__restrict__ d = A.d;
+    double *__restrict__ partials = A.partials;
+    DevScalars *__restrict__ sc = A.sc;
     __shared__ double smem[4 * 32];
     const double C = sc->adj_c, gscale = sc->gscale;
     const int reg_kind = sc->reg_kind;
@@ -667,7 +752,7 @@ __global__ void __launch_bounds__(GP_THREADS) k_grad_finalize(const float *__res
     if ((npix & 3) == 0) {
         // four consecutive pixels per thread: 16-byte loads, 8 splits (128 B) in flight
         const int nq = npix >> 2;
-        for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
+        for (int q = vg.bx * blockDim.x + threadIdx.x; q < nq; q += vg.nbx * blockDim.x) {
             const float4 *g4 = reinterpret_cast<const float4 *>(gpart) + q;
             const size_t stride = (size_t)nq;
             double g[4] = {0.0, 0.0, 0.0, 0.0};
@@ -695,7 +780,7 @@ __global__ void __launch_bounds__(GP_THREADS) k_grad_finalize(const float *__res
             for (int j = 0; j < 4; j++) finish(4 * q + j, g[j]);
         }
     } else {
-        for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
+        for (int p = vg.bx * blockDim.x + threadIdx.x; p < npix; p += vg.nbx * blockDim.x) {
             double g = 0.0;
             int s = 0;
             for (; s + 16 <= splits; s += 16) {  // 16 loads in flight, summed in split order
@@ -712,20 +797,30 @@ __global__ void __launch_bounds__(GP_THREADS) k_grad_finalize(const float *__res
     if (mode != GRAD_FUSED) return;
     block_sum<4>(acc, smem);
     if (threadIdx.x == 0)
-        for (int i = 0; i < 4; i++) partials[4 * blockIdx.x + i] = acc[i];
-    if (last_block(&sc->counter[RED_GRAD])) {
+        for (int i = 0; i < 4; i++) partials[4 * vg.bx + i] = acc[i];
+    if (last_block_of(&sc->counter[RED_GRAD], vg.nbx)) {
         double o[4];
-        finish_sum<4>(partials, gridDim.x, o, smem);
+        finish_sum<4>(partials, vg.nbx, o, smem);
         if (threadIdx.x == 0) {
             for (int i = 0; i < 4; i++) sc->grad_dots[dot_slot][i] = o[i];
             if (!isfinite(o[0])) sc->nonfinite |= 4u;
             sc->counter[RED_GRAD] = 0;
-            run_fused_ctrl(sc, fc);
+            run_fused_ctrl(sc, A.fc);
         }
     }
 }
 
-int gp_grad_finalize(gpair_ctx *c, int which, int mode, float alpha)
+__global__ void __launch_bounds__(GP_THREADS) k_grad_finalize(const GradFinalizeArgs a)
+{
+    grad_finalize_body(a, gp_vgrid_hw());
+}
+
+struct GradFinalizeOp {
+    using Args = GradFinalizeArgs;
+    static __device__ __forceinline__ void run(const Args &a, const GpVGrid &v) { grad_finalize_body(a, v); }
+};
+
+static GradFinalizeArgs grad_finalize_args(gpair_ctx *c, int which, int mode, float alpha, FusedCtrl fc)
 {
     // alpha < 0 requests the value held in the device CG state (graph-captured runs)
     const int alpha_from_state = alpha < 0.f;
@@ -735,10 +830,16 @@ int gp_grad_finalize(gpair_ctx *c, int which, int mode, float alpha)
     int g = gp_cdiv((c->npix & 3) == 0 ? c->npix / 4 : c->npix, GP_THREADS);
     if (g > GP_MAX_PARTIALS) g = GP_MAX_PARTIALS;
     if (g < 1) g = 1;
-    k_grad_finalize<<<g, GP_THREADS, 0, c->stream>>>(c->gpart, c->splits, c->npix, mode, img,
-                                                     c->model, alpha, alpha_from_state, c->data_grad, c->entropy_grad, out,
-                                                     c->full_grad, c->descent_dir, which == GPAIR_IMG_TEMP ? 1 : 0,
-                                                     slot_partials(c, RED_GRAD), c->sc, take_fused_ctrl(c));
+    GradFinalizeArgs a = {c->gpart, c->splits, c->npix, mode, img, c->model, alpha, alpha_from_state,
+                          c->data_grad, c->entropy_grad, out, c->full_grad, c->descent_dir,
+                          which == GPAIR_IMG_TEMP ? 1 : 0, slot_partials(c, RED_GRAD), c->sc, fc, g, 1};
+    return a;
+}
+
+int gp_grad_finalize(gpair_ctx *c, int which, int mode, float alpha)
+{
+    const GradFinalizeArgs a = grad_finalize_args(c, which, mode, alpha, take_fused_ctrl(c));
+    k_grad_finalize<<<a.nbx, GP_THREADS, 0, c->stream>>>(a);
     GP_LAUNCH_CHECK(c);
     return GPAIR_OK;
 }
@@ -805,15 +906,28 @@ int gp_dot(gpair_ctx *c, const float *a, const float *b, int n)
 }
 
 // d = beta d - g_new, and d.g_new (FP64)
-__global__ void __launch_bounds__(GP_THREADS) k_descent(float *__restrict__ d, const float *__restrict__ g, int n,
-                                                        int beta_from_state, double beta_host,
-                                                        double *__restrict__ partials, DevScalars *__restrict__ sc,
-                                                        FusedCtrl fc)
+struct DescentArgs {
+    float *d;
+    const float *g;
+    int n, beta_from_state;
+    double beta_host;
+    double *partials;
+    DevScalars *sc;
+    FusedCtrl fc;
+    GP_VGRID_FIELDS;
+};
+
+__device__ __forceinline__ void descent_body(const DescentArgs &A, const GpVGrid &vg)
 {
+    float *__restrict__ d = A.d;
+    const float *__restrict__ g = A.g;
+    const int n = A.n;
+    double *__restrict__ partials = A.partials;
+    DevScalars *__restrict__ sc = A.sc;
     __shared__ double smem[32];
-    const double beta = beta_from_state ? sc->cg.beta : beta_host;
+    const double beta = A.beta_from_state ? sc->cg.beta : A.beta_host;
     double acc[1] = {0.0};
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    for (int p = vg.bx * blockDim.x + threadIdx.x; p < n; p += vg.nbx * blockDim.x) {
         // beta = 0 (first iteration, restarts) must not read the old direction:
         // 0 * d_old is NaN when a previous run left non-finite values there
         float dn = beta != 0.0 ? (float)(beta * (double)d[p] - (double)g[p]) : -g[p];
@@ -821,23 +935,36 @@ __global__ void __launch_bounds__(GP_THREADS) k_descent(float *__restrict__ d, c
         acc[0] += (double)dn * (double)g[p];
     }
     block_sum<1>(acc, smem);
-    if (threadIdx.x == 0) partials[blockIdx.x] = acc[0];
-    if (last_block(&sc->counter[RED_DIR])) {
+    if (threadIdx.x == 0) partials[vg.bx] = acc[0];
+    if (last_block_of(&sc->counter[RED_DIR], vg.nbx)) {
         double o[1];
-        finish_sum<1>(partials, gridDim.x, o, smem);
+        finish_sum<1>(partials, vg.nbx, o, smem);
         if (threadIdx.x == 0) {
             sc->dir_dot = o[0];
             sc->counter[RED_DIR] = 0;
-            run_fused_ctrl(sc, fc);
+            run_fused_ctrl(sc, A.fc);
         }
     }
 }
 
+__global__ void __launch_bounds__(GP_THREADS) k_descent(const DescentArgs a) { descent_body(a, gp_vgrid_hw()); }
+
+struct DescentOp {
+    using Args = DescentArgs;
+    static __device__ __forceinline__ void run(const Args &a, const GpVGrid &v) { descent_body(a, v); }
+};
+
+static DescentArgs descent_args(gpair_ctx *c, int beta_from_state, double beta_host, FusedCtrl fc)
+{
+    DescentArgs a = {c->descent_dir, c->full_grad_new, c->npix, beta_from_state, beta_host,
+                     slot_partials(c, RED_DIR), c->sc, fc, red_grid(c->npix), 1};
+    return a;
+}
+
 int gp_descent_dir(gpair_ctx *c, int beta_from_state, double beta_host)
 {
-    k_descent<<<red_grid(c->npix), GP_THREADS, 0, c->stream>>>(c->descent_dir, c->full_grad_new, c->npix,
-                                                               beta_from_state, beta_host,
-                                                               slot_partials(c, RED_DIR), c->sc, take_fused_ctrl(c));
+    const DescentArgs a = descent_args(c, beta_from_state, beta_host, take_fused_ctrl(c));
+    k_descent<<<a.nbx, GP_THREADS, 0, c->stream>>>(a);
     GP_LAUNCH_CHECK(c);
     return GPAIR_OK;
 }
@@ -1066,25 +1193,53 @@ int gp_lbfgs_direction(gpair_ctx *c)
 }
 
 // image = max(image + s d, minval); optionally full_grad = full_grad_new
-__global__ void k_update_image(float *__restrict__ img, const float *__restrict__ d, int n, int step_from_state,
-                               double step_host, double minval, const float *__restrict__ gnew,
-                               float *__restrict__ gold, const DevScalars *__restrict__ sc)
+struct UpdateImageArgs {
+    float *img;
+    const float *d;
+    int n, step_from_state;
+    double step_host, minval;
+    const float *gnew;
+    float *gold;
+    const DevScalars *sc;
+    GP_VGRID_FIELDS;
+};
+
+__device__ __forceinline__ void update_image_body(const UpdateImageArgs &A, const GpVGrid &vg)
 {
-    int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n) return;
-    double s = step_from_state ? sc->cg.sel : step_host;
-    if (step_from_state) minval = sc->cg.minvalue;
-    double t = (double)img[p] + s * (double)d[p];
-    if (t < minval) t = minval;
-    img[p] = (float)t;
-    if (gold) gold[p] = gnew[p];
+    float *__restrict__ img = A.img;
+    const float *__restrict__ d = A.d;
+    const float *__restrict__ gnew = A.gnew;
+    float *__restrict__ gold = A.gold;
+    const int n = A.n;
+    const double s = A.step_from_state ? A.sc->cg.sel : A.step_host;
+    const double minval = A.step_from_state ? A.sc->cg.minvalue : A.minval;
+    for (int p = vg.bx * blockDim.x + threadIdx.x; p < n; p += vg.nbx * blockDim.x) {
+        double t = (double)img[p] + s * (double)d[p];
+        if (t < minval) t = minval;
+        img[p] = (float)t;
+        if (gold) gold[p] = gnew[p];
+    }
+}
+
+__global__ void __launch_bounds__(256) k_update_image(const UpdateImageArgs a) { update_image_body(a, gp_vgrid_hw()); }
+
+struct UpdateImageOp {
+    using Args = UpdateImageArgs;
+    static __device__ __forceinline__ void run(const Args &a, const GpVGrid &v) { update_image_body(a, v); }
+};
+
+static UpdateImageArgs update_image_args(gpair_ctx *c, int step_from_state, double step_host, double minval,
+                                         int backup)
+{
+    UpdateImageArgs a = {c->image, c->descent_dir, c->npix, step_from_state, step_host, minval, c->full_grad_new,
+                         backup ? c->full_grad : nullptr, c->sc, gp_cdiv(c->npix, 256), 1};
+    return a;
 }
 
 int gp_update_image(gpair_ctx *c, int step_from_state, double step_host, double minval, int backup)
 {
-    k_update_image<<<gp_cdiv(c->npix, 256), 256, 0, c->stream>>>(c->image, c->descent_dir, c->npix, step_from_state,
-                                                                 step_host, minval, c->full_grad_new,
-                                                                 backup ? c->full_grad : nullptr, c->sc);
+    const UpdateImageArgs a = update_image_args(c, step_from_state, step_host, minval, backup);
+    k_update_image<<<a.nbx, 256, 0, c->stream>>>(a);
     GP_LAUNCH_CHECK(c);
     return GPAIR_OK;
 }
@@ -1160,23 +1315,37 @@ __global__ void __launch_bounds__(GP_THREADS) k_trials_prep(const float *__restr
 // epp partial entries) / F_j, then V2 and T3 residuals as in k_vis_data; mock
 // data and adjoint weights are not needed for trials. The last block of the
 // whole grid sums each trial's partials in block order and runs the controller.
-__global__ void __launch_bounds__(GP_THREADS) k_vis_chi2_batch(const float2 *__restrict__ vpart, int epp, int nuv,
-                                                               int npow, int nbis, const float *__restrict__ data,
-                                                               const float *__restrict__ data_err,
-                                                               const int4 *__restrict__ tri,
-                                                               const float2 *__restrict__ phasor,
-                                                               double *__restrict__ partials,
-                                                               DevScalars *__restrict__ sc, FusedCtrl fc,
-                                                               const int *__restrict__ gate)
+struct VisChi2BatchArgs {
+    const float2 *vpart;
+    int epp, nuv, npow, nbis;
+    const float *data, *data_err;
+    const int4 *tri;
+    const float2 *phasor;
+    double *partials;
+    DevScalars *sc;
+    FusedCtrl fc;
+    const int *gate;
+    GP_VGRID_FIELDS;
+};
+
+__device__ __forceinline__ void vis_chi2_batch_body(const VisChi2BatchArgs &A, const GpVGrid &vg)
 {
+    const float2 *__restrict__ vpart = A.vpart;
+    const int epp = A.epp, nuv = A.nuv, npow = A.npow, nbis = A.nbis;
+    const float *__restrict__ data = A.data;
+    const float *__restrict__ data_err = A.data_err;
+    const int4 *__restrict__ tri = A.tri;
+    const float2 *__restrict__ phasor = A.phasor;
+    double *__restrict__ partials = A.partials;
+    DevScalars *__restrict__ sc = A.sc;
     __shared__ double smem[32];
-    if (gate && !*gate) return;  // lockstep batches: this instance's line search is over
-    const int j = blockIdx.y;
+    if (A.gate && !*A.gate) return;  // lockstep batches: this instance's line search is over
+    const int j = vg.by;
     const double invF = sc->t_invflux[j];
     const float2 *vp = vpart + (size_t)j * epp * nuv;
     double chi[1] = {0.0};
     const int nitems = npow + nbis;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nitems; i += gridDim.x * blockDim.x) {
+    for (int i = vg.bx * blockDim.x + threadIdx.x; i < nitems; i += vg.nbx * blockDim.x) {
         if (i < npow) {
             double2 V = sum_vpart(vp, epp, nuv, i, invF);
             double m2 = V.x * V.x + V.y * V.y;
@@ -1200,24 +1369,34 @@ __global__ void __launch_bounds__(GP_THREADS) k_vis_chi2_batch(const float2 *__r
         }
     }
     block_sum<1>(chi, smem);
-    if (threadIdx.x == 0) partials[(size_t)j * gridDim.x + blockIdx.x] = chi[0];
-    if (last_block_of(&sc->t_counter[GP_NTR], gridDim.x * gridDim.y)) {
+    if (threadIdx.x == 0) partials[(size_t)j * vg.nbx + vg.bx] = chi[0];
+    if (last_block_of(&sc->t_counter[GP_NTR], vg.nbx * vg.nby)) {
         // one warp per trial, all trials at once; fixed lane order and shuffle tree
         const int lane = threadIdx.x & 31;
-        for (int jj = threadIdx.x >> 5; jj < (int)gridDim.y; jj += blockDim.x >> 5) {
-            const double *pp = partials + (size_t)jj * gridDim.x;
+        for (int jj = threadIdx.x >> 5; jj < vg.nby; jj += blockDim.x >> 5) {
+            const double *pp = partials + (size_t)jj * vg.nbx;
             double v = 0.0;
-            for (int b = lane; b < (int)gridDim.x; b += 32) v += __ldcg(&pp[b]);
+            for (int b = lane; b < vg.nbx; b += 32) v += __ldcg(&pp[b]);
             for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
             if (lane == 0) sc->t_chi2[jj] = v;
         }
         __syncthreads();
         if (threadIdx.x == 0) {
             sc->t_counter[GP_NTR] = 0;
-            run_fused_ctrl(sc, fc);
+            run_fused_ctrl(sc, A.fc);
         }
     }
 }
+
+__global__ void __launch_bounds__(GP_THREADS) k_vis_chi2_batch(const VisChi2BatchArgs a)
+{
+    vis_chi2_batch_body(a, gp_vgrid_hw());
+}
+
+struct VisChi2BatchOp {
+    using Args = VisChi2BatchArgs;
+    static __device__ __forceinline__ void run(const Args &a, const GpVGrid &v) { vis_chi2_batch_body(a, v); }
+};
 
 // Blocks per trial: at most one wave of resident blocks over the whole batch
 // (a partial second wave would leave most SMs idle while it runs), at most 256
@@ -1283,16 +1462,21 @@ int gp_trials_prep_launch(gpair_ctx *c)
 
 // chi2 of the GP_NTR trials of a batch from their partial visibilities (epp
 // entries per trial), then the fused controller
-static int batch_chi2(gpair_ctx *c, int epp)
+static VisChi2BatchArgs batch_chi2_args(gpair_ctx *c, int epp, FusedCtrl fc, const int *gate)
 {
     int nb = gp_cdiv(c->npow + c->nbis, GP_THREADS * 2);
     if (nb > c->batch_wave[1]) nb = c->batch_wave[1];  // one wave over the batch
     if (nb > 1024) nb = 1024;
     if (nb < 1) nb = 1;
-    dim3 g(nb, GP_NTR);
-    k_vis_chi2_batch<<<g, GP_THREADS, 0, c->stream>>>(c->vpart_b, epp, c->nuv, c->npow, c->nbis, c->data,
-                                                      c->data_err, c->tri, c->phasor, c->partials_b, c->sc,
-                                                      take_fused_ctrl(c), c->gate);
+    VisChi2BatchArgs a = {c->vpart_b, epp, c->nuv, c->npow, c->nbis, c->data, c->data_err, c->tri, c->phasor,
+                          c->partials_b, c->sc, fc, gate, nb, GP_NTR};
+    return a;
+}
+
+static int batch_chi2(gpair_ctx *c, int epp)
+{
+    const VisChi2BatchArgs a = batch_chi2_args(c, epp, take_fused_ctrl(c), c->gate);
+    k_vis_chi2_batch<<<dim3(a.nbx, a.nby), GP_THREADS, 0, c->stream>>>(a);
     GP_LAUNCH_CHECK(c);
     return GPAIR_OK;
 }
@@ -1873,28 +2057,44 @@ __device__ void cg_set_handles(DevScalars *__restrict__ sc, int what, cudaGraphC
 // graph: h_ls keeps the line-search loop going, h_grad selects the gradient
 // branch of a trial, h_iter keeps the iteration loop going. At the end of an
 // iteration it appends (J, chi2, S, step, beta) to the device trace.
-__global__ void k_cg_ctrl_g(DevScalars *__restrict__ sc, int what, cudaGraphConditionalHandle h_iter,
-                            cudaGraphConditionalHandle h_ls, cudaGraphConditionalHandle h_grad,
-                            double *__restrict__ trace, int trace_cap)
+struct CtrlArgs {
+    DevScalars *sc;
+    int what;
+    cudaGraphConditionalHandle h_iter, h_ls, h_grad;
+    double *trace;
+    int trace_cap;
+    GP_VGRID_FIELDS;
+};
+
+__device__ __forceinline__ void cg_ctrl_g_body(const CtrlArgs &A, const GpVGrid &vg)
 {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (threadIdx.x != 0 || vg.bx != 0) return;
+    DevScalars *__restrict__ sc = A.sc;
     CgState &s = sc->cg;
-    if (what == CTRL_END && s.run_it < trace_cap && trace) {
-        double *t = trace + 5 * (size_t)s.run_it;
+    if (A.what == CTRL_END && s.run_it < A.trace_cap && A.trace) {
+        double *t = A.trace + 5 * (size_t)s.run_it;
         t[0] = s.J;
         t[1] = s.chi2;
         t[2] = s.entropy;
         t[3] = s.sel;
         t[4] = s.beta;
     }
-    cg_control(sc, what);
-    if (h_iter) cg_set_handles(sc, what, h_iter, h_ls, h_grad);
+    cg_control(sc, A.what);
+    if (A.h_iter) cg_set_handles(sc, A.what, A.h_iter, A.h_ls, A.h_grad);
 }
+
+__global__ void k_cg_ctrl_g(const CtrlArgs a) { cg_ctrl_g_body(a, gp_vgrid_hw()); }
+
+struct CtrlOp {
+    using Args = CtrlArgs;
+    static __device__ __forceinline__ void run(const Args &a, const GpVGrid &v) { cg_ctrl_g_body(a, v); }
+};
 
 int gp_cg_kernel_graph(gpair_ctx *c, int which_ctrl, unsigned long long h_iter, unsigned long long h_ls,
                        unsigned long long h_grad, double *trace, int trace_cap)
 {
-    k_cg_ctrl_g<<<1, 32, 0, c->stream>>>(c->sc, which_ctrl, h_iter, h_ls, h_grad, trace, trace_cap);
+    const CtrlArgs a = {c->sc, which_ctrl, h_iter, h_ls, h_grad, trace, trace_cap, 1, 1};
+    k_cg_ctrl_g<<<1, 32, 0, c->stream>>>(a);
     GP_LAUNCH_CHECK(c);
     return GPAIR_OK;
 }
@@ -1904,4 +2104,85 @@ int gp_cg_kernel(gpair_ctx *c, int which_ctrl)
     k_cg_ctrl<<<1, 32, 0, c->stream>>>(c->sc, which_ctrl);
     GP_LAUNCH_CHECK(c);
     return GPAIR_OK;
+}
+
+// ------------------------------------------------- grouped stage launches
+//
+// Lockstep batches run each stage of an iteration as one launch over all their
+// instances (group.cuh): the argument structs below are built by the same
+// functions as the single launches, with the controller step each stage takes
+// in a lockstep iteration and no graph handles (the batch's routers steer).
+
+static FusedCtrl ctrl_only(int what)
+{
+    FusedCtrl f;
+    memset(&f, 0, sizeof(f));
+    f.what = what;
+    return f;
+}
+
+size_t gp_stage_args_size(int stage)
+{
+    switch (stage) {
+    case GS_VIS_DATA: return sizeof(VisDataArgs);
+    case GS_ADJ_WEIGHTS: return sizeof(AdjWeightsArgs);
+    case GS_GRAD_FINALIZE: return sizeof(GradFinalizeArgs);
+    case GS_DESCENT: return sizeof(DescentArgs);
+    case GS_CHI2_BATCH: return sizeof(VisChi2BatchArgs);
+    case GS_UPDATE: return sizeof(UpdateImageArgs);
+    case GS_CTRL_END: return sizeof(CtrlArgs);
+    default: return gp_tc_stage_args_size(stage);
+    }
+}
+
+template <class A>
+static int put_args(const A &a, void *out, int *nblocks)
+{
+    memcpy(out, &a, sizeof(A));
+    *nblocks = a.nbx * a.nby;
+    return GPAIR_OK;
+}
+
+int gp_stage_args(gpair_ctx *c, int stage, double *trace, void *out, int *nblocks)
+{
+    switch (stage) {
+    case GS_VIS_DATA: return put_args(vis_data_args(c, 0, ctrl_only(-1)), out, nblocks);
+    case GS_ADJ_WEIGHTS: return put_args(adj_weights_args(c), out, nblocks);
+    case GS_GRAD_FINALIZE:
+        return put_args(grad_finalize_args(c, GPAIR_IMG_CURR, GRAD_FUSED, -1.f, ctrl_only(CTRL_BEGIN)), out, nblocks);
+    case GS_DESCENT: return put_args(descent_args(c, 1, 0.0, ctrl_only(CTRL_AFTER_DIR)), out, nblocks);
+    case GS_CHI2_BATCH:
+        return put_args(batch_chi2_args(c, c->epp, ctrl_only(CTRL_AFTER_BATCH), nullptr), out, nblocks);
+    case GS_UPDATE: return put_args(update_image_args(c, 1, 0.0, 1e-8, 1), out, nblocks);
+    case GS_CTRL_END: {
+        const CtrlArgs a = {c->sc, CTRL_END, 0, 0, 0, trace, 1, 1, 1};
+        return put_args(a, out, nblocks);
+    }
+    default: return GPAIR_ERR_INVALID;
+    }
+}
+
+template <class Op, int THREADS>
+static int group_launch(gpair_ctx *c, const void *d_args, const int *d_start, int n, int total, const int *gate)
+{
+    k_grouped<Op, THREADS>
+        <<<total, THREADS, 0, c->stream>>>((const typename Op::Args *)d_args, d_start, n, gate);
+    GP_LAUNCH_CHECK(c);
+    return GPAIR_OK;
+}
+
+int gp_stage_group_launch(gpair_ctx *c, int stage, const void *d_args, const int *d_start, int n, int total,
+                          const int *gate)
+{
+    if (total < 1 || n < 1) return GPAIR_ERR_INVALID;
+    switch (stage) {
+    case GS_VIS_DATA: return group_launch<VisDataOp, GP_THREADS>(c, d_args, d_start, n, total, gate);
+    case GS_ADJ_WEIGHTS: return group_launch<AdjWeightsOp, GP_THREADS>(c, d_args, d_start, n, total, gate);
+    case GS_GRAD_FINALIZE: return group_launch<GradFinalizeOp, GP_THREADS>(c, d_args, d_start, n, total, gate);
+    case GS_DESCENT: return group_launch<DescentOp, GP_THREADS>(c, d_args, d_start, n, total, gate);
+    case GS_CHI2_BATCH: return group_launch<VisChi2BatchOp, GP_THREADS>(c, d_args, d_start, n, total, gate);
+    case GS_UPDATE: return group_launch<UpdateImageOp, 256>(c, d_args, d_start, n, total, gate);
+    case GS_CTRL_END: return group_launch<CtrlOp, 32>(c, d_args, d_start, n, total, gate);
+    default: return GPAIR_ERR_INVALID;
+    }
 }

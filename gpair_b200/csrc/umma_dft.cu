@@ -40,6 +40,7 @@
 #include <string.h>
 
 #include "gpair_internal.cuh"
+#include "group.cuh"
 #include "reduce.cuh"
 #include "umma.cuh"
 
@@ -160,10 +161,15 @@ struct TcArgs {
 struct __align__(64) TcGroupInst {
     CUtensorMap A_hi, A_lo, A_x, B_hi, B_lo, B_x;  // A_x, B_x: OP_F16F8's second 8-bit operands
     int m_tiles, n_tiles, kb_total, units;
+    // forward epilogue
     const float2 *fya, *fyr;
     int nanc, nuv, lpad, elog2;
     const float *rsc;
     float2 *vpart;
+    // store epilogue (adjoint): split-K partial images
+    int kb_per_split;
+    float *gpart;
+    int out_ld, out_rows, out_cols;
 };
 #define TC_GROUP_MAX 256  // instances of one grouped launch (prefix sums in shared memory)
 
@@ -234,12 +240,21 @@ __device__ __forceinline__ void tc_unit(const TcArgs &a, const int *gpre, int u,
 {
     if (GROUP) {
         while (gpre[ci + 1] <= u) ci++;
-        const int lu = u - gpre[ci], nt = a.grp[ci].n_tiles;
+        const TcGroupInst &gi = a.grp[ci];
+        const int lu = u - gpre[ci], nt = gi.n_tiles;
         n = lu % nt;
-        m = lu / nt;
-        split = 0;
-        kb0 = 0;
-        kb1 = a.grp[ci].kb_total;
+        if (EPI == EPI_FWD) {
+            m = lu / nt;
+            split = 0;
+            kb0 = 0;
+            kb1 = gi.kb_total;
+        } else {
+            const int rest = lu / nt;
+            m = rest % gi.m_tiles;
+            split = rest / gi.m_tiles;
+            kb0 = split * gi.kb_per_split;
+            kb1 = min(gi.kb_total, kb0 + gi.kb_per_split);
+        }
     } else {
         tc_decode<EPI>(a, u, m, n, kb0, kb1, split);
     }
@@ -262,9 +277,9 @@ template <int PAIR> struct TcGeo {
 };
 static_assert(TcGeo<0>::STAGES * TcGeo<0>::STAGE == TcGeo<1>::STAGES * TcGeo<1>::STAGE, "same smem in both modes");
 
-// GROUP = 1 (forward only): one launch over the units of several instances
-// (TcGroupInst), each with its own maps and epilogue arguments; the kernel's
-// map parameters are not used.
+// GROUP = 1: one launch over the units of several instances (TcGroupInst),
+// each with its own maps and epilogue arguments; the kernel's map parameters
+// are not used.
 //
 // OP_F16F8: each stage holds A_hi (f16, 128-byte rows), A8_hi and A8_lo (E4M3,
 // 64-byte rows), B_hi, B8_hi and B8_lo; per K-block 4 kind::f16 MMAs (A_hi B_hi)
@@ -277,7 +292,6 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
               const __grid_constant__ CUtensorMap tA_x, const __grid_constant__ CUtensorMap tB_hi,
               const __grid_constant__ CUtensorMap tB_lo, const __grid_constant__ CUtensorMap tB_x, const TcArgs a)
 {
-    static_assert(!GROUP || EPI == EPI_FWD, "grouped launches run the forward");
     static_assert(OP != OP_F16F8 || (EPI == EPI_FWD && NPROD == 3), "the 8-bit cross terms serve the forward");
     constexpr bool F8 = OP == OP_F16F8;
     using G = TcGeo<PAIR>;
@@ -636,9 +650,18 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     break;
                 }
                 umma::tc_fence_after();
-                float *out = a.gpart + (size_t)split * a.out_rows * a.out_ld;
+                float *gpart = a.gpart;
+                int out_ld = a.out_ld, out_rows = a.out_rows, out_cols = a.out_cols;
+                if (GROUP) {
+                    const TcGroupInst &gi = a.grp[ci];
+                    gpart = gi.gpart;
+                    out_ld = gi.out_ld;
+                    out_rows = gi.out_rows;
+                    out_cols = gi.out_cols;
+                }
+                float *out = gpart + (size_t)split * out_rows * out_ld;
                 const int x = arow;
-                const bool xv = x < a.out_cols;
+                const bool xv = x < out_cols;
 #pragma unroll 1
                 for (int c = 0; c < TC_BN / 16; c++) {
                     uint32_t r[16];
@@ -648,7 +671,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 #pragma unroll
                         for (int j = 0; j < 16; j++) {
                             const int y = y0 + c * 16 + j;
-                            if (y < a.out_rows) out[(size_t)y * a.out_ld + x] = __uint_as_float(r[j]);
+                            if (y < out_rows) out[(size_t)y * out_ld + x] = __uint_as_float(r[j]);
                         }
                     }
                 }
@@ -787,19 +810,41 @@ static inline int pr_warps_per_row(int N)
     return w;
 }
 
+struct PrepRowsArgs {
+    const float *img, *d;
+    float *dst;
+    const float *model;
+    int N, W, Lpad, Kx_pad;
+    void *hi, *lo;  // OT
+    uint8_t *h8, *l8;
+    float *rsc;
+    int reduce;
+    double *partials;
+    DevScalars *sc;
+    const int *gate;
+    GP_VGRID_FIELDS;
+};
+
 template <typename OT, int MODE>
-__global__ void __launch_bounds__(PR_THREADS)
-    k_tc_prep_rows(const float *__restrict__ img, const float *__restrict__ d, float *__restrict__ dst,
-                   const float *__restrict__ model, int N, int W, int Lpad, int Kx_pad, OT *__restrict__ hi,
-                   OT *__restrict__ lo, uint8_t *__restrict__ h8, uint8_t *__restrict__ l8,
-                   float *__restrict__ rsc, int reduce, double *__restrict__ partials,
-                   DevScalars *__restrict__ sc, const int *__restrict__ gate)
+__device__ __forceinline__ void tc_prep_rows_body(const PrepRowsArgs &A, const GpVGrid &vg)
 {
+    const float *__restrict__ img = A.img;
+    const float *__restrict__ d = A.d;
+    float *__restrict__ dst = A.dst;
+    const float *__restrict__ model = A.model;
+    const int N = A.N, W = A.W, Lpad = A.Lpad, Kx_pad = A.Kx_pad, reduce = A.reduce;
+    OT *__restrict__ hi = (OT *)A.hi;
+    OT *__restrict__ lo = (OT *)A.lo;
+    uint8_t *__restrict__ h8 = A.h8;
+    uint8_t *__restrict__ l8 = A.l8;
+    float *__restrict__ rsc = A.rsc;
+    double *__restrict__ partials = A.partials;
+    DevScalars *__restrict__ sc = A.sc;
     __shared__ double smem[3 * 32];
     __shared__ float wmax[PR_WARPS_MAX];
-    if (gate && !*gate) return;  // lockstep batches: this instance's line search is over
+    if (A.gate && !*A.gate) return;  // lockstep batches: this instance's line search is over
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int j = MODE == 2 ? (int)blockIdx.y : 0;
+    const int j = MODE == 2 ? vg.by : 0;
     const double s = MODE == 1 ? sc->cg.s : MODE == 2 ? sc->cg.ts[j] : 0.0;
     const double minval = MODE ? sc->cg.minvalue : 0.0;
     const int reg_kind = sc->reg_kind;
@@ -812,7 +857,7 @@ __global__ void __launch_bounds__(PR_THREADS)
     double acc[2] = {0.0, 0.0};
     float mx = 0.f;
     const bool vec = (N & 7) == 0 && N <= 8 * nt;
-    for (int ybase = blockIdx.x * R; ybase < N; ybase += gridDim.x * R) {  // block-uniform
+    for (int ybase = vg.bx * R; ybase < N; ybase += vg.nbx * R) {  // block-uniform
         const int y = ybase + rw;
         const bool yv = y < N;
         const size_t rp = (size_t)(yv ? y : 0) * N;
@@ -915,14 +960,14 @@ __global__ void __launch_bounds__(PR_THREADS)
     block_sum<2>(acc, smem);
     const double bmax = block_max((double)mx, smem);
     if (MODE == 2) {
-        double *pp = partials + (size_t)j * gridDim.x * 2;
+        double *pp = partials + (size_t)j * vg.nbx * 2;
         if (threadIdx.x == 0) {
-            pp[2 * blockIdx.x] = acc[0];
-            pp[2 * blockIdx.x + 1] = acc[1];
+            pp[2 * vg.bx] = acc[0];
+            pp[2 * vg.bx + 1] = acc[1];
         }
-        if (last_block(&sc->t_counter[j])) {
+        if (last_block_of(&sc->t_counter[j], vg.nbx)) {
             double o[2];
-            finish_sum<2>(pp, gridDim.x, o, smem);
+            finish_sum<2>(pp, vg.nbx, o, smem);
             if (threadIdx.x == 0) {
                 sc->t_flux[j] = o[0];
                 sc->t_invflux[j] = 1.0 / o[0];
@@ -933,16 +978,16 @@ __global__ void __launch_bounds__(PR_THREADS)
         return;
     }
     if (threadIdx.x == 0) {
-        partials[3 * blockIdx.x] = acc[0];
-        partials[3 * blockIdx.x + 1] = acc[1];
-        partials[3 * blockIdx.x + 2] = bmax;
+        partials[3 * vg.bx] = acc[0];
+        partials[3 * vg.bx + 1] = acc[1];
+        partials[3 * vg.bx + 2] = bmax;
     }
-    if (last_block(&sc->counter[RED_PREP])) {
+    if (last_block_of(&sc->counter[RED_PREP], vg.nbx)) {
         double v3[3];
-        finish_sum<3>(partials, gridDim.x, v3, smem);
+        finish_sum<3>(partials, vg.nbx, v3, smem);
         // max over the blocks' maxima (any order gives the same value)
         double m = 0.0;
-        for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) m = fmax(m, __ldcg(&partials[3 * b + 2]));
+        for (int b = threadIdx.x; b < vg.nbx; b += blockDim.x) m = fmax(m, __ldcg(&partials[3 * b + 2]));
         m = block_max(m, smem);
         if (threadIdx.x == 0) {
             sc->flux = v3[0];
@@ -957,6 +1002,17 @@ __global__ void __launch_bounds__(PR_THREADS)
         }
     }
 }
+
+template <typename OT, int MODE>
+__global__ void __launch_bounds__(PR_THREADS) k_tc_prep_rows(const PrepRowsArgs a)
+{
+    tc_prep_rows_body<OT, MODE>(a, gp_vgrid_hw());
+}
+
+template <typename OT, int MODE> struct PrepRowsOp {
+    using Args = PrepRowsArgs;
+    static __device__ __forceinline__ void run(const Args &a, const GpVGrid &v) { tc_prep_rows_body<OT, MODE>(a, v); }
+};
 
 // Fy anchors every 16 image rows and the one-row rotation of every uv point
 __global__ void k_tc_fy_anchors(const float2 *__restrict__ fy, int nuv, int N, int nanc, float2 *__restrict__ fya,
@@ -1047,12 +1103,25 @@ __global__ void __launch_bounds__(256) k_tc_build_w(const float2 *__restrict__ c
 // rows >= N are not touched.
 #define BW_SEG 8
 #define BW_ROWS 16
+struct BuildWArgs {
+    const float2 *cw, *uvc;
+    float pix;
+    int nuv, N, K2_pad;
+    void *w_hi, *w_lo;  // OT
+    DevScalars *sc;
+    GP_VGRID_FIELDS;
+};
+
 template <typename OT>
-__global__ void __launch_bounds__(256) k_tc_build_w_uv(const float2 *__restrict__ cw,
-                                                        const float2 *__restrict__ uvc, float pix, int nuv, int N,
-                                                        int K2_pad, OT *__restrict__ w_hi,
-                                                        OT *__restrict__ w_lo, DevScalars *__restrict__ sc)
+__device__ __forceinline__ void tc_build_w_uv_body(const BuildWArgs &A, const GpVGrid &vg)
 {
+    const float2 *__restrict__ cw = A.cw;
+    const float2 *__restrict__ uvc = A.uvc;
+    const float pix = A.pix;
+    const int nuv = A.nuv, N = A.N, K2_pad = A.K2_pad;
+    OT *__restrict__ w_hi = (OT *)A.w_hi;
+    OT *__restrict__ w_lo = (OT *)A.w_lo;
+    DevScalars *__restrict__ sc = A.sc;
     __shared__ __align__(16) float2 rp[BW_SEG][128];
     const double cmax = sc->cmax;
     int ex = 0;
@@ -1061,9 +1130,9 @@ __global__ void __launch_bounds__(256) k_tc_build_w_uv(const float2 *__restrict_
         frexp(cmax * 1.4143, &ex);
         wscale = ldexpf(1.f, 15 - ex);
     }
-    if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0)
+    if (vg.bx == 0 && vg.by == 0 && threadIdx.x == 0)
         sc->gscale = 1.0 / ((double)wscale * (double)(1 << TC_TW_LOG2));
-    const int kbase = blockIdx.x * 128;
+    const int kbase = vg.bx * 128;
     for (int e = threadIdx.x; e < BW_SEG * 128; e += blockDim.x) {
         const int j = e >> 7, k = kbase + (e & 127);
         float2 r = make_float2(1.f, 0.f);
@@ -1078,8 +1147,8 @@ __global__ void __launch_bounds__(256) k_tc_build_w_uv(const float2 *__restrict_
     }
     __syncthreads();
     const int lane = threadIdx.x & 31;
-    const int g = blockIdx.x * 32 + lane;
-    const int y0 = (blockIdx.y * 8 + (threadIdx.x >> 5)) * BW_ROWS;
+    const int g = vg.bx * 32 + lane;
+    const int y0 = (vg.by * 8 + (threadIdx.x >> 5)) * BW_ROWS;
     if (8 * g >= K2_pad || y0 >= N) return;
     float2 cs[4], an[4];
     double tv[4];
@@ -1135,6 +1204,17 @@ __global__ void __launch_bounds__(256) k_tc_build_w_uv(const float2 *__restrict_
         }
     }
 }
+
+template <typename OT>
+__global__ void __launch_bounds__(256) k_tc_build_w_uv(const BuildWArgs a)
+{
+    tc_build_w_uv_body<OT>(a, gp_vgrid_hw());
+}
+
+template <typename OT> struct BuildWOp {
+    using Args = BuildWArgs;
+    static __device__ __forceinline__ void run(const Args &a, const GpVGrid &v) { tc_build_w_uv_body<OT>(a, v); }
+};
 
 // ------------------------------------------------------------ host side
 
@@ -1379,6 +1459,8 @@ int gp_tc_prepare(gpair_ctx *c)
     if ((rc = tc_set_smem<EPI_STORE, 1, 0>(c))) return rc;
     if ((rc = tc_set_smem<EPI_FWD, 0, 1>(c))) return rc;
     if ((rc = tc_set_smem<EPI_FWD, 1, 1>(c))) return rc;
+    if ((rc = tc_set_smem<EPI_STORE, 0, 1>(c))) return rc;
+    if ((rc = tc_set_smem<EPI_STORE, 1, 1>(c))) return rc;
     t->npairs = t->nsm / 2;
     if (pair) {
         // clusters of two that can be resident at once (an SM left over in a GPC cannot host a pair)
@@ -1528,37 +1610,52 @@ static TcMaps tc_fwd_maps(const TcState *t, bool batch)
 // Row-wise prep launches (k_tc_prep_rows): PR_THREADS threads per block, R rows
 // per block and pass; at most GP_MAX_PARTIALS blocks (three partials each fit
 // the RED_PREP slot), a batch at most 1024 per trial (two partials each).
-template <typename OT, int MODE>
-static void tc_prep_rows_kernel(gpair_ctx *c, TcState *t, dim3 g, int W, const float *img, float *dst, int reduce,
-                                double *partials)
-{
-    const bool b = MODE == 2;
-    k_tc_prep_rows<OT, MODE><<<g, PR_THREADS, 0, c->stream>>>(
-        img, c->descent_dir, dst, c->model, c->N, W, b ? t->Lb : 0, t->Kx_pad, (OT *)(b ? t->imgb_hi : t->img_hi),
-        (OT *)(b ? t->imgb_lo : t->img_lo), (uint8_t *)(b ? t->imgb8h : t->img8h),
-        (uint8_t *)(b ? t->imgb8l : t->img8l), b ? t->rscb : t->rsc, reduce, partials, c->sc,
-        b ? c->gate : nullptr);
-}
-
-static int tc_prep_rows_launch(gpair_ctx *c, TcState *t, int mode, int reduce, double *partials,
-                               const float *img = nullptr)
+static PrepRowsArgs tc_prep_rows_args(gpair_ctx *c, TcState *t, int mode, int reduce, double *partials,
+                                      const float *img)
 {
     const int W = pr_warps_per_row(c->N), R = PR_WARPS_MAX / W;
     int gx = gp_cdiv(c->N, R);
     const int cap = mode == 2 ? 1024 : GP_MAX_PARTIALS;
     if (gx > cap) gx = cap;
     if (gx < 1) gx = 1;
-    const dim3 g(gx, mode == 2 ? GP_NTR : 1, 1);
-    const bool f16 = t->op == OP_F16;
-    if (mode == 0) {
-        if (f16) tc_prep_rows_kernel<__half, 0>(c, t, g, W, img, nullptr, reduce, partials);
-        else tc_prep_rows_kernel<float, 0>(c, t, g, W, img, nullptr, reduce, partials);
-    } else if (mode == 1) {
-        if (f16) tc_prep_rows_kernel<__half, 1>(c, t, g, W, c->image, c->image_temp, 1, partials);
-        else tc_prep_rows_kernel<float, 1>(c, t, g, W, c->image, c->image_temp, 1, partials);
+    const bool b = mode == 2;
+    PrepRowsArgs a;
+    memset(&a, 0, sizeof(a));
+    a.img = mode == 0 ? img : c->image;
+    a.d = c->descent_dir;
+    a.dst = mode == 1 ? c->image_temp : mode == 2 ? c->image_trials : nullptr;
+    a.model = c->model;
+    a.N = c->N;
+    a.W = W;
+    a.Lpad = b ? t->Lb : 0;
+    a.Kx_pad = t->Kx_pad;
+    a.hi = b ? t->imgb_hi : t->img_hi;
+    a.lo = b ? t->imgb_lo : t->img_lo;
+    a.h8 = (uint8_t *)(b ? t->imgb8h : t->img8h);
+    a.l8 = (uint8_t *)(b ? t->imgb8l : t->img8l);
+    a.rsc = b ? t->rscb : t->rsc;
+    a.reduce = mode ? 1 : reduce;
+    a.partials = partials;
+    a.sc = c->sc;
+    a.gate = b ? c->gate : nullptr;
+    a.nbx = gx;
+    a.nby = b ? GP_NTR : 1;
+    return a;
+}
+
+static int tc_prep_rows_launch(gpair_ctx *c, TcState *t, int mode, int reduce, double *partials,
+                               const float *img = nullptr)
+{
+    const PrepRowsArgs a = tc_prep_rows_args(c, t, mode, reduce, partials, img);
+    const dim3 g(a.nbx, a.nby, 1);
+    if (t->op == OP_F16) {
+        if (mode == 0) k_tc_prep_rows<__half, 0><<<g, PR_THREADS, 0, c->stream>>>(a);
+        else if (mode == 1) k_tc_prep_rows<__half, 1><<<g, PR_THREADS, 0, c->stream>>>(a);
+        else k_tc_prep_rows<__half, 2><<<g, PR_THREADS, 0, c->stream>>>(a);
     } else {
-        if (f16) tc_prep_rows_kernel<__half, 2>(c, t, g, W, c->image, c->image_trials, 1, partials);
-        else tc_prep_rows_kernel<float, 2>(c, t, g, W, c->image, c->image_trials, 1, partials);
+        if (mode == 0) k_tc_prep_rows<float, 0><<<g, PR_THREADS, 0, c->stream>>>(a);
+        else if (mode == 1) k_tc_prep_rows<float, 1><<<g, PR_THREADS, 0, c->stream>>>(a);
+        else k_tc_prep_rows<float, 2><<<g, PR_THREADS, 0, c->stream>>>(a);
     }
     GP_LAUNCH_CHECK(c);
     return GPAIR_OK;
@@ -1706,14 +1803,20 @@ int gp_tc_prep_split_trial(gpair_ctx *c)
     return tc_prep_rows_launch(c, t, 1, 1, c->partials);
 }
 
+// 32 groups of 4 uv points x 8 warps of BW_ROWS rows per block
+static BuildWArgs tc_build_w_args(gpair_ctx *c, TcState *t)
+{
+    BuildWArgs a = {c->cw, c->uvc, c->pix, c->nuv, c->N, t->K2_pad, t->w_hi, t->w_lo, c->sc,
+                    gp_cdiv(t->K2_pad / 8, 32), gp_cdiv(c->N, 8 * BW_ROWS)};
+    return a;
+}
+
 template <typename OT>
 static void launch_build_w(gpair_ctx *c, TcState *t)
 {
     if (c->have_uv) {
-        // 32 groups of 4 uv points x 8 warps of BW_ROWS rows per block
-        dim3 g(gp_cdiv(t->K2_pad / 8, 32), gp_cdiv(c->N, 8 * BW_ROWS));
-        k_tc_build_w_uv<OT><<<g, 256, 0, c->stream>>>(c->cw, c->uvc, c->pix, c->nuv, c->N, t->K2_pad,
-                                                       (OT *)t->w_hi, (OT *)t->w_lo, c->sc);
+        const BuildWArgs a = tc_build_w_args(c, t);
+        k_tc_build_w_uv<OT><<<dim3(a.nbx, a.nby), 256, 0, c->stream>>>(a);
     } else {
         dim3 g(gp_cdiv(c->nuv ? c->nuv : 1, 32), gp_cdiv(c->N, 32));
         k_tc_build_w<OT><<<g, 256, 0, c->stream>>>(c->cw, nullptr, c->fy, c->pix, c->nuv, c->N, t->K2_pad,
@@ -1772,7 +1875,7 @@ int gp_tc_adjoint(gpair_ctx *c, int which)
 // TcGroupInst array in global memory, share the persistent CTAs (or CTA pairs).
 // All instances use the same operand kind, product count and tile layout.
 struct TcGroup {
-    int n, op, nprod, pair, npairs, nsm;  // op: the forward's operand kind
+    int n, epi, op, nprod, pair, npairs, nsm;  // op: the operand kind of the contraction (the forward's: fop)
     TcGroupInst *d_inst;  // [n], device
     CUtensorMap map0;     // a valid map for the kernel's unused map parameters
     const int *gate;      // [n], device, owned by the caller
@@ -1797,13 +1900,68 @@ int gp_tc_group_key(gpair_ctx *c)
     return (fop * 4 + nprod) * 2 + (c->tc_pair ? 1 : 0);
 }
 
-// Builds the group of ctx[0..n-1] (their tensor state and batch buffers are
-// allocated here if needed). GPAIR_ERR_STATE when the instances cannot share
-// one launch (a CUDA-core instance, or another operand kind or tile layout).
-int gp_tc_group_build(gpair_ctx **ctx, int n, const int *gate, unsigned int *err, void **out)
+// one instance's entry of a grouped contraction of kind GP_TCG_*
+static void tc_group_inst(gpair_ctx *c, TcState *t, int kind, TcGroupInst &g)
+{
+    const int mt = t->pair ? 256 : TC_BM;
+    if (kind == GP_TCG_ADJOINT) {
+        g.A_hi = t->m_fxt_hi;
+        g.A_lo = t->m_fxt_lo;
+        g.A_x = t->m_fxt_hi;
+        g.B_hi = t->m_w_hi;
+        g.B_lo = t->m_w_lo;
+        g.B_x = t->m_w_hi;
+        g.m_tiles = t->xrows_pad / mt;
+        g.n_tiles = t->M_pad / TC_BN;
+        g.kb_total = t->K2_pad / t->bk;
+        g.kb_per_split = t->kb_per;
+        g.units = g.m_tiles * g.n_tiles * t->splits;
+        g.gpart = c->gpart;
+        g.out_ld = c->N;
+        g.out_rows = c->N;
+        g.out_cols = c->N;
+        return;
+    }
+    const bool batch = kind == GP_TCG_TRIALS;
+    const TcMaps fm = tc_fwd_maps(t, batch);
+    g.A_hi = *fm.a_hi;
+    g.A_lo = *fm.a_lo;
+    g.A_x = *fm.a_x;
+    g.B_hi = *fm.b_hi;
+    g.B_lo = *fm.b_lo;
+    g.B_x = *fm.b_x;
+    g.m_tiles = t->rows_pad / mt;
+    g.n_tiles = batch ? (GP_NTR * t->Lb) / TC_BN : t->M_pad / TC_BN;
+    g.kb_total = t->Kx_pad / t->bk;
+    g.kb_per_split = g.kb_total;
+    g.units = g.m_tiles * g.n_tiles;
+    g.fya = t->fya;
+    g.fyr = t->fyr;
+    g.nanc = t->nanc;
+    g.nuv = c->nuv;
+    if (batch) {
+        g.lpad = t->Lb;
+        const int erows = t->Lb < TC_BN ? t->Lb : TC_BN;
+        g.elog2 = erows == 32 ? 5 : erows == 64 ? 6 : erows == 128 ? 7 : 8;
+        g.rsc = t->rscb;
+        g.vpart = c->vpart_b;
+    } else {
+        g.lpad = t->M_pad;  // one image, partial entries of one 256-row tile each
+        g.elog2 = 8;
+        g.rsc = t->rsc;
+        g.vpart = c->vpart;
+    }
+}
+
+// Builds the group of ctx[0..n-1] for a contraction of kind GP_TCG_* (their
+// tensor state and batch buffers are allocated here if needed).
+// GPAIR_ERR_STATE when the instances cannot share one launch (a CUDA-core
+// instance, or another operand kind or tile layout).
+int gp_tc_group_build_kind(gpair_ctx **ctx, int n, int kind, const int *gate, unsigned int *err, void **out)
 {
     *out = nullptr;
     if (n <= 0 || n > TC_GROUP_MAX) return GPAIR_ERR_STATE;
+    if (kind < GP_TCG_TRIALS || kind > GP_TCG_ADJOINT) return GPAIR_ERR_INVALID;
     TcGroupInst *h = (TcGroupInst *)calloc((size_t)n, sizeof(TcGroupInst));
     if (!h) return GPAIR_ERR_ALLOC;
     int rc = GPAIR_OK;
@@ -1816,33 +1974,13 @@ int gp_tc_group_build(gpair_ctx **ctx, int n, const int *gate, unsigned int *err
         }
         TcState *t = tc_state_ready(c, &rc);
         if (rc) break;
-        if ((rc = gp_batch_alloc(c))) break;
+        if (kind == GP_TCG_TRIALS && (rc = gp_batch_alloc(c))) break;
         if (t0 && (t->fop != t0->fop || t->nprod != t0->nprod || t->pair != t0->pair)) {
             rc = GPAIR_ERR_STATE;
             break;
         }
         if (!t0) t0 = t;
-        TcGroupInst &g = h[i];
-        const TcMaps fm = tc_fwd_maps(t, true);
-        g.A_hi = *fm.a_hi;
-        g.A_lo = *fm.a_lo;
-        g.A_x = *fm.a_x;
-        g.B_hi = *fm.b_hi;
-        g.B_lo = *fm.b_lo;
-        g.B_x = *fm.b_x;
-        g.m_tiles = t->rows_pad / (t->pair ? 256 : TC_BM);
-        g.n_tiles = (GP_NTR * t->Lb) / TC_BN;
-        g.kb_total = t->Kx_pad / t->bk;
-        g.units = g.m_tiles * g.n_tiles;
-        g.fya = t->fya;
-        g.fyr = t->fyr;
-        g.nanc = t->nanc;
-        g.nuv = c->nuv;
-        g.lpad = t->Lb;
-        const int erows = t->Lb < TC_BN ? t->Lb : TC_BN;
-        g.elog2 = erows == 32 ? 5 : erows == 64 ? 6 : erows == 128 ? 7 : 8;
-        g.rsc = t->rscb;
-        g.vpart = c->vpart_b;
+        tc_group_inst(c, t, kind, h[i]);
     }
     TcGroup *G = nullptr;
     if (!rc) {
@@ -1851,7 +1989,8 @@ int gp_tc_group_build(gpair_ctx **ctx, int n, const int *gate, unsigned int *err
     }
     if (!rc) {
         G->n = n;
-        G->op = t0->fop;
+        G->epi = kind == GP_TCG_ADJOINT ? EPI_STORE : EPI_FWD;
+        G->op = kind == GP_TCG_ADJOINT ? t0->op : t0->fop;
         G->nprod = t0->nprod;
         G->pair = t0->pair;
         G->npairs = t0->npairs;
@@ -1862,7 +2001,7 @@ int gp_tc_group_build(gpair_ctx **ctx, int n, const int *gate, unsigned int *err
         gpair_ctx *c = ctx[0];
         if (cudaMalloc(&G->d_inst, sizeof(TcGroupInst) * (size_t)n) != cudaSuccess ||
             cudaMemcpy(G->d_inst, h, sizeof(TcGroupInst) * (size_t)n, cudaMemcpyHostToDevice) != cudaSuccess) {
-            snprintf(c->last_error, sizeof(c->last_error), "grouped forward: device arrays");
+            snprintf(c->last_error, sizeof(c->last_error), "grouped contraction: device arrays");
             rc = GPAIR_ERR_CUDA;
         }
     }
@@ -1875,7 +2014,12 @@ int gp_tc_group_build(gpair_ctx **ctx, int n, const int *gate, unsigned int *err
     return GPAIR_OK;
 }
 
-template <int PAIR>
+int gp_tc_group_build(gpair_ctx **ctx, int n, const int *gate, unsigned int *err, void **out)
+{
+    return gp_tc_group_build_kind(ctx, n, GP_TCG_TRIALS, gate, err, out);
+}
+
+template <int EPI, int PAIR>
 static cudaError_t tc_group_launch_kind(TcGroup *G, cudaStream_t st, const TcArgs &a)
 {
     cudaLaunchConfig_t cfg;
@@ -1892,17 +2036,17 @@ static cudaError_t tc_group_launch_kind(TcGroup *G, cudaStream_t st, const TcArg
     cfg.attrs = at;
     cfg.numAttrs = PAIR ? 1 : 0;
     const CUtensorMap &m = G->map0;
-    if (G->op == OP_F16F8)
+    if (EPI == EPI_FWD && G->op == OP_F16F8)
         return cudaLaunchKernelEx(&cfg, k_tc_gemm<EPI_FWD, OP_F16F8, 3, PAIR, 1>, m, m, m, m, m, m, a);
-    if (G->op == OP_F16) return cudaLaunchKernelEx(&cfg, k_tc_gemm<EPI_FWD, OP_F16, 3, PAIR, 1>, m, m, m, m, m, m, a);
-    if (G->nprod == 3)
-        return cudaLaunchKernelEx(&cfg, k_tc_gemm<EPI_FWD, OP_TF32, 3, PAIR, 1>, m, m, m, m, m, m, a);
-    return cudaLaunchKernelEx(&cfg, k_tc_gemm<EPI_FWD, OP_TF32, 1, PAIR, 1>, m, m, m, m, m, m, a);
+    if (G->op == OP_F16) return cudaLaunchKernelEx(&cfg, k_tc_gemm<EPI, OP_F16, 3, PAIR, 1>, m, m, m, m, m, m, a);
+    if (G->nprod == 3) return cudaLaunchKernelEx(&cfg, k_tc_gemm<EPI, OP_TF32, 3, PAIR, 1>, m, m, m, m, m, m, a);
+    return cudaLaunchKernelEx(&cfg, k_tc_gemm<EPI, OP_TF32, 1, PAIR, 1>, m, m, m, m, m, m, a);
 }
 
-// the grouped forward of every gated instance, on c's stream (persistent: one
-// CTA per SM or one pair per two SMs, whatever the number of gated units)
-int gp_tc_group_forward(void *grp, gpair_ctx *c)
+// the grouped contraction of every gated instance, on stream st (persistent:
+// one CTA per SM or one pair per two SMs, whatever the number of gated units);
+// c gives the wait budget and the failure-test switch
+int gp_tc_group_run(void *grp, gpair_ctx *c, cudaStream_t st)
 {
     TcGroup *G = (TcGroup *)grp;
     TcArgs a;
@@ -1913,11 +2057,95 @@ int gp_tc_group_forward(void *grp, gpair_ctx *c)
     a.err = G->err;
     a.budget = c->tc_wait_budget > 0 ? c->tc_wait_budget : TC_WAIT_BUDGET;
     a.skip_loads = c->tc_skip_loads;
-    cudaError_t e = G->pair ? tc_group_launch_kind<1>(G, c->stream, a) : tc_group_launch_kind<0>(G, c->stream, a);
+    cudaError_t e;
+    if (G->epi == EPI_STORE)
+        e = G->pair ? tc_group_launch_kind<EPI_STORE, 1>(G, st, a) : tc_group_launch_kind<EPI_STORE, 0>(G, st, a);
+    else
+        e = G->pair ? tc_group_launch_kind<EPI_FWD, 1>(G, st, a) : tc_group_launch_kind<EPI_FWD, 0>(G, st, a);
     if (e != cudaSuccess) {
         snprintf(c->last_error, sizeof(c->last_error), "grouped contraction launch: %s", cudaGetErrorString(e));
         return GPAIR_ERR_CUDA;
     }
     c->launches++;
     return GPAIR_OK;
+}
+
+int gp_tc_group_forward(void *grp, gpair_ctx *c) { return gp_tc_group_run(grp, c, c->stream); }
+
+// ------------------------------------------------- grouped stage launches
+//
+// The tensor path's own stages of a lockstep iteration as one launch over all
+// instances (group.cuh): the current image's prep (flux, regulariser, max and
+// forward operand), the batched trials' prep, and the adjoint weight operand.
+
+int gp_tc_stage_sizes(gpair_ctx *c, int *mt, int *splits)
+{
+    int rc;
+    TcState *t = tc_state_ready(c, &rc);
+    if (rc) return rc;
+    if (mt) *mt = t->M_pad / TC_BN;
+    if (splits) *splits = t->splits;
+    return GPAIR_OK;
+}
+
+size_t gp_tc_stage_args_size(int stage)
+{
+    switch (stage) {
+    case GS_PREP_IMAGE:
+    case GS_PREP_TRIALS: return sizeof(PrepRowsArgs);
+    case GS_BUILD_W: return sizeof(BuildWArgs);
+    default: return 0;
+    }
+}
+
+int gp_tc_stage_args(gpair_ctx *c, int stage, void *out, int *nblocks, int *op)
+{
+    int rc;
+    TcState *t = tc_state_ready(c, &rc);
+    if (rc) return rc;
+    *op = t->op;
+    if (stage == GS_PREP_IMAGE || stage == GS_PREP_TRIALS) {
+        if (stage == GS_PREP_TRIALS && (rc = gp_tc_batch_prepare(c, nullptr))) return rc;
+        const PrepRowsArgs a = stage == GS_PREP_IMAGE ? tc_prep_rows_args(c, t, 0, 1, c->partials, c->image)
+                                                      : tc_prep_rows_args(c, t, 2, 1, c->partials_b, nullptr);
+        memcpy(out, &a, sizeof(a));
+        *nblocks = a.nbx * a.nby;
+        return GPAIR_OK;
+    }
+    if (stage == GS_BUILD_W) {
+        if (!c->have_uv) return GPAIR_ERR_STATE;  // the table-only path reads Fy from its table
+        const BuildWArgs a = tc_build_w_args(c, t);
+        memcpy(out, &a, sizeof(a));
+        *nblocks = a.nbx * a.nby;
+        return GPAIR_OK;
+    }
+    return GPAIR_ERR_INVALID;
+}
+
+template <class Op, int THREADS>
+static int tc_group_stage(gpair_ctx *c, const void *d_args, const int *d_start, int n, int total, const int *gate)
+{
+    k_grouped<Op, THREADS>
+        <<<total, THREADS, 0, c->stream>>>((const typename Op::Args *)d_args, d_start, n, gate);
+    GP_LAUNCH_CHECK(c);
+    return GPAIR_OK;
+}
+
+int gp_tc_stage_group_launch(gpair_ctx *c, int stage, int op, const void *d_args, const int *d_start, int n,
+                             int total, const int *gate)
+{
+    if (total < 1 || n < 1) return GPAIR_ERR_INVALID;
+    const bool f16 = op == OP_F16;
+    switch (stage) {
+    case GS_PREP_IMAGE:
+        return f16 ? tc_group_stage<PrepRowsOp<__half, 0>, PR_THREADS>(c, d_args, d_start, n, total, gate)
+                   : tc_group_stage<PrepRowsOp<float, 0>, PR_THREADS>(c, d_args, d_start, n, total, gate);
+    case GS_PREP_TRIALS:
+        return f16 ? tc_group_stage<PrepRowsOp<__half, 2>, PR_THREADS>(c, d_args, d_start, n, total, gate)
+                   : tc_group_stage<PrepRowsOp<float, 2>, PR_THREADS>(c, d_args, d_start, n, total, gate);
+    case GS_BUILD_W:
+        return f16 ? tc_group_stage<BuildWOp<__half>, 256>(c, d_args, d_start, n, total, gate)
+                   : tc_group_stage<BuildWOp<float>, 256>(c, d_args, d_start, n, total, gate);
+    default: return GPAIR_ERR_INVALID;
+    }
 }

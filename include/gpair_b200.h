@@ -364,18 +364,27 @@ int gpair_cg_checkpoint_load(gpair_ctx *ctx, const void *buffer, size_t bytes);
  * per-context results; each context's last_run_stats holds the batch's device time.
  *
  * Lockstep batches (the default of gpair_batch_create when line_search is
- * GPAIR_LS_BATCH, every context is on a tensor-core path with the same operand kind
- * and tile layout, and n <= 256): the reconstructions advance one CG step at a
- * time together, and each batched line-search evaluation runs the forward DFTs of
- * the trial images of every instance still searching as ONE grouped tcgen05 launch
- * (per-instance operand maps and epilogue arguments in device memory). Each
- * instance's results are bitwise those of its separate run. Otherwise, or with
- * GPAIR_BATCH_INDEPENDENT, every context's loop is an independent graph branch.
- * gpair_batch_grouped tells which one was built. gpair_batch_run returns
- * GPAIR_ERR_STATE when a context's operand or batch buffers were rebuilt since the
- * batch was created (another precision, tile layout, problem or image size). */
+ * GPAIR_LS_BATCH and some context is on a tensor-core path): the reconstructions
+ * advance one CG step at a time together.
+ *   Staged (gpair_batch_grouped = 2; every context on a tensor-core path with one
+ *   operand element type -- f16 or TF32 -- and given by (u, v), n <= 4096): every
+ *   stage of an iteration (image prep, V2/T3/chi2, adjoint weights and operand,
+ *   gradient, direction, trial prep, trial chi2, image update, controller) is ONE
+ *   launch over all instances, and every contraction (criterion forward, adjoint,
+ *   trial forward) one grouped tcgen05 launch per class of contexts with the same
+ *   operand kind, product count and tile layout (at most 256 per launch), with
+ *   per-instance operand maps and arguments in device memory.
+ *   Forwards only (gpair_batch_grouped = 1; otherwise, or with
+ *   GPAIR_BATCH_FORWARDS_ONLY): each instance runs its own stage kernels; the
+ *   trial forwards of every tensor-core class are grouped launches.
+ * Each instance's results are bitwise those of its separate run. Otherwise, or with
+ * GPAIR_BATCH_INDEPENDENT, every context's loop is an independent graph branch
+ * (gpair_batch_grouped = 0). gpair_batch_run returns GPAIR_ERR_STATE when a
+ * context's operand or batch buffers were rebuilt since the batch was created
+ * (another precision, tile layout, problem or image size). */
 typedef struct gpair_batch gpair_batch;
 #define GPAIR_BATCH_INDEPENDENT 1
+#define GPAIR_BATCH_FORWARDS_ONLY 2
 int gpair_batch_create(gpair_batch **batch, gpair_ctx **ctx, int n, int line_search);
 int gpair_batch_create_ex(gpair_batch **batch, gpair_ctx **ctx, int n, int line_search, int flags);
 int gpair_batch_grouped(const gpair_batch *batch);

@@ -106,3 +106,31 @@ def test_reference_arm_maps_no_library_of_this_project():
     assert line["cpu_baseline"]["value"] == line["value"]
     assert line["e2e"] == {"value": line["value"], "unit": line["unit"], "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}
+
+
+def test_small_workload_reference_cg_runs_on_the_reference_code():
+    """The CPU side of the 64x64 plain-method block: the reference's own compiled
+    code builds the data (getoifits.c, init_data, set_model) at the workload's
+    own size, and a few CG iterations through its cpu.c descend from the flat
+    start."""
+    import os
+
+    import pytest
+
+    from oracle import oracle as O
+
+    if not os.path.exists(O.REF_LIB) or not os.path.exists(O.REF_MAIN_LIB):
+        pytest.skip("reference library not built")
+    ref = bench.reference_problem("small")
+    assert ref["width"] == 64 and ref["npow"] == 900 and ref["nbis"] == 600
+    saved = os.dup(1)
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)  # cpu.c's image2vis prints on every call
+    try:
+        out = bench.small_plain_cg_cpu(3)
+    finally:
+        os.dup2(saved, 1)
+        os.close(saved)
+        os.close(devnull)
+    assert out["kind"] == "reference" and out["cores"] == 1
+    assert out["grad_evals"] >= 3 and out["J"] > 0

@@ -898,27 +898,38 @@ def test_alternating_line_searches_reuse_their_graphs(rec):
     assert outs[1]["criterion_evals"] % g.LS_TRIALS == 3 % g.LS_TRIALS
 
 
-@pytest.mark.parametrize("ls,independent,pair,mixed,prec", [
-    (0, False, True, False, g.PREC_SPLIT16), (1, True, True, False, g.PREC_SPLIT16),
-    (1, False, True, False, g.PREC_SPLIT16), (1, False, False, False, g.PREC_SPLIT16),
-    (1, False, True, True, g.PREC_SPLIT16), (1, False, True, False, g.PREC_SPLIT16F8)])
-def test_batch_graph_equals_separate_runs(ls, independent, pair, mixed, prec):
+@pytest.mark.parametrize("ls,independent,pair,mixed,prec,fwd_only,layout", [
+    (0, False, True, None, g.PREC_SPLIT16, False, 0),
+    (1, True, True, None, g.PREC_SPLIT16, False, 0),
+    (1, False, True, None, g.PREC_SPLIT16, False, 2),
+    (1, False, True, None, g.PREC_SPLIT16, True, 1),
+    (1, False, False, None, g.PREC_SPLIT16, False, 2),
+    (1, False, "alt", None, g.PREC_SPLIT16, False, 2),
+    (1, False, True, g.PREC_FP32, g.PREC_SPLIT16, False, 1),
+    (1, False, True, g.PREC_TF32X3, g.PREC_SPLIT16, False, 1),
+    (1, False, True, None, g.PREC_TF32X3, False, 2),
+    (1, False, True, g.PREC_SPLIT16, g.PREC_SPLIT16F8, False, 2),
+    (1, False, True, None, g.PREC_SPLIT16F8, True, 1)])
+def test_batch_graph_equals_separate_runs(ls, independent, pair, mixed, prec, fwd_only, layout):
     """Consistency check (library against itself; single runs are oracle-pinned by
     the CG tests above): gpair_batch_*, one graph, one launch; the results are the
     separate runs' bit for bit, twice in a row (the graph is reused). With the
-    batched line search the instances run in lockstep and each batched evaluation's
-    forwards are one grouped tcgen05 launch per class of tensor instances (CTA
-    pairs or single CTAs); an instance on the CUDA-core path (mixed) keeps its own
-    evaluation in the lockstep graph; with independent=True every CG loop is an
-    independent branch."""
+    batched line search the instances run in lockstep. Staged (layout 2): every
+    stage is one launch over all instances and every contraction one grouped
+    tcgen05 launch per class (CTA pairs, single CTAs, both ("alt"), f16 and E4M3
+    operand classes side by side, TF32). Forwards only (layout 1: requested, or
+    one instance on another operand element type -- the CUDA cores or TF32 beside
+    f16): each instance keeps its own stage kernels and the trial forwards are
+    grouped per class. With independent=True every CG loop is an independent
+    branch (layout 0)."""
     from gpair_b200.instances import instance
     ps = [instance(20_000_000 + k) for k in range(4)]
     recs = [g.Reconstructor(0) for _ in ps]
     try:
         for k, (r, p) in enumerate(zip(recs, ps)):
-            r.set_tc_pair(pair)
+            r.set_tc_pair(bool(k % 2) if pair == "alt" else pair)
             r.set_problem(p)
-            r.set_precision(g.PREC_FP32 if (mixed and k == 1) else prec)
+            r.set_precision(mixed if (mixed is not None and k == 1) else prec)
         singles, imgs = [], []
         for r, p in zip(recs, ps):
             r.set_image(p.start_image())
@@ -926,8 +937,8 @@ def test_batch_graph_equals_separate_runs(ls, independent, pair, mixed, prec):
             imgs.append(r.get_image())
         for r, p in zip(recs, ps):
             r.set_image(p.start_image())
-        with g.api.Batch(recs, line_search=ls, independent=independent) as b:
-            assert b.grouped == (ls == 1 and not independent)
+        with g.api.Batch(recs, line_search=ls, independent=independent, forwards_only=fwd_only) as b:
+            assert b.grouped == layout
             for rep in range(2):
                 for r, p in zip(recs, ps):
                     r.set_image(p.start_image())
@@ -941,11 +952,13 @@ def test_batch_graph_equals_separate_runs(ls, independent, pair, mixed, prec):
             r.close()
 
 
-def test_grouped_batch_wait_timeout_is_reported_and_recovers():
-    """The grouped forward's bounded waits run out (built from a first context whose
-    producer issues no TMA loads): every instance's run ends with GPAIR_ERR_TIMEOUT
-    instead of hanging; rebuilt with the normal wait, the same contexts give the
-    separate runs' results bit for bit."""
+@pytest.mark.parametrize("fwd_only", [False, True])
+def test_grouped_batch_wait_timeout_is_reported_and_recovers(fwd_only):
+    """The grouped contractions' bounded waits run out (built from a first context
+    whose producer issues no TMA loads; staged: already the criterion forward,
+    forwards only: the trial forward): every instance's run ends with
+    GPAIR_ERR_TIMEOUT instead of hanging; rebuilt with the normal wait, the same
+    contexts give the separate runs' results bit for bit."""
     from gpair_b200.instances import instance
     ps = [instance(20_000_100 + k) for k in range(3)]
     recs = [g.Reconstructor(0) for _ in ps]
@@ -963,15 +976,15 @@ def test_grouped_batch_wait_timeout_is_reported_and_recovers():
         try:
             for r, p in zip(recs, ps):
                 r.set_image(p.start_image())
-            with g.api.Batch(recs, line_search=g.LS_BATCH) as b:
-                assert b.grouped
+            with g.api.Batch(recs, line_search=g.LS_BATCH, forwards_only=fwd_only) as b:
+                assert b.grouped == (1 if fwd_only else 2)
                 with pytest.raises(g.GpairError, match=r"\(-5\)"):
                     b.run(3)
         finally:
             assert L.gpair_set_tc_wait(recs[0].h, 0, 0) == 0
         for r, p in zip(recs, ps):
             r.set_image(p.start_image())
-        with g.api.Batch(recs, line_search=g.LS_BATCH) as b:
+        with g.api.Batch(recs, line_search=g.LS_BATCH, forwards_only=fwd_only) as b:
             out = b.run(3)
             for r, a, o, img in zip(recs, singles, out, imgs):
                 assert o["status"] == 0 and o["J"] == a["J"]
