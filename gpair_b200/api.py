@@ -139,6 +139,7 @@ def lib() -> C.CDLL:
         L.gpair_set_stage_timing.argtypes = [vp, i]
         L.gpair_set_tc_wait.argtypes = [vp, C.c_longlong, i]
         L.gpair_set_tc_pair.argtypes = [vp, i]
+        L.gpair_set_pdl.argtypes = [vp, i]
         L.gpair_get_tc_pair.argtypes = [vp]
         L.gpair_last_run_stage_ms.argtypes = [vp, C.POINTER(d), C.POINTER(i), i]
         L.gpair_get_oi_fits_data.argtypes = [i, f, f, i, vp, i, vp, i, vp, C.POINTER(OiData)]
@@ -455,6 +456,10 @@ class Reconstructor:
     def set_tc_pair(self, on: bool = True):
         """Tensor-core contractions on CTA pairs (cta_group::2) or single CTAs."""
         self._c(self._L.gpair_set_tc_pair(self.h, 1 if on else 0))
+
+    def set_pdl(self, on: bool = True):
+        """Programmatic dependent launches of the evaluation chain (default on)."""
+        self._c(self._L.gpair_set_pdl(self.h, 1 if on else 0))
 
     def set_precision(self, mode: int):
         self._c(self._L.gpair_set_precision(self.h, mode))

@@ -324,6 +324,7 @@ __global__ void k_lockstep_route(int what, DevScalars *const *__restrict__ scs, 
                                  const cudaGraphConditionalHandle *__restrict__ h_post,
                                  cudaGraphConditionalHandle h_any, unsigned int *__restrict__ gerr)
 {
+    gp_pdl_enter();
     __shared__ int any;
     if (threadIdx.x == 0) any = 0;
     __syncthreads();
@@ -408,9 +409,8 @@ static int lockstep_route(BatchGraph *B, gpair_ctx *c, int what, cudaGraphCondit
     int rc = capture_fn(
         c,
         [&]() {
-            k_lockstep_route<<<1, 256, 0, c->stream>>>(what, B->scs, n, B->flags, B->flags + n, B->hd, B->hd + n,
-                                                       h_any, B->gerr);
-            GP_LAUNCH_CHECK(c);
+            GP_LAUNCH(c, gp_launch(c, k_lockstep_route, dim3(1), dim3(256), 0, what, B->scs, n, B->flags,
+                                   B->flags + n, B->hd, B->hd + n, h_any, B->gerr));
             return GPAIR_OK;
         },
         &g, nullptr);
@@ -725,9 +725,9 @@ static int build_lockstep_staged(gpair_ctx **ctx_in, int n, BatchGraph *B)
         return GPAIR_OK;
     };
     auto route = [&](int what, cudaGraphConditionalHandle h) {
-        k_lockstep_route<<<1, 256, 0, c0->stream>>>(what, B->scs, n, B->flags, B->flags + n, nullptr, nullptr, h,
-                                                     B->gerr);
-        GP_LAUNCH_CHECK(c0);
+        GP_LAUNCH(c0, gp_launch(c0, k_lockstep_route, dim3(1), dim3(256), 0, what, B->scs, n, B->flags,
+                                B->flags + n, (const cudaGraphConditionalHandle *)nullptr,
+                                (const cudaGraphConditionalHandle *)nullptr, h, B->gerr));
         return GPAIR_OK;
     };
 

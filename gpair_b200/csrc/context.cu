@@ -122,6 +122,10 @@ extern "C" int gpair_create(gpair_ctx **out, int device)
     c->device = device;
     c->precision = GPAIR_PREC_FP32;
     c->tc_pair = 1;  // tensor-core contractions on CTA pairs (gpair_set_tc_pair)
+    {
+        const char *e = getenv("GPAIR_PDL");  // programmatic dependent launches (gpair_set_pdl)
+        c->pdl = (e && e[0] == '0') ? 0 : 1;
+    }
     c->fuse_ctrl = -1;
     c->last_image_src = -1;
     int rc = GPAIR_OK;
@@ -376,6 +380,14 @@ extern "C" int gpair_set_tc_pair(gpair_ctx *c, int on)
 }
 
 extern "C" int gpair_get_tc_pair(gpair_ctx *c) { return c ? c->tc_pair : -1; }
+
+extern "C" int gpair_set_pdl(gpair_ctx *c, int on)
+{
+    if (!c) return GPAIR_ERR_INVALID;
+    c->pdl = on ? 1 : 0;
+    gp_cg_graph_free(c);  // captured graphs hold the launch attribute
+    return GPAIR_OK;
+}
 
 extern "C" int gpair_set_tc_wait(gpair_ctx *c, long long budget_cycles, int skip_loads)
 {

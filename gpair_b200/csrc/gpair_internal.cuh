@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdio.h>
+#include <string.h>
 
 #include "gpair_b200.h"
 
@@ -313,6 +314,8 @@ struct gpair_ctx {
     unsigned int buf_gen;
     // tensor-core contractions on CTA pairs (tcgen05 cta_group::2) instead of single CTAs
     int tc_pair;
+    // programmatic dependent launches of the evaluation chain (gp_launch), default on
+    int pdl;
 };
 
 // ---------------------------------------------------------------- helpers
@@ -338,6 +341,60 @@ struct gpair_ctx {
     } while (0)
 
 static inline int gp_cdiv(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+// a launch through gp_launch / gp_launch_on (its own error return), then the usual check
+#define GP_LAUNCH(ctx, call)                                                                        \
+    do {                                                                                            \
+        cudaError_t le_ = (call);                                                                   \
+        if (le_ != cudaSuccess) {                                                                   \
+            snprintf((ctx)->last_error, sizeof((ctx)->last_error), "launch: %s (%s:%d)",           \
+                     cudaGetErrorString(le_), __FILE__, __LINE__);                                  \
+            return GPAIR_ERR_CUDA;                                                                  \
+        }                                                                                           \
+        GP_LAUNCH_CHECK(ctx);                                                                       \
+    } while (0)
+
+// ------------------------------------------ programmatic dependent launches
+//
+// The kernels of the evaluation chain are launched with programmatic stream
+// serialization (gp_launch, when c->pdl is set): the next kernel on the stream
+// is launched while the current one finishes, so that its launch and block
+// scheduling overlap the current kernel's tail instead of following it. Every
+// kernel launched this way waits (gp_pdl_wait: griddepcontrol.wait, the full
+// completion and memory flush of the kernel before it) before it reads or
+// writes global memory, and then lets its own dependent launch
+// (gp_pdl_trigger). Launched without the attribute, both are no-ops.
+__device__ __forceinline__ void gp_pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void gp_pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void gp_pdl_enter()
+{
+    gp_pdl_wait();
+    gp_pdl_trigger();
+}
+
+template <typename... KP, typename... A>
+static inline cudaError_t gp_launch_on(cudaStream_t st, int pdl, void (*k)(KP...), dim3 grid, dim3 block,
+                                       size_t smem, A &&...args)
+{
+    cudaLaunchConfig_t cfg;
+    memset(&cfg, 0, sizeof(cfg));
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, k, static_cast<A &&>(args)...);
+}
+
+template <typename... KP, typename... A>
+static inline cudaError_t gp_launch(gpair_ctx *c, void (*k)(KP...), dim3 grid, dim3 block, size_t smem, A &&...args)
+{
+    return gp_launch_on(c->stream, c->pdl, k, grid, block, smem, static_cast<A &&>(args)...);
+}
 
 // stage timing (context.cu): bracket the launches of one stage
 void gp_stage_begin(gpair_ctx *c, int stage);

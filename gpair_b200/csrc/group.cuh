@@ -11,6 +11,8 @@
 // body count their blocks against nbx (nby), never gridDim.
 #pragma once
 
+#include "gpair_internal.cuh"
+
 struct GpVGrid {
     int bx, by, nbx, nby;
 };
@@ -36,6 +38,7 @@ __global__ void __launch_bounds__(THREADS) k_grouped(const typename Op::Args *__
                                                      const int *__restrict__ start, int n,
                                                      const int *__restrict__ gate)
 {
+    gp_pdl_enter();  // after the kernel before it on the stream (programmatic dependent launch)
     const int b = (int)blockIdx.x;
     int lo = 0, hi = n;  // start[lo] <= b < start[hi]
     while (hi - lo > 1) {

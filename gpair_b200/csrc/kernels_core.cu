@@ -412,7 +412,11 @@ __device__ __forceinline__ void vis_data_body(const VisDataArgs &A, const GpVGri
 
 #undef VIS_AT
 
-__global__ void __launch_bounds__(GP_THREADS) k_vis_data(const VisDataArgs a) { vis_data_body(a, gp_vgrid_hw()); }
+__global__ void __launch_bounds__(GP_THREADS) k_vis_data(const VisDataArgs a)
+{
+    gp_pdl_enter();
+    vis_data_body(a, gp_vgrid_hw());
+}
 
 struct VisDataOp {
     using Args = VisDataArgs;
@@ -439,8 +443,7 @@ int gp_vis_data(gpair_ctx *c) { return vis_data_launch(c, 0); }
 static int vis_data_launch(gpair_ctx *c, int direct)
 {
     const VisDataArgs a = vis_data_args(c, direct, take_fused_ctrl(c));
-    k_vis_data<<<a.nbx, GP_THREADS, 0, c->stream>>>(a);
-    GP_LAUNCH_CHECK(c);
+    GP_LAUNCH(c, gp_launch(c, k_vis_data, dim3(a.nbx), dim3(GP_THREADS), 0, a));
     return GPAIR_OK;
 }
 
@@ -521,6 +524,7 @@ __device__ __forceinline__ void adj_weights_body(const AdjWeightsArgs &A, const 
 
 __global__ void __launch_bounds__(GP_THREADS) k_adj_weights(const AdjWeightsArgs a)
 {
+    gp_pdl_enter();
     adj_weights_body(a, gp_vgrid_hw());
 }
 
@@ -617,8 +621,7 @@ static int adj_splits(int N, int nuv)
 int gp_adj_weights_only(gpair_ctx *c)
 {
     const AdjWeightsArgs a = adj_weights_args(c);
-    k_adj_weights<<<a.nbx, GP_THREADS, 0, c->stream>>>(a);
-    GP_LAUNCH_CHECK(c);
+    GP_LAUNCH(c, gp_launch(c, k_adj_weights, dim3(a.nbx), dim3(GP_THREADS), 0, a));
     return GPAIR_OK;
 }
 
@@ -812,6 +815,7 @@ __device__ __forceinline__ void grad_finalize_body(const GradFinalizeArgs &A, co
 
 __global__ void __launch_bounds__(GP_THREADS) k_grad_finalize(const GradFinalizeArgs a)
 {
+    gp_pdl_enter();
     grad_finalize_body(a, gp_vgrid_hw());
 }
 
@@ -839,8 +843,7 @@ static GradFinalizeArgs grad_finalize_args(gpair_ctx *c, int which, int mode, fl
 int gp_grad_finalize(gpair_ctx *c, int which, int mode, float alpha)
 {
     const GradFinalizeArgs a = grad_finalize_args(c, which, mode, alpha, take_fused_ctrl(c));
-    k_grad_finalize<<<a.nbx, GP_THREADS, 0, c->stream>>>(a);
-    GP_LAUNCH_CHECK(c);
+    GP_LAUNCH(c, gp_launch(c, k_grad_finalize, dim3(a.nbx), dim3(GP_THREADS), 0, a));
     return GPAIR_OK;
 }
 
@@ -947,7 +950,11 @@ __device__ __forceinline__ void descent_body(const DescentArgs &A, const GpVGrid
     }
 }
 
-__global__ void __launch_bounds__(GP_THREADS) k_descent(const DescentArgs a) { descent_body(a, gp_vgrid_hw()); }
+__global__ void __launch_bounds__(GP_THREADS) k_descent(const DescentArgs a)
+{
+    gp_pdl_enter();
+    descent_body(a, gp_vgrid_hw());
+}
 
 struct DescentOp {
     using Args = DescentArgs;
@@ -964,8 +971,7 @@ static DescentArgs descent_args(gpair_ctx *c, int beta_from_state, double beta_h
 int gp_descent_dir(gpair_ctx *c, int beta_from_state, double beta_host)
 {
     const DescentArgs a = descent_args(c, beta_from_state, beta_host, take_fused_ctrl(c));
-    k_descent<<<a.nbx, GP_THREADS, 0, c->stream>>>(a);
-    GP_LAUNCH_CHECK(c);
+    GP_LAUNCH(c, gp_launch(c, k_descent, dim3(a.nbx), dim3(GP_THREADS), 0, a));
     return GPAIR_OK;
 }
 
@@ -999,6 +1005,7 @@ __global__ void __launch_bounds__(GP_THREADS) k_lbfgs_pair(const float *__restri
                                                            float *__restrict__ Y, int n, double *__restrict__ partials,
                                                            DevScalars *__restrict__ sc, FusedCtrl fc)
 {
+    gp_pdl_enter();
     __shared__ double smem[GP_LB_NPD * 32];
     const CgState &cs = sc->cg;
     const int active = cs.lb_xvalid;
@@ -1051,6 +1058,7 @@ __global__ void __launch_bounds__(GP_THREADS) k_lbfgs_dots(const float *__restri
                                                            int n, double *__restrict__ partials,
                                                            DevScalars *__restrict__ sc, FusedCtrl fc)
 {
+    gp_pdl_enter();
     __shared__ double smem[GP_LB_NQD * 32];
     const CgState &cs = sc->cg;
     const int m = cs.lb_count;
@@ -1102,6 +1110,7 @@ __global__ void __launch_bounds__(GP_THREADS) k_lbfgs_combine(const float *__res
                                                               double *__restrict__ partials,
                                                               DevScalars *__restrict__ sc, FusedCtrl fc)
 {
+    gp_pdl_enter();
     __shared__ double smem[32];
     const CgState &cs = sc->cg;
     const int m = cs.lb_count;
@@ -1176,19 +1185,16 @@ int gp_lbfgs_direction(gpair_ctx *c)
     if (rc) return rc;
     const int g = red_grid(c->npix);
     c->fuse_ctrl = CTRL_LB_PAIR;
-    k_lbfgs_pair<<<g, GP_THREADS, 0, c->stream>>>(c->image, c->lb_xold, c->full_grad_new, c->full_grad, c->lb_s,
-                                                  c->lb_y, c->npix, slot_partials(c, RED_LBP), c->sc,
-                                                  take_fused_ctrl(c));
-    GP_LAUNCH_CHECK(c);
+    GP_LAUNCH(c, gp_launch(c, k_lbfgs_pair, dim3(g), dim3(GP_THREADS), 0, c->image, c->lb_xold, c->full_grad_new,
+                           c->full_grad, c->lb_s, c->lb_y, c->npix, slot_partials(c, RED_LBP), c->sc,
+                           take_fused_ctrl(c)));
     c->fuse_ctrl = CTRL_LB_COEF;
-    k_lbfgs_dots<<<g, GP_THREADS, 0, c->stream>>>(c->image, c->full_grad_new, c->lb_s, c->lb_y, c->npix,
-                                                  slot_partials(c, RED_LBD), c->sc, take_fused_ctrl(c));
-    GP_LAUNCH_CHECK(c);
+    GP_LAUNCH(c, gp_launch(c, k_lbfgs_dots, dim3(g), dim3(GP_THREADS), 0, c->image, c->full_grad_new, c->lb_s,
+                           c->lb_y, c->npix, slot_partials(c, RED_LBD), c->sc, take_fused_ctrl(c)));
     c->fuse_ctrl = last;
-    k_lbfgs_combine<<<g, GP_THREADS, 0, c->stream>>>(c->image, c->full_grad_new, c->lb_s, c->lb_y,
-                                                     c->descent_dir, c->lb_xold, c->npix, slot_partials(c, RED_DIR),
-                                                     c->sc, take_fused_ctrl(c));
-    GP_LAUNCH_CHECK(c);
+    GP_LAUNCH(c, gp_launch(c, k_lbfgs_combine, dim3(g), dim3(GP_THREADS), 0, c->image, c->full_grad_new, c->lb_s,
+                           c->lb_y, c->descent_dir, c->lb_xold, c->npix, slot_partials(c, RED_DIR), c->sc,
+                           take_fused_ctrl(c)));
     return GPAIR_OK;
 }
 
@@ -1221,7 +1227,11 @@ __device__ __forceinline__ void update_image_body(const UpdateImageArgs &A, cons
     }
 }
 
-__global__ void __launch_bounds__(256) k_update_image(const UpdateImageArgs a) { update_image_body(a, gp_vgrid_hw()); }
+__global__ void __launch_bounds__(256) k_update_image(const UpdateImageArgs a)
+{
+    gp_pdl_enter();
+    update_image_body(a, gp_vgrid_hw());
+}
 
 struct UpdateImageOp {
     using Args = UpdateImageArgs;
@@ -1239,8 +1249,7 @@ static UpdateImageArgs update_image_args(gpair_ctx *c, int step_from_state, doub
 int gp_update_image(gpair_ctx *c, int step_from_state, double step_host, double minval, int backup)
 {
     const UpdateImageArgs a = update_image_args(c, step_from_state, step_host, minval, backup);
-    k_update_image<<<a.nbx, 256, 0, c->stream>>>(a);
-    GP_LAUNCH_CHECK(c);
+    GP_LAUNCH(c, gp_launch(c, k_update_image, dim3(a.nbx), dim3(256), 0, a));
     return GPAIR_OK;
 }
 
@@ -1390,6 +1399,7 @@ __device__ __forceinline__ void vis_chi2_batch_body(const VisChi2BatchArgs &A, c
 
 __global__ void __launch_bounds__(GP_THREADS) k_vis_chi2_batch(const VisChi2BatchArgs a)
 {
+    gp_pdl_enter();
     vis_chi2_batch_body(a, gp_vgrid_hw());
 }
 
@@ -1476,8 +1486,7 @@ static VisChi2BatchArgs batch_chi2_args(gpair_ctx *c, int epp, FusedCtrl fc, con
 static int batch_chi2(gpair_ctx *c, int epp)
 {
     const VisChi2BatchArgs a = batch_chi2_args(c, epp, take_fused_ctrl(c), c->gate);
-    k_vis_chi2_batch<<<dim3(a.nbx, a.nby), GP_THREADS, 0, c->stream>>>(a);
-    GP_LAUNCH_CHECK(c);
+    GP_LAUNCH(c, gp_launch(c, k_vis_chi2_batch, dim3(a.nbx, a.nby), dim3(GP_THREADS), 0, a));
     return GPAIR_OK;
 }
 
@@ -2083,7 +2092,11 @@ __device__ __forceinline__ void cg_ctrl_g_body(const CtrlArgs &A, const GpVGrid 
     if (A.h_iter) cg_set_handles(sc, A.what, A.h_iter, A.h_ls, A.h_grad);
 }
 
-__global__ void k_cg_ctrl_g(const CtrlArgs a) { cg_ctrl_g_body(a, gp_vgrid_hw()); }
+__global__ void k_cg_ctrl_g(const CtrlArgs a)
+{
+    gp_pdl_enter();
+    cg_ctrl_g_body(a, gp_vgrid_hw());
+}
 
 struct CtrlOp {
     using Args = CtrlArgs;
@@ -2094,8 +2107,7 @@ int gp_cg_kernel_graph(gpair_ctx *c, int which_ctrl, unsigned long long h_iter, 
                        unsigned long long h_grad, double *trace, int trace_cap)
 {
     const CtrlArgs a = {c->sc, which_ctrl, h_iter, h_ls, h_grad, trace, trace_cap, 1, 1};
-    k_cg_ctrl_g<<<1, 32, 0, c->stream>>>(a);
-    GP_LAUNCH_CHECK(c);
+    GP_LAUNCH(c, gp_launch(c, k_cg_ctrl_g, dim3(1), dim3(32), 0, a));
     return GPAIR_OK;
 }
 
@@ -2165,9 +2177,8 @@ int gp_stage_args(gpair_ctx *c, int stage, double *trace, void *out, int *nblock
 template <class Op, int THREADS>
 static int group_launch(gpair_ctx *c, const void *d_args, const int *d_start, int n, int total, const int *gate)
 {
-    k_grouped<Op, THREADS>
-        <<<total, THREADS, 0, c->stream>>>((const typename Op::Args *)d_args, d_start, n, gate);
-    GP_LAUNCH_CHECK(c);
+    GP_LAUNCH(c, gp_launch(c, k_grouped<Op, THREADS>, dim3(total), dim3(THREADS), 0,
+                           (const typename Op::Args *)d_args, d_start, n, gate));
     return GPAIR_OK;
 }
 

@@ -294,6 +294,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 {
     static_assert(OP != OP_F16F8 || (EPI == EPI_FWD && NPROD == 3), "the 8-bit cross terms serve the forward");
     constexpr bool F8 = OP == OP_F16F8;
+    gp_pdl_enter();  // operands and gates come from the kernels before it
     using G = TcGeo<PAIR>;
     extern __shared__ unsigned char smem_raw[];
     unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -1006,6 +1007,7 @@ __device__ __forceinline__ void tc_prep_rows_body(const PrepRowsArgs &A, const G
 template <typename OT, int MODE>
 __global__ void __launch_bounds__(PR_THREADS) k_tc_prep_rows(const PrepRowsArgs a)
 {
+    gp_pdl_enter();
     tc_prep_rows_body<OT, MODE>(a, gp_vgrid_hw());
 }
 
@@ -1208,6 +1210,7 @@ __device__ __forceinline__ void tc_build_w_uv_body(const BuildWArgs &A, const Gp
 template <typename OT>
 __global__ void __launch_bounds__(256) k_tc_build_w_uv(const BuildWArgs a)
 {
+    gp_pdl_enter();
     tc_build_w_uv_body<OT>(a, gp_vgrid_hw());
 }
 
@@ -1540,22 +1543,38 @@ struct TcMaps {
     const CUtensorMap *a_hi, *a_lo, *a_x, *b_hi, *b_lo, *b_x;
 };
 
+// launch attributes of a contraction: the cluster of a CTA pair and the
+// programmatic dependent launch (gp_launch)
+static int tc_attrs(cudaLaunchAttribute *at, int pair, int pdl)
+{
+    int n = 0;
+    if (pair) {
+        at[n].id = cudaLaunchAttributeClusterDimension;
+        at[n].val.clusterDim.x = 2;
+        at[n].val.clusterDim.y = 1;
+        at[n].val.clusterDim.z = 1;
+        n++;
+    }
+    if (pdl) {
+        at[n].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[n].val.programmaticStreamSerializationAllowed = 1;
+        n++;
+    }
+    return n;
+}
+
 template <int EPI, int PAIR>
-static cudaError_t tc_launch_kind(TcState *t, dim3 grid, cudaStream_t st, const TcMaps &m, const TcArgs &a)
+static cudaError_t tc_launch_kind(TcState *t, dim3 grid, cudaStream_t st, int pdl, const TcMaps &m, const TcArgs &a)
 {
     cudaLaunchConfig_t cfg;
     memset(&cfg, 0, sizeof(cfg));
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeClusterDimension;
-    at[0].val.clusterDim.x = PAIR ? 2 : 1;
-    at[0].val.clusterDim.y = 1;
-    at[0].val.clusterDim.z = 1;
+    cudaLaunchAttribute at[2];
     cfg.gridDim = grid;
     cfg.blockDim = dim3(TC_THREADS, 1, 1);
     cfg.dynamicSmemBytes = TC_SMEM_BYTES;
     cfg.stream = st;
     cfg.attrs = at;
-    cfg.numAttrs = PAIR ? 1 : 0;
+    cfg.numAttrs = tc_attrs(at, PAIR, pdl);
     if (EPI == EPI_FWD && t->fop == OP_F16F8)
         return cudaLaunchKernelEx(&cfg, k_tc_gemm<EPI_FWD, OP_F16F8, 3, PAIR, 0>, *m.a_hi, *m.a_lo, *m.a_x, *m.b_hi,
                                   *m.b_lo, *m.b_x, a);
@@ -1580,10 +1599,10 @@ static int tc_launch(gpair_ctx *c, TcState *t, const TcMaps &m, TcArgs &a)
     cudaError_t e;
     if (t->pair) {
         const int np = a.units < t->npairs ? a.units : t->npairs;
-        e = tc_launch_kind<EPI, 1>(t, dim3(2 * np, 1, 1), c->stream, m, a);
+        e = tc_launch_kind<EPI, 1>(t, dim3(2 * np, 1, 1), c->stream, c->pdl, m, a);
     } else {
         const int g = a.units < t->nsm ? a.units : t->nsm;
-        e = tc_launch_kind<EPI, 0>(t, dim3(g, 1, 1), c->stream, m, a);
+        e = tc_launch_kind<EPI, 0>(t, dim3(g, 1, 1), c->stream, c->pdl, m, a);
     }
     if (e != cudaSuccess) {
         snprintf(c->last_error, sizeof(c->last_error), "tensor-core contraction launch: %s", cudaGetErrorString(e));
@@ -1647,17 +1666,14 @@ static int tc_prep_rows_launch(gpair_ctx *c, TcState *t, int mode, int reduce, d
                                const float *img = nullptr)
 {
     const PrepRowsArgs a = tc_prep_rows_args(c, t, mode, reduce, partials, img);
-    const dim3 g(a.nbx, a.nby, 1);
-    if (t->op == OP_F16) {
-        if (mode == 0) k_tc_prep_rows<__half, 0><<<g, PR_THREADS, 0, c->stream>>>(a);
-        else if (mode == 1) k_tc_prep_rows<__half, 1><<<g, PR_THREADS, 0, c->stream>>>(a);
-        else k_tc_prep_rows<__half, 2><<<g, PR_THREADS, 0, c->stream>>>(a);
-    } else {
-        if (mode == 0) k_tc_prep_rows<float, 0><<<g, PR_THREADS, 0, c->stream>>>(a);
-        else if (mode == 1) k_tc_prep_rows<float, 1><<<g, PR_THREADS, 0, c->stream>>>(a);
-        else k_tc_prep_rows<float, 2><<<g, PR_THREADS, 0, c->stream>>>(a);
-    }
-    GP_LAUNCH_CHECK(c);
+    const dim3 g(a.nbx, a.nby, 1), b(PR_THREADS);
+    const bool f16 = t->op == OP_F16;
+    if (mode == 0)
+        GP_LAUNCH(c, gp_launch(c, f16 ? k_tc_prep_rows<__half, 0> : k_tc_prep_rows<float, 0>, g, b, 0, a));
+    else if (mode == 1)
+        GP_LAUNCH(c, gp_launch(c, f16 ? k_tc_prep_rows<__half, 1> : k_tc_prep_rows<float, 1>, g, b, 0, a));
+    else
+        GP_LAUNCH(c, gp_launch(c, f16 ? k_tc_prep_rows<__half, 2> : k_tc_prep_rows<float, 2>, g, b, 0, a));
     return GPAIR_OK;
 }
 
@@ -1812,16 +1828,16 @@ static BuildWArgs tc_build_w_args(gpair_ctx *c, TcState *t)
 }
 
 template <typename OT>
-static void launch_build_w(gpair_ctx *c, TcState *t)
+static cudaError_t launch_build_w(gpair_ctx *c, TcState *t)
 {
     if (c->have_uv) {
         const BuildWArgs a = tc_build_w_args(c, t);
-        k_tc_build_w_uv<OT><<<dim3(a.nbx, a.nby), 256, 0, c->stream>>>(a);
-    } else {
-        dim3 g(gp_cdiv(c->nuv ? c->nuv : 1, 32), gp_cdiv(c->N, 32));
-        k_tc_build_w<OT><<<g, 256, 0, c->stream>>>(c->cw, nullptr, c->fy, c->pix, c->nuv, c->N, t->K2_pad,
-                                                    (OT *)t->w_hi, (OT *)t->w_lo, c->sc);
+        return gp_launch(c, k_tc_build_w_uv<OT>, dim3(a.nbx, a.nby), dim3(256), 0, a);
     }
+    dim3 g(gp_cdiv(c->nuv ? c->nuv : 1, 32), gp_cdiv(c->N, 32));
+    k_tc_build_w<OT><<<g, 256, 0, c->stream>>>(c->cw, nullptr, c->fy, c->pix, c->nuv, c->N, t->K2_pad,
+                                                (OT *)t->w_hi, (OT *)t->w_lo, c->sc);
+    return cudaSuccess;
 }
 
 // adjoint A-side weights W from c_k and Fy (hi/lo, one global scale)
@@ -1830,9 +1846,7 @@ int gp_tc_build_w(gpair_ctx *c)
     int rc;
     TcState *t = tc_state_ready(c, &rc);
     if (rc) return rc;
-    if (t->op == OP_F16) launch_build_w<__half>(c, t);
-    else launch_build_w<float>(c, t);
-    GP_LAUNCH_CHECK(c);
+    GP_LAUNCH(c, t->op == OP_F16 ? launch_build_w<__half>(c, t) : launch_build_w<float>(c, t));
     return GPAIR_OK;
 }
 
@@ -2020,21 +2034,17 @@ int gp_tc_group_build(gpair_ctx **ctx, int n, const int *gate, unsigned int *err
 }
 
 template <int EPI, int PAIR>
-static cudaError_t tc_group_launch_kind(TcGroup *G, cudaStream_t st, const TcArgs &a)
+static cudaError_t tc_group_launch_kind(TcGroup *G, cudaStream_t st, int pdl, const TcArgs &a)
 {
     cudaLaunchConfig_t cfg;
     memset(&cfg, 0, sizeof(cfg));
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeClusterDimension;
-    at[0].val.clusterDim.x = PAIR ? 2 : 1;
-    at[0].val.clusterDim.y = 1;
-    at[0].val.clusterDim.z = 1;
+    cudaLaunchAttribute at[2];
     cfg.gridDim = dim3(PAIR ? 2 * (unsigned)G->npairs : (unsigned)G->nsm, 1, 1);
     cfg.blockDim = dim3(TC_THREADS, 1, 1);
     cfg.dynamicSmemBytes = TC_SMEM_GROUP_BYTES;
     cfg.stream = st;
     cfg.attrs = at;
-    cfg.numAttrs = PAIR ? 1 : 0;
+    cfg.numAttrs = tc_attrs(at, PAIR, pdl);
     const CUtensorMap &m = G->map0;
     if (EPI == EPI_FWD && G->op == OP_F16F8)
         return cudaLaunchKernelEx(&cfg, k_tc_gemm<EPI_FWD, OP_F16F8, 3, PAIR, 1>, m, m, m, m, m, m, a);
@@ -2059,9 +2069,11 @@ int gp_tc_group_run(void *grp, gpair_ctx *c, cudaStream_t st)
     a.skip_loads = c->tc_skip_loads;
     cudaError_t e;
     if (G->epi == EPI_STORE)
-        e = G->pair ? tc_group_launch_kind<EPI_STORE, 1>(G, st, a) : tc_group_launch_kind<EPI_STORE, 0>(G, st, a);
+        e = G->pair ? tc_group_launch_kind<EPI_STORE, 1>(G, st, c->pdl, a)
+                    : tc_group_launch_kind<EPI_STORE, 0>(G, st, c->pdl, a);
     else
-        e = G->pair ? tc_group_launch_kind<EPI_FWD, 1>(G, st, a) : tc_group_launch_kind<EPI_FWD, 0>(G, st, a);
+        e = G->pair ? tc_group_launch_kind<EPI_FWD, 1>(G, st, c->pdl, a)
+                    : tc_group_launch_kind<EPI_FWD, 0>(G, st, c->pdl, a);
     if (e != cudaSuccess) {
         snprintf(c->last_error, sizeof(c->last_error), "grouped contraction launch: %s", cudaGetErrorString(e));
         return GPAIR_ERR_CUDA;
@@ -2125,9 +2137,8 @@ int gp_tc_stage_args(gpair_ctx *c, int stage, void *out, int *nblocks, int *op)
 template <class Op, int THREADS>
 static int tc_group_stage(gpair_ctx *c, const void *d_args, const int *d_start, int n, int total, const int *gate)
 {
-    k_grouped<Op, THREADS>
-        <<<total, THREADS, 0, c->stream>>>((const typename Op::Args *)d_args, d_start, n, gate);
-    GP_LAUNCH_CHECK(c);
+    GP_LAUNCH(c, gp_launch(c, k_grouped<Op, THREADS>, dim3(total), dim3(THREADS), 0,
+                           (const typename Op::Args *)d_args, d_start, n, gate));
     return GPAIR_OK;
 }
 

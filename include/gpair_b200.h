@@ -507,6 +507,15 @@ int gpair_set_tc_wait(gpair_ctx *ctx, long long budget_cycles, int skip_loads);
  * Results agree to rounding; the operands are rebuilt on a change. */
 int gpair_set_tc_pair(gpair_ctx *ctx, int on);
 int gpair_get_tc_pair(gpair_ctx *ctx);
+
+/* ---- overlapped kernel launches ----
+ * No counterpart in the reference. on = 1 (default; environment variable
+ * GPAIR_PDL=0 makes 0 the default of new contexts): the kernels of an
+ * evaluation are launched as programmatic dependent launches, so that each
+ * kernel's launch and block scheduling overlap the end of the kernel before it
+ * (each waits for that kernel's completion before it touches memory). Results
+ * are the same either way; captured graphs are rebuilt on a change. */
+int gpair_set_pdl(gpair_ctx *ctx, int on);
 int gpair_last_run_stage_ms(gpair_ctx *ctx, double *stage_ms, int *stage_launches, int max_stages);
 
 /* ---- allocation-free data stage ----

@@ -898,6 +898,29 @@ def test_alternating_line_searches_reuse_their_graphs(rec):
     assert outs[1]["criterion_evals"] % g.LS_TRIALS == 3 % g.LS_TRIALS
 
 
+@pytest.mark.parametrize("ls", [g.LS_WOLFE, g.LS_BATCH])
+@pytest.mark.parametrize("prec", [g.PREC_FP32, g.PREC_SPLIT16, g.PREC_SPLIT16F8])
+def test_programmatic_dependent_launches_change_no_result(rec, prec, ls):
+    """Consistency check (library against itself): the evaluation chain launched
+    as programmatic dependent launches (each kernel waits for the one before it
+    on the stream) gives bit for bit the results of plain stream order."""
+    p = _problem("small")
+    rec.set_problem(p)
+    rec.set_precision(prec)
+    outs = []
+    try:
+        for pdl in (False, True):
+            rec.set_pdl(pdl)
+            rec.set_image(p.start_image())
+            o = rec.cg(6, method=2, trace=True, line_search=ls)
+            outs.append((o, rec.get_image()))
+    finally:
+        rec.set_pdl(True)
+    assert np.array_equal(outs[0][0]["trace_J"], outs[1][0]["trace_J"])
+    assert outs[0][0]["criterion_evals"] == outs[1][0]["criterion_evals"]
+    assert np.array_equal(outs[0][1], outs[1][1])
+
+
 @pytest.mark.parametrize("ls,independent,pair,mixed,prec,fwd_only,layout", [
     (0, False, True, None, g.PREC_SPLIT16, False, 0),
     (1, True, True, None, g.PREC_SPLIT16, False, 0),
