@@ -351,7 +351,8 @@ def many_instances(n: int, iters: int) -> dict:
     """n independent reconstructions of uneven size (widths 64-256, 500-8,000 uv)
     for `iters` batched-line-search CG iterations each: one after another, all
     at once through gpair_cg_run_many (each context's graph on its own stream),
-    and as one graph launch (gpair_batch_run) in three layouts: the staged lockstep
+    (after gpair_set_shared_splits: the adjoint split-K lengths for instances that
+    share the GPU) and as one graph launch (gpair_batch_run) in three layouts: the staged lockstep
     batch (every stage of an iteration one launch over all instances, every
     contraction one grouped tcgen05 launch per class), the lockstep batch with
     grouped trial forwards only, and every CG loop an independent branch of the
@@ -383,6 +384,11 @@ def many_instances(n: int, iters: int) -> dict:
             r.cg(iters, method=2, line_search=g.LS_BATCH)
         t_seq = time.perf_counter() - t0
         flops = sum(r.last_run_stats()[1] for r in recs)
+        # run together, the instances split the adjoint's K dimension for the GPU they share
+        g.api.shared_splits(recs)
+        for r, p in zip(recs, ps):
+            r.set_image(p.start_image())
+        g.cg_many(recs, 1, line_search=g.LS_BATCH)  # rebuilds the graphs
         for r, p in zip(recs, ps):
             r.set_image(p.start_image())
         t0 = time.perf_counter()

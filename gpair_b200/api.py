@@ -87,6 +87,7 @@ class CgParams(C.Structure):
 LS_WOLFE, LS_BATCH, LS_TRIALS = 0, 1, 8
 BATCH_INDEPENDENT = 1  # gpair_batch_create_ex flag: independent branches, no lockstep grouping
 BATCH_FORWARDS_ONLY = 2  # gpair_batch_create_ex flag: lockstep with grouped trial forwards only
+BATCH_STAGE_STAMPS = 4  # gpair_batch_create_ex flag: device timer stamps between the staged launches
 TUNE_PRECISION, TUNE_SPLITS, TUNE_CACHE, TUNE_BATCHED, TUNE_TILE = 1, 2, 4, 8, 16
 TUNE_MAX_CANDIDATES = 16
 
@@ -140,6 +141,7 @@ def lib() -> C.CDLL:
         L.gpair_set_tc_wait.argtypes = [vp, C.c_longlong, i]
         L.gpair_set_tc_pair.argtypes = [vp, i]
         L.gpair_set_pdl.argtypes = [vp, i]
+        L.gpair_set_shared_splits.argtypes = [vp, i]
         L.gpair_get_tc_pair.argtypes = [vp]
         L.gpair_last_run_stage_ms.argtypes = [vp, C.POINTER(d), C.POINTER(i), i]
         L.gpair_get_oi_fits_data.argtypes = [i, f, f, i, vp, i, vp, i, vp, C.POINTER(OiData)]
@@ -160,6 +162,7 @@ def lib() -> C.CDLL:
         L.gpair_batch_create.argtypes = [C.POINTER(vp), C.POINTER(vp), i, i]
         L.gpair_batch_create_ex.argtypes = [C.POINTER(vp), C.POINTER(vp), i, i, i]
         L.gpair_batch_grouped.argtypes = [vp]
+        L.gpair_batch_stage_stamps.argtypes = [vp, vp, i, i]
         L.gpair_batch_run.argtypes = [vp, C.POINTER(CgParams), C.POINTER(CgResult)]
         L.gpair_batch_destroy.argtypes = [vp]
         L.gpair_cg_run_many.argtypes = [C.POINTER(vp), i, C.POINTER(CgParams), C.POINTER(CgResult)]
@@ -670,6 +673,15 @@ def cg_many(recs, iterations: int, method: int = 2, alpha: Optional[float] = Non
     return [_result_dict(res[i]) for i in range(n)]
 
 
+def shared_splits(recs) -> None:
+    """gpair_set_shared_splits: adjoint split-K lengths for contexts that run
+    together, so that their units jointly fill the GPU instead of each alone."""
+    L = lib()
+    n = len(recs)
+    handles = (C.c_void_p * n)(*[r.h.value for r in recs])
+    _check(L.gpair_set_shared_splits(handles, n), recs[0].h)
+
+
 class Batch:
     """Many reconstructions in one CUDA graph launch (gpair_batch_*). With the
     batched line search and the contexts on tensor-core paths the instances run in
@@ -680,13 +692,15 @@ class Batch:
     independent branch of the graph (independent=True, or no tensor-core context).
     Build after the contexts hold their problems, images and configuration."""
 
-    def __init__(self, recs, line_search: int = LS_BATCH, independent: bool = False, forwards_only: bool = False):
+    def __init__(self, recs, line_search: int = LS_BATCH, independent: bool = False, forwards_only: bool = False,
+                 stamps: bool = False):
         self._L = lib()
         self.recs = list(recs)
         self.line_search = line_search
         h = C.c_void_p()
         arr = (C.c_void_p * len(self.recs))(*[r.h.value for r in self.recs])
-        flags = (BATCH_INDEPENDENT if independent else 0) | (BATCH_FORWARDS_ONLY if forwards_only else 0)
+        flags = ((BATCH_INDEPENDENT if independent else 0) | (BATCH_FORWARDS_ONLY if forwards_only else 0) |
+                 (BATCH_STAGE_STAMPS if stamps else 0))
         _check(self._L.gpair_batch_create_ex(C.byref(h), arr, len(self.recs), line_search, flags), self.recs[0].h)
         self.h = h
         self.grouped = int(self._L.gpair_batch_grouped(self.h))
@@ -704,6 +718,26 @@ class Batch:
         res = (CgResult * len(self.recs))()
         _check(self._L.gpair_batch_run(self.h, C.byref(prm), res), self.recs[0].h)
         return [_result_dict(res[i]) for i in range(len(self.recs))]
+
+    STAMP_NAMES = ["prep", "forward", "vis_data", "adj_weights", "build_w", "adjoint", "grad_finalize",
+                   "descent", "route_ls0", "(ls start)", "trials_prep", "trials_forward", "trials_chi2",
+                   "route_lsn", "(post start)", "update", "ctrl_end", "route_end"]
+
+    def stage_times_us(self, reset: bool = True) -> dict:
+        """Per-launch device time (us) of a staged batch built with stamps=True,
+        summed over every iteration and batched evaluation since the last reset
+        (each includes one timer kernel's launch); "batched_evaluations" counts
+        the batched-evaluation rounds. {} without stamps."""
+        buf = np.zeros(39, np.uint64)
+        n = self._L.gpair_batch_stage_stamps(self.h, _p(buf), 39, 1 if reset else 0)
+        if n <= 0:
+            return {}
+        out = {}
+        for k, name in enumerate(self.STAMP_NAMES):
+            if not name.startswith("("):
+                out[name] = float(buf[19 + k + 1]) / 1e3
+        out["batched_evaluations"] = int(buf[38])
+        return out
 
     def close(self):
         if getattr(self, "h", None):

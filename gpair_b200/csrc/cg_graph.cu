@@ -258,7 +258,32 @@ struct BatchGraph {
     void *stg_args[GS_COUNT];  // device: argument structs of every instance, lockstep order
     int *stg_start[GS_COUNT];  // device: block starts [n + 1]
     int stg_total[GS_COUNT];
+    // staged batches built with stage stamps: device timer after every launch of
+    // the last iteration (GP_NSTAMPS values, overwritten by every iteration)
+    unsigned long long *stamps;
 };
+
+// Stamp positions of a staged iteration: the pre-phase (start, then after the
+// prep, forwards, V2/T3/chi2, c_k, W, adjoints, gradient, direction, router),
+// a batched evaluation (start, then after the trial prep, trial forwards,
+// trial chi2, router) and the post-phase (start, then after the update,
+// controller, router). The buffer holds the last value of every stamp
+// [0, GP_NSTAMPS), the time since the stamp before it summed over the whole
+// run [GP_NSTAMPS, 2 GP_NSTAMPS) (0 for the three segment starts) and the
+// number of batched evaluations [2 GP_NSTAMPS].
+#define GP_NSTAMPS 19
+#define GP_STAMP_WORDS (2 * GP_NSTAMPS + 1)
+
+__global__ void k_stamp(unsigned long long *__restrict__ t, int i)
+{
+    if (threadIdx.x == 0) {
+        unsigned long long v;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(v));
+        if (i != 0 && i != 10 && i != 15) t[GP_NSTAMPS + i] += v - t[i - 1];
+        if (i == 10) t[2 * GP_NSTAMPS] += 1ull;
+        t[i] = v;
+    }
+}
 
 void gp_batch_graph_free(void *bg)
 {
@@ -283,6 +308,7 @@ void gp_batch_graph_free(void *bg)
         if (B->stg_args[s]) cudaFree(B->stg_args[s]);
         if (B->stg_start[s]) cudaFree(B->stg_start[s]);
     }
+    if (B->stamps) cudaFree(B->stamps);
     if (B->gerr) cudaFree(B->gerr);
     if (B->flags) cudaFree(B->flags);
     if (B->hd) cudaFree(B->hd);
@@ -644,7 +670,7 @@ static int stage_table(BatchGraph *B, gpair_ctx **ctx, int n, int stage, double 
 
 // GPAIR_ERR_STATE: the instances cannot run fully staged (the caller builds the
 // lockstep with grouped trial forwards only, or independent branches)
-static int build_lockstep_staged(gpair_ctx **ctx_in, int n, BatchGraph *B)
+static int build_lockstep_staged(gpair_ctx **ctx_in, int n, BatchGraph *B, int with_stamps)
 {
     if (n > 4096) return GPAIR_ERR_STATE;
     std::vector<int> key((size_t)n), order((size_t)n);
@@ -724,6 +750,17 @@ static int build_lockstep_staged(gpair_ctx **ctx_in, int n, BatchGraph *B)
         }
         return GPAIR_OK;
     };
+    if (with_stamps) {
+        GP_CUDA(c0, cudaMalloc(&B->stamps, sizeof(unsigned long long) * GP_STAMP_WORDS));
+        GP_CUDA(c0, cudaMemset(B->stamps, 0, sizeof(unsigned long long) * GP_STAMP_WORDS));
+    }
+    // a device timer stamp (plain launch: it follows the complete kernel before it)
+    auto stamp = [&](int i) {
+        if (!B->stamps) return GPAIR_OK;
+        k_stamp<<<1, 32, 0, c0->stream>>>(B->stamps, i);
+        GP_LAUNCH_CHECK(c0);
+        return GPAIR_OK;
+    };
     auto route = [&](int what, cudaGraphConditionalHandle h) {
         GP_LAUNCH(c0, gp_launch(c0, k_lockstep_route, dim3(1), dim3(256), 0, what, B->scs, n, B->flags,
                                 B->flags + n, (const cudaGraphConditionalHandle *)nullptr,
@@ -749,15 +786,16 @@ static int build_lockstep_staged(gpair_ctx **ctx_in, int n, BatchGraph *B)
         c0,
         [&]() {
             int r;
-            if ((r = stage(GS_PREP_IMAGE, act))) return r;
-            if ((r = gemms(B->grps_img))) return r;
-            if ((r = stage(GS_VIS_DATA, act))) return r;
-            if ((r = stage(GS_ADJ_WEIGHTS, act))) return r;
-            if ((r = stage(GS_BUILD_W, act))) return r;
-            if ((r = gemms(B->grps_adj))) return r;
-            if ((r = stage(GS_GRAD_FINALIZE, act))) return r;
-            if ((r = stage(GS_DESCENT, act))) return r;
-            return route(GR_LS0S, h_ls);
+            if ((r = stamp(0)) || (r = stage(GS_PREP_IMAGE, act)) || (r = stamp(1))) return r;
+            if ((r = gemms(B->grps_img)) || (r = stamp(2))) return r;
+            if ((r = stage(GS_VIS_DATA, act)) || (r = stamp(3))) return r;
+            if ((r = stage(GS_ADJ_WEIGHTS, act)) || (r = stamp(4))) return r;
+            if ((r = stage(GS_BUILD_W, act)) || (r = stamp(5))) return r;
+            if ((r = gemms(B->grps_adj)) || (r = stamp(6))) return r;
+            if ((r = stage(GS_GRAD_FINALIZE, act)) || (r = stamp(7))) return r;
+            if ((r = stage(GS_DESCENT, act)) || (r = stamp(8))) return r;
+            if ((r = route(GR_LS0S, h_ls))) return r;
+            return stamp(9);
         },
         &g_pre, &npre);
     if (rc || (rc = add_child(c0, B1, g_pre, nullptr, 0, &n_pre))) return rc;
@@ -768,9 +806,10 @@ static int build_lockstep_staged(gpair_ctx **ctx_in, int n, BatchGraph *B)
         c0,
         [&]() {
             int r;
-            if ((r = stage(GS_UPDATE, act))) return r;
-            if ((r = stage(GS_CTRL_END, act))) return r;
-            return route(GR_END, h_iter);
+            if ((r = stamp(15)) || (r = stage(GS_UPDATE, act)) || (r = stamp(16))) return r;
+            if ((r = stage(GS_CTRL_END, act)) || (r = stamp(17))) return r;
+            if ((r = route(GR_END, h_iter))) return r;
+            return stamp(18);
         },
         &g_post, &npost);
     if (rc || (rc = add_child(c0, B1, g_post, &n_lsw, 1, &n_post))) return rc;
@@ -779,10 +818,11 @@ static int build_lockstep_staged(gpair_ctx **ctx_in, int n, BatchGraph *B)
         c0,
         [&]() {
             int r;
-            if ((r = stage(GS_PREP_TRIALS, lsg))) return r;
-            if ((r = gemms(B->grps))) return r;
-            if ((r = stage(GS_CHI2_BATCH, lsg))) return r;
-            return route(GR_LSN, h_ls);
+            if ((r = stamp(10)) || (r = stage(GS_PREP_TRIALS, lsg)) || (r = stamp(11))) return r;
+            if ((r = gemms(B->grps)) || (r = stamp(12))) return r;
+            if ((r = stage(GS_CHI2_BATCH, lsg)) || (r = stamp(13))) return r;
+            if ((r = route(GR_LSN, h_ls))) return r;
+            return stamp(14);
         },
         &g_ls, &nls);
     if (rc || (rc = add_child(c0, B2, g_ls, nullptr, 0, &n_ls))) return rc;
@@ -816,8 +856,8 @@ int gp_batch_graph_build(gpair_ctx **ctx, int n, int ls_mode, int allow_group, v
         G->trace_cap = 1;  // one row; batch runs return no trace
         if (cudaMalloc(&G->trace, sizeof(double) * 5) != cudaSuccess) rc = GPAIR_ERR_ALLOC;
     }
-    if (!rc && allow_group >= 2 && ls_mode == GPAIR_LS_BATCH) {
-        rc = build_lockstep_staged(ctx, n, B);
+    if (!rc && (allow_group & 3) >= 2 && ls_mode == GPAIR_LS_BATCH) {
+        rc = build_lockstep_staged(ctx, n, B, allow_group & 4);
         if (rc == GPAIR_OK) {
             B->grouped = 2;
         } else if (rc == GPAIR_ERR_STATE) {
@@ -826,7 +866,7 @@ int gp_batch_graph_build(gpair_ctx **ctx, int n, int ls_mode, int allow_group, v
             rc = GPAIR_OK;
         }
     }
-    if (!rc && !B->grouped && allow_group && ls_mode == GPAIR_LS_BATCH) {
+    if (!rc && !B->grouped && (allow_group & 3) && ls_mode == GPAIR_LS_BATCH) {
         rc = build_lockstep(ctx, n, B);
         if (rc == GPAIR_OK) {
             B->grouped = 1;
@@ -864,6 +904,22 @@ int gp_batch_graph_launch(void *bg, cudaStream_t stream)
 int gp_batch_graph_precision(void *bg, int i) { return ((BatchGraph *)bg)->loops[i].precision; }
 unsigned int gp_batch_graph_buf_gen(void *bg, int i) { return ((BatchGraph *)bg)->loops[i].buf_gen; }
 int gp_batch_graph_grouped(void *bg) { return bg ? ((BatchGraph *)bg)->grouped : 0; }
+
+// the stage stamps of a staged batch (none recorded: 0); `reset` zeroes them
+// afterwards (on st), so that the next run's sums start from zero
+int gp_batch_graph_stamps(void *bg, unsigned long long *out, int max, cudaStream_t st, int reset)
+{
+    BatchGraph *B = (BatchGraph *)bg;
+    if (!B || !B->stamps) return 0;
+    const int n = max < GP_STAMP_WORDS ? max : GP_STAMP_WORDS;
+    if (n > 0 && cudaMemcpyAsync(out, B->stamps, sizeof(unsigned long long) * n, cudaMemcpyDeviceToHost, st) !=
+                     cudaSuccess)
+        return GPAIR_ERR_CUDA;
+    if (reset && cudaMemsetAsync(B->stamps, 0, sizeof(unsigned long long) * GP_STAMP_WORDS, st) != cudaSuccess)
+        return GPAIR_ERR_CUDA;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return GPAIR_ERR_CUDA;
+    return GP_STAMP_WORDS;
+}
 
 long long gp_batch_graph_launches(void *bg, int i, int iterations_done, int criterion_evals, int grad_evals,
                                   int batches)

@@ -27,6 +27,7 @@ int gp_batch_graph_launch(void *bg, cudaStream_t stream);
 int gp_batch_graph_precision(void *bg, int i);
 unsigned int gp_batch_graph_buf_gen(void *bg, int i);
 int gp_batch_graph_grouped(void *bg);
+int gp_batch_graph_stamps(void *bg, unsigned long long *out, int max, cudaStream_t st, int reset);
 long long gp_batch_graph_launches(void *bg, int i, int iterations_done, int criterion_evals, int grad_evals,
                                   int batches);
 
@@ -380,6 +381,15 @@ extern "C" int gpair_set_tc_pair(gpair_ctx *c, int on)
 }
 
 extern "C" int gpair_get_tc_pair(gpair_ctx *c) { return c ? c->tc_pair : -1; }
+
+extern "C" int gpair_set_shared_splits(gpair_ctx **ctx, int n)
+{
+    if (!ctx || n < 1) return GPAIR_ERR_INVALID;
+    for (int i = 0; i < n; i++)
+        if (!ctx[i] || ctx[i]->device != ctx[0]->device) return GPAIR_ERR_INVALID;
+    GP_CUDA(ctx[0], cudaSetDevice(ctx[0]->device));
+    return gp_tc_shared_splits(ctx, n);
+}
 
 extern "C" int gpair_set_pdl(gpair_ctx *c, int on)
 {
@@ -917,10 +927,18 @@ extern "C" int gpair_batch_create(gpair_batch **out, gpair_ctx **ctx, int n, int
 
 extern "C" int gpair_batch_grouped(const gpair_batch *b) { return b ? gp_batch_graph_grouped(b->graph) : 0; }
 
+extern "C" int gpair_batch_stage_stamps(const gpair_batch *b, unsigned long long *ns, int max, int reset)
+{
+    if (!b || (!ns && max > 0)) return GPAIR_ERR_INVALID;
+    if (cudaSetDevice(b->device) != cudaSuccess) return GPAIR_ERR_CUDA;
+    return gp_batch_graph_stamps(b->graph, ns, max, b->stream, reset);
+}
+
 extern "C" int gpair_batch_create_ex(gpair_batch **out, gpair_ctx **ctx, int n, int line_search, int flags)
 {
     if (!out || !ctx || n <= 0) return GPAIR_ERR_INVALID;
-    if (flags & ~(GPAIR_BATCH_INDEPENDENT | GPAIR_BATCH_FORWARDS_ONLY)) return GPAIR_ERR_INVALID;
+    if (flags & ~(GPAIR_BATCH_INDEPENDENT | GPAIR_BATCH_FORWARDS_ONLY | GPAIR_BATCH_STAGE_STAMPS))
+        return GPAIR_ERR_INVALID;
     if (line_search != GPAIR_LS_WOLFE && line_search != GPAIR_LS_BATCH) return GPAIR_ERR_INVALID;
     *out = nullptr;
     for (int i = 0; i < n; i++) {
@@ -953,7 +971,8 @@ extern "C" int gpair_batch_create_ex(gpair_batch **out, gpair_ctx **ctx, int n, 
         ctx[i]->fuse_handles = 0;
     }
     // 2: every stage grouped where the instances allow it, 1: grouped forwards only, 0: independent
-    const int group = (flags & GPAIR_BATCH_INDEPENDENT) ? 0 : (flags & GPAIR_BATCH_FORWARDS_ONLY) ? 1 : 2;
+    int group = (flags & GPAIR_BATCH_INDEPENDENT) ? 0 : (flags & GPAIR_BATCH_FORWARDS_ONLY) ? 1 : 2;
+    if (flags & GPAIR_BATCH_STAGE_STAMPS) group |= 4;  // device timer stamps between the staged launches
     if (!rc) rc = gp_batch_graph_build(ctx, n, line_search, group, &b->graph);
     if (rc) {
         gpair_batch_destroy(b);

@@ -212,6 +212,13 @@ __device__ __forceinline__ void tc_fail(unsigned int *err, volatile int *abort_f
     *abort_flag = 1;
 }
 
+// One step of Fy along y: w * e^{-2 pi i s v_k}, with the rounding fixed (one
+// rounded product, then one fused multiply-add per component)
+__device__ __forceinline__ float2 fy_step(float2 w, float2 rot)
+{
+    return make_float2(fmaf(w.x, rot.x, -__fmul_rn(w.y, rot.y)), fmaf(w.x, rot.y, __fmul_rn(w.y, rot.x)));
+}
+
 template <int EPI>
 __device__ __forceinline__ void tc_decode(const TcArgs &a, int u, int &m, int &n, int &kb0, int &kb1, int &split)
 {
@@ -611,38 +618,90 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 }
                 umma::tc_fence_after();
                 const int emask = (1 << elog2) - 1;
-                float sre = 0.f, sim = 0.f;
+                if (lpad < TC_BN) {
+                    // several images per tile (a batch stack of lpad = 32, 64 or 128 rows
+                    // each; y0 is a multiple of lpad): chunk q of every image has the
+                    // same 16 values of Fy, formed once for all of them. Each image's
+                    // sum takes its chunks and rows in the order of the loop below.
+                    const int per = lpad >> 4, nimg = TC_BN / lpad;
+                    float are[TC_BN / 32], aim[TC_BN / 32];
 #pragma unroll
-                for (int c = 0; c < TC_BN / 16; c++) {
-                    uint32_t r[16];
-                    umma::tmem_ld16(taddr + (uint32_t)(c * 16), r);
-                    // power-of-two scales of the 16 image rows (same address in every lane)
-                    float rs[16];
-                    const float4 *rp = reinterpret_cast<const float4 *>(rsc + y0 + 16 * c);
-#pragma unroll
-                    for (int v4 = 0; v4 < 4; v4++) *reinterpret_cast<float4 *>(&rs[4 * v4]) = __ldg(rp + v4);
-                    umma::tmem_ld_wait();
-                    float2 w = an[c];
-#pragma unroll
-                    for (int j = 0; j < 16; j++) {
-                        const float tv = __uint_as_float(r[j]) * rs[j];
-                        sre = fmaf(tv, w.x, sre);
-                        sim = fmaf(tv, w.y, sim);
-                        const float wx = w.x * rot.x - w.y * rot.y;
-                        w.y = w.x * rot.y + w.y * rot.x;
-                        w.x = wx;
+                    for (int i = 0; i < TC_BN / 32; i++) {
+                        are[i] = 0.f;
+                        aim[i] = 0.f;
                     }
-                    if (((y0 + 16 * c + 16) & emask) == 0) {
-                        // end of a partial entry (warp-uniform): combine the Re/Im row
-                        // pair, store. even row: (sum T_re F_re, sum T_re F_im);
-                        // odd row: (sum T_im F_re, sum T_im F_im)
-                        const int entry = (y0 + 16 * c) >> elog2;
-                        const float re = sre, im = sim;
-                        const float ore = __shfl_xor_sync(0xffffffffu, re, 1);
-                        const float oim = __shfl_xor_sync(0xffffffffu, im, 1);
-                        if ((lane & 1) == 0 && vk) vpart[(size_t)entry * nuv + k] = make_float2(re - oim, im + ore);
-                        sre = 0.f;
-                        sim = 0.f;
+                    for (int qq = 0; qq < per; qq++) {
+                        float2 wv[16];
+                        wv[0] = (vk && qq < nanc) ? __ldg(&anc[qq]) : make_float2(0.f, 0.f);
+#pragma unroll
+                        for (int j = 1; j < 16; j++) wv[j] = fy_step(wv[j - 1], rot);
+#pragma unroll
+                        for (int ti = 0; ti < TC_BN / 32; ti++) {
+                            if (ti < nimg) {  // warp-uniform
+                                const int c = ti * per + qq;
+                                uint32_t r[16];
+                                umma::tmem_ld16(taddr + (uint32_t)(c * 16), r);
+                                float rs[16];
+                                const float4 *rp = reinterpret_cast<const float4 *>(rsc + y0 + 16 * c);
+#pragma unroll
+                                for (int v4 = 0; v4 < 4; v4++)
+                                    *reinterpret_cast<float4 *>(&rs[4 * v4]) = __ldg(rp + v4);
+                                umma::tmem_ld_wait();
+                                float sr = are[ti], si = aim[ti];
+#pragma unroll
+                                for (int j = 0; j < 16; j++) {
+                                    const float tv = __uint_as_float(r[j]) * rs[j];
+                                    sr = fmaf(tv, wv[j].x, sr);
+                                    si = fmaf(tv, wv[j].y, si);
+                                }
+                                are[ti] = sr;
+                                aim[ti] = si;
+                            }
+                        }
+                    }
+#pragma unroll
+                    for (int ti = 0; ti < TC_BN / 32; ti++) {
+                        if (ti < nimg) {
+                            const int entry = (y0 + ti * lpad) >> elog2;
+                            const float re = are[ti], im = aim[ti];
+                            const float ore = __shfl_xor_sync(0xffffffffu, re, 1);
+                            const float oim = __shfl_xor_sync(0xffffffffu, im, 1);
+                            if ((lane & 1) == 0 && vk)
+                                vpart[(size_t)entry * nuv + k] = make_float2(re - oim, im + ore);
+                        }
+                    }
+                } else {
+                    float sre = 0.f, sim = 0.f;
+#pragma unroll
+                    for (int c = 0; c < TC_BN / 16; c++) {
+                        uint32_t r[16];
+                        umma::tmem_ld16(taddr + (uint32_t)(c * 16), r);
+                        // power-of-two scales of the 16 image rows (same address in every lane)
+                        float rs[16];
+                        const float4 *rp = reinterpret_cast<const float4 *>(rsc + y0 + 16 * c);
+#pragma unroll
+                        for (int v4 = 0; v4 < 4; v4++) *reinterpret_cast<float4 *>(&rs[4 * v4]) = __ldg(rp + v4);
+                        umma::tmem_ld_wait();
+                        float2 w = an[c];
+#pragma unroll
+                        for (int j = 0; j < 16; j++) {
+                            const float tv = __uint_as_float(r[j]) * rs[j];
+                            sre = fmaf(tv, w.x, sre);
+                            sim = fmaf(tv, w.y, sim);
+                            w = fy_step(w, rot);
+                        }
+                        if (((y0 + 16 * c + 16) & emask) == 0) {
+                            // end of a partial entry (warp-uniform): combine the Re/Im row
+                            // pair, store. even row: (sum T_re F_re, sum T_re F_im);
+                            // odd row: (sum T_im F_re, sum T_im F_im)
+                            const int entry = (y0 + 16 * c) >> elog2;
+                            const float re = sre, im = sim;
+                            const float ore = __shfl_xor_sync(0xffffffffu, re, 1);
+                            const float oim = __shfl_xor_sync(0xffffffffu, im, 1);
+                            if ((lane & 1) == 0 && vk) vpart[(size_t)entry * nuv + k] = make_float2(re - oim, im + ore);
+                            sre = 0.f;
+                            sim = 0.f;
+                        }
                     }
                 }
             } else {
@@ -782,16 +841,26 @@ __device__ __forceinline__ float warp_max_f(float v)
     return v;
 }
 
+// max over aligned groups of `lanes` lanes (a power of two <= 32)
+__device__ __forceinline__ float group_max_f(float v, int lanes)
+{
+    for (int off = lanes >> 1; off > 0; off >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, off));
+    return v;
+}
+
 // Row-wise prep of the forward's image operand. A block of PR_THREADS threads
-// works on R = 8 / W image rows at a time, W warps (a power of two) per row:
+// works on R image rows at a time: W warps (a power of two) per row when N >
+// 256 (R = 8 / W), else one warp for 32 / lpr rows of lpr lanes each (lpr: the
+// fewest lanes, a power of two, whose 8 pixels each cover the row; 32 when N is
+// not a multiple of 8), so that narrow rows leave no lane idle:
 //   MODE 0  the image as it is; with `reduce`, its flux, regulariser and max
 //   MODE 1  the line-search trial I = max(I + s d, minval), s = cg.s, written to
 //           dst, with its flux, regulariser and max
-//   MODE 2  trial j = blockIdx.y of a batched search, s = cg.ts[j], written to
+//   MODE 2  trial j (the grid's y) of a batched search, s = cg.ts[j], written to
 //           dst + j npix and to operand rows j Lpad + y, with its flux and
 //           regulariser; nothing when `gate` is set and *gate is 0
 // Every row gets its own power-of-two scale 2^(15 - e), e the exponent of the
-// row's max |I| (a reduction over the row's warps: no pass over the whole image
+// row's max |I| (a reduction over the row's lanes or warps: no pass over the whole image
 // has to end before the split), and the forward epilogue multiplies
 // accumulator column y by rsc[row] = 2^(e - 15 - TC_TW_LOG2), exactly. With N a
 // multiple of 8 and N <= 256 W every lane holds 8 consecutive pixels of its row
@@ -815,7 +884,7 @@ struct PrepRowsArgs {
     const float *img, *d;
     float *dst;
     const float *model;
-    int N, W, Lpad, Kx_pad;
+    int N, W, lpr, Lpad, Kx_pad;  // W warps per row (N > 256) or lpr lanes per row (W = 1)
     void *hi, *lo;  // OT
     uint8_t *h8, *l8;
     float *rsc;
@@ -852,9 +921,13 @@ __device__ __forceinline__ void tc_prep_rows_body(const PrepRowsArgs &A, const G
     const bool red = MODE ? true : reduce != 0;
     if (MODE == 2) dst += (size_t)j * N * N;
     const size_t row0 = (size_t)j * Lpad;
-    const int R = PR_WARPS_MAX / W;            // rows per block and pass
-    const int sub = warp % W, rw = warp / W;   // this warp's part of its row, row within the pass
-    const int t = sub * 32 + lane, nt = 32 * W;  // thread within the row's group
+    // LPR lanes per row (W = 1 and narrow rows: several rows per warp), else W warps per row
+    const int LPR = A.lpr, RPW = 32 / LPR;
+    const int R = W > 1 ? PR_WARPS_MAX / W : PR_WARPS_MAX * RPW;  // rows per block and pass
+    const int sub = warp % W;                                     // this warp's part of its row
+    const int rw = W > 1 ? warp / W : warp * RPW + lane / LPR;    // row within the pass
+    const int t = W > 1 ? sub * 32 + lane : lane % LPR;           // thread within the row's group
+    const int nt = W > 1 ? 32 * W : LPR;
     double acc[2] = {0.0, 0.0};
     float mx = 0.f;
     const bool vec = (N & 7) == 0 && N <= 8 * nt;
@@ -910,13 +983,17 @@ __device__ __forceinline__ void tc_prep_rows_body(const PrepRowsArgs &A, const G
                 rmax = fmaxf(rmax, fabsf(I));
             }
         }
-        // max over the row's W warps
-        rmax = warp_max_f(rmax);
-        if (lane == 0) wmax[warp] = rmax;
-        __syncthreads();
-        rmax = 0.f;
-        for (int q = 0; q < W; q++) rmax = fmaxf(rmax, wmax[rw * W + q]);
-        __syncthreads();  // wmax is rewritten by the next pass
+        // max over the row's lanes (LPR), or over its W warps
+        if (W == 1) {
+            rmax = group_max_f(rmax, LPR);
+        } else {
+            rmax = warp_max_f(rmax);
+            if (lane == 0) wmax[warp] = rmax;
+            __syncthreads();
+            rmax = 0.f;
+            for (int q = 0; q < W; q++) rmax = fmaxf(rmax, wmax[rw * W + q]);
+            __syncthreads();  // wmax is rewritten by the next pass
+        }
         int ex = 0;
         frexpf(rmax, &ex);
         const float scale = ldexpf(1.f, 15 - ex);
@@ -1525,6 +1602,50 @@ int gp_tc_set_kb_per(gpair_ctx *c, int kb_per)
     return GPAIR_OK;
 }
 
+// Split-K lengths for n contexts that share the GPU (concurrent runs, batches):
+// their adjoint units together fill the SMs about twice, each context's share
+// in proportion to its adjoint work, instead of each filling the GPU alone.
+// Longer splits mean fewer partial images to write in the adjoint and to sum
+// in the gradient. Captured CG graphs of a changed context are dropped.
+static TcState *tc_state_ready(gpair_ctx *c, int *rc);
+
+int gp_tc_shared_splits(gpair_ctx **ctx, int n)
+{
+    if (!ctx || n < 1) return GPAIR_ERR_INVALID;
+    double total = 0.0;
+    int slots = 0;
+    for (int i = 0; i < n; i++) {
+        if (!ctx[i] || !ctx[i]->have_problem) return GPAIR_ERR_STATE;
+        if (ctx[i]->precision == GPAIR_PREC_FP32) continue;
+        int rc;
+        TcState *t = tc_state_ready(ctx[i], &rc);
+        if (rc) return rc;
+        const int tiles = (t->xrows_pad / (t->pair ? 256 : TC_BM)) * (t->M_pad / TC_BN);
+        total += (double)tiles * (double)(t->K2_pad / t->bk);
+        if (!slots) slots = t->pair ? t->npairs : t->nsm;
+    }
+    if (total <= 0.0) return GPAIR_OK;
+    const double target = 2.0 * slots;  // units over all contexts
+    for (int i = 0; i < n; i++) {
+        gpair_ctx *c = ctx[i];
+        if (c->precision == GPAIR_PREC_FP32) continue;
+        TcState *t = (TcState *)c->tc_state;
+        const int kb_total = t->K2_pad / t->bk;
+        int want = (int)(target * (double)kb_total / total + 0.5);  // splits of this context
+        if (want < 1) want = 1;
+        if (want > kb_total) want = kb_total;
+        int kb_per = (kb_total + want - 1) / want;
+        const int cap = TC_SPLIT_PRODUCTS / t->bk;
+        if (kb_per > cap) kb_per = cap;
+        if (kb_per != t->kb_per) {
+            int rc = gp_tc_set_kb_per(c, kb_per);
+            if (rc) return rc;
+            gp_cg_graph_free(c);  // a captured CG graph holds the old split count
+        }
+    }
+    return GPAIR_OK;
+}
+
 static TcState *tc_state_ready(gpair_ctx *c, int *rc)
 {
     TcState *t = (TcState *)c->tc_state;
@@ -1629,10 +1750,22 @@ static TcMaps tc_fwd_maps(const TcState *t, bool batch)
 // Row-wise prep launches (k_tc_prep_rows): PR_THREADS threads per block, R rows
 // per block and pass; at most GP_MAX_PARTIALS blocks (three partials each fit
 // the RED_PREP slot), a batch at most 1024 per trial (two partials each).
+// lanes per row with one warp per row: 8 pixels per lane (16-byte loads) when N
+// is a multiple of 8, the fewest lanes (a power of two) that cover the row;
+// else a whole warp
+static inline int pr_lanes_per_row(int N)
+{
+    if ((N & 7) != 0 || N > 256) return 32;
+    int l = 1;
+    while (8 * l < N) l <<= 1;
+    return l;
+}
+
 static PrepRowsArgs tc_prep_rows_args(gpair_ctx *c, TcState *t, int mode, int reduce, double *partials,
                                       const float *img)
 {
-    const int W = pr_warps_per_row(c->N), R = PR_WARPS_MAX / W;
+    const int W = pr_warps_per_row(c->N), lpr = W > 1 ? 32 : pr_lanes_per_row(c->N);
+    const int R = W > 1 ? PR_WARPS_MAX / W : PR_WARPS_MAX * (32 / lpr);
     int gx = gp_cdiv(c->N, R);
     const int cap = mode == 2 ? 1024 : GP_MAX_PARTIALS;
     if (gx > cap) gx = cap;
@@ -1646,6 +1779,7 @@ static PrepRowsArgs tc_prep_rows_args(gpair_ctx *c, TcState *t, int mode, int re
     a.model = c->model;
     a.N = c->N;
     a.W = W;
+    a.lpr = lpr;
     a.Lpad = b ? t->Lb : 0;
     a.Kx_pad = t->Kx_pad;
     a.hi = b ? t->imgb_hi : t->img_hi;

@@ -385,9 +385,24 @@ int gpair_cg_checkpoint_load(gpair_ctx *ctx, const void *buffer, size_t bytes);
 typedef struct gpair_batch gpair_batch;
 #define GPAIR_BATCH_INDEPENDENT 1
 #define GPAIR_BATCH_FORWARDS_ONLY 2
+/* Staged batches only: a device timer stamp (ns) after every launch of an
+ * iteration, for a breakdown of where an iteration's time goes. The stamps
+ * themselves add one small kernel per launch. */
+#define GPAIR_BATCH_STAGE_STAMPS 4
 int gpair_batch_create(gpair_batch **batch, gpair_ctx **ctx, int n, int line_search);
 int gpair_batch_create_ex(gpair_batch **batch, gpair_ctx **ctx, int n, int line_search, int flags);
 int gpair_batch_grouped(const gpair_batch *batch);
+/* Stage stamps of a batch created with GPAIR_BATCH_STAGE_STAMPS; returns the
+ * number of words (39), or 0 without stamps. Positions 0-18: the device timer
+ * (ns) at the pre-phase start, then after the image prep, criterion forwards,
+ * V2/T3/chi2, c_k, W, adjoints, gradient, direction and router; a batched
+ * evaluation's start, then after the trial prep, trial forwards, trial chi2
+ * and router; the post-phase start, then after the image update, controller
+ * and router (the last values of the run). Words 19-37: the time since the
+ * stamp before each position, summed over every iteration and batched
+ * evaluation since the last reset (0 at the three starts). Word 38: batched
+ * evaluations since the last reset. reset != 0 zeroes the words afterwards. */
+int gpair_batch_stage_stamps(const gpair_batch *batch, unsigned long long *ns, int max, int reset);
 int gpair_batch_run(gpair_batch *batch, const gpair_cg_params *p, gpair_cg_result *results);
 int gpair_batch_destroy(gpair_batch *batch);
 
@@ -516,6 +531,17 @@ int gpair_get_tc_pair(gpair_ctx *ctx);
  * (each waits for that kernel's completion before it touches memory). Results
  * are the same either way; captured graphs are rebuilt on a change. */
 int gpair_set_pdl(gpair_ctx *ctx, int on);
+
+/* ---- split-K lengths for contexts that share the GPU ----
+ * No counterpart in the reference. The adjoint contraction of a context alone
+ * splits its K dimension (2 nuv) so that its units fill every SM, which for a
+ * small image means many short splits and many partial images to write and sum.
+ * For n contexts run together (gpair_cg_run_many, gpair_batch_*), this sets each
+ * tensor-core context's split-K length so that all their units together fill
+ * the SMs about twice, each context's share in proportion to its adjoint work
+ * (at most the FP32-accumulation cap per split). CUDA-core contexts are left as
+ * they are. Results change by rounding only; call before capturing a batch. */
+int gpair_set_shared_splits(gpair_ctx **ctx, int n);
 int gpair_last_run_stage_ms(gpair_ctx *ctx, double *stage_ms, int *stage_launches, int max_stages);
 
 /* ---- allocation-free data stage ----

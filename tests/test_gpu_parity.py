@@ -975,6 +975,47 @@ def test_batch_graph_equals_separate_runs(ls, independent, pair, mixed, prec, fw
             r.close()
 
 
+def test_shared_splits_keep_parity_and_staged_batches_exact():
+    """gpair_set_shared_splits on contexts that run together: longer adjoint
+    splits (fewer partial images); the data gradient still meets 1e-5 against the
+    FP64 oracle, and a staged batch with its stage stamps equals the separate runs
+    bit for bit."""
+    from gpair_b200.instances import instance
+    ps = [instance(20_000_200 + k) for k in range(4)]
+    recs = [g.Reconstructor(0) for _ in ps]
+    try:
+        for r, p in zip(recs, ps):
+            r.set_problem(p)
+            r.set_precision(g.PREC_SPLIT16)
+        g.api.shared_splits(recs)
+        for r, p in zip(recs, ps):
+            img = _rand_image(p, 5)
+            r.set_image(img)
+            chi2, _ = r.criterion()
+            r.gradient()
+            e = O.evaluate64(p, img)
+            assert abs(chi2 - e["chi2"]) / e["chi2"] <= 1e-5
+            assert _rel(r.data_gradient(), e["data_grad"]) <= 1e-5
+        singles, imgs = [], []
+        for r, p in zip(recs, ps):
+            r.set_image(p.start_image())
+            singles.append(r.cg(4, method=2, line_search=g.LS_BATCH))
+            imgs.append(r.get_image())
+        for r, p in zip(recs, ps):
+            r.set_image(p.start_image())
+        with g.api.Batch(recs, line_search=g.LS_BATCH, stamps=True) as b:
+            assert b.grouped == 2
+            out = b.run(4)
+            t = b.stage_times_us()
+            assert t["batched_evaluations"] >= 4 and t["trials_forward"] > 0 and t["adjoint"] > 0
+            for r, a, o, img in zip(recs, singles, out, imgs):
+                assert o["status"] == 0 and o["J"] == a["J"]
+                assert np.array_equal(r.get_image(), img)
+    finally:
+        for r in recs:
+            r.close()
+
+
 @pytest.mark.parametrize("fwd_only", [False, True])
 def test_grouped_batch_wait_timeout_is_reported_and_recovers(fwd_only):
     """The grouped contractions' bounded waits run out (built from a first context
