@@ -54,8 +54,13 @@
 #define TC_B_BYTES (TC_BN * TC_ROWB)
 #define TC_STAGE_BYTES (2 * TC_A_BYTES + 2 * TC_B_BYTES)
 #define TC_TMEM_COLS 512
-#define TC_SMEM_BYTES (1024 + TC_STAGES * TC_STAGE_BYTES + 256)
-#define TC_SMEM_GROUP_BYTES (TC_SMEM_BYTES + 4 * 272)  // + unit prefix sums of up to TC_GROUP_MAX instances
+// after the stages: barriers (256 B), the unit prefix sums of a grouped launch
+// (up to TC_GROUP_MAX instances), then the forward epilogue's row scales of a
+// unit, one copy per epilogue warp and accumulator buffer
+#define TC_RS_OFF (256 + 4 * 272)
+#define TC_RS_BYTES (4 * 2 * TC_BN * 4)
+#define TC_SMEM_BYTES (1024 + TC_STAGES * TC_STAGE_BYTES + TC_RS_OFF + TC_RS_BYTES)
+#define TC_SMEM_GROUP_BYTES TC_SMEM_BYTES
 #define TC_WAIT_BUDGET 4000000000LL  // default clock cycles (~2 s) per pipeline wait
 #define RPMAS_TC ((3.14159265358979323 / 180.0) / 3600000.0)  // radians per milliarcsecond
 
@@ -314,6 +319,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     uint32_t *tmem_slot = (uint32_t *)(done_bar + 1);
     volatile int *abort_flag = (volatile int *)(tmem_slot + 1);
     int *gpre = (int *)(smem + G::STAGES * G::STAGE + 256);  // GROUP: unit prefix sums
+    float *rsbuf = (float *)(smem + G::STAGES * G::STAGE + TC_RS_OFF);  // forward: row scales of a unit
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t rank = PAIR ? umma::cluster_ctarank() : 0u;
@@ -612,6 +618,18 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     const int j = ((y0 + 16 * c) % lpad) >> 4;  // anchor of the row within its image
                     an[c] = (vk && j < nanc) ? __ldg(&anc[j]) : make_float2(0.f, 0.f);
                 }
+                // the unit's 256 row scales into this warp's shared copy (one L2 round
+                // trip per unit, issued before the accumulator is ready; the copy of
+                // buffer b was last read by this warp two units ago)
+                float *rsw = rsbuf + ((warp & 3) * 2 + b) * TC_BN;
+                __syncwarp();
+                {
+                    const float4 *src = reinterpret_cast<const float4 *>(rsc + y0);
+                    float4 *d4 = reinterpret_cast<float4 *>(rsw);
+                    d4[lane] = __ldg(src + lane);
+                    d4[lane + 32] = __ldg(src + lane + 32);
+                }
+                __syncwarp();
                 if (!umma::mbar_wait(&tfull[b], (uint32_t)(t >> 1) & 1u, a.budget)) {
                     tc_fail(a.err, abort_flag, 8u);
                     break;
@@ -630,7 +648,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                         are[i] = 0.f;
                         aim[i] = 0.f;
                     }
-                    for (int qq = 0; qq < per; qq++) {
+#pragma unroll 1
+                    for (int qq = 0; qq < per; qq++) {  // a loop, not unrolled: the tile code stays in the instruction cache
                         float2 wv[16];
                         wv[0] = (vk && qq < nanc) ? __ldg(&anc[qq]) : make_float2(0.f, 0.f);
 #pragma unroll
@@ -642,10 +661,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                                 uint32_t r[16];
                                 umma::tmem_ld16(taddr + (uint32_t)(c * 16), r);
                                 float rs[16];
-                                const float4 *rp = reinterpret_cast<const float4 *>(rsc + y0 + 16 * c);
+                                const float4 *rp = reinterpret_cast<const float4 *>(rsw + 16 * c);
 #pragma unroll
-                                for (int v4 = 0; v4 < 4; v4++)
-                                    *reinterpret_cast<float4 *>(&rs[4 * v4]) = __ldg(rp + v4);
+                                for (int v4 = 0; v4 < 4; v4++) *reinterpret_cast<float4 *>(&rs[4 * v4]) = rp[v4];
                                 umma::tmem_ld_wait();
                                 float sr = are[ti], si = aim[ti];
 #pragma unroll
@@ -676,11 +694,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     for (int c = 0; c < TC_BN / 16; c++) {
                         uint32_t r[16];
                         umma::tmem_ld16(taddr + (uint32_t)(c * 16), r);
-                        // power-of-two scales of the 16 image rows (same address in every lane)
+                        // power-of-two scales of the 16 image rows (shared memory, same address in every lane)
                         float rs[16];
-                        const float4 *rp = reinterpret_cast<const float4 *>(rsc + y0 + 16 * c);
+                        const float4 *rp = reinterpret_cast<const float4 *>(rsw + 16 * c);
 #pragma unroll
-                        for (int v4 = 0; v4 < 4; v4++) *reinterpret_cast<float4 *>(&rs[4 * v4]) = __ldg(rp + v4);
+                        for (int v4 = 0; v4 < 4; v4++) *reinterpret_cast<float4 *>(&rs[4 * v4]) = rp[v4];
                         umma::tmem_ld_wait();
                         float2 w = an[c];
 #pragma unroll
