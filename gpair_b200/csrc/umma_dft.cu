@@ -859,18 +859,11 @@ __device__ __forceinline__ float warp_max_f(float v)
     return v;
 }
 
-// max over aligned groups of `lanes` lanes (a power of two <= 32)
-__device__ __forceinline__ float group_max_f(float v, int lanes)
-{
-    for (int off = lanes >> 1; off > 0; off >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, off));
-    return v;
-}
 
 // Row-wise prep of the forward's image operand. A block of PR_THREADS threads
-// works on R image rows at a time: W warps (a power of two) per row when N >
-// 256 (R = 8 / W), else one warp for 32 / lpr rows of lpr lanes each (lpr: the
-// fewest lanes, a power of two, whose 8 pixels each cover the row; 32 when N is
-// not a multiple of 8), so that narrow rows leave no lane idle:
+// works on R = 8 / W image rows at a time, W warps (a power of two) per row.
+// (Narrow rows packed several to a warp, with a quarter of the blocks at 64²,
+// measured slower in a 64-instance batch: 13.2 ms of trial prep against 11.3.)
 //   MODE 0  the image as it is; with `reduce`, its flux, regulariser and max
 //   MODE 1  the line-search trial I = max(I + s d, minval), s = cg.s, written to
 //           dst, with its flux, regulariser and max
@@ -878,7 +871,7 @@ __device__ __forceinline__ float group_max_f(float v, int lanes)
 //           dst + j npix and to operand rows j Lpad + y, with its flux and
 //           regulariser; nothing when `gate` is set and *gate is 0
 // Every row gets its own power-of-two scale 2^(15 - e), e the exponent of the
-// row's max |I| (a reduction over the row's lanes or warps: no pass over the whole image
+// row's max |I| (a reduction over the row's warps: no pass over the whole image
 // has to end before the split), and the forward epilogue multiplies
 // accumulator column y by rsc[row] = 2^(e - 15 - TC_TW_LOG2), exactly. With N a
 // multiple of 8 and N <= 256 W every lane holds 8 consecutive pixels of its row
@@ -902,7 +895,7 @@ struct PrepRowsArgs {
     const float *img, *d;
     float *dst;
     const float *model;
-    int N, W, lpr, Lpad, Kx_pad;  // W warps per row (N > 256) or lpr lanes per row (W = 1)
+    int N, W, Lpad, Kx_pad;  // W warps per row
     void *hi, *lo;  // OT
     uint8_t *h8, *l8;
     float *rsc;
@@ -939,13 +932,9 @@ __device__ __forceinline__ void tc_prep_rows_body(const PrepRowsArgs &A, const G
     const bool red = MODE ? true : reduce != 0;
     if (MODE == 2) dst += (size_t)j * N * N;
     const size_t row0 = (size_t)j * Lpad;
-    // LPR lanes per row (W = 1 and narrow rows: several rows per warp), else W warps per row
-    const int LPR = A.lpr, RPW = 32 / LPR;
-    const int R = W > 1 ? PR_WARPS_MAX / W : PR_WARPS_MAX * RPW;  // rows per block and pass
-    const int sub = warp % W;                                     // this warp's part of its row
-    const int rw = W > 1 ? warp / W : warp * RPW + lane / LPR;    // row within the pass
-    const int t = W > 1 ? sub * 32 + lane : lane % LPR;           // thread within the row's group
-    const int nt = W > 1 ? 32 * W : LPR;
+    const int R = PR_WARPS_MAX / W;            // rows per block and pass
+    const int sub = warp % W, rw = warp / W;   // this warp's part of its row, row within the pass
+    const int t = sub * 32 + lane, nt = 32 * W;  // thread within the row's group
     double acc[2] = {0.0, 0.0};
     float mx = 0.f;
     const bool vec = (N & 7) == 0 && N <= 8 * nt;
@@ -1001,17 +990,13 @@ __device__ __forceinline__ void tc_prep_rows_body(const PrepRowsArgs &A, const G
                 rmax = fmaxf(rmax, fabsf(I));
             }
         }
-        // max over the row's lanes (LPR), or over its W warps
-        if (W == 1) {
-            rmax = group_max_f(rmax, LPR);
-        } else {
-            rmax = warp_max_f(rmax);
-            if (lane == 0) wmax[warp] = rmax;
-            __syncthreads();
-            rmax = 0.f;
-            for (int q = 0; q < W; q++) rmax = fmaxf(rmax, wmax[rw * W + q]);
-            __syncthreads();  // wmax is rewritten by the next pass
-        }
+        // max over the row's W warps
+        rmax = warp_max_f(rmax);
+        if (lane == 0) wmax[warp] = rmax;
+        __syncthreads();
+        rmax = 0.f;
+        for (int q = 0; q < W; q++) rmax = fmaxf(rmax, wmax[rw * W + q]);
+        __syncthreads();  // wmax is rewritten by the next pass
         int ex = 0;
         frexpf(rmax, &ex);
         const float scale = ldexpf(1.f, 15 - ex);
@@ -1768,22 +1753,10 @@ static TcMaps tc_fwd_maps(const TcState *t, bool batch)
 // Row-wise prep launches (k_tc_prep_rows): PR_THREADS threads per block, R rows
 // per block and pass; at most GP_MAX_PARTIALS blocks (three partials each fit
 // the RED_PREP slot), a batch at most 1024 per trial (two partials each).
-// lanes per row with one warp per row: 8 pixels per lane (16-byte loads) when N
-// is a multiple of 8, the fewest lanes (a power of two) that cover the row;
-// else a whole warp
-static inline int pr_lanes_per_row(int N)
-{
-    if ((N & 7) != 0 || N > 256) return 32;
-    int l = 1;
-    while (8 * l < N) l <<= 1;
-    return l;
-}
-
 static PrepRowsArgs tc_prep_rows_args(gpair_ctx *c, TcState *t, int mode, int reduce, double *partials,
                                       const float *img)
 {
-    const int W = pr_warps_per_row(c->N), lpr = W > 1 ? 32 : pr_lanes_per_row(c->N);
-    const int R = W > 1 ? PR_WARPS_MAX / W : PR_WARPS_MAX * (32 / lpr);
+    const int W = pr_warps_per_row(c->N), R = PR_WARPS_MAX / W;
     int gx = gp_cdiv(c->N, R);
     const int cap = mode == 2 ? 1024 : GP_MAX_PARTIALS;
     if (gx > cap) gx = cap;
@@ -1797,7 +1770,6 @@ static PrepRowsArgs tc_prep_rows_args(gpair_ctx *c, TcState *t, int mode, int re
     a.model = c->model;
     a.N = c->N;
     a.W = W;
-    a.lpr = lpr;
     a.Lpad = b ? t->Lb : 0;
     a.Kx_pad = t->Kx_pad;
     a.hi = b ? t->imgb_hi : t->img_hi;

@@ -3,6 +3,17 @@ evaluation, for the named workloads.
 
     python -m gpair_b200.stage_report [--workloads precision large] [--reps 10]
     python -m gpair_b200.stage_report --workloads large --cg 1 [--method 2] [--line-search 0]
+    python -m gpair_b200.stage_report --batch 64 [--iters 30] [--precision 4]
+
+A workload is a named one (gpair_b200.synth.workload) or instance:SEED, one
+problem of the many-instance workload (gpair_b200.instances.instance).
+
+With --batch N: N instances of the many-instance workload, autotuned as the
+benchmark tunes them, their adjoint split-K lengths set for sharing the GPU
+(gpair_set_shared_splits), run as one staged lockstep batch with the batched
+line search; prints the device time and the per-launch time of every stage
+summed over the run (device timer stamps, gpair_batch_stage_stamps), with the
+SM clock sampled during the run.
 
 With --cg N the module instead runs N CG iterations from the flat prior,
 driven from the host (every kernel a plain launch, so that a profiler's
@@ -53,9 +64,58 @@ def stage_bytes(p: api.Problem, splits: int, row_tiles: int) -> dict:
     }
 
 
+def problem(name: str) -> api.Problem:
+    """A named workload, or instance:SEED of the many-instance workload."""
+    if name.startswith("instance:"):
+        from .instances import instance
+        return instance(int(name.split(":", 1)[1]))
+    return api.workload_problem(name)
+
+
+def batch_report(n: int, iters: int, precision: int) -> dict:
+    """Stage breakdown of a staged lockstep batch of n many-instance problems."""
+    from .clocks import ClockSampler
+    from .instances import instances
+    ps = instances(n)
+    recs = [api.Reconstructor(0) for _ in ps]
+    try:
+        for r, p in zip(recs, ps):
+            r.set_problem(p)
+            r.set_precision(precision)
+            r.set_image(p.start_image())
+        flags = api.TUNE_PRECISION | api.TUNE_SPLITS | api.TUNE_CACHE | api.TUNE_BATCHED | api.TUNE_TILE
+        for r in recs:
+            r.autotune(flags, reps=2)
+        api.shared_splits(recs)
+        with api.Batch(recs, line_search=api.LS_BATCH, stamps=True) as b:
+            for r, p in zip(recs, ps):
+                r.set_image(p.start_image())
+            b.run(1)  # first launch
+            b.stage_times_us(reset=True)
+            for r, p in zip(recs, ps):
+                r.set_image(p.start_image())
+            sampler = ClockSampler(0)
+            sampler.start()
+            res = b.run(iters)
+            clocks = sampler.stop()
+            dev_ms = recs[0].last_run_stats()[0]
+            flops = sum(r.last_run_stats()[1] for r in recs)
+            stages = b.stage_times_us()
+            layout = b.grouped
+    finally:
+        for r in recs:
+            r.close()
+    total = sum(v for k, v in stages.items() if k != "batched_evaluations")
+    return {"instances": n, "iterations": iters, "precision": precision, "layout": layout,
+            "device_ms": dev_ms, "tflops": flops / (dev_ms * 1e-3) / 1e12, "clocks": clocks,
+            "all_ok": all(o["status"] == 0 for o in res),
+            "stage_us": stages, "stage_share": {k: v / total for k, v in stages.items() if k != "batched_evaluations"},
+            "timing": "device timer stamps after every launch (one small timer kernel each), summed over the run"}
+
+
 def report(name: str, reps: int = 10, pair: bool = False, precision: int = api.PREC_SPLIT16) -> dict:
     from .clocks import ClockSampler
-    p = api.workload_problem(name)
+    p = problem(name)
     with api.Reconstructor(0) as rec:
         rec.set_problem(p)
         rec.set_precision(precision)
@@ -119,10 +179,15 @@ def main(argv=None):
     ap.add_argument("--line-search", type=int, default=0, help="0 the reference's search, 1 batched")
     ap.add_argument("--precision", type=int, default=api.PREC_SPLIT16)
     ap.add_argument("--tc-pair", type=int, default=1, help="contractions on CTA pairs (cta_group::2, 1) or single CTAs (0)")
+    ap.add_argument("--batch", type=int, default=0, help="stage breakdown of a staged batch of this many instances")
+    ap.add_argument("--iters", type=int, default=30, help="CG iterations of the --batch run")
     args = ap.parse_args(argv)
+    if args.batch > 0:
+        print(json.dumps(batch_report(args.batch, args.iters, args.precision)), flush=True)
+        return
     for w in args.workloads:
         if args.cg > 0:
-            p = api.workload_problem(w)
+            p = problem(w)
             with api.Reconstructor(0) as rec:
                 rec.set_problem(p)
                 rec.set_precision(args.precision)
