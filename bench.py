@@ -347,7 +347,7 @@ def combine_over_ranks(times, work, device=None):
     return [float(x) for x in t.tolist()], [float(x) for x in w.tolist()]
 
 
-def many_instances(n: int, iters: int) -> dict:
+def many_instances(n: int, iters: int, precision: int) -> dict:
     """n independent reconstructions of uneven size (widths 64-256, 500-8,000 uv)
     for `iters` batched-line-search CG iterations each: one after another, all
     at once through gpair_cg_run_many (each context's graph on its own stream),
@@ -363,15 +363,17 @@ def many_instances(n: int, iters: int) -> dict:
     ps = instances(n)
     recs = [g.Reconstructor(0) for _ in ps]
     try:
+        # one precision path and single-CTA tiles for all instances (one class per contraction
+        # in a staged batch: 80.2 ms against 82.4 ms with precision and tile autotuned per
+        # instance, python -m gpair_b200.stage_report --batch 64 --tune splits|all); the
+        # adjoint split-K length autotuned per instance shape, cached across equal shapes
         for r, p in zip(recs, ps):
+            r.set_tc_pair(False)
             r.set_problem(p)
-            r.set_precision(g.PREC_SPLIT16)
+            r.set_precision(precision)
             r.set_image(p.start_image())
-        # autotuned configuration per instance shape (precision path, tensor-core tile,
-        # adjoint split-K), cached across instances of the same shape
         t0 = time.perf_counter()
-        flags = (g.api.TUNE_PRECISION | g.api.TUNE_SPLITS | g.api.TUNE_CACHE | g.api.TUNE_BATCHED |
-                 g.api.TUNE_TILE)
+        flags = g.api.TUNE_SPLITS | g.api.TUNE_CACHE | g.api.TUNE_BATCHED
         tuned = [r.autotune(flags, reps=2) for r in recs]
         t_tune = time.perf_counter() - t0
         for r, p in zip(recs, ps):
@@ -427,7 +429,8 @@ def many_instances(n: int, iters: int) -> dict:
             "one_launch_independent_s": one["independent"]["s"],
             "tflops_one_launch_independent": one["independent"]["tflops"],
             "all_ok": all(r_["status"] == 0 for r_ in res) and all(v["all_ok"] for v in one.values()),
-            "autotune": {"s": t_tune, "tuned": sum(not t["from_cache"] for t in tuned),
+            "autotune": {"what": "adjoint split-K per instance shape; precision path and single-CTA tiles fixed",
+                         "s": t_tune, "tuned": sum(not t["from_cache"] for t in tuned),
                          "fp32_path": sum(t["precision"] == g.PREC_FP32 for t in tuned),
                          "split16_path": sum(t["precision"] == g.PREC_SPLIT16 for t in tuned),
                          "split16f8_path": sum(t["precision"] == g.PREC_SPLIT16F8 for t in tuned),
@@ -822,7 +825,7 @@ def run_ours(args, rank, world, local):
             line["time_to_objective"] = time_to_objective(args.tto_problems, race_fr=args.tto_race_fr,
                                                           method=args.tto_method)
         if args.instances > 0:
-            line["many_instances"] = many_instances(args.instances, args.instance_iters)
+            line["many_instances"] = many_instances(args.instances, args.instance_iters, prec)
         if args.small_iters > 0:
             cpu = None
             if cpu_small is not None:

@@ -255,6 +255,7 @@ struct BatchGraph {
     // staged lockstep: every stage grouped (per class: the image forward and the adjoint)
     int staged;
     void **grps_img, **grps_adj;
+    int nadj;  // grouped adjoints (classes without the forward operand kind)
     void *stg_args[GS_COUNT];  // device: argument structs of every instance, lockstep order
     int *stg_start[GS_COUNT];  // device: block starts [n + 1]
     int stg_total[GS_COUNT];
@@ -299,8 +300,9 @@ void gp_batch_graph_free(void *bg)
     for (int k = 0; k < B->ngrp; k++) {
         gp_tc_group_free(B->grps[k]);
         if (B->grps_img) gp_tc_group_free(B->grps_img[k]);
-        if (B->grps_adj) gp_tc_group_free(B->grps_adj[k]);
     }
+    for (int k = 0; k < B->nadj; k++)
+        if (B->grps_adj) gp_tc_group_free(B->grps_adj[k]);
     free(B->grps);
     free(B->grps_img);
     free(B->grps_adj);
@@ -690,6 +692,13 @@ static int build_lockstep_staged(gpair_ctx **ctx_in, int n, BatchGraph *B, int w
             cls_begin.push_back(k);
     cls_begin.push_back(n);
     const int ngrp = (int)cls_begin.size() - 1;
+    // adjoint classes: the same without the forward operand kind (key >> 3), contiguous in key order
+    std::vector<int> acls_begin;
+    for (int k = 0; k < n; k++)
+        if (acls_begin.empty() || (key[order[k]] >> 3) != (key[order[k - 1]] >> 3) || k - acls_begin.back() == 256)
+            acls_begin.push_back(k);
+    acls_begin.push_back(n);
+    const int nadj = (int)acls_begin.size() - 1;
     // every instance's tensor state and batch buffers (no allocation inside a capture)
     for (int k = 0; k < n; k++) {
         int rc = gp_batch_alloc(ctx[k]);
@@ -716,14 +725,18 @@ static int build_lockstep_staged(gpair_ctx **ctx_in, int n, BatchGraph *B, int w
     B->ngrp = ngrp;
     B->grps = (void **)calloc((size_t)ngrp, sizeof(void *));
     B->grps_img = (void **)calloc((size_t)ngrp, sizeof(void *));
-    B->grps_adj = (void **)calloc((size_t)ngrp, sizeof(void *));
+    B->grps_adj = (void **)calloc((size_t)nadj, sizeof(void *));
     if (!B->grps || !B->grps_img || !B->grps_adj) return GPAIR_ERR_ALLOC;
+    B->nadj = nadj;
     int rc = GPAIR_OK;
     for (int q = 0; q < ngrp && !rc; q++) {
         const int k0 = cls_begin[q], k1 = cls_begin[q + 1];
         rc = gp_tc_group_build_kind(&ctx[k0], k1 - k0, GP_TCG_TRIALS, lsg + k0, B->gerr, &B->grps[q]);
         if (!rc) rc = gp_tc_group_build_kind(&ctx[k0], k1 - k0, GP_TCG_IMAGE, act + k0, B->gerr, &B->grps_img[q]);
-        if (!rc) rc = gp_tc_group_build_kind(&ctx[k0], k1 - k0, GP_TCG_ADJOINT, act + k0, B->gerr, &B->grps_adj[q]);
+    }
+    for (int q = 0; q < nadj && !rc; q++) {
+        const int k0 = acls_begin[q], k1 = acls_begin[q + 1];
+        rc = gp_tc_group_build_kind(&ctx[k0], k1 - k0, GP_TCG_ADJOINT, act + k0, B->gerr, &B->grps_adj[q]);
     }
     if (rc) return rc == GPAIR_ERR_STATE ? GPAIR_ERR_CUDA : rc;  // the instances were eligible
     std::vector<double *> trace((size_t)n);
@@ -743,9 +756,9 @@ static int build_lockstep_staged(gpair_ctx **ctx_in, int n, BatchGraph *B, int w
                   : gp_stage_group_launch(c0, st, B->stg_args[st], B->stg_start[st], n, B->stg_total[st], gate);
     };
     // grouped contractions: each class on c0's stream, with the wait budget of its first instance
-    auto gemms = [&](void **grps) {
-        for (int q = 0; q < ngrp; q++) {
-            int r = gp_tc_group_run(grps[q], ctx[cls_begin[q]], c0->stream);
+    auto gemms = [&](void **grps, const std::vector<int> &cb) {
+        for (size_t q = 0; q + 1 < cb.size(); q++) {
+            int r = gp_tc_group_run(grps[q], ctx[cb[q]], c0->stream);
             if (r) return r;
         }
         return GPAIR_OK;
@@ -787,11 +800,11 @@ static int build_lockstep_staged(gpair_ctx **ctx_in, int n, BatchGraph *B, int w
         [&]() {
             int r;
             if ((r = stamp(0)) || (r = stage(GS_PREP_IMAGE, act)) || (r = stamp(1))) return r;
-            if ((r = gemms(B->grps_img)) || (r = stamp(2))) return r;
+            if ((r = gemms(B->grps_img, cls_begin)) || (r = stamp(2))) return r;
             if ((r = stage(GS_VIS_DATA, act)) || (r = stamp(3))) return r;
             if ((r = stage(GS_ADJ_WEIGHTS, act)) || (r = stamp(4))) return r;
             if ((r = stage(GS_BUILD_W, act)) || (r = stamp(5))) return r;
-            if ((r = gemms(B->grps_adj)) || (r = stamp(6))) return r;
+            if ((r = gemms(B->grps_adj, acls_begin)) || (r = stamp(6))) return r;
             if ((r = stage(GS_GRAD_FINALIZE, act)) || (r = stamp(7))) return r;
             if ((r = stage(GS_DESCENT, act)) || (r = stamp(8))) return r;
             if ((r = route(GR_LS0S, h_ls))) return r;
@@ -819,7 +832,7 @@ static int build_lockstep_staged(gpair_ctx **ctx_in, int n, BatchGraph *B, int w
         [&]() {
             int r;
             if ((r = stamp(10)) || (r = stage(GS_PREP_TRIALS, lsg)) || (r = stamp(11))) return r;
-            if ((r = gemms(B->grps)) || (r = stamp(12))) return r;
+            if ((r = gemms(B->grps, cls_begin)) || (r = stamp(12))) return r;
             if ((r = stage(GS_CHI2_BATCH, lsg)) || (r = stamp(13))) return r;
             if ((r = route(GR_LSN, h_ls))) return r;
             return stamp(14);

@@ -225,7 +225,9 @@ int gp_set_problem_core(gpair_ctx *c, int N, float pix, int nuv, const gpair_uv 
     GP_CUDA(c, cudaMalloc(&c->uvc, nk * sizeof(float2)));
     GP_CUDA(c, cudaMalloc(&c->fx, nk * N * sizeof(float2)));
     GP_CUDA(c, cudaMalloc(&c->fy, nk * N * sizeof(float2)));
-    GP_CUDA(c, cudaMalloc(&c->vpart, (size_t)c->mt * nk * sizeof(float2)));
+    // partial visibility entries: the CUDA-core forward's row tiles or the tensor forward's entries
+    const int mt_cap = c->mt > gp_tc_forward_entries(N) ? c->mt : gp_tc_forward_entries(N);
+    GP_CUDA(c, cudaMalloc(&c->vpart, (size_t)mt_cap * nk * sizeof(float2)));
     GP_CUDA(c, cudaMalloc(&c->visd, nk * sizeof(double2)));
     GP_CUDA(c, cudaMalloc(&c->visi, nk * sizeof(float2)));
     GP_CUDA(c, cudaMalloc(&c->cw, nk * sizeof(float2)));

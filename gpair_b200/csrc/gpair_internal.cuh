@@ -457,6 +457,7 @@ void gp_tc_group_free(void *grp);
 // forward row tiles and adjoint split count of a context's tensor state (what
 // its forward and adjoint launches would set in c->mt and c->splits)
 int gp_tc_stage_sizes(gpair_ctx *c, int *mt, int *splits);
+int gp_tc_forward_entries(int N);
 int gp_tc_shared_splits(gpair_ctx **ctx, int n);
 
 // Grouped stage kernels (group.cuh): the argument struct of one instance for

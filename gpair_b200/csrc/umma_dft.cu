@@ -16,20 +16,22 @@
 // N = 256 operand (TMEM columns).
 // Forward DFT (kernel_visi.cl / cpu.c:449-475):
 //   T[n][y] = sum_x Fx16[n][x] I[y][x],  row n = 2k+c holds (Re, Im) Fx[k][x]
-//   epilogue: the thread of row n sums over its 256 columns against one
-//   contiguous row of Fy (prefetched a chunk ahead); the Re/Im row pair is
-//   combined with one shuffle: Vpart[ytile][k] = sum_y (T[2k][y] + i T[2k+1][y]) Fy[k][y]
+//   epilogue: the thread of row n sums over its 128 columns against Fy (an
+//   anchor every 16 rows, rotated within the chunk); the Re/Im row pair is
+//   combined with one shuffle: Vpart[entry][k] = sum_y (T[2k][y] + i T[2k+1][y]) Fy[k][y],
+//   one entry per 128 image rows (per image of a stack of smaller images)
 // Adjoint (kernel_grad_pow.cl + kernel_grad_bis.cl / cpu.c:279-369):
 //   G[y][x] = sum_k' FxT[x][k'] W[y][k'],  W[y][2k] = Re(c_k Fy[k][y]),
 //   W[y][2k+1] = -Im(c_k Fy[k][y]),  FxT[x][2k+c] = (Re, Im) Fx[k][x]
-//   the thread of image column x stores G[y][x] for its 256 rows (consecutive
+//   the thread of image column x stores G[y][x] for its 128 rows (consecutive
 //   lanes write consecutive x); split over k' into S partial images that
 //   k_grad_finalize sums in a fixed order
 //
-// One persistent CTA per SM (or CTA pair per two SMs), 192 threads: warp 0
+// One persistent CTA per SM (or CTA pair per two SMs), 320 threads: warp 0
 // issues TMA loads (a ring of 2 stages of 96 KB, or 3 of 64 KB per CTA of a
 // pair), warp 1 owns TMEM (512 columns = two FP32 accumulators of 256
-// columns) and one of its threads issues tcgen05.mma; warps 2-5 drain TMEM.
+// columns) and one of its threads issues tcgen05.mma; warps 2-9 drain TMEM,
+// two per lane quarter, each taking 128 of the accumulator's 256 columns.
 // All waits are bounded; a timeout sets an error code, the roles stop, TMEM is
 // released, and the host reports GPAIR_ERR_TIMEOUT.
 #include <cuda.h>
@@ -48,7 +50,14 @@
 #define TC_BN 256
 #define TC_ROWB 128  // bytes of one K-block row: 64 f16 or 32 TF32 elements
 #define TC_STAGES 2
-#define TC_THREADS 192
+// warps: 0 TMA producer, 1 MMA issuer, then the epilogue warps: the forward has
+// TC_EPI_WARPS, two per TMEM lane quarter, each with TC_EPI_COLS accumulator
+// columns; the adjoint's store epilogue TC_STORE_WARPS, one per quarter (eight
+// measured 35 % slower there: the extra warps share the issue slots of the TMA
+// and MMA warps' sub-partitions while the units are MMA-bound)
+#define TC_EPI_WARPS 8
+#define TC_EPI_COLS (TC_BN * 4 / TC_EPI_WARPS)
+#define TC_STORE_WARPS 4
 #define TC_TW_LOG2 10  // twiddle operands are scaled by 2^10
 #define TC_A_BYTES (TC_BM * TC_ROWB)
 #define TC_B_BYTES (TC_BN * TC_ROWB)
@@ -58,13 +67,16 @@
 // (up to TC_GROUP_MAX instances), then the forward epilogue's row scales of a
 // unit, one copy per epilogue warp and accumulator buffer
 #define TC_RS_OFF (256 + 4 * 272)
-#define TC_RS_BYTES (4 * 2 * TC_BN * 4)
+#define TC_RS_BYTES (TC_EPI_WARPS * 2 * TC_EPI_COLS * 4)
 #define TC_SMEM_BYTES (1024 + TC_STAGES * TC_STAGE_BYTES + TC_RS_OFF + TC_RS_BYTES)
 #define TC_SMEM_GROUP_BYTES TC_SMEM_BYTES
 #define TC_WAIT_BUDGET 4000000000LL  // default clock cycles (~2 s) per pipeline wait
 #define RPMAS_TC ((3.14159265358979323 / 180.0) / 3600000.0)  // radians per milliarcsecond
 
 enum { EPI_FWD = 0, EPI_STORE = 1 };
+
+template <int EPI> constexpr int tc_epi_warps() { return EPI == EPI_FWD ? TC_EPI_WARPS : TC_STORE_WARPS; }
+template <int EPI> constexpr int tc_threads() { return 64 + 32 * tc_epi_warps<EPI>(); }
 
 // Operand element types: f16 (kind::f16, K = 16 per MMA) or TF32 held as FP32
 // bit patterns (kind::tf32, K = 8 per MMA). Both fill 128-byte K-block rows,
@@ -299,7 +311,7 @@ static_assert(TcGeo<0>::STAGES * TcGeo<0>::STAGE == TcGeo<1>::STAGES * TcGeo<1>:
 // the three f16 products. Maps: (A_hi, A_lo, A_x) = (f16 hi, E4M3 hi, E4M3 lo)
 // and likewise for B; A_x and B_x are not used by the other operand kinds.
 template <int EPI, int OP, int NPROD, int PAIR, int GROUP>
-__global__ void __launch_bounds__(TC_THREADS, 1)
+__global__ void __launch_bounds__(tc_threads<EPI>(), 1)
     k_tc_gemm(const __grid_constant__ CUtensorMap tA_hi, const __grid_constant__ CUtensorMap tA_lo,
               const __grid_constant__ CUtensorMap tA_x, const __grid_constant__ CUtensorMap tB_hi,
               const __grid_constant__ CUtensorMap tB_lo, const __grid_constant__ CUtensorMap tB_x, const TcArgs a)
@@ -333,7 +345,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         }
         for (int b = 0; b < 2; b++) {
             umma::mbar_init(&tfull[b], 1);
-            umma::mbar_init(&tempty[b], PAIR ? 256 : 128);  // pair: both CTAs' epilogues release
+            umma::mbar_init(&tempty[b], (PAIR ? 2 : 1) * 32 * tc_epi_warps<EPI>());  // pair: both CTAs' epilogues release
         }
         umma::mbar_init(done_bar, 1);
         *abort_flag = 0;
@@ -578,7 +590,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         __syncwarp();
     } else {
         // ---------------------------------------------------- epilogue
-        const int q = warp & 3;  // TMEM lane quarter this warp may access
+        const int ew = warp - 2;                 // epilogue warp
+        const int q = warp & 3;                  // TMEM lane quarter this warp may access
+        constexpr int ECOLS = TC_BN * 4 / tc_epi_warps<EPI>();  // accumulator columns per epilogue warp
+        const int c0 = (ew >> 2) * ECOLS;                        // its first accumulator column
         // the accumulator buffers are released on the leader's barriers
         const uint32_t te0 = PAIR ? umma::mapa_shared(umma::smem_u32(&tempty[0]), 0) : 0u;
         const uint32_t te1 = PAIR ? umma::mapa_shared(umma::smem_u32(&tempty[1]), 0) : 0u;
@@ -589,10 +604,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             const int b = t & 1;
             const int arow = m * G::MT + (int)rank * 128 + q * 32 + lane;  // row of the twiddle-side operand
             const int y0 = n * TC_BN;                                      // first image row of the columns
-            const uint32_t taddr = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * TC_BN);
+            const uint32_t taddr = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * TC_BN + c0);
             if (EPI == EPI_FWD) {
-                // Fy[k][y] along this thread's 256 columns: an FP64-accurate anchor every
-                // 16 rows, rotated by r_k = e^{-2 pi i s v_k} within the chunk (<= 15 steps)
+                // Fy[k][y] along this thread's TC_EPI_COLS columns: an FP64-accurate anchor
+                // every 16 rows, rotated by r_k = e^{-2 pi i s v_k} within the chunk (<= 15
+                // steps). Partial entries hold at most TC_EPI_COLS rows (elog2 <= 7), so
+                // that no entry spans two epilogue warps.
                 const float2 *fya = a.fya, *fyr = a.fyr;
                 const float *rsc = a.rsc;
                 float2 *vpart = a.vpart;
@@ -612,22 +629,21 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 const bool vk = k < nuv;
                 const float2 rot = vk ? __ldg(&fyr[k]) : make_float2(0.f, 0.f);
                 const float2 *anc = fya + (size_t)(vk ? k : 0) * nanc;
-                float2 an[TC_BN / 16];
+                float2 an[TC_EPI_COLS / 16];
 #pragma unroll
-                for (int c = 0; c < TC_BN / 16; c++) {
-                    const int j = ((y0 + 16 * c) % lpad) >> 4;  // anchor of the row within its image
+                for (int c = 0; c < TC_EPI_COLS / 16; c++) {
+                    const int j = ((y0 + c0 + 16 * c) % lpad) >> 4;  // anchor of the row within its image
                     an[c] = (vk && j < nanc) ? __ldg(&anc[j]) : make_float2(0.f, 0.f);
                 }
-                // the unit's 256 row scales into this warp's shared copy (one L2 round
-                // trip per unit, issued before the accumulator is ready; the copy of
-                // buffer b was last read by this warp two units ago)
-                float *rsw = rsbuf + ((warp & 3) * 2 + b) * TC_BN;
+                // the row scales of this warp's columns into its shared copy (one L2
+                // round trip per unit, issued before the accumulator is ready; the copy
+                // of buffer b was last read by this warp two units ago)
+                float *rsw = rsbuf + (ew * 2 + b) * TC_EPI_COLS;
                 __syncwarp();
                 {
-                    const float4 *src = reinterpret_cast<const float4 *>(rsc + y0);
-                    float4 *d4 = reinterpret_cast<float4 *>(rsw);
-                    d4[lane] = __ldg(src + lane);
-                    d4[lane + 32] = __ldg(src + lane + 32);
+                    static_assert(TC_EPI_COLS == 128, "one float4 per lane");
+                    const float4 *src = reinterpret_cast<const float4 *>(rsc + y0 + c0);
+                    reinterpret_cast<float4 *>(rsw)[lane] = __ldg(src + lane);
                 }
                 __syncwarp();
                 if (!umma::mbar_wait(&tfull[b], (uint32_t)(t >> 1) & 1u, a.budget)) {
@@ -636,15 +652,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 }
                 umma::tc_fence_after();
                 const int emask = (1 << elog2) - 1;
-                if (lpad < TC_BN) {
-                    // several images per tile (a batch stack of lpad = 32, 64 or 128 rows
-                    // each; y0 is a multiple of lpad): chunk q of every image has the
-                    // same 16 values of Fy, formed once for all of them. Each image's
-                    // sum takes its chunks and rows in the order of the loop below.
-                    const int per = lpad >> 4, nimg = TC_BN / lpad;
-                    float are[TC_BN / 32], aim[TC_BN / 32];
+                if (lpad < TC_EPI_COLS) {
+                    // several images in this warp's columns (a batch stack of lpad = 32 or
+                    // 64 rows each; y0 + c0 is a multiple of lpad): chunk q of every image
+                    // has the same 16 values of Fy, formed once for all of them. Each
+                    // image's sum takes its chunks and rows in the order of the loop below.
+                    const int per = lpad >> 4, nimg = TC_EPI_COLS / lpad;
+                    float are[TC_EPI_COLS / 32], aim[TC_EPI_COLS / 32];
 #pragma unroll
-                    for (int i = 0; i < TC_BN / 32; i++) {
+                    for (int i = 0; i < TC_EPI_COLS / 32; i++) {
                         are[i] = 0.f;
                         aim[i] = 0.f;
                     }
@@ -655,7 +671,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 #pragma unroll
                         for (int j = 1; j < 16; j++) wv[j] = fy_step(wv[j - 1], rot);
 #pragma unroll
-                        for (int ti = 0; ti < TC_BN / 32; ti++) {
+                        for (int ti = 0; ti < TC_EPI_COLS / 32; ti++) {
                             if (ti < nimg) {  // warp-uniform
                                 const int c = ti * per + qq;
                                 uint32_t r[16];
@@ -678,9 +694,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                         }
                     }
 #pragma unroll
-                    for (int ti = 0; ti < TC_BN / 32; ti++) {
+                    for (int ti = 0; ti < TC_EPI_COLS / 32; ti++) {
                         if (ti < nimg) {
-                            const int entry = (y0 + ti * lpad) >> elog2;
+                            const int entry = (y0 + c0 + ti * lpad) >> elog2;
                             const float re = are[ti], im = aim[ti];
                             const float ore = __shfl_xor_sync(0xffffffffu, re, 1);
                             const float oim = __shfl_xor_sync(0xffffffffu, im, 1);
@@ -691,7 +707,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 } else {
                     float sre = 0.f, sim = 0.f;
 #pragma unroll
-                    for (int c = 0; c < TC_BN / 16; c++) {
+                    for (int c = 0; c < TC_EPI_COLS / 16; c++) {
                         uint32_t r[16];
                         umma::tmem_ld16(taddr + (uint32_t)(c * 16), r);
                         // power-of-two scales of the 16 image rows (shared memory, same address in every lane)
@@ -708,11 +724,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                             sim = fmaf(tv, w.y, sim);
                             w = fy_step(w, rot);
                         }
-                        if (((y0 + 16 * c + 16) & emask) == 0) {
+                        if (((y0 + c0 + 16 * c + 16) & emask) == 0) {
                             // end of a partial entry (warp-uniform): combine the Re/Im row
                             // pair, store. even row: (sum T_re F_re, sum T_re F_im);
                             // odd row: (sum T_im F_re, sum T_im F_im)
-                            const int entry = (y0 + 16 * c) >> elog2;
+                            const int entry = (y0 + c0 + 16 * c) >> elog2;
                             const float re = sre, im = sim;
                             const float ore = __shfl_xor_sync(0xffffffffu, re, 1);
                             const float oim = __shfl_xor_sync(0xffffffffu, im, 1);
@@ -741,14 +757,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 const int x = arow;
                 const bool xv = x < out_cols;
 #pragma unroll 1
-                for (int c = 0; c < TC_BN / 16; c++) {
+                for (int c = 0; c < ECOLS / 16; c++) {
                     uint32_t r[16];
                     umma::tmem_ld16(taddr + (uint32_t)(c * 16), r);
                     umma::tmem_ld_wait();
                     if (xv) {
 #pragma unroll
                         for (int j = 0; j < 16; j++) {
-                            const int y = y0 + c * 16 + j;
+                            const int y = y0 + c0 + c * 16 + j;
                             if (y < out_rows) out[(size_t)y * out_ld + x] = __uint_as_float(r[j]);
                         }
                     }
@@ -1555,7 +1571,7 @@ int gp_tc_prepare(gpair_ctx *c)
         at[0].val.clusterDim.y = 1;
         at[0].val.clusterDim.z = 1;
         cfg.gridDim = dim3(2 * (unsigned)t->npairs, 1, 1);
-        cfg.blockDim = dim3(TC_THREADS, 1, 1);
+        cfg.blockDim = dim3(tc_threads<EPI_FWD>(), 1, 1);
         cfg.dynamicSmemBytes = TC_SMEM_BYTES;
         cfg.attrs = at;
         cfg.numAttrs = 1;
@@ -1694,7 +1710,7 @@ static cudaError_t tc_launch_kind(TcState *t, dim3 grid, cudaStream_t st, int pd
     memset(&cfg, 0, sizeof(cfg));
     cudaLaunchAttribute at[2];
     cfg.gridDim = grid;
-    cfg.blockDim = dim3(TC_THREADS, 1, 1);
+    cfg.blockDim = dim3(tc_threads<EPI>(), 1, 1);
     cfg.dynamicSmemBytes = TC_SMEM_BYTES;
     cfg.stream = st;
     cfg.attrs = at;
@@ -1819,12 +1835,12 @@ int gp_tc_forward_gemm(gpair_ctx *c)
     a.nanc = t->nanc;
     a.N = c->N;
     a.nuv = c->nuv;
-    a.lpad = t->M_pad;  // one image, partial entries of one 256-row tile each
-    a.elog2 = 8;
+    a.lpad = t->M_pad;  // one image, partial entries of TC_EPI_COLS rows (one epilogue warp's columns)
+    a.elog2 = 7;
     a.rsc = t->rsc;
     a.vpart = c->vpart;
     if ((rc = tc_launch<EPI_FWD>(c, t, tc_fwd_maps(t, false), a))) return rc;
-    c->mt = a.n_tiles;
+    c->mt = t->M_pad / TC_EPI_COLS;
     return GPAIR_OK;
 }
 
@@ -1839,7 +1855,7 @@ int gp_tc_batch_prepare(gpair_ctx *c, int *epp)
     if (!t->imgb_hi) {
         const int N = c->N;
         t->Lb = N <= 32 ? 32 : N <= 64 ? 64 : N <= 128 ? 128 : round_up(N, TC_BN);
-        const int erows = t->Lb < TC_BN ? t->Lb : TC_BN;
+        const int erows = t->Lb < TC_EPI_COLS ? t->Lb : TC_EPI_COLS;
         t->epp_b = t->Lb / erows;
         const size_t rows = (size_t)GP_NTR * t->Lb, n = rows * t->Kx_pad;
         GP_CUDA(c, cudaMalloc(&t->rscb, sizeof(float) * rows));
@@ -1901,8 +1917,8 @@ int gp_tc_forward_batch_gemm(gpair_ctx *c)
     a.N = c->N;
     a.nuv = c->nuv;
     a.lpad = t->Lb;
-    const int erows = t->Lb < TC_BN ? t->Lb : TC_BN;
-    a.elog2 = erows == 32 ? 5 : erows == 64 ? 6 : erows == 128 ? 7 : 8;
+    const int erows = t->Lb < TC_EPI_COLS ? t->Lb : TC_EPI_COLS;
+    a.elog2 = erows == 32 ? 5 : erows == 64 ? 6 : 7;
     a.rsc = t->rscb;
     a.vpart = c->vpart_b;
     return tc_launch<EPI_FWD>(c, t, tc_fwd_maps(t, true), a);
@@ -2028,14 +2044,16 @@ void gp_tc_group_free(void *grp)
     free(G);
 }
 
-// the operand kind, product count and tile layout of a context's tensor path
-// (instances with equal keys can share a grouped launch), or -1 on the CUDA cores
+// the tile layout, operand kind, product count and forward operand kind of a
+// context's tensor path (instances with equal keys can share a grouped forward;
+// with equal key >> 3 -- all but the forward operand kind -- a grouped adjoint),
+// or -1 on the CUDA cores. Sorting by key keeps both kinds of class contiguous.
 int gp_tc_group_key(gpair_ctx *c)
 {
     if (c->precision == GPAIR_PREC_FP32) return -1;
     int op, nprod, fop;
     tc_mode(c->precision, &op, &nprod, &fop);
-    return (fop * 4 + nprod) * 2 + (c->tc_pair ? 1 : 0);
+    return (((c->tc_pair ? 1 : 0) * 8 + op) * 4 + nprod) * 8 + fop;
 }
 
 // one instance's entry of a grouped contraction of kind GP_TCG_*
@@ -2079,13 +2097,13 @@ static void tc_group_inst(gpair_ctx *c, TcState *t, int kind, TcGroupInst &g)
     g.nuv = c->nuv;
     if (batch) {
         g.lpad = t->Lb;
-        const int erows = t->Lb < TC_BN ? t->Lb : TC_BN;
-        g.elog2 = erows == 32 ? 5 : erows == 64 ? 6 : erows == 128 ? 7 : 8;
+        const int erows = t->Lb < TC_EPI_COLS ? t->Lb : TC_EPI_COLS;
+        g.elog2 = erows == 32 ? 5 : erows == 64 ? 6 : 7;
         g.rsc = t->rscb;
         g.vpart = c->vpart_b;
     } else {
-        g.lpad = t->M_pad;  // one image, partial entries of one 256-row tile each
-        g.elog2 = 8;
+        g.lpad = t->M_pad;  // one image, partial entries of TC_EPI_COLS rows
+        g.elog2 = 7;
         g.rsc = t->rsc;
         g.vpart = c->vpart;
     }
@@ -2113,7 +2131,9 @@ int gp_tc_group_build_kind(gpair_ctx **ctx, int n, int kind, const int *gate, un
         TcState *t = tc_state_ready(c, &rc);
         if (rc) break;
         if (kind == GP_TCG_TRIALS && (rc = gp_batch_alloc(c))) break;
-        if (t0 && (t->fop != t0->fop || t->nprod != t0->nprod || t->pair != t0->pair)) {
+        // the adjoint is the same contraction for both forward operand kinds of an op
+        if (t0 && ((kind == GP_TCG_ADJOINT ? t->op != t0->op : t->fop != t0->fop) || t->nprod != t0->nprod ||
+                   t->pair != t0->pair)) {
             rc = GPAIR_ERR_STATE;
             break;
         }
@@ -2164,7 +2184,7 @@ static cudaError_t tc_group_launch_kind(TcGroup *G, cudaStream_t st, int pdl, co
     memset(&cfg, 0, sizeof(cfg));
     cudaLaunchAttribute at[2];
     cfg.gridDim = dim3(PAIR ? 2 * (unsigned)G->npairs : (unsigned)G->nsm, 1, 1);
-    cfg.blockDim = dim3(TC_THREADS, 1, 1);
+    cfg.blockDim = dim3(tc_threads<EPI>(), 1, 1);
     cfg.dynamicSmemBytes = TC_SMEM_GROUP_BYTES;
     cfg.stream = st;
     cfg.attrs = at;
@@ -2214,12 +2234,15 @@ int gp_tc_group_forward(void *grp, gpair_ctx *c) { return gp_tc_group_run(grp, c
 // instances (group.cuh): the current image's prep (flux, regulariser, max and
 // forward operand), the batched trials' prep, and the adjoint weight operand.
 
+// partial visibility entries of the forward of one N x N image (rows of TC_EPI_COLS)
+int gp_tc_forward_entries(int N) { return round_up(N, TC_BN) / TC_EPI_COLS; }
+
 int gp_tc_stage_sizes(gpair_ctx *c, int *mt, int *splits)
 {
     int rc;
     TcState *t = tc_state_ready(c, &rc);
     if (rc) return rc;
-    if (mt) *mt = t->M_pad / TC_BN;
+    if (mt) *mt = t->M_pad / TC_EPI_COLS;
     if (splits) *splits = t->splits;
     return GPAIR_OK;
 }

@@ -27,10 +27,11 @@ Bytes per stage are the stage's compulsory traffic, as its kernels move it:
 
   prep           image + prior read for flux / entropy / max (8 B/px), image
                  read again and the f16 hi/lo operand written (8 B/px)
-  vis_data       V2: partial visibilities (8 B per row tile), data + inverse
+  vis_data       V2: partial visibilities (8 B per partial entry: one per 128
+                 image rows, rounded up to 256), data + inverse
                  error (8 B), visibilities written (16 + 8 B), mock (4 B), uv
                  weight (8 B); T3: indices (16 B), three gathered visibilities
-                 (3 x 8 B per row tile), phasor (8 B), data + error (16 B),
+                 (3 x 8 B per partial entry), phasor (8 B), data + error (16 B),
                  mock (8 B), vertex weights written (24 B)
   adj_weights    uv weights + CSR gather of vertex weights (16 B per point +
                  12 B per triangle vertex), then the adjoint's f16 hi/lo weight
@@ -72,18 +73,25 @@ def problem(name: str) -> api.Problem:
     return api.workload_problem(name)
 
 
-def batch_report(n: int, iters: int, precision: int) -> dict:
-    """Stage breakdown of a staged lockstep batch of n many-instance problems."""
+def batch_report(n: int, iters: int, precision: int, tune: str = "all") -> dict:
+    """Stage breakdown of a staged lockstep batch of n many-instance problems.
+    tune "all": every instance's precision path, tile and split-K autotuned
+    alone; "splits": `precision` and single CTAs for all (one class per
+    contraction), only the split-K length tuned."""
     from .clocks import ClockSampler
     from .instances import instances
     ps = instances(n)
     recs = [api.Reconstructor(0) for _ in ps]
     try:
         for r, p in zip(recs, ps):
+            if tune == "splits":
+                r.set_tc_pair(False)
             r.set_problem(p)
             r.set_precision(precision)
             r.set_image(p.start_image())
-        flags = api.TUNE_PRECISION | api.TUNE_SPLITS | api.TUNE_CACHE | api.TUNE_BATCHED | api.TUNE_TILE
+        flags = api.TUNE_SPLITS | api.TUNE_CACHE | api.TUNE_BATCHED
+        if tune == "all":
+            flags |= api.TUNE_PRECISION | api.TUNE_TILE
         for r in recs:
             r.autotune(flags, reps=2)
         api.shared_splits(recs)
@@ -106,7 +114,7 @@ def batch_report(n: int, iters: int, precision: int) -> dict:
         for r in recs:
             r.close()
     total = sum(v for k, v in stages.items() if k != "batched_evaluations")
-    return {"instances": n, "iterations": iters, "precision": precision, "layout": layout,
+    return {"instances": n, "iterations": iters, "precision": precision, "tune": tune, "layout": layout,
             "device_ms": dev_ms, "tflops": flops / (dev_ms * 1e-3) / 1e12, "clocks": clocks,
             "all_ok": all(o["status"] == 0 for o in res),
             "stage_us": stages, "stage_share": {k: v / total for k, v in stages.items() if k != "batched_evaluations"},
@@ -136,7 +144,7 @@ def report(name: str, reps: int = 10, pair: bool = False, precision: int = api.P
         with open(peaks_path) as f:
             d = json.load(f)
         hbm, tf = d["hbm_gbs"], d["bf16_tflops"]
-    row_tiles = (p.width + 255) // 256
+    row_tiles = 2 * ((p.width + 255) // 256)  # partial entries of the tensor forward
     splits = _default_splits(p, pair)
     by = stage_bytes(p, splits, row_tiles)
     out = {"workload": name, "precision": precision, "N": p.width, "nuv": p.nuv, "npow": p.npow, "nbis": p.nbis,
@@ -181,9 +189,11 @@ def main(argv=None):
     ap.add_argument("--tc-pair", type=int, default=1, help="contractions on CTA pairs (cta_group::2, 1) or single CTAs (0)")
     ap.add_argument("--batch", type=int, default=0, help="stage breakdown of a staged batch of this many instances")
     ap.add_argument("--iters", type=int, default=30, help="CG iterations of the --batch run")
+    ap.add_argument("--tune", choices=["all", "splits"], default="all",
+                    help="--batch: autotune precision, tile and split-K per instance, or split-K only")
     args = ap.parse_args(argv)
     if args.batch > 0:
-        print(json.dumps(batch_report(args.batch, args.iters, args.precision)), flush=True)
+        print(json.dumps(batch_report(args.batch, args.iters, args.precision, args.tune)), flush=True)
         return
     for w in args.workloads:
         if args.cg > 0:
