@@ -123,6 +123,7 @@ extern "C" int gpair_create(gpair_ctx **out, int device)
     c->device = device;
     c->precision = GPAIR_PREC_FP32;
     c->tc_pair = 1;  // tensor-core contractions on CTA pairs (gpair_set_tc_pair)
+    c->gf_parts = 8;
     {
         const char *e = getenv("GPAIR_PDL");  // programmatic dependent launches (gpair_set_pdl)
         c->pdl = (e && e[0] == '0') ? 0 : 1;

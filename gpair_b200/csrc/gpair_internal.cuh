@@ -279,6 +279,7 @@ struct gpair_ctx {
     // steps s and gradient changes y, and the image the last direction started from
     float *lb_s, *lb_y, *lb_xold;
     float2 *vpart_b;
+    double2 *visb;  // visibilities of the GP_NTR trials [GP_NTR][K], when their partial entries are many
     double *partials_b;
     int batch_wave[2];  // blocks per trial that fill one wave: [0] trial prep, [1] trial chi2
     int epp;  // forward partial entries per trial image
@@ -316,6 +317,9 @@ struct gpair_ctx {
     int tc_pair;
     // programmatic dependent launches of the evaluation chain (gp_launch), default on
     int pdl;
+    // most threads per four pixels in the gradient's split sum (k_grad_finalize): 8 alone,
+    // 1 for contexts that share the GPU (gpair_set_shared_splits)
+    int gf_parts;
 };
 
 // ---------------------------------------------------------------- helpers

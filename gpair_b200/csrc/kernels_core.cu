@@ -440,8 +440,31 @@ static int vis_data_launch(gpair_ctx *c, int direct);
 
 int gp_vis_data(gpair_ctx *c) { return vis_data_launch(c, 0); }
 
+// V_k = (sum of the forward's partial entries, in entry order) / F into visd: with
+// many entries per uv point, summed once here instead of once per triangle vertex
+// that gathers V_k (the same sum, so the same values)
+__global__ void __launch_bounds__(GP_THREADS) k_vis_sum(const float2 *__restrict__ vpart, int mt, int nuv,
+                                                        const DevScalars *__restrict__ sc,
+                                                        double2 *__restrict__ visd)
+{
+    gp_pdl_enter();
+    const double invF = sc->invflux;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nuv; k += gridDim.x * blockDim.x)
+        visd[k] = sum_vpart(vpart, mt, nuv, k, invF);
+}
+
+// more partial entries than this: V is summed once (k_vis_sum) before the triangles gather it
+#define VIS_PRESUM_ENTRIES 2
+
 static int vis_data_launch(gpair_ctx *c, int direct)
 {
+    if (!direct && c->mt > VIS_PRESUM_ENTRIES && c->nuv > 0) {
+        int nb = gp_cdiv(c->nuv, GP_THREADS);
+        if (nb > 4 * 148) nb = 4 * 148;
+        GP_LAUNCH(c, gp_launch(c, k_vis_sum, dim3(nb), dim3(GP_THREADS), 0, (const float2 *)c->vpart, c->mt, c->nuv,
+                               (const DevScalars *)c->sc, c->visd));
+        direct = 1;
+    }
     const VisDataArgs a = vis_data_args(c, direct, take_fused_ctrl(c));
     GP_LAUNCH(c, gp_launch(c, k_vis_data, dim3(a.nbx), dim3(GP_THREADS), 0, a));
     return GPAIR_OK;
@@ -711,6 +734,7 @@ struct GradFinalizeArgs {
     double *partials;
     DevScalars *sc;
     FusedCtrl fc;
+    int parts;  // threads per four pixels (a power of two); 1: one thread sums all splits
     GP_VGRID_FIELDS;
 };
 
@@ -752,33 +776,62 @@ __device__ __forceinline__ void grad_finalize_body(const GradFinalizeArgs &A, co
             acc[3] += dd * go;
         }
     };
-    if ((npix & 3) == 0) {
+    // the split sum of pixels 4q .. 4q + 3 over splits [s0, s1), in split order (FP64)
+    auto quad_sum = [&](int q, int nq, int s0, int s1, double (&g)[4]) {
+        const float4 *g4 = reinterpret_cast<const float4 *>(gpart) + q;
+        const size_t stride = (size_t)nq;
+        int s = s0;
+        for (; s + 8 <= s1; s += 8) {
+            float4 a[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++) a[j] = __ldcs(g4 + (size_t)(s + j) * stride);
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                g[0] += a[j].x;
+                g[1] += a[j].y;
+                g[2] += a[j].z;
+                g[3] += a[j].w;
+            }
+        }
+        for (; s < s1; s++) {
+            const float4 a = __ldcs(g4 + (size_t)s * stride);
+            g[0] += a.x;
+            g[1] += a.y;
+            g[2] += a.z;
+            g[3] += a.w;
+        }
+    };
+    const int P = A.parts;
+    if ((npix & 3) == 0 && P > 1) {
+        // P threads per four pixels (small images: enough loads in flight to cover the
+        // latency): part pp sums splits [pp S / P, (pp + 1) S / P); the parts are added
+        // in part order through shared memory
+        __shared__ double psum[GP_THREADS][4];
+        const int nq = npix >> 2, qpb = blockDim.x / P;
+        const int lq = threadIdx.x % qpb, pp = threadIdx.x / qpb;
+        for (int qbase = vg.bx * qpb; qbase < nq; qbase += vg.nbx * qpb) {  // block-uniform
+            const int q = qbase + lq;
+            double g[4] = {0.0, 0.0, 0.0, 0.0};
+            if (q < nq) quad_sum(q, nq, (pp * splits) / P, ((pp + 1) * splits) / P, g);
+#pragma unroll
+            for (int j = 0; j < 4; j++) psum[threadIdx.x][j] = g[j];
+            __syncthreads();
+            if (pp == 0 && q < nq) {
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    double t = psum[lq][j];
+                    for (int r = 1; r < P; r++) t += psum[r * qpb + lq][j];
+                    finish(4 * q + j, t);
+                }
+            }
+            __syncthreads();  // psum is rewritten by the next pass
+        }
+    } else if ((npix & 3) == 0) {
         // four consecutive pixels per thread: 16-byte loads, 8 splits (128 B) in flight
         const int nq = npix >> 2;
         for (int q = vg.bx * blockDim.x + threadIdx.x; q < nq; q += vg.nbx * blockDim.x) {
-            const float4 *g4 = reinterpret_cast<const float4 *>(gpart) + q;
-            const size_t stride = (size_t)nq;
             double g[4] = {0.0, 0.0, 0.0, 0.0};
-            int s = 0;
-            for (; s + 8 <= splits; s += 8) {
-                float4 a[8];
-#pragma unroll
-                for (int j = 0; j < 8; j++) a[j] = __ldcs(g4 + (size_t)(s + j) * stride);
-#pragma unroll
-                for (int j = 0; j < 8; j++) {
-                    g[0] += a[j].x;
-                    g[1] += a[j].y;
-                    g[2] += a[j].z;
-                    g[3] += a[j].w;
-                }
-            }
-            for (; s < splits; s++) {
-                const float4 a = __ldcs(g4 + (size_t)s * stride);
-                g[0] += a.x;
-                g[1] += a.y;
-                g[2] += a.z;
-                g[3] += a.w;
-            }
+            quad_sum(q, nq, 0, splits, g);
 #pragma unroll
             for (int j = 0; j < 4; j++) finish(4 * q + j, g[j]);
         }
@@ -830,13 +883,20 @@ static GradFinalizeArgs grad_finalize_args(gpair_ctx *c, int which, int mode, fl
     const int alpha_from_state = alpha < 0.f;
     const float *img = (which == GPAIR_IMG_TEMP) ? c->image_temp : c->image;
     float *out = (which == GPAIR_IMG_TEMP) ? c->grad_temp : c->full_grad_new;
-    // one thread per pixel (per four pixels when the image size allows 16-byte loads)
-    int g = gp_cdiv((c->npix & 3) == 0 ? c->npix / 4 : c->npix, GP_THREADS);
+    // one thread per pixel (per four pixels when the image size allows 16-byte loads);
+    // for images too small to fill two waves of 148 SMs that way, up to c->gf_parts
+    // threads per four pixels, each summing a contiguous part of the splits (contexts
+    // that share the GPU keep one: their instances fill it together)
+    int P = 1;
+    const long long units = (c->npix & 3) == 0 ? c->npix / 4 : c->npix;
+    if ((c->npix & 3) == 0)
+        while (2 * P <= c->gf_parts && 2 * P <= c->splits && gp_cdiv(units * P, GP_THREADS) < 2 * 148) P *= 2;
+    int g = gp_cdiv(units * P, GP_THREADS);
     if (g > GP_MAX_PARTIALS) g = GP_MAX_PARTIALS;
     if (g < 1) g = 1;
     GradFinalizeArgs a = {c->gpart, c->splits, c->npix, mode, img, c->model, alpha, alpha_from_state,
                           c->data_grad, c->entropy_grad, out, c->full_grad, c->descent_dir,
-                          which == GPAIR_IMG_TEMP ? 1 : 0, slot_partials(c, RED_GRAD), c->sc, fc, g, 1};
+                          which == GPAIR_IMG_TEMP ? 1 : 0, slot_partials(c, RED_GRAD), c->sc, fc, P, g, 1};
     return a;
 }
 
@@ -1334,6 +1394,7 @@ struct VisChi2BatchArgs {
     DevScalars *sc;
     FusedCtrl fc;
     const int *gate;
+    const double2 *visb;  // the trials' visibilities summed beforehand (k_vis_sum_batch), or null
     GP_VGRID_FIELDS;
 };
 
@@ -1352,25 +1413,27 @@ __device__ __forceinline__ void vis_chi2_batch_body(const VisChi2BatchArgs &A, c
     const int j = vg.by;
     const double invF = sc->t_invflux[j];
     const float2 *vp = vpart + (size_t)j * epp * nuv;
+    const double2 *vb = A.visb ? A.visb + (size_t)j * nuv : nullptr;
+#define VIS_B(k) (vb ? vb[(k)] : sum_vpart(vp, epp, nuv, (k), invF))
     double chi[1] = {0.0};
     const int nitems = npow + nbis;
     for (int i = vg.bx * blockDim.x + threadIdx.x; i < nitems; i += vg.nbx * blockDim.x) {
         if (i < npow) {
-            double2 V = sum_vpart(vp, epp, nuv, i, invF);
+            double2 V = VIS_B(i);
             double m2 = V.x * V.x + V.y * V.y;
             double r = (m2 - (double)data[i]) * data_err[i];
             chi[0] += r * r;
         } else {
             const int t = i - npow;
             int4 q = tri[t];
-            double2 va = sum_vpart(vp, epp, nuv, q.x, invF);
-            double2 vb = sum_vpart(vp, epp, nuv, q.y, invF);
-            double2 vc = sum_vpart(vp, epp, nuv, q.z, invF);
+            double2 va = VIS_B(q.x);
+            double2 vbb = VIS_B(q.y);
+            double2 vc = VIS_B(q.z);
             if (q.w & 1) va = cconj(va);
-            if (q.w & 2) vb = cconj(vb);
+            if (q.w & 2) vbb = cconj(vbb);
             if (q.w & 4) vc = cconj(vc);
             float2 phf = phasor[t];
-            double2 t3 = cmul(cmul(cmul(va, vb), vc), make_double2(phf.x, phf.y));
+            double2 t3 = cmul(cmul(cmul(va, vbb), vc), make_double2(phf.x, phf.y));
             const int r0 = npow + 2 * t;
             double rre = (t3.x - (double)data[r0]) * data_err[r0];
             double rim = (t3.y - (double)data[r0 + 1]) * data_err[r0 + 1];
@@ -1395,6 +1458,24 @@ __device__ __forceinline__ void vis_chi2_batch_body(const VisChi2BatchArgs &A, c
             run_fused_ctrl(sc, A.fc);
         }
     }
+}
+
+#undef VIS_B
+
+// the trials' visibilities V_jk = (sum of trial j's partial entries) / F_j into visb,
+// summed once instead of once per gathering triangle vertex (the same sum)
+__global__ void __launch_bounds__(GP_THREADS) k_vis_sum_batch(const float2 *__restrict__ vpart, int epp, int nuv,
+                                                              const DevScalars *__restrict__ sc,
+                                                              double2 *__restrict__ visb,
+                                                              const int *__restrict__ gate)
+{
+    gp_pdl_enter();
+    if (gate && !*gate) return;  // lockstep batches: this instance's line search is over
+    const int j = blockIdx.y;
+    const double invF = sc->t_invflux[j];
+    const float2 *vp = vpart + (size_t)j * epp * nuv;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nuv; k += gridDim.x * blockDim.x)
+        visb[(size_t)j * nuv + k] = sum_vpart(vp, epp, nuv, k, invF);
 }
 
 __global__ void __launch_bounds__(GP_THREADS) k_vis_chi2_batch(const VisChi2BatchArgs a)
@@ -1443,6 +1524,8 @@ int gp_batch_alloc(gpair_ctx *c)
     GP_CUDA(c, cudaMalloc(&c->image_trials, sizeof(float) * (size_t)GP_NTR * c->npix));
     GP_CUDA(c, cudaMalloc(&c->vpart_b, sizeof(float2) * (size_t)GP_NTR * epp_max * (c->nuv ? c->nuv : 1)));
     GP_CUDA(c, cudaMalloc(&c->partials_b, sizeof(double) * (size_t)GP_NTR * 1024 * 2));
+    if (epp_max > VIS_PRESUM_ENTRIES)
+        GP_CUDA(c, cudaMalloc(&c->visb, sizeof(double2) * (size_t)GP_NTR * (c->nuv ? c->nuv : 1)));
     int nsm = 148;
     GP_CUDA(c, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
     c->batch_wave[0] = batch_wave_blocks((const void *)k_trials_prep, nsm);
@@ -1456,9 +1539,11 @@ void gp_batch_free(gpair_ctx *c)
     if (c->image_trials) cudaFree(c->image_trials);
     if (c->vpart_b) cudaFree(c->vpart_b);
     if (c->partials_b) cudaFree(c->partials_b);
+    if (c->visb) cudaFree(c->visb);
     c->image_trials = nullptr;
     c->vpart_b = nullptr;
     c->partials_b = nullptr;
+    c->visb = nullptr;
 }
 
 int gp_trials_prep_launch(gpair_ctx *c)
@@ -1472,20 +1557,29 @@ int gp_trials_prep_launch(gpair_ctx *c)
 
 // chi2 of the GP_NTR trials of a batch from their partial visibilities (epp
 // entries per trial), then the fused controller
-static VisChi2BatchArgs batch_chi2_args(gpair_ctx *c, int epp, FusedCtrl fc, const int *gate)
+// presum: read the visibilities from visb (k_vis_sum_batch runs first) when the
+// partial entries are many; grouped launches pass 0
+static VisChi2BatchArgs batch_chi2_args(gpair_ctx *c, int epp, FusedCtrl fc, const int *gate, int presum = 0)
 {
     int nb = gp_cdiv(c->npow + c->nbis, GP_THREADS * 2);
     if (nb > c->batch_wave[1]) nb = c->batch_wave[1];  // one wave over the batch
     if (nb > 1024) nb = 1024;
     if (nb < 1) nb = 1;
+    const double2 *vb = (presum && epp > VIS_PRESUM_ENTRIES && c->visb) ? c->visb : nullptr;
     VisChi2BatchArgs a = {c->vpart_b, epp, c->nuv, c->npow, c->nbis, c->data, c->data_err, c->tri, c->phasor,
-                          c->partials_b, c->sc, fc, gate, nb, GP_NTR};
+                          c->partials_b, c->sc, fc, gate, vb, nb, GP_NTR};
     return a;
 }
 
 static int batch_chi2(gpair_ctx *c, int epp)
 {
-    const VisChi2BatchArgs a = batch_chi2_args(c, epp, take_fused_ctrl(c), c->gate);
+    const VisChi2BatchArgs a = batch_chi2_args(c, epp, take_fused_ctrl(c), c->gate, 1);
+    if (a.visb) {
+        int nb = gp_cdiv(c->nuv, GP_THREADS);
+        if (nb > 148) nb = 148;  // 8 trials: about eight blocks per SM
+        GP_LAUNCH(c, gp_launch(c, k_vis_sum_batch, dim3(nb, GP_NTR), dim3(GP_THREADS), 0, (const float2 *)c->vpart_b,
+                               epp, c->nuv, (const DevScalars *)c->sc, c->visb, c->gate));
+    }
     GP_LAUNCH(c, gp_launch(c, k_vis_chi2_batch, dim3(a.nbx, a.nby), dim3(GP_THREADS), 0, a));
     return GPAIR_OK;
 }

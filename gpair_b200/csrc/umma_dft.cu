@@ -1643,6 +1643,11 @@ int gp_tc_shared_splits(gpair_ctx **ctx, int n)
         total += (double)tiles * (double)(t->K2_pad / t->bk);
         if (!slots) slots = t->pair ? t->npairs : t->nsm;
     }
+    for (int i = 0; i < n; i++)
+        if (ctx[i]->gf_parts != 1) {
+            ctx[i]->gf_parts = 1;  // one thread per four pixels in the gradient's split sum
+            gp_cg_graph_free(ctx[i]);
+        }
     if (total <= 0.0) return GPAIR_OK;
     const double target = 2.0 * slots;  // units over all contexts
     for (int i = 0; i < n; i++) {

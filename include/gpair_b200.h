@@ -539,8 +539,10 @@ int gpair_set_pdl(gpair_ctx *ctx, int on);
  * For n contexts run together (gpair_cg_run_many, gpair_batch_*), this sets each
  * tensor-core context's split-K length so that all their units together fill
  * the SMs about twice, each context's share in proportion to its adjoint work
- * (at most the FP32-accumulation cap per split). CUDA-core contexts are left as
- * they are. Results change by rounding only; call before capturing a batch. */
+ * (at most the FP32-accumulation cap per split), and the gradient's sum of the
+ * partial images to one thread per four pixels (a context alone spreads a small
+ * image's sum over up to 8). The split-K lengths of CUDA-core contexts are left
+ * as they are. Results change by rounding only; call before capturing a batch. */
 int gpair_set_shared_splits(gpair_ctx **ctx, int n);
 int gpair_last_run_stage_ms(gpair_ctx *ctx, double *stage_ms, int *stage_launches, int max_stages);
 
