@@ -351,7 +351,8 @@ def many_instances(n: int, iters: int, precision: int) -> dict:
     """n independent reconstructions of uneven size (widths 64-256, 500-8,000 uv)
     for `iters` batched-line-search CG iterations each: one after another, all
     at once through gpair_cg_run_many (each context's graph on its own stream),
-    (after gpair_set_shared_splits: the adjoint split-K lengths for instances that
+    (with one precision path and tile layout for all, chosen by timing staged batches,
+    and gpair_set_shared_splits: the adjoint split-K lengths for instances that
     share the GPU) and as one graph launch (gpair_batch_run) in three layouts: the staged lockstep
     batch (every stage of an iteration one launch over all instances, every
     contraction one grouped tcgen05 launch per class), the lockstep batch with
@@ -363,10 +364,8 @@ def many_instances(n: int, iters: int, precision: int) -> dict:
     ps = instances(n)
     recs = [g.Reconstructor(0) for _ in ps]
     try:
-        # one precision path and single-CTA tiles for all instances (one class per contraction
-        # in a staged batch: 80.2 ms against 82.4 ms with precision and tile autotuned per
-        # instance, python -m gpair_b200.stage_report --batch 64 --tune splits|all); the
-        # adjoint split-K length autotuned per instance shape, cached across equal shapes
+        # sequential baseline: the given precision path on single CTAs, the adjoint split-K
+        # length autotuned per instance shape (cached across equal shapes)
         for r, p in zip(recs, ps):
             r.set_tc_pair(False)
             r.set_problem(p)
@@ -386,8 +385,14 @@ def many_instances(n: int, iters: int, precision: int) -> dict:
             r.cg(iters, method=2, line_search=g.LS_BATCH)
         t_seq = time.perf_counter() - t0
         flops = sum(r.last_run_stats()[1] for r in recs)
-        # run together, the instances split the adjoint's K dimension for the GPU they share
-        g.api.shared_splits(recs)
+        # run together: one precision path and tile layout for all instances (one class per
+        # contraction in a staged batch: 80.2 ms against 82.4 ms with precision and tile
+        # autotuned per instance, python -m gpair_b200.stage_report --batch 64 --tune
+        # splits|all), chosen by timing a staged batch under each candidate, and the adjoint's
+        # K dimension split for the GPU the instances share (gpair_set_shared_splits)
+        t0 = time.perf_counter()
+        layout = g.api.tune_batch_layout(recs, ps)
+        t_layout = time.perf_counter() - t0
         for r, p in zip(recs, ps):
             r.set_image(p.start_image())
         g.cg_many(recs, 1, line_search=g.LS_BATCH)  # rebuilds the graphs
@@ -429,8 +434,11 @@ def many_instances(n: int, iters: int, precision: int) -> dict:
             "one_launch_independent_s": one["independent"]["s"],
             "tflops_one_launch_independent": one["independent"]["tflops"],
             "all_ok": all(r_["status"] == 0 for r_ in res) and all(v["all_ok"] for v in one.values()),
-            "autotune": {"what": "adjoint split-K per instance shape; precision path and single-CTA tiles fixed",
-                         "s": t_tune, "tuned": sum(not t["from_cache"] for t in tuned),
+            "autotune": {"what": ("sequential runs: the bench precision on single CTAs, adjoint split-K per shape; "
+                                  "run together: one precision path and tile layout for all, from timed staged-batch "
+                                  "runs of each candidate (gpair_b200.api.tune_batch_layout), shared split-K"),
+                         "layout": layout, "layout_s": t_layout, "s": t_tune,
+                         "tuned": sum(not t["from_cache"] for t in tuned),
                          "fp32_path": sum(t["precision"] == g.PREC_FP32 for t in tuned),
                          "split16_path": sum(t["precision"] == g.PREC_SPLIT16 for t in tuned),
                          "split16f8_path": sum(t["precision"] == g.PREC_SPLIT16F8 for t in tuned),

@@ -682,6 +682,47 @@ def shared_splits(recs) -> None:
     _check(L.gpair_set_shared_splits(handles, n), recs[0].h)
 
 
+def tune_batch_layout(recs, problems, candidates=None, iterations: int = 2) -> dict:
+    """Chooses one precision path and tile layout for reconstructions that run as
+    one staged batch: for each candidate (precision, CTA pairs) every context takes
+    it, its adjoint split-K length is autotuned (GPAIR_TUNE_SPLITS, batched
+    objective) and set for sharing the GPU (shared_splits), and a staged batch runs
+    `iterations` CG iterations from the problems' start images (device time).
+    The fastest candidate is applied to the contexts and returned with every
+    candidate's time. One candidate for all keeps one grouped launch per
+    contraction; choosing per instance splits the launches by class."""
+    if candidates is None:
+        candidates = [(PREC_SPLIT16F8, False), (PREC_SPLIT16F8, True), (PREC_SPLIT16, False), (PREC_SPLIT16, True)]
+    times = {}
+
+    def take(prec, pair):
+        for r, p in zip(recs, problems):
+            r.set_tc_pair(pair)
+            r.set_precision(prec)
+            r.set_image(p.start_image())
+        for r in recs:
+            r.autotune(TUNE_SPLITS | TUNE_CACHE | TUNE_BATCHED, reps=2)
+        shared_splits(recs)
+
+    for prec, pair in candidates:
+        take(prec, pair)
+        with Batch(recs, line_search=LS_BATCH) as b:
+            for r, p in zip(recs, problems):
+                r.set_image(p.start_image())
+            b.run(1)  # first launch
+            for r, p in zip(recs, problems):
+                r.set_image(p.start_image())
+            b.run(iterations)
+            times[(prec, pair)] = recs[0].last_run_stats()[0]
+    best = min(times, key=times.get)
+    take(*best)
+    for r, p in zip(recs, problems):
+        r.set_image(p.start_image())
+    return {"precision": best[0], "tc_pair": best[1],
+            "candidates_ms": [{"precision": k[0], "tc_pair": k[1], "ms": v} for k, v in times.items()],
+            "iterations": iterations}
+
+
 class Batch:
     """Many reconstructions in one CUDA graph launch (gpair_batch_*). With the
     batched line search and the contexts on tensor-core paths the instances run in

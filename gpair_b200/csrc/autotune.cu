@@ -16,7 +16,8 @@
 //              within the FP32-accumulation cap and the partial-image buffer
 // Objective: one criterion + gradient evaluation, or (GPAIR_TUNE_BATCHED) that
 // plus two batched 8-trial evaluations, the work of a batched-line-search
-// iteration. Choices are cached per (device, width, uv count to 1/8, objective).
+// iteration. Choices are cached per (device, width, uv count to 1/8, objective,
+// and the precision path and tile layout when those are not tuned).
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
@@ -36,7 +37,7 @@ struct Choice {
 };
 
 std::mutex g_mu;
-std::map<std::tuple<int, int, int>, Choice> g_cache;
+std::map<std::tuple<int, int, int, int>, Choice> g_cache;
 
 int uv_bucket(int nuv) { return nuv <= 0 ? 0 : (int)floor(log2((double)nuv) * 8.0); }
 
@@ -105,9 +106,14 @@ extern "C" int gpair_autotune(gpair_ctx *c, int flags, int reps, gpair_tune_resu
     if (!c || !c->have_problem || !c->have_image) return GPAIR_ERR_STATE;
     if (reps <= 0) reps = 3;
     GP_CUDA(c, cudaSetDevice(c->device));
+    // the settings that are not tuned are part of the key: a choice made for another
+    // fixed precision path or tile layout is not reused
+    const int fixed = ((flags & GPAIR_TUNE_PRECISION) ? 0 : c->precision + 1) * 4 +
+                      ((flags & GPAIR_TUNE_TILE) ? 0 : c->tc_pair + 1);
     const auto key = std::make_tuple(c->device, c->N,
                                      uv_bucket(c->nuv) * 4 + ((flags & GPAIR_TUNE_BATCHED) ? 1 : 0) +
-                                         ((flags & GPAIR_TUNE_TILE) ? 2 : 0));
+                                         ((flags & GPAIR_TUNE_TILE) ? 2 : 0),
+                                     fixed);
     if (res) memset(res, 0, sizeof(*res));
     if (flags & GPAIR_TUNE_CACHE) {
         Choice ch;

@@ -470,12 +470,15 @@ int gpair_time_batch_stages(gpair_ctx *ctx, int reps, double *stage_ms, int max_
 /* Autotuner: times criterion + gradient evaluations of the loaded problem (current
  * image) under candidate configurations and keeps the fastest. Candidates: the
  * precision path (GPAIR_TUNE_PRECISION: FP32 CUDA cores, split-f16 or split-f16/E4M3
- * tensor cores; all meet the 1e-5 accuracy bounds), the adjoint's split-K tile length
+ * tensor cores; all meet the 1e-5 accuracy bounds on the benchmark workloads, though
+ * split-f16/E4M3's chi2 error can pass 1e-5 where |V| is far below the total flux at
+ * most uv points, as for a pixel-by-pixel random image), the adjoint's split-K tile length
  * (GPAIR_TUNE_SPLITS: half, default and double the heuristic's K-blocks per split,
  * within the FP32-accumulation cap) and the tensor-core tile (GPAIR_TUNE_TILE:
  * 256 x 256 output tiles on CTA pairs or 128 x 256 on single CTAs, as
  * gpair_set_tc_pair selects). GPAIR_TUNE_CACHE reuses the choice made for a
- * problem of the same device, width and uv count (to 1/8) and objective in this process. */
+ * problem of the same device, width and uv count (to 1/8) and objective in this
+ * process, made with the same precision path and tile when those are not tuned. */
 #define GPAIR_TUNE_PRECISION 1
 #define GPAIR_TUNE_SPLITS 2
 #define GPAIR_TUNE_CACHE 4

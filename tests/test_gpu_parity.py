@@ -1016,6 +1016,43 @@ def test_shared_splits_keep_parity_and_staged_batches_exact():
             r.close()
 
 
+def test_batch_layout_tuner_applies_its_choice():
+    """gpair_b200.api.tune_batch_layout times a staged batch under each candidate
+    layout and leaves every context on the fastest one (precision path and tile),
+    with its batch-shared split-K lengths; a staged batch built afterwards is one
+    class per contraction and equals the separate runs bit for bit."""
+    from gpair_b200.instances import instance
+    ps = [instance(20_000_300 + k) for k in range(3)]
+    recs = [g.Reconstructor(0) for _ in ps]
+    L = g.lib()
+    try:
+        for r, p in zip(recs, ps):
+            r.set_problem(p)
+            r.set_precision(g.PREC_SPLIT16)
+        cands = [(g.PREC_SPLIT16, False), (g.PREC_SPLIT16F8, True)]
+        out = g.api.tune_batch_layout(recs, ps, candidates=cands, iterations=1)
+        assert (out["precision"], out["tc_pair"]) in cands and len(out["candidates_ms"]) == 2
+        for r in recs:
+            assert L.gpair_get_precision(r.h) == out["precision"]
+            assert L.gpair_get_tc_pair(r.h) == int(out["tc_pair"])
+        singles, imgs = [], []
+        for r, p in zip(recs, ps):
+            r.set_image(p.start_image())
+            singles.append(r.cg(3, method=2, line_search=g.LS_BATCH))
+            imgs.append(r.get_image())
+        for r, p in zip(recs, ps):
+            r.set_image(p.start_image())
+        with g.api.Batch(recs, line_search=g.LS_BATCH) as b:
+            assert b.grouped == 2
+            res = b.run(3)
+            for r, a, o, img in zip(recs, singles, res, imgs):
+                assert o["status"] == 0 and o["J"] == a["J"]
+                assert np.array_equal(r.get_image(), img)
+    finally:
+        for r in recs:
+            r.close()
+
+
 @pytest.mark.parametrize("fwd_only", [False, True])
 def test_grouped_batch_wait_timeout_is_reported_and_recovers(fwd_only):
     """The grouped contractions' bounded waits run out (built from a first context
