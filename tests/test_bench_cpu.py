@@ -134,3 +134,14 @@ def test_small_workload_reference_cg_runs_on_the_reference_code():
         os.close(devnull)
     assert out["kind"] == "reference" and out["cores"] == 1
     assert out["grad_evals"] >= 3 and out["J"] > 0
+
+
+def test_stage_report_instance_workloads_match_the_profiled_problems():
+    """stage_report's instance:SEED workloads are the many-instance generator's
+    problems (the small-image trial-forward profiles use seeds 30,000,000 and
+    30,000,040)."""
+    from gpair_b200 import stage_report
+    p = stage_report.problem("instance:30000000")
+    assert p.width == 64 and p.nuv == 6871 and p.nbis == 4576
+    p = stage_report.problem("instance:30000040")
+    assert p.width == 128 and p.nuv == 5664 and p.nbis == 3776
