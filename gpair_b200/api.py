@@ -88,6 +88,12 @@ LS_WOLFE, LS_BATCH, LS_TRIALS = 0, 1, 8
 BATCH_INDEPENDENT = 1  # gpair_batch_create_ex flag: independent branches, no lockstep grouping
 BATCH_FORWARDS_ONLY = 2  # gpair_batch_create_ex flag: lockstep with grouped trial forwards only
 BATCH_STAGE_STAMPS = 4  # gpair_batch_create_ex flag: device timer stamps between the staged launches
+
+
+def batch_prep_passes(p: int) -> int:
+    """gpair_batch_create_ex flag GPAIR_BATCH_PREP_PASSES(p): passes of image rows per block of a
+    staged batch's trial prep (0: chosen by the batch)."""
+    return (p & 63) << 8
 TUNE_PRECISION, TUNE_SPLITS, TUNE_CACHE, TUNE_BATCHED, TUNE_TILE = 1, 2, 4, 8, 16
 TUNE_MAX_CANDIDATES = 16
 
@@ -162,6 +168,7 @@ def lib() -> C.CDLL:
         L.gpair_batch_create.argtypes = [C.POINTER(vp), C.POINTER(vp), i, i]
         L.gpair_batch_create_ex.argtypes = [C.POINTER(vp), C.POINTER(vp), i, i, i]
         L.gpair_batch_grouped.argtypes = [vp]
+        L.gpair_batch_prep_passes.argtypes = [vp]
         L.gpair_batch_stage_stamps.argtypes = [vp, vp, i, i]
         L.gpair_batch_run.argtypes = [vp, C.POINTER(CgParams), C.POINTER(CgResult)]
         L.gpair_batch_destroy.argtypes = [vp]
@@ -734,17 +741,18 @@ class Batch:
     Build after the contexts hold their problems, images and configuration."""
 
     def __init__(self, recs, line_search: int = LS_BATCH, independent: bool = False, forwards_only: bool = False,
-                 stamps: bool = False):
+                 stamps: bool = False, prep_passes: int = 0):
         self._L = lib()
         self.recs = list(recs)
         self.line_search = line_search
         h = C.c_void_p()
         arr = (C.c_void_p * len(self.recs))(*[r.h.value for r in self.recs])
         flags = ((BATCH_INDEPENDENT if independent else 0) | (BATCH_FORWARDS_ONLY if forwards_only else 0) |
-                 (BATCH_STAGE_STAMPS if stamps else 0))
+                 (BATCH_STAGE_STAMPS if stamps else 0) | batch_prep_passes(prep_passes))
         _check(self._L.gpair_batch_create_ex(C.byref(h), arr, len(self.recs), line_search, flags), self.recs[0].h)
         self.h = h
         self.grouped = int(self._L.gpair_batch_grouped(self.h))
+        self.prep_passes = int(self._L.gpair_batch_prep_passes(self.h))  # 0: not staged
 
     def run(self, iterations: int, method: int = 2, alpha: Optional[float] = None, resume: bool = False, **kw):
         prm = CgParams()

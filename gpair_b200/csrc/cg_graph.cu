@@ -256,6 +256,7 @@ struct BatchGraph {
     int staged;
     void **grps_img, **grps_adj;
     int nadj;  // grouped adjoints (classes without the forward operand kind)
+    int prep_passes;  // passes of rows per block of the grouped trial prep
     void *stg_args[GS_COUNT];  // device: argument structs of every instance, lockstep order
     int *stg_start[GS_COUNT];  // device: block starts [n + 1]
     int stg_total[GS_COUNT];
@@ -640,7 +641,8 @@ static int build_lockstep(gpair_ctx **ctx_in, int n, BatchGraph *B)
 // its own single launch, so its results are bitwise those of a separate run.
 
 // argument structs and block starts of one stage over the instances ctx[0..n-1]
-static int stage_table(BatchGraph *B, gpair_ctx **ctx, int n, int stage, double *const *trace, int *op_out)
+static int stage_table(BatchGraph *B, gpair_ctx **ctx, int n, int stage, double *const *trace, int *op_out,
+                       int prep_passes)
 {
     const bool tc = stage == GS_PREP_IMAGE || stage == GS_PREP_TRIALS || stage == GS_BUILD_W;
     const size_t sz = tc ? gp_tc_stage_args_size(stage) : gp_stage_args_size(stage);
@@ -650,7 +652,7 @@ static int stage_table(BatchGraph *B, gpair_ctx **ctx, int n, int stage, double 
     for (int k = 0; k < n; k++) {
         int nb = 0, op = -1, rc;
         if (tc) {
-            rc = gp_tc_stage_args(ctx[k], stage, h.data() + sz * k, &nb, &op);
+            rc = gp_tc_stage_args(ctx[k], stage, h.data() + sz * k, &nb, &op, prep_passes);
             if (!rc && op0 >= 0 && op != op0) rc = GPAIR_ERR_STATE;  // one operand element type per launch
             op0 = op;
         } else {
@@ -672,7 +674,7 @@ static int stage_table(BatchGraph *B, gpair_ctx **ctx, int n, int stage, double 
 
 // GPAIR_ERR_STATE: the instances cannot run fully staged (the caller builds the
 // lockstep with grouped trial forwards only, or independent branches)
-static int build_lockstep_staged(gpair_ctx **ctx_in, int n, BatchGraph *B, int with_stamps)
+static int build_lockstep_staged(gpair_ctx **ctx_in, int n, BatchGraph *B, int with_stamps, int prep_passes_req)
 {
     if (n > 4096) return GPAIR_ERR_STATE;
     std::vector<int> key((size_t)n), order((size_t)n);
@@ -742,7 +744,12 @@ static int build_lockstep_staged(gpair_ctx **ctx_in, int n, BatchGraph *B, int w
     std::vector<double *> trace((size_t)n);
     for (int k = 0; k < n; k++) trace[k] = B->loops[order[k]].trace;
     int op = -1;
-    for (int st = 0; st < GS_COUNT && !rc; st++) rc = stage_table(B, ctx.data(), n, st, trace.data(), &op);
+    // the trial prep's trial sums are per image row where rows are one warp wide, so its
+    // blocks can take several passes without changing a result
+    const int prep_passes = prep_passes_req ? prep_passes_req : gp_tc_prep_trials_passes(ctx.data(), n, op_prep);
+    B->prep_passes = prep_passes;
+    for (int st = 0; st < GS_COUNT && !rc; st++)
+        rc = stage_table(B, ctx.data(), n, st, trace.data(), &op, prep_passes);
     if (rc) return rc == GPAIR_ERR_STATE ? GPAIR_ERR_CUDA : rc;
     GP_CUDA(c0, cudaMalloc(&B->scs, sizeof(DevScalars *) * (size_t)n));
     std::vector<DevScalars *> hs((size_t)n);
@@ -870,7 +877,7 @@ int gp_batch_graph_build(gpair_ctx **ctx, int n, int ls_mode, int allow_group, v
         if (cudaMalloc(&G->trace, sizeof(double) * 5) != cudaSuccess) rc = GPAIR_ERR_ALLOC;
     }
     if (!rc && (allow_group & 3) >= 2 && ls_mode == GPAIR_LS_BATCH) {
-        rc = build_lockstep_staged(ctx, n, B, allow_group & 4);
+        rc = build_lockstep_staged(ctx, n, B, allow_group & 4, (allow_group >> 8) & 63);
         if (rc == GPAIR_OK) {
             B->grouped = 2;
         } else if (rc == GPAIR_ERR_STATE) {
@@ -917,6 +924,7 @@ int gp_batch_graph_launch(void *bg, cudaStream_t stream)
 int gp_batch_graph_precision(void *bg, int i) { return ((BatchGraph *)bg)->loops[i].precision; }
 unsigned int gp_batch_graph_buf_gen(void *bg, int i) { return ((BatchGraph *)bg)->loops[i].buf_gen; }
 int gp_batch_graph_grouped(void *bg) { return bg ? ((BatchGraph *)bg)->grouped : 0; }
+int gp_batch_graph_prep_passes(void *bg) { return bg && ((BatchGraph *)bg)->staged ? ((BatchGraph *)bg)->prep_passes : 0; }
 
 // the stage stamps of a staged batch (none recorded: 0); `reset` zeroes them
 // afterwards (on st), so that the next run's sums start from zero

@@ -27,6 +27,7 @@ int gp_batch_graph_launch(void *bg, cudaStream_t stream);
 int gp_batch_graph_precision(void *bg, int i);
 unsigned int gp_batch_graph_buf_gen(void *bg, int i);
 int gp_batch_graph_grouped(void *bg);
+int gp_batch_graph_prep_passes(void *bg);
 int gp_batch_graph_stamps(void *bg, unsigned long long *out, int max, cudaStream_t st, int reset);
 long long gp_batch_graph_launches(void *bg, int i, int iterations_done, int criterion_evals, int grad_evals,
                                   int batches);
@@ -929,6 +930,7 @@ extern "C" int gpair_batch_create(gpair_batch **out, gpair_ctx **ctx, int n, int
 }
 
 extern "C" int gpair_batch_grouped(const gpair_batch *b) { return b ? gp_batch_graph_grouped(b->graph) : 0; }
+extern "C" int gpair_batch_prep_passes(const gpair_batch *b) { return b ? gp_batch_graph_prep_passes(b->graph) : 0; }
 
 extern "C" int gpair_batch_stage_stamps(const gpair_batch *b, unsigned long long *ns, int max, int reset)
 {
@@ -940,8 +942,10 @@ extern "C" int gpair_batch_stage_stamps(const gpair_batch *b, unsigned long long
 extern "C" int gpair_batch_create_ex(gpair_batch **out, gpair_ctx **ctx, int n, int line_search, int flags)
 {
     if (!out || !ctx || n <= 0) return GPAIR_ERR_INVALID;
-    if (flags & ~(GPAIR_BATCH_INDEPENDENT | GPAIR_BATCH_FORWARDS_ONLY | GPAIR_BATCH_STAGE_STAMPS))
+    if (flags & ~(GPAIR_BATCH_INDEPENDENT | GPAIR_BATCH_FORWARDS_ONLY | GPAIR_BATCH_STAGE_STAMPS | (63 << 8)))
         return GPAIR_ERR_INVALID;
+    const int prep_passes = (flags >> 8) & 63;  // GPAIR_BATCH_PREP_PASSES(p); 0: chosen by the batch
+    if (prep_passes & (prep_passes - 1)) return GPAIR_ERR_INVALID;
     if (line_search != GPAIR_LS_WOLFE && line_search != GPAIR_LS_BATCH) return GPAIR_ERR_INVALID;
     *out = nullptr;
     for (int i = 0; i < n; i++) {
@@ -976,6 +980,7 @@ extern "C" int gpair_batch_create_ex(gpair_batch **out, gpair_ctx **ctx, int n, 
     // 2: every stage grouped where the instances allow it, 1: grouped forwards only, 0: independent
     int group = (flags & GPAIR_BATCH_INDEPENDENT) ? 0 : (flags & GPAIR_BATCH_FORWARDS_ONLY) ? 1 : 2;
     if (flags & GPAIR_BATCH_STAGE_STAMPS) group |= 4;  // device timer stamps between the staged launches
+    group |= prep_passes << 8;
     if (!rc) rc = gp_batch_graph_build(ctx, n, line_search, group, &b->graph);
     if (rc) {
         gpair_batch_destroy(b);

@@ -489,7 +489,9 @@ int gp_stage_group_launch(gpair_ctx *c, int stage, const void *d_args, const int
 // the umma_dft.cu stages (GS_PREP_IMAGE, GS_PREP_TRIALS, GS_BUILD_W); `op` is the
 // operand kind of every instance in the launch
 size_t gp_tc_stage_args_size(int stage);
-int gp_tc_stage_args(gpair_ctx *c, int stage, void *out, int *nblocks, int *op);
+// passes: GS_PREP_TRIALS only, passes of rows per block (1: the single launch's grid)
+int gp_tc_stage_args(gpair_ctx *c, int stage, void *out, int *nblocks, int *op, int passes = 1);
+int gp_tc_prep_trials_passes(gpair_ctx *const *ctx, int n, int op);
 int gp_tc_stage_group_launch(gpair_ctx *c, int stage, int op, const void *d_args, const int *d_start, int n,
                              int total, const int *gate);
 int gp_tc_build_w(gpair_ctx *c);

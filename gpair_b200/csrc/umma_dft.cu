@@ -954,6 +954,12 @@ __device__ __forceinline__ void tc_prep_rows_body(const PrepRowsArgs &A, const G
     double acc[2] = {0.0, 0.0};
     float mx = 0.f;
     const bool vec = (N & 7) == 0 && N <= 8 * nt;
+    // Trial images one warp wide (N <= 256): flux and regulariser summed per
+    // image row into partials[j][y], then over the rows in a fixed order, so
+    // the sums do not depend on the block grid (a staged batch gives a block
+    // several passes). Wider rows: per-block partials.
+    const bool rowsum = MODE == 2 && W == 1;
+    double *__restrict__ rowp = partials + (size_t)j * N * 2;
     for (int ybase = vg.bx * R; ybase < N; ybase += vg.nbx * R) {  // block-uniform
         const int y = ybase + rw;
         const bool yv = y < N;
@@ -1006,13 +1012,27 @@ __device__ __forceinline__ void tc_prep_rows_body(const PrepRowsArgs &A, const G
                 rmax = fmaxf(rmax, fabsf(I));
             }
         }
-        // max over the row's W warps
+        // max over the row's W warps (one warp: the shuffle tree has it already)
         rmax = warp_max_f(rmax);
-        if (lane == 0) wmax[warp] = rmax;
-        __syncthreads();
-        rmax = 0.f;
-        for (int q = 0; q < W; q++) rmax = fmaxf(rmax, wmax[rw * W + q]);
-        __syncthreads();  // wmax is rewritten by the next pass
+        if (W > 1) {  // block-uniform
+            if (lane == 0) wmax[warp] = rmax;
+            __syncthreads();
+            rmax = 0.f;
+            for (int q = 0; q < W; q++) rmax = fmaxf(rmax, wmax[rw * W + q]);
+            __syncthreads();  // wmax is rewritten by the next pass
+        }
+        if (rowsum) {
+            // this row's flux and regulariser, one fixed shuffle tree; lanes past
+            // the row add +0.0
+#pragma unroll
+            for (int i = 0; i < 2; i++)
+                for (int off = 16; off > 0; off >>= 1) acc[i] += __shfl_down_sync(0xffffffffu, acc[i], off);
+            if (yv && lane == 0) {
+                rowp[2 * y] = acc[0];
+                rowp[2 * y + 1] = acc[1];
+            }
+            acc[0] = acc[1] = 0.0;
+        }
         int ex = 0;
         frexpf(rmax, &ex);
         const float scale = ldexpf(1.f, 15 - ex);
@@ -1054,17 +1074,21 @@ __device__ __forceinline__ void tc_prep_rows_body(const PrepRowsArgs &A, const G
         mx = fmaxf(mx, rmax);
     }
     if (!red) return;  // uniform over the grid
-    block_sum<2>(acc, smem);
-    const double bmax = block_max((double)mx, smem);
     if (MODE == 2) {
-        double *pp = partials + (size_t)j * vg.nbx * 2;
-        if (threadIdx.x == 0) {
-            pp[2 * vg.bx] = acc[0];
-            pp[2 * vg.bx + 1] = acc[1];
+        double *pp = rowp;
+        int np = N;
+        if (!rowsum) {
+            block_sum<2>(acc, smem);
+            pp = partials + (size_t)j * vg.nbx * 2;
+            np = vg.nbx;
+            if (threadIdx.x == 0) {
+                pp[2 * vg.bx] = acc[0];
+                pp[2 * vg.bx + 1] = acc[1];
+            }
         }
         if (last_block_of(&sc->t_counter[j], vg.nbx)) {
             double o[2];
-            finish_sum<2>(pp, vg.nbx, o, smem);
+            finish_sum<2>(pp, np, o, smem);
             if (threadIdx.x == 0) {
                 sc->t_flux[j] = o[0];
                 sc->t_invflux[j] = 1.0 / o[0];
@@ -1074,6 +1098,8 @@ __device__ __forceinline__ void tc_prep_rows_body(const PrepRowsArgs &A, const G
         }
         return;
     }
+    block_sum<2>(acc, smem);
+    const double bmax = block_max((double)mx, smem);
     if (threadIdx.x == 0) {
         partials[3 * vg.bx] = acc[0];
         partials[3 * vg.bx + 1] = acc[1];
@@ -2262,7 +2288,18 @@ size_t gp_tc_stage_args_size(int stage)
     }
 }
 
-int gp_tc_stage_args(gpair_ctx *c, int stage, void *out, int *nblocks, int *op)
+// blocks of one trial image in the trial prep when a block takes `passes`
+// passes of rows (per-row sums, rows one warp wide) or the single launch's grid
+static int tc_prep_trial_blocks(int N, int passes)
+{
+    const int W = pr_warps_per_row(N), R = PR_WARPS_MAX / W;
+    int gx = gp_cdiv(N, R);
+    if (gx > 1024) gx = 1024;
+    if (W == 1 && passes > 1) gx = gp_cdiv(gx, passes);
+    return gx < 1 ? 1 : gx;
+}
+
+int gp_tc_stage_args(gpair_ctx *c, int stage, void *out, int *nblocks, int *op, int passes)
 {
     int rc;
     TcState *t = tc_state_ready(c, &rc);
@@ -2270,8 +2307,9 @@ int gp_tc_stage_args(gpair_ctx *c, int stage, void *out, int *nblocks, int *op)
     *op = t->op;
     if (stage == GS_PREP_IMAGE || stage == GS_PREP_TRIALS) {
         if (stage == GS_PREP_TRIALS && (rc = gp_tc_batch_prepare(c, nullptr))) return rc;
-        const PrepRowsArgs a = stage == GS_PREP_IMAGE ? tc_prep_rows_args(c, t, 0, 1, c->partials, c->image)
-                                                      : tc_prep_rows_args(c, t, 2, 1, c->partials_b, nullptr);
+        PrepRowsArgs a = stage == GS_PREP_IMAGE ? tc_prep_rows_args(c, t, 0, 1, c->partials, c->image)
+                                                : tc_prep_rows_args(c, t, 2, 1, c->partials_b, nullptr);
+        if (stage == GS_PREP_TRIALS) a.nbx = tc_prep_trial_blocks(c->N, passes);
         memcpy(out, &a, sizeof(a));
         *nblocks = a.nbx * a.nby;
         return GPAIR_OK;
@@ -2284,6 +2322,34 @@ int gp_tc_stage_args(gpair_ctx *c, int stage, void *out, int *nblocks, int *op)
         return GPAIR_OK;
     }
     return GPAIR_ERR_INVALID;
+}
+
+// Passes of rows per block for the grouped trial prep of a staged batch: the
+// smallest power of two that brings the launch (every instance's 8 trial
+// images) within four waves of resident blocks. One pass per block leaves the
+// launch bound by each block's fixed start and end (instance lookup, scalars,
+// the last-block reduction): 80 registers a thread give 3 blocks of 256 per SM.
+int gp_tc_prep_trials_passes(gpair_ctx *const *ctx, int n, int op)
+{
+    if (n < 1) return 1;
+    int nsm = 0, per = 0;
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx[0]->device) != cudaSuccess || nsm < 1)
+        return 1;
+    const cudaError_t e =
+        op == OP_F16
+            ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_grouped<PrepRowsOp<__half, 2>, PR_THREADS>,
+                                                            PR_THREADS, 0)
+            : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_grouped<PrepRowsOp<float, 2>, PR_THREADS>,
+                                                            PR_THREADS, 0);
+    if (e != cudaSuccess || per < 1) return 1;
+    const long long waves4 = 4LL * per * nsm;
+    int p = 1;
+    for (; p < 32; p *= 2) {
+        long long total = 0;
+        for (int k = 0; k < n; k++) total += (long long)GP_NTR * tc_prep_trial_blocks(ctx[k]->N, p);
+        if (total <= waves4) break;
+    }
+    return p;
 }
 
 template <class Op, int THREADS>

@@ -73,8 +73,9 @@ def problem(name: str) -> api.Problem:
     return api.workload_problem(name)
 
 
-def batch_report(n: int, iters: int, precision: int, tune: str = "all") -> dict:
-    """Stage breakdown of a staged lockstep batch of n many-instance problems.
+def batch_report(n: int, iters: int, precision: int, tune: str = "all", prep_passes=(0,)) -> list:
+    """Stage breakdown of a staged lockstep batch of n many-instance problems,
+    one report per trial-prep pass count (0: the batch's own choice).
     tune "all": every instance's precision path, tile and split-K autotuned
     alone; "splits": `precision` and single CTAs for all (one class per
     contraction), only the split-K length tuned."""
@@ -82,6 +83,7 @@ def batch_report(n: int, iters: int, precision: int, tune: str = "all") -> dict:
     from .instances import instances
     ps = instances(n)
     recs = [api.Reconstructor(0) for _ in ps]
+    out = []
     try:
         for r, p in zip(recs, ps):
             if tune == "splits":
@@ -95,30 +97,35 @@ def batch_report(n: int, iters: int, precision: int, tune: str = "all") -> dict:
         for r in recs:
             r.autotune(flags, reps=2)
         api.shared_splits(recs)
-        with api.Batch(recs, line_search=api.LS_BATCH, stamps=True) as b:
-            for r, p in zip(recs, ps):
-                r.set_image(p.start_image())
-            b.run(1)  # first launch
-            b.stage_times_us(reset=True)
-            for r, p in zip(recs, ps):
-                r.set_image(p.start_image())
-            sampler = ClockSampler(0)
-            sampler.start()
-            res = b.run(iters)
-            clocks = sampler.stop()
-            dev_ms = recs[0].last_run_stats()[0]
-            flops = sum(r.last_run_stats()[1] for r in recs)
-            stages = b.stage_times_us()
-            layout = b.grouped
+        for passes in prep_passes:
+            with api.Batch(recs, line_search=api.LS_BATCH, stamps=True, prep_passes=passes) as b:
+                for r, p in zip(recs, ps):
+                    r.set_image(p.start_image())
+                b.run(1)  # first launch
+                b.stage_times_us(reset=True)
+                for r, p in zip(recs, ps):
+                    r.set_image(p.start_image())
+                sampler = ClockSampler(0)
+                sampler.start()
+                res = b.run(iters)
+                clocks = sampler.stop()
+                dev_ms = recs[0].last_run_stats()[0]
+                flops = sum(r.last_run_stats()[1] for r in recs)
+                stages = b.stage_times_us()
+                total = sum(v for k, v in stages.items() if k != "batched_evaluations")
+                out.append({
+                    "instances": n, "iterations": iters, "precision": precision, "tune": tune,
+                    "layout": b.grouped, "prep_passes": b.prep_passes, "device_ms": dev_ms,
+                    "tflops": flops / (dev_ms * 1e-3) / 1e12, "clocks": clocks,
+                    "all_ok": all(o["status"] == 0 for o in res), "J": [o["J"] for o in res],
+                    "stage_us": stages,
+                    "stage_share": {k: v / total for k, v in stages.items() if k != "batched_evaluations"},
+                    "timing": "device timer stamps after every launch (one small timer kernel each), summed over "
+                              "the run"})
     finally:
         for r in recs:
             r.close()
-    total = sum(v for k, v in stages.items() if k != "batched_evaluations")
-    return {"instances": n, "iterations": iters, "precision": precision, "tune": tune, "layout": layout,
-            "device_ms": dev_ms, "tflops": flops / (dev_ms * 1e-3) / 1e12, "clocks": clocks,
-            "all_ok": all(o["status"] == 0 for o in res),
-            "stage_us": stages, "stage_share": {k: v / total for k, v in stages.items() if k != "batched_evaluations"},
-            "timing": "device timer stamps after every launch (one small timer kernel each), summed over the run"}
+    return out
 
 
 def report(name: str, reps: int = 10, pair: bool = False, precision: int = api.PREC_SPLIT16) -> dict:
@@ -191,9 +198,12 @@ def main(argv=None):
     ap.add_argument("--iters", type=int, default=30, help="CG iterations of the --batch run")
     ap.add_argument("--tune", choices=["all", "splits"], default="all",
                     help="--batch: autotune precision, tile and split-K per instance, or split-K only")
+    ap.add_argument("--prep-passes", type=int, nargs="+", default=[0],
+                    help="--batch: passes of image rows per trial-prep block, one run each (0: the batch's choice)")
     args = ap.parse_args(argv)
     if args.batch > 0:
-        print(json.dumps(batch_report(args.batch, args.iters, args.precision, args.tune)), flush=True)
+        for rep in batch_report(args.batch, args.iters, args.precision, args.tune, args.prep_passes):
+            print(json.dumps(rep), flush=True)
         return
     for w in args.workloads:
         if args.cg > 0:

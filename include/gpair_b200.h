@@ -389,9 +389,17 @@ typedef struct gpair_batch gpair_batch;
  * iteration, for a breakdown of where an iteration's time goes. The stamps
  * themselves add one small kernel per launch. */
 #define GPAIR_BATCH_STAGE_STAMPS 4
+/* Staged batches only: passes of image rows per block of the grouped trial-image
+ * prep, p = 1, 2, 4, ..., 32 (0 or absent: the smallest that brings the launch
+ * within four waves of resident blocks). Trial images at most 256 pixels wide sum
+ * their flux and regulariser per image row, so p changes no result; wider ones
+ * keep the grid of their single launch. gpair_batch_prep_passes returns the
+ * passes a staged batch uses (0: not staged). */
+#define GPAIR_BATCH_PREP_PASSES(p) (((p) & 63) << 8)
 int gpair_batch_create(gpair_batch **batch, gpair_ctx **ctx, int n, int line_search);
 int gpair_batch_create_ex(gpair_batch **batch, gpair_ctx **ctx, int n, int line_search, int flags);
 int gpair_batch_grouped(const gpair_batch *batch);
+int gpair_batch_prep_passes(const gpair_batch *batch);
 /* Stage stamps of a batch created with GPAIR_BATCH_STAGE_STAMPS; returns the
  * number of words (39), or 0 without stamps. Positions 0-18: the device timer
  * (ns) at the pre-phase start, then after the image prep, criterion forwards,

@@ -975,6 +975,60 @@ def test_batch_graph_equals_separate_runs(ls, independent, pair, mixed, prec, fw
             r.close()
 
 
+def test_staged_trial_prep_passes_change_no_result():
+    """Consistency check (library against itself): a staged batch's trial prep
+    with 1 to 32 passes of image rows per block (GPAIR_BATCH_PREP_PASSES) gives
+    the separate runs bit for bit -- the trial flux and regulariser are summed
+    per image row, then over the rows in a fixed order -- and a pass count that
+    is not a power of two is refused."""
+    from gpair_b200.instances import instance
+    ps = [instance(20_000_000 + k) for k in range(4)]
+    recs = [g.Reconstructor(0) for _ in ps]
+    try:
+        for r, p in zip(recs, ps):
+            r.set_problem(p)
+            r.set_precision(g.PREC_SPLIT16F8)
+        singles, imgs = [], []
+        for r, p in zip(recs, ps):
+            r.set_image(p.start_image())
+            singles.append(r.cg(5, method=2, line_search=g.LS_BATCH))
+            imgs.append(r.get_image())
+        for passes in (0, 2, 32):
+            for r, p in zip(recs, ps):
+                r.set_image(p.start_image())
+            with g.api.Batch(recs, line_search=g.LS_BATCH, prep_passes=passes) as b:
+                assert b.grouped == 2
+                assert b.prep_passes == (passes or b.prep_passes) and b.prep_passes >= 1
+                out = b.run(5)
+                for r, a, o, img in zip(recs, singles, out, imgs):
+                    assert o["status"] == 0 and o["iterations"] == 5
+                    assert o["J"] == a["J"] and o["criterion_evals"] == a["criterion_evals"]
+                    assert np.array_equal(r.get_image(), img)
+        with pytest.raises(g.GpairError):
+            g.api.Batch(recs, line_search=g.LS_BATCH, prep_passes=3)
+    finally:
+        for r in recs:
+            r.close()
+
+
+@pytest.mark.parametrize("prec", [g.PREC_SPLIT16, g.PREC_SPLIT16F8])
+@pytest.mark.parametrize("width", [33, 44])
+def test_batched_line_search_matches_fp64_at_ragged_widths(rec, prec, width):
+    """The tensor-core trial prep on rows that are not a multiple of 8 pixels
+    (33: the scalar row path; 44: also not a multiple of 8) against the FP64
+    oracle's batched search."""
+    w, oi = synth.make_workload_data("tiny", 21, 22, 23)
+    p = g.problem_from_oifits(oi, width, w.pixellation_mas * w.image_width / width, w.alpha)
+    rec.set_problem(p)
+    rec.set_precision(prec)
+    img0 = p.start_image()
+    _, tr = O.reconstruct64(p, img0, 3, line_search=1)
+    rec.set_image(img0)
+    out = rec.cg(3, method=2, trace=True, line_search=g.LS_BATCH)
+    assert np.allclose(out["trace_J"][:3], tr["J"][:3], rtol=1e-5)
+    assert np.allclose(out["trace_step"][:2], tr["step"][:2], rtol=1e-12)
+
+
 def test_shared_splits_keep_parity_and_staged_batches_exact():
     """gpair_set_shared_splits on contexts that run together: longer adjoint
     splits (fewer partial images); the data gradient still meets 1e-5 against the
