@@ -70,3 +70,22 @@ def test_library_is_built_for_sm100a_only():
     # the build passes -gencode arch=compute_100a,code=sm_100a and nothing else
     from gpair_b200 import build as B
     assert B.ARCH == ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def test_batch_flags_are_checked_before_any_context_is_touched():
+    """gpair_batch_create_ex refuses unknown flag bits and a trial-prep pass count
+    that is not a power of two (GPAIR_ERR_INVALID) before it reads a context; a
+    valid pass count then reaches the context check (a null context:
+    GPAIR_ERR_STATE). No GPU call is made."""
+    from gpair_b200 import api
+    lib = g.lib()
+    b = C.c_void_p()
+    arr = (C.c_void_p * 1)(None)
+    assert api.batch_prep_passes(4) == 4 << 8
+    for flags in (api.batch_prep_passes(3), api.batch_prep_passes(6), 1 << 14, 1 << 3):
+        assert lib.gpair_batch_create_ex(C.byref(b), arr, 1, api.LS_BATCH, flags) == -1, flags  # INVALID
+        assert not b.value
+    for p in (0, 1, 2, 4, 8, 16, 32):
+        assert lib.gpair_batch_create_ex(C.byref(b), arr, 1, api.LS_BATCH, api.batch_prep_passes(p)) == -4, p
+        assert not b.value
+    assert lib.gpair_batch_prep_passes(None) == 0
