@@ -415,7 +415,8 @@ def many_instances(n: int, iters: int, precision: int) -> dict:
                 t0 = time.perf_counter()
                 res_b = b.run(iters)
                 dt = time.perf_counter() - t0
-                one[mode] = {"s": dt, "grouped": b.grouped, "all_ok": all(r_["status"] == 0 for r_ in res_b),
+                one[mode] = {"s": dt, "grouped": b.grouped, "prep_passes": b.prep_passes,
+                             "all_ok": all(r_["status"] == 0 for r_ in res_b),
                              "tflops": sum(r.last_run_stats()[1] for r in recs) / max(dt, 1e-12) / 1e12}
         t_one = one["staged"]["s"]
     finally:
@@ -429,6 +430,7 @@ def many_instances(n: int, iters: int, precision: int) -> dict:
             "tflops_sequential": flops / max(t_seq, 1e-12) / 1e12,
             "one_launch_s": t_one, "one_launch_speedup": t_seq / max(t_one, 1e-12),
             "tflops_one_launch": one["staged"]["tflops"], "one_launch_grouped": one["staged"]["grouped"],
+            "one_launch_prep_passes": one["staged"]["prep_passes"],
             "one_launch_forwards_only_s": one["forwards_only"]["s"],
             "tflops_one_launch_forwards_only": one["forwards_only"]["tflops"],
             "one_launch_independent_s": one["independent"]["s"],
